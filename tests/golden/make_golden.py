@@ -1,0 +1,197 @@
+"""Generate golden input/output vectors by running the reference itself.
+
+Usage (in a container where the reference source is available):
+
+    python tests/golden/make_golden.py --ref /root/reference/src
+
+Each configuration runs in its own subprocess because the reference reads its
+parameters at import time (one process = one configuration).  The reference
+runs on the CPU in FP64 with TorchDynamo disabled (its ``@torch.compile``
+functions then run eagerly, which the reference documents as bit-identical).
+
+Outputs ``tests/golden/<name>.npz``.  Inputs are seeded numpy draws; the
+fixtures hold both inputs and reference outputs so the tests never need the
+reference at run time.
+"""
+
+import argparse
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+SHT_CONFIGS = {
+    # name: (configure dict, batch columns, store tables)
+    "sht_l16": ({"l_max": 16, "minc": 1, "n_r_max": 5}, 3, True),
+    "sht_l32m4": ({"l_max": 32, "minc": 4, "n_r_max": 5}, 3, True),
+    "sht_l20": ({"l_max": 20, "minc": 1, "n_r_max": 5}, 2, True),
+    "sht_l31m2": ({"l_max": 31, "minc": 2, "n_r_max": 5}, 2, True),
+    "sht_l64": ({"l_max": 64, "minc": 1, "n_r_max": 5}, 1, False),
+}
+
+NL_CONFIGS = {
+    "nl_bouss": {"l_max": 8, "minc": 1, "n_r_max": 4, "mode": 0},
+    "nl_anel": {"l_max": 8, "minc": 1, "n_r_max": 5, "strat": 5.0, "polind": 2.0,
+                "g0": 0.0, "g1": 0.0, "g2": 1.0, "mode": 0, "ek": 1e-4, "ra": 3e6},
+}
+
+
+def _spec(rng, lm_max, l_of_lm, B, decay=1.0):
+    """Random complex spectrum with |c| ~ (l+1)^-decay."""
+    amp = (l_of_lm.astype(np.float64) + 1.0) ** (-decay)
+    x = (rng.standard_normal((lm_max, B)) + 1j * rng.standard_normal((lm_max, B)))
+    return x * amp[:, None]
+
+
+def worker_sht(name, ref):
+    cfg, B, tables = SHT_CONFIGS[name]
+    cfg = dict(cfg, device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, sht, plms, horizontal_data as hd, blocking
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))
+    n = lambda x: x.detach().cpu().numpy()
+    rng = np.random.default_rng(1234)
+    lm, nt, npp = params.lm_max, params.n_theta_max, params.n_phi_max
+    l_of = n(blocking.st_lm2l)
+    out = dict(l_max=params.l_max, minc=params.minc, lm_max=lm,
+               n_theta_max=nt, n_phi_max=npp, n_m_max=params.n_m_max)
+    # Slm keeps a nonzero imaginary part at m=0: irfft must drop it.
+    Slm = _spec(rng, lm, l_of, B)
+    Q, S, T = (_spec(rng, lm, l_of, B) for _ in range(3))
+    grid = rng.standard_normal((B, nt, npp))
+    vt = rng.standard_normal((B, nt, npp))
+    vp = rng.standard_normal((B, nt, npp))
+    or2 = 1.0 + rng.random(B)
+    Bl, ddB, J, dJ = (_spec(rng, lm, l_of, B) for _ in range(4))
+    out.update(Slm=Slm, Q=Q, S=S, T=T, grid=grid, vt=vt, vp=vp, or2=or2,
+               Bl=Bl, ddB=ddB, J=J, dJ=dJ)
+    out["scal_to_spat"] = n(sht.scal_to_spat(t(Slm)))
+    out["scal_to_spat_1d"] = n(sht.scal_to_spat(t(Slm[:, 0].copy())))
+    out["scal_to_SH"] = n(sht.scal_to_SH(t(grid)))
+    out["scal_to_SH_1d"] = n(sht.scal_to_SH(t(grid[0].copy())))
+    br, bt, bp = sht.torpol_to_spat(t(Q), t(S), t(T))
+    out.update(torpol_br=n(br), torpol_bt=n(bt), torpol_bp=n(bp))
+    br1, bt1, bp1 = sht.torpol_to_spat(t(Q[:, 0].copy()), t(S[:, 0].copy()), t(T[:, 0].copy()))
+    out.update(torpol1_br=n(br1), torpol1_bt=n(bt1), torpol1_bp=n(bp1))
+    s_, t_ = sht.spat_to_sphertor(t(vt), t(vp))
+    out.update(sphertor_S=n(s_), sphertor_T=n(t_))
+    s1, t1 = sht.spat_to_sphertor(t(vt[0].copy()), t(vp[0].copy()))
+    out.update(sphertor1_S=n(s1), sphertor1_T=n(t1))
+    gt, gp = sht.scal_to_grad_spat(t(Slm))
+    out.update(grad_t=n(gt), grad_p=n(gp))
+    out["curlr"] = n(sht.pol_to_curlr_spat(t(Q)))
+    pg_t, pg_p = sht.pol_to_grad_spat(t(S))
+    out.update(polgrad_t=n(pg_t), polgrad_p=n(pg_p))
+    dt_, dp_ = sht.torpol_to_dphspat(t(S[:, 0].copy()), t(T[:, 0].copy()))
+    out.update(dph_t=n(dt_), dph_p=n(dp_))
+    cr, ct, cp = sht.torpol_to_curl_spat(t(or2), t(Bl), t(ddB), t(J), t(dJ))
+    out.update(curl_r=n(cr), curl_t=n(ct), curl_p=n(cp))
+    st_t, st_p = sht.sphtor_to_spat(t(S[:, 0].copy()), t(T[:, 0].copy()))
+    out.update(sphtor_t=n(st_t), sphtor_p=n(st_p))
+    q_, s2, t2 = sht.spat_to_qst(t(grid[0].copy()), t(vt[0].copy()), t(vp[0].copy()))
+    out.update(qst_q=n(q_), qst_s=n(s2), qst_t=n(t2))
+    e10 = np.zeros(lm, dtype=np.complex128)
+    e10[1] = 1.0
+    out["y10"] = n(sht.scal_to_spat(t(e10)))
+    if tables:
+        out.update(theta_ord=n(hd.theta_ord), gauss=n(hd.gauss), Plm=n(plms.Plm),
+                   dPlm=n(plms.dPlm), wPlm=n(plms.wPlm), wdPlm=n(plms.wdPlm),
+                   O_sin_theta_E2_grid=n(hd.O_sin_theta_E2_grid),
+                   cosn_theta_E2_grid=n(hd.cosn_theta_E2_grid))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def worker_nl(name, ref):
+    cfg = dict(NL_CONFIGS[name], device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, radial_functions as rf, horizontal_data as hd
+    from magic_torch import pre_calculations as pc, courant
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))
+    n = lambda x: x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x)
+    rng = np.random.default_rng(99)
+    N, nt, npp = params.n_r_max, params.n_theta_max, params.n_phi_max
+    out = dict(n_r_max=N, n_theta_max=nt, n_phi_max=npp, l_max=params.l_max,
+               or1=n(rf.or1), or2=n(rf.or2), or4=n(rf.or4), r=n(rf.r) if hasattr(rf, "r") else None,
+               orho1=n(rf.orho1), orho2=n(rf.orho2), otemp1=n(rf.otemp1),
+               beta=n(rf.beta), visc=n(rf.visc), lambda_=n(rf.lambda_),
+               delxr2=n(rf.delxr2), delxh2=n(rf.delxh2),
+               ViscHeatFac=float(rf.ViscHeatFac), OhmLossFac=float(rf.OhmLossFac),
+               LFfac=float(pc.LFfac), opm=float(pc.opm),
+               ost2=n(hd.O_sin_theta_E2_grid), cosn=n(hd.cosn_theta_E2_grid))
+    from magic_torch.radial_scheme import r as r_grid
+    out["r"] = n(r_grid)
+    g = lambda: rng.standard_normal((N, nt, npp))
+    if name == "nl_bouss":
+        from magic_torch.get_nl import get_nl
+        names = ["vr", "vt", "vp", "cvr", "cvt", "cvp", "s", "br", "bt", "bp",
+                 "cbr", "cbt", "cbp", "xi"]
+        ins = {k: g() for k in names}
+        res = get_nl(*[t(ins[k]) for k in names])
+        onames = ["Advr", "Advt", "Advp", "VSr", "VSt", "VSp", "VxBr", "VxBt", "VxBp",
+                  "VXir", "VXit", "VXip"]
+        out.update(ins)
+        out.update({"out_" + k: n(v) for k, v in zip(onames, res)})
+        # Courant: damped magnetic (default), undamped, and non-magnetic forms.
+        courfac, alffac = 2.5, 1.0
+        out.update(courfac=courfac, alffac=alffac)
+        d1, d2 = courant.courant_check(t(ins["vr"]), t(ins["vt"]), t(ins["vp"]),
+                                       t(ins["br"]), t(ins["bt"]), t(ins["bp"]),
+                                       courfac=courfac, alffac=alffac)
+        out.update(cour_damp_r=n(d1), cour_damp_h=n(d2))
+        d1, d2 = courant.courant_check(t(ins["vr"]), t(ins["vt"]), t(ins["vp"]),
+                                       courfac=courfac, alffac=alffac)
+        out.update(cour_nomag_r=n(d1), cour_nomag_h=n(d2))
+        vr2, vh2 = courant._courant_mag_nodamp(
+            t(ins["vr"]), t(ins["vt"]), t(ins["vp"]), t(ins["br"]), t(ins["bt"]),
+            t(ins["bp"]), courfac ** 2, alffac ** 2)
+        out.update(cour_nodamp_vr2=n(vr2), cour_nodamp_vh2=n(vh2))
+        cases = [(1e-4, 1e-4, 1e-3, 2e-3), (2e-4, 1e-4, 1e-5, 3e-5),
+                 (1e-6, 1e-4, 1e-3, 1e-3), (1e-5, 1e-4, 3e-5, 1e-4)]
+        res = [courant.dt_courant(*c) for c in cases]
+        out["dtc_cases"] = np.array(cases)
+        out["dtc_changed"] = np.array([r_[0] for r_ in res])
+        out["dtc_new"] = np.array([r_[1] for r_ in res])
+    else:
+        from magic_torch.get_nl_anel import get_nl_anel
+        names = ["vr", "vt", "vp", "dvrdr", "dvtdr", "dvpdr", "dvrdt", "dvrdp",
+                 "dvtdp", "dvpdp", "cvr", "s", "xi", "br", "bt", "bp", "cbr", "cbt", "cbp"]
+        ins = {k: g() for k in names}
+        res = get_nl_anel(*[t(ins[k]) for k in names])
+        onames = ["Advr", "Advt", "Advp", "VSr", "VSt", "VSp", "VxBr", "VxBt", "VxBp",
+                  "VXir", "VXit", "VXip", "heat"]
+        out.update(ins)
+        out.update({"out_" + k: n(v) for k, v in zip(onames, res)})
+    out = {k: v for k, v in out.items() if v is not None}
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--worker", default=None)
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    if a.worker:
+        (worker_sht if a.worker in SHT_CONFIGS else worker_nl)(a.worker, a.ref)
+        return
+    env = dict(os.environ, TORCHDYNAMO_DISABLE="1", MAGIC_DEVICE="cpu")
+    names = list(SHT_CONFIGS) + list(NL_CONFIGS)
+    if a.only:
+        names = [x for x in names if x in a.only.split(",")]
+    for name in names:
+        print("golden:", name, flush=True)
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--worker", name,
+                        "--ref", a.ref], check=True, env=env, cwd="/tmp")
+
+
+if __name__ == "__main__":
+    main()

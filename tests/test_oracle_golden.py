@@ -1,0 +1,141 @@
+"""Pin the CPU oracle against golden vectors produced by the reference itself.
+
+Tolerance: 1e-12 normwise relative (both sides FP64; differences are rounding
+order only).  Tables are pinned at 1e-13.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_err
+from oracle import grid as og
+from oracle import nonlinear as onl
+from oracle import sht as osht
+
+SHT = ["sht_l16", "sht_l32m4", "sht_l20", "sht_l31m2", "sht_l64"]
+TOL = 1e-12
+
+_grids = {}
+
+
+def _grid(z):
+    key = (int(z["l_max"]), int(z["minc"]))
+    if key not in _grids:
+        _grids[key] = og.Grid(*key)
+    return _grids[key]
+
+
+@pytest.mark.parametrize("name", SHT)
+def test_sizes(name):
+    z = load_golden(name)
+    s = og.grid_sizes(int(z["l_max"]), int(z["minc"]))
+    for k in ("lm_max", "n_theta_max", "n_phi_max", "n_m_max"):
+        assert s[k] == int(z[k]), k
+
+
+@pytest.mark.parametrize("name", [n for n in SHT if n != "sht_l64"])
+def test_tables(name):
+    z = load_golden(name)
+    g = _grid(z)
+    assert rel_err(g.theta_ord, z["theta_ord"]) < 1e-14
+    assert rel_err(g.gauss, z["gauss"]) < 1e-13
+    for k in ("Plm", "dPlm", "wPlm", "wdPlm"):
+        assert rel_err(getattr(g, k), z[k]) < 1e-13, k
+    assert rel_err(g.O_sin_theta_E2_grid, z["O_sin_theta_E2_grid"]) < 1e-13
+    assert rel_err(g.cosn_theta_E2_grid, z["cosn_theta_E2_grid"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", SHT)
+def test_scalar(name):
+    z = load_golden(name)
+    g = _grid(z)
+    assert rel_err(osht.scal_to_spat(g, z["Slm"]), z["scal_to_spat"]) < TOL
+    assert rel_err(osht.scal_to_spat(g, z["Slm"][:, 0]), z["scal_to_spat_1d"]) < TOL
+    assert rel_err(osht.scal_to_SH(g, z["grid"]), z["scal_to_SH"]) < TOL
+    assert rel_err(osht.scal_to_SH(g, z["grid"][0]), z["scal_to_SH_1d"]) < TOL
+    assert rel_err(osht.scal_to_spat(g, np.eye(1, int(z["lm_max"]), 1)[0].astype(complex)),
+                   z["y10"]) < TOL
+
+
+@pytest.mark.parametrize("name", SHT)
+def test_vector(name):
+    z = load_golden(name)
+    g = _grid(z)
+    br, bt, bp = osht.torpol_to_spat(g, z["Q"], z["S"], z["T"])
+    assert rel_err(br, z["torpol_br"]) < TOL
+    assert rel_err(bt, z["torpol_bt"]) < TOL
+    assert rel_err(bp, z["torpol_bp"]) < TOL
+    br, bt, bp = osht.torpol_to_spat(g, z["Q"][:, 0], z["S"][:, 0], z["T"][:, 0])
+    assert rel_err(bt, z["torpol1_bt"]) < TOL and rel_err(bp, z["torpol1_bp"]) < TOL
+    s, t = osht.spat_to_sphertor(g, z["vt"], z["vp"])
+    assert rel_err(s, z["sphertor_S"]) < TOL
+    assert rel_err(t, z["sphertor_T"]) < TOL
+    s, t = osht.spat_to_sphertor(g, z["vt"][0], z["vp"][0])
+    assert rel_err(s, z["sphertor1_S"]) < TOL and rel_err(t, z["sphertor1_T"]) < TOL
+
+
+@pytest.mark.parametrize("name", SHT)
+def test_helpers(name):
+    z = load_golden(name)
+    g = _grid(z)
+    gt, gp = osht.scal_to_grad_spat(g, z["Slm"])
+    assert rel_err(gt, z["grad_t"]) < TOL and rel_err(gp, z["grad_p"]) < TOL
+    assert rel_err(osht.pol_to_curlr_spat(g, z["Q"]), z["curlr"]) < TOL
+    pt, pp = osht.pol_to_grad_spat(g, z["S"])
+    assert rel_err(pt, z["polgrad_t"]) < TOL and rel_err(pp, z["polgrad_p"]) < TOL
+    dt, dp = osht.torpol_to_dphspat(g, z["S"][:, 0], z["T"][:, 0])
+    assert rel_err(dt, z["dph_t"]) < TOL and rel_err(dp, z["dph_p"]) < TOL
+    cr, ct, cp = osht.torpol_to_curl_spat(g, z["or2"], z["Bl"], z["ddB"], z["J"], z["dJ"])
+    assert rel_err(cr, z["curl_r"]) < TOL
+    assert rel_err(ct, z["curl_t"]) < TOL
+    assert rel_err(cp, z["curl_p"]) < TOL
+    vt, vp = osht.sphtor_to_spat(g, z["S"][:, 0], z["T"][:, 0])
+    assert rel_err(vt, z["sphtor_t"]) < TOL and rel_err(vp, z["sphtor_p"]) < TOL
+    q, s, t = osht.spat_to_qst(g, z["grid"][0], z["vt"][0], z["vp"][0])
+    assert rel_err(q, z["qst_q"]) < TOL
+    assert rel_err(s, z["qst_s"]) < TOL and rel_err(t, z["qst_t"]) < TOL
+
+
+def test_get_nl():
+    z = load_golden("nl_bouss")
+    names = ["vr", "vt", "vp", "cvr", "cvt", "cvp", "s", "br", "bt", "bp",
+             "cbr", "cbt", "cbp", "xi"]
+    res = onl.get_nl(*[z[k] for k in names], z["or2"], z["or4"], z["ost2"], float(z["LFfac"]))
+    onames = ["Advr", "Advt", "Advp", "VSr", "VSt", "VSp", "VxBr", "VxBt", "VxBp",
+              "VXir", "VXit", "VXip"]
+    for k, v in zip(onames, res):
+        assert rel_err(v, z["out_" + k]) < 1e-14, k
+
+
+def test_get_nl_anel():
+    z = load_golden("nl_anel")
+    names = ["vr", "vt", "vp", "dvrdr", "dvtdr", "dvpdr", "dvrdt", "dvrdp",
+             "dvtdp", "dvpdp", "cvr", "s", "xi", "br", "bt", "bp", "cbr", "cbt", "cbp"]
+    prof = [z[k] for k in ("r", "or1", "or2", "or4", "beta", "orho1", "otemp1",
+                           "visc", "lambda_", "ost2", "cosn")]
+    res = onl.get_nl_anel(*[z[k] for k in names], *prof, float(z["LFfac"]),
+                          float(z["ViscHeatFac"]), float(z["OhmLossFac"]))
+    onames = ["Advr", "Advt", "Advp", "VSr", "VSt", "VSp", "VxBr", "VxBt", "VxBp",
+              "VXir", "VXit", "VXip", "heat"]
+    assert float(z["OhmLossFac"]) != 0.0 and float(z["ViscHeatFac"]) != 0.0
+    for k, v in zip(onames, res):
+        assert rel_err(v, z["out_" + k]) < 1e-13, k
+
+
+def test_courant():
+    z = load_golden("nl_bouss")
+    common = dict(courfac=float(z["courfac"]), alffac=float(z["alffac"]), or2=z["or2"],
+                  or4=z["or4"], orho1=z["orho1"], orho2=z["orho2"], ost2=z["ost2"],
+                  delxr2=z["delxr2"], delxh2=z["delxh2"], LFfac=float(z["LFfac"]),
+                  opm=float(z["opm"]))
+    r, h = onl.courant_check(z["vr"], z["vt"], z["vp"], z["br"], z["bt"], z["bp"], **common)
+    assert rel_err(r, z["cour_damp_r"]) < 1e-14 and rel_err(h, z["cour_damp_h"]) < 1e-14
+    r, h = onl.courant_check(z["vr"], z["vt"], z["vp"], None, None, None, **common)
+    assert rel_err(r, z["cour_nomag_r"]) < 1e-14 and rel_err(h, z["cour_nomag_h"]) < 1e-14
+    r, h = onl.courant_check(z["vr"], z["vt"], z["vp"], z["br"], z["bt"], z["bp"],
+                             damp=False, **common)
+    np.testing.assert_allclose(r, np.sqrt(z["delxr2"] / z["cour_nodamp_vr2"]), rtol=1e-14)
+    np.testing.assert_allclose(h, np.sqrt(z["delxh2"] / z["cour_nodamp_vh2"]), rtol=1e-14)
+    for case, ch, new in zip(z["dtc_cases"], z["dtc_changed"], z["dtc_new"]):
+        c2, n2 = onl.dt_courant(*case)
+        assert c2 == bool(ch) and n2 == new
