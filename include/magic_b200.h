@@ -1,0 +1,204 @@
+/*
+ * magic_b200 — C ABI of the B200 (sm_100a) pseudo-spectral nonlinear stage.
+ *
+ * Replaces, for the spherical-shell dynamo code torch-magic, the Python
+ * functions of its transform module (magic_torch/sht.py) and of its
+ * nonlinear-term builders (magic_torch/get_nl.py, get_nl_anel.py,
+ * courant.py).  Each entry point below names the reference function it
+ * replaces (path:line inside the reference project).
+ *
+ * Conventions (identical to the reference):
+ *   - spectral arrays: complex128 stored as interleaved (re, im) doubles,
+ *     shape (lm_max, B) row-major with row stride `ld` complex elements
+ *     (ld >= B), m-major lm order: lm = lStart[m/minc] + (l - m);
+ *   - grid arrays: float64, shape (B, n_theta_max, n_phi_max) contiguous,
+ *     theta rows interleaved [N0, S0, N1, S1, ...];
+ *   - synthesis = irfft(norm="forward") (unscaled), analysis =
+ *     rfft(norm="forward") (scaled by 1/n_phi); the FFT index is m/minc.
+ *
+ * All pointers except `mt_plan*` and the `*_desc`/`*_params` structs are
+ * DEVICE pointers owned by the caller.  `work` is caller-owned device
+ * scratch of at least the size the matching `mt_*_workspace` query returns.
+ * No entry point synchronises the host; all work is enqueued on `stream`
+ * (a cudaStream_t passed as void*).  Return value: 0 (MT_OK) or an
+ * mt_status code; mt_last_error() gives a message (thread-local).
+ *
+ * Plans are read-only after creation: several host threads may use one plan
+ * concurrently on different streams with different workspaces.
+ */
+#ifndef MAGIC_B200_H
+#define MAGIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MT_API __attribute__((visibility("default")))
+#else
+#define MT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mt_plan mt_plan;
+
+enum mt_status {
+  MT_OK = 0,
+  MT_ERR_ARG = 1,         /* bad argument (null pointer, bad size, ...)     */
+  MT_ERR_CUDA = 2,        /* a CUDA runtime call failed                     */
+  MT_ERR_UNSUPPORTED = 3, /* grid or option this build does not handle      */
+  MT_ERR_WORKSPACE = 4,   /* workspace smaller than the query returned      */
+  MT_ERR_NO_DEVICE = 5    /* no sm_100 device visible                       */
+};
+
+enum mt_precision {
+  MT_PREC_FP64 = 0,       /* plain FP64 Legendre contractions (DMMA)        */
+  MT_PREC_SPLIT = 1       /* split-BF16 tcgen05 contractions, FP32 accumulate */
+};
+
+/* Grid description.  n_theta_max / n_phi_max = 0 derive the reference's
+ * sizes from l_max (magic_torch/params.py:57-76). */
+typedef struct {
+  int l_max;
+  int minc;
+  int n_theta_max;
+  int n_phi_max;          /* points per azimuthal sector (n_phi_tot / minc) */
+  int precision;          /* enum mt_precision                               */
+} mt_grid_desc;
+
+typedef struct {
+  int l_max, minc, n_theta_max, n_phi_max, n_m_max, lm_max, nhs, precision;
+} mt_plan_info;
+
+/* Build all horizontal tables on the current device: Gauss-Legendre nodes
+ * and weights (replaces magic_torch/horizontal_data.py:16-50), P_l^m and
+ * sin(theta) dP_l^m/dtheta in FP64 (replaces magic_torch/plms.py:21-186),
+ * FFT twiddles.  Synchronous. */
+MT_API int mt_plan_create(const mt_grid_desc* desc, mt_plan** plan);
+MT_API int mt_plan_destroy(mt_plan* plan);
+MT_API int mt_plan_get_info(const mt_plan* plan, mt_plan_info* info);
+
+/* Copy the plan's FP64 tables to caller device buffers (any may be NULL):
+ * theta_ord, gauss (n_theta_max, geographic order), Plm, dPlm (lm_max, nhs).
+ * Used to check the tables against the oracle. */
+MT_API int mt_plan_copy_tables(const mt_plan* plan, double* theta_ord, double* gauss,
+                        double* plm, double* dplm, void* stream);
+
+/* ---- transforms (magic_torch/sht.py) ------------------------------------ */
+
+/* Workspace bytes for a transform over B columns (all four transforms and the
+ * helpers below use the same query). */
+MT_API size_t mt_transform_workspace(const mt_plan* plan, int B, int n_fields);
+
+/* scal_to_spat (magic_torch/sht.py:298-348): Slm (lm_max, ld) -> grid. */
+MT_API int mt_scal_to_spat(const mt_plan* plan, const double* Slm, int64_t ld, int B,
+                    double* grid, void* work, size_t work_bytes, void* stream);
+
+/* scal_to_SH (magic_torch/sht.py:351-405): grid -> Slm (lm_max, ld). */
+MT_API int mt_scal_to_SH(const mt_plan* plan, const double* grid, int B, double* Slm,
+                  int64_t ld, void* work, size_t work_bytes, void* stream);
+
+/* torpol_to_spat (magic_torch/sht.py:408-497): Q,S,T -> br, bt, bp. */
+MT_API int mt_torpol_to_spat(const mt_plan* plan, const double* Q, const double* S,
+                      const double* T, int64_t ld, int B, double* br, double* bt,
+                      double* bp, void* work, size_t work_bytes, void* stream);
+
+/* spat_to_sphertor (magic_torch/sht.py:575-667): (vt, vp) -> (S, T),
+ * divided by l(l+1), l=0 set to zero. */
+MT_API int mt_spat_to_sphertor(const mt_plan* plan, const double* vt, const double* vp,
+                        int B, double* S, double* T, int64_t ld, void* work,
+                        size_t work_bytes, void* stream);
+
+/* scal_to_grad_spat (magic_torch/sht.py:500-567): Slm -> (dtheta, dphi)
+ * sin-weighted gradient grids.  pol_to_grad_spat (sht.py:706-722) is this with
+ * `scale_dlh` = 1 (input multiplied by l(l+1) on load). */
+MT_API int mt_scal_to_grad_spat(const mt_plan* plan, const double* Slm, int64_t ld, int B,
+                         int scale_dlh, double* gt, double* gp, void* work,
+                         size_t work_bytes, void* stream);
+
+/* ---- grid-space nonlinear terms ----------------------------------------- */
+
+/* get_nl (magic_torch/get_nl.py:30-87) on grids of n_r levels:
+ * in[14] = vr,vt,vp,cvr,cvt,cvp,s,br,bt,bp,cbr,cbt,cbp,xi (each n_r x n_theta
+ * x n_phi); out[12] = Advr,Advt,Advp,VSr,VSt,VSp,VxBr,VxBt,VxBp,VXir,VXit,VXip;
+ * or2, or4: (n_r); LFfac scalar. */
+MT_API int mt_get_nl(const mt_plan* plan, int n_r, const double* const* in,
+              double* const* out, const double* or2, const double* or4,
+              double LFfac, void* stream);
+
+typedef struct {
+  const double *r, *or1, *or2, *or4, *beta, *orho1, *otemp1, *visc, *lambda_;
+  double LFfac, ViscHeatFac, OhmLossFac;
+  int l_mag;
+} mt_anel_params;
+
+/* get_nl_anel (magic_torch/get_nl_anel.py:41-136): in[19] = vr,vt,vp,dvrdr,
+ * dvtdr,dvpdr,dvrdt,dvrdp,dvtdp,dvpdp,cvr,s,xi,br,bt,bp,cbr,cbt,cbp;
+ * out[13] = the 12 of get_nl followed by heatTerms. */
+MT_API int mt_get_nl_anel(const mt_plan* plan, int n_r, const double* const* in,
+                   double* const* out, const mt_anel_params* p, void* stream);
+
+typedef struct {
+  const double *or2, *or4, *orho1, *orho2, *delxr2, *delxh2; /* (n_r) */
+  double courfac, alffac, LFfac, opm;
+  int mode;               /* 0 non-magnetic, 1 magnetic damped, 2 undamped */
+} mt_courant_params;
+
+/* courant_check (magic_torch/courant.py:80-127): per-level dtrkc, dthkc
+ * (n_r) from grids vr,vt,vp[,br,bt,bp].  work: mt_courant_workspace bytes. */
+MT_API size_t mt_courant_workspace(const mt_plan* plan, int n_r);
+MT_API int mt_courant(const mt_plan* plan, int n_r, const double* vr, const double* vt,
+               const double* vp, const double* br, const double* bt,
+               const double* bp, const mt_courant_params* p, double* dtrkc,
+               double* dthkc, void* work, size_t work_bytes, void* stream);
+
+/* ---- fused nonlinear stage ---------------------------------------------- */
+
+/* Spectral inputs of the Boussinesq radial loop (magic_torch/step_time.py:
+ * 931-1213), each (lm_max, ld) complex over n_r levels (column = level).
+ * b, db, ddb, aj, dj may be NULL when l_mag = 0; xi NULL when no composition. */
+typedef struct {
+  const double *w, *dw, *ddw, *z, *dz, *s, *b, *db, *ddb, *aj, *dj, *xi;
+  int64_t ld;
+} mt_bouss_in;
+
+/* Spectral outputs over the bulk levels 1..n_r-2 (written at columns 1..n_r-2
+ * of (lm_max, ld) arrays; columns 0 and n_r-1 are left untouched):
+ * AdvrLM, AdvtLM, AdvpLM, dVSrLM, VStLM, VxBrLM, VxBtLM, VxBpLM, dVXirLM,
+ * VXitLM (the last five may be NULL as their inputs). */
+typedef struct {
+  double *Advr, *Advt, *Advp, *VSr, *VSt, *VxBr, *VxBt, *VxBp, *VXir, *VXit;
+  int64_t ld;
+} mt_bouss_out;
+
+typedef struct {
+  const double *or2, *or4, *orho1, *orho2, *delxr2, *delxh2; /* (n_r) */
+  double LFfac, courfac, alffac, opm;
+  int l_mag, l_chem, cour_mode; /* cour_mode as mt_courant_params.mode      */
+  int parts;  /* 0 = whole stage; else a mask run in order on the same work:
+                 1 Legendre synthesis, 2 phi FFT + products + Courant maxima,
+                 4 Legendre analysis + Courant steps (lets a caller time or
+                 overlap the three launches individually)                     */
+} mt_bouss_params;
+
+MT_API size_t mt_nl_bouss_workspace(const mt_plan* plan, int n_r, int l_mag, int l_chem);
+
+/* Whole nonlinear stage of one radial loop in four launches: Legendre
+ * synthesis of the 14 grid fields (inputs assembled on load: Q = l(l+1) w,
+ * T_curl = or2 l(l+1) w - ddw, ...), fused inverse phi-FFT + get_nl products
+ * + Courant maxima + forward phi-FFT, Legendre analysis of the 12 products
+ * (with the 1/l(l+1) division).  dtrkc, dthkc: (n_r) Courant steps. */
+MT_API int mt_nl_bouss(const mt_plan* plan, int n_r, const mt_bouss_in* in,
+                const mt_bouss_out* out, const mt_bouss_params* p, double* dtrkc,
+                double* dthkc, void* work, size_t work_bytes, void* stream);
+
+/* Thread-local message for the last non-zero status. */
+MT_API const char* mt_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAGIC_B200_H */

@@ -1,0 +1,118 @@
+"""ctypes binding of libmagic_b200.so (the C ABI in include/magic_b200.h).
+
+The library is built in-tree (``magic_b200/csrc/build.py``).  There is no
+fallback: if the library is missing or cannot be loaded, ``lib()`` raises.
+"""
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmagic_b200.so")
+
+MT_OK = 0
+MT_PREC_FP64 = 0
+MT_PREC_SPLIT = 1
+
+_dp = C.c_void_p  # device pointer
+_i64 = C.c_int64
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("l_max", C.c_int), ("minc", C.c_int), ("n_theta_max", C.c_int),
+                ("n_phi_max", C.c_int), ("precision", C.c_int)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("l_max", "minc", "n_theta_max", "n_phi_max",
+                                       "n_m_max", "lm_max", "nhs", "precision")]
+
+
+class AnelParams(C.Structure):
+    _fields_ = [(n, _dp) for n in ("r", "or1", "or2", "or4", "beta", "orho1", "otemp1",
+                                   "visc", "lambda_")] + \
+               [("LFfac", C.c_double), ("ViscHeatFac", C.c_double),
+                ("OhmLossFac", C.c_double), ("l_mag", C.c_int)]
+
+
+class CourantParams(C.Structure):
+    _fields_ = [(n, _dp) for n in ("or2", "or4", "orho1", "orho2", "delxr2", "delxh2")] + \
+               [("courfac", C.c_double), ("alffac", C.c_double), ("LFfac", C.c_double),
+                ("opm", C.c_double), ("mode", C.c_int)]
+
+
+class BoussIn(C.Structure):
+    _fields_ = [(n, _dp) for n in ("w", "dw", "ddw", "z", "dz", "s", "b", "db", "ddb",
+                                   "aj", "dj", "xi")] + [("ld", _i64)]
+
+
+class BoussOut(C.Structure):
+    _fields_ = [(n, _dp) for n in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt",
+                                   "VxBp", "VXir", "VXit")] + [("ld", _i64)]
+
+
+class BoussParams(C.Structure):
+    _fields_ = [(n, _dp) for n in ("or2", "or4", "orho1", "orho2", "delxr2", "delxh2")] + \
+               [("LFfac", C.c_double), ("courfac", C.c_double), ("alffac", C.c_double),
+                ("opm", C.c_double), ("l_mag", C.c_int), ("l_chem", C.c_int),
+                ("cour_mode", C.c_int), ("parts", C.c_int)]
+
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "mt_plan_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
+    "mt_plan_destroy": (C.c_int, [C.c_void_p]),
+    "mt_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
+    "mt_plan_copy_tables": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
+    "mt_transform_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int]),
+    "mt_scal_to_spat": (C.c_int, [C.c_void_p, _dp, _i64, C.c_int, _dp, _dp, C.c_size_t, _dp]),
+    "mt_scal_to_SH": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, _i64, _dp, C.c_size_t, _dp]),
+    "mt_torpol_to_spat": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp,
+                                    _dp, C.c_size_t, _dp]),
+    "mt_spat_to_sphertor": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _i64, _dp,
+                                      C.c_size_t, _dp]),
+    "mt_scal_to_grad_spat": (C.c_int, [C.c_void_p, _dp, _i64, C.c_int, C.c_int, _dp, _dp,
+                                       _dp, C.c_size_t, _dp]),
+    "mt_get_nl": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(_dp), _dp, _dp,
+                            C.c_double, _dp]),
+    "mt_get_nl_anel": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_dp), C.POINTER(_dp),
+                                 C.POINTER(AnelParams), _dp]),
+    "mt_courant_workspace": (C.c_size_t, [C.c_void_p, C.c_int]),
+    "mt_courant": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp,
+                             C.POINTER(CourantParams), _dp, _dp, _dp, C.c_size_t, _dp]),
+    "mt_nl_bouss_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "mt_nl_bouss": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(BoussIn), C.POINTER(BoussOut),
+                              C.POINTER(BoussParams), _dp, _dp, _dp, C.c_size_t, _dp]),
+    "mt_last_error": (C.c_char_p, []),
+}
+
+EXPORTED = tuple(_PROTOS)
+
+_lib = None
+
+
+def lib():
+    """Load (once) and return the library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m magic_b200.csrc.build` "
+                "(magic_b200 has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MagicError(RuntimeError):
+    pass
+
+
+def check(rc):
+    if rc != MT_OK:
+        msg = lib().mt_last_error().decode(errors="replace")
+        raise MagicError(f"magic_b200 status {rc}: {msg}")

@@ -1,0 +1,611 @@
+// extern "C" entry points (include/magic_b200.h).
+#include <algorithm>
+#include <string>
+
+#include "fourier.cuh"
+#include "legendre.cuh"
+
+namespace mt {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+// legendre_f64.cu
+template <class OP, int R>
+int launch_synth_f64(const SynthArgs<OP::NX>& a, cudaStream_t st);
+template <class OP, int R>
+int launch_anal_f64(const AnalArgs<OP::NX, OP::NO>& a, cudaStream_t st);
+
+// nonlinear.cu
+
+static int prime_decomposition(int n) {
+  // smallest 2^i 3^j 5^k >= n, i < 13, j < 7, k < 7 (magic_torch/params.py:12-24)
+  long best = -1;
+  for (int i = 0; i < 13; ++i)
+    for (int j = 0; j < 7; ++j)
+      for (int k = 0; k < 7; ++k) {
+        long v = 1;
+        for (int q = 0; q < i; ++q) v *= 2;
+        for (int q = 0; q < j; ++q) v *= 3;
+        for (int q = 0; q < k; ++q) v *= 5;
+        if (v >= n && (best < 0 || v < best)) best = v;
+      }
+  return (int)best;
+}
+
+static int check_plan(const mt_plan* p) {
+  MT_REQUIRE(p != nullptr, MT_ERR_ARG, "null plan");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == p->device, MT_ERR_ARG, "plan used on a different device than it was built on");
+  return MT_OK;
+}
+
+#define MT_TRY(expr)              \
+  do {                            \
+    int _rc = (expr);             \
+    if (_rc != MT_OK) return _rc; \
+  } while (0)
+
+static size_t fourier_bytes(const mt_plan* p, int64_t ncols) {
+  return (size_t)p->n_m * p->n_theta * ncols * sizeof(double2);
+}
+
+}  // namespace mt
+
+using namespace mt;
+
+extern "C" {
+
+const char* mt_last_error(void) { return g_err.c_str(); }
+
+int mt_plan_create(const mt_grid_desc* desc, mt_plan** out) {
+  MT_REQUIRE(desc && out, MT_ERR_ARG, "null argument");
+  *out = nullptr;
+  MT_REQUIRE(desc->l_max >= 1 && desc->minc >= 1 && desc->minc <= desc->l_max + 1, MT_ERR_ARG,
+             "l_max >= 1 and 1 <= minc required");
+  MT_REQUIRE(desc->precision == MT_PREC_FP64, MT_ERR_UNSUPPORTED,
+             "this library build supports MT_PREC_FP64 plans only");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return MT_ERR_NO_DEVICE;
+  }
+  int dev = 0;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  MT_CHECK_CUDA(cudaGetDeviceProperties(&prop, dev));
+  MT_REQUIRE(prop.major == 10, MT_ERR_NO_DEVICE, "an sm_100 (B200) device is required");
+
+  mt_plan* p = new mt_plan();
+  p->desc = *desc;
+  p->device = dev;
+  p->l_max = desc->l_max;
+  p->minc = desc->minc;
+  int n_phi_tot = prime_decomposition(2 * ((30 * desc->l_max) / 20));
+  p->n_phi = desc->n_phi_max > 0 ? desc->n_phi_max : n_phi_tot / desc->minc;
+  p->n_theta = desc->n_theta_max > 0 ? desc->n_theta_max : n_phi_tot / 2;
+  p->n_m = desc->l_max / desc->minc + 1;
+  p->lm_max = 0;
+  for (int m = 0; m <= desc->l_max; m += desc->minc) p->lm_max += desc->l_max - m + 1;
+  p->nhs = p->n_theta / 2;
+  p->precision = desc->precision;
+  auto fail = [&](int code, const char* msg) {
+    set_error(msg);
+    mt_plan_destroy(p);
+    return code;
+  };
+  if (p->n_theta < 2 || p->n_theta % 2) return fail(MT_ERR_UNSUPPORTED, "n_theta_max must be even");
+  if (p->n_phi > fft_max_nphi()) return fail(MT_ERR_UNSUPPORTED, "n_phi_max above 1280");
+  if (2 * (p->n_m - 1) >= p->n_phi)
+    return fail(MT_ERR_UNSUPPORTED, "n_phi_max too small for l_max/minc (modes alias)");
+  int rc = build_tables(p);
+  if (rc != MT_OK) {
+    std::string keep = g_err;
+    mt_plan_destroy(p);
+    g_err = keep;
+    return rc;
+  }
+  *out = p;
+  return MT_OK;
+}
+
+int mt_plan_destroy(mt_plan* p) {
+  if (!p) return MT_OK;
+  void* ptrs[] = {p->d_lstart, p->d_theta, p->d_gauss, p->d_plm, p->d_dplm, p->d_dlh,
+                  p->d_wq,     p->d_wq_v,  p->d_ost2,  p->d_cosn, p->d_twiddle};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+  return MT_OK;
+}
+
+int mt_plan_get_info(const mt_plan* p, mt_plan_info* info) {
+  MT_REQUIRE(p && info, MT_ERR_ARG, "null argument");
+  info->l_max = p->l_max;
+  info->minc = p->minc;
+  info->n_theta_max = p->n_theta;
+  info->n_phi_max = p->n_phi;
+  info->n_m_max = p->n_m;
+  info->lm_max = p->lm_max;
+  info->nhs = p->nhs;
+  info->precision = p->precision;
+  return MT_OK;
+}
+
+int mt_plan_copy_tables(const mt_plan* p, double* theta, double* gauss, double* plm, double* dplm,
+                        void* stream) {
+  MT_TRY(check_plan(p));
+  cudaStream_t st = (cudaStream_t)stream;
+  size_t tsz = (size_t)p->lm_max * p->nhs * sizeof(double);
+  if (theta)
+    MT_CHECK_CUDA(cudaMemcpyAsync(theta, p->d_theta, p->n_theta * 8, cudaMemcpyDeviceToDevice, st));
+  if (gauss)
+    MT_CHECK_CUDA(cudaMemcpyAsync(gauss, p->d_gauss, p->n_theta * 8, cudaMemcpyDeviceToDevice, st));
+  if (plm) MT_CHECK_CUDA(cudaMemcpyAsync(plm, p->d_plm, tsz, cudaMemcpyDeviceToDevice, st));
+  if (dplm) MT_CHECK_CUDA(cudaMemcpyAsync(dplm, p->d_dplm, tsz, cudaMemcpyDeviceToDevice, st));
+  return MT_OK;
+}
+
+size_t mt_transform_workspace(const mt_plan* p, int B, int n_fields) {
+  if (!p || B < 1 || n_fields < 1) return 0;
+  return fourier_bytes(p, (int64_t)B * n_fields);
+}
+
+static int check_ws(const mt_plan* p, int B, int nf, size_t bytes, const void* work) {
+  MT_REQUIRE(B >= 1, MT_ERR_ARG, "B >= 1 required");
+  MT_REQUIRE(work != nullptr, MT_ERR_ARG, "null workspace");
+  MT_REQUIRE(bytes >= mt_transform_workspace(p, B, nf), MT_ERR_WORKSPACE, "workspace too small");
+  return MT_OK;
+}
+
+int mt_scal_to_spat(const mt_plan* p, const double* Slm, int64_t ld, int B, double* grid,
+                    void* work, size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(Slm && grid && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
+  MT_TRY(check_ws(p, B, 1, work_bytes, work));
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* F = (double2*)work;
+  SynthArgs<1> s{};
+  s.t = p->tab;
+  s.src[0] = {(const double2*)Slm, nullptr, kRaw};
+  s.ld = ld;
+  s.ncols = B;
+  s.F = F;
+  s.f_row = B;
+  s.f_m = (int64_t)p->n_theta * B;
+  s.col_f = B;
+  s.col_c = 1;
+  MT_TRY((launch_synth_f64<SynScalar, 16>(s, st)));
+  ToGridArgs g{};
+  g.t = p->tab;
+  g.F = F;
+  g.f_m = s.f_m;
+  g.f_row = s.f_row;
+  g.ncols = B;
+  g.B = B;
+  g.out[0] = grid;
+  return launch_fourier_to_grid(g, st);
+}
+
+int mt_scal_to_grad_spat(const mt_plan* p, const double* Slm, int64_t ld, int B, int scale_dlh,
+                         double* gt, double* gp, void* work, size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(Slm && gt && gp && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
+  MT_TRY(check_ws(p, B, 2, work_bytes, work));
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* F = (double2*)work;
+  SynthArgs<1> s{};
+  s.t = p->tab;
+  s.src[0] = {(const double2*)Slm, nullptr, scale_dlh ? kDlh : kRaw};
+  s.ld = ld;
+  s.ncols = B;
+  s.F = F;
+  s.f_row = 2 * (int64_t)B;
+  s.f_m = (int64_t)p->n_theta * s.f_row;
+  s.col_f = B;
+  s.col_c = 1;
+  MT_TRY((launch_synth_f64<SynGrad, 16>(s, st)));
+  ToGridArgs g{};
+  g.t = p->tab;
+  g.F = F;
+  g.f_m = s.f_m;
+  g.f_row = s.f_row;
+  g.ncols = 2 * B;
+  g.B = B;
+  g.out[0] = gt;
+  g.out[1] = gp;
+  return launch_fourier_to_grid(g, st);
+}
+
+int mt_torpol_to_spat(const mt_plan* p, const double* Q, const double* S, const double* T,
+                      int64_t ld, int B, double* br, double* bt, double* bp, void* work,
+                      size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(Q && S && T && br && bt && bp && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
+  MT_TRY(check_ws(p, B, 3, work_bytes, work));
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* F = (double2*)work;
+  SynthArgs<3> s{};
+  s.t = p->tab;
+  s.src[0] = {(const double2*)Q, nullptr, kRaw};
+  s.src[1] = {(const double2*)S, nullptr, kRaw};
+  s.src[2] = {(const double2*)T, nullptr, kRaw};
+  s.ld = ld;
+  s.ncols = B;
+  s.F = F;
+  s.f_row = 3 * (int64_t)B;
+  s.f_m = (int64_t)p->n_theta * s.f_row;
+  s.col_f = B;
+  s.col_c = 1;
+  MT_TRY((launch_synth_f64<SynTorpol, 8>(s, st)));
+  ToGridArgs g{};
+  g.t = p->tab;
+  g.F = F;
+  g.f_m = s.f_m;
+  g.f_row = s.f_row;
+  g.ncols = 3 * B;
+  g.B = B;
+  g.out[0] = br;
+  g.out[1] = bt;
+  g.out[2] = bp;
+  return launch_fourier_to_grid(g, st);
+}
+
+int mt_scal_to_SH(const mt_plan* p, const double* grid, int B, double* Slm, int64_t ld,
+                  void* work, size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(Slm && grid && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
+  MT_TRY(check_ws(p, B, 1, work_bytes, work));
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* F = (double2*)work;
+  ToFourierArgs f{};
+  f.t = p->tab;
+  f.in[0] = grid;
+  f.ncols = B;
+  f.B = B;
+  f.vector = 0;
+  f.F = F;
+  f.f_row = B;
+  f.f_m = (int64_t)p->n_theta * B;
+  MT_TRY(launch_grid_to_fourier(f, st));
+  AnalArgs<1, 1> a{};
+  a.t = p->tab;
+  a.F = F;
+  a.f_m = f.f_m;
+  a.f_row = f.f_row;
+  a.col_x = B;
+  a.col_c = 1;
+  a.ncols = B;
+  a.out[0] = (double2*)Slm;
+  a.ld = ld;
+  a.out_col0 = 0;
+  return launch_anal_f64<AnaScalar, 8>(a, st);
+}
+
+int mt_spat_to_sphertor(const mt_plan* p, const double* vt, const double* vp, int B, double* S,
+                        double* T, int64_t ld, void* work, size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(vt && vp && S && T && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
+  MT_TRY(check_ws(p, B, 2, work_bytes, work));
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* F = (double2*)work;
+  ToFourierArgs f{};
+  f.t = p->tab;
+  f.in[0] = vt;
+  f.in[1] = vp;
+  f.ncols = 2 * B;
+  f.B = B;
+  f.vector = 1;
+  f.F = F;
+  f.f_row = 2 * (int64_t)B;
+  f.f_m = (int64_t)p->n_theta * f.f_row;
+  MT_TRY(launch_grid_to_fourier(f, st));
+  AnalArgs<2, 2> a{};
+  a.t = p->tab;
+  a.F = F;
+  a.f_m = f.f_m;
+  a.f_row = f.f_row;
+  a.col_x = B;
+  a.col_c = 1;
+  a.ncols = B;
+  a.out[0] = (double2*)S;
+  a.out[1] = (double2*)T;
+  a.ld = ld;
+  a.out_col0 = 0;
+  return launch_anal_f64<AnaSphtor, 8>(a, st);
+}
+
+int mt_get_nl(const mt_plan* p, int n_r, const double* const* in, double* const* out,
+              const double* or2, const double* or4, double LFfac, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(in && out && or2 && or4 && n_r >= 1, MT_ERR_ARG, "bad argument");
+  GridNlArgs a{};
+  a.n_r = n_r;
+  a.nt = p->n_theta;
+  a.np = p->n_phi;
+  for (int i = 0; i < 14; ++i) {
+    MT_REQUIRE(in[i], MT_ERR_ARG, "null input grid");
+    a.in[i] = in[i];
+  }
+  for (int i = 0; i < 12; ++i) {
+    MT_REQUIRE(out[i], MT_ERR_ARG, "null output grid");
+    a.out[i] = out[i];
+  }
+  a.or2 = or2;
+  a.or4 = or4;
+  a.ost2 = p->d_ost2;
+  a.cosn = p->d_cosn;
+  a.LFfac = LFfac;
+  a.l_mag = 1;
+  return launch_get_nl_grid(false, a, (cudaStream_t)stream);
+}
+
+int mt_get_nl_anel(const mt_plan* p, int n_r, const double* const* in, double* const* out,
+                   const mt_anel_params* q, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(in && out && q && n_r >= 1, MT_ERR_ARG, "bad argument");
+  MT_REQUIRE(q->r && q->or1 && q->or2 && q->or4 && q->beta && q->orho1 && q->otemp1 && q->visc &&
+                 q->lambda_,
+             MT_ERR_ARG, "null radial profile");
+  GridNlArgs a{};
+  a.n_r = n_r;
+  a.nt = p->n_theta;
+  a.np = p->n_phi;
+  for (int i = 0; i < 19; ++i) {
+    MT_REQUIRE(in[i], MT_ERR_ARG, "null input grid");
+    a.in[i] = in[i];
+  }
+  for (int i = 0; i < 13; ++i) {
+    MT_REQUIRE(out[i], MT_ERR_ARG, "null output grid");
+    a.out[i] = out[i];
+  }
+  a.r = q->r;
+  a.or1 = q->or1;
+  a.or2 = q->or2;
+  a.or4 = q->or4;
+  a.beta = q->beta;
+  a.orho1 = q->orho1;
+  a.otemp1 = q->otemp1;
+  a.visc = q->visc;
+  a.lambda_ = q->lambda_;
+  a.ost2 = p->d_ost2;
+  a.cosn = p->d_cosn;
+  a.LFfac = q->LFfac;
+  a.ViscHeatFac = q->ViscHeatFac;
+  a.OhmLossFac = q->OhmLossFac;
+  a.l_mag = q->l_mag;
+  return launch_get_nl_grid(true, a, (cudaStream_t)stream);
+}
+
+size_t mt_courant_workspace(const mt_plan* p, int n_r) {
+  (void)p;
+  return n_r > 0 ? (size_t)2 * n_r * sizeof(unsigned long long) : 0;
+}
+
+int mt_courant(const mt_plan* p, int n_r, const double* vr, const double* vt, const double* vp,
+               const double* br, const double* bt, const double* bp, const mt_courant_params* q,
+               double* dtrkc, double* dthkc, void* work, size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(q && vr && vt && vp && dtrkc && dthkc && n_r >= 1, MT_ERR_ARG, "bad argument");
+  MT_REQUIRE(q->mode >= 0 && q->mode <= 2, MT_ERR_ARG, "mode must be 0, 1 or 2");
+  MT_REQUIRE(q->mode == 0 || (br && bt && bp), MT_ERR_ARG, "magnetic grids required");
+  MT_REQUIRE(q->or2 && q->or4 && q->orho1 && q->orho2 && q->delxr2 && q->delxh2, MT_ERR_ARG,
+             "null radial profile");
+  MT_REQUIRE(work && work_bytes >= mt_courant_workspace(p, n_r), MT_ERR_WORKSPACE,
+             "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* mx = (unsigned long long*)work;
+  MT_CHECK_CUDA(cudaMemsetAsync(mx, 0, 2 * n_r * sizeof(unsigned long long), st));
+  CourantGridArgs a{};
+  a.n_r = n_r;
+  a.nt = p->n_theta;
+  a.np = p->n_phi;
+  a.mode = q->mode;
+  a.vr = vr;
+  a.vt = vt;
+  a.vp = vp;
+  a.br = br;
+  a.bt = bt;
+  a.bp = bp;
+  a.or2 = q->or2;
+  a.or4 = q->or4;
+  a.orho1 = q->orho1;
+  a.orho2 = q->orho2;
+  a.delxr2 = q->delxr2;
+  a.delxh2 = q->delxh2;
+  a.ost2 = p->d_ost2;
+  a.LFfac = q->LFfac;
+  a.cf2 = q->courfac * q->courfac;
+  a.af2 = q->alffac * q->alffac;
+  double h = 0.5 * (1.0 + q->opm);
+  a.valfac = h * h;
+  a.vr2max = mx;
+  a.vh2max = mx + n_r;
+  MT_TRY(launch_courant_grid(a, st));
+  return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
+}
+
+}  // extern "C"
+
+namespace mt {
+
+static int bouss_nfi(int mag, int chem) { return (mag ? 6 : 0) + 7 + (chem ? 1 : 0); }
+static int bouss_nfo(int mag, int chem) { return 6 + (mag ? 3 : 0) + (chem ? 3 : 0); }
+
+template <bool MAG, bool CHEM>
+static int nl_bouss_t(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt_bouss_out* out,
+                      const mt_bouss_params* q, double* dtrkc, double* dthkc, void* work,
+                      cudaStream_t st) {
+  const int nfi = bouss_nfi(MAG, CHEM), nfo = bouss_nfo(MAG, CHEM);
+  char* w = (char*)work;
+  double2* F = (double2*)w;
+  w += fourier_bytes(p, (int64_t)n_r * nfi);
+  double2* G = (double2*)w;
+  w += fourier_bytes(p, (int64_t)(n_r - 2) * nfo);
+  unsigned long long* mx = (unsigned long long*)w;
+  const int parts = q->parts ? q->parts : 7;
+  auto c = [](const double* x) { return (const double2*)x; };
+  const int64_t f_row = (int64_t)n_r * nfi, f_m = (int64_t)p->n_theta * f_row;
+
+  // Legendre synthesis of the 14 grid fields, two launches
+  // (magic_torch/step_time.py:980-1013 input assembly on load)
+  if ((parts & 1) && MAG) {
+    SynthArgs<6> s{};
+    s.t = p->tab;
+    s.src[0] = {c(in->b), nullptr, kDlh};
+    s.src[1] = {c(in->db), nullptr, kRaw};
+    s.src[2] = {c(in->aj), nullptr, kRaw};
+    s.src[3] = {c(in->aj), nullptr, kDlh};
+    s.src[4] = {c(in->dj), nullptr, kRaw};
+    s.src[5] = {c(in->b), c(in->ddb), kCurlT};
+    s.ld = in->ld;
+    s.ncols = n_r;
+    s.or2 = q->or2;
+    s.F = F;
+    s.f_row = f_row;
+    s.f_m = f_m;
+    s.col_f = 1;
+    s.col_c = nfi;
+    MT_TRY((launch_synth_f64<SynGroups<2, 0>, 8>(s, st)));
+  }
+  if (parts & 1) {
+    using SO = SynGroups<2, CHEM ? 2 : 1>;
+    SynthArgs<SO::NX> s{};
+    s.t = p->tab;
+    s.src[0] = {c(in->w), nullptr, kDlh};
+    s.src[1] = {c(in->dw), nullptr, kRaw};
+    s.src[2] = {c(in->z), nullptr, kRaw};
+    s.src[3] = {c(in->z), nullptr, kDlh};
+    s.src[4] = {c(in->dz), nullptr, kRaw};
+    s.src[5] = {c(in->w), c(in->ddw), kCurlT};
+    s.src[6] = {c(in->s), nullptr, kRaw};
+    if (CHEM) s.src[SO::NX - 1] = {c(in->xi), nullptr, kRaw};
+    s.ld = in->ld;
+    s.ncols = n_r;
+    s.or2 = q->or2;
+    s.F = F + (MAG ? 6 : 0);
+    s.f_row = f_row;
+    s.f_m = f_m;
+    s.col_f = 1;
+    s.col_c = nfi;
+    MT_TRY((launch_synth_f64<SO, 8>(s, st)));
+  }
+
+  NlBoussArgs nl{};
+  nl.t = p->tab;
+  nl.n_r = n_r;
+  nl.F = F;
+  nl.f_m = f_m;
+  nl.f_row = f_row;
+  nl.G = G;
+  nl.g_row = (int64_t)(n_r - 2) * nfo;
+  nl.g_m = (int64_t)p->n_theta * nl.g_row;
+  nl.or2 = q->or2;
+  nl.or4 = q->or4;
+  nl.orho1 = q->orho1;
+  nl.orho2 = q->orho2;
+  nl.delxr2 = q->delxr2;
+  nl.delxh2 = q->delxh2;
+  nl.LFfac = q->LFfac;
+  nl.cour_mode = MAG ? q->cour_mode : 0;
+  nl.cf2 = q->courfac * q->courfac;
+  nl.af2 = q->alffac * q->alffac;
+  double h = 0.5 * (1.0 + q->opm);
+  nl.valfac = h * h;
+  nl.vr2max = mx;
+  nl.vh2max = mx + n_r;
+  if (parts & 2) {
+    MT_CHECK_CUDA(cudaMemsetAsync(mx, 0, 2 * n_r * sizeof(unsigned long long), st));
+    MT_TRY(launch_nl_bouss(MAG, CHEM, nl, st));
+  }
+  if (!(parts & 4)) return MT_OK;
+
+  // Legendre analysis of the products, two launches
+  // (magic_torch/step_time.py:1066-1124)
+  auto anal_args = [&](auto& a, int field0) {
+    a.t = p->tab;
+    a.F = G + field0;
+    a.f_m = nl.g_m;
+    a.f_row = nl.g_row;
+    a.col_x = 1;
+    a.col_c = nfo;
+    a.ncols = n_r - 2;
+    a.ld = out->ld;
+    a.out_col0 = 1;
+  };
+  {
+    AnalArgs<6, 5> a{};
+    anal_args(a, 0);
+    a.out[0] = (double2*)out->Advr;
+    a.out[1] = (double2*)out->Advt;
+    a.out[2] = (double2*)out->Advp;
+    a.out[3] = (double2*)out->VSr;
+    a.out[4] = (double2*)out->VSt;
+    MT_TRY((launch_anal_f64<AnaGroups<1, 2>, 8>(a, st)));
+  }
+  if (MAG && CHEM) {
+    AnalArgs<6, 5> a{};
+    anal_args(a, 6);
+    a.out[0] = (double2*)out->VxBr;
+    a.out[1] = (double2*)out->VxBt;
+    a.out[2] = (double2*)out->VxBp;
+    a.out[3] = (double2*)out->VXir;
+    a.out[4] = (double2*)out->VXit;
+    MT_TRY((launch_anal_f64<AnaGroups<1, 2>, 8>(a, st)));
+  } else if (MAG) {
+    AnalArgs<3, 3> a{};
+    anal_args(a, 6);
+    a.out[0] = (double2*)out->VxBr;
+    a.out[1] = (double2*)out->VxBt;
+    a.out[2] = (double2*)out->VxBp;
+    MT_TRY((launch_anal_f64<AnaGroups<1, 0>, 8>(a, st)));
+  } else if (CHEM) {
+    AnalArgs<3, 2> a{};
+    anal_args(a, 6);
+    a.out[0] = (double2*)out->VXir;
+    a.out[1] = (double2*)out->VXit;
+    MT_TRY((launch_anal_f64<AnaGroups<2, 0>, 8>(a, st)));
+  }
+  return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
+}
+
+}  // namespace mt
+
+extern "C" {
+
+size_t mt_nl_bouss_workspace(const mt_plan* p, int n_r, int l_mag, int l_chem) {
+  if (!p || n_r < 3) return 0;
+  size_t f = fourier_bytes(p, (int64_t)n_r * bouss_nfi(l_mag, l_chem));
+  size_t g = fourier_bytes(p, (int64_t)(n_r - 2) * bouss_nfo(l_mag, l_chem));
+  return f + g + 2 * (size_t)n_r * sizeof(unsigned long long) + 256;
+}
+
+int mt_nl_bouss(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt_bouss_out* out,
+                const mt_bouss_params* q, double* dtrkc, double* dthkc, void* work,
+                size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(in && out && q && dtrkc && dthkc && n_r >= 3, MT_ERR_ARG, "bad argument");
+  MT_REQUIRE(in->w && in->dw && in->ddw && in->z && in->dz && in->s, MT_ERR_ARG,
+             "null velocity/entropy input");
+  MT_REQUIRE(!q->l_mag || (in->b && in->db && in->ddb && in->aj && in->dj), MT_ERR_ARG,
+             "null magnetic input");
+  MT_REQUIRE(!q->l_chem || in->xi, MT_ERR_ARG, "null composition input");
+  MT_REQUIRE(in->ld >= n_r && out->ld >= n_r, MT_ERR_ARG, "ld >= n_r required");
+  MT_REQUIRE(out->Advr && out->Advt && out->Advp && out->VSr && out->VSt, MT_ERR_ARG,
+             "null output");
+  MT_REQUIRE(q->or2 && q->or4 && q->orho1 && q->orho2 && q->delxr2 && q->delxh2, MT_ERR_ARG,
+             "null radial profile");
+  MT_REQUIRE(q->cour_mode >= 0 && q->cour_mode <= 2, MT_ERR_ARG, "bad cour_mode");
+  MT_REQUIRE(q->parts >= 0 && q->parts <= 7, MT_ERR_ARG, "parts must be a mask of 1, 2, 4");
+  MT_REQUIRE(work && work_bytes >= mt_nl_bouss_workspace(p, n_r, q->l_mag, q->l_chem),
+             MT_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (q->l_mag)
+    return q->l_chem ? nl_bouss_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                     : nl_bouss_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+  return q->l_chem ? nl_bouss_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                   : nl_bouss_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,378 @@
+// Grid-space nonlinear terms.
+//
+// * k_nl_bouss: the fused phi stage of the Boussinesq radial loop.  One CTA
+//   per (interleaved theta row, radial level): the 14 Fourier rows written by
+//   the Legendre synthesis are expanded and inverse-FFT'd in shared memory
+//   (two real fields per complex FFT), the get_nl products
+//   (magic_torch/get_nl.py:57-87) and the Courant maxima
+//   (magic_torch/courant.py:25-77) are formed point by point, and the 12
+//   products are forward-FFT'd and truncated to n_m modes for the Legendre
+//   analysis.  Grids never reach HBM.
+// * k_get_nl / k_get_nl_anel / k_courant_grid: the same formulas on grids
+//   held in HBM, for the drop-in get_nl / get_nl_anel / courant_check.
+#include <algorithm>
+
+#include "fft.cuh"
+#include "fourier.cuh"
+
+namespace mt {
+
+// ------------------------------------------------------------ point formulas
+
+struct BoussIn {
+  double vr, vt, vp, cvr, cvt, cvp, s, br, bt, bp, cbr, cbt, cbp, xi;
+};
+struct BoussOut {
+  double o[12];  // Advr Advt Advp VSr VSt VSp VxBr VxBt VxBp VXir VXit VXip
+};
+
+// magic_torch/get_nl.py:57-85
+__device__ __forceinline__ void bouss_point(const BoussIn& f, double or2, double or4, double ost2,
+                                            double LFfac, bool mag, BoussOut& r) {
+  double LFr = 0.0, LFt = 0.0, LFp = 0.0;
+  if (mag) {
+    LFr = LFfac * ost2 * (f.cbt * f.bp - f.cbp * f.bt);
+    LFt = LFfac * or4 * (f.cbp * f.br - f.cbr * f.bp);
+    LFp = LFfac * or4 * (f.cbr * f.bt - f.cbt * f.br);
+  }
+  r.o[0] = -ost2 * (f.cvt * f.vp - f.cvp * f.vt) + LFr;
+  r.o[1] = -or4 * (f.cvp * f.vr - f.cvr * f.vp) + LFt;
+  r.o[2] = -or4 * (f.cvr * f.vt - f.cvt * f.vr) + LFp;
+  r.o[3] = f.vr * f.s;
+  r.o[4] = or2 * f.vt * f.s;
+  r.o[5] = or2 * f.vp * f.s;
+  r.o[6] = ost2 * (f.vt * f.bp - f.vp * f.bt);
+  r.o[7] = or4 * (f.vp * f.br - f.vr * f.bp);
+  r.o[8] = or4 * (f.vr * f.bt - f.vt * f.br);
+  r.o[9] = f.vr * f.xi;
+  r.o[10] = or2 * f.vt * f.xi;
+  r.o[11] = or2 * f.vp * f.xi;
+}
+
+// magic_torch/courant.py:25-77; mode 0 non-magnetic, 1 damped, 2 undamped.
+__device__ __forceinline__ void courant_point(int mode, double vr, double vt, double vp, double br,
+                                              double bt, double bp, double or2, double or4,
+                                              double orho1, double orho2, double ost2,
+                                              double LFfac, double cf2, double af2, double valri2,
+                                              double valhi2, double& vr2, double& vh2) {
+  double vflr2 = orho2 * vr * vr;
+  double vflh2 = (vt * vt + vp * vp) * ost2 * orho2;
+  if (mode == 0) {
+    vr2 = cf2 * or4 * vflr2;
+    vh2 = cf2 * or2 * vflh2;
+    return;
+  }
+  double valr = br * br * LFfac * orho1;
+  double valh2 = (bt * bt + bp * bp) * LFfac * ost2 * orho1;
+  double valr2 = valr, valh2m = valh2;
+  if (mode == 1) {
+    valr2 = valr * valr / (valr + valri2);
+    valh2m = valh2 * valh2 / (valh2 + valhi2);
+  }
+  vr2 = or4 * (cf2 * vflr2 + af2 * valr2);
+  vh2 = or2 * (cf2 * vflh2 + af2 * valh2m);
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < nw ? red[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  return v;  // valid in thread 0
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  v = v + 0.0;  // -0 -> +0: bit patterns of non-negative doubles order like integers
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// ------------------------------------------------------- fused Boussinesq
+
+template <bool MAG, bool CHEM>
+struct BoussFields {
+  static constexpr int NFI = (MAG ? 6 : 0) + 7 + (CHEM ? 1 : 0);
+  static constexpr int NFO = 6 + (MAG ? 3 : 0) + (CHEM ? 3 : 0);
+  static constexpr int RI = (NFI + 1) / 2, RO = (NFO + 1) / 2;
+  static constexpr int RB = RI > RO ? RI : RO;  // complex rows of the shared buffer
+  static constexpr int IV = MAG ? 6 : 0;  // index of vr
+};
+
+constexpr int kNlThreads = 512;
+constexpr int kNlCap = 10;  // complex values per thread and FFT stage (4 rows, n_phi <= 1280)
+
+template <typename T>
+__device__ __forceinline__ double fld(const cplx<T>* buf, int N, int f, int n) {
+  cplx<T> z = buf[(f >> 1) * N + n];
+  return (f & 1) ? z.y : z.x;
+}
+
+template <bool MAG, bool CHEM>
+__global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
+  using BF = BoussFields<MAG, CHEM>;
+  extern __shared__ double smem[];
+  __shared__ double red[32];
+  cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);
+  const Tables& t = a.t;
+  const int N = t.n_phi, M = t.n_m;
+  const int row = blockIdx.x, r = blockIdx.y;
+  for (int i = threadIdx.x; i < BF::RI * N; i += blockDim.x) buf[i] = {0.0, 0.0};
+  __syncthreads();
+  // expand the half spectra of the NFI fields into RI complex rows
+  const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * BF::NFI;
+  for (int e = threadIdx.x; e < M * BF::RI; e += blockDim.x) {
+    int k = e / BF::RI, q = e % BF::RI;
+    double2 A = __ldg(&Fr[k * a.f_m + 2 * q]);
+    double2 B = make_double2(0.0, 0.0);
+    if (2 * q + 1 < BF::NFI) B = __ldg(&Fr[k * a.f_m + 2 * q + 1]);
+    cplx<double>* z = buf + q * N;
+    if (k == 0) {
+      z[0] = {A.x, B.x};
+    } else {
+      z[k] = {A.x - B.y, A.y + B.x};
+      z[N - k] = {A.x + B.y, B.x - A.y};
+    }
+  }
+  __syncthreads();
+  for (int q0 = 0; q0 < BF::RI; q0 += 4)
+    fft_rows<true, kNlCap>(buf + q0 * N, min(4, BF::RI - q0), N, N, t.fft_radix, t.fft_nstages,
+                           t.twiddle);
+
+  const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
+  const double orho1 = a.orho1[r], orho2 = a.orho2[r];
+  const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
+  double mr = 0.0, mh = 0.0;
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    BoussIn f;
+    constexpr int iv = BF::IV;
+    if constexpr (MAG) {
+      f.br = fld(buf, N, 0, n); f.bt = fld(buf, N, 1, n); f.bp = fld(buf, N, 2, n);
+      f.cbr = fld(buf, N, 3, n); f.cbt = fld(buf, N, 4, n); f.cbp = fld(buf, N, 5, n);
+    } else {
+      f.br = f.bt = f.bp = f.cbr = f.cbt = f.cbp = 0.0;
+    }
+    f.vr = fld(buf, N, iv + 0, n); f.vt = fld(buf, N, iv + 1, n); f.vp = fld(buf, N, iv + 2, n);
+    f.cvr = fld(buf, N, iv + 3, n); f.cvt = fld(buf, N, iv + 4, n); f.cvp = fld(buf, N, iv + 5, n);
+    f.s = fld(buf, N, iv + 6, n);
+    f.xi = 0.0;
+    if constexpr (CHEM) f.xi = fld(buf, N, iv + 7, n);
+    double vr2, vh2;
+    courant_point(a.cour_mode, f.vr, f.vt, f.vp, f.br, f.bt, f.bp, or2, or4, orho1, orho2, ost2,
+                  a.LFfac, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+    mr = fmax(mr, vr2);
+    mh = fmax(mh, vh2);
+    BoussOut o;
+    bouss_point(f, or2, or4, ost2, a.LFfac, MAG, o);
+    // output field order: Advr..VSp, [VxBr..VxBp], [VXir..VXip]
+    double out[BF::NFO];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) out[i] = o.o[i];
+    if constexpr (MAG) { out[6] = o.o[6]; out[7] = o.o[7]; out[8] = o.o[8]; }
+    if constexpr (CHEM) {
+      constexpr int c = MAG ? 9 : 6;
+      out[c] = o.o[9]; out[c + 1] = o.o[10]; out[c + 2] = o.o[11];
+    }
+    // point n is owned by this thread alone: overwrite its inputs in place
+#pragma unroll
+    for (int q = 0; q < BF::RO; ++q)
+      buf[q * N + n] = {out[2 * q], (2 * q + 1 < BF::NFO) ? out[2 * q + 1] : 0.0};
+  }
+  double vmr = block_max(mr, red);
+  if (threadIdx.x == 0) atomic_max_pos(&a.vr2max[r], vmr);
+  double vmh = block_max(mh, red);
+  if (threadIdx.x == 0) atomic_max_pos(&a.vh2max[r], vmh);
+  if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
+  __syncthreads();
+  for (int q0 = 0; q0 < BF::RO; q0 += 4)
+    fft_rows<false, kNlCap>(buf + q0 * N, min(4, BF::RO - q0), N, N, t.fft_radix, t.fft_nstages,
+                            t.twiddle);
+  const double ws = t.wq[row] / N, wv = t.wq_v[row] / N;
+  double2* Gr = a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * BF::NFO;
+  for (int e = threadIdx.x; e < M * BF::RO; e += blockDim.x) {
+    int k = e / BF::RO, q = e % BF::RO;
+    const cplx<double>* z = buf + q * N;
+    cplx<double> Z = z[k], Zc = z[(N - k) % N];
+    double ax = 0.5 * (Z.x + Zc.x), ay = 0.5 * (Z.y - Zc.y);
+    double bx = 0.5 * (Z.y + Zc.y), by = -0.5 * (Z.x - Zc.x);
+    int f0 = 2 * q, f1 = 2 * q + 1;
+    // scalar analyses (radial components): Advr, VSr, VxBr, VXir
+    auto wt = [&](int f) {
+      bool radial = (f == 0 || f == 3 || (MAG && f == 6) || (CHEM && f == (MAG ? 9 : 6)));
+      return radial ? ws : wv;
+    };
+    double w0 = wt(f0);
+    Gr[k * a.g_m + f0] = make_double2(w0 * ax, w0 * ay);
+    if (f1 < BF::NFO) {
+      double w1 = wt(f1);
+      Gr[k * a.g_m + f1] = make_double2(w1 * bx, w1 * by);
+    }
+  }
+}
+
+template <bool MAG, bool CHEM>
+static int launch_nl_bouss_t(const NlBoussArgs& a, cudaStream_t st) {
+  using BF = BoussFields<MAG, CHEM>;
+  size_t sm = (size_t)BF::RB * a.t.n_phi * 16;
+  auto kern = k_nl_bouss<MAG, CHEM>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(a.t.n_theta, a.n_r);
+  kern<<<grid, kNlThreads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int launch_nl_bouss(bool mag, bool chem, const NlBoussArgs& a, cudaStream_t st) {
+  if (mag) return chem ? launch_nl_bouss_t<true, true>(a, st) : launch_nl_bouss_t<true, false>(a, st);
+  return chem ? launch_nl_bouss_t<false, true>(a, st) : launch_nl_bouss_t<false, false>(a, st);
+}
+
+__global__ void k_courant_finish(int n_r, const unsigned long long* vr2, const unsigned long long* vh2,
+                                 const double* delxr2, const double* delxh2, double* dtr,
+                                 double* dth) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_r) return;
+  double a = __longlong_as_double((long long)vr2[r]);
+  double b = __longlong_as_double((long long)vh2[r]);
+  dtr[r] = a > 0.0 ? sqrt(delxr2[r] / a) : 1e10;  // magic_torch/courant.py:122-125
+  dth[r] = b > 0.0 ? sqrt(delxh2[r] / b) : 1e10;
+}
+
+int launch_courant_finish(int n_r, const unsigned long long* vr2, const unsigned long long* vh2,
+                          const double* delxr2, const double* delxh2, double* dtr, double* dth,
+                          cudaStream_t st) {
+  k_courant_finish<<<(n_r + 127) / 128, 128, 0, st>>>(n_r, vr2, vh2, delxr2, delxh2, dtr, dth);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+// ---------------------------------------------------- grid-space drop-ins
+
+
+__global__ void k_get_nl(GridNlArgs a) {
+  int64_t total = (int64_t)a.n_r * a.nt * a.np;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int r = (int)(i / ((int64_t)a.nt * a.np));
+    int th = (int)((i / a.np) % a.nt);
+    BoussIn f;
+    f.vr = a.in[0][i]; f.vt = a.in[1][i]; f.vp = a.in[2][i];
+    f.cvr = a.in[3][i]; f.cvt = a.in[4][i]; f.cvp = a.in[5][i];
+    f.s = a.in[6][i];
+    f.br = a.in[7][i]; f.bt = a.in[8][i]; f.bp = a.in[9][i];
+    f.cbr = a.in[10][i]; f.cbt = a.in[11][i]; f.cbp = a.in[12][i];
+    f.xi = a.in[13][i];
+    BoussOut o;
+    bouss_point(f, a.or2[r], a.or4[r], a.ost2[th], a.LFfac, true, o);
+#pragma unroll
+    for (int q = 0; q < 12; ++q) a.out[q][i] = o.o[q];
+  }
+}
+
+// magic_torch/get_nl_anel.py:63-134
+__global__ void k_get_nl_anel(GridNlArgs a) {
+  int64_t total = (int64_t)a.n_r * a.nt * a.np;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int r = (int)(i / ((int64_t)a.nt * a.np));
+    int th = (int)((i / a.np) % a.nt);
+    const double vr = a.in[0][i], vt = a.in[1][i], vp = a.in[2][i];
+    const double dvrdr = a.in[3][i], dvtdr = a.in[4][i], dvpdr = a.in[5][i];
+    const double dvrdt = a.in[6][i], dvrdp = a.in[7][i], dvtdp = a.in[8][i], dvpdp = a.in[9][i];
+    const double cvr = a.in[10][i], s = a.in[11][i], xi = a.in[12][i];
+    const double br = a.in[13][i], bt = a.in[14][i], bp = a.in[15][i];
+    const double cbr = a.in[16][i], cbt = a.in[17][i], cbp = a.in[18][i];
+    const double R = a.r[r], or1 = a.or1[r], or2 = a.or2[r], or4 = a.or4[r];
+    const double beta = a.beta[r], orho1 = a.orho1[r], otemp1 = a.otemp1[r];
+    const double visc = a.visc[r], lam = a.lambda_[r];
+    const double ost2 = a.ost2[th], cosn = a.cosn[th], LF = a.LFfac;
+    double LFr = LF * ost2 * (cbt * bp - cbp * bt);
+    double LFt = LF * or4 * (cbp * br - cbr * bp);
+    double LFp = LF * or4 * (cbr * bt - cbt * br);
+    double Advr = -or2 * orho1 * (vr * (dvrdr - (2.0 * or1 + beta) * vr) +
+                                  ost2 * (vt * (dvrdt - R * vt) + vp * (dvrdp - R * vp)));
+    double Advt = or4 * orho1 * (-vr * (dvtdr - beta * vt) + vt * (cosn * vt + dvpdp + dvrdr) +
+                                 vp * (cosn * vp - dvtdp));
+    double Advp = or4 * orho1 * (-vr * (dvpdr - beta * vp) - vt * (dvtdp + cvr) - vp * dvpdp);
+    a.out[0][i] = Advr + LFr;
+    a.out[1][i] = Advt + LFt;
+    a.out[2][i] = Advp + LFp;
+    a.out[3][i] = vr * s;
+    a.out[4][i] = or2 * vt * s;
+    a.out[5][i] = or2 * vp * s;
+    a.out[6][i] = orho1 * ost2 * (vt * bp - vp * bt);
+    a.out[7][i] = orho1 * or4 * (vp * br - vr * bp);
+    a.out[8][i] = orho1 * or4 * (vr * bt - vt * br);
+    a.out[9][i] = vr * xi;
+    a.out[10][i] = or2 * vt * xi;
+    a.out[11][i] = or2 * vp * xi;
+    double prefac = a.ViscHeatFac * or4 * orho1 * otemp1 * visc;
+    double beta_r = beta * R;
+    double e_rr = dvrdr - (2.0 * or1 + beta) * vr;
+    double e_tt = cosn * vt + dvpdp + dvrdr - or1 * vr;
+    double e_pp = dvpdp + cosn * vt + or1 * vr;
+    double e_tp = 2.0 * dvtdp + cvr - 2.0 * cosn * vp;
+    double e_rt = R * dvtdr - (2.0 + beta_r) * vt + or1 * dvrdt;
+    double e_rp = R * dvpdr - (2.0 + beta_r) * vp + or1 * dvrdp;
+    double bv = beta * vr;
+    double heat = prefac * (2.0 * e_rr * e_rr + 2.0 * e_tt * e_tt + 2.0 * e_pp * e_pp +
+                            e_tp * e_tp + ost2 * (e_rt * e_rt + e_rp * e_rp) -
+                            2.0 * (1.0 / 3.0) * bv * bv);
+    if (a.l_mag && a.OhmLossFac != 0.0)
+      heat += a.OhmLossFac * lam * or2 * otemp1 * (or2 * cbr * cbr + ost2 * (cbt * cbt + cbp * cbp));
+    a.out[12][i] = heat;
+  }
+}
+
+int launch_get_nl_grid(bool anel, const GridNlArgs& a, cudaStream_t st) {
+  int64_t total = (int64_t)a.n_r * a.nt * a.np;
+  int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  if (blocks < 1) blocks = 1;
+  if (anel) k_get_nl_anel<<<blocks, 256, 0, st>>>(a);
+  else k_get_nl<<<blocks, 256, 0, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+
+// one CTA per (level, slab of theta rows)
+__global__ void k_courant_grid(CourantGridArgs a) {
+  __shared__ double red[32];
+  const int r = blockIdx.y;
+  const int64_t per = (int64_t)a.nt * a.np;
+  const int64_t base = (int64_t)r * per;
+  const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
+  double mr = 0.0, mh = 0.0;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < per;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    int th = (int)(j / a.np);
+    int64_t i = base + j;
+    double br = 0.0, bt = 0.0, bp = 0.0;
+    if (a.mode != 0) { br = a.br[i]; bt = a.bt[i]; bp = a.bp[i]; }
+    double vr2, vh2;
+    courant_point(a.mode, a.vr[i], a.vt[i], a.vp[i], br, bt, bp, a.or2[r], a.or4[r], a.orho1[r],
+                  a.orho2[r], a.ost2[th], a.LFfac, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+    mr = fmax(mr, vr2);
+    mh = fmax(mh, vh2);
+  }
+  double v = block_max(mr, red);
+  if (threadIdx.x == 0) atomic_max_pos(&a.vr2max[r], v);
+  v = block_max(mh, red);
+  if (threadIdx.x == 0) atomic_max_pos(&a.vh2max[r], v);
+}
+
+int launch_courant_grid(const CourantGridArgs& a, cudaStream_t st) {
+  int64_t per = (int64_t)a.nt * a.np;
+  int bx = (int)std::min<int64_t>((per + 255) / 256, 32);
+  dim3 grid(bx, a.n_r);
+  k_courant_grid<<<grid, 256, 0, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+}  // namespace mt

@@ -1,0 +1,28 @@
+"""Boussinesq radial profiles for synthetic workloads.
+
+Chebyshev-Gauss-Lobatto radii between r_icb = radratio/(1-radratio) and
+r_cmb = 1/(1-radratio), outer boundary first (magic_torch/chebyshev.py), with
+or2 = 1/r^2, or4 = 1/r^4, orho1 = orho2 = 1 (Boussinesq,
+magic_torch/radial_functions.py:19-31) and the Courant spacings delxr2, delxh2
+(magic_torch/radial_functions.py:190-197).
+"""
+
+import math
+
+import torch
+
+
+def boussinesq_profiles(n_r, l_max, radratio=0.35, device="cuda"):
+    r_cmb = 1.0 / (1.0 - radratio)
+    r_icb = r_cmb - 1.0
+    k = torch.arange(n_r, dtype=torch.float64)
+    r = r_icb + (r_cmb - r_icb) * 0.5 * (1.0 + torch.cos(math.pi * k / (n_r - 1)))
+    dr = r[:-1] - r[1:]
+    delxr2 = torch.empty(n_r, dtype=torch.float64)
+    delxr2[0] = dr[0] ** 2
+    delxr2[-1] = dr[-1] ** 2
+    delxr2[1:-1] = torch.minimum(dr[:-1], dr[1:]) ** 2
+    prof = dict(r=r, or2=1.0 / r ** 2, or4=1.0 / r ** 4, orho1=torch.ones(n_r, dtype=torch.float64),
+                orho2=torch.ones(n_r, dtype=torch.float64), delxr2=delxr2,
+                delxh2=r ** 2 / float(l_max * (l_max + 1)))
+    return {k: v.to(device) for k, v in prof.items()}

@@ -1,0 +1,81 @@
+"""GPU parity of the fused nonlinear stage (synthesis -> phi FFT + get_nl + Courant ->
+analysis) against the oracle's restatement of the radial loop (FP64, 1e-12)."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from oracle import grid as og
+from oracle import stage as ostage
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # l_max, minc, n_r, l_mag, l_chem
+    (16, 1, 5, True, False),
+    (32, 4, 7, True, True),
+    (20, 1, 6, False, True),
+    (16, 1, 4, False, False),
+    (63, 1, 9, True, False),
+]
+
+
+def _fields(g, N, rng, l_mag, l_chem):
+    amp = (g.lm2l + 1.0) ** -1.5
+
+    def spec():
+        x = (rng.standard_normal((g.lm_max, N)) + 1j * rng.standard_normal((g.lm_max, N)))
+        x = x * amp[:, None]
+        x[g.lm2m == 0] = x[g.lm2m == 0].real
+        return x
+
+    names = ["w", "dw", "ddw", "z", "dz", "s"] + (["b", "db", "ddb", "aj", "dj"] if l_mag else [])
+    names += ["xi"] if l_chem else []
+    return {k: spec() for k in names}
+
+
+@pytest.mark.parametrize("l_max,minc,N,l_mag,l_chem", CASES)
+def test_nl_bouss_matches_oracle(l_max, minc, N, l_mag, l_chem):
+    from magic_b200 import Plan
+
+    g = og.Grid(l_max, minc)
+    p = Plan(l_max, minc)
+    rng = np.random.default_rng(7 * l_max + N)
+    f = _fields(g, N, rng, l_mag, l_chem)
+    prof = ostage.bouss_profiles(N, l_max=l_max)
+    LF, cf, af, opm = 200.0, 2.5, 1.0, 0.2
+    ref, rdt, rdh = ostage.nl_bouss_stage(g, f, prof, LF, cf, af, opm, l_mag, l_chem)
+    cu = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()
+    out, dt, dh = p.nl_bouss({k: cu(v) for k, v in f.items()}, {k: cu(v) for k, v in prof.items()},
+                             LF, cf, af, opm, l_mag=l_mag, l_chem=l_chem)
+    assert set(out) == set(ref)
+    # S and T of one vector field share its scale: T(Adv) cancels ~50x between
+    # its two contributions for random fields, so errors are measured against
+    # max(|S|, |T|) of the pair (both sides FP64, different summation order).
+    pair = {"Advt": "Advp", "Advp": "Advt", "VxBt": "VxBp", "VxBp": "VxBt"}
+    for k in ref:
+        got = out[k].cpu().numpy()
+        assert np.all(got[:, 0] == 0) and np.all(got[:, -1] == 0), k
+        scale = np.abs(ref[k]).max()
+        if k in pair:
+            scale = max(scale, np.abs(ref[pair[k]]).max())
+        assert np.abs(got - ref[k]).max() / scale < 1e-12, k
+    assert rel_err(dt.cpu().numpy(), rdt) < 1e-12
+    assert rel_err(dh.cpu().numpy(), rdh) < 1e-12
+
+
+def test_nl_bouss_argument_guards():
+    """Null or undersized arguments are refused on the host before any launch."""
+    import ctypes
+
+    from magic_b200 import Plan, _lib
+
+    p = Plan(16)
+    L = _lib.lib()
+    small = torch.empty(64, dtype=torch.uint8, device="cuda")
+    rc = L.mt_nl_bouss(p._h, 5, None, None, None, None, None,
+                       ctypes.c_void_p(small.data_ptr()), 64, None)
+    assert rc == 1 and b"bad argument" in L.mt_last_error()
+    assert p.nl_bouss_workspace(5, True, False) > 64
+    assert p.nl_bouss_workspace(2, True, False) == 0  # needs >= 3 levels
