@@ -214,6 +214,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--levels", type=int, default=N_R,
+                    help="radial levels (profiling runs use fewer than the 97 of the workload)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -237,11 +240,12 @@ def main():
     from magic_b200 import Plan
     from magic_b200.profiles import boussinesq_profiles
 
+    n_r = args.levels
     plan = Plan(L_MAX, 1, precision=args.precision, device=dev)
-    fields = synth_inputs(plan, N_R, dev, seed=rank)
-    prof = boussinesq_profiles(N_R, L_MAX, device=dev)
-    out = {k: torch.zeros(plan.lm_max, N_R, dtype=torch.complex128, device=dev) for k in OUTS}
-    work = torch.empty(plan.nl_bouss_workspace(N_R, True, False), dtype=torch.uint8, device=dev)
+    fields = synth_inputs(plan, n_r, dev, seed=rank)
+    prof = boussinesq_profiles(n_r, L_MAX, device=dev)
+    out = {k: torch.zeros(plan.lm_max, n_r, dtype=torch.complex128, device=dev) for k in OUTS}
+    work = torch.empty(plan.nl_bouss_workspace(n_r, True, False), dtype=torch.uint8, device=dev)
 
     def step(parts=0):
         return plan.nl_bouss(fields, prof, LF, CF, AF, OPM, l_mag=True, l_chem=False, out=out,
@@ -288,9 +292,13 @@ def main():
     part_ms = {parts[p]: sum(a.elapsed_time(b) for a, b in ev[p]) / len(ev[p]) for p in parts}
 
     # --- end to end through the public API with pinned host buffers
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"levels": n_r, "ms_per_step": ms, "kernel_ms": part_ms}), flush=True)
+        return
     host_in = {k: v.cpu().pin_memory() for k, v in fields.items()}
     host_out = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in out.items()}
-    host_dt = torch.empty(2, N_R, dtype=torch.float64).pin_memory()
+    host_dt = torch.empty(2, n_r, dtype=torch.float64).pin_memory()
     dev_in = {k: torch.empty_like(v) for k, v in fields.items()}
     h2d = sum(v.numel() * v.element_size() for v in host_in.values())
     d2h = sum(v.numel() * v.element_size() for v in host_out.values()) + host_dt.numel() * 8
@@ -325,14 +333,14 @@ def main():
 
     # --- roofline of the dominant kernel
     peaks, src = measured_peaks()
-    synth_f, anal_f = flops_per_step(plan.nhs, plan.lm_max, N_R)
+    synth_f, anal_f = flops_per_step(plan.nhs, plan.lm_max, n_r)
     dom = max(part_ms, key=part_ms.get)
     roof = None
     if dom == "phi_fft_products":
         # algorithmic bytes: Fourier rows in (13 fields x 97 levels) and out
         # (9 fields x 95 levels), each n_theta x n_m complex FP64
         row = plan.n_theta_max * plan.n_m_max * 16
-        byts = (13 * N_R + 9 * (N_R - 2)) * row
+        byts = (13 * n_r + 9 * (n_r - 2)) * row
         ach = byts / (part_ms[dom] * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": ach / peaks["hbm_gbs"], "traffic": None, "kernel": dom,

@@ -96,7 +96,8 @@ int mt_plan_create(const mt_grid_desc* desc, mt_plan** out) {
     return code;
   };
   if (p->n_theta < 2 || p->n_theta % 2) return fail(MT_ERR_UNSUPPORTED, "n_theta_max must be even");
-  if (p->n_phi > fft_max_nphi()) return fail(MT_ERR_UNSUPPORTED, "n_phi_max above 1280");
+  if (p->n_phi > fft_max_nphi())
+    return fail(MT_ERR_UNSUPPORTED, "n_phi_max above the shared-memory FFT limit (1170)");
   if (2 * (p->n_m - 1) >= p->n_phi)
     return fail(MT_ERR_UNSUPPORTED, "n_phi_max too small for l_max/minc (modes alias)");
   int rc = build_tables(p);

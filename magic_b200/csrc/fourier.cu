@@ -1,62 +1,66 @@
 // phi stage of the drop-in transforms: Fourier rows <-> grid rows.
 //
-// Two real rows a, b share one complex FFT of length n_phi (z = a + i b).
-// Inverse (synthesis, irfft norm="forward"): the half spectra A, B (modes
-// 0..n_m-1, zero above) are expanded to the full Hermitian spectrum of z,
-//   Z[k] = A[k] + i B[k],  Z[N-k] = conj(A[k]) + i conj(B[k]),  k >= 1,
-//   Z[0] = Re A[0] + i Re B[0]  (irfft ignores the imaginary part of mode 0),
-// then a = Re ifft(Z), b = Im ifft(Z), unnormalised.
-// Forward (analysis, rfft norm="forward"), for k < n_m:
-//   A[k] = (Z[k] + conj Z[N-k]) / 2,  B[k] = (Z[k] - conj Z[N-k]) / (2i),
-// scaled by 1/N and by the row's quadrature weight (2 pi w, or 2 pi w/sin^2
-// for vector components), so the Legendre analysis needs only P and dP.
+// Every grid row is one real field: synthesis is irfft(norm="forward")
+// (unnormalised, Im of mode 0 ignored), analysis rfft(norm="forward"), both
+// through a half-length complex FFT (fft.cuh).  Analysis outputs are scaled
+// by 1/N and by the row's quadrature weight (2 pi w, or 2 pi w/sin^2 for
+// vector components), so the Legendre analysis needs only P and dP.
 #include "fft.cuh"
 #include "fourier.cuh"
 
 namespace mt {
 
-constexpr int kRowsPerCta = 4;  // complex rows = 8 real columns
-constexpr int kFftThreads = 512;
-constexpr int kFftCap = 10;  // complex values per thread and stage: 4 rows x 1280 / 512
+constexpr int kColsPerCta = 8;  // real columns (grid rows) per CTA
+constexpr int kFftThreads = 256;
+
+// Expand the half spectra staged at row[0..M) (zero above) into Z (in place).
+template <typename R>
+__device__ __forceinline__ void c2r_prepare(cplx<R>* row, int H, const double2* __restrict__ tw,
+                                            int tid, int nthr) {
+  for (int k = tid; k <= H / 2; k += nthr) {
+    int kc = H - k;
+    cplx<R> Xk = row[pad16(k)];
+    if (k == 0) {
+      Xk.y = 0;  // irfft ignores Im X[0]; X[H] is zero (2 (n_m - 1) < N)
+      row[pad16(0)] = c2r_pre(Xk, cplx<R>{0, 0}, 0, tw);
+    } else {
+      cplx<R> Xc = row[pad16(kc)];
+      cplx<R> Zk = c2r_pre(Xk, Xc, k, tw);
+      cplx<R> Zc = c2r_pre(Xc, Xk, kc, tw);
+      row[pad16(k)] = Zk;
+      if (kc != k) row[pad16(kc)] = Zc;
+    }
+  }
+}
 
 __global__ void __launch_bounds__(kFftThreads) k_fourier_to_grid(ToGridArgs a) {
   extern __shared__ double smem[];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);
   const Tables& t = a.t;
-  const int N = t.n_phi, M = t.n_m, nt = t.n_theta;
+  const int N = t.n_phi, H = N / 2, M = t.n_m, nt = t.n_theta;
+  const int stride = padded_len(H);
   const int row = blockIdx.y;
-  const int col0 = blockIdx.x * 2 * kRowsPerCta;
-  for (int i = threadIdx.x; i < kRowsPerCta * N; i += blockDim.x) buf[i] = {0.0, 0.0};
+  const int col0 = blockIdx.x * kColsPerCta;
+  const int ncol = min(kColsPerCta, a.ncols - col0);
+  for (int i = threadIdx.x; i < ncol * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
-  const double2* Fr = a.F + (int64_t)row * a.f_row;
-  for (int e = threadIdx.x; e < M * kRowsPerCta; e += blockDim.x) {
-    int k = e / kRowsPerCta, q = e % kRowsPerCta;
-    int c = col0 + 2 * q;
-    double2 A = make_double2(0.0, 0.0), B = A;
-    if (c < a.ncols) A = Fr[k * a.f_m + c];
-    if (c + 1 < a.ncols) B = Fr[k * a.f_m + c + 1];
-    cplx<double>* z = buf + q * N;
-    if (k == 0) {
-      z[0] = {A.x, B.x};
-    } else {
-      z[k] = {A.x - B.y, A.y + B.x};
-      z[N - k] = {A.x + B.y, B.x - A.y};
-    }
+  const double2* Fr = a.F + (int64_t)row * a.f_row + col0;
+  for (int e = threadIdx.x; e < M * ncol; e += blockDim.x) {
+    int k = e / ncol, q = e - k * ncol;
+    double2 X = Fr[k * a.f_m + q];
+    buf[q * stride + pad16(k)] = {X.x, X.y};
   }
   __syncthreads();
-  fft_rows<true, kFftCap>(buf, kRowsPerCta, N, N, t.fft_radix, t.fft_nstages, t.twiddle);
-  for (int e = threadIdx.x; e < kRowsPerCta * N; e += blockDim.x) {
-    int q = e / N, n = e % N;
-    cplx<double> z = buf[e];
-    int c = col0 + 2 * q;
-    if (c < a.ncols) {
-      int f = c / a.B, b = c % a.B;
-      a.out[f][((int64_t)b * nt + row) * N + n] = z.x;
-    }
-    if (c + 1 < a.ncols) {
-      int f = (c + 1) / a.B, b = (c + 1) % a.B;
-      a.out[f][((int64_t)b * nt + row) * N + n] = z.y;
-    }
+  for (int q = threadIdx.x / 64; q < ncol; q += kFftThreads / 64)
+    c2r_prepare(buf + q * stride, H, t.twiddle, threadIdx.x % 64, 64);
+  __syncthreads();
+  fft_rows<true>(buf, buf + kColsPerCta * stride, ncol, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
+  for (int e = threadIdx.x; e < ncol * N; e += blockDim.x) {
+    int q = e / N, n = e - q * N;
+    cplx<double> z = buf[q * stride + pad16(n >> 1)];
+    int c = col0 + q;
+    int f = c / a.B, b = c % a.B;
+    a.out[f][((int64_t)b * nt + row) * N + n] = (n & 1) ? z.y : z.x;
   }
 }
 
@@ -64,42 +68,39 @@ __global__ void __launch_bounds__(kFftThreads) k_grid_to_fourier(ToFourierArgs a
   extern __shared__ double smem[];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);
   const Tables& t = a.t;
-  const int N = t.n_phi, M = t.n_m, nt = t.n_theta;
+  const int N = t.n_phi, H = N / 2, M = t.n_m, nt = t.n_theta;
+  const int stride = padded_len(H);
   const int row = blockIdx.y;
-  const int col0 = blockIdx.x * 2 * kRowsPerCta;
-  for (int e = threadIdx.x; e < kRowsPerCta * N; e += blockDim.x) {
-    int q = e / N, n = e % N;
-    int c = col0 + 2 * q;
-    double x = 0.0, y = 0.0;
-    if (c < a.ncols) x = a.in[c / a.B][((int64_t)(c % a.B) * nt + row) * N + n];
-    if (c + 1 < a.ncols) y = a.in[(c + 1) / a.B][((int64_t)((c + 1) % a.B) * nt + row) * N + n];
-    buf[e] = {x, y};
+  const int col0 = blockIdx.x * kColsPerCta;
+  const int ncol = min(kColsPerCta, a.ncols - col0);
+  for (int e = threadIdx.x; e < ncol * H; e += blockDim.x) {
+    int q = e / H, h = e - q * H;
+    int c = col0 + q;
+    const double* src = a.in[c / a.B] + ((int64_t)(c % a.B) * nt + row) * N;
+    double2 v = *reinterpret_cast<const double2*>(src + 2 * h);
+    buf[q * stride + pad16(h)] = {v.x, v.y};
   }
   __syncthreads();
-  fft_rows<false, kFftCap>(buf, kRowsPerCta, N, N, t.fft_radix, t.fft_nstages, t.twiddle);
+  fft_rows<false>(buf, buf + kColsPerCta * stride, ncol, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
   const double w = (a.vector ? t.wq_v[row] : t.wq[row]) / N;
-  double2* Fr = a.F + (int64_t)row * a.f_row;
-  for (int e = threadIdx.x; e < M * kRowsPerCta; e += blockDim.x) {
-    int k = e / kRowsPerCta, q = e % kRowsPerCta;
-    int c = col0 + 2 * q;
-    const cplx<double>* z = buf + q * N;
-    cplx<double> Z = z[k], Zc = z[(N - k) % N];
-    // A = (Z + conj Zc)/2 ; B = (Z - conj Zc)/(2i)
-    double ax = 0.5 * (Z.x + Zc.x), ay = 0.5 * (Z.y - Zc.y);
-    double dx = Z.x - Zc.x, dy = Z.y + Zc.y;
-    double bx = 0.5 * dy, by = -0.5 * dx;
-    if (c < a.ncols) Fr[k * a.f_m + c] = make_double2(w * ax, w * ay);
-    if (c + 1 < a.ncols) Fr[k * a.f_m + c + 1] = make_double2(w * bx, w * by);
+  double2* Fr = a.F + (int64_t)row * a.f_row + col0;
+  for (int e = threadIdx.x; e < M * ncol; e += blockDim.x) {
+    int k = e / ncol, q = e - k * ncol;
+    const cplx<double>* z = buf + q * stride;
+    cplx<double> X = r2c_post(z[pad16(k)], z[pad16((H - k) % H)], k, t.twiddle);
+    Fr[k * a.f_m + q] = make_double2(w * X.x, w * X.y);
   }
 }
 
-static size_t fft_smem(const Tables& t) { return (size_t)kRowsPerCta * t.n_phi * 16; }
+static size_t fft_smem(const Tables& t) {
+  return (size_t)(kColsPerCta + kFftRowBatch) * padded_len(t.n_phi / 2) * sizeof(double2);
+}
 
 int launch_fourier_to_grid(const ToGridArgs& a, cudaStream_t st) {
   size_t sm = fft_smem(a.t);
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_fourier_to_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-  dim3 grid((a.ncols + 2 * kRowsPerCta - 1) / (2 * kRowsPerCta), a.t.n_theta);
+  dim3 grid((a.ncols + kColsPerCta - 1) / kColsPerCta, a.t.n_theta);
   k_fourier_to_grid<<<grid, kFftThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
@@ -109,14 +110,14 @@ int launch_grid_to_fourier(const ToFourierArgs& a, cudaStream_t st) {
   size_t sm = fft_smem(a.t);
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_grid_to_fourier, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-  dim3 grid((a.ncols + 2 * kRowsPerCta - 1) / (2 * kRowsPerCta), a.t.n_theta);
+  dim3 grid((a.ncols + kColsPerCta - 1) / kColsPerCta, a.t.n_theta);
   k_grid_to_fourier<<<grid, kFftThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
 
-// Largest n_phi the fixed per-thread register budget supports (every radix:
-// ceil(CAP/R) * R * threads >= rows * n_phi).
-int fft_max_nphi() { return kFftCap * kFftThreads / kRowsPerCta; }
+// Largest n_phi the fused stage's shared memory holds: 14 field rows plus a
+// 7-row scratch of H = n_phi/2 padded complex FP64 values within 227 KB.
+int fft_max_nphi() { return 1200; }
 
 }  // namespace mt

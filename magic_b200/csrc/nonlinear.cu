@@ -99,89 +99,99 @@ template <bool MAG, bool CHEM>
 struct BoussFields {
   static constexpr int NFI = (MAG ? 6 : 0) + 7 + (CHEM ? 1 : 0);
   static constexpr int NFO = 6 + (MAG ? 3 : 0) + (CHEM ? 3 : 0);
-  static constexpr int RI = (NFI + 1) / 2, RO = (NFO + 1) / 2;
-  static constexpr int RB = RI > RO ? RI : RO;  // complex rows of the shared buffer
-  static constexpr int IV = MAG ? 6 : 0;  // index of vr
+  static constexpr int NB = NFI > NFO ? NFI : NFO;  // rows of the shared buffer
+  static constexpr int IV = MAG ? 6 : 0;            // row of vr
 };
 
 constexpr int kNlThreads = 512;
-constexpr int kNlCap = 10;  // complex values per thread and FFT stage (4 rows, n_phi <= 1280)
 
-template <typename T>
-__device__ __forceinline__ double fld(const cplx<T>* buf, int N, int f, int n) {
-  cplx<T> z = buf[(f >> 1) * N + n];
-  return (f & 1) ? z.y : z.x;
+template <typename R>
+__device__ __forceinline__ void c2r_prepare_nl(cplx<R>* row, int H, const double2* __restrict__ tw,
+                                               int tid, int nthr) {
+  for (int k = tid; k <= H / 2; k += nthr) {
+    int kc = H - k;
+    cplx<R> Xk = row[pad16(k)];
+    if (k == 0) {
+      Xk.y = 0;
+      row[pad16(0)] = c2r_pre(Xk, cplx<R>{0, 0}, 0, tw);
+    } else {
+      cplx<R> Xc = row[pad16(kc)];
+      cplx<R> Zk = c2r_pre(Xk, Xc, k, tw);
+      cplx<R> Zc = c2r_pre(Xc, Xk, kc, tw);
+      row[pad16(k)] = Zk;
+      if (kc != k) row[pad16(kc)] = Zc;
+    }
+  }
 }
 
 template <bool MAG, bool CHEM>
 __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   using BF = BoussFields<MAG, CHEM>;
+  constexpr int NFI = BF::NFI, NFO = BF::NFO;
   extern __shared__ double smem[];
   __shared__ double red[32];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);
   const Tables& t = a.t;
-  const int N = t.n_phi, M = t.n_m;
+  const int N = t.n_phi, H = N / 2, M = t.n_m;
+  const int stride = padded_len(H);
   const int row = blockIdx.x, r = blockIdx.y;
-  for (int i = threadIdx.x; i < BF::RI * N; i += blockDim.x) buf[i] = {0.0, 0.0};
+  for (int i = threadIdx.x; i < NFI * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
-  // expand the half spectra of the NFI fields into RI complex rows
-  const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * BF::NFI;
-  for (int e = threadIdx.x; e < M * BF::RI; e += blockDim.x) {
-    int k = e / BF::RI, q = e % BF::RI;
-    double2 A = __ldg(&Fr[k * a.f_m + 2 * q]);
-    double2 B = make_double2(0.0, 0.0);
-    if (2 * q + 1 < BF::NFI) B = __ldg(&Fr[k * a.f_m + 2 * q + 1]);
-    cplx<double>* z = buf + q * N;
-    if (k == 0) {
-      z[0] = {A.x, B.x};
-    } else {
-      z[k] = {A.x - B.y, A.y + B.x};
-      z[N - k] = {A.x + B.y, B.x - A.y};
-    }
+  // half spectra of the NFI fields (one real field per buffer row)
+  const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
+  for (int e = threadIdx.x; e < M * NFI; e += blockDim.x) {
+    int k = e / NFI, f = e - k * NFI;
+    double2 X = __ldg(&Fr[k * a.f_m + f]);
+    buf[f * stride + pad16(k)] = {X.x, X.y};
   }
   __syncthreads();
-  for (int q0 = 0; q0 < BF::RI; q0 += 4)
-    fft_rows<true, kNlCap>(buf + q0 * N, min(4, BF::RI - q0), N, N, t.fft_radix, t.fft_nstages,
-                           t.twiddle);
+  for (int f = threadIdx.x / 32; f < NFI; f += kNlThreads / 32)
+    c2r_prepare_nl(buf + f * stride, H, t.twiddle, threadIdx.x % 32, 32);
+  __syncthreads();
+  fft_rows<true>(buf, buf + BF::NB * stride, NFI, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
 
   const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
   const double orho1 = a.orho1[r], orho2 = a.orho2[r];
   const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
   double mr = 0.0, mh = 0.0;
-  for (int n = threadIdx.x; n < N; n += blockDim.x) {
-    BoussIn f;
-    constexpr int iv = BF::IV;
-    if constexpr (MAG) {
-      f.br = fld(buf, N, 0, n); f.bt = fld(buf, N, 1, n); f.bp = fld(buf, N, 2, n);
-      f.cbr = fld(buf, N, 3, n); f.cbt = fld(buf, N, 4, n); f.cbp = fld(buf, N, 5, n);
-    } else {
-      f.br = f.bt = f.bp = f.cbr = f.cbt = f.cbp = 0.0;
-    }
-    f.vr = fld(buf, N, iv + 0, n); f.vt = fld(buf, N, iv + 1, n); f.vp = fld(buf, N, iv + 2, n);
-    f.cvr = fld(buf, N, iv + 3, n); f.cvt = fld(buf, N, iv + 4, n); f.cvp = fld(buf, N, iv + 5, n);
-    f.s = fld(buf, N, iv + 6, n);
-    f.xi = 0.0;
-    if constexpr (CHEM) f.xi = fld(buf, N, iv + 7, n);
-    double vr2, vh2;
-    courant_point(a.cour_mode, f.vr, f.vt, f.vp, f.br, f.bt, f.bp, or2, or4, orho1, orho2, ost2,
-                  a.LFfac, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
-    mr = fmax(mr, vr2);
-    mh = fmax(mh, vh2);
-    BoussOut o;
-    bouss_point(f, or2, or4, ost2, a.LFfac, MAG, o);
-    // output field order: Advr..VSp, [VxBr..VxBp], [VXir..VXip]
-    double out[BF::NFO];
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    cplx<double> zin[NFI];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) out[i] = o.o[i];
-    if constexpr (MAG) { out[6] = o.o[6]; out[7] = o.o[7]; out[8] = o.o[8]; }
-    if constexpr (CHEM) {
-      constexpr int c = MAG ? 9 : 6;
-      out[c] = o.o[9]; out[c + 1] = o.o[10]; out[c + 2] = o.o[11];
-    }
-    // point n is owned by this thread alone: overwrite its inputs in place
+    for (int f = 0; f < NFI; ++f) zin[f] = buf[f * stride + pad16(i)];
+    double out[2][NFO];
 #pragma unroll
-    for (int q = 0; q < BF::RO; ++q)
-      buf[q * N + n] = {out[2 * q], (2 * q + 1 < BF::NFO) ? out[2 * q + 1] : 0.0};
+    for (int h = 0; h < 2; ++h) {  // grid points 2i and 2i+1
+      auto v = [&](int f) { return h ? zin[f].y : zin[f].x; };
+      BoussIn fi;
+      constexpr int iv = BF::IV;
+      if constexpr (MAG) {
+        fi.br = v(0); fi.bt = v(1); fi.bp = v(2); fi.cbr = v(3); fi.cbt = v(4); fi.cbp = v(5);
+      } else {
+        fi.br = fi.bt = fi.bp = fi.cbr = fi.cbt = fi.cbp = 0.0;
+      }
+      fi.vr = v(iv); fi.vt = v(iv + 1); fi.vp = v(iv + 2);
+      fi.cvr = v(iv + 3); fi.cvt = v(iv + 4); fi.cvp = v(iv + 5);
+      fi.s = v(iv + 6);
+      fi.xi = 0.0;
+      if constexpr (CHEM) fi.xi = v(iv + 7);
+      double vr2, vh2;
+      courant_point(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, or2, or4, orho1, orho2,
+                    ost2, a.LFfac, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+      mr = fmax(mr, vr2);
+      mh = fmax(mh, vh2);
+      BoussOut o;
+      bouss_point(fi, or2, or4, ost2, a.LFfac, MAG, o);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) out[h][q] = o.o[q];
+      if constexpr (MAG) { out[h][6] = o.o[6]; out[h][7] = o.o[7]; out[h][8] = o.o[8]; }
+      if constexpr (CHEM) {
+        constexpr int c = MAG ? 9 : 6;
+        out[h][c] = o.o[9]; out[h][c + 1] = o.o[10]; out[h][c + 2] = o.o[11];
+      }
+    }
+    // complex element i (points 2i, 2i+1) belongs to this thread alone
+#pragma unroll
+    for (int q = 0; q < NFO; ++q) buf[q * stride + pad16(i)] = {out[0][q], out[1][q]};
   }
   double vmr = block_max(mr, red);
   if (threadIdx.x == 0) atomic_max_pos(&a.vr2max[r], vmr);
@@ -189,36 +199,24 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   if (threadIdx.x == 0) atomic_max_pos(&a.vh2max[r], vmh);
   if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
   __syncthreads();
-  for (int q0 = 0; q0 < BF::RO; q0 += 4)
-    fft_rows<false, kNlCap>(buf + q0 * N, min(4, BF::RO - q0), N, N, t.fft_radix, t.fft_nstages,
-                            t.twiddle);
+  fft_rows<false>(buf, buf + BF::NB * stride, NFO, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
   const double ws = t.wq[row] / N, wv = t.wq_v[row] / N;
-  double2* Gr = a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * BF::NFO;
-  for (int e = threadIdx.x; e < M * BF::RO; e += blockDim.x) {
-    int k = e / BF::RO, q = e % BF::RO;
-    const cplx<double>* z = buf + q * N;
-    cplx<double> Z = z[k], Zc = z[(N - k) % N];
-    double ax = 0.5 * (Z.x + Zc.x), ay = 0.5 * (Z.y - Zc.y);
-    double bx = 0.5 * (Z.y + Zc.y), by = -0.5 * (Z.x - Zc.x);
-    int f0 = 2 * q, f1 = 2 * q + 1;
-    // scalar analyses (radial components): Advr, VSr, VxBr, VXir
-    auto wt = [&](int f) {
-      bool radial = (f == 0 || f == 3 || (MAG && f == 6) || (CHEM && f == (MAG ? 9 : 6)));
-      return radial ? ws : wv;
-    };
-    double w0 = wt(f0);
-    Gr[k * a.g_m + f0] = make_double2(w0 * ax, w0 * ay);
-    if (f1 < BF::NFO) {
-      double w1 = wt(f1);
-      Gr[k * a.g_m + f1] = make_double2(w1 * bx, w1 * by);
-    }
+  double2* Gr = a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * NFO;
+  for (int e = threadIdx.x; e < M * NFO; e += blockDim.x) {
+    int k = e / NFO, o = e - k * NFO;
+    const cplx<double>* z = buf + o * stride;
+    cplx<double> X = r2c_post(z[pad16(k)], z[pad16((H - k) % H)], k, t.twiddle);
+    // radial components (Advr, VSr, VxBr, VXir) are scalar analyses
+    bool radial = (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
+    double w = radial ? ws : wv;
+    Gr[k * a.g_m + o] = make_double2(w * X.x, w * X.y);
   }
 }
 
 template <bool MAG, bool CHEM>
 static int launch_nl_bouss_t(const NlBoussArgs& a, cudaStream_t st) {
   using BF = BoussFields<MAG, CHEM>;
-  size_t sm = (size_t)BF::RB * a.t.n_phi * 16;
+  size_t sm = (size_t)(BF::NB + kFftRowBatch) * padded_len(a.t.n_phi / 2) * sizeof(double2);
   auto kern = k_nl_bouss<MAG, CHEM>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid(a.t.n_theta, a.n_r);

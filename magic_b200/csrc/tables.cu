@@ -129,6 +129,7 @@ __global__ void k_twiddle(int n, double2* tw) {
 
 static int factor_radices(int n, int* out) {
   int ns = 0;
+  while (n % 8 == 0 && ns < kMaxFftStages) { out[ns++] = 8; n /= 8; }
   while (n % 4 == 0 && ns < kMaxFftStages) { out[ns++] = 4; n /= 4; }
   while (n % 2 == 0 && ns < kMaxFftStages) { out[ns++] = 2; n /= 2; }
   while (n % 3 == 0 && ns < kMaxFftStages) { out[ns++] = 3; n /= 3; }
@@ -146,7 +147,8 @@ int build_tables(mt_plan* p) {
   }
   MT_REQUIRE(pos == p->lm_max, MT_ERR_ARG, "lm_max mismatch");
   int radix[kMaxFftStages];
-  int nst = factor_radices(p->n_phi, radix);
+  MT_REQUIRE(p->n_phi % 2 == 0, MT_ERR_UNSUPPORTED, "n_phi_max must be even");
+  int nst = factor_radices(p->n_phi / 2, radix);  // real FFTs run as half-length complex FFTs
   MT_REQUIRE(nst > 0, MT_ERR_UNSUPPORTED, "n_phi_max must factor into 2, 3, 5");
 
   size_t tsz = (size_t)p->lm_max * nhs * sizeof(double);
