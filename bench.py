@@ -52,6 +52,31 @@ def flops_per_step(nhs, lm_max, n_r):
     return synth, anal
 
 
+def split_mma_flops(plan, n_r):
+    """Dense bf16 tensor-pipe FLOPs the split kernels issue per step (6 plane products
+    per table per 16-wide K chunk, M = 128 rows per CTA, padded tiles included)."""
+    nhs = plan.nhs
+    nth = 1 if nhs <= 256 else 2
+    wth = (((nhs + nth - 1) // nth) + 15) // 16 * 16
+    rows_s = n_r * 2 * 13
+    rows_a = (n_r - 2) * 2 * 8
+    tiles_s = -(-rows_s // 128)
+    tiles_a = -(-rows_a // 128)
+    syn = ana = 0.0
+    nchj = -(-nhs // 16)
+    for mc in range(plan.n_m_max):
+        nlm = plan.l_max - mc * plan.minc + 1
+        nk = [(nlm + 1) // 2, nlm // 2]
+        nch = [-(-k // 16) for k in nk]
+        for combo in (0, 1):
+            chunks = nch[combo] + nch[1 - combo]  # P chunks + dP chunks
+            syn += tiles_s * nth * chunks * 6 * 2.0 * 128 * wth * 16
+        for par in (0, 1):
+            wk = (nk[par] + 15) // 16 * 16
+            ana += tiles_a * nchj * 2 * 6 * 2.0 * 128 * wk * 16
+    return syn, ana
+
+
 def synth_inputs(plan, n_r, device, seed=0):
     g = torch.Generator(device="cpu").manual_seed(seed)
     l = torch.as_tensor(plan.lm2l, dtype=torch.float64)
@@ -212,7 +237,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--levels", type=int, default=N_R,
@@ -246,6 +271,8 @@ def main():
     prof = boussinesq_profiles(n_r, L_MAX, device=dev)
     out = {k: torch.zeros(plan.lm_max, n_r, dtype=torch.complex128, device=dev) for k in OUTS}
     work = torch.empty(plan.nl_bouss_workspace(n_r, True, False), dtype=torch.uint8, device=dev)
+
+    work.zero_()
 
     def step(parts=0):
         return plan.nl_bouss(fields, prof, LF, CF, AF, OPM, l_mag=True, l_chem=False, out=out,
@@ -336,15 +363,27 @@ def main():
     synth_f, anal_f = flops_per_step(plan.nhs, plan.lm_max, n_r)
     dom = max(part_ms, key=part_ms.get)
     roof = None
+    split = args.precision == "split"
     if dom == "phi_fft_products":
-        # algorithmic bytes: Fourier rows in (13 fields x 97 levels) and out
-        # (9 fields x 95 levels), each n_theta x n_m complex FP64
-        row = plan.n_theta_max * plan.n_m_max * 16
+        # algorithmic bytes: Fourier rows in (13 fields x n_r levels) and out
+        # (9 fields x (n_r - 2) levels), each n_theta x n_m complex values
+        # (FP64 complex in the plain path; FP32 sym/asym in, FP32 north/south
+        # out in the split path)
+        row = plan.n_theta_max * plan.n_m_max * (8 if split else 16)
         byts = (13 * n_r + 9 * (n_r - 2)) * row
         ach = byts / (part_ms[dom] * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": ach / peaks["hbm_gbs"], "traffic": None, "kernel": dom,
                 "peak_source": src}
+    elif split:
+        s_mma, a_mma = split_mma_flops(plan, n_r)
+        fl = s_mma if dom == "legendre_synthesis" else a_mma
+        pk = peaks["bf16_tflops"]
+        ach = fl / (part_ms[dom] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": ach / pk, "traffic": None, "kernel": dom,
+                "flops": "dense bf16 MMA FLOPs issued (6 plane products, padded tiles)",
+                "peak_source": f"{src} bf16_tflops (burst)"}
     else:
         fl = synth_f if dom == "legendre_synthesis" else anal_f
         pk = dgemm_peak(dev) if rank == 0 else float("nan")
@@ -360,12 +399,13 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic", "config": workload_config(args.precision),
+                "dtype": "bf16x3/f32" if split else "f64", "data": "synthetic",
+                "config": workload_config(args.precision),
                 "clocks": clocks.summary(),
                 "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
-                "gpu_launches": 6 * args.steps,
+                "gpu_launches": (4 if split else 6) * args.steps,
                 "kernel_ms": part_ms, "sht_tflops": sht_tflops,
                 "roofline": roof}
         if world == 1 and not args.no_cpu:

@@ -1,9 +1,11 @@
 // extern "C" entry points (include/magic_b200.h).
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include "fourier.cuh"
 #include "legendre.cuh"
+#include "split_kernels.cuh"
 
 namespace mt {
 
@@ -16,7 +18,9 @@ int launch_synth_f64(const SynthArgs<OP::NX>& a, cudaStream_t st);
 template <class OP, int R>
 int launch_anal_f64(const AnalArgs<OP::NX, OP::NO>& a, cudaStream_t st);
 
-// nonlinear.cu
+// split_tables.cu
+const SplitTables& split_tables(const mt_plan* p);
+const std::vector<int>& split_wk_host(const mt_plan* p);
 
 static int prime_decomposition(int n) {
   // smallest 2^i 3^j 5^k >= n, i < 13, j < 7, k < 7 (magic_torch/params.py:12-24)
@@ -64,8 +68,8 @@ int mt_plan_create(const mt_grid_desc* desc, mt_plan** out) {
   *out = nullptr;
   MT_REQUIRE(desc->l_max >= 1 && desc->minc >= 1 && desc->minc <= desc->l_max + 1, MT_ERR_ARG,
              "l_max >= 1 and 1 <= minc required");
-  MT_REQUIRE(desc->precision == MT_PREC_FP64, MT_ERR_UNSUPPORTED,
-             "this library build supports MT_PREC_FP64 plans only");
+  MT_REQUIRE(desc->precision == MT_PREC_FP64 || desc->precision == MT_PREC_SPLIT,
+             MT_ERR_UNSUPPORTED, "precision must be MT_PREC_FP64 or MT_PREC_SPLIT");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("no CUDA device");
@@ -101,6 +105,7 @@ int mt_plan_create(const mt_grid_desc* desc, mt_plan** out) {
   if (2 * (p->n_m - 1) >= p->n_phi)
     return fail(MT_ERR_UNSUPPORTED, "n_phi_max too small for l_max/minc (modes alias)");
   int rc = build_tables(p);
+  if (rc == MT_OK && p->precision == MT_PREC_SPLIT) rc = build_split_tables(p);
   if (rc != MT_OK) {
     std::string keep = g_err;
     mt_plan_destroy(p);
@@ -117,6 +122,7 @@ int mt_plan_destroy(mt_plan* p) {
                   p->d_wq,     p->d_wq_v,  p->d_ost2,  p->d_cosn, p->d_twiddle};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  free_split_tables(p);
   delete p;
   return MT_OK;
 }
@@ -571,12 +577,205 @@ static int nl_bouss_t(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt
   return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
 }
 
+// ---- split-precision fused stage ------------------------------------------
+
+struct SplitWs {
+  size_t err, fs, gs, mx, total;
+  int64_t rows_syn, rows_nl;
+};
+
+static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
+  SplitWs w;
+  w.rows_syn = (int64_t)n_r * 2 * bouss_nfi(mag, chem);
+  w.rows_nl = (int64_t)(n_r - 2) * 2 * bouss_nfo(mag, chem);
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  w.err = 0;
+  w.fs = 256;
+  w.gs = w.fs + al((size_t)p->n_m * 2 * p->nhs * w.rows_syn * sizeof(float));
+  w.mx = w.gs + al((size_t)p->n_m * 2 * p->nhs * w.rows_nl * sizeof(float));
+  w.total = w.mx + al(2 * (size_t)n_r * sizeof(unsigned long long));
+  return w;
+}
+
+static RowOp rop(int tP, int cP, int kP, int tD = 0, int cD = 0, int kD = 0, int scale = 0) {
+  RowOp o;
+  o.tP = (int8_t)tP;
+  o.cP = (int8_t)cP;
+  o.kP = (int8_t)kP;
+  o.tD = (int8_t)tD;
+  o.cD = (int8_t)cD;
+  o.kD = (int8_t)kD;
+  o.scale = (int8_t)scale;
+  o.pad = 0;
+  return o;
+}
+
+// coef codes: 1 +1, 2 -1, 3 +m, 4 -m
+static void syn_group_ops(RowOp* ops, int Q, int S, int T) {
+  ops[0] = rop(Q, 0, 1);            // r.re = (P.Q).re
+  ops[1] = rop(Q, 1, 1);            // r.im
+  ops[2] = rop(T, 1, 4, S, 0, 1);   // theta.re = -m (P.T).im + (dP.S).re
+  ops[3] = rop(T, 0, 3, S, 1, 1);   // theta.im = +m (P.T).re + (dP.S).im
+  ops[4] = rop(S, 1, 4, T, 0, 2);   // phi.re = -m (P.S).im - (dP.T).re
+  ops[5] = rop(S, 0, 3, T, 1, 2);   // phi.im = +m (P.S).re - (dP.T).im
+}
+
+static int ana_scalar_ops(RowOp* ops, int x) {
+  ops[0] = rop(x, 0, 1);
+  ops[1] = rop(x, 1, 1);
+  return 2;
+}
+// S = dP.a - i m P.b ; T = -dP.b - i m P.a  (a = theta field, b = phi field), / l(l+1)
+static int ana_s_ops(RowOp* ops, int a, int b) {
+  ops[0] = rop(b, 1, 3, a, 0, 1, 1);
+  ops[1] = rop(b, 0, 4, a, 1, 1, 1);
+  return 2;
+}
+static int ana_t_ops(RowOp* ops, int a, int b) {
+  ops[0] = rop(a, 1, 3, b, 0, 2, 1);
+  ops[1] = rop(a, 0, 4, b, 1, 2, 1);
+  return 2;
+}
+
+template <bool MAG, bool CHEM>
+static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
+                            const mt_bouss_out* out, const mt_bouss_params* q, double* dtrkc,
+                            double* dthkc, void* work, cudaStream_t st) {
+  const int nfi = bouss_nfi(MAG, CHEM), nfo = bouss_nfo(MAG, CHEM);
+  const SplitWs W = split_ws(p, n_r, MAG, CHEM);
+  char* w = (char*)work;
+  int* err = (int*)(w + W.err);
+  float* Fs = (float*)(w + W.fs);
+  float* Gs = (float*)(w + W.gs);
+  unsigned long long* mx = (unsigned long long*)(w + W.mx);
+  const int parts = q->parts ? q->parts : 7;
+  auto c = [](const double* x) { return (const double2*)x; };
+  const int64_t fs_j = W.rows_syn, fs_c = (int64_t)p->nhs * fs_j, fs_m = 2 * fs_c;
+  const int64_t g_j = W.rows_nl, g_h = (int64_t)p->nhs * g_j, g_m = 2 * g_h;
+
+  if (parts & 1) {
+    MT_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    SplitSynArgs s{};
+    s.t = p->tab;
+    s.s = split_tables(p);
+    int x = 0;
+    if (MAG) {
+      s.src[x++] = {c(in->b), nullptr, kDlh};
+      s.src[x++] = {c(in->db), nullptr, kRaw};
+      s.src[x++] = {c(in->aj), nullptr, kRaw};
+      s.src[x++] = {c(in->aj), nullptr, kDlh};
+      s.src[x++] = {c(in->dj), nullptr, kRaw};
+      s.src[x++] = {c(in->b), c(in->ddb), kCurlT};
+    }
+    s.src[x++] = {c(in->w), nullptr, kDlh};
+    s.src[x++] = {c(in->dw), nullptr, kRaw};
+    s.src[x++] = {c(in->z), nullptr, kRaw};
+    s.src[x++] = {c(in->z), nullptr, kDlh};
+    s.src[x++] = {c(in->dz), nullptr, kRaw};
+    s.src[x++] = {c(in->w), c(in->ddw), kCurlT};
+    const int xs = x;
+    s.src[x++] = {c(in->s), nullptr, kRaw};
+    if (CHEM) s.src[x++] = {c(in->xi), nullptr, kRaw};
+    const int G = MAG ? 4 : 2;
+    for (int g = 0; g < G; ++g) syn_group_ops(&s.ops[6 * g], 3 * g, 3 * g + 1, 3 * g + 2);
+    ana_scalar_ops(&s.ops[6 * G], xs);
+    if (CHEM) ana_scalar_ops(&s.ops[6 * G + 2], xs + 1);
+    s.ld = in->ld;
+    s.or2 = q->or2;
+    s.nrows = (int)W.rows_syn;
+    s.row_per_level = 2 * nfi;
+    s.Fs = Fs;
+    s.fs_m = fs_m;
+    s.fs_c = fs_c;
+    s.fs_j = fs_j;
+    s.err = err;
+    MT_TRY(launch_synth_split(s, st));
+  }
+  if (parts & 2) {
+    MT_CHECK_CUDA(cudaMemsetAsync(mx, 0, 2 * n_r * sizeof(unsigned long long), st));
+    NlSplitArgs nl{};
+    nl.t = p->tab;
+    nl.n_r = n_r;
+    nl.Fs = Fs;
+    nl.fs_m = fs_m;
+    nl.fs_c = fs_c;
+    nl.fs_j = fs_j;
+    nl.G = Gs;
+    nl.g_m = g_m;
+    nl.g_h = g_h;
+    nl.g_j = g_j;
+    nl.or2 = q->or2;
+    nl.or4 = q->or4;
+    nl.orho1 = q->orho1;
+    nl.orho2 = q->orho2;
+    nl.delxr2 = q->delxr2;
+    nl.delxh2 = q->delxh2;
+    nl.LFfac = q->LFfac;
+    nl.cour_mode = MAG ? q->cour_mode : 0;
+    nl.cf2 = q->courfac * q->courfac;
+    nl.af2 = q->alffac * q->alffac;
+    double h = 0.5 * (1.0 + q->opm);
+    nl.valfac = h * h;
+    nl.vr2max = mx;
+    nl.vh2max = mx + n_r;
+    MT_TRY(launch_nl_bouss_split(MAG, CHEM, nl, st));
+  }
+  if (!(parts & 4)) return MT_OK;
+  SplitAnaArgs a{};
+  a.t = p->tab;
+  a.s = split_tables(p);
+  {
+    const std::vector<int>& wk = split_wk_host(p);
+    a.wk_max = *std::max_element(wk.begin(), wk.end());
+  }
+  a.G = Gs;
+  a.g_m = g_m;
+  a.g_h = g_h;
+  a.g_j = g_j;
+  a.g_level = 2 * nfo;
+  int o = 0, r = 0;
+  // output fields and their row programs (magic_torch/step_time.py:1066-1124)
+  r += ana_scalar_ops(&a.ops[r], 0);
+  a.out[o++] = (double2*)out->Advr;
+  r += ana_s_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advt;
+  r += ana_t_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advp;
+  r += ana_scalar_ops(&a.ops[r], 3);
+  a.out[o++] = (double2*)out->VSr;
+  r += ana_s_ops(&a.ops[r], 4, 5);
+  a.out[o++] = (double2*)out->VSt;
+  if (MAG) {
+    r += ana_scalar_ops(&a.ops[r], 6);
+    a.out[o++] = (double2*)out->VxBr;
+    r += ana_s_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBt;
+    r += ana_t_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBp;
+  }
+  if (CHEM) {
+    const int x0 = MAG ? 9 : 6;
+    r += ana_scalar_ops(&a.ops[r], x0);
+    a.out[o++] = (double2*)out->VXir;
+    r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
+    a.out[o++] = (double2*)out->VXit;
+  }
+  a.row_per_level = r;
+  a.nrows = (n_r - 2) * r;
+  a.ld = out->ld;
+  a.out_col0 = 1;
+  a.err = err;
+  MT_TRY(launch_anal_split(a, st));
+  return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
+}
+
 }  // namespace mt
 
 extern "C" {
 
 size_t mt_nl_bouss_workspace(const mt_plan* p, int n_r, int l_mag, int l_chem) {
   if (!p || n_r < 3) return 0;
+  if (p->precision == MT_PREC_SPLIT) return split_ws(p, n_r, l_mag, l_chem).total;
   size_t f = fourier_bytes(p, (int64_t)n_r * bouss_nfi(l_mag, l_chem));
   size_t g = fourier_bytes(p, (int64_t)(n_r - 2) * bouss_nfo(l_mag, l_chem));
   return f + g + 2 * (size_t)n_r * sizeof(unsigned long long) + 256;
@@ -602,6 +801,13 @@ int mt_nl_bouss(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt_bouss
   MT_REQUIRE(work && work_bytes >= mt_nl_bouss_workspace(p, n_r, q->l_mag, q->l_chem),
              MT_ERR_WORKSPACE, "workspace too small");
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_SPLIT) {
+    if (q->l_mag)
+      return q->l_chem ? nl_bouss_split_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                       : nl_bouss_split_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+    return q->l_chem ? nl_bouss_split_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                     : nl_bouss_split_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+  }
   if (q->l_mag)
     return q->l_chem ? nl_bouss_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
                      : nl_bouss_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);

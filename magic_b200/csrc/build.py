@@ -18,7 +18,8 @@ ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libmagic_b200.so")
 BUILD = os.path.join(ROOT, "_build")
 
-SOURCES = ["api.cu", "tables.cu", "legendre_f64.cu", "fourier.cu", "nonlinear.cu"]
+SOURCES = ["api.cu", "tables.cu", "legendre_f64.cu", "fourier.cu", "nonlinear.cu",
+           "split_tables.cu", "legendre_split.cu", "nl_split.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

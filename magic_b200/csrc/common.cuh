@@ -73,8 +73,11 @@ struct mt_plan {
 
 namespace mt {
 
-// Build all tables of a plan on the current device (tables.cu).
+// Build all tables of a plan on the current device (tables.cu); the bf16x3
+// table images of split-precision plans (split_tables.cu).
 int build_tables(mt_plan* p);
+int build_split_tables(mt_plan* p);
+void free_split_tables(mt_plan* p);
 
 // Transform launchers (legendre_f64.cu, fourier.cu).
 enum class SynthOp { kScalar = 0, kTorpol = 1, kGrad = 2 };

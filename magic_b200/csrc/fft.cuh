@@ -160,30 +160,37 @@ __device__ __forceinline__ void dft_small(cplx<R> (&v)[RADIX]) {
   }
 }
 
+// floor(n / d) for 0 <= n < 2^22 from a float reciprocal of d (exact in this
+// range: the product is off by < 2^-24 relative, far below the 0.5/d margin).
+__device__ __forceinline__ int fdiv(int n, float rcp) {
+  return __float2int_rd(((float)n + 0.5f) * rcp);
+}
+
 // One out-of-place Stockham stage over `nrows` rows of length H: src rows at
 // src + row * stride, dst rows at dst + row * stride (padded indexing).
-// tw: exp(-2 pi i n / (tw_mul * H)), indexed with stride tw_mul.
+// tw: shared-memory table exp(-2 pi i n / H), n < H.
 template <int RADIX, bool INV, typename R>
 __device__ __forceinline__ void fft_stage(const cplx<R>* __restrict__ src, cplx<R>* __restrict__ dst,
                                           int nrows, int H, int stride, int Ns,
-                                          const double2* __restrict__ tw, int tw_mul) {
+                                          const cplx<R>* __restrict__ tw) {
   const int nbr = H / RADIX;
   const int total = nrows * nbr;
-  const int twstep = (H / (Ns * RADIX)) * tw_mul;
+  const int twstep = H / (Ns * RADIX);
+  const float rcp_nbr = 1.0f / (float)nbr, rcp_ns = 1.0f / (float)Ns;
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
-    const int row = b / nbr, j = b - row * nbr;
+    const int row = fdiv(b, rcp_nbr), j = b - row * nbr;
     const cplx<R>* x = src + row * stride;
-    const int jm = j % Ns;
+    const int jm = j - fdiv(j, rcp_ns) * Ns;
     cplx<R> v[RADIX];
 #pragma unroll
-    for (int r = 0; r < RADIX; ++r) {
-      cplx<R> e = x[pad16(j + r * nbr)];
-      if (r > 0 && jm > 0) {
-        double2 w = __ldg(&tw[r * jm * twstep]);
-        cplx<R> ww = {(R)w.x, INV ? (R)-w.y : (R)w.y};
-        e = cmul(e, ww);
+    for (int r = 0; r < RADIX; ++r) v[r] = x[pad16(j + r * nbr)];
+    if (jm > 0) {
+#pragma unroll
+      for (int r = 1; r < RADIX; ++r) {
+        cplx<R> w = tw[r * jm * twstep];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
       }
-      v[r] = e;
     }
     dft_small<RADIX, INV>(v);
     cplx<R>* y = dst + row * stride;
@@ -198,11 +205,12 @@ constexpr int kFftRowBatch = 7;  // rows per pass through the scratch buffer
 
 // Full transform of `nrows` rows (in place), ping-ponging each batch of at
 // most kFftRowBatch rows through `scratch` (kFftRowBatch * stride values).
-// Radices come from the plan (product H, each of 2, 3, 4, 5, 8).
+// Radices come from the plan (product H, each of 2, 3, 4, 5, 8); tw is the
+// shared-memory table exp(-2 pi i n/H), n < H (fft_twiddles_to_smem).
 template <bool INV, typename R>
 __device__ __forceinline__ void fft_rows(cplx<R>* buf, cplx<R>* scratch, int nrows, int H,
                                          int stride, const int* radix, int nstages,
-                                         const double2* __restrict__ tw, int tw_mul) {
+                                         const cplx<R>* __restrict__ tw) {
   for (int r0 = 0; r0 < nrows; r0 += kFftRowBatch) {
     cplx<R>* a = buf + r0 * stride;
     cplx<R>* b = scratch;
@@ -211,11 +219,11 @@ __device__ __forceinline__ void fft_rows(cplx<R>* buf, cplx<R>* scratch, int nro
     for (int s = 0; s < nstages; ++s) {
       int rad = radix[s];
       switch (rad) {
-        case 8: fft_stage<8, INV>(a, b, nr, H, stride, Ns, tw, tw_mul); break;
-        case 4: fft_stage<4, INV>(a, b, nr, H, stride, Ns, tw, tw_mul); break;
-        case 3: fft_stage<3, INV>(a, b, nr, H, stride, Ns, tw, tw_mul); break;
-        case 2: fft_stage<2, INV>(a, b, nr, H, stride, Ns, tw, tw_mul); break;
-        default: fft_stage<5, INV>(a, b, nr, H, stride, Ns, tw, tw_mul); break;
+        case 8: fft_stage<8, INV>(a, b, nr, H, stride, Ns, tw); break;
+        case 4: fft_stage<4, INV>(a, b, nr, H, stride, Ns, tw); break;
+        case 3: fft_stage<3, INV>(a, b, nr, H, stride, Ns, tw); break;
+        case 2: fft_stage<2, INV>(a, b, nr, H, stride, Ns, tw); break;
+        default: fft_stage<5, INV>(a, b, nr, H, stride, Ns, tw); break;
       }
       Ns *= rad;
       cplx<R>* t = a;
@@ -228,6 +236,25 @@ __device__ __forceinline__ void fft_rows(cplx<R>* buf, cplx<R>* scratch, int nro
       __syncthreads();
     }
   }
+}
+
+// H-point twiddles exp(-2 pi i n/H) = tw_N[2n] into shared memory (caller syncs).
+template <typename R>
+__device__ __forceinline__ void fft_twiddles_to_smem(cplx<R>* tws, int H,
+                                                     const double2* __restrict__ tw_N) {
+  for (int n = threadIdx.x; n < H; n += blockDim.x) {
+    double2 w = __ldg(&tw_N[2 * n]);
+    tws[n] = {(R)w.x, (R)w.y};
+  }
+}
+
+// 16-byte global -> shared copy that does not hold a register (cp.async).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
 }
 
 // ---- real rows through half-length complex FFTs --------------------------

@@ -42,21 +42,25 @@ __global__ void __launch_bounds__(kFftThreads) k_fourier_to_grid(ToGridArgs a) {
   const int row = blockIdx.y;
   const int col0 = blockIdx.x * kColsPerCta;
   const int ncol = min(kColsPerCta, a.ncols - col0);
+  cplx<double>* tws = buf + (kColsPerCta + kFftRowBatch) * stride;
+  fft_twiddles_to_smem(tws, H, t.twiddle);
   for (int i = threadIdx.x; i < ncol * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
   const double2* Fr = a.F + (int64_t)row * a.f_row + col0;
+  const float rcp = 1.0f / (float)ncol;
   for (int e = threadIdx.x; e < M * ncol; e += blockDim.x) {
-    int k = e / ncol, q = e - k * ncol;
-    double2 X = Fr[k * a.f_m + q];
-    buf[q * stride + pad16(k)] = {X.x, X.y};
+    int k = fdiv(e, rcp), q = e - k * ncol;
+    cp_async16(&buf[q * stride + pad16(k)], &Fr[k * a.f_m + q]);
   }
+  cp_async_wait_all();
   __syncthreads();
   for (int q = threadIdx.x / 64; q < ncol; q += kFftThreads / 64)
     c2r_prepare(buf + q * stride, H, t.twiddle, threadIdx.x % 64, 64);
   __syncthreads();
-  fft_rows<true>(buf, buf + kColsPerCta * stride, ncol, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
+  fft_rows<true>(buf, buf + kColsPerCta * stride, ncol, H, stride, t.fft_radix, t.fft_nstages, tws);
+  const float rcpN = 1.0f / (float)N;
   for (int e = threadIdx.x; e < ncol * N; e += blockDim.x) {
-    int q = e / N, n = e - q * N;
+    int q = fdiv(e, rcpN), n = e - q * N;
     cplx<double> z = buf[q * stride + pad16(n >> 1)];
     int c = col0 + q;
     int f = c / a.B, b = c % a.B;
@@ -73,19 +77,23 @@ __global__ void __launch_bounds__(kFftThreads) k_grid_to_fourier(ToFourierArgs a
   const int row = blockIdx.y;
   const int col0 = blockIdx.x * kColsPerCta;
   const int ncol = min(kColsPerCta, a.ncols - col0);
+  cplx<double>* tws = buf + (kColsPerCta + kFftRowBatch) * stride;
+  fft_twiddles_to_smem(tws, H, t.twiddle);
+  const float rcpH = 1.0f / (float)H;
   for (int e = threadIdx.x; e < ncol * H; e += blockDim.x) {
-    int q = e / H, h = e - q * H;
+    int q = fdiv(e, rcpH), h = e - q * H;
     int c = col0 + q;
     const double* src = a.in[c / a.B] + ((int64_t)(c % a.B) * nt + row) * N;
     double2 v = *reinterpret_cast<const double2*>(src + 2 * h);
     buf[q * stride + pad16(h)] = {v.x, v.y};
   }
   __syncthreads();
-  fft_rows<false>(buf, buf + kColsPerCta * stride, ncol, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
+  fft_rows<false>(buf, buf + kColsPerCta * stride, ncol, H, stride, t.fft_radix, t.fft_nstages, tws);
   const double w = (a.vector ? t.wq_v[row] : t.wq[row]) / N;
   double2* Fr = a.F + (int64_t)row * a.f_row + col0;
+  const float rcpc = 1.0f / (float)ncol;
   for (int e = threadIdx.x; e < M * ncol; e += blockDim.x) {
-    int k = e / ncol, q = e - k * ncol;
+    int k = fdiv(e, rcpc), q = e - k * ncol;
     const cplx<double>* z = buf + q * stride;
     cplx<double> X = r2c_post(z[pad16(k)], z[pad16((H - k) % H)], k, t.twiddle);
     Fr[k * a.f_m + q] = make_double2(w * X.x, w * X.y);
@@ -93,7 +101,8 @@ __global__ void __launch_bounds__(kFftThreads) k_grid_to_fourier(ToFourierArgs a
 }
 
 static size_t fft_smem(const Tables& t) {
-  return (size_t)(kColsPerCta + kFftRowBatch) * padded_len(t.n_phi / 2) * sizeof(double2);
+  return ((size_t)(kColsPerCta + kFftRowBatch) * padded_len(t.n_phi / 2) + t.n_phi / 2) *
+         sizeof(double2);
 }
 
 int launch_fourier_to_grid(const ToGridArgs& a, cudaStream_t st) {
@@ -117,7 +126,8 @@ int launch_grid_to_fourier(const ToFourierArgs& a, cudaStream_t st) {
 }
 
 // Largest n_phi the fused stage's shared memory holds: 14 field rows plus a
-// 7-row scratch of H = n_phi/2 padded complex FP64 values within 227 KB.
-int fft_max_nphi() { return 1200; }
+// 7-row scratch of H = n_phi/2 padded complex FP64 values and the H-point
+// twiddle table within 227 KB.
+int fft_max_nphi() { return 1168; }
 
 }  // namespace mt

@@ -52,7 +52,7 @@ struct SynthCfg {
 };
 
 template <class OP, int R>
-__global__ void __launch_bounds__(256) k_synth_f64(SynthArgs<OP::NX> a) {
+__global__ void __launch_bounds__(256, 2) k_synth_f64(SynthArgs<OP::NX> a) {
   using C = SynthCfg<OP, R>;
   constexpr int NX = OP::NX, NP = OP::NP, NT = OP::NT, NO = OP::NO;
   constexpr int TH = C::TH, KC = C::KC, SA = C::SA, SB = C::SB, WC = C::WC;
@@ -197,7 +197,7 @@ struct AnalCfg {
 };
 
 template <class OP, int R>
-__global__ void __launch_bounds__(256) k_anal_f64(AnalArgs<OP::NX, OP::NO> a) {
+__global__ void __launch_bounds__(256, 2) k_anal_f64(AnalArgs<OP::NX, OP::NO> a) {
   using C = AnalCfg<OP, R>;
   constexpr int NX = OP::NX, NP = OP::NP, NT = OP::NT, NO = OP::NO;
   constexpr int TK = C::TK, KC = C::KC, SA = C::SA, SB = C::SB, WC = C::WC;

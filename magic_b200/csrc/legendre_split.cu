@@ -1,0 +1,429 @@
+// Split-precision (bf16x3, FP32 accumulate) Legendre contractions on tcgen05.
+//
+// Orientation: the data operand is A (M = 128 rows per CTA, one row per
+// output real component), the Legendre table is B (N = theta rows for the
+// synthesis, l rows for the analysis), K runs over l (synthesis) or theta
+// pairs (analysis) in chunks of 16.  Each output row is a fixed linear
+// combination "A_P . P + A_dP . dP": the row's A_P and A_dP entries are
+// scaled source values (e.g. v_theta.re = (dP.S).re - m (P.T).im), so one
+// fp32 TMEM accumulator holds the finished field component.
+//
+// Equatorial parity: the synthesis CTA for combo c in {sym, asym} contracts
+// P over l - m of parity c and dP over the other parity; north = sym + asym,
+// south = sym - asym (formed by the phi-stage kernel).  The analysis CTA for
+// output parity p reads the folded Fourier data north + south (P rows of even
+// parity, dP rows of odd) or north - south (the other two cases).
+//
+// Warp roles (192 threads): warps 0-3 build the A tiles (bf16x3 split in
+// registers, written in the canonical core-matrix layout) and run the
+// epilogue (tcgen05.ld, one TMEM lane per thread); warp 4 owns TMEM and
+// bulk-copies the pre-split table chunks; warp 5 lane 0 issues tcgen05.mma
+// (6 plane products per table per chunk) and commits to the stage barriers.
+#include "legendre.cuh"
+#include "split.cuh"
+#include "split_kernels.cuh"
+#include "umma.cuh"
+
+namespace mt {
+
+constexpr int kSplitStages = 3;
+constexpr int kSplitThreads = 192;
+
+// plane pairs (a, b) of the six retained products
+__device__ __constant__ int8_t kPairA[6] = {0, 0, 1, 0, 1, 2};
+__device__ __constant__ int8_t kPairB[6] = {0, 1, 0, 2, 1, 0};
+
+__device__ __forceinline__ double coef_value(int code, double m) {
+  switch (code) {
+    case 1: return 1.0;
+    case 2: return -1.0;
+    case 3: return m;
+    case 4: return -m;
+    default: return 0.0;
+  }
+}
+
+// Write 16 consecutive K values of one row as 3 planes into an A tile.
+__device__ __forceinline__ void put_row16(uint8_t* tile, int row, const double (&v)[16]) {
+  __nv_bfloat16 q[3][16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) split3(v[i], q[0][i], q[1][i], q[2][i]);
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      uint4 w;
+      w.x = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 0]);
+      w.y = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 2]);
+      w.z = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 4]);
+      w.w = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 6]);
+      *reinterpret_cast<uint4*>(tile + s * (kSplitRows * 32) + core_off(row, 8 * half)) = w;
+    }
+  }
+}
+
+__device__ __forceinline__ double term_value(const TermSrc& s, int64_t row, int64_t ld, int col,
+                                             double dlh, const double* or2, int comp) {
+  const double2* pa = s.a + row * ld + col;
+  double2 v = __ldg(pa);
+  double x = comp ? v.y : v.x;
+  switch (s.recipe) {
+    case kRaw: return x;
+    case kDlh: return dlh * x;
+    case kCurlT: {
+      double2 w = __ldg(s.b + row * ld + col);
+      return __ldg(&or2[col]) * dlh * x - (comp ? w.y : w.x);
+    }
+    default: return 0.0;
+  }
+}
+
+// Shared memory of one CTA: stages of [A_P | A_dP | B_P | B_dP], then barriers.
+struct SplitSmem {
+  uint32_t a_plane, b_plane, stage_bytes, bar_off;
+  __host__ __device__ SplitSmem(int brows) {
+    a_plane = kSplitRows * 32;
+    b_plane = brows * 32;
+    stage_bytes = 6 * a_plane + 6 * b_plane;
+    bar_off = kSplitStages * stage_bytes;
+  }
+  __host__ __device__ size_t total() const { return bar_off + 8 * (3 * kSplitStages + 1) + 16; }
+};
+
+// ------------------------------------------------------------- synthesis
+
+__global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const Tables& t = a.t;
+  const SplitTables& st = a.s;
+  const int wth = st.wth;
+  const SplitSmem L(wth);
+  uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* full_b = full_a + kSplitStages;
+  uint64_t* empty = full_b + kSplitStages;
+  uint64_t* accb = empty + kSplitStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  // an earlier CTA already timed out: skip the work so a fault costs one wait, not one per CTA
+  if (*(volatile int*)a.err) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int rt = blockIdx.x;
+  const int combo = blockIdx.y & 1, tau = blockIdx.y >> 1;
+  const int mc = blockIdx.z;
+  const int m = mc * t.minc;
+  const int nlm = t.l_max - m + 1;
+  const int ls = t.lstart[mc];
+  const int par_t[2] = {combo, 1 - combo};  // parity of l - m contracted with P, dP
+  int nch_t[2];
+  for (int q = 0; q < 2; ++q) nch_t[q] = (split_nk(nlm, par_t[q]) + kSplitKC - 1) / kSplitKC;
+  const int nch = max(nch_t[0], nch_t[1]);
+  const uint32_t tcols = wth <= 32 ? 32 : (wth <= 64 ? 64 : (wth <= 128 ? 128 : 256));
+
+  if (tid == 0) {
+    for (int s = 0; s < kSplitStages; ++s) {
+      mbar_init(&full_a[s], kSplitRows);
+      mbar_init(&full_b[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accb, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 4) tmem_alloc(tmem_slot, tcols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  if (warp < 4) {
+    // ---------------- producer: row tid of this tile ----------------
+    const int R = rt * kSplitRows + tid;
+    const bool live = R < a.nrows;
+    const int lev = live ? R / a.row_per_level : 0;
+    const int q = live ? R - lev * a.row_per_level : 0;
+    const RowOp op = a.ops[q];
+    const double dm = (double)m;
+    const double cP = coef_value(op.kP, dm), cD = coef_value(op.kD, dm);
+    for (int c = 0; c < nch; ++c) {
+      const int s = c % kSplitStages;
+      if (c >= kSplitStages &&
+          !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 1))
+        break;
+      uint8_t* stage = smem + s * L.stage_bytes;
+      double vp[16], vd[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int kp = 2 * (kSplitKC * c + i) + par_t[0];
+        const int kd = 2 * (kSplitKC * c + i) + par_t[1];
+        vp[i] = 0.0;
+        vd[i] = 0.0;
+        if (live && op.kP && kp < nlm) {
+          double l = m + kp;
+          vp[i] = cP * term_value(a.src[op.tP], ls + kp, a.ld, lev, l * (l + 1.0), a.or2, op.cP);
+        }
+        if (live && op.kD && kd < nlm) {
+          double l = m + kd;
+          vd[i] = cD * term_value(a.src[op.tD], ls + kd, a.ld, lev, l * (l + 1.0), a.or2, op.cD);
+        }
+      }
+      put_row16(stage, tid, vp);
+      put_row16(stage + 3 * L.a_plane, tid, vd);
+      fence_proxy_async();
+      mbar_arrive(&full_a[s]);
+    }
+    // ---------------- epilogue ----------------
+    const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 2);
+    tc_fence_after();
+    if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
+      float* out = a.Fs + (int64_t)mc * a.fs_m + (int64_t)combo * a.fs_c;
+      for (int c0 = 0; c0 < wth; c0 += 16) {
+        float v[16];
+        tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
+        if (live) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int th = tau * wth + c0 + i;
+            if (th < t.nhs) out[(int64_t)th * a.fs_j + R] = v[i];
+          }
+        }
+      }
+    }
+  } else if (warp == 4) {
+    // ---------------- table loader ----------------
+    if (lane == 0) {
+      const uint8_t* img[2];
+      for (int q = 0; q < 2; ++q)
+        img[q] = st.syn + st.syn_off[((mc * 2 + q) * 2 + par_t[q]) * st.nthtile + tau];
+      const uint32_t chunk = 3 * L.b_plane;
+      int issued = 0;
+      for (int c = 0; c < nch; ++c) {
+        const int s = c % kSplitStages;
+        if (c >= kSplitStages &&
+            !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 3))
+          break;
+        uint8_t* stage = smem + s * L.stage_bytes + 6 * L.a_plane;
+        uint32_t bytes = (c < nch_t[0] ? chunk : 0) + (c < nch_t[1] ? chunk : 0);
+        mbar_expect_tx(&full_b[s], bytes);
+        for (int q = 0; q < 2; ++q)
+          if (c < nch_t[q]) bulk_g2s(stage + q * chunk, img[q] + (int64_t)c * chunk, chunk, &full_b[s]);
+        issued = c + 1;
+      }
+      // drain: every issued copy must land before the CTA may exit
+      for (int c = max(0, issued - kSplitStages); c < issued; ++c)
+        mbar_wait(&full_b[c % kSplitStages], (c / kSplitStages) & 1, abort_flag, nullptr, 0);
+    }
+  } else {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16(kSplitRows, wth);
+      uint32_t acc = 0;
+      for (int c = 0; c < nch; ++c) {
+        const int s = c % kSplitStages;
+        const uint32_t ph = (c / kSplitStages) & 1;
+        if (!mbar_wait(&full_a[s], ph, abort_flag, a.err, 4)) break;
+        if (!mbar_wait(&full_b[s], ph, abort_flag, a.err, 5)) break;
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * L.stage_bytes);
+        const uint32_t sb = sa + 6 * L.a_plane;
+        for (int q = 0; q < 2; ++q) {
+          if (c >= nch_t[q]) continue;
+#pragma unroll
+          for (int pp = 0; pp < 6; ++pp) {
+            uint64_t da = umma_desc(sa + q * 3 * L.a_plane + kPairA[pp] * L.a_plane, 128, 256);
+            uint64_t db = umma_desc(sb + q * 3 * L.b_plane + kPairB[pp] * L.b_plane, 128, 256);
+            umma_bf16(tbase, da, db, idesc, acc);
+            acc = 1;
+          }
+        }
+        umma_commit(&empty[s]);
+      }
+      umma_commit(accb);  // also on abort: lets the epilogue wait finish after in-flight MMAs
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 4) {
+    tc_fence_after();
+    tmem_dealloc(tbase, tcols);
+  }
+}
+
+// -------------------------------------------------------------- analysis
+
+__global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const Tables& t = a.t;
+  const SplitTables& st = a.s;
+  const int rt = blockIdx.x, par = blockIdx.y, mc = blockIdx.z;
+  const int wk = st.ana_wk[mc * 2 + par];
+  if (wk == 0 || *(volatile int*)a.err) return;
+  const SplitSmem L(a.wk_max);
+  uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* full_b = full_a + kSplitStages;
+  uint64_t* empty = full_b + kSplitStages;
+  uint64_t* accb = empty + kSplitStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m = mc * t.minc;
+  const int nlm = t.l_max - m + 1;
+  const int ls = t.lstart[mc];
+  const int nch = (t.nhs + kSplitKC - 1) / kSplitKC;
+  // folded input for P rows: north+south if the output parity is even; dP the reverse
+  const int fold_t[2] = {par, 1 - par};
+  const uint32_t tcols = wk <= 32 ? 32 : (wk <= 64 ? 64 : (wk <= 128 ? 128 : 256));
+  const uint32_t b_plane = wk * 32;
+
+  if (tid == 0) {
+    for (int s = 0; s < kSplitStages; ++s) {
+      mbar_init(&full_a[s], kSplitRows);
+      mbar_init(&full_b[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accb, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 4) tmem_alloc(tmem_slot, tcols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  if (warp < 4) {
+    const int R = rt * kSplitRows + tid;
+    const bool live = R < a.nrows;
+    const int lev = live ? R / a.row_per_level : 0;
+    const int q = live ? R - lev * a.row_per_level : 0;
+    const RowOp op = a.ops[q];
+    const double dm = (double)m;
+    const double cP = coef_value(op.kP, dm), cD = coef_value(op.kD, dm);
+    const float* g = a.G + (int64_t)mc * a.g_m;
+    const int64_t colP = (int64_t)lev * a.g_level + 2 * op.tP + op.cP;
+    const int64_t colD = (int64_t)lev * a.g_level + 2 * op.tD + op.cD;
+    const double sgP = fold_t[0] ? -1.0 : 1.0, sgD = fold_t[1] ? -1.0 : 1.0;
+    for (int c = 0; c < nch; ++c) {
+      const int s = c % kSplitStages;
+      if (c >= kSplitStages &&
+          !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 11))
+        break;
+      uint8_t* stage = smem + s * L.stage_bytes;
+      double vp[16], vd[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int j = kSplitKC * c + i;
+        vp[i] = 0.0;
+        vd[i] = 0.0;
+        if (live && j < t.nhs) {
+          const float* gj = g + (int64_t)j * a.g_j;
+          if (op.kP) vp[i] = cP * ((double)__ldg(gj + colP) + sgP * (double)__ldg(gj + a.g_h + colP));
+          if (op.kD) vd[i] = cD * ((double)__ldg(gj + colD) + sgD * (double)__ldg(gj + a.g_h + colD));
+        }
+      }
+      put_row16(stage, tid, vp);
+      put_row16(stage + 3 * L.a_plane, tid, vd);
+      fence_proxy_async();
+      mbar_arrive(&full_a[s]);
+    }
+    const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 12);
+    tc_fence_after();
+    if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
+      const int o = q >> 1, comp = q & 1;
+      double* out = live ? reinterpret_cast<double*>(a.out[o]) : nullptr;
+      for (int c0 = 0; c0 < wk; c0 += 16) {
+        float v[16];
+        tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
+        if (out) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int k = 2 * (c0 + i) + par;
+            if (k < nlm) {
+              const double l = (double)(m + k);
+              const double sc = op.scale ? (m + k > 0 ? 1.0 / (l * (l + 1.0)) : 0.0) : 1.0;
+              out[2 * ((int64_t)(ls + k) * a.ld + a.out_col0 + lev) + comp] = sc * (double)v[i];
+            }
+          }
+        }
+      }
+    }
+  } else if (warp == 4) {
+    if (lane == 0) {
+      const uint8_t* img[2];
+      for (int q = 0; q < 2; ++q) img[q] = st.ana + st.ana_off[(mc * 2 + q) * 2 + par];
+      const uint32_t chunk = 3 * b_plane;
+      int issued = 0;
+      for (int c = 0; c < nch; ++c) {
+        const int s = c % kSplitStages;
+        if (c >= kSplitStages &&
+            !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 13))
+          break;
+        uint8_t* stage = smem + s * L.stage_bytes + 6 * L.a_plane;
+        mbar_expect_tx(&full_b[s], 2 * chunk);
+        for (int q = 0; q < 2; ++q)
+          bulk_g2s(stage + q * 3 * L.b_plane, img[q] + (int64_t)c * chunk, chunk, &full_b[s]);
+        issued = c + 1;
+      }
+      for (int c = max(0, issued - kSplitStages); c < issued; ++c)
+        mbar_wait(&full_b[c % kSplitStages], (c / kSplitStages) & 1, abort_flag, nullptr, 0);
+    }
+  } else {
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16(kSplitRows, wk);
+      uint32_t acc = 0;
+      for (int c = 0; c < nch; ++c) {
+        const int s = c % kSplitStages;
+        const uint32_t ph = (c / kSplitStages) & 1;
+        if (!mbar_wait(&full_a[s], ph, abort_flag, a.err, 14)) break;
+        if (!mbar_wait(&full_b[s], ph, abort_flag, a.err, 15)) break;
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * L.stage_bytes);
+        const uint32_t sb = sa + 6 * L.a_plane;
+        for (int q = 0; q < 2; ++q) {
+#pragma unroll
+          for (int pp = 0; pp < 6; ++pp) {
+            uint64_t da = umma_desc(sa + q * 3 * L.a_plane + kPairA[pp] * L.a_plane, 128, 256);
+            uint64_t db = umma_desc(sb + q * 3 * L.b_plane + kPairB[pp] * b_plane, 128, 256);
+            umma_bf16(tbase, da, db, idesc, acc);
+            acc = 1;
+          }
+        }
+        umma_commit(&empty[s]);
+      }
+      umma_commit(accb);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 4) {
+    tc_fence_after();
+    tmem_dealloc(tbase, tcols);
+  }
+}
+
+int launch_synth_split(const SplitSynArgs& a, cudaStream_t st) {
+  const SplitSmem L(a.s.wth);
+  size_t sm = L.total();
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_synth_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+  dim3 grid((a.nrows + kSplitRows - 1) / kSplitRows, 2 * a.s.nthtile, a.t.n_m);
+  k_synth_split<<<grid, kSplitThreads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st) {
+  const SplitSmem L(a.wk_max);
+  size_t sm = L.total();
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_anal_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+  dim3 grid((a.nrows + kSplitRows - 1) / kSplitRows, 2, a.t.n_m);
+  k_anal_split<<<grid, kSplitThreads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+size_t split_synth_smem(int wth) { return SplitSmem(wth).total(); }
+
+}  // namespace mt

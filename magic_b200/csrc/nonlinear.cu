@@ -135,20 +135,22 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   const int N = t.n_phi, H = N / 2, M = t.n_m;
   const int stride = padded_len(H);
   const int row = blockIdx.x, r = blockIdx.y;
+  cplx<double>* tws = buf + (BF::NB + kFftRowBatch) * stride;
+  fft_twiddles_to_smem(tws, H, t.twiddle);
   for (int i = threadIdx.x; i < NFI * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
   // half spectra of the NFI fields (one real field per buffer row)
   const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
   for (int e = threadIdx.x; e < M * NFI; e += blockDim.x) {
     int k = e / NFI, f = e - k * NFI;
-    double2 X = __ldg(&Fr[k * a.f_m + f]);
-    buf[f * stride + pad16(k)] = {X.x, X.y};
+    cp_async16(&buf[f * stride + pad16(k)], &Fr[k * a.f_m + f]);
   }
+  cp_async_wait_all();
   __syncthreads();
   for (int f = threadIdx.x / 32; f < NFI; f += kNlThreads / 32)
     c2r_prepare_nl(buf + f * stride, H, t.twiddle, threadIdx.x % 32, 32);
   __syncthreads();
-  fft_rows<true>(buf, buf + BF::NB * stride, NFI, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
+  fft_rows<true>(buf, buf + BF::NB * stride, NFI, H, stride, t.fft_radix, t.fft_nstages, tws);
 
   const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
   const double orho1 = a.orho1[r], orho2 = a.orho2[r];
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   if (threadIdx.x == 0) atomic_max_pos(&a.vh2max[r], vmh);
   if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
   __syncthreads();
-  fft_rows<false>(buf, buf + BF::NB * stride, NFO, H, stride, t.fft_radix, t.fft_nstages, t.twiddle, 2);
+  fft_rows<false>(buf, buf + BF::NB * stride, NFO, H, stride, t.fft_radix, t.fft_nstages, tws);
   const double ws = t.wq[row] / N, wv = t.wq_v[row] / N;
   double2* Gr = a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * NFO;
   for (int e = threadIdx.x; e < M * NFO; e += blockDim.x) {
@@ -216,7 +218,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
 template <bool MAG, bool CHEM>
 static int launch_nl_bouss_t(const NlBoussArgs& a, cudaStream_t st) {
   using BF = BoussFields<MAG, CHEM>;
-  size_t sm = (size_t)(BF::NB + kFftRowBatch) * padded_len(a.t.n_phi / 2) * sizeof(double2);
+  size_t sm = ((size_t)(BF::NB + kFftRowBatch) * padded_len(a.t.n_phi / 2) + a.t.n_phi / 2) *
+              sizeof(double2);
   auto kern = k_nl_bouss<MAG, CHEM>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid(a.t.n_theta, a.n_r);

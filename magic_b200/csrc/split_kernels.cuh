@@ -1,0 +1,65 @@
+// Argument blocks of the split-precision stage kernels.
+#pragma once
+
+#include "legendre.cuh"
+#include "split.cuh"
+
+namespace mt {
+
+// One output real component as a linear combination of two scaled sources:
+// value = coef(kP) * src(tP, cP) contracted with P + coef(kD) * src(tD, cD)
+// contracted with dP.  coef codes: 0 zero, 1 +1, 2 -1, 3 +m, 4 -m.
+// cP/cD select the real (0) or imaginary (1) part; scale = 1 divides the
+// analysis result by l(l+1) (0 for l = 0).
+struct RowOp {
+  int8_t tP, cP, kP, tD, cD, kD, scale, pad;
+};
+
+struct SplitSynArgs {
+  Tables t;
+  SplitTables s;
+  TermSrc src[16];
+  int64_t ld;           // row stride of the spectral sources (complex)
+  const double* or2;    // per level, for kCurlT
+  int nrows;            // levels * row_per_level
+  int row_per_level;    // 2 * fields
+  RowOp ops[32];        // per (field, re/im) of a level
+  float* Fs;            // [m][sym|asym][theta pair][row]
+  int64_t fs_m, fs_c, fs_j;
+  int* err;
+};
+
+struct SplitAnaArgs {
+  Tables t;
+  SplitTables s;
+  int wk_max;           // max rows of the analysis table images
+  const float* G;       // [m][north|south][theta pair][level * g_level + 2 field + re/im]
+  int64_t g_m, g_h, g_j, g_level;
+  int nrows, row_per_level;
+  RowOp ops[32];
+  double2* out[16];     // (lm_max, ld) outputs, one per output field
+  int64_t ld;
+  int out_col0;
+  int* err;
+};
+
+int launch_synth_split(const SplitSynArgs& a, cudaStream_t st);
+int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st);
+
+struct NlSplitArgs {
+  Tables t;
+  int n_r;
+  const float* Fs;      // synthesis output (sym/asym), row = level * 2 nfi + 2 f + re/im
+  int64_t fs_m, fs_c, fs_j;
+  float* G;             // products (north/south), row = (level-1) * 2 nfo + 2 f + re/im
+  int64_t g_m, g_h, g_j;
+  const double *or2, *or4, *orho1, *orho2, *delxr2, *delxh2;
+  double LFfac;
+  int cour_mode;
+  double cf2, af2, valfac;
+  unsigned long long *vr2max, *vh2max;
+};
+
+int launch_nl_bouss_split(bool mag, bool chem, const NlSplitArgs& a, cudaStream_t st);
+
+}  // namespace mt
