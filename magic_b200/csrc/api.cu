@@ -581,13 +581,14 @@ static int nl_bouss_t(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt
 
 struct SplitWs {
   size_t err, fs, gs, mx, total;
-  int64_t rows_syn, rows_nl;
+  int64_t rows_syn, rows_nl, g_level;
 };
 
 static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
   SplitWs w;
   w.rows_syn = (int64_t)n_r * 2 * bouss_nfi(mag, chem);
-  w.rows_nl = (int64_t)(n_r - 2) * 2 * bouss_nfo(mag, chem);
+  w.g_level = (2 * bouss_nfo(mag, chem) + 3) & ~3;  // floats per level, 16-byte multiple
+  w.rows_nl = (int64_t)(n_r - 2) * w.g_level;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   w.err = 0;
   w.fs = 256;
@@ -658,24 +659,44 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     SplitSynArgs s{};
     s.t = p->tab;
     s.s = split_tables(p);
+    // source arrays, then terms = recipes over them (step_time.py:980-1013)
+    int na = 0;
+    auto arr = [&](const double* ptr) {
+      s.arr[na] = c(ptr);
+      return na++;
+    };
     int x = 0;
+    auto term = [&](int ia, int ib, int recipe) {
+      s.term[x].ia = (int8_t)ia;
+      s.term[x].ib = (int8_t)ib;
+      s.term[x].recipe = (int8_t)recipe;
+      s.term[x].pad = 0;
+      ++x;
+    };
     if (MAG) {
-      s.src[x++] = {c(in->b), nullptr, kDlh};
-      s.src[x++] = {c(in->db), nullptr, kRaw};
-      s.src[x++] = {c(in->aj), nullptr, kRaw};
-      s.src[x++] = {c(in->aj), nullptr, kDlh};
-      s.src[x++] = {c(in->dj), nullptr, kRaw};
-      s.src[x++] = {c(in->b), c(in->ddb), kCurlT};
+      const int ib = arr(in->b), idb = arr(in->db), iaj = arr(in->aj), idj = arr(in->dj),
+                iddb = arr(in->ddb);
+      term(ib, 0, kDlh);
+      term(idb, 0, kRaw);
+      term(iaj, 0, kRaw);
+      term(iaj, 0, kDlh);
+      term(idj, 0, kRaw);
+      term(ib, iddb, kCurlT);
     }
-    s.src[x++] = {c(in->w), nullptr, kDlh};
-    s.src[x++] = {c(in->dw), nullptr, kRaw};
-    s.src[x++] = {c(in->z), nullptr, kRaw};
-    s.src[x++] = {c(in->z), nullptr, kDlh};
-    s.src[x++] = {c(in->dz), nullptr, kRaw};
-    s.src[x++] = {c(in->w), c(in->ddw), kCurlT};
+    const int iw = arr(in->w), idw = arr(in->dw), iz = arr(in->z), idz = arr(in->dz),
+              iddw = arr(in->ddw), is = arr(in->s);
+    const int ixi = CHEM ? arr(in->xi) : 0;
+    term(iw, 0, kDlh);
+    term(idw, 0, kRaw);
+    term(iz, 0, kRaw);
+    term(iz, 0, kDlh);
+    term(idz, 0, kRaw);
+    term(iw, iddw, kCurlT);
     const int xs = x;
-    s.src[x++] = {c(in->s), nullptr, kRaw};
-    if (CHEM) s.src[x++] = {c(in->xi), nullptr, kRaw};
+    term(is, 0, kRaw);
+    if (CHEM) term(ixi, 0, kRaw);
+    s.narr = na;
+    s.n_lev = n_r;
     const int G = MAG ? 4 : 2;
     for (int g = 0; g < G; ++g) syn_group_ops(&s.ops[6 * g], 3 * g, 3 * g + 1, 3 * g + 2);
     ana_scalar_ops(&s.ops[6 * G], xs);
@@ -684,6 +705,7 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     s.or2 = q->or2;
     s.nrows = (int)W.rows_syn;
     s.row_per_level = 2 * nfi;
+    s.stg_lev = std::min(n_r, 127 / s.row_per_level + 2);
     s.Fs = Fs;
     s.fs_m = fs_m;
     s.fs_c = fs_c;
@@ -704,6 +726,7 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     nl.g_m = g_m;
     nl.g_h = g_h;
     nl.g_j = g_j;
+    nl.g_level = W.g_level;
     nl.or2 = q->or2;
     nl.or4 = q->or4;
     nl.orho1 = q->orho1;
@@ -732,7 +755,8 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
   a.g_m = g_m;
   a.g_h = g_h;
   a.g_j = g_j;
-  a.g_level = 2 * nfo;
+  a.g_level = W.g_level;
+  a.n_lev = n_r - 2;
   int o = 0, r = 0;
   // output fields and their row programs (magic_torch/step_time.py:1066-1124)
   r += ana_scalar_ops(&a.ops[r], 0);
@@ -762,6 +786,7 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
   }
   a.row_per_level = r;
   a.nrows = (n_r - 2) * r;
+  a.stg_lev = std::min(n_r - 2, 127 / r + 2);
   a.ld = out->ld;
   a.out_col0 = 1;
   a.err = err;

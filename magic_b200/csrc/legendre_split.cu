@@ -26,7 +26,7 @@
 
 namespace mt {
 
-constexpr int kSplitStages = 3;
+constexpr int kSplitStages = 2;
 constexpr int kSplitThreads = 192;
 
 // plane pairs (a, b) of the six retained products
@@ -43,11 +43,21 @@ __device__ __forceinline__ double coef_value(int code, double m) {
   }
 }
 
+// Three bf16 planes of a float: hi = bf16(v), mid = bf16(v - hi), lo = v - hi - mid.
+// A float has 24 significant bits, so hi + mid + lo == v exactly (no underflow).
+__device__ __forceinline__ void split3f(float v, __nv_bfloat16& h, __nv_bfloat16& m,
+                                       __nv_bfloat16& l) {
+  h = __float2bfloat16_rn(v);
+  float r = v - __bfloat162float(h);
+  m = __float2bfloat16_rn(r);
+  l = __float2bfloat16_rn(r - __bfloat162float(m));
+}
+
 // Write 16 consecutive K values of one row as 3 planes into an A tile.
-__device__ __forceinline__ void put_row16(uint8_t* tile, int row, const double (&v)[16]) {
+__device__ __forceinline__ void put_row16(uint8_t* tile, int row, const float (&v)[16]) {
   __nv_bfloat16 q[3][16];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) split3(v[i], q[0][i], q[1][i], q[2][i]);
+  for (int i = 0; i < 16; ++i) split3f(v[i], q[0][i], q[1][i], q[2][i]);
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
 #pragma unroll
@@ -62,33 +72,50 @@ __device__ __forceinline__ void put_row16(uint8_t* tile, int row, const double (
   }
 }
 
-__device__ __forceinline__ double term_value(const TermSrc& s, int64_t row, int64_t ld, int col,
-                                             double dlh, const double* or2, int comp) {
-  const double2* pa = s.a + row * ld + col;
-  double2 v = __ldg(pa);
-  double x = comp ? v.y : v.x;
-  switch (s.recipe) {
-    case kRaw: return x;
-    case kDlh: return dlh * x;
-    case kCurlT: {
-      double2 w = __ldg(s.b + row * ld + col);
-      return __ldg(&or2[col]) * dlh * x - (comp ? w.y : w.x);
-    }
-    default: return 0.0;
-  }
+// 16-byte global -> shared copy; src_bytes = 0 zero-fills (no global read).
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// barrier among the 128 producer threads (warps 0-3) only
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+// the same barrier, returning whether `ok` holds in all 128 producer threads
+// (keeps a timeout from splitting the producers between iterations)
+__device__ __forceinline__ bool producers_all(bool ok) {
+  uint32_t r;
+  asm volatile(
+      "{\n.reg .pred p, q;\nsetp.ne.u32 q, %1, 0;\nbar.red.and.pred p, 1, 128, q;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)ok)
+      : "memory");
+  return r != 0;
 }
 
-// Shared memory of one CTA: stages of [A_P | A_dP | B_P | B_dP], then barriers.
+// Shared memory of one CTA: operand stages [A_P | A_dP | B_P | B_dP], two
+// staging buffers for the raw inputs of a K chunk, then barriers.
 struct SplitSmem {
-  uint32_t a_plane, b_plane, stage_bytes, bar_off;
-  __host__ __device__ SplitSmem(int brows) {
+  uint32_t a_plane, b_plane, stage_bytes, stg_off, stg_bytes, bar_off;
+  __host__ __device__ SplitSmem(int brows, uint32_t staging) {
     a_plane = kSplitRows * 32;
     b_plane = brows * 32;
     stage_bytes = 6 * a_plane + 6 * b_plane;
-    bar_off = kSplitStages * stage_bytes;
+    stg_off = kSplitStages * stage_bytes;
+    stg_bytes = (staging + 127) & ~127u;
+    bar_off = stg_off + 2 * stg_bytes;
   }
   __host__ __device__ size_t total() const { return bar_off + 8 * (3 * kSplitStages + 1) + 16; }
 };
+
+__host__ __device__ inline uint32_t syn_staging_bytes(int narr, int stg_lev) {
+  return (uint32_t)narr * 32 * stg_lev * 16;
+}
+__host__ __device__ inline uint32_t ana_staging_bytes(int stg_lev, int g_level) {
+  return (uint32_t)2 * kSplitKC * stg_lev * g_level * 4;
+}
 
 // ------------------------------------------------------------- synthesis
 
@@ -97,7 +124,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a
   const Tables& t = a.t;
   const SplitTables& st = a.s;
   const int wth = st.wth;
-  const SplitSmem L(wth);
+  const SplitSmem L(wth, syn_staging_bytes(a.narr, a.stg_lev));
   uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + L.bar_off);
   uint64_t* full_b = full_a + kSplitStages;
   uint64_t* empty = full_b + kSplitStages;
@@ -138,33 +165,73 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a
 
   if (warp < 4) {
     // ---------------- producer: row tid of this tile ----------------
+    // Chunk c needs l - m in [32 c, 32 c + 32) of every source array at the
+    // tile's levels [lev0, lev0 + nlev): staged with coalesced cp.async one
+    // chunk ahead, then each thread assembles its row from shared memory.
     const int R = rt * kSplitRows + tid;
     const bool live = R < a.nrows;
     const int lev = live ? R / a.row_per_level : 0;
     const int q = live ? R - lev * a.row_per_level : 0;
+    const int lev0 = (rt * kSplitRows) / a.row_per_level;
+    const int nlev = min(a.stg_lev, a.n_lev - lev0);
+    const int lv = lev - lev0;
     const RowOp op = a.ops[q];
+    const TermIx tP = a.term[op.tP], tD = a.term[op.tD];
     const double dm = (double)m;
     const double cP = coef_value(op.kP, dm), cD = coef_value(op.kD, dm);
+    const double or2l = live ? a.or2[lev] : 0.0;
+    auto stg = [&](int b) { return reinterpret_cast<double2*>(smem + L.stg_off + b * L.stg_bytes); };
+    auto issue = [&](int c) {
+      double2* d = stg(c & 1);
+      const int per = 32 * nlev, total = a.narr * per;
+      for (int e = tid; e < total; e += kSplitRows) {
+        const int ia = e / per, rem = e - ia * per;
+        const int kk = rem / nlev, lvv = rem - kk * nlev;
+        const int k = 32 * c + kk;
+        const double2* src = a.arr[ia] + (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
+        cp_async16_zfill(&d[(ia * 32 + kk) * a.stg_lev + lvv], src, k < nlm ? 16u : 0u);
+      }
+      cp_async_commit();
+    };
+    issue(0);
     for (int c = 0; c < nch; ++c) {
       const int s = c % kSplitStages;
-      if (c >= kSplitStages &&
-          !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 1))
-        break;
+      cp_async_wait0();
+      producers_sync();  // chunk c staged; everyone finished reading the other buffer
+      if (c + 1 < nch) issue(c + 1);
+      bool ok = c < kSplitStages ||
+                mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 1);
+      if (!producers_all(ok)) break;
+      const double2* d = stg(c & 1);
       uint8_t* stage = smem + s * L.stage_bytes;
-      double vp[16], vd[16];
+      float vp[16], vd[16];
+      const float fcP = (float)cP, fcD = (float)cD, for2 = (float)or2l;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const int kp = 2 * (kSplitKC * c + i) + par_t[0];
-        const int kd = 2 * (kSplitKC * c + i) + par_t[1];
-        vp[i] = 0.0;
-        vd[i] = 0.0;
-        if (live && op.kP && kp < nlm) {
-          double l = m + kp;
-          vp[i] = cP * term_value(a.src[op.tP], ls + kp, a.ld, lev, l * (l + 1.0), a.or2, op.cP);
+        vp[i] = 0.f;
+        vd[i] = 0.f;
+        const int kkp = 2 * i + par_t[0], kkd = 2 * i + par_t[1];
+        if (live && op.kP && 32 * c + kkp < nlm) {
+          const float l = (float)(m + 32 * c + kkp);
+          const double2 v = d[(tP.ia * 32 + kkp) * a.stg_lev + lv];
+          float x = (float)(op.cP ? v.y : v.x);
+          if (tP.recipe == kDlh) x *= l * (l + 1.f);
+          else if (tP.recipe == kCurlT) {
+            const double2 w = d[(tP.ib * 32 + kkp) * a.stg_lev + lv];
+            x = for2 * l * (l + 1.f) * x - (float)(op.cP ? w.y : w.x);
+          }
+          vp[i] = fcP * x;
         }
-        if (live && op.kD && kd < nlm) {
-          double l = m + kd;
-          vd[i] = cD * term_value(a.src[op.tD], ls + kd, a.ld, lev, l * (l + 1.0), a.or2, op.cD);
+        if (live && op.kD && 32 * c + kkd < nlm) {
+          const float l = (float)(m + 32 * c + kkd);
+          const double2 v = d[(tD.ia * 32 + kkd) * a.stg_lev + lv];
+          float x = (float)(op.cD ? v.y : v.x);
+          if (tD.recipe == kDlh) x *= l * (l + 1.f);
+          else if (tD.recipe == kCurlT) {
+            const double2 w = d[(tD.ib * 32 + kkd) * a.stg_lev + lv];
+            x = for2 * l * (l + 1.f) * x - (float)(op.cD ? w.y : w.x);
+          }
+          vd[i] = fcD * x;
         }
       }
       put_row16(stage, tid, vp);
@@ -172,6 +239,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a
       fence_proxy_async();
       mbar_arrive(&full_a[s]);
     }
+    cp_async_wait0();
     // ---------------- epilogue ----------------
     const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 2);
     tc_fence_after();
@@ -258,7 +326,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a)
   const int rt = blockIdx.x, par = blockIdx.y, mc = blockIdx.z;
   const int wk = st.ana_wk[mc * 2 + par];
   if (wk == 0 || *(volatile int*)a.err) return;
-  const SplitSmem L(a.wk_max);
+  const SplitSmem L(a.wk_max, ana_staging_bytes(a.stg_lev, (int)a.g_level));
   uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + L.bar_off);
   uint64_t* full_b = full_a + kSplitStages;
   uint64_t* empty = full_b + kSplitStages;
@@ -293,33 +361,60 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a)
   const uint32_t tbase = *tmem_slot;
 
   if (warp < 4) {
+    // Chunk c needs theta pairs [16 c, 16 c + 16) of the north and south rows at
+    // the tile's levels: staged with cp.async one chunk ahead.
     const int R = rt * kSplitRows + tid;
     const bool live = R < a.nrows;
     const int lev = live ? R / a.row_per_level : 0;
     const int q = live ? R - lev * a.row_per_level : 0;
+    const int lev0 = (rt * kSplitRows) / a.row_per_level;
+    const int nlev = min(a.stg_lev, a.n_lev - lev0);
+    const int lv = lev - lev0;
     const RowOp op = a.ops[q];
     const double dm = (double)m;
     const double cP = coef_value(op.kP, dm), cD = coef_value(op.kD, dm);
-    const float* g = a.G + (int64_t)mc * a.g_m;
-    const int64_t colP = (int64_t)lev * a.g_level + 2 * op.tP + op.cP;
-    const int64_t colD = (int64_t)lev * a.g_level + 2 * op.tD + op.cD;
-    const double sgP = fold_t[0] ? -1.0 : 1.0, sgD = fold_t[1] ? -1.0 : 1.0;
+    const int gl = (int)a.g_level;
+    const int rowlen = a.stg_lev * gl;  // floats per staged (hemisphere, theta pair) row
+    const int colP = lv * gl + 2 * op.tP + op.cP;
+    const int colD = lv * gl + 2 * op.tD + op.cD;
+    const float sgP = fold_t[0] ? -1.f : 1.f, sgD = fold_t[1] ? -1.f : 1.f;
+    auto stg = [&](int b) { return reinterpret_cast<float*>(smem + L.stg_off + b * L.stg_bytes); };
+    const float* gm = a.G + (int64_t)mc * a.g_m + (int64_t)lev0 * gl;
+    auto issue = [&](int c) {
+      float* d = stg(c & 1);
+      const int cpl = nlev * gl / 4;  // 16-byte pieces per (hemisphere, theta pair)
+      const int total = 2 * kSplitKC * cpl;
+      for (int e = tid; e < total; e += kSplitRows) {
+        const int hj = e / cpl, p4 = e - hj * cpl;
+        const int h = hj / kSplitKC, jl = hj - h * kSplitKC;
+        const int j = kSplitKC * c + jl;
+        const float* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j + 4 * p4;
+        cp_async16_zfill(d + hj * rowlen + 4 * p4, src, j < t.nhs ? 16u : 0u);
+      }
+      cp_async_commit();
+    };
+    issue(0);
     for (int c = 0; c < nch; ++c) {
       const int s = c % kSplitStages;
-      if (c >= kSplitStages &&
-          !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 11))
-        break;
+      cp_async_wait0();
+      producers_sync();
+      if (c + 1 < nch) issue(c + 1);
+      bool ok = c < kSplitStages ||
+                mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 11);
+      if (!producers_all(ok)) break;
+      const float* d = stg(c & 1);
       uint8_t* stage = smem + s * L.stage_bytes;
-      double vp[16], vd[16];
+      float vp[16], vd[16];
+      const float fcP = (float)cP, fcD = (float)cD;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const int j = kSplitKC * c + i;
-        vp[i] = 0.0;
-        vd[i] = 0.0;
-        if (live && j < t.nhs) {
-          const float* gj = g + (int64_t)j * a.g_j;
-          if (op.kP) vp[i] = cP * ((double)__ldg(gj + colP) + sgP * (double)__ldg(gj + a.g_h + colP));
-          if (op.kD) vd[i] = cD * ((double)__ldg(gj + colD) + sgD * (double)__ldg(gj + a.g_h + colD));
+        vp[i] = 0.f;
+        vd[i] = 0.f;
+        if (live) {
+          const float* n = d + i * rowlen;
+          const float* so = d + (kSplitKC + i) * rowlen;
+          if (op.kP) vp[i] = fcP * (n[colP] + sgP * so[colP]);
+          if (op.kD) vd[i] = fcD * (n[colD] + sgD * so[colD]);
         }
       }
       put_row16(stage, tid, vp);
@@ -327,6 +422,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a)
       fence_proxy_async();
       mbar_arrive(&full_a[s]);
     }
+    cp_async_wait0();
     const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 12);
     tc_fence_after();
     if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
@@ -403,7 +499,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a)
 }
 
 int launch_synth_split(const SplitSynArgs& a, cudaStream_t st) {
-  const SplitSmem L(a.s.wth);
+  const SplitSmem L(a.s.wth, syn_staging_bytes(a.narr, a.stg_lev));
   size_t sm = L.total();
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_synth_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
@@ -414,7 +510,7 @@ int launch_synth_split(const SplitSynArgs& a, cudaStream_t st) {
 }
 
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st) {
-  const SplitSmem L(a.wk_max);
+  const SplitSmem L(a.wk_max, ana_staging_bytes(a.stg_lev, (int)a.g_level));
   size_t sm = L.total();
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_anal_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
@@ -424,6 +520,6 @@ int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st) {
   return MT_OK;
 }
 
-size_t split_synth_smem(int wth) { return SplitSmem(wth).total(); }
+
 
 }  // namespace mt

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kNlSplitThreads) k_nl_bouss_split(NlSplitArgs 
   __syncthreads();
   fft_rows<false>(buf, buf + BF::NB * stride, NFO, H, stride, t.fft_radix, t.fft_nstages, tws);
   const float ws = (float)(t.wq[row] / N), wv = (float)(t.wq_v[row] / N);
-  float* Gr = a.G + (int64_t)(row & 1) * a.g_h + (int64_t)j * a.g_j + (int64_t)(r - 1) * 2 * NFO;
+  float* Gr = a.G + (int64_t)(row & 1) * a.g_h + (int64_t)j * a.g_j + (int64_t)(r - 1) * a.g_level;
   for (int e = threadIdx.x; e < M * NFO; e += blockDim.x) {
     int k = e / NFO, o = e - k * NFO;
     const cplx<float>* z = buf + o * stride;

@@ -15,14 +15,23 @@ struct RowOp {
   int8_t tP, cP, kP, tD, cD, kD, scale, pad;
 };
 
+// A synthesis term: recipe (legendre.cuh) applied to source arrays ia, ib.
+struct TermIx {
+  int8_t ia, ib, recipe, pad;
+};
+
 struct SplitSynArgs {
   Tables t;
   SplitTables s;
-  TermSrc src[16];
+  const double2* arr[12];  // spectral source arrays, (lm_max, ld) complex over levels
+  int narr;
+  TermIx term[16];
   int64_t ld;           // row stride of the spectral sources (complex)
   const double* or2;    // per level, for kCurlT
-  int nrows;            // levels * row_per_level
+  int n_lev;            // levels (columns) of the sources
+  int nrows;            // n_lev * row_per_level
   int row_per_level;    // 2 * fields
+  int stg_lev;          // levels one 128-row tile can touch (staging width)
   RowOp ops[32];        // per (field, re/im) of a level
   float* Fs;            // [m][sym|asym][theta pair][row]
   int64_t fs_m, fs_c, fs_j;
@@ -34,7 +43,9 @@ struct SplitAnaArgs {
   SplitTables s;
   int wk_max;           // max rows of the analysis table images
   const float* G;       // [m][north|south][theta pair][level * g_level + 2 field + re/im]
-  int64_t g_m, g_h, g_j, g_level;
+  int64_t g_m, g_h, g_j, g_level;  // g_level: floats per level, multiple of 4
+  int n_lev;            // levels of G
+  int stg_lev;          // levels one 128-row tile can touch
   int nrows, row_per_level;
   RowOp ops[32];
   double2* out[16];     // (lm_max, ld) outputs, one per output field
@@ -51,8 +62,8 @@ struct NlSplitArgs {
   int n_r;
   const float* Fs;      // synthesis output (sym/asym), row = level * 2 nfi + 2 f + re/im
   int64_t fs_m, fs_c, fs_j;
-  float* G;             // products (north/south), row = (level-1) * 2 nfo + 2 f + re/im
-  int64_t g_m, g_h, g_j;
+  float* G;             // products (north/south), row = (level-1) * g_level + 2 f + re/im
+  int64_t g_m, g_h, g_j, g_level;
   const double *or2, *or4, *orho1, *orho2, *delxr2, *delxh2;
   double LFfac;
   int cour_mode;
