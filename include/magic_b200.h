@@ -96,6 +96,24 @@ MT_API size_t mt_transform_workspace(const mt_plan* plan, int B, int n_fields);
 MT_API int mt_scal_to_spat(const mt_plan* plan, const double* Slm, int64_t ld, int B,
                     double* grid, void* work, size_t work_bytes, void* stream);
 
+/* Allocation-free scal_to_spat, for callers that cannot allocate device
+ * memory while they run: a host code linked through this C ABI that budgets
+ * all GPU memory once at start-up, or a process whose device memory is held by
+ * another allocator, cannot hand a fresh cudaMalloc'd workspace to every call.
+ * No counterpart in the reference.  Same inputs, outputs and results as
+ * mt_scal_to_spat, but the workspace is a fixed array of
+ * MT_NOALLOC_SCRATCH_BYTES inside the library: every GPU that loads the
+ * library holds it until the process exits.  B is limited to
+ * n_m_max * n_theta_max * B * 16 <= MT_NOALLOC_SCRATCH_BYTES (about 10
+ * columns at l_max = 255); larger B returns MT_ERR_WORKSPACE before any
+ * launch.  The first call on a device looks up the array's device address
+ * (no allocation); make that first call before any stream capture.  All calls
+ * on a device share the array: calls that can overlap on the GPU (different
+ * streams, different host threads) race and must be serialised by the caller. */
+#define MT_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+MT_API int mt_scal_to_spat_noalloc(const mt_plan* plan, const double* Slm, int64_t ld, int B,
+                                   double* grid, void* stream);
+
 /* scal_to_SH (magic_torch/sht.py:351-405): grid -> Slm (lm_max, ld). */
 MT_API int mt_scal_to_SH(const mt_plan* plan, const double* grid, int B, double* Slm,
                   int64_t ld, void* work, size_t work_bytes, void* stream);

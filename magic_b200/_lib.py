@@ -66,6 +66,7 @@ _PROTOS = {
     "mt_plan_copy_tables": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "mt_transform_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int]),
     "mt_scal_to_spat": (C.c_int, [C.c_void_p, _dp, _i64, C.c_int, _dp, _dp, C.c_size_t, _dp]),
+    "mt_scal_to_spat_noalloc": (C.c_int, [C.c_void_p, _dp, _i64, C.c_int, _dp, _dp]),
     "mt_scal_to_SH": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, _i64, _dp, C.c_size_t, _dp]),
     "mt_torpol_to_spat": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp,
                                     _dp, C.c_size_t, _dp]),

@@ -1,5 +1,6 @@
 // extern "C" entry points (include/magic_b200.h).
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -193,6 +194,50 @@ int mt_scal_to_spat(const mt_plan* p, const double* Slm, int64_t ld, int B, doub
   g.B = B;
   g.out[0] = grid;
   return launch_fourier_to_grid(g, st);
+}
+
+}  // extern "C"
+
+namespace mt {
+
+// Fixed scratch of mt_scal_to_spat_noalloc.  Host code must not pass the
+// symbol itself to a kernel (on the host it names a stand-in, not device
+// memory): its device address is looked up once per device with
+// cudaGetSymbolAddress while that device is current.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MT_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+constexpr int kNoallocMaxDevices = 64;
+static void* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev >= 0 && dev < kNoallocMaxDevices, MT_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    MT_CHECK_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MT_OK;
+}
+
+}  // namespace mt
+
+extern "C" {
+
+int mt_scal_to_spat_noalloc(const mt_plan* p, const double* Slm, int64_t ld, int B, double* grid,
+                            void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(B >= 1, MT_ERR_ARG, "B >= 1 required");
+  const size_t need = mt_transform_workspace(p, B, 1);
+  MT_REQUIRE(need <= MT_NOALLOC_SCRATCH_BYTES, MT_ERR_WORKSPACE,
+             "mt_scal_to_spat_noalloc: B too large for the fixed 16 MiB scratch "
+             "(need n_m_max * n_theta_max * B * 16 bytes); use mt_scal_to_spat with a workspace");
+  void* work = nullptr;
+  MT_TRY(noalloc_scratch(&work));
+  return mt_scal_to_spat(p, Slm, ld, B, grid, work, MT_NOALLOC_SCRATCH_BYTES, stream);
 }
 
 int mt_scal_to_grad_spat(const mt_plan* p, const double* Slm, int64_t ld, int B, int scale_dlh,
