@@ -19,7 +19,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -93,61 +92,80 @@ def synth_inputs(plan, n_r, device, seed=0):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every
+    10 ms while the timed region runs (reads only; nothing is set)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.started = threading.Event()
+        self.nvml = None
+
+    def _handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        self.nvml = pynvml
+        try:
+            idx = torch.cuda._get_nvml_device_index(self.device)
+        except Exception:
+            idx = self.device.index or 0
+        return pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _run(self):
+        try:
+            h = self._handle()
+            nv = self.nvml
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            while True:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     reasons_fn(h)))
+                self.started.set()
+                if self.stop.wait(0.01):
+                    break
+        except Exception as e:  # no NVML: the line says so
+            self.error = repr(e)
+        finally:
+            self.started.set()
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        self.started.wait(10.0)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
+        self.stop.set()
+        self.t.join(10.0)
+        if self.nvml is not None:
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            p = [x.strip() for x in ln.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        load = sorted(sm)[len(sm) // 2:] if len(sm) > 4 else sm
-        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0,
+                    "source": getattr(self, "error", "nvml")}
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS.items()
+                          if r & bit})
+        sm = [c for c, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "source": "nvml, 10 ms"}
+
+
+# DRAM bytes (read + write) of one launch of the phi-stage kernel from an ncu
+# capture of the same kernel at n_r = 17 (profiles/split_stage_kernels_l255_n17_ncu.md),
+# per Fourier row moved (13 fields x n_r in, 9 fields x (n_r - 2) out); traffic grows
+# in proportion to the rows, so the full-size launch is scaled by its row count.
+NCU_PHI_TRAFFIC = {"split": (230.526976e6 + 106.615296e6) / (13 * 17 + 9 * 15)}
 
 
 def measured_peaks():
@@ -291,7 +309,7 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
-    with ClockSampler(dev.index) as clocks:
+    with ClockSampler(dev) as clocks:
         e0.record(stream)
         for _ in range(args.steps):
             step()
@@ -318,41 +336,68 @@ def main():
     torch.cuda.synchronize()
     part_ms = {parts[p]: sum(a.elapsed_time(b) for a, b in ev[p]) / len(ev[p]) for p in parts}
 
-    # --- end to end through the public API with pinned host buffers
+    # --- end to end through the public API with pinned host buffers: every
+    # step copies its 11 input spectra host->device and its 8 output spectra and
+    # the Courant steps device->host; copies of neighbouring steps overlap the
+    # stage on separate streams (double-buffered device inputs and outputs).
     if args.no_e2e:
         if rank == 0:
             print(json.dumps({"levels": n_r, "ms_per_step": ms, "kernel_ms": part_ms}), flush=True)
         return
     host_in = {k: v.cpu().pin_memory() for k, v in fields.items()}
-    host_out = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in out.items()}
-    host_dt = torch.empty(2, n_r, dtype=torch.float64).pin_memory()
-    dev_in = {k: torch.empty_like(v) for k, v in fields.items()}
+    dev_in = [{k: torch.empty_like(v) for k, v in fields.items()} for _ in range(2)]
+    dev_out = [{k: torch.zeros_like(v) for k, v in out.items()} for _ in range(2)]
+    host_out = [{k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in out.items()}
+                for _ in range(2)]
+    host_dt = [torch.empty(2, n_r, dtype=torch.float64).pin_memory() for _ in range(2)]
     h2d = sum(v.numel() * v.element_size() for v in host_in.values())
-    d2h = sum(v.numel() * v.element_size() for v in host_out.values()) + host_dt.numel() * 8
+    d2h = sum(v.numel() * v.element_size() for v in host_out[0].values()) + host_dt[0].numel() * 8
+    s_in = torch.cuda.Stream(dev)
+    s_out = torch.cuda.Stream(dev)
+    ev = lambda: torch.cuda.Event()
+    used = [ev(), ev()]      # stage of buffer b finished (inputs free, outputs ready)
+    copied = [ev(), ev()]    # inputs of buffer b on the device
+    drained = [ev(), ev()]   # outputs of buffer b on the host
+    for b in range(2):
+        used[b].record(stream)
+        drained[b].record(stream)
 
-    def e2e_step():
-        for k in FIELDS:
-            dev_in[k].copy_(host_in[k], non_blocking=True)
-        o, dtr, dth = plan.nl_bouss(dev_in, prof, LF, CF, AF, OPM, l_mag=True, out=out, work=work)
-        for k in OUTS:
-            host_out[k].copy_(o[k], non_blocking=True)
-        host_dt[0].copy_(dtr, non_blocking=True)
-        host_dt[1].copy_(dth, non_blocking=True)
+    def e2e_step(i):
+        b = i % 2
+        with torch.cuda.stream(s_in):
+            s_in.wait_event(used[b])
+            for k in FIELDS:
+                dev_in[b][k].copy_(host_in[k], non_blocking=True)
+            copied[b].record(s_in)
+        stream.wait_event(copied[b])
+        stream.wait_event(drained[b])
+        o, dtr, dth = plan.nl_bouss(dev_in[b], prof, LF, CF, AF, OPM, l_mag=True, out=dev_out[b],
+                                    work=work)
+        used[b].record(stream)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(used[b])
+            for k in OUTS:
+                host_out[b][k].copy_(o[k], non_blocking=True)
+            host_dt[b][0].copy_(dtr, non_blocking=True)
+            host_dt[b][1].copy_(dth, non_blocking=True)
+            drained[b].record(s_out)
 
-    for _ in range(2):
-        e2e_step()
+    for i in range(2):
+        e2e_step(i)
     torch.cuda.synchronize()
     k_e2e = max(3, args.steps // 2)
     barrier()
     torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(k_e2e):
-        e2e_step()
-    b.record(stream)
+    a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a_ev.record(stream)
+    for i in range(k_e2e):
+        e2e_step(i)
+    stream.wait_event(drained[(k_e2e - 1) % 2])
+    stream.wait_event(drained[k_e2e % 2])
+    b_ev.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = a.elapsed_time(b) / k_e2e
+    e2e_ms = a_ev.elapsed_time(b_ev) / k_e2e
     if dist is not None:
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -372,9 +417,12 @@ def main():
         row = plan.n_theta_max * plan.n_m_max * (8 if split else 16)
         byts = (13 * n_r + 9 * (n_r - 2)) * row
         ach = byts / (part_ms[dom] * 1e-3) / 1e9
+        per_row = NCU_PHI_TRAFFIC.get(args.precision)
+        traffic = per_row * (13 * n_r + 9 * (n_r - 2)) if per_row else None
         roof = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": ach / peaks["hbm_gbs"], "traffic": None, "kernel": dom,
-                "peak_source": src}
+                "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "algorithmic_bytes": byts,
+                "kernel": dom, "peak_source": src,
+                "traffic_source": "ncu dram bytes at n_r=17 scaled by rows" if per_row else None}
     elif split:
         s_mma, a_mma = split_mma_flops(plan, n_r)
         fl = s_mma if dom == "legendre_synthesis" else a_mma

@@ -48,10 +48,22 @@ struct SplitTables {
   const uint8_t* ana;
   const int64_t* ana_off;  // (n_m * 2 * 2) byte offsets
   const int* ana_wk;       // (n_m * 2) row count (k of that parity) padded to 16
+  // synthesis A-operand images: K chunks of (m, combo) = max over the two
+  // tables; prefix sums over (m, combo) in that order ((n_m * 2 + 1) entries)
+  const int* syn_nch;
+  const int* syn_chunk_prefix;
 };
 
 __host__ __device__ inline int split_nk(int nlm, int parity) { return (nlm + 1 - parity) / 2; }
 __host__ __device__ inline int round16(int n) { return (n + 15) & ~15; }
+
+// K chunks of the synthesis CTA (m, combo): P over l - m of parity combo and
+// dP over the other parity, 16 values of each per chunk.
+__host__ __device__ inline int syn_nchunks(int nlm, int combo) {
+  const int a = (split_nk(nlm, combo) + 15) / 16, b = (split_nk(nlm, 1 - combo) + 15) / 16;
+  return a > b ? a : b;
+}
+
 
 int build_split_tables(mt_plan* p);
 void free_split_tables(mt_plan* p);

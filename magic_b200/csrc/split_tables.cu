@@ -72,9 +72,9 @@ struct SplitStore {
   SplitTables t;
   uint8_t *syn = nullptr, *ana = nullptr;
   int64_t *syn_off = nullptr, *ana_off = nullptr;
-  int* ana_wk = nullptr;
+  int *ana_wk = nullptr, *syn_nch = nullptr, *syn_prefix = nullptr;
   std::vector<int64_t> h_syn_off, h_ana_off;
-  std::vector<int> h_wk;
+  std::vector<int> h_wk, h_syn_nch, h_syn_prefix;
 };
 
 int build_split_tables(mt_plan* p) {
@@ -115,11 +115,28 @@ int build_split_tables(mt_plan* p) {
       }
   }
   int64_t ana_bytes = pos;
+  S->h_syn_nch.resize((size_t)nm * 2);
+  S->h_syn_prefix.resize((size_t)nm * 2 + 1);
+  int acc = 0;
+  for (int mc = 0; mc < nm; ++mc)
+    for (int combo = 0; combo < 2; ++combo) {
+      int n = syn_nchunks(p->l_max - mc * p->minc + 1, combo);
+      S->h_syn_nch[mc * 2 + combo] = n;
+      S->h_syn_prefix[mc * 2 + combo] = acc;
+      acc += n;
+    }
+  S->h_syn_prefix[(size_t)nm * 2] = acc;
   MT_CHECK_CUDA(cudaMalloc(&S->syn, syn_bytes > 0 ? syn_bytes : 16));
   MT_CHECK_CUDA(cudaMalloc(&S->ana, ana_bytes > 0 ? ana_bytes : 16));
   MT_CHECK_CUDA(cudaMalloc(&S->syn_off, S->h_syn_off.size() * sizeof(int64_t)));
   MT_CHECK_CUDA(cudaMalloc(&S->ana_off, S->h_ana_off.size() * sizeof(int64_t)));
   MT_CHECK_CUDA(cudaMalloc(&S->ana_wk, S->h_wk.size() * sizeof(int)));
+  MT_CHECK_CUDA(cudaMalloc(&S->syn_nch, S->h_syn_nch.size() * sizeof(int)));
+  MT_CHECK_CUDA(cudaMalloc(&S->syn_prefix, S->h_syn_prefix.size() * sizeof(int)));
+  MT_CHECK_CUDA(cudaMemcpy(S->syn_nch, S->h_syn_nch.data(), S->h_syn_nch.size() * sizeof(int),
+                           cudaMemcpyHostToDevice));
+  MT_CHECK_CUDA(cudaMemcpy(S->syn_prefix, S->h_syn_prefix.data(),
+                           S->h_syn_prefix.size() * sizeof(int), cudaMemcpyHostToDevice));
   MT_CHECK_CUDA(cudaMemcpy(S->syn_off, S->h_syn_off.data(), S->h_syn_off.size() * sizeof(int64_t),
                            cudaMemcpyHostToDevice));
   MT_CHECK_CUDA(cudaMemcpy(S->ana_off, S->h_ana_off.data(), S->h_ana_off.size() * sizeof(int64_t),
@@ -137,13 +154,15 @@ int build_split_tables(mt_plan* p) {
   S->t.ana = S->ana;
   S->t.ana_off = S->ana_off;
   S->t.ana_wk = S->ana_wk;
+  S->t.syn_nch = S->syn_nch;
+  S->t.syn_chunk_prefix = S->syn_prefix;
   return MT_OK;
 }
 
 void free_split_tables(mt_plan* p) {
   SplitStore* S = (SplitStore*)p->split;
   if (!S) return;
-  void* ptrs[] = {S->syn, S->ana, S->syn_off, S->ana_off, S->ana_wk};
+  void* ptrs[] = {S->syn, S->ana, S->syn_off, S->ana_off, S->ana_wk, S->syn_nch, S->syn_prefix};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete S;
@@ -155,5 +174,8 @@ const std::vector<int64_t>& split_syn_off_host(const mt_plan* p) {
   return ((SplitStore*)p->split)->h_syn_off;
 }
 const std::vector<int>& split_wk_host(const mt_plan* p) { return ((SplitStore*)p->split)->h_wk; }
+int split_syn_total_chunks(const mt_plan* p) {
+  return ((SplitStore*)p->split)->h_syn_prefix.back();
+}
 
 }  // namespace mt
