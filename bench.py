@@ -453,7 +453,7 @@ def main():
                 "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
-                "gpu_launches": (4 if split else 6) * args.steps,
+                "gpu_launches": (5 if split else 6) * args.steps,
                 "kernel_ms": part_ms, "sht_tflops": sht_tflops,
                 "roofline": roof}
         if world == 1 and not args.no_cpu:

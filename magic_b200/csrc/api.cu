@@ -22,6 +22,7 @@ int launch_anal_f64(const AnalArgs<OP::NX, OP::NO>& a, cudaStream_t st);
 // split_tables.cu
 const SplitTables& split_tables(const mt_plan* p);
 const std::vector<int>& split_wk_host(const mt_plan* p);
+int split_syn_total_chunks(const mt_plan* p);
 
 static int prime_decomposition(int n) {
   // smallest 2^i 3^j 5^k >= n, i < 13, j < 7, k < 7 (magic_torch/params.py:12-24)
@@ -625,7 +626,7 @@ static int nl_bouss_t(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt
 // ---- split-precision fused stage ------------------------------------------
 
 struct SplitWs {
-  size_t err, fs, gs, mx, total;
+  size_t err, fs, gs, mx, aimg, total;
   int64_t rows_syn, rows_nl, g_level;
 };
 
@@ -639,7 +640,8 @@ static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
   w.fs = 256;
   w.gs = w.fs + al((size_t)p->n_m * 2 * p->nhs * w.rows_syn * sizeof(float));
   w.mx = w.gs + al((size_t)p->n_m * 2 * p->nhs * w.rows_nl * sizeof(float));
-  w.total = w.mx + al(2 * (size_t)n_r * sizeof(unsigned long long));
+  w.aimg = w.mx + al(2 * (size_t)n_r * sizeof(unsigned long long));
+  w.total = w.aimg + al(synth_split_image_bytes((int)w.rows_syn, split_syn_total_chunks(p)));
   return w;
 }
 
@@ -755,6 +757,8 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     s.fs_m = fs_m;
     s.fs_c = fs_c;
     s.fs_j = fs_j;
+    s.aimg = (uint8_t*)(w + W.aimg);
+    s.total_chunks = split_syn_total_chunks(p);
     s.err = err;
     MT_TRY(launch_synth_split(s, st));
   }

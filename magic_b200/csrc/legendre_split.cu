@@ -14,9 +14,12 @@
 // output parity p reads the folded Fourier data north + south (P rows of even
 // parity, dP rows of odd) or north - south (the other two cases).
 //
-// Warp roles (192 threads): warps 0-3 build the A tiles (bf16x3 split in
-// registers, written in the canonical core-matrix layout) and run the
-// epilogue (tcgen05.ld, one TMEM lane per thread); warp 4 owns TMEM and
+// Synthesis: a packing kernel writes the A operand as pre-split bf16x3 images,
+// then a 4-warp GEMM kernel bulk-copies A and table chunks into a 3-stage
+// ring and issues the plane products (two CTAs per SM).
+// Analysis warp roles (192 threads): warps 0-3 build the A tiles (bf16x3
+// split in registers, written in the canonical core-matrix layout) and run
+// the epilogue (tcgen05.ld, one TMEM lane per thread); warp 4 owns TMEM and
 // bulk-copies the pre-split table chunks; warp 5 lane 0 issues tcgen05.mma
 // (6 plane products per table per chunk) and commits to the stage barriers.
 #include "legendre.cuh"
@@ -118,17 +121,115 @@ __host__ __device__ inline uint32_t ana_staging_bytes(int stg_lev, int g_level) 
 }
 
 // ------------------------------------------------------------- synthesis
+//
+// Two kernels.  k_syn_pack builds the A operand: block (tile rt, chunk c, m)
+// stages l - m in [32 c, 32 c + 32) of every source array at the tile's
+// levels, assembles the rows of the four (table, parity) chunks and writes
+// them as bf16x3 planes in the canonical layout (an image chunk is
+// 3 planes x 128 rows x 16 K = 12 KiB).  Image order per (rt, m, combo):
+// chunk c, then table (P, dP), so one K step reads one contiguous chunk.
+// k_synth_gemm is then a pure bulk-copy-fed tcgen05 GEMM.
 
-__global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a) {
+constexpr int kPackThreads = 256;
+constexpr uint32_t kImgPlane = kSplitRows * 32;  // one bf16 plane of a 128 x 16 chunk
+constexpr uint32_t kImgChunk = 3 * kImgPlane;
+
+__host__ __device__ inline int64_t syn_img_chunk(int64_t total_chunks, int rt, int prefix, int c,
+                                                 int q) {
+  return (((int64_t)rt * total_chunks + prefix + c) * 2 + q);
+}
+
+__global__ void __launch_bounds__(kPackThreads, 4) k_syn_pack(SplitSynArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const Tables& t = a.t;
+  const int rt = blockIdx.x, c = blockIdx.y, mc = blockIdx.z;
+  const int m = mc * t.minc;
+  const int nlm = t.l_max - m + 1;
+  if (c >= syn_nchunks(nlm, 0)) return;
+  const int ls = t.lstart[mc];
+  const int tid = threadIdx.x;
+  const int lev0 = (rt * kSplitRows) / a.row_per_level;
+  const int nlev = min(a.stg_lev, a.n_lev - lev0);
+  double2* d = reinterpret_cast<double2*>(smem);
+  {
+    const int per = 32 * nlev, total = a.narr * per;
+    for (int e = tid; e < total; e += kPackThreads) {
+      const int ia = e / per, rem = e - ia * per;
+      const int kk = rem / nlev, lvv = rem - kk * nlev;
+      const int k = 32 * c + kk;
+      const double2* src = a.arr[ia] + (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
+      cp_async16_zfill(&d[(ia * 32 + kk) * a.stg_lev + lvv], src, k < nlm ? 16u : 0u);
+    }
+    cp_async_commit();
+    cp_async_wait0();
+    __syncthreads();
+  }
+#pragma unroll 1
+  for (int task = tid; task < 4 * kSplitRows; task += kPackThreads) {
+    const int qp = task / kSplitRows, row = task % kSplitRows;
+    const int q = qp >> 1, p = qp & 1;  // table (0 P, 1 dP), parity of l - m
+    const int R = rt * kSplitRows + row;
+    const bool live = R < a.nrows;
+    const int lev = live ? R / a.row_per_level : lev0;
+    const int qf = live ? R - lev * a.row_per_level : 0;
+    const int lv = lev - lev0;
+    const RowOp op = a.ops[qf];
+    const int code = q ? op.kD : op.kP;
+    const int cpart = q ? op.cD : op.cP;
+    const TermIx tm = a.term[q ? op.tD : op.tP];
+    const float f = (float)coef_value(code, (double)m);
+    const float or2l = live ? (float)a.or2[lev] : 0.f;
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int kk = 2 * i + p;
+      v[i] = 0.f;
+      if (live && code && 32 * c + kk < nlm) {
+        const float l = (float)(m + 32 * c + kk);
+        const double2 x2 = d[(tm.ia * 32 + kk) * a.stg_lev + lv];
+        float x = (float)(cpart ? x2.y : x2.x);
+        if (tm.recipe == kDlh) x *= l * (l + 1.f);
+        else if (tm.recipe == kCurlT) {
+          const double2 w = d[(tm.ib * 32 + kk) * a.stg_lev + lv];
+          x = or2l * l * (l + 1.f) * x - (float)(cpart ? w.y : w.x);
+        }
+        v[i] = f * x;
+      }
+    }
+    const int combo = q == 0 ? p : 1 - p;
+    uint8_t* dst = a.aimg + syn_img_chunk(a.total_chunks, rt, a.s.syn_chunk_prefix[mc * 2 + combo],
+                                          c, q) * kImgChunk;
+    put_row16(dst, row, v);
+  }
+}
+
+constexpr int kGemmStages = 3;
+constexpr int kGemmThreads = 128;
+
+// Shared memory of one GEMM CTA: stages of [A chunk | B chunk], then barriers.
+struct GemmSmem {
+  uint32_t b_plane, stage_bytes, bar_off;
+  __host__ __device__ explicit GemmSmem(int brows)
+      : b_plane((uint32_t)brows * 32),
+        stage_bytes(kImgChunk + 3 * (uint32_t)brows * 32),
+        bar_off(kGemmStages * (kImgChunk + 3 * (uint32_t)brows * 32)) {}
+  __host__ __device__ size_t total() const { return bar_off + 8 * (2 * kGemmStages + 1) + 16; }
+};
+
+// Warp 0 lane 0 bulk-copies the A image chunk and the table chunk of each K
+// step, warp 1 lane 0 issues the six plane products per step, warp 2 owns
+// TMEM; all four warps run the epilogue (one TMEM lane = one output row per
+// thread).  K steps: chunk c of the P table (parity combo), then chunk c of
+// the dP table (the other parity), skipping chunks a table does not have.
+__global__ void __launch_bounds__(kGemmThreads, 2) k_synth_gemm(SplitSynArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   const Tables& t = a.t;
   const SplitTables& st = a.s;
   const int wth = st.wth;
-  const SplitSmem L(wth, syn_staging_bytes(a.narr, a.stg_lev));
-  uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + L.bar_off);
-  uint64_t* full_b = full_a + kSplitStages;
-  uint64_t* empty = full_b + kSplitStages;
-  uint64_t* accb = empty + kSplitStages;
+  const GemmSmem L(wth);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* empty = full + kGemmStages;
+  uint64_t* accb = empty + kGemmStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -140,7 +241,6 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a
   const int mc = blockIdx.z;
   const int m = mc * t.minc;
   const int nlm = t.l_max - m + 1;
-  const int ls = t.lstart[mc];
   const int par_t[2] = {combo, 1 - combo};  // parity of l - m contracted with P, dP
   int nch_t[2];
   for (int q = 0; q < 2; ++q) nch_t[q] = (split_nk(nlm, par_t[q]) + kSplitKC - 1) / kSplitKC;
@@ -148,170 +248,102 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_synth_split(SplitSynArgs a
   const uint32_t tcols = wth <= 32 ? 32 : (wth <= 64 ? 64 : (wth <= 128 ? 128 : 256));
 
   if (tid == 0) {
-    for (int s = 0; s < kSplitStages; ++s) {
-      mbar_init(&full_a[s], kSplitRows);
-      mbar_init(&full_b[s], 1);
+    for (int s = 0; s < kGemmStages; ++s) {
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     mbar_init(accb, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 4) tmem_alloc(tmem_slot, tcols);
+  if (warp == 2) tmem_alloc(tmem_slot, tcols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
 
-  if (warp < 4) {
-    // ---------------- producer: row tid of this tile ----------------
-    // Chunk c needs l - m in [32 c, 32 c + 32) of every source array at the
-    // tile's levels [lev0, lev0 + nlev): staged with coalesced cp.async one
-    // chunk ahead, then each thread assembles its row from shared memory.
-    const int R = rt * kSplitRows + tid;
-    const bool live = R < a.nrows;
-    const int lev = live ? R / a.row_per_level : 0;
-    const int q = live ? R - lev * a.row_per_level : 0;
-    const int lev0 = (rt * kSplitRows) / a.row_per_level;
-    const int nlev = min(a.stg_lev, a.n_lev - lev0);
-    const int lv = lev - lev0;
-    const RowOp op = a.ops[q];
-    const TermIx tP = a.term[op.tP], tD = a.term[op.tD];
-    const double dm = (double)m;
-    const double cP = coef_value(op.kP, dm), cD = coef_value(op.kD, dm);
-    const double or2l = live ? a.or2[lev] : 0.0;
-    auto stg = [&](int b) { return reinterpret_cast<double2*>(smem + L.stg_off + b * L.stg_bytes); };
-    auto issue = [&](int c) {
-      double2* d = stg(c & 1);
-      const int per = 32 * nlev, total = a.narr * per;
-      for (int e = tid; e < total; e += kSplitRows) {
-        const int ia = e / per, rem = e - ia * per;
-        const int kk = rem / nlev, lvv = rem - kk * nlev;
-        const int k = 32 * c + kk;
-        const double2* src = a.arr[ia] + (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
-        cp_async16_zfill(&d[(ia * 32 + kk) * a.stg_lev + lvv], src, k < nlm ? 16u : 0u);
-      }
-      cp_async_commit();
-    };
-    issue(0);
-    for (int c = 0; c < nch; ++c) {
-      const int s = c % kSplitStages;
-      cp_async_wait0();
-      producers_sync();  // chunk c staged; everyone finished reading the other buffer
-      if (c + 1 < nch) issue(c + 1);
-      bool ok = c < kSplitStages ||
-                mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 1);
-      if (!producers_all(ok)) break;
-      const double2* d = stg(c & 1);
-      uint8_t* stage = smem + s * L.stage_bytes;
-      float vp[16], vd[16];
-      const float fcP = (float)cP, fcD = (float)cD, for2 = (float)or2l;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        vp[i] = 0.f;
-        vd[i] = 0.f;
-        const int kkp = 2 * i + par_t[0], kkd = 2 * i + par_t[1];
-        if (live && op.kP && 32 * c + kkp < nlm) {
-          const float l = (float)(m + 32 * c + kkp);
-          const double2 v = d[(tP.ia * 32 + kkp) * a.stg_lev + lv];
-          float x = (float)(op.cP ? v.y : v.x);
-          if (tP.recipe == kDlh) x *= l * (l + 1.f);
-          else if (tP.recipe == kCurlT) {
-            const double2 w = d[(tP.ib * 32 + kkp) * a.stg_lev + lv];
-            x = for2 * l * (l + 1.f) * x - (float)(op.cP ? w.y : w.x);
-          }
-          vp[i] = fcP * x;
-        }
-        if (live && op.kD && 32 * c + kkd < nlm) {
-          const float l = (float)(m + 32 * c + kkd);
-          const double2 v = d[(tD.ia * 32 + kkd) * a.stg_lev + lv];
-          float x = (float)(op.cD ? v.y : v.x);
-          if (tD.recipe == kDlh) x *= l * (l + 1.f);
-          else if (tD.recipe == kCurlT) {
-            const double2 w = d[(tD.ib * 32 + kkd) * a.stg_lev + lv];
-            x = for2 * l * (l + 1.f) * x - (float)(op.cD ? w.y : w.x);
-          }
-          vd[i] = fcD * x;
-        }
-      }
-      put_row16(stage, tid, vp);
-      put_row16(stage + 3 * L.a_plane, tid, vd);
-      fence_proxy_async();
-      mbar_arrive(&full_a[s]);
-    }
-    cp_async_wait0();
-    // ---------------- epilogue ----------------
-    const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 2);
-    tc_fence_after();
-    if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
-      float* out = a.Fs + (int64_t)mc * a.fs_m + (int64_t)combo * a.fs_c;
-      for (int c0 = 0; c0 < wth; c0 += 16) {
-        float v[16];
-        tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
-        if (live) {
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int th = tau * wth + c0 + i;
-            if (th < t.nhs) out[(int64_t)th * a.fs_j + R] = v[i];
-          }
-        }
-      }
-    }
-  } else if (warp == 4) {
-    // ---------------- table loader ----------------
-    if (lane == 0) {
-      const uint8_t* img[2];
-      for (int q = 0; q < 2; ++q)
-        img[q] = st.syn + st.syn_off[((mc * 2 + q) * 2 + par_t[q]) * st.nthtile + tau];
-      const uint32_t chunk = 3 * L.b_plane;
-      int issued = 0;
-      for (int c = 0; c < nch; ++c) {
-        const int s = c % kSplitStages;
-        if (c >= kSplitStages &&
-            !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 3))
+  if (warp == 0 && lane == 0) {
+    // ---------------- loader ----------------
+    const uint8_t* aimg =
+        a.aimg + syn_img_chunk(a.total_chunks, rt, st.syn_chunk_prefix[mc * 2 + combo], 0, 0) *
+                     kImgChunk;
+    const uint8_t* img[2];
+    for (int q = 0; q < 2; ++q)
+      img[q] = st.syn + st.syn_off[((mc * 2 + q) * 2 + par_t[q]) * st.nthtile + tau];
+    const uint32_t bchunk = 3 * L.b_plane;
+    int step = 0;
+    bool ok = true;
+    for (int c = 0; c < nch && ok; ++c) {
+      for (int q = 0; q < 2; ++q) {
+        if (c >= nch_t[q]) continue;
+        const int s = step % kGemmStages;
+        if (step >= kGemmStages &&
+            !mbar_wait(&empty[s], ((step / kGemmStages) - 1) & 1, abort_flag, a.err, 3)) {
+          ok = false;
           break;
-        uint8_t* stage = smem + s * L.stage_bytes + 6 * L.a_plane;
-        uint32_t bytes = (c < nch_t[0] ? chunk : 0) + (c < nch_t[1] ? chunk : 0);
-        mbar_expect_tx(&full_b[s], bytes);
-        for (int q = 0; q < 2; ++q)
-          if (c < nch_t[q]) bulk_g2s(stage + q * chunk, img[q] + (int64_t)c * chunk, chunk, &full_b[s]);
-        issued = c + 1;
+        }
+        uint8_t* stage = smem + s * L.stage_bytes;
+        mbar_expect_tx(&full[s], kImgChunk + bchunk);
+        bulk_g2s(stage, aimg + (int64_t)(2 * c + q) * kImgChunk, kImgChunk, &full[s]);
+        bulk_g2s(stage + kImgChunk, img[q] + (int64_t)c * bchunk, bchunk, &full[s]);
+        ++step;
       }
-      // drain: every issued copy must land before the CTA may exit
-      for (int c = max(0, issued - kSplitStages); c < issued; ++c)
-        mbar_wait(&full_b[c % kSplitStages], (c / kSplitStages) & 1, abort_flag, nullptr, 0);
     }
-  } else {
+    // drain: every issued copy must land before the CTA may exit
+    for (int k = max(0, step - kGemmStages); k < step; ++k)
+      mbar_wait(&full[k % kGemmStages], (k / kGemmStages) & 1, abort_flag, nullptr, 0);
+  } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
-    if (lane == 0) {
-      const uint32_t idesc = umma_idesc_bf16(kSplitRows, wth);
-      uint32_t acc = 0;
-      for (int c = 0; c < nch; ++c) {
-        const int s = c % kSplitStages;
-        const uint32_t ph = (c / kSplitStages) & 1;
-        if (!mbar_wait(&full_a[s], ph, abort_flag, a.err, 4)) break;
-        if (!mbar_wait(&full_b[s], ph, abort_flag, a.err, 5)) break;
+    const uint32_t idesc = umma_idesc_bf16(kSplitRows, wth);
+    uint32_t acc = 0;
+    int step = 0;
+    bool ok = true;
+    for (int c = 0; c < nch && ok; ++c) {
+      for (int q = 0; q < 2; ++q) {
+        if (c >= nch_t[q]) continue;
+        const int s = step % kGemmStages;
+        if (!mbar_wait(&full[s], (step / kGemmStages) & 1, abort_flag, a.err, 4)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
         const uint32_t sa = smem_u32(smem + s * L.stage_bytes);
-        const uint32_t sb = sa + 6 * L.a_plane;
-        for (int q = 0; q < 2; ++q) {
-          if (c >= nch_t[q]) continue;
+        const uint32_t sb = sa + kImgChunk;
 #pragma unroll
-          for (int pp = 0; pp < 6; ++pp) {
-            uint64_t da = umma_desc(sa + q * 3 * L.a_plane + kPairA[pp] * L.a_plane, 128, 256);
-            uint64_t db = umma_desc(sb + q * 3 * L.b_plane + kPairB[pp] * L.b_plane, 128, 256);
-            umma_bf16(tbase, da, db, idesc, acc);
-            acc = 1;
-          }
+        for (int pp = 0; pp < 6; ++pp) {
+          const uint64_t da = umma_desc(sa + kPairA[pp] * kImgPlane, 128, 256);
+          const uint64_t db = umma_desc(sb + kPairB[pp] * L.b_plane, 128, 256);
+          umma_bf16(tbase, da, db, idesc, acc);
+          acc = 1;
         }
         umma_commit(&empty[s]);
+        ++step;
       }
-      umma_commit(accb);  // also on abort: lets the epilogue wait finish after in-flight MMAs
+    }
+    umma_commit(accb);  // also on abort: lets the epilogue wait finish after in-flight MMAs
+  }
+  __syncwarp();
+  // ---------------- epilogue ----------------
+  const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 2);
+  tc_fence_after();
+  if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
+    const int R = rt * kSplitRows + tid;
+    float* out = a.Fs + (int64_t)mc * a.fs_m + (int64_t)combo * a.fs_c;
+    for (int c0 = 0; c0 < wth; c0 += 16) {
+      float v[16];
+      tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
+      if (R < a.nrows) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int th = tau * wth + c0 + i;
+          if (th < t.nhs) out[(int64_t)th * a.fs_j + R] = v[i];
+        }
+      }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 4) {
+  if (warp == 2) {
     tc_fence_after();
     tmem_dealloc(tbase, tcols);
   }
@@ -499,14 +531,25 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a)
 }
 
 int launch_synth_split(const SplitSynArgs& a, cudaStream_t st) {
-  const SplitSmem L(a.s.wth, syn_staging_bytes(a.narr, a.stg_lev));
-  size_t sm = L.total();
-  MT_CHECK_CUDA(cudaFuncSetAttribute(k_synth_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const int ntiles = (a.nrows + kSplitRows - 1) / kSplitRows;
+  const size_t pack_sm = syn_staging_bytes(a.narr, a.stg_lev);
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_syn_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pack_sm));
+  dim3 pgrid(ntiles, syn_nchunks(a.t.l_max + 1, 0), a.t.n_m);
+  k_syn_pack<<<pgrid, kPackThreads, pack_sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  const GemmSmem L(a.s.wth);
+  const size_t sm = L.total();
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_synth_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-  dim3 grid((a.nrows + kSplitRows - 1) / kSplitRows, 2 * a.s.nthtile, a.t.n_m);
-  k_synth_split<<<grid, kSplitThreads, sm, st>>>(a);
+  dim3 grid(ntiles, 2 * a.s.nthtile, a.t.n_m);
+  k_synth_gemm<<<grid, kGemmThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
+}
+
+size_t synth_split_image_bytes(int nrows, int64_t total_chunks) {
+  return (size_t)((nrows + kSplitRows - 1) / kSplitRows) * (size_t)total_chunks * 2 * kImgChunk;
 }
 
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st) {

@@ -35,6 +35,8 @@ struct SplitSynArgs {
   RowOp ops[32];        // per (field, re/im) of a level
   float* Fs;            // [m][sym|asym][theta pair][row]
   int64_t fs_m, fs_c, fs_j;
+  uint8_t* aimg;        // A-operand images (workspace), synth_split_image_bytes
+  int64_t total_chunks; // K chunks summed over (m, combo)
   int* err;
 };
 
@@ -55,6 +57,7 @@ struct SplitAnaArgs {
 };
 
 int launch_synth_split(const SplitSynArgs& a, cudaStream_t st);
+size_t synth_split_image_bytes(int nrows, int64_t total_chunks);
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st);
 
 struct NlSplitArgs {
