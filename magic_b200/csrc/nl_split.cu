@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "fft.cuh"
+#include "fft_hw.cuh"
 #include "fourier.cuh"
 #include "split_kernels.cuh"
 
@@ -58,6 +59,31 @@ __device__ __forceinline__ void courant_point_f(int mode, float vr, float vt, fl
   double valr = (double)br * br * LFfac * orho1;
   double valh2 = ((double)bt * bt + (double)bp * bp) * LFfac * ost2 * orho1;
   double valr2 = valr, valh2m = valh2;
+  if (mode == 1) {
+    valr2 = valr * valr / (valr + valri2);
+    valh2m = valh2 * valh2 / (valh2 + valhi2);
+  }
+  vr2 = or4 * (cf2 * vflr2 + af2 * valr2);
+  vh2 = or2 * (cf2 * vflh2 + af2 * valh2m);
+}
+
+// courant_point_f with FP32 arithmetic (grid values are FP32 already; the
+// maxima keep ~1e-7 relative accuracy)
+__device__ __forceinline__ void courant_point_s(int mode, float vr, float vt, float vp, float br,
+                                                float bt, float bp, float or2, float or4,
+                                                float orho1, float orho2, float ost2, float LFfac,
+                                                float cf2, float af2, float valri2, float valhi2,
+                                                float& vr2, float& vh2) {
+  const float vflr2 = orho2 * vr * vr;
+  const float vflh2 = (vt * vt + vp * vp) * ost2 * orho2;
+  if (mode == 0) {
+    vr2 = cf2 * or4 * vflr2;
+    vh2 = cf2 * or2 * vflh2;
+    return;
+  }
+  const float valr = br * br * LFfac * orho1;
+  const float valh2 = (bt * bt + bp * bp) * LFfac * ost2 * orho1;
+  float valr2 = valr, valh2m = valh2;
   if (mode == 1) {
     valr2 = valr * valr / (valr + valri2);
     valh2m = valh2 * valh2 / (valh2 + valhi2);
@@ -196,8 +222,140 @@ __global__ void __launch_bounds__(kNlSplitThreads) k_nl_bouss_split(NlSplitArgs 
   }
 }
 
+// The same stage for n_phi = 32 Q (Q in 8, 12, 16, 24): every field row is
+// transformed by one half-warp (fft_hw.cuh), so between the block-wide
+// phases (load, inverse FFTs, products, forward FFTs, store) the rows
+// proceed independently.  Threads: one half-warp per row of the larger of the
+// input and output field sets.
+template <bool MAG, bool CHEM>
+__host__ __device__ constexpr int hw_threads() {
+  return 32 * ((SplitFields<MAG, CHEM>::NB + 1) / 2);
+}
+
+template <bool MAG, bool CHEM, int Q>
+__global__ void __maxnreg__(96)
+    k_nl_bouss_split_hw(NlSplitArgs a) {
+  using BF = SplitFields<MAG, CHEM>;
+  constexpr int NFI = BF::NFI, NFO = BF::NFO, H = 16 * Q, S = H + 1;
+  constexpr int T = hw_threads<MAG, CHEM>();
+  extern __shared__ __align__(16) float smemf[];
+  __shared__ double red[32];
+  cplx<float>* buf = reinterpret_cast<cplx<float>*>(smemf);  // NB rows, S apart
+  cplx<float>* twH = buf + BF::NB * S;
+  cplx<float>* twN = twH + H;
+  const Tables& t = a.t;
+  const int M = t.n_m;
+  const int row = blockIdx.x, r = blockIdx.y;
+  const int j = row >> 1;
+  const float hs = (row & 1) ? -1.f : 1.f;  // north = sym + asym, south = sym - asym
+  const int tid = threadIdx.x, hw = tid >> 4, lane = tid & 15;
+  const unsigned mask = 0xFFFFu << (16 * (hw & 1));
+  for (int n = tid; n < H; n += T) {
+    const double2 wh = __ldg(&t.twiddle[2 * n]), wn = __ldg(&t.twiddle[n]);
+    twH[n] = {(float)wh.x, (float)wh.y};
+    twN[n] = {(float)wn.x, (float)wn.y};
+  }
+  const float* fsym = a.Fs + (int64_t)j * a.fs_j + (int64_t)r * 2 * NFI;
+  for (int e = tid; e < NFI * H; e += T) {
+    const int k = e / NFI, f = e - k * NFI;
+    cplx<float> X = {0.f, 0.f};
+    if (k < M) {
+      const float2 sy = __ldg(reinterpret_cast<const float2*>(fsym + k * a.fs_m) + f);
+      const float2 as = __ldg(reinterpret_cast<const float2*>(fsym + k * a.fs_m + a.fs_c) + f);
+      X = {sy.x + hs * as.x, sy.y + hs * as.y};
+    }
+    buf[f * S + hw_swz<Q>(k)] = X;
+  }
+  __syncthreads();
+  if (hw < NFI) hw_row_fft<Q, true, true>(buf + hw * S, lane, mask, twH, twN);
+  __syncthreads();
+
+  const float or2 = (float)a.or2[r], or4 = (float)a.or4[r], ost2 = (float)t.ost2[row];
+  const float orho1 = (float)a.orho1[r], orho2 = (float)a.orho2[r];
+  const float valri2 = (float)(a.valfac / a.delxr2[r]), valhi2 = (float)(a.valfac / a.delxh2[r]);
+  const float LF = (float)a.LFfac, cf2 = (float)a.cf2, af2 = (float)a.af2;
+  float mr = 0.f, mh = 0.f;
+  for (int i = tid; i < H; i += T) {
+    const int si = hw_swz<Q>(i);
+    cplx<float> zin[NFI];
+#pragma unroll
+    for (int f = 0; f < NFI; ++f) zin[f] = buf[f * S + si];
+    float out[2][NFO];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      auto v = [&](int f) { return h ? zin[f].y : zin[f].x; };
+      BoussInF fi;
+      constexpr int iv = BF::IV;
+      if constexpr (MAG) {
+        fi.br = v(0); fi.bt = v(1); fi.bp = v(2); fi.cbr = v(3); fi.cbt = v(4); fi.cbp = v(5);
+      } else {
+        fi.br = fi.bt = fi.bp = fi.cbr = fi.cbt = fi.cbp = 0.f;
+      }
+      fi.vr = v(iv); fi.vt = v(iv + 1); fi.vp = v(iv + 2);
+      fi.cvr = v(iv + 3); fi.cvt = v(iv + 4); fi.cvp = v(iv + 5);
+      fi.s = v(iv + 6);
+      fi.xi = 0.f;
+      if constexpr (CHEM) fi.xi = v(iv + 7);
+      float vr2, vh2;
+      courant_point_s(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, or2, or4, orho1,
+                      orho2, ost2, LF, cf2, af2, valri2, valhi2, vr2, vh2);
+      mr = fmaxf(mr, vr2);
+      mh = fmaxf(mh, vh2);
+      float o[12];
+      bouss_point_f(fi, or2, or4, ost2, LF, MAG, o);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) out[h][q] = o[q];
+      if constexpr (MAG) { out[h][6] = o[6]; out[h][7] = o[7]; out[h][8] = o[8]; }
+      if constexpr (CHEM) {
+        constexpr int c = MAG ? 9 : 6;
+        out[h][c] = o[9]; out[h][c + 1] = o[10]; out[h][c + 2] = o[11];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NFO; ++q) buf[q * S + si] = {out[0][q], out[1][q]};
+  }
+  double vmr = block_max_d((double)mr, red);
+  if (tid == 0) atomicMax(&a.vr2max[r], (unsigned long long)__double_as_longlong(vmr + 0.0));
+  double vmh = block_max_d((double)mh, red);
+  if (tid == 0) atomicMax(&a.vh2max[r], (unsigned long long)__double_as_longlong(vmh + 0.0));
+  if (r == 0 || r == a.n_r - 1) return;
+  __syncthreads();
+  if (hw < NFO) hw_row_fft<Q, false, false>(buf + hw * S, lane, mask, twH, twN);
+  __syncthreads();
+  const float ws = (float)(t.wq[row] / (2 * H)), wv = (float)(t.wq_v[row] / (2 * H));
+  float* Gr = a.G + (int64_t)(row & 1) * a.g_h + (int64_t)j * a.g_j + (int64_t)(r - 1) * a.g_level;
+  for (int e = tid; e < M * NFO; e += T) {
+    const int k = e / NFO, o = e - k * NFO;
+    const cplx<float>* z = buf + o * S;
+    const cplx<float> X = r2c_post_w(z[hw_swz<Q>(k)], z[hw_swz<Q>((H - k) % H)], twN[k]);
+    const bool radial = (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
+    const float w = radial ? ws : wv;
+    reinterpret_cast<float2*>(Gr + k * a.g_m)[o] = make_float2(w * X.x, w * X.y);
+  }
+}
+
+template <bool MAG, bool CHEM, int Q>
+static int launch_hw(const NlSplitArgs& a, cudaStream_t st) {
+  using BF = SplitFields<MAG, CHEM>;
+  constexpr int H = 16 * Q;
+  const size_t sm = ((size_t)BF::NB * (H + 1) + 2 * H) * sizeof(cplx<float>);
+  auto kern = k_nl_bouss_split_hw<MAG, CHEM, Q>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(a.t.n_theta, a.n_r);
+  kern<<<grid, hw_threads<MAG, CHEM>(), sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
 template <bool MAG, bool CHEM>
 static int launch_t(const NlSplitArgs& a, cudaStream_t st) {
+  switch (a.t.n_phi) {
+    case 256: return launch_hw<MAG, CHEM, 8>(a, st);
+    case 384: return launch_hw<MAG, CHEM, 12>(a, st);
+    case 512: return launch_hw<MAG, CHEM, 16>(a, st);
+    case 768: return launch_hw<MAG, CHEM, 24>(a, st);
+    default: break;
+  }
   using BF = SplitFields<MAG, CHEM>;
   size_t sm = ((size_t)(BF::NB + kFftRowBatch) * padded_len(a.t.n_phi / 2) + a.t.n_phi / 2) *
               sizeof(cplx<float>);

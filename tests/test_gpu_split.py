@@ -1,10 +1,15 @@
 """GPU parity of the split-precision (bf16x3 tcgen05, FP32 accumulate) fused stage
 against the FP64 oracle.
 
-Tolerance: 2e-5 of the output's scale (the vector pair's max(|S|, |T|) for S and
-T, as in the FP64 stage test).  Measured on B200: 1e-6 to 8e-6 for random
-rough fields (|c_lm| ~ (l+1)^-1.5) up to l_max = 127; the error comes from the
-FP32 Fourier intermediates, FP32 phi FFTs and FP32 tensor-core accumulation.
+Tolerance: relative to the output's scale (the vector pair's max(|S|, |T|) for
+S and T, as in the FP64 stage test), 2e-5 up to l_max = 127 and 5e-5 above.
+Measured on B200 for random rough fields (|c_lm| ~ (l+1)^-1.5): 1e-6 to 9e-6
+up to l_max = 127, 2e-6 to 2.4e-5 at l_max = 255.  The error comes from the
+FP32 Fourier intermediates, FP32 phi FFTs and FP32 tensor-core accumulation,
+and grows with l_max: the vector analysis (Advt, Advp, VxBt, VxBp) weights
+grid rows by 1/sin^2(theta), which amplifies grid-level error near the poles.
+In the FP64 oracle, rounding only the l_max = 255 grid fields to FP32 already
+gives 1e-6 on Advt/Advp (3e-8 on Advr).
 The Courant steps come from FP32 grid values: 1e-5 relative.
 """
 
@@ -23,6 +28,9 @@ CASES = [
     (20, 1, 6, False, True),
     (63, 1, 9, True, False),
     (127, 1, 5, True, False),
+    (85, 1, 4, False, True),
+    (170, 1, 3, True, True),
+    (255, 1, 3, True, False),
 ]
 PAIR = {"Advt": "Advp", "Advp": "Advt", "VxBt": "VxBp", "VxBp": "VxBt"}
 
@@ -67,7 +75,8 @@ def test_split_stage_matches_oracle(l_max, minc, N, l_mag, l_chem):
             scale = max(scale, np.abs(ref[PAIR[k]]).max())
         worst[k] = np.abs(got - ref[k]).max() / scale
     print("split stage errors", {k: f"{v:.2e}" for k, v in worst.items()})
+    tol = 2e-5 if l_max <= 127 else 5e-5
     for k, v in worst.items():
-        assert v < 2e-5, (k, v)
+        assert v < tol, (k, v)
     assert np.abs(dt.cpu().numpy() - rdt).max() / np.abs(rdt).max() < 1e-5
     assert np.abs(dh.cpu().numpy() - rdh).max() / np.abs(rdh).max() < 1e-5
