@@ -641,7 +641,11 @@ static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
   w.gs = w.fs + al((size_t)p->n_m * 2 * p->nhs * w.rows_syn * sizeof(float));
   w.mx = w.gs + al((size_t)p->n_m * 2 * p->nhs * w.rows_nl * sizeof(float));
   w.aimg = w.mx + al(2 * (size_t)n_r * sizeof(unsigned long long));
-  w.total = w.aimg + al(synth_split_image_bytes((int)w.rows_syn, split_syn_total_chunks(p)));
+  // A-operand images: the synthesis ones are dead before the analysis writes its own
+  const size_t syn = synth_split_image_bytes((int)w.rows_syn, split_syn_total_chunks(p));
+  const size_t ana = anal_split_image_bytes(p->n_m, p->nhs, n_r - 2,
+                                            128 / (2 * bouss_nfo(mag, chem)));
+  w.total = w.aimg + al(std::max(syn, ana));
   return w;
 }
 
@@ -691,6 +695,7 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
                             double* dthkc, void* work, cudaStream_t st) {
   const int nfi = bouss_nfi(MAG, CHEM), nfo = bouss_nfo(MAG, CHEM);
   const SplitWs W = split_ws(p, n_r, MAG, CHEM);
+  constexpr int kSplitRowsHost = 128;
   char* w = (char*)work;
   int* err = (int*)(w + W.err);
   float* Fs = (float*)(w + W.fs);
@@ -833,11 +838,12 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
     a.out[o++] = (double2*)out->VXit;
   }
-  a.row_per_level = r;
-  a.nrows = (n_r - 2) * r;
-  a.stg_lev = std::min(n_r - 2, 127 / r + 2);
+  a.n_out = o;
+  a.cols = 2 * nfo;
+  a.lev_tile = kSplitRowsHost / a.cols;
   a.ld = out->ld;
   a.out_col0 = 1;
+  a.aimg = (uint8_t*)(w + W.aimg);
   a.err = err;
   MT_TRY(launch_anal_split(a, st));
   return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);

@@ -102,14 +102,44 @@ __device__ __forceinline__ cplx<float> r2c_post_w(cplx<float> Zk, cplx<float> Zc
   return {0.5f * (F.x + t.y), 0.5f * (F.y - t.x)};
 }
 
+// Twiddle tables of the two radix-4 passes, laid out [butterfly][r - 1] so
+// that the 16 lanes read words 3 apart (no bank conflicts):
+//   tw2[3 jm + r - 1] = w^(4 r jm), jm < Q;  tw3[3 j + r - 1] = w^(r j), j < 4 Q;
+// w = exp(-2 pi i / H).  Filled from the N-point table tw_N (N = 2 H).
+template <int Q>
+__device__ __forceinline__ void hw_twiddles_to_smem(cplx<float>* tw2, cplx<float>* tw3,
+                                                    cplx<float>* twN,
+                                                    const double2* __restrict__ tw_N, int tid,
+                                                    int nthreads) {
+  constexpr int H = 16 * Q;
+  for (int e = tid; e < 3 * Q + 12 * Q + H; e += nthreads) {
+    int idx;
+    cplx<float>* dst;
+    if (e < 3 * Q) {
+      idx = 2 * (4 * (e % 3 + 1) * (e / 3));
+      dst = tw2 + e;
+    } else if (e < 15 * Q) {
+      const int q = e - 3 * Q;
+      idx = 2 * ((q % 3 + 1) * (q / 3));
+      dst = tw3 + q;
+    } else {
+      idx = e - 15 * Q;
+      dst = twN + idx;
+    }
+    const double2 w = __ldg(&tw_N[idx]);
+    *dst = {(float)w.x, (float)w.y};
+  }
+}
+
 // In-place transform of one row (swizzled layout) by the 16 lanes in `mask`.
-// twH[n] = exp(-2 pi i n / H), twN[k] = exp(-2 pi i k / (2 H)), n, k < H.
+// tw2, tw3: hw_twiddles_to_smem; twN[k] = exp(-2 pi i k / (2 H)), k < H.
 // PRE: the row holds the half spectrum X[0..H) of a real row of length 2 H and
 // the transform input is Z[k] = c2r_pre(X[k], X[H - k]) (Im X[0] dropped,
 // X[H] = 0); the result z[n] then carries x[2 n] + i x[2 n + 1].
 template <int Q, bool INV, bool PRE>
 __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned mask,
-                                           const cplx<float>* __restrict__ twH,
+                                           const cplx<float>* __restrict__ tw2,
+                                           const cplx<float>* __restrict__ tw3,
                                            const cplx<float>* __restrict__ twN) {
   constexpr int H = 16 * Q, NBF = Q / 4;
   static_assert(Q % 4 == 0, "two radix-4 passes of 4 Q butterflies over 16 lanes");
@@ -146,7 +176,7 @@ __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned 
     cplx<float> u[4] = {v[4 * it], v[4 * it + 1], v[4 * it + 2], v[4 * it + 3]};
 #pragma unroll
     for (int r = 1; r < 4; ++r) {
-      cplx<float> w = twH[4 * r * jm];
+      cplx<float> w = tw2[3 * jm + r - 1];
       if (INV) w.y = -w.y;
       u[r] = cmul(u[r], w);
     }
@@ -168,7 +198,7 @@ __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned 
     cplx<float> u[4] = {v[4 * it], v[4 * it + 1], v[4 * it + 2], v[4 * it + 3]};
 #pragma unroll
     for (int r = 1; r < 4; ++r) {
-      cplx<float> w = twH[r * j];
+      cplx<float> w = tw3[3 * j + r - 1];
       if (INV) w.y = -w.y;
       u[r] = cmul(u[r], w);
     }

@@ -29,9 +29,6 @@
 
 namespace mt {
 
-constexpr int kSplitStages = 2;
-constexpr int kSplitThreads = 192;
-
 // plane pairs (a, b) of the six retained products
 __device__ __constant__ int8_t kPairA[6] = {0, 0, 1, 0, 1, 2};
 __device__ __constant__ int8_t kPairB[6] = {0, 1, 0, 2, 1, 0};
@@ -83,41 +80,8 @@ __device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, uin
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-// barrier among the 128 producer threads (warps 0-3) only
-__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
-// the same barrier, returning whether `ok` holds in all 128 producer threads
-// (keeps a timeout from splitting the producers between iterations)
-__device__ __forceinline__ bool producers_all(bool ok) {
-  uint32_t r;
-  asm volatile(
-      "{\n.reg .pred p, q;\nsetp.ne.u32 q, %1, 0;\nbar.red.and.pred p, 1, 128, q;\n"
-      "selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)ok)
-      : "memory");
-  return r != 0;
-}
-
-// Shared memory of one CTA: operand stages [A_P | A_dP | B_P | B_dP], two
-// staging buffers for the raw inputs of a K chunk, then barriers.
-struct SplitSmem {
-  uint32_t a_plane, b_plane, stage_bytes, stg_off, stg_bytes, bar_off;
-  __host__ __device__ SplitSmem(int brows, uint32_t staging) {
-    a_plane = kSplitRows * 32;
-    b_plane = brows * 32;
-    stage_bytes = 6 * a_plane + 6 * b_plane;
-    stg_off = kSplitStages * stage_bytes;
-    stg_bytes = (staging + 127) & ~127u;
-    bar_off = stg_off + 2 * stg_bytes;
-  }
-  __host__ __device__ size_t total() const { return bar_off + 8 * (3 * kSplitStages + 1) + 16; }
-};
-
 __host__ __device__ inline uint32_t syn_staging_bytes(int narr, int stg_lev) {
   return (uint32_t)narr * 32 * stg_lev * 16;
-}
-__host__ __device__ inline uint32_t ana_staging_bytes(int stg_lev, int g_level) {
-  return (uint32_t)2 * kSplitKC * stg_lev * g_level * 4;
 }
 
 // ------------------------------------------------------------- synthesis
@@ -350,19 +314,80 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_synth_gemm(SplitSynArgs a) 
 }
 
 // -------------------------------------------------------------- analysis
+//
+// k_ana_pack folds the north/south Fourier rows of the phi stage into
+// bf16x3 A-operand images: block (tile rt, theta-pair chunk c, m) stages 16
+// theta pairs of both hemispheres at the tile's levels and writes, for
+// fold 0 (north + south) and fold 1 (north - south), a 128 x 16 chunk whose
+// rows are the raw Fourier columns (level lv, column col) of the tile.
+// k_anal_gemm (CTA = tile, output parity, m) accumulates
+//   acc0[col][l] = sum_j fold_par(col)[j] P_l(j),
+//   acc1[col][l] = sum_j fold_(1-par)(col)[j] dP_l(j)
+// in two TMEM accumulators and its epilogue forms each output component as
+// coef(kP) acc0[colP] + coef(kD) acc1[colD] (the row program), exchanging
+// accumulator rows through shared memory.
 
-__global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a) {
+__host__ __device__ inline int64_t ana_img_chunk(int n_m, int nchj, int rt, int mc, int fold,
+                                                 int c) {
+  return (((int64_t)rt * n_m + mc) * 2 + fold) * nchj + c;
+}
+
+__global__ void __launch_bounds__(kPackThreads, 4) k_ana_pack(SplitAnaArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const Tables& t = a.t;
+  const int rt = blockIdx.x, c = blockIdx.y, mc = blockIdx.z;
+  const int nchj = gridDim.y;
+  const int tid = threadIdx.x;
+  const int lev0 = rt * a.lev_tile;
+  const int nlev = min(a.lev_tile, a.n_lev - lev0);
+  const int gl = (int)a.g_level;
+  const int rowlen = a.lev_tile * gl;  // floats per staged (hemisphere, theta pair)
+  float* d = reinterpret_cast<float*>(smem);
+  {
+    const float* gm = a.G + (int64_t)mc * a.g_m + (int64_t)lev0 * gl;
+    const int cpl = nlev * gl / 4;  // 16-byte pieces per (hemisphere, theta pair)
+    const int total = 2 * kSplitKC * cpl;
+    for (int e = tid; e < total; e += kPackThreads) {
+      const int hj = e / cpl, p4 = e - hj * cpl;
+      const int h = hj / kSplitKC, jl = hj - h * kSplitKC;
+      const int j = kSplitKC * c + jl;
+      const float* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j + 4 * p4;
+      cp_async16_zfill(d + hj * rowlen + 4 * p4, src, j < t.nhs ? 16u : 0u);
+    }
+    cp_async_commit();
+    cp_async_wait0();
+    __syncthreads();
+  }
+#pragma unroll 1
+  for (int task = tid; task < 2 * kSplitRows; task += kPackThreads) {
+    const int fold = task / kSplitRows, row = task % kSplitRows;
+    const int lv = row / a.cols, col = row - lv * a.cols;
+    const bool live = lv < nlev;
+    const float sg = fold ? -1.f : 1.f;
+    const float* n = d + lv * gl + col;
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      v[i] = live ? n[i * rowlen] + sg * n[(kSplitKC + i) * rowlen] : 0.f;
+    uint8_t* dst = a.aimg + ana_img_chunk(t.n_m, nchj, rt, mc, fold, c) * kImgChunk;
+    put_row16(dst, row, v);
+  }
+}
+
+// Warp 0 lane 0 loads, warp 1 lane 0 issues the MMAs, warp 2 owns TMEM, all
+// four warps run the epilogue.  K steps: theta-pair chunk c of the P table
+// (into acc0), then of the dP table (into acc1).
+__global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   const Tables& t = a.t;
   const SplitTables& st = a.s;
   const int rt = blockIdx.x, par = blockIdx.y, mc = blockIdx.z;
   const int wk = st.ana_wk[mc * 2 + par];
   if (wk == 0 || *(volatile int*)a.err) return;
-  const SplitSmem L(a.wk_max, ana_staging_bytes(a.stg_lev, (int)a.g_level));
-  uint64_t* full_a = reinterpret_cast<uint64_t*>(smem + L.bar_off);
-  uint64_t* full_b = full_a + kSplitStages;
-  uint64_t* empty = full_b + kSplitStages;
-  uint64_t* accb = empty + kSplitStages;
+  const GemmSmem L(a.wk_max);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* empty = full + kGemmStages;
+  uint64_t* accb = empty + kGemmStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -370,161 +395,127 @@ __global__ void __launch_bounds__(kSplitThreads, 1) k_anal_split(SplitAnaArgs a)
   const int m = mc * t.minc;
   const int nlm = t.l_max - m + 1;
   const int ls = t.lstart[mc];
-  const int nch = (t.nhs + kSplitKC - 1) / kSplitKC;
-  // folded input for P rows: north+south if the output parity is even; dP the reverse
-  const int fold_t[2] = {par, 1 - par};
-  const uint32_t tcols = wk <= 32 ? 32 : (wk <= 64 ? 64 : (wk <= 128 ? 128 : 256));
-  const uint32_t b_plane = wk * 32;
+  const int nchj = (t.nhs + kSplitKC - 1) / kSplitKC;
+  // two accumulators of wk columns; 512 (all of TMEM) only above l_max = 255
+  uint32_t tcols = 32;
+  while (tcols < 2u * wk) tcols *= 2;
+  const uint32_t b_plane = wk * 32, bchunk = 3 * b_plane;
 
   if (tid == 0) {
-    for (int s = 0; s < kSplitStages; ++s) {
-      mbar_init(&full_a[s], kSplitRows);
-      mbar_init(&full_b[s], 1);
+    for (int s = 0; s < kGemmStages; ++s) {
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     mbar_init(accb, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 4) tmem_alloc(tmem_slot, tcols);
+  if (warp == 2) tmem_alloc(tmem_slot, tcols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
 
-  if (warp < 4) {
-    // Chunk c needs theta pairs [16 c, 16 c + 16) of the north and south rows at
-    // the tile's levels: staged with cp.async one chunk ahead.
-    const int R = rt * kSplitRows + tid;
-    const bool live = R < a.nrows;
-    const int lev = live ? R / a.row_per_level : 0;
-    const int q = live ? R - lev * a.row_per_level : 0;
-    const int lev0 = (rt * kSplitRows) / a.row_per_level;
-    const int nlev = min(a.stg_lev, a.n_lev - lev0);
-    const int lv = lev - lev0;
-    const RowOp op = a.ops[q];
-    const double dm = (double)m;
-    const double cP = coef_value(op.kP, dm), cD = coef_value(op.kD, dm);
-    const int gl = (int)a.g_level;
-    const int rowlen = a.stg_lev * gl;  // floats per staged (hemisphere, theta pair) row
-    const int colP = lv * gl + 2 * op.tP + op.cP;
-    const int colD = lv * gl + 2 * op.tD + op.cD;
-    const float sgP = fold_t[0] ? -1.f : 1.f, sgD = fold_t[1] ? -1.f : 1.f;
-    auto stg = [&](int b) { return reinterpret_cast<float*>(smem + L.stg_off + b * L.stg_bytes); };
-    const float* gm = a.G + (int64_t)mc * a.g_m + (int64_t)lev0 * gl;
-    auto issue = [&](int c) {
-      float* d = stg(c & 1);
-      const int cpl = nlev * gl / 4;  // 16-byte pieces per (hemisphere, theta pair)
-      const int total = 2 * kSplitKC * cpl;
-      for (int e = tid; e < total; e += kSplitRows) {
-        const int hj = e / cpl, p4 = e - hj * cpl;
-        const int h = hj / kSplitKC, jl = hj - h * kSplitKC;
-        const int j = kSplitKC * c + jl;
-        const float* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j + 4 * p4;
-        cp_async16_zfill(d + hj * rowlen + 4 * p4, src, j < t.nhs ? 16u : 0u);
-      }
-      cp_async_commit();
-    };
-    issue(0);
-    for (int c = 0; c < nch; ++c) {
-      const int s = c % kSplitStages;
-      cp_async_wait0();
-      producers_sync();
-      if (c + 1 < nch) issue(c + 1);
-      bool ok = c < kSplitStages ||
-                mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 11);
-      if (!producers_all(ok)) break;
-      const float* d = stg(c & 1);
-      uint8_t* stage = smem + s * L.stage_bytes;
-      float vp[16], vd[16];
-      const float fcP = (float)cP, fcD = (float)cD;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        vp[i] = 0.f;
-        vd[i] = 0.f;
-        if (live) {
-          const float* n = d + i * rowlen;
-          const float* so = d + (kSplitKC + i) * rowlen;
-          if (op.kP) vp[i] = fcP * (n[colP] + sgP * so[colP]);
-          if (op.kD) vd[i] = fcD * (n[colD] + sgD * so[colD]);
-        }
-      }
-      put_row16(stage, tid, vp);
-      put_row16(stage + 3 * L.a_plane, tid, vd);
-      fence_proxy_async();
-      mbar_arrive(&full_a[s]);
+  if (warp == 0 && lane == 0) {
+    // ---------------- loader ----------------
+    const uint8_t* aimg[2];
+    const uint8_t* img[2];
+    for (int q = 0; q < 2; ++q) {
+      const int fold = q ? 1 - par : par;
+      aimg[q] = a.aimg + ana_img_chunk(t.n_m, nchj, rt, mc, fold, 0) * kImgChunk;
+      img[q] = st.ana + st.ana_off[(mc * 2 + q) * 2 + par];
     }
-    cp_async_wait0();
-    const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 12);
-    tc_fence_after();
-    if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
-      const int o = q >> 1, comp = q & 1;
-      double* out = live ? reinterpret_cast<double*>(a.out[o]) : nullptr;
-      for (int c0 = 0; c0 < wk; c0 += 16) {
-        float v[16];
-        tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
-        if (out) {
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int k = 2 * (c0 + i) + par;
-            if (k < nlm) {
-              const double l = (double)(m + k);
-              const double sc = op.scale ? (m + k > 0 ? 1.0 / (l * (l + 1.0)) : 0.0) : 1.0;
-              out[2 * ((int64_t)(ls + k) * a.ld + a.out_col0 + lev) + comp] = sc * (double)v[i];
-            }
-          }
-        }
-      }
-    }
-  } else if (warp == 4) {
-    if (lane == 0) {
-      const uint8_t* img[2];
-      for (int q = 0; q < 2; ++q) img[q] = st.ana + st.ana_off[(mc * 2 + q) * 2 + par];
-      const uint32_t chunk = 3 * b_plane;
-      int issued = 0;
-      for (int c = 0; c < nch; ++c) {
-        const int s = c % kSplitStages;
-        if (c >= kSplitStages &&
-            !mbar_wait(&empty[s], ((c / kSplitStages) - 1) & 1, abort_flag, a.err, 13))
+    int step = 0;
+    bool ok = true;
+    for (int c = 0; c < nchj && ok; ++c) {
+      for (int q = 0; q < 2; ++q) {
+        const int s = step % kGemmStages;
+        if (step >= kGemmStages &&
+            !mbar_wait(&empty[s], ((step / kGemmStages) - 1) & 1, abort_flag, a.err, 13)) {
+          ok = false;
           break;
-        uint8_t* stage = smem + s * L.stage_bytes + 6 * L.a_plane;
-        mbar_expect_tx(&full_b[s], 2 * chunk);
-        for (int q = 0; q < 2; ++q)
-          bulk_g2s(stage + q * 3 * L.b_plane, img[q] + (int64_t)c * chunk, chunk, &full_b[s]);
-        issued = c + 1;
+        }
+        uint8_t* stage = smem + s * L.stage_bytes;
+        mbar_expect_tx(&full[s], kImgChunk + bchunk);
+        bulk_g2s(stage, aimg[q] + (int64_t)c * kImgChunk, kImgChunk, &full[s]);
+        bulk_g2s(stage + kImgChunk, img[q] + (int64_t)c * bchunk, bchunk, &full[s]);
+        ++step;
       }
-      for (int c = max(0, issued - kSplitStages); c < issued; ++c)
-        mbar_wait(&full_b[c % kSplitStages], (c / kSplitStages) & 1, abort_flag, nullptr, 0);
     }
-  } else {
-    if (lane == 0) {
-      const uint32_t idesc = umma_idesc_bf16(kSplitRows, wk);
-      uint32_t acc = 0;
-      for (int c = 0; c < nch; ++c) {
-        const int s = c % kSplitStages;
-        const uint32_t ph = (c / kSplitStages) & 1;
-        if (!mbar_wait(&full_a[s], ph, abort_flag, a.err, 14)) break;
-        if (!mbar_wait(&full_b[s], ph, abort_flag, a.err, 15)) break;
+    for (int k = max(0, step - kGemmStages); k < step; ++k)
+      mbar_wait(&full[k % kGemmStages], (k / kGemmStages) & 1, abort_flag, nullptr, 0);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    const uint32_t idesc = umma_idesc_bf16(kSplitRows, wk);
+    int step = 0;
+    bool ok = true;
+    for (int c = 0; c < nchj && ok; ++c) {
+      for (int q = 0; q < 2; ++q) {
+        const int s = step % kGemmStages;
+        if (!mbar_wait(&full[s], (step / kGemmStages) & 1, abort_flag, a.err, 14)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
         const uint32_t sa = smem_u32(smem + s * L.stage_bytes);
-        const uint32_t sb = sa + 6 * L.a_plane;
-        for (int q = 0; q < 2; ++q) {
+        const uint32_t sb = sa + kImgChunk;
 #pragma unroll
-          for (int pp = 0; pp < 6; ++pp) {
-            uint64_t da = umma_desc(sa + q * 3 * L.a_plane + kPairA[pp] * L.a_plane, 128, 256);
-            uint64_t db = umma_desc(sb + q * 3 * L.b_plane + kPairB[pp] * b_plane, 128, 256);
-            umma_bf16(tbase, da, db, idesc, acc);
-            acc = 1;
-          }
+        for (int pp = 0; pp < 6; ++pp) {
+          const uint64_t da = umma_desc(sa + kPairA[pp] * kImgPlane, 128, 256);
+          const uint64_t db = umma_desc(sb + kPairB[pp] * b_plane, 128, 256);
+          umma_bf16(tbase + q * wk, da, db, idesc, (c > 0 || pp > 0) ? 1u : 0u);
         }
         umma_commit(&empty[s]);
+        ++step;
       }
-      umma_commit(accb);
+    }
+    umma_commit(accb);
+  }
+  __syncwarp();
+  // ---------------- epilogue ----------------
+  const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 12);
+  tc_fence_after();
+  if (__syncthreads_and(ok && !*abort_flag)) {
+    // every copy landed and every MMA finished: the stages are free for the exchange
+    constexpr int XS = 17;  // padded row of 16 columns
+    float* xch = reinterpret_cast<float*>(smem);  // [2][128][XS]
+    const int lev0 = rt * a.lev_tile;
+    const int nlev = min(a.lev_tile, a.n_lev - lev0);
+    const double dm = (double)m;
+    for (int c0 = 0; c0 < wk; c0 += 16) {
+      float v[16];
+      tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) xch[tid * XS + i] = v[i];
+      tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + wk + c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) xch[(kSplitRows + tid) * XS + i] = v[i];
+      __syncthreads();
+      const int ntask = a.n_out * 16 * nlev;
+      for (int task = tid; task < ntask; task += kGemmThreads) {
+        const int lv = task % nlev, rest = task / nlev;
+        const int i = rest % 16, o = rest / 16;
+        const int k = 2 * (c0 + i) + par;
+        if (k >= nlm) continue;
+        double re_im[2];
+#pragma unroll
+        for (int comp = 0; comp < 2; ++comp) {
+          const RowOp op = a.ops[2 * o + comp];
+          const float* x0 = xch + (lv * a.cols + 2 * op.tP + op.cP) * XS + i;
+          const float* x1 = xch + (kSplitRows + lv * a.cols + 2 * op.tD + op.cD) * XS + i;
+          re_im[comp] = coef_value(op.kP, dm) * (double)*x0 + coef_value(op.kD, dm) * (double)*x1;
+        }
+        const double l = (double)(m + k);
+        const double sc = a.ops[2 * o].scale ? (m + k > 0 ? 1.0 / (l * (l + 1.0)) : 0.0) : 1.0;
+        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] =
+            make_double2(sc * re_im[0], sc * re_im[1]);
+      }
+      __syncthreads();
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 4) {
+  if (warp == 2) {
     tc_fence_after();
     tmem_dealloc(tbase, tcols);
   }
@@ -553,16 +544,25 @@ size_t synth_split_image_bytes(int nrows, int64_t total_chunks) {
 }
 
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st) {
-  const SplitSmem L(a.wk_max, ana_staging_bytes(a.stg_lev, (int)a.g_level));
-  size_t sm = L.total();
-  MT_CHECK_CUDA(cudaFuncSetAttribute(k_anal_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const int ntiles = (a.n_lev + a.lev_tile - 1) / a.lev_tile;
+  const int nchj = (a.t.nhs + kSplitKC - 1) / kSplitKC;
+  const size_t pack_sm = (size_t)2 * kSplitKC * a.lev_tile * a.g_level * sizeof(float);
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_ana_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pack_sm));
+  k_ana_pack<<<dim3(ntiles, nchj, a.t.n_m), kPackThreads, pack_sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  const GemmSmem L(a.wk_max);
+  const size_t sm = L.total();
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_anal_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-  dim3 grid((a.nrows + kSplitRows - 1) / kSplitRows, 2, a.t.n_m);
-  k_anal_split<<<grid, kSplitThreads, sm, st>>>(a);
+  k_anal_gemm<<<dim3(ntiles, 2, a.t.n_m), kGemmThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
 
-
+size_t anal_split_image_bytes(int n_m, int nhs, int n_lev, int lev_tile) {
+  const int ntiles = (n_lev + lev_tile - 1) / lev_tile;
+  return (size_t)ntiles * n_m * 2 * ((nhs + kSplitKC - 1) / kSplitKC) * kImgChunk;
+}
 
 }  // namespace mt

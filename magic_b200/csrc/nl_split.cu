@@ -241,8 +241,9 @@ __global__ void __maxnreg__(96)
   extern __shared__ __align__(16) float smemf[];
   __shared__ double red[32];
   cplx<float>* buf = reinterpret_cast<cplx<float>*>(smemf);  // NB rows, S apart
-  cplx<float>* twH = buf + BF::NB * S;
-  cplx<float>* twN = twH + H;
+  cplx<float>* tw2 = buf + BF::NB * S;
+  cplx<float>* tw3 = tw2 + 3 * Q;
+  cplx<float>* twN = tw3 + 12 * Q;
   const Tables& t = a.t;
   const int M = t.n_m;
   const int row = blockIdx.x, r = blockIdx.y;
@@ -250,11 +251,7 @@ __global__ void __maxnreg__(96)
   const float hs = (row & 1) ? -1.f : 1.f;  // north = sym + asym, south = sym - asym
   const int tid = threadIdx.x, hw = tid >> 4, lane = tid & 15;
   const unsigned mask = 0xFFFFu << (16 * (hw & 1));
-  for (int n = tid; n < H; n += T) {
-    const double2 wh = __ldg(&t.twiddle[2 * n]), wn = __ldg(&t.twiddle[n]);
-    twH[n] = {(float)wh.x, (float)wh.y};
-    twN[n] = {(float)wn.x, (float)wn.y};
-  }
+  hw_twiddles_to_smem<Q>(tw2, tw3, twN, t.twiddle, tid, T);
   const float* fsym = a.Fs + (int64_t)j * a.fs_j + (int64_t)r * 2 * NFI;
   for (int e = tid; e < NFI * H; e += T) {
     const int k = e / NFI, f = e - k * NFI;
@@ -267,7 +264,7 @@ __global__ void __maxnreg__(96)
     buf[f * S + hw_swz<Q>(k)] = X;
   }
   __syncthreads();
-  if (hw < NFI) hw_row_fft<Q, true, true>(buf + hw * S, lane, mask, twH, twN);
+  if (hw < NFI) hw_row_fft<Q, true, true>(buf + hw * S, lane, mask, tw2, tw3, twN);
   __syncthreads();
 
   const float or2 = (float)a.or2[r], or4 = (float)a.or4[r], ost2 = (float)t.ost2[row];
@@ -320,7 +317,7 @@ __global__ void __maxnreg__(96)
   if (tid == 0) atomicMax(&a.vh2max[r], (unsigned long long)__double_as_longlong(vmh + 0.0));
   if (r == 0 || r == a.n_r - 1) return;
   __syncthreads();
-  if (hw < NFO) hw_row_fft<Q, false, false>(buf + hw * S, lane, mask, twH, twN);
+  if (hw < NFO) hw_row_fft<Q, false, false>(buf + hw * S, lane, mask, tw2, tw3, twN);
   __syncthreads();
   const float ws = (float)(t.wq[row] / (2 * H)), wv = (float)(t.wq_v[row] / (2 * H));
   float* Gr = a.G + (int64_t)(row & 1) * a.g_h + (int64_t)j * a.g_j + (int64_t)(r - 1) * a.g_level;
@@ -338,9 +335,11 @@ template <bool MAG, bool CHEM, int Q>
 static int launch_hw(const NlSplitArgs& a, cudaStream_t st) {
   using BF = SplitFields<MAG, CHEM>;
   constexpr int H = 16 * Q;
-  const size_t sm = ((size_t)BF::NB * (H + 1) + 2 * H) * sizeof(cplx<float>);
+  const size_t sm = ((size_t)BF::NB * (H + 1) + 15 * Q + H) * sizeof(cplx<float>);
   auto kern = k_nl_bouss_split_hw<MAG, CHEM, Q>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
   dim3 grid(a.t.n_theta, a.n_r);
   kern<<<grid, hw_threads<MAG, CHEM>(), sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());

@@ -44,21 +44,24 @@ struct SplitAnaArgs {
   Tables t;
   SplitTables s;
   int wk_max;           // max rows of the analysis table images
-  const float* G;       // [m][north|south][theta pair][level * g_level + 2 field + re/im]
+  const float* G;       // [m][north|south][theta pair][level * g_level + column]
   int64_t g_m, g_h, g_j, g_level;  // g_level: floats per level, multiple of 4
   int n_lev;            // levels of G
-  int stg_lev;          // levels one 128-row tile can touch
-  int nrows, row_per_level;
-  RowOp ops[32];
-  double2* out[16];     // (lm_max, ld) outputs, one per output field
+  int cols;             // Fourier columns per level (2 per grid output field)
+  int lev_tile;         // levels per 128-row tile: floor(128 / cols)
+  int n_out;            // spectral outputs; ops[2 o + re/im] is output o's row program
+  RowOp ops[32];        // tP/tD name grid output fields (column 2 t + c)
+  double2* out[16];     // (lm_max, ld) outputs
   int64_t ld;
   int out_col0;
+  uint8_t* aimg;        // folded A-operand images (workspace), anal_split_image_bytes
   int* err;
 };
 
 int launch_synth_split(const SplitSynArgs& a, cudaStream_t st);
 size_t synth_split_image_bytes(int nrows, int64_t total_chunks);
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st);
+size_t anal_split_image_bytes(int n_m, int nhs, int n_lev, int lev_tile);
 
 struct NlSplitArgs {
   Tables t;
