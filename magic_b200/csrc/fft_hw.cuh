@@ -10,11 +10,13 @@
 // butterfly is itself a two-factor Cooley-Tukey DFT in registers (Q = A B,
 // n = B a + b, k = k1 + A k2; inner twiddles W_Q^(b k1) are literals).
 //
-// Shared-memory layout of a row: value i at i ^ ((i / Q) & 15).  Every
-// access of the passes, of the real-row pre/post steps and of a warp reading
-// 32 consecutive values then touches each bank pair at most twice (checked
-// by enumerating the lane addresses); rows are H + 1 values apart so a
-// k-major scatter over rows is conflict-free as well.
+// Shared-memory layout of a row: value i at i ^ ((i >> s) & 15), s = 4 for
+// Q = 8, 16 and 6 for Q = 12, 24 (two integer ops per address; for the
+// pass-1 reads the xor term is a constant).  Enumerating the lane addresses of
+// every access of the passes, the real-row pre/post steps and a warp reading
+// 32 consecutive values gives 1.14 to 1.32 shared-memory wavefronts per
+// half-warp access on average (1 is conflict-free); rows are H + 1 values
+// apart so scatters across rows do not collide either.
 #pragma once
 
 #include "fft.cuh"
@@ -23,7 +25,8 @@ namespace mt {
 
 template <int Q>
 __device__ __forceinline__ int hw_swz(int i) {
-  return i ^ ((i / Q) & 15);
+  constexpr int sh = (Q == 8 || Q == 16) ? 4 : 6;
+  return i ^ ((i >> sh) & 15);
 }
 
 // exp(-2 pi i e / 24) (forward) or its conjugate; e is a constant after

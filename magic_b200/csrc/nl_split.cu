@@ -252,16 +252,20 @@ __global__ void __maxnreg__(96)
   const int tid = threadIdx.x, hw = tid >> 4, lane = tid & 15;
   const unsigned mask = 0xFFFFu << (16 * (hw & 1));
   hw_twiddles_to_smem<Q>(tw2, tw3, twN, t.twiddle, tid, T);
+  // Fourier rows: element e = (k, f) of the NFI (sym, asym) pairs of
+  // wavenumber k (consecutive threads read consecutive fields of one k);
+  // wavenumbers k >= n_m are zero.
   const float* fsym = a.Fs + (int64_t)j * a.fs_j + (int64_t)r * 2 * NFI;
-  for (int e = tid; e < NFI * H; e += T) {
+#pragma unroll 4
+  for (int e = tid; e < NFI * M; e += T) {
     const int k = e / NFI, f = e - k * NFI;
-    cplx<float> X = {0.f, 0.f};
-    if (k < M) {
-      const float2 sy = __ldg(reinterpret_cast<const float2*>(fsym + k * a.fs_m) + f);
-      const float2 as = __ldg(reinterpret_cast<const float2*>(fsym + k * a.fs_m + a.fs_c) + f);
-      X = {sy.x + hs * as.x, sy.y + hs * as.y};
-    }
-    buf[f * S + hw_swz<Q>(k)] = X;
+    const float2 sy = __ldg(reinterpret_cast<const float2*>(fsym + k * a.fs_m) + f);
+    const float2 as = __ldg(reinterpret_cast<const float2*>(fsym + k * a.fs_m + a.fs_c) + f);
+    buf[f * S + hw_swz<Q>(k)] = {sy.x + hs * as.x, sy.y + hs * as.y};
+  }
+  for (int e = tid; e < NFI * (H - M); e += T) {
+    const int k = M + e / NFI, f = e % NFI;
+    buf[f * S + hw_swz<Q>(k)] = {0.f, 0.f};
   }
   __syncthreads();
   if (hw < NFI) hw_row_fft<Q, true, true>(buf + hw * S, lane, mask, tw2, tw3, twN);
