@@ -116,13 +116,16 @@ __global__ void __launch_bounds__(kPackThreads, 4) k_syn_pack(SplitSynArgs a) {
   const int nlev = min(a.stg_lev, a.n_lev - lev0);
   double2* d = reinterpret_cast<double2*>(smem);
   {
-    const int per = 32 * nlev, total = a.narr * per;
-    for (int e = tid; e < total; e += kPackThreads) {
-      const int ia = e / per, rem = e - ia * per;
-      const int kk = rem / nlev, lvv = rem - kk * nlev;
+    // thread -> (kk, level) of the chunk, looping over the source arrays;
+    // l - m beyond the spectrum is zero-filled (no global read)
+    for (int e = tid; e < 32 * a.stg_lev; e += kPackThreads) {
+      const int kk = e / a.stg_lev, lvv = e - kk * a.stg_lev;
+      if (lvv >= nlev) continue;
       const int k = 32 * c + kk;
-      const double2* src = a.arr[ia] + (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
-      cp_async16_zfill(&d[(ia * 32 + kk) * a.stg_lev + lvv], src, k < nlm ? 16u : 0u);
+      const int64_t off = (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
+      const uint32_t bytes = k < nlm ? 16u : 0u;
+      for (int ia = 0; ia < a.narr; ++ia)
+        cp_async16_zfill(&d[(ia * 32 + kk) * a.stg_lev + lvv], a.arr[ia] + off, bytes);
     }
     cp_async_commit();
     cp_async_wait0();
@@ -138,27 +141,25 @@ __global__ void __launch_bounds__(kPackThreads, 4) k_syn_pack(SplitSynArgs a) {
     const int qf = live ? R - lev * a.row_per_level : 0;
     const int lv = lev - lev0;
     const RowOp op = a.ops[qf];
-    const int code = q ? op.kD : op.kP;
-    const int cpart = q ? op.cD : op.cP;
     const TermIx tm = a.term[q ? op.tD : op.tP];
-    const float f = (float)coef_value(code, (double)m);
-    const float or2l = live ? (float)a.or2[lev] : 0.f;
+    const int cpart = q ? op.cD : op.cP;
+    // value = f * (mul(l) * src_a - cw * src_b), branch-free over the recipes:
+    //   raw: mul = 1; dlh: mul = l(l+1); curl: mul = or2 l(l+1), cw = 1
+    const float f = live ? (float)coef_value(q ? op.kD : op.kP, (double)m) : 0.f;
+    const float dl = tm.recipe == kRaw ? 0.f : 1.f;
+    const float o2 = tm.recipe == kCurlT ? (float)a.or2[lev] : 1.f;
+    const float cw = tm.recipe == kCurlT ? 1.f : 0.f;
+    const double2* xa = d + tm.ia * 32 * a.stg_lev + lv;
+    const double2* xb = d + tm.ib * 32 * a.stg_lev + lv;
     float v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int kk = 2 * i + p;
-      v[i] = 0.f;
-      if (live && code && 32 * c + kk < nlm) {
-        const float l = (float)(m + 32 * c + kk);
-        const double2 x2 = d[(tm.ia * 32 + kk) * a.stg_lev + lv];
-        float x = (float)(cpart ? x2.y : x2.x);
-        if (tm.recipe == kDlh) x *= l * (l + 1.f);
-        else if (tm.recipe == kCurlT) {
-          const double2 w = d[(tm.ib * 32 + kk) * a.stg_lev + lv];
-          x = or2l * l * (l + 1.f) * x - (float)(cpart ? w.y : w.x);
-        }
-        v[i] = f * x;
-      }
+      const float l = (float)(m + 32 * c + kk);
+      const float mul = o2 * (1.f + dl * (l * (l + 1.f) - 1.f));
+      const double2 x2 = xa[kk * a.stg_lev], w2 = xb[kk * a.stg_lev];
+      const float x = (float)(cpart ? x2.y : x2.x), w = (float)(cpart ? w2.y : w2.x);
+      v[i] = f != 0.f ? f * (mul * x - (cw != 0.f ? w : 0.f)) : 0.f;
     }
     const int combo = q == 0 ? p : 1 - p;
     uint8_t* dst = a.aimg + syn_img_chunk(a.total_chunks, rt, a.s.syn_chunk_prefix[mc * 2 + combo],
@@ -345,14 +346,14 @@ __global__ void __launch_bounds__(kPackThreads, 4) k_ana_pack(SplitAnaArgs a) {
   float* d = reinterpret_cast<float*>(smem);
   {
     const float* gm = a.G + (int64_t)mc * a.g_m + (int64_t)lev0 * gl;
+    // warp -> (hemisphere, theta pair) rows, lanes -> consecutive 16-byte pieces
     const int cpl = nlev * gl / 4;  // 16-byte pieces per (hemisphere, theta pair)
-    const int total = 2 * kSplitKC * cpl;
-    for (int e = tid; e < total; e += kPackThreads) {
-      const int hj = e / cpl, p4 = e - hj * cpl;
-      const int h = hj / kSplitKC, jl = hj - h * kSplitKC;
-      const int j = kSplitKC * c + jl;
-      const float* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j + 4 * p4;
-      cp_async16_zfill(d + hj * rowlen + 4 * p4, src, j < t.nhs ? 16u : 0u);
+    for (int hj = tid >> 5; hj < 2 * kSplitKC; hj += kPackThreads / 32) {
+      const int h = hj / kSplitKC, j = kSplitKC * c + hj % kSplitKC;
+      const float* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j;
+      const uint32_t bytes = j < t.nhs ? 16u : 0u;
+      for (int p4 = tid & 31; p4 < cpl; p4 += 32)
+        cp_async16_zfill(d + hj * rowlen + 4 * p4, src + 4 * p4, bytes);
     }
     cp_async_commit();
     cp_async_wait0();
