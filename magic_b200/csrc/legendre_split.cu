@@ -103,7 +103,7 @@ __host__ __device__ inline int64_t syn_img_chunk(int64_t total_chunks, int rt, i
   return (((int64_t)rt * total_chunks + prefix + c) * 2 + q);
 }
 
-__global__ void __launch_bounds__(kPackThreads, 4) k_syn_pack(SplitSynArgs a) {
+__global__ void __launch_bounds__(kPackThreads, 6) k_syn_pack(SplitSynArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const Tables& t = a.t;
   const int rt = blockIdx.x, c = blockIdx.y, mc = blockIdx.z;
@@ -333,7 +333,7 @@ __host__ __device__ inline int64_t ana_img_chunk(int n_m, int nchj, int rt, int 
   return (((int64_t)rt * n_m + mc) * 2 + fold) * nchj + c;
 }
 
-__global__ void __launch_bounds__(kPackThreads, 4) k_ana_pack(SplitAnaArgs a) {
+__global__ void __launch_bounds__(kPackThreads, 8) k_ana_pack(SplitAnaArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const Tables& t = a.t;
   const int rt = blockIdx.x, c = blockIdx.y, mc = blockIdx.z;
@@ -477,12 +477,31 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
   const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 12);
   tc_fence_after();
   if (__syncthreads_and(ok && !*abort_flag)) {
-    // every copy landed and every MMA finished: the stages are free for the exchange
+    // every copy landed and every MMA finished: the stages are free for the
+    // exchange buffer and the per-CTA tables of the row programs
     constexpr int XS = 17;  // padded row of 16 columns
     float* xch = reinterpret_cast<float*>(smem);  // [2][128][XS]
+    double* cf = reinterpret_cast<double*>(smem + 2 * kSplitRows * XS * sizeof(float));
+    int* colx = reinterpret_cast<int*>(cf + 64);  // exchange row of each term (acc1 rows + 128)
+    double* osc = reinterpret_cast<double*>(colx + 64);  // 1/(l(l+1)) of l - m = 2 kk + par
     const int lev0 = rt * a.lev_tile;
     const int nlev = min(a.lev_tile, a.n_lev - lev0);
     const double dm = (double)m;
+    for (int q = tid; q < 2 * a.n_out; q += kGemmThreads) {
+      const RowOp op = a.ops[q];
+      cf[2 * q] = coef_value(op.kP, dm);
+      cf[2 * q + 1] = coef_value(op.kD, dm);
+      colx[2 * q] = 2 * op.tP + op.cP;
+      colx[2 * q + 1] = kSplitRows + 2 * op.tD + op.cD;
+    }
+    for (int kk = tid; kk < wk; kk += kGemmThreads) {
+      const double l = (double)(m + 2 * kk + par);
+      osc[kk] = l > 0.0 ? 1.0 / (l * (l + 1.0)) : 0.0;
+    }
+    // task = (output o, column i, level slot lv), lv fastest: consecutive
+    // threads write consecutive levels of one (output, l)
+    const int lvs = a.lev_tile <= 8 ? 3 : 4;
+    const int ntask = a.n_out << (4 + lvs);
     for (int c0 = 0; c0 < wk; c0 += 16) {
       float v[16];
       tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
@@ -492,24 +511,19 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
 #pragma unroll
       for (int i = 0; i < 16; ++i) xch[(kSplitRows + tid) * XS + i] = v[i];
       __syncthreads();
-      const int ntask = a.n_out * 16 * nlev;
       for (int task = tid; task < ntask; task += kGemmThreads) {
-        const int lv = task % nlev, rest = task / nlev;
-        const int i = rest % 16, o = rest / 16;
-        const int k = 2 * (c0 + i) + par;
-        if (k >= nlm) continue;
-        double re_im[2];
-#pragma unroll
-        for (int comp = 0; comp < 2; ++comp) {
-          const RowOp op = a.ops[2 * o + comp];
-          const float* x0 = xch + (lv * a.cols + 2 * op.tP + op.cP) * XS + i;
-          const float* x1 = xch + (kSplitRows + lv * a.cols + 2 * op.tD + op.cD) * XS + i;
-          re_im[comp] = coef_value(op.kP, dm) * (double)*x0 + coef_value(op.kD, dm) * (double)*x1;
-        }
-        const double l = (double)(m + k);
-        const double sc = a.ops[2 * o].scale ? (m + k > 0 ? 1.0 / (l * (l + 1.0)) : 0.0) : 1.0;
-        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] =
-            make_double2(sc * re_im[0], sc * re_im[1]);
+        const int lv = task & ((1 << lvs) - 1), rest = task >> lvs;
+        const int i = rest & 15, o = rest >> 4;
+        const int kk = c0 + i, k = 2 * kk + par;
+        if (lv >= nlev || k >= nlm) continue;
+        const int base = lv * a.cols;
+        const int q = 4 * o;
+        const double re = cf[q] * (double)xch[(base + colx[q]) * XS + i] +
+                          cf[q + 1] * (double)xch[(base + colx[q + 1]) * XS + i];
+        const double im = cf[q + 2] * (double)xch[(base + colx[q + 2]) * XS + i] +
+                          cf[q + 3] * (double)xch[(base + colx[q + 3]) * XS + i];
+        const double sc = a.ops[2 * o].scale ? osc[kk] : 1.0;
+        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] = make_double2(sc * re, sc * im);
       }
       __syncthreads();
     }
