@@ -80,8 +80,13 @@ __device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, uin
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// Staged source values of one synthesis chunk: array ia, l - m offset kk,
+// level lv at double2 index ia * syn_stage_pitch + kk * stg_lev + lv.  The
+// pitch is odd so lanes reading different arrays at one (kk, lv) hit
+// different banks.
+__host__ __device__ inline int syn_stage_pitch(int stg_lev) { return 32 * stg_lev + 1; }
 __host__ __device__ inline uint32_t syn_staging_bytes(int narr, int stg_lev) {
-  return (uint32_t)narr * 32 * stg_lev * 16;
+  return (uint32_t)narr * syn_stage_pitch(stg_lev) * 16;
 }
 
 // ------------------------------------------------------------- synthesis
@@ -115,6 +120,7 @@ __global__ void __launch_bounds__(kPackThreads, 6) k_syn_pack(SplitSynArgs a) {
   const int lev0 = (rt * kSplitRows) / a.row_per_level;
   const int nlev = min(a.stg_lev, a.n_lev - lev0);
   double2* d = reinterpret_cast<double2*>(smem);
+  const int pitch = syn_stage_pitch(a.stg_lev);
   {
     // thread -> (kk, level) of the chunk, looping over the source arrays;
     // l - m beyond the spectrum is zero-filled (no global read)
@@ -125,7 +131,7 @@ __global__ void __launch_bounds__(kPackThreads, 6) k_syn_pack(SplitSynArgs a) {
       const int64_t off = (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
       const uint32_t bytes = k < nlm ? 16u : 0u;
       for (int ia = 0; ia < a.narr; ++ia)
-        cp_async16_zfill(&d[(ia * 32 + kk) * a.stg_lev + lvv], a.arr[ia] + off, bytes);
+        cp_async16_zfill(&d[ia * pitch + kk * a.stg_lev + lvv], a.arr[ia] + off, bytes);
     }
     cp_async_commit();
     cp_async_wait0();
@@ -149,17 +155,18 @@ __global__ void __launch_bounds__(kPackThreads, 6) k_syn_pack(SplitSynArgs a) {
     const float dl = tm.recipe == kRaw ? 0.f : 1.f;
     const float o2 = tm.recipe == kCurlT ? (float)a.or2[lev] : 1.f;
     const float cw = tm.recipe == kCurlT ? 1.f : 0.f;
-    const double2* xa = d + tm.ia * 32 * a.stg_lev + lv;
-    const double2* xb = d + tm.ib * 32 * a.stg_lev + lv;
+    const double* xa = reinterpret_cast<const double*>(d + tm.ia * pitch + lv) + cpart;
+    const double* xb = reinterpret_cast<const double*>(d + tm.ib * pitch + lv) + cpart;
+    const int kst = 2 * a.stg_lev;  // doubles between consecutive kk
     float v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int kk = 2 * i + p;
       const float l = (float)(m + 32 * c + kk);
       const float mul = o2 * (1.f + dl * (l * (l + 1.f) - 1.f));
-      const double2 x2 = xa[kk * a.stg_lev], w2 = xb[kk * a.stg_lev];
-      const float x = (float)(cpart ? x2.y : x2.x), w = (float)(cpart ? w2.y : w2.x);
-      v[i] = f != 0.f ? f * (mul * x - (cw != 0.f ? w : 0.f)) : 0.f;
+      const float x = (float)xa[kk * kst];
+      const float w = cw != 0.f ? (float)xb[kk * kst] : 0.f;
+      v[i] = f != 0.f ? f * (mul * x - w) : 0.f;
     }
     const int combo = q == 0 ? p : 1 - p;
     uint8_t* dst = a.aimg + syn_img_chunk(a.total_chunks, rt, a.s.syn_chunk_prefix[mc * 2 + combo],
