@@ -29,6 +29,14 @@ __device__ __forceinline__ int hw_swz(int i) {
   return i ^ ((i >> sh) & 15);
 }
 
+// hw_swz(lane + 16 t) for lane < 16 and a compile-time t: the xor mask then
+// depends on t only, so the address is (lane ^ const) + const.
+template <int Q>
+__device__ __forceinline__ int hw_swz16(int lane, int t) {
+  constexpr int sh = (Q == 8 || Q == 16) ? 4 : 6;
+  return (lane ^ ((t >> (sh - 4)) & 15)) + 16 * t;
+}
+
 // exp(-2 pi i e / 24) (forward) or its conjugate; e is a constant after
 // unrolling, so the switch folds to literals (cos/sin of multiples of 15 deg).
 template <bool INV>
@@ -151,7 +159,7 @@ __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned 
 #pragma unroll
   for (int r = 0; r < Q; ++r) {
     const int k = lane + 16 * r;
-    cplx<float> x = row[hw_swz<Q>(k)];
+    cplx<float> x = row[hw_swz16<Q>(lane, r)];
     if constexpr (PRE) {
       cplx<float> xc = row[hw_swz<Q>((H - k) % H)];
       if (k == 0) {
@@ -171,7 +179,7 @@ __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned 
 #pragma unroll
   for (int it = 0; it < NBF; ++it)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[hw_swz<Q>(lane + 16 * it + 4 * Q * r)];
+    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[hw_swz16<Q>(lane, it + Q / 4 * r)];
   __syncwarp(mask);
 #pragma unroll
   for (int it = 0; it < NBF; ++it) {
@@ -193,7 +201,7 @@ __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned 
 #pragma unroll
   for (int it = 0; it < NBF; ++it)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[hw_swz<Q>(lane + 16 * it + 4 * Q * r)];
+    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[hw_swz16<Q>(lane, it + Q / 4 * r)];
   __syncwarp(mask);
 #pragma unroll
   for (int it = 0; it < NBF; ++it) {
@@ -207,7 +215,7 @@ __device__ __forceinline__ void hw_row_fft(cplx<float>* row, int lane, unsigned 
     }
     dft_small<4, INV>(u);
 #pragma unroll
-    for (int r = 0; r < 4; ++r) row[hw_swz<Q>(j + 4 * Q * r)] = u[r];
+    for (int r = 0; r < 4; ++r) row[hw_swz16<Q>(lane, it + Q / 4 * r)] = u[r];
   }
   __syncwarp(mask);
 }
