@@ -339,31 +339,32 @@ def main():
     # --- end to end through the public API with pinned host buffers: every
     # step copies its 11 input spectra host->device and its 8 output spectra and
     # the Courant steps device->host; copies of neighbouring steps overlap the
-    # stage on separate streams (double-buffered device inputs and outputs).
+    # stage on separate streams (NB buffer sets of device inputs and outputs).
     if args.no_e2e:
         if rank == 0:
             print(json.dumps({"levels": n_r, "ms_per_step": ms, "kernel_ms": part_ms}), flush=True)
         return
     host_in = {k: v.cpu().pin_memory() for k, v in fields.items()}
-    dev_in = [{k: torch.empty_like(v) for k, v in fields.items()} for _ in range(2)]
-    dev_out = [{k: torch.zeros_like(v) for k, v in out.items()} for _ in range(2)]
+    NB = 3
+    dev_in = [{k: torch.empty_like(v) for k, v in fields.items()} for _ in range(NB)]
+    dev_out = [{k: torch.zeros_like(v) for k, v in out.items()} for _ in range(NB)]
     host_out = [{k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in out.items()}
-                for _ in range(2)]
-    host_dt = [torch.empty(2, n_r, dtype=torch.float64).pin_memory() for _ in range(2)]
+                for _ in range(NB)]
+    host_dt = [torch.empty(2, n_r, dtype=torch.float64).pin_memory() for _ in range(NB)]
     h2d = sum(v.numel() * v.element_size() for v in host_in.values())
     d2h = sum(v.numel() * v.element_size() for v in host_out[0].values()) + host_dt[0].numel() * 8
     s_in = torch.cuda.Stream(dev)
     s_out = torch.cuda.Stream(dev)
     ev = lambda: torch.cuda.Event()
-    used = [ev(), ev()]      # stage of buffer b finished (inputs free, outputs ready)
-    copied = [ev(), ev()]    # inputs of buffer b on the device
-    drained = [ev(), ev()]   # outputs of buffer b on the host
-    for b in range(2):
+    used = [ev() for _ in range(NB)]     # stage of buffer b finished (inputs free, outputs ready)
+    copied = [ev() for _ in range(NB)]   # inputs of buffer b on the device
+    drained = [ev() for _ in range(NB)]  # outputs of buffer b on the host
+    for b in range(NB):
         used[b].record(stream)
         drained[b].record(stream)
 
     def e2e_step(i):
-        b = i % 2
+        b = i % NB
         with torch.cuda.stream(s_in):
             s_in.wait_event(used[b])
             for k in FIELDS:
@@ -382,18 +383,18 @@ def main():
             host_dt[b][1].copy_(dth, non_blocking=True)
             drained[b].record(s_out)
 
-    for i in range(2):
+    for i in range(NB):
         e2e_step(i)
     torch.cuda.synchronize()
-    k_e2e = max(3, args.steps // 2)
+    k_e2e = max(10, args.steps)
     barrier()
     torch.cuda.synchronize()
     a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a_ev.record(stream)
     for i in range(k_e2e):
         e2e_step(i)
-    stream.wait_event(drained[(k_e2e - 1) % 2])
-    stream.wait_event(drained[k_e2e % 2])
+    for b in range(NB):
+        stream.wait_event(drained[b])
     b_ev.record(stream)
     torch.cuda.synchronize()
     barrier()
