@@ -61,6 +61,139 @@ static size_t fourier_bytes(const mt_plan* p, int64_t ncols) {
 
 using namespace mt;
 
+namespace mt {
+
+// ---- split-precision drop-in transforms -----------------------------------
+//
+// Synthesis: packing + tcgen05 GEMM (legendre_split.cu) with the batch
+// columns in place of radial levels, then the FP32 phi stage
+// (split_transforms.cu) writes the FP64 grids.  Analysis: FP32 phi stage,
+// then folding + tcgen05 GEMM.  Workspace: [error int | Fourier rows | operand
+// images].
+
+struct SplitTrWs {
+  size_t f, img, total;
+};
+
+static RowOp rop(int tP, int cP, int kP, int tD = 0, int cD = 0, int kD = 0, int scale = 0);
+static void syn_group_ops(RowOp* ops, int Q, int S, int T);
+static int ana_scalar_ops(RowOp* ops, int x);
+static int ana_s_ops(RowOp* ops, int a, int b);
+static int ana_t_ops(RowOp* ops, int a, int b);
+
+static SplitTrWs split_tr_ws(const mt_plan* p, int B, int nf) {
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t rows = (size_t)B * 2 * nf;
+  const size_t gl = (size_t)((2 * nf + 3) & ~3);
+  const size_t fs = (size_t)p->n_m * 2 * p->nhs * rows * sizeof(float);
+  const size_t g = (size_t)p->n_m * 2 * p->nhs * B * gl * sizeof(float);
+  const size_t img = std::max(synth_split_image_bytes((int)rows, split_syn_total_chunks(p)),
+                              anal_split_image_bytes(p->n_m, p->nhs, B, 128 / (2 * nf)));
+  SplitTrWs w;
+  w.f = 256;
+  w.img = w.f + al(std::max(fs, g));
+  w.total = w.img + al(img);
+  return w;
+}
+
+// Synthesis of nf grid fields per column from narr spectral arrays; terms and
+// row programs (2 nf per column) as in the fused stage.
+static int split_synth_tr(const mt_plan* p, int B, int nf, int narr, const double* const* arr,
+                          int64_t ld, const TermIx* terms, int nterms, const RowOp* ops,
+                          double* const* out, void* work, cudaStream_t st) {
+  const SplitTrWs W = split_tr_ws(p, B, nf);
+  char* w = (char*)work;
+  int* err = (int*)w;
+  MT_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  SplitSynArgs s{};
+  s.t = p->tab;
+  s.s = split_tables(p);
+  for (int i = 0; i < narr; ++i) s.arr[i] = (const double2*)arr[i];
+  s.narr = narr;
+  for (int i = 0; i < nterms; ++i) s.term[i] = terms[i];
+  s.ld = ld;
+  s.or2 = nullptr;
+  s.n_lev = B;
+  s.row_per_level = 2 * nf;
+  s.nrows = B * 2 * nf;
+  s.stg_lev = std::min(B, 127 / s.row_per_level + 2);
+  for (int i = 0; i < 2 * nf; ++i) s.ops[i] = ops[i];
+  s.Fs = (float*)(w + W.f);
+  s.fs_j = s.nrows;
+  s.fs_c = (int64_t)p->nhs * s.fs_j;
+  s.fs_m = 2 * s.fs_c;
+  s.aimg = (uint8_t*)(w + W.img);
+  s.total_chunks = split_syn_total_chunks(p);
+  s.err = err;
+  MT_TRY(launch_synth_split(s, st));
+  SplitPhiArgs f{};
+  f.t = p->tab;
+  f.nrows = B * nf;
+  f.nf = nf;
+  f.Fs = s.Fs;
+  f.fs_m = s.fs_m;
+  f.fs_c = s.fs_c;
+  f.fs_j = s.fs_j;
+  for (int i = 0; i < nf; ++i) f.out[i] = out[i];
+  return launch_split_phi(true, f, st);
+}
+
+// Analysis of nf grid fields per column into n_out spectral outputs.
+static int split_anal_tr(const mt_plan* p, int B, int nf, int vector_mask,
+                         const double* const* in, int n_out, const RowOp* ops, double* const* out,
+                         int64_t ld, void* work, cudaStream_t st) {
+  const SplitTrWs W = split_tr_ws(p, B, nf);
+  char* w = (char*)work;
+  int* err = (int*)w;
+  MT_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  SplitPhiArgs f{};
+  f.t = p->tab;
+  f.nrows = B * nf;
+  f.nf = nf;
+  f.vector_mask = vector_mask;
+  f.G = (float*)(w + W.f);
+  f.g_level = (2 * nf + 3) & ~3;
+  f.g_j = (int64_t)B * f.g_level;
+  f.g_h = (int64_t)p->nhs * f.g_j;
+  f.g_m = 2 * f.g_h;
+  for (int i = 0; i < nf; ++i) f.in[i] = in[i];
+  MT_TRY(launch_split_phi(false, f, st));
+  SplitAnaArgs a{};
+  a.t = p->tab;
+  a.s = split_tables(p);
+  {
+    const std::vector<int>& wk = split_wk_host(p);
+    a.wk_max = *std::max_element(wk.begin(), wk.end());
+  }
+  a.G = f.G;
+  a.g_m = f.g_m;
+  a.g_h = f.g_h;
+  a.g_j = f.g_j;
+  a.g_level = f.g_level;
+  a.n_lev = B;
+  a.cols = 2 * nf;
+  a.lev_tile = 128 / a.cols;
+  a.n_out = n_out;
+  for (int i = 0; i < 2 * n_out; ++i) a.ops[i] = ops[i];
+  for (int i = 0; i < n_out; ++i) a.out[i] = (double2*)out[i];
+  a.ld = ld;
+  a.out_col0 = 0;
+  a.aimg = (uint8_t*)(w + W.img);
+  a.err = err;
+  return launch_anal_split(a, st);
+}
+
+static TermIx term_ix(int ia, int recipe) {
+  TermIx x;
+  x.ia = (int8_t)ia;
+  x.ib = 0;
+  x.recipe = (int8_t)recipe;
+  x.pad = 0;
+  return x;
+}
+
+}  // namespace mt
+
 extern "C" {
 
 const char* mt_last_error(void) { return g_err.c_str(); }
@@ -158,6 +291,7 @@ int mt_plan_copy_tables(const mt_plan* p, double* theta, double* gauss, double* 
 
 size_t mt_transform_workspace(const mt_plan* p, int B, int n_fields) {
   if (!p || B < 1 || n_fields < 1) return 0;
+  if (p->precision == MT_PREC_SPLIT) return split_tr_ws(p, B, n_fields).total;
   return fourier_bytes(p, (int64_t)B * n_fields);
 }
 
@@ -174,6 +308,11 @@ int mt_scal_to_spat(const mt_plan* p, const double* Slm, int64_t ld, int B, doub
   MT_REQUIRE(Slm && grid && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
   MT_TRY(check_ws(p, B, 1, work_bytes, work));
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_SPLIT) {
+    const TermIx tm[1] = {term_ix(0, kRaw)};
+    const RowOp ops[2] = {rop(0, 0, 1), rop(0, 1, 1)};
+    return split_synth_tr(p, B, 1, 1, &Slm, ld, tm, 1, ops, &grid, work, st);
+  }
   double2* F = (double2*)work;
   SynthArgs<1> s{};
   s.t = p->tab;
@@ -247,6 +386,14 @@ int mt_scal_to_grad_spat(const mt_plan* p, const double* Slm, int64_t ld, int B,
   MT_REQUIRE(Slm && gt && gp && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
   MT_TRY(check_ws(p, B, 2, work_bytes, work));
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_SPLIT) {
+    // theta = dP.S, phi = i m P.S
+    const TermIx tm[1] = {term_ix(0, scale_dlh ? kDlh : kRaw)};
+    const RowOp ops[4] = {rop(0, 0, 0, 0, 0, 1), rop(0, 0, 0, 0, 1, 1), rop(0, 1, 4),
+                          rop(0, 0, 3)};
+    double* outs[2] = {gt, gp};
+    return split_synth_tr(p, B, 2, 1, &Slm, ld, tm, 1, ops, outs, work, st);
+  }
   double2* F = (double2*)work;
   SynthArgs<1> s{};
   s.t = p->tab;
@@ -278,6 +425,14 @@ int mt_torpol_to_spat(const mt_plan* p, const double* Q, const double* S, const 
   MT_REQUIRE(Q && S && T && br && bt && bp && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
   MT_TRY(check_ws(p, B, 3, work_bytes, work));
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_SPLIT) {
+    const TermIx tm[3] = {term_ix(0, kRaw), term_ix(1, kRaw), term_ix(2, kRaw)};
+    RowOp ops[6];
+    syn_group_ops(ops, 0, 1, 2);
+    const double* arrs[3] = {Q, S, T};
+    double* outs[3] = {br, bt, bp};
+    return split_synth_tr(p, B, 3, 3, arrs, ld, tm, 3, ops, outs, work, st);
+  }
   double2* F = (double2*)work;
   SynthArgs<3> s{};
   s.t = p->tab;
@@ -311,6 +466,11 @@ int mt_scal_to_SH(const mt_plan* p, const double* grid, int B, double* Slm, int6
   MT_REQUIRE(Slm && grid && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
   MT_TRY(check_ws(p, B, 1, work_bytes, work));
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_SPLIT) {
+    RowOp ops[2];
+    ana_scalar_ops(ops, 0);
+    return split_anal_tr(p, B, 1, 0, &grid, 1, ops, &Slm, ld, work, st);
+  }
   double2* F = (double2*)work;
   ToFourierArgs f{};
   f.t = p->tab;
@@ -342,6 +502,14 @@ int mt_spat_to_sphertor(const mt_plan* p, const double* vt, const double* vp, in
   MT_REQUIRE(vt && vp && S && T && ld >= B, MT_ERR_ARG, "bad spectral/grid argument");
   MT_TRY(check_ws(p, B, 2, work_bytes, work));
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_SPLIT) {
+    RowOp ops[4];
+    ana_s_ops(ops, 0, 1);
+    ana_t_ops(ops + 2, 0, 1);
+    const double* ins[2] = {vt, vp};
+    double* outs[2] = {S, T};
+    return split_anal_tr(p, B, 2, 3, ins, 2, ops, outs, ld, work, st);
+  }
   double2* F = (double2*)work;
   ToFourierArgs f{};
   f.t = p->tab;
@@ -649,7 +817,7 @@ static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
   return w;
 }
 
-static RowOp rop(int tP, int cP, int kP, int tD = 0, int cD = 0, int kD = 0, int scale = 0) {
+static RowOp rop(int tP, int cP, int kP, int tD, int cD, int kD, int scale) {
   RowOp o;
   o.tP = (int8_t)tP;
   o.cP = (int8_t)cP;

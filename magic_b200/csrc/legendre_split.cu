@@ -507,7 +507,8 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
     }
     // task = (output o, column i, level slot lv), lv fastest: consecutive
     // threads write consecutive levels of one (output, l)
-    const int lvs = a.lev_tile <= 8 ? 3 : 4;
+    int lvs = 0;  // level slot: smallest power of two >= lev_tile
+    while ((1 << lvs) < a.lev_tile) ++lvs;
     const int ntask = a.n_out << (4 + lvs);
     for (int c0 = 0; c0 < wk; c0 += 16) {
       float v[16];

@@ -79,4 +79,20 @@ struct NlSplitArgs {
 
 int launch_nl_bouss_split(bool mag, bool chem, const NlSplitArgs& a, cudaStream_t st);
 
+// phi stage of the split drop-in transforms (split_transforms.cu); rows are
+// (column b, field f), r = b * nf + f
+struct SplitPhiArgs {
+  Tables t;
+  int nrows;            // B * nf
+  int nf;               // fields per column
+  int vector_mask;      // bit f: field f takes the vector weight 2 pi w / sin^2 (analysis)
+  const float* Fs;      // synthesis output [m][sym|asym][theta pair][2 r + re/im]
+  int64_t fs_m, fs_c, fs_j;
+  float* G;             // analysis input [m][north|south][theta pair][b * g_level + 2 f + re/im]
+  int64_t g_m, g_h, g_j, g_level;
+  double* out[3];       // synthesis: grids (B, n_theta, n_phi) per field
+  const double* in[3];  // analysis: grids per field
+};
+int launch_split_phi(bool to_grid, const SplitPhiArgs& a, cudaStream_t st);
+
 }  // namespace mt
