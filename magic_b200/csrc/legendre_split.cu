@@ -188,136 +188,195 @@ struct GemmSmem {
   __host__ __device__ size_t total() const { return bar_off + 8 * (2 * kGemmStages + 1) + 16; }
 };
 
-// Warp 0 lane 0 bulk-copies the A image chunk and the table chunk of each K
-// step, warp 1 lane 0 issues the six plane products per step, warp 2 owns
-// TMEM; all four warps run the epilogue (one TMEM lane = one output row per
-// thread).  K steps: chunk c of the P table (parity combo), then chunk c of
-// the dP table (the other parity), skipping chunks a table does not have.
-__global__ void __launch_bounds__(kGemmThreads, 2) k_synth_gemm(SplitSynArgs a) {
+// Persistent synthesis GEMM: one CTA per SM walks the work items
+// (tile, sym/asym, theta tile, m) with a stride of gridDim.x.  Warp 0 lane 0
+// bulk-copies the A image chunk and the table chunk of every K step into a
+// kPStages ring, warp 1 lane 0 issues the six plane products per step into
+// one of two TMEM accumulators (columns 0 and 256) and commits it when the
+// item's K loop ends, warps 2-9 drain the other accumulator into Fs (warp w
+// reads TMEM lanes 32 (w % 4) ..., warps w and w + 4 split the columns) and
+// hand it back.  K steps of an item:
+// chunk c of the P table (parity combo), then chunk c of the dP table (the
+// other parity), skipping chunks a table does not have.
+constexpr int kPStages = 5;
+constexpr int kPEpiWarps = 8;  // two per TMEM lane quarter, each half of the columns
+constexpr int kPThreads = 64 + 32 * kPEpiWarps;
+
+struct PSmem {
+  uint32_t stage_bytes, bar_off;
+  __host__ __device__ explicit PSmem(int brows)
+      : stage_bytes(kImgChunk + 3 * (uint32_t)brows * 32),
+        bar_off(kPStages * (kImgChunk + 3 * (uint32_t)brows * 32)) {}
+  // full/empty per stage, tfull/tempty per accumulator, done, tmem slot, abort flag
+  __host__ __device__ size_t total() const { return bar_off + 8 * (2 * kPStages + 5) + 16; }
+};
+
+__global__ void __launch_bounds__(kPThreads, 1) k_synth_gemm(SplitSynArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   const Tables& t = a.t;
   const SplitTables& st = a.s;
   const int wth = st.wth;
-  const GemmSmem L(wth);
+  const PSmem L(wth);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bar_off);
-  uint64_t* empty = full + kGemmStages;
-  uint64_t* accb = empty + kGemmStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  uint64_t* empty = full + kPStages;
+  uint64_t* tfull = empty + kPStages;  // [2] accumulator ready
+  uint64_t* tempty = tfull + 2;        // [2] accumulator drained
+  uint64_t* done = tempty + 2;         // every MMA issued by this CTA finished
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   // an earlier CTA already timed out: skip the work so a fault costs one wait, not one per CTA
   if (*(volatile int*)a.err) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int rt = blockIdx.x;
-  const int combo = blockIdx.y & 1, tau = blockIdx.y >> 1;
-  const int mc = blockIdx.z;
-  const int m = mc * t.minc;
-  const int nlm = t.l_max - m + 1;
-  const int par_t[2] = {combo, 1 - combo};  // parity of l - m contracted with P, dP
-  int nch_t[2];
-  for (int q = 0; q < 2; ++q) nch_t[q] = (split_nk(nlm, par_t[q]) + kSplitKC - 1) / kSplitKC;
-  const int nch = max(nch_t[0], nch_t[1]);
-  const uint32_t tcols = wth <= 32 ? 32 : (wth <= 64 ? 64 : (wth <= 128 ? 128 : 256));
+  const int ntiles = (a.nrows + kSplitRows - 1) / kSplitRows, ny = 2 * st.nthtile;
+  const int nitems = ntiles * ny * t.n_m;
+  struct Item {
+    int rt, combo, tau, mc, nlm, nch_t[2];
+  };
+  auto decode = [&](int item) {
+    Item it;
+    it.rt = item % ntiles;
+    const int r = item / ntiles, y = r % ny;
+    it.mc = r / ny;
+    it.combo = y & 1;
+    it.tau = y >> 1;
+    it.nlm = t.l_max - it.mc * t.minc + 1;
+    it.nch_t[0] = (split_nk(it.nlm, it.combo) + kSplitKC - 1) / kSplitKC;
+    it.nch_t[1] = (split_nk(it.nlm, 1 - it.combo) + kSplitKC - 1) / kSplitKC;
+    return it;
+  };
 
   if (tid == 0) {
-    for (int s = 0; s < kGemmStages; ++s) {
+    for (int s = 0; s < kPStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accb, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 32 * kPEpiWarps);
+    }
+    mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 2) tmem_alloc(tmem_slot, tcols);
+  if (warp == 1) tmem_alloc(tmem_slot, 512);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
 
-  if (warp == 0 && lane == 0) {
+  if (warp == 0) {
     // ---------------- loader ----------------
-    const uint8_t* aimg =
-        a.aimg + syn_img_chunk(a.total_chunks, rt, st.syn_chunk_prefix[mc * 2 + combo], 0, 0) *
-                     kImgChunk;
-    const uint8_t* img[2];
-    for (int q = 0; q < 2; ++q)
-      img[q] = st.syn + st.syn_off[((mc * 2 + q) * 2 + par_t[q]) * st.nthtile + tau];
-    const uint32_t bchunk = 3 * L.b_plane;
-    int step = 0;
-    bool ok = true;
-    for (int c = 0; c < nch && ok; ++c) {
-      for (int q = 0; q < 2; ++q) {
-        if (c >= nch_t[q]) continue;
-        const int s = step % kGemmStages;
-        if (step >= kGemmStages &&
-            !mbar_wait(&empty[s], ((step / kGemmStages) - 1) & 1, abort_flag, a.err, 3)) {
-          ok = false;
-          break;
+    if (lane == 0) {
+      const uint32_t bchunk = 3 * (uint32_t)wth * 32;
+      int g = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+        const Item it = decode(item);
+        const uint8_t* aimg =
+            a.aimg + syn_img_chunk(a.total_chunks, it.rt,
+                                   st.syn_chunk_prefix[it.mc * 2 + it.combo], 0, 0) * kImgChunk;
+        const uint8_t* img[2];
+        for (int q = 0; q < 2; ++q)
+          img[q] = st.syn + st.syn_off[((it.mc * 2 + q) * 2 + (q ? 1 - it.combo : it.combo)) *
+                                           st.nthtile + it.tau];
+        const int nch = max(it.nch_t[0], it.nch_t[1]);
+        for (int c = 0; c < nch && ok; ++c) {
+          for (int q = 0; q < 2; ++q) {
+            if (c >= it.nch_t[q]) continue;
+            const int s = g % kPStages;
+            if (g >= kPStages &&
+                !mbar_wait(&empty[s], ((g / kPStages) - 1) & 1, abort_flag, a.err, 3)) {
+              ok = false;
+              break;
+            }
+            uint8_t* stage = smem + s * L.stage_bytes;
+            mbar_expect_tx(&full[s], kImgChunk + bchunk);
+            bulk_g2s(stage, aimg + (int64_t)(2 * c + q) * kImgChunk, kImgChunk, &full[s]);
+            bulk_g2s(stage + kImgChunk, img[q] + (int64_t)c * bchunk, bchunk, &full[s]);
+            ++g;
+          }
         }
-        uint8_t* stage = smem + s * L.stage_bytes;
-        mbar_expect_tx(&full[s], kImgChunk + bchunk);
-        bulk_g2s(stage, aimg + (int64_t)(2 * c + q) * kImgChunk, kImgChunk, &full[s]);
-        bulk_g2s(stage + kImgChunk, img[q] + (int64_t)c * bchunk, bchunk, &full[s]);
-        ++step;
       }
+      // every issued copy must land before the CTA may exit
+      for (int k = max(0, g - kPStages); k < g; ++k)
+        mbar_drain(&full[k % kPStages], (k / kPStages) & 1);
     }
-    // drain: every issued copy must land before the CTA may exit
-    for (int k = max(0, step - kGemmStages); k < step; ++k)
-      mbar_wait(&full[k % kGemmStages], (k / kGemmStages) & 1, abort_flag, nullptr, 0);
-  } else if (warp == 1 && lane == 0) {
+  } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
-    const uint32_t idesc = umma_idesc_bf16(kSplitRows, wth);
-    uint32_t acc = 0;
-    int step = 0;
-    bool ok = true;
-    for (int c = 0; c < nch && ok; ++c) {
-      for (int q = 0; q < 2; ++q) {
-        if (c >= nch_t[q]) continue;
-        const int s = step % kGemmStages;
-        if (!mbar_wait(&full[s], (step / kGemmStages) & 1, abort_flag, a.err, 4)) {
-          ok = false;
-          break;
-        }
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16(kSplitRows, wth);
+      int g = 0, n = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x, ++n) {
+        const Item it = decode(item);
+        const int buf = n & 1;
+        if (n >= 2 && !mbar_wait(&tempty[buf], ((n >> 1) - 1) & 1, abort_flag, a.err, 6)) break;
         tc_fence_after();
-        const uint32_t sa = smem_u32(smem + s * L.stage_bytes);
-        const uint32_t sb = sa + kImgChunk;
+        const uint32_t acc_col = tbase + 256u * buf;
+        uint32_t acc = 0;
+        const int nch = max(it.nch_t[0], it.nch_t[1]);
+        for (int c = 0; c < nch && ok; ++c) {
+          for (int q = 0; q < 2; ++q) {
+            if (c >= it.nch_t[q]) continue;
+            const int s = g % kPStages;
+            if (!mbar_wait(&full[s], (g / kPStages) & 1, abort_flag, a.err, 4)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(smem + s * L.stage_bytes);
+            const uint32_t sb = sa + kImgChunk;
 #pragma unroll
-        for (int pp = 0; pp < 6; ++pp) {
-          const uint64_t da = umma_desc(sa + kPairA[pp] * kImgPlane, 128, 256);
-          const uint64_t db = umma_desc(sb + kPairB[pp] * L.b_plane, 128, 256);
-          umma_bf16(tbase, da, db, idesc, acc);
-          acc = 1;
+            for (int pp = 0; pp < 6; ++pp) {
+              const uint64_t da = umma_desc(sa + kPairA[pp] * kImgPlane, 128, 256);
+              const uint64_t db = umma_desc(sb + kPairB[pp] * (uint32_t)wth * 32, 128, 256);
+              umma_bf16(acc_col, da, db, idesc, acc);
+              acc = 1;
+            }
+            umma_commit(&empty[s]);
+            ++g;
+          }
         }
-        umma_commit(&empty[s]);
-        ++step;
+        if (ok) umma_commit(&tfull[buf]);
       }
+      umma_commit(done);  // arrives once every MMA above has finished
     }
-    umma_commit(accb);  // also on abort: lets the epilogue wait finish after in-flight MMAs
+  } else {
+    // ---------------- epilogue (warps 2-9) ----------------
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
+    int n = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++n) {
+      const int buf = n & 1;
+      const bool ok = mbar_wait(&tfull[buf], (n >> 1) & 1, abort_flag, a.err, 2);
+      if (!__all_sync(0xffffffffu, ok && !*abort_flag)) break;
+      tc_fence_after();
+      const Item it = decode(item);
+      const int R = it.rt * kSplitRows + quarter * 32 + lane;
+      float* out = a.Fs + (int64_t)it.mc * a.fs_m + (int64_t)it.combo * a.fs_c;
+      const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16) + 256u * buf;
+      for (int c0 = 16 * half; c0 < wth; c0 += 32) {
+        float v[16];
+        tmem_ld16(taddr + c0, v);
+        if (R < a.nrows) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int th = it.tau * wth + c0 + i;
+            if (th < t.nhs) out[(int64_t)th * a.fs_j + R] = v[i];
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty[buf]);
+    }
   }
   __syncwarp();
-  // ---------------- epilogue ----------------
-  const bool ok = mbar_wait(accb, 0, abort_flag, a.err, 2);
-  tc_fence_after();
-  if (__all_sync(0xffffffffu, ok && !*abort_flag)) {
-    const int R = rt * kSplitRows + tid;
-    float* out = a.Fs + (int64_t)mc * a.fs_m + (int64_t)combo * a.fs_c;
-    for (int c0 = 0; c0 < wth; c0 += 16) {
-      float v[16];
-      tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
-      if (R < a.nrows) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int th = tau * wth + c0 + i;
-          if (th < t.nhs) out[(int64_t)th * a.fs_j + R] = v[i];
-        }
-      }
-    }
-  }
+  if (warp == 1) mbar_drain(done, 0);  // no MMA may still write TMEM at dealloc
   tc_fence_before();
   __syncthreads();
-  if (warp == 2) {
+  if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tbase, tcols);
+    tmem_dealloc(tbase, 512);
   }
 }
 
@@ -451,7 +510,7 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
       }
     }
     for (int k = max(0, step - kGemmStages); k < step; ++k)
-      mbar_wait(&full[k % kGemmStages], (k / kGemmStages) & 1, abort_flag, nullptr, 0);
+      mbar_drain(&full[k % kGemmStages], (k / kGemmStages) & 1);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
     const uint32_t idesc = umma_idesc_bf16(kSplitRows, wk);
@@ -552,12 +611,15 @@ int launch_synth_split(const SplitSynArgs& a, cudaStream_t st) {
   dim3 pgrid(ntiles, syn_nchunks(a.t.l_max + 1, 0), a.t.n_m);
   k_syn_pack<<<pgrid, kPackThreads, pack_sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
-  const GemmSmem L(a.s.wth);
+  const PSmem L(a.s.wth);
   const size_t sm = L.total();
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_synth_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-  dim3 grid(ntiles, 2 * a.s.nthtile, a.t.n_m);
-  k_synth_gemm<<<grid, kGemmThreads, sm, st>>>(a);
+  int dev = 0, nsm = 148;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_CHECK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int nitems = ntiles * 2 * a.s.nthtile * a.t.n_m;
+  k_synth_gemm<<<std::min(nitems, nsm), kPThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
