@@ -212,6 +212,41 @@ MT_API int mt_nl_bouss(const mt_plan* plan, int n_r, const mt_bouss_in* in,
                 const mt_bouss_out* out, const mt_bouss_params* p, double* dtrkc,
                 double* dthkc, void* work, size_t work_bytes, void* stream);
 
+/* ---- fused anelastic nonlinear stage (split precision) --------------------
+ * The nonlinear part of radial_loop_anel (magic_torch/step_time.py:1215-1475):
+ * Legendre synthesis of the 18 grid fields (19 with composition; velocity and
+ * its derivatives zero on the two boundary levels as in the reference),
+ * get_nl_anel products with viscous and Ohmic heating (get_nl_anel.py:41-136)
+ * and Courant maxima in the phi stage, Legendre analysis of the bulk levels.
+ * Requires a plan created with MT_PREC_SPLIT (FP64 callers compose the
+ * drop-in transforms and mt_get_nl_anel exactly as radial_loop_anel does).
+ * Inputs: spectral (lm_max, ld) complex over n_r levels; b .. dj NULL
+ * without magnetic field, xi NULL without composition. */
+typedef struct {
+  const double *w, *dw, *ddw, *z, *dz, *s, *xi, *b, *db, *ddb, *aj, *dj;
+  int64_t ld;
+} mt_anel_in;
+
+/* Outputs over the bulk levels (columns 1..n_r-2): AdvrLM, AdvtLM, AdvpLM,
+ * dVSrLM, VStLM, VxBrLM, VxBtLM, VxBpLM, dVXirLM, VXitLM, heatTermsLM (the
+ * magnetic and composition ones may be NULL when their inputs are). */
+typedef struct {
+  double *Advr, *Advt, *Advp, *VSr, *VSt, *VxBr, *VxBt, *VxBp, *VXir, *VXit, *heat;
+  int64_t ld;
+} mt_anel_out;
+
+typedef struct {
+  const double *r, *or1, *or2, *or4, *beta, *orho1, *orho2, *otemp1, *visc,
+      *lambda_, *delxr2, *delxh2; /* (n_r) */
+  double LFfac, ViscHeatFac, OhmLossFac, courfac, alffac, opm;
+  int l_mag, l_chem, cour_mode; /* cour_mode as mt_courant_params.mode */
+} mt_anel_stage_params;
+
+MT_API size_t mt_nl_anel_workspace(const mt_plan* plan, int n_r, int l_mag, int l_chem);
+MT_API int mt_nl_anel(const mt_plan* plan, int n_r, const mt_anel_in* in,
+               const mt_anel_out* out, const mt_anel_stage_params* p, double* dtrkc,
+               double* dthkc, void* work, size_t work_bytes, void* stream);
+
 /* Thread-local message for the last non-zero status. */
 MT_API const char* mt_last_error(void);
 

@@ -58,6 +58,24 @@ class BoussParams(C.Structure):
                 ("cour_mode", C.c_int), ("parts", C.c_int)]
 
 
+class AnelIn(C.Structure):
+    _fields_ = [(n, _dp) for n in ("w", "dw", "ddw", "z", "dz", "s", "xi", "b", "db", "ddb",
+                                   "aj", "dj")] + [("ld", _i64)]
+
+
+class AnelOut(C.Structure):
+    _fields_ = [(n, _dp) for n in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp",
+                                   "VXir", "VXit", "heat")] + [("ld", _i64)]
+
+
+class AnelStageParams(C.Structure):
+    _fields_ = [(n, _dp) for n in ("r", "or1", "or2", "or4", "beta", "orho1", "orho2", "otemp1",
+                                   "visc", "lambda_", "delxr2", "delxh2")] + \
+               [(n, C.c_double) for n in ("LFfac", "ViscHeatFac", "OhmLossFac", "courfac",
+                                          "alffac", "opm")] + \
+               [("l_mag", C.c_int), ("l_chem", C.c_int), ("cour_mode", C.c_int)]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "mt_plan_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
@@ -84,6 +102,9 @@ _PROTOS = {
     "mt_nl_bouss_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "mt_nl_bouss": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(BoussIn), C.POINTER(BoussOut),
                               C.POINTER(BoussParams), _dp, _dp, _dp, C.c_size_t, _dp]),
+    "mt_nl_anel_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "mt_nl_anel": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(AnelIn), C.POINTER(AnelOut),
+                             C.POINTER(AnelStageParams), _dp, _dp, _dp, C.c_size_t, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }
 

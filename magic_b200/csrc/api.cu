@@ -798,10 +798,11 @@ struct SplitWs {
   int64_t rows_syn, rows_nl, g_level;
 };
 
-static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
+// Workspace of a split stage with nfi grid fields in and nfo products out.
+static SplitWs split_stage_ws(const mt_plan* p, int n_r, int nfi, int nfo) {
   SplitWs w;
-  w.rows_syn = (int64_t)n_r * 2 * bouss_nfi(mag, chem);
-  w.g_level = (2 * bouss_nfo(mag, chem) + 3) & ~3;  // floats per level, 16-byte multiple
+  w.rows_syn = (int64_t)n_r * 2 * nfi;
+  w.g_level = (2 * nfo + 3) & ~3;  // floats per level, 16-byte multiple
   w.rows_nl = (int64_t)(n_r - 2) * w.g_level;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   w.err = 0;
@@ -811,11 +812,18 @@ static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
   w.aimg = w.mx + al(2 * (size_t)n_r * sizeof(unsigned long long));
   // A-operand images: the synthesis ones are dead before the analysis writes its own
   const size_t syn = synth_split_image_bytes((int)w.rows_syn, split_syn_total_chunks(p));
-  const size_t ana = anal_split_image_bytes(p->n_m, p->nhs, n_r - 2,
-                                            128 / (2 * bouss_nfo(mag, chem)));
+  const size_t ana = anal_split_image_bytes(p->n_m, p->nhs, n_r - 2, 128 / (2 * nfo));
   w.total = w.aimg + al(std::max(syn, ana));
   return w;
 }
+
+static SplitWs split_ws(const mt_plan* p, int n_r, int mag, int chem) {
+  return split_stage_ws(p, n_r, bouss_nfi(mag, chem), bouss_nfo(mag, chem));
+}
+
+// anelastic stage: grid fields in, products out (nl_anel_split.cu)
+static int anel_nfi(int mag, int chem) { return 12 + (chem ? 1 : 0) + (mag ? 6 : 0); }
+static int anel_nfo(int mag, int chem) { return 7 + (mag ? 3 : 0) + (chem ? 3 : 0); }
 
 static RowOp rop(int tP, int cP, int kP, int tD, int cD, int kD, int scale) {
   RowOp o;
@@ -1019,6 +1027,185 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
 
 }  // namespace mt
 
+namespace mt {
+
+// Fused anelastic stage in split precision: synthesis (input assembly of
+// radial_loop_anel, magic_torch/step_time.py:1233-1316), phi stage
+// (nl_anel_split.cu), analysis of the bulk levels (:1329-1391), Courant steps.
+template <bool MAG, bool CHEM>
+static int nl_anel_split_t(const mt_plan* p, int n_r, const mt_anel_in* in,
+                           const mt_anel_out* out, const mt_anel_stage_params* q, double* dtrkc,
+                           double* dthkc, void* work, cudaStream_t st) {
+  const int nfi = anel_nfi(MAG, CHEM), nfo = anel_nfo(MAG, CHEM);
+  const SplitWs W = split_stage_ws(p, n_r, nfi, nfo);
+  char* w = (char*)work;
+  int* err = (int*)(w + W.err);
+  float* Fs = (float*)(w + W.fs);
+  float* Gs = (float*)(w + W.gs);
+  unsigned long long* mx = (unsigned long long*)(w + W.mx);
+  const int64_t fs_j = W.rows_syn, fs_c = (int64_t)p->nhs * fs_j, fs_m = 2 * fs_c;
+  const int64_t g_j = W.rows_nl, g_h = (int64_t)p->nhs * g_j, g_m = 2 * g_h;
+  MT_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  {
+    SplitSynArgs s{};
+    s.t = p->tab;
+    s.s = split_tables(p);
+    int na = 0;
+    auto arr = [&](const double* ptr) {
+      s.arr[na] = (const double2*)ptr;
+      return na++;
+    };
+    int x = 0;
+    auto term = [&](int ia, int ib, int recipe) {
+      s.term[x].ia = (int8_t)ia;
+      s.term[x].ib = (int8_t)ib;
+      s.term[x].recipe = (int8_t)recipe;
+      s.term[x].pad = 0;
+      return x++;
+    };
+    const int iw = arr(in->w), idw = arr(in->dw), iddw = arr(in->ddw), iz = arr(in->z),
+              idz = arr(in->dz), is = arr(in->s);
+    const int tQv = term(iw, 0, kDlh), tdw = term(idw, 0, kRaw), tz = term(iz, 0, kRaw);
+    const int tQd = term(idw, 0, kDlh), tddw = term(iddw, 0, kRaw), tdz = term(idz, 0, kRaw);
+    const int tcv = term(iz, 0, kDlh), ts = term(is, 0, kRaw);
+    RowOp* o = s.ops;
+    syn_group_ops(o, tQv, tdw, tz);       // vr vt vp
+    syn_group_ops(o + 6, tQd, tddw, tdz);  // dvrdr dvtdr dvpdr
+    // dvrdt, dvrdp = grad of l(l+1) w: (dP X, i m P X)
+    o[12] = rop(0, 0, 0, tQv, 0, 1);
+    o[13] = rop(0, 0, 0, tQv, 1, 1);
+    o[14] = rop(tQv, 1, 4);
+    o[15] = rop(tQv, 0, 3);
+    // dvtdp, dvpdp before 1/sin^2: theta = i m dP dw - m^2 P z, phi = -m^2 P dw - i m dP z
+    o[16] = rop(tz, 0, 5, tdw, 1, 4);
+    o[17] = rop(tz, 1, 5, tdw, 0, 3);
+    o[18] = rop(tdw, 0, 5, tz, 1, 3);
+    o[19] = rop(tdw, 1, 5, tz, 0, 4);
+    ana_scalar_ops(o + 20, tcv);  // cvr = l(l+1) z
+    ana_scalar_ops(o + 22, ts);   // s
+    int rows = 24;
+    if (CHEM) {
+      const int ixi = arr(in->xi);
+      ana_scalar_ops(o + rows, term(ixi, 0, kRaw));
+      rows += 2;
+    }
+    if (MAG) {
+      const int ib = arr(in->b), idb = arr(in->db), iaj = arr(in->aj), idj = arr(in->dj),
+                iddb = arr(in->ddb);
+      const int tQb = term(ib, 0, kDlh), tdb = term(idb, 0, kRaw), taj = term(iaj, 0, kRaw);
+      const int tQa = term(iaj, 0, kDlh), tdj = term(idj, 0, kRaw), tcT = term(ib, iddb, kCurlT);
+      syn_group_ops(o + rows, tQb, tdb, taj);
+      syn_group_ops(o + rows + 6, tQa, tdj, tcT);
+      rows += 12;
+    }
+    s.narr = na;
+    s.n_lev = n_r;
+    s.ld = in->ld;
+    s.or2 = q->or2;
+    s.row_per_level = rows;
+    s.nrows = n_r * rows;
+    s.stg_lev = std::min(n_r, 127 / rows + 2);
+    s.Fs = Fs;
+    s.fs_m = fs_m;
+    s.fs_c = fs_c;
+    s.fs_j = fs_j;
+    s.aimg = (uint8_t*)(w + W.aimg);
+    s.total_chunks = split_syn_total_chunks(p);
+    s.err = err;
+    MT_TRY(launch_synth_split(s, st));
+  }
+  {
+    MT_CHECK_CUDA(cudaMemsetAsync(mx, 0, 2 * n_r * sizeof(unsigned long long), st));
+    NlAnelArgs nl{};
+    nl.t = p->tab;
+    nl.n_r = n_r;
+    nl.Fs = Fs;
+    nl.fs_m = fs_m;
+    nl.fs_c = fs_c;
+    nl.fs_j = fs_j;
+    nl.G = Gs;
+    nl.g_m = g_m;
+    nl.g_h = g_h;
+    nl.g_j = g_j;
+    nl.g_level = W.g_level;
+    nl.r = q->r;
+    nl.or1 = q->or1;
+    nl.or2 = q->or2;
+    nl.or4 = q->or4;
+    nl.beta = q->beta;
+    nl.orho1 = q->orho1;
+    nl.orho2 = q->orho2;
+    nl.otemp1 = q->otemp1;
+    nl.visc = q->visc;
+    nl.lambda_ = q->lambda_;
+    nl.delxr2 = q->delxr2;
+    nl.delxh2 = q->delxh2;
+    nl.LFfac = q->LFfac;
+    nl.ViscHeatFac = q->ViscHeatFac;
+    nl.OhmLossFac = MAG ? q->OhmLossFac : 0.0;
+    nl.cour_mode = MAG ? q->cour_mode : 0;
+    nl.cf2 = q->courfac * q->courfac;
+    nl.af2 = q->alffac * q->alffac;
+    const double h = 0.5 * (1.0 + q->opm);
+    nl.valfac = h * h;
+    nl.vr2max = mx;
+    nl.vh2max = mx + n_r;
+    MT_TRY(launch_nl_anel_split(MAG, CHEM, nl, st));
+  }
+  SplitAnaArgs a{};
+  a.t = p->tab;
+  a.s = split_tables(p);
+  {
+    const std::vector<int>& wk = split_wk_host(p);
+    a.wk_max = *std::max_element(wk.begin(), wk.end());
+  }
+  a.G = Gs;
+  a.g_m = g_m;
+  a.g_h = g_h;
+  a.g_j = g_j;
+  a.g_level = W.g_level;
+  a.n_lev = n_r - 2;
+  int o = 0, r = 0;
+  r += ana_scalar_ops(&a.ops[r], 0);
+  a.out[o++] = (double2*)out->Advr;
+  r += ana_s_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advt;
+  r += ana_t_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advp;
+  r += ana_scalar_ops(&a.ops[r], 3);
+  a.out[o++] = (double2*)out->VSr;
+  r += ana_s_ops(&a.ops[r], 4, 5);
+  a.out[o++] = (double2*)out->VSt;
+  if (MAG) {
+    r += ana_scalar_ops(&a.ops[r], 6);
+    a.out[o++] = (double2*)out->VxBr;
+    r += ana_s_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBt;
+    r += ana_t_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBp;
+  }
+  if (CHEM) {
+    const int x0 = MAG ? 9 : 6;
+    r += ana_scalar_ops(&a.ops[r], x0);
+    a.out[o++] = (double2*)out->VXir;
+    r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
+    a.out[o++] = (double2*)out->VXit;
+  }
+  r += ana_scalar_ops(&a.ops[r], nfo - 1);
+  a.out[o++] = (double2*)out->heat;
+  a.n_out = o;
+  a.cols = 2 * nfo;
+  a.lev_tile = 128 / a.cols;
+  a.ld = out->ld;
+  a.out_col0 = 1;
+  a.aimg = (uint8_t*)(w + W.aimg);
+  a.err = err;
+  MT_TRY(launch_anal_split(a, st));
+  return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
+}
+
+}  // namespace mt
+
 extern "C" {
 
 size_t mt_nl_bouss_workspace(const mt_plan* p, int n_r, int l_mag, int l_chem) {
@@ -1061,6 +1248,45 @@ int mt_nl_bouss(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt_bouss
                      : nl_bouss_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
   return q->l_chem ? nl_bouss_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
                    : nl_bouss_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+}
+
+
+size_t mt_nl_anel_workspace(const mt_plan* p, int n_r, int l_mag, int l_chem) {
+  if (!p || n_r < 3 || p->precision != MT_PREC_SPLIT) return 0;
+  return split_stage_ws(p, n_r, anel_nfi(l_mag, l_chem), anel_nfo(l_mag, l_chem)).total;
+}
+
+int mt_nl_anel(const mt_plan* p, int n_r, const mt_anel_in* in, const mt_anel_out* out,
+               const mt_anel_stage_params* q, double* dtrkc, double* dthkc, void* work,
+               size_t work_bytes, void* stream) {
+  MT_TRY(check_plan(p));
+  MT_REQUIRE(p->precision == MT_PREC_SPLIT, MT_ERR_UNSUPPORTED,
+             "mt_nl_anel needs a MT_PREC_SPLIT plan (FP64 callers compose the drop-in "
+             "transforms and mt_get_nl_anel as radial_loop_anel does)");
+  MT_REQUIRE(in && out && q && dtrkc && dthkc && n_r >= 3, MT_ERR_ARG, "bad argument");
+  MT_REQUIRE(in->w && in->dw && in->ddw && in->z && in->dz && in->s, MT_ERR_ARG,
+             "null velocity/entropy input");
+  MT_REQUIRE(!q->l_mag || (in->b && in->db && in->ddb && in->aj && in->dj), MT_ERR_ARG,
+             "null magnetic input");
+  MT_REQUIRE(!q->l_chem || in->xi, MT_ERR_ARG, "null composition input");
+  MT_REQUIRE(in->ld >= n_r && out->ld >= n_r, MT_ERR_ARG, "ld >= n_r required");
+  MT_REQUIRE(out->Advr && out->Advt && out->Advp && out->VSr && out->VSt && out->heat,
+             MT_ERR_ARG, "null output");
+  MT_REQUIRE(!q->l_mag || (out->VxBr && out->VxBt && out->VxBp), MT_ERR_ARG,
+             "null magnetic output");
+  MT_REQUIRE(!q->l_chem || (out->VXir && out->VXit), MT_ERR_ARG, "null composition output");
+  MT_REQUIRE(q->r && q->or1 && q->or2 && q->or4 && q->beta && q->orho1 && q->orho2 && q->otemp1 &&
+                 q->visc && q->lambda_ && q->delxr2 && q->delxh2,
+             MT_ERR_ARG, "null radial profile");
+  MT_REQUIRE(q->cour_mode >= 0 && q->cour_mode <= 2, MT_ERR_ARG, "bad cour_mode");
+  MT_REQUIRE(work && work_bytes >= mt_nl_anel_workspace(p, n_r, q->l_mag, q->l_chem),
+             MT_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (q->l_mag)
+    return q->l_chem ? nl_anel_split_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                     : nl_anel_split_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+  return q->l_chem ? nl_anel_split_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                   : nl_anel_split_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
 }
 
 }  // extern "C"

@@ -39,6 +39,7 @@ __device__ __forceinline__ double coef_value(int code, double m) {
     case 2: return -1.0;
     case 3: return m;
     case 4: return -m;
+    case 5: return -m * m;
     default: return 0.0;
   }
 }

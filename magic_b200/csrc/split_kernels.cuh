@@ -8,7 +8,7 @@ namespace mt {
 
 // One output real component as a linear combination of two scaled sources:
 // value = coef(kP) * src(tP, cP) contracted with P + coef(kD) * src(tD, cD)
-// contracted with dP.  coef codes: 0 zero, 1 +1, 2 -1, 3 +m, 4 -m.
+// contracted with dP.  coef codes: 0 zero, 1 +1, 2 -1, 3 +m, 4 -m, 5 -m^2.
 // cP/cD select the real (0) or imaginary (1) part; scale = 1 divides the
 // analysis result by l(l+1) (0 for l = 0).
 struct RowOp {
@@ -32,7 +32,7 @@ struct SplitSynArgs {
   int nrows;            // n_lev * row_per_level
   int row_per_level;    // 2 * fields
   int stg_lev;          // levels one 128-row tile can touch (staging width)
-  RowOp ops[32];        // per (field, re/im) of a level
+  RowOp ops[40];        // per (field, re/im) of a level
   float* Fs;            // [m][sym|asym][theta pair][row]
   int64_t fs_m, fs_c, fs_j;
   uint8_t* aimg;        // A-operand images (workspace), synth_split_image_bytes
@@ -78,6 +78,23 @@ struct NlSplitArgs {
 };
 
 int launch_nl_bouss_split(bool mag, bool chem, const NlSplitArgs& a, cudaStream_t st);
+
+// phi stage of the fused anelastic stage (nl_anel_split.cu); Fs/G as NlSplitArgs
+struct NlAnelArgs {
+  Tables t;
+  int n_r;
+  const float* Fs;
+  int64_t fs_m, fs_c, fs_j;
+  float* G;
+  int64_t g_m, g_h, g_j, g_level;
+  const double *r, *or1, *or2, *or4, *beta, *orho1, *orho2, *otemp1, *visc, *lambda_, *delxr2,
+      *delxh2;
+  double LFfac, ViscHeatFac, OhmLossFac;
+  int cour_mode;
+  double cf2, af2, valfac;
+  unsigned long long *vr2max, *vh2max;
+};
+int launch_nl_anel_split(bool mag, bool chem, const NlAnelArgs& a, cudaStream_t st);
 
 // phi stage of the split drop-in transforms (split_transforms.cu); rows are
 // (column b, field f), r = b * nf + f

@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import check
+from ._lib import MagicError, check
 
 _CD = torch.complex128
 _RD = torch.float64
@@ -308,4 +308,59 @@ class Plan:
             work = self._work(need)
         check(L.mt_nl_bouss(self._h, n_r, C.byref(bi), C.byref(bo), C.byref(bp), _ptr(dtr),
                             _ptr(dth), _ptr(work), work.numel(), self._stream()))
+        return out, dtr, dth
+
+    def nl_anel_workspace(self, n_r, l_mag=True, l_chem=False):
+        return _lib.lib().mt_nl_anel_workspace(self._h, int(n_r), int(l_mag), int(l_chem))
+
+    def nl_anel(self, fields, prof, LFfac, ViscHeatFac, OhmLossFac, courfac, alffac, opm,
+                l_mag=True, l_chem=False, damp=True, out=None, work=None):
+        """Fused anelastic nonlinear stage (magic_torch/step_time.py:1215-1475: transforms,
+        get_nl_anel with viscous and Ohmic heating, forward transforms, CFL); split-precision
+        plans only.
+
+        ``fields``: dict of spectral (lm_max, n_r) complex128 arrays w, dw, ddw, z, dz, s
+        (+ b, db, ddb, aj, dj if l_mag, xi if l_chem).  ``prof``: r, or1, or2, or4, beta,
+        orho1, orho2, otemp1, visc, lambda_, delxr2, delxh2 over the n_r levels.  Returns
+        (outputs dict Advr Advt Advp VSr VSt [VxBr VxBt VxBp] [VXir VXit] heat, dtrkc,
+        dthkc); outputs are (lm_max, n_r) with boundary columns zero.
+        """
+        w = fields["w"]
+        n_r = w.shape[1]
+        L = _lib.lib()
+        need = L.mt_nl_anel_workspace(self._h, n_r, int(l_mag), int(l_chem))
+        if need == 0:
+            raise MagicError("nl_anel needs a precision='split' plan and n_r >= 3")
+        names = ["w", "dw", "ddw", "z", "dz", "s"] + (["b", "db", "ddb", "aj", "dj"] if l_mag
+                                                       else []) + (["xi"] if l_chem else [])
+        ins = {}
+        for k in names:
+            x = fields[k]
+            if x.shape != (self.lm_max, n_r) or x.dtype != _CD or x.device != self.device:
+                raise ValueError(f"fields[{k}]: expected ({self.lm_max}, {n_r}) complex128")
+            ins[k] = x.contiguous()
+        onames = ["Advr", "Advt", "Advp", "VSr", "VSt"] + (["VxBr", "VxBt", "VxBp"] if l_mag
+                                                           else []) + \
+            (["VXir", "VXit"] if l_chem else []) + ["heat"]
+        if out is None:
+            out = {k: torch.zeros(self.lm_max, n_r, dtype=_CD, device=self.device) for k in onames}
+        pnames = ("r", "or1", "or2", "or4", "beta", "orho1", "orho2", "otemp1", "visc",
+                  "lambda_", "delxr2", "delxh2")
+        keep = {k: self._prof(prof[k], n_r) for k in pnames}
+        ai = _lib.AnelIn(*[ins[k].data_ptr() if k in ins else None for k in
+                           ("w", "dw", "ddw", "z", "dz", "s", "xi", "b", "db", "ddb", "aj",
+                            "dj")], n_r)
+        ao = _lib.AnelOut(*[out[k].data_ptr() if k in out else None for k in
+                            ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp",
+                             "VXir", "VXit", "heat")], out["Advr"].stride(0))
+        ap = _lib.AnelStageParams(*[keep[k].data_ptr() for k in pnames], float(LFfac),
+                                  float(ViscHeatFac), float(OhmLossFac), float(courfac),
+                                  float(alffac), float(opm), int(l_mag), int(l_chem),
+                                  (1 if damp else 2) if l_mag else 0)
+        dtr = torch.empty(n_r, dtype=_RD, device=self.device)
+        dth = torch.empty_like(dtr)
+        if work is None or work.numel() < need:
+            work = self._work(need)
+        check(L.mt_nl_anel(self._h, n_r, C.byref(ai), C.byref(ao), C.byref(ap), _ptr(dtr),
+                           _ptr(dth), _ptr(work), work.numel(), self._stream()))
         return out, dtr, dth

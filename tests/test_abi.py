@@ -54,7 +54,8 @@ def test_struct_layouts_match_header(libpath, tmp_path):
     structs = {"mt_grid_desc": _lib.GridDesc, "mt_plan_info": _lib.PlanInfo,
                "mt_anel_params": _lib.AnelParams, "mt_courant_params": _lib.CourantParams,
                "mt_bouss_in": _lib.BoussIn, "mt_bouss_out": _lib.BoussOut,
-               "mt_bouss_params": _lib.BoussParams}
+               "mt_bouss_params": _lib.BoussParams, "mt_anel_in": _lib.AnelIn,
+               "mt_anel_out": _lib.AnelOut, "mt_anel_stage_params": _lib.AnelStageParams}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
              "int main(void){"]
     for cname, py in structs.items():

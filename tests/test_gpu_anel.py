@@ -1,0 +1,90 @@
+"""GPU parity of the split-precision fused anelastic stage (bf16x3 tcgen05
+Legendre GEMMs, FP32 phi stage with get_nl_anel, viscous and Ohmic heating)
+against the FP64 oracle restatement of radial_loop_anel
+(magic_torch/step_time.py:1215-1475).
+
+Tolerance: relative to the output's scale (the vector pair's max(|S|, |T|)
+for the S/T outputs), 2e-5 up to l_max = 127 and 5e-5 above, as for the
+Boussinesq stage; Courant steps 1e-5.  The l_max = 383 case (n_phi = 1152,
+block FFT) is the anelastic benchmark configuration's resolution with a few
+radial levels.  Measured on B200: 4e-7 to 1.5e-6 up to l_max = 42, up to
+1.8e-5 (Advt) at l_max = 127 and 2.2e-5 at l_max = 383.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import grid as og
+from oracle import stage as ostage
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    (16, 1, 5, True, False),
+    (32, 4, 6, True, True),
+    (20, 1, 5, False, True),
+    (42, 1, 4, False, False),
+    (127, 1, 4, True, False),
+    (255, 1, 3, True, True),
+    (383, 1, 3, True, False),
+]
+PAIR = {"Advt": "Advp", "Advp": "Advt", "VxBt": "VxBp", "VxBp": "VxBt"}
+
+
+def _fields(g, N, rng, l_mag, l_chem):
+    amp = (g.lm2l + 1.0) ** -1.5
+
+    def spec():
+        x = (rng.standard_normal((g.lm_max, N)) + 1j * rng.standard_normal((g.lm_max, N)))
+        x = x * amp[:, None]
+        x[g.lm2m == 0] = x[g.lm2m == 0].real
+        return x
+
+    names = ["w", "dw", "ddw", "z", "dz", "s"] + (["b", "db", "ddb", "aj", "dj"] if l_mag else [])
+    names += ["xi"] if l_chem else []
+    return {k: spec() for k in names}
+
+
+@pytest.mark.parametrize("l_max,minc,N,l_mag,l_chem", CASES)
+def test_split_anel_stage_matches_oracle(l_max, minc, N, l_mag, l_chem):
+    from magic_b200 import Plan
+
+    g = og.Grid(l_max, minc)
+    p = Plan(l_max, minc, precision="split")
+    rng = np.random.default_rng(7 * l_max + N)
+    f = _fields(g, N, rng, l_mag, l_chem)
+    prof = ostage.anel_profiles(N, l_max=l_max)
+    LF, vhf, ohm, cf, af, opm = 200.0, 0.3, 0.2, 2.5, 1.0, 0.2
+    ref, rdt, rdh = ostage.nl_anel_stage(g, f, prof, LF, vhf, ohm, cf, af, opm, l_mag, l_chem)
+    cu = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()
+    work = torch.zeros(p.nl_anel_workspace(N, l_mag, l_chem), dtype=torch.uint8, device="cuda")
+    out, dt, dh = p.nl_anel({k: cu(v) for k, v in f.items()}, {k: cu(v) for k, v in prof.items()},
+                            LF, vhf, ohm, cf, af, opm, l_mag=l_mag, l_chem=l_chem, work=work)
+    torch.cuda.synchronize()
+    assert int(work[:4].view(torch.int32).item()) == 0, "device wait timed out"
+    worst = {}
+    for k in ref:
+        got = out[k].cpu().numpy()
+        assert np.all(got[:, 0] == 0) and np.all(got[:, -1] == 0), k
+        scale = np.abs(ref[k]).max()
+        if k in PAIR:
+            scale = max(scale, np.abs(ref[PAIR[k]]).max())
+        worst[k] = np.abs(got - ref[k]).max() / scale
+    print("split anel stage errors", {k: f"{v:.2e}" for k, v in worst.items()})
+    tol = 2e-5 if l_max <= 127 else 5e-5
+    for k, v in worst.items():
+        assert v < tol, (k, v)
+    assert np.abs(dt.cpu().numpy() - rdt).max() / np.abs(rdt).max() < 1e-5
+    assert np.abs(dh.cpu().numpy() - rdh).max() / np.abs(rdh).max() < 1e-5
+
+
+def test_anel_requires_split_plan():
+    from magic_b200 import Plan
+    from magic_b200._lib import MagicError
+
+    p = Plan(16, 1)
+    with pytest.raises(MagicError):
+        p.nl_anel({k: torch.zeros(p.lm_max, 4, dtype=torch.complex128, device="cuda")
+                   for k in ["w", "dw", "ddw", "z", "dz", "s"]}, {}, 1.0, 0.0, 0.0, 1.0, 1.0, 1.0,
+                  l_mag=False)
