@@ -232,6 +232,59 @@ def cpu_stage_sample(n_levels=5, seed=0):
                       f"table build {build_s:.1f} s excluded"}
 
 
+def run_anel(args, rank, world):
+    """Optional line: the fused anelastic stage at the anelastic benchmark
+    resolution (l_max = 383, n_theta = 576, n_phi = 1152, n_r = 129, hydrodynamic,
+    split precision), device-timed with inputs resident."""
+    from magic_b200 import Plan
+    from magic_b200.profiles import anelastic_profiles
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    l_max, n_r = 383, args.levels if args.levels != N_R else 129
+    plan = Plan(l_max, 1, precision="split", device=dev)
+    g = torch.Generator(device="cpu").manual_seed(rank)
+    l = torch.as_tensor(plan.lm2l, dtype=torch.float64)
+    m0 = torch.as_tensor(plan.lm2m == 0)
+    fields = {}
+    for k in ("w", "dw", "ddw", "z", "dz", "s"):
+        ph = torch.rand(plan.lm_max, n_r, generator=g, dtype=torch.float64) * 2 * math.pi
+        c = torch.polar(1e-4 * (l + 1.0)[:, None] ** -2 * torch.ones(1, n_r, dtype=torch.float64), ph)
+        c[m0] = c[m0].real.to(c.dtype)
+        fields[k] = c.to(dev)
+    prof = anelastic_profiles(n_r, l_max, device=dev)
+    work = torch.empty(plan.nl_anel_workspace(n_r, False, False), dtype=torch.uint8, device=dev)
+    out = None
+
+    def step():
+        nonlocal out
+        out, _, _ = plan.nl_anel(fields, prof, 1.0, 0.3, 0.0, 2.5, 1.0, 1.0, l_mag=False,
+                                 out=out, work=work)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if rank == 0:
+        print(json.dumps({"metric": "anelastic nonlinear stage steps/s @lmax=383, 1 B200",
+                          "value": 1000.0 / ms, "unit": "steps/s", "n_gpus": 1,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "dtype": "bf16x3/f32", "data": "synthetic",
+                          "config": {"workload": "anelastic hydro radial-loop nonlinear stage "
+                                                 "(split)", "l_max": l_max, "n_theta": 576,
+                                     "n_phi": 1152, "n_r": n_r, "grid_fields_in": 12,
+                                     "spectral_out": 6},
+                          "clocks": clocks.summary()}), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -258,6 +311,9 @@ def main():
     ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--workload", default="bouss", choices=["bouss", "anel"],
+                    help="bouss: the headline Boussinesq MHD stage; anel: the fused anelastic "
+                         "stage at l_max=383 (extra line, split precision)")
     ap.add_argument("--levels", type=int, default=N_R,
                     help="radial levels (profiling runs use fewer than the 97 of the workload)")
     args = ap.parse_args()
@@ -268,6 +324,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "anel":
+        run_anel(args, rank, world)
         return
 
     torch.cuda.set_device(local)
