@@ -165,7 +165,7 @@ class ClockSampler:
 # capture of the same kernel at n_r = 17 (profiles/split_stage_kernels_l255_n17_ncu.md),
 # per Fourier row moved (13 fields x n_r in, 9 fields x (n_r - 2) out); traffic grows
 # in proportion to the rows, so the full-size launch is scaled by its row count.
-NCU_PHI_TRAFFIC = {"split": (230.526976e6 + 106.615296e6) / (13 * 17 + 9 * 15)}
+NCU_PHI_TRAFFIC = {"split": (230.161408e6 + 104.267520e6) / (13 * 17 + 9 * 15)}
 
 
 def measured_peaks():
