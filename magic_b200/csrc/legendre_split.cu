@@ -73,6 +73,22 @@ __device__ __forceinline__ void put_row16(uint8_t* tile, int row, const float (&
   }
 }
 
+// Write K values 8 half .. 8 half + 7 of one row as 3 planes into an A tile.
+__device__ __forceinline__ void put_row8(uint8_t* tile, int row, int half, const float (&v)[8]) {
+  __nv_bfloat16 q[3][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) split3f(v[i], q[0][i], q[1][i], q[2][i]);
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    uint4 w;
+    w.x = *reinterpret_cast<uint32_t*>(&q[s][0]);
+    w.y = *reinterpret_cast<uint32_t*>(&q[s][2]);
+    w.z = *reinterpret_cast<uint32_t*>(&q[s][4]);
+    w.w = *reinterpret_cast<uint32_t*>(&q[s][6]);
+    *reinterpret_cast<uint4*>(tile + s * (kSplitRows * 32) + core_off(row, 8 * half)) = w;
+  }
+}
+
 // 16-byte global -> shared copy; src_bytes = 0 zero-fills (no global read).
 __device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, uint32_t src_bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
@@ -109,7 +125,7 @@ __host__ __device__ inline int64_t syn_img_chunk(int64_t total_chunks, int rt, i
   return (((int64_t)rt * total_chunks + prefix + c) * 2 + q);
 }
 
-__global__ void __launch_bounds__(kPackThreads, 6) k_syn_pack(SplitSynArgs a) {
+__global__ void __launch_bounds__(kPackThreads, 4) k_syn_pack(SplitSynArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const Tables& t = a.t;
   const int rt = blockIdx.x, c = blockIdx.y, mc = blockIdx.z;
@@ -138,41 +154,67 @@ __global__ void __launch_bounds__(kPackThreads, 6) k_syn_pack(SplitSynArgs a) {
     cp_async_wait0();
     __syncthreads();
   }
+  // task = (table q, parity p, row pair): rows 2 pr, 2 pr + 1 are the real and
+  // imaginary rows of one field (rows per level are even), whose programs read
+  // the same terms with the components swapped, so one 16-byte load serves both
 #pragma unroll 1
-  for (int task = tid; task < 4 * kSplitRows; task += kPackThreads) {
-    const int qp = task / kSplitRows, row = task % kSplitRows;
+  for (int task = tid; task < 2 * kSplitRows; task += kPackThreads) {
+    const int qp = task / (kSplitRows / 2), row0 = 2 * (task % (kSplitRows / 2));
     const int q = qp >> 1, p = qp & 1;  // table (0 P, 1 dP), parity of l - m
-    const int R = rt * kSplitRows + row;
-    const bool live = R < a.nrows;
-    const int lev = live ? R / a.row_per_level : lev0;
-    const int qf = live ? R - lev * a.row_per_level : 0;
+    const int R0 = rt * kSplitRows + row0;
+    const bool live = R0 < a.nrows;
+    const int lev = live ? R0 / a.row_per_level : lev0;
+    const int qf = live ? R0 - lev * a.row_per_level : 0;
     const int lv = lev - lev0;
-    const RowOp op = a.ops[qf];
-    const TermIx tm = a.term[q ? op.tD : op.tP];
-    const int cpart = q ? op.cD : op.cP;
-    // value = f * (mul(l) * src_a - cw * src_b), branch-free over the recipes:
-    //   raw: mul = 1; dlh: mul = l(l+1); curl: mul = or2 l(l+1), cw = 1
-    const float f = live ? (float)coef_value(q ? op.kD : op.kP, (double)m) : 0.f;
-    const float dl = tm.recipe == kRaw ? 0.f : 1.f;
-    const float o2 = tm.recipe == kCurlT ? (float)a.or2[lev] : 1.f;
-    const float cw = tm.recipe == kCurlT ? 1.f : 0.f;
-    const double* xa = reinterpret_cast<const double*>(d + tm.ia * pitch + lv) + cpart;
-    const double* xb = reinterpret_cast<const double*>(d + tm.ib * pitch + lv) + cpart;
-    const int kst = 2 * a.stg_lev;  // doubles between consecutive kk
-    float v[16];
+    const float o2l = a.or2 ? (float)a.or2[lev] : 1.f;
+    struct RowSrc {
+      const double2 *xa, *xb;
+      int cpart;
+      float f, dl, o2, cw;
+      int tix;
+    } rs[2];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int kk = 2 * i + p;
-      const float l = (float)(m + 32 * c + kk);
-      const float mul = o2 * (1.f + dl * (l * (l + 1.f) - 1.f));
-      const float x = (float)xa[kk * kst];
-      const float w = cw != 0.f ? (float)xb[kk * kst] : 0.f;
-      v[i] = f != 0.f ? f * (mul * x - w) : 0.f;
+    for (int h = 0; h < 2; ++h) {
+      const RowOp op = a.ops[qf + h];
+      const int tix = q ? op.tD : op.tP;
+      const TermIx tm = a.term[tix];
+      rs[h].tix = tix;
+      rs[h].cpart = q ? op.cD : op.cP;
+      // value = f * (mul(l) * src_a - cw * src_b), branch-free over the recipes:
+      //   raw: mul = 1; dlh: mul = l(l+1); curl: mul = or2 l(l+1), cw = 1
+      rs[h].f = live ? (float)coef_value(q ? op.kD : op.kP, (double)m) : 0.f;
+      rs[h].dl = tm.recipe == kRaw ? 0.f : 1.f;
+      rs[h].o2 = tm.recipe == kCurlT ? o2l : 1.f;
+      rs[h].cw = tm.recipe == kCurlT ? 1.f : 0.f;
+      rs[h].xa = d + tm.ia * pitch + lv;
+      rs[h].xb = d + tm.ib * pitch + lv;
     }
+    const bool same = rs[0].tix == rs[1].tix;
     const int combo = q == 0 ? p : 1 - p;
     uint8_t* dst = a.aimg + syn_img_chunk(a.total_chunks, rt, a.s.syn_chunk_prefix[mc * 2 + combo],
                                           c, q) * kImgChunk;
-    put_row16(dst, row, v);
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      float v0[8], v1[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int kk = 2 * (8 * half + i) + p;
+        const float l = (float)(m + 32 * c + kk);
+        const int off = kk * a.stg_lev;
+        const double2 x0 = rs[0].xa[off];
+        const double2 w0 = rs[0].cw != 0.f ? rs[0].xb[off] : make_double2(0.0, 0.0);
+        const double2 x1 = same ? x0 : rs[1].xa[off];
+        const double2 w1 = same ? w0 : (rs[1].cw != 0.f ? rs[1].xb[off] : make_double2(0.0, 0.0));
+        const float mul0 = rs[0].o2 * (1.f + rs[0].dl * (l * (l + 1.f) - 1.f));
+        const float mul1 = rs[1].o2 * (1.f + rs[1].dl * (l * (l + 1.f) - 1.f));
+        const float a0 = (float)(rs[0].cpart ? x0.y : x0.x), b0 = (float)(rs[0].cpart ? w0.y : w0.x);
+        const float a1 = (float)(rs[1].cpart ? x1.y : x1.x), b1 = (float)(rs[1].cpart ? w1.y : w1.x);
+        v0[i] = rs[0].f != 0.f ? rs[0].f * (mul0 * a0 - b0) : 0.f;
+        v1[i] = rs[1].f != 0.f ? rs[1].f * (mul1 * a1 - b1) : 0.f;
+      }
+      put_row8(dst, row0, half, v0);
+      put_row8(dst, row0 + 1, half, v1);
+    }
   }
 }
 
