@@ -607,11 +607,15 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
       const double l = (double)(m + 2 * kk + par);
       osc[kk] = l > 0.0 ? 1.0 / (l * (l + 1.0)) : 0.0;
     }
-    // task = (output o, column i, level slot lv), lv fastest: consecutive
-    // threads write consecutive levels of one (output, l)
+    // (output o, level slot lv) pairs, lv fastest, R threads per pair splitting
+    // the 16 columns of a chunk: consecutive threads write consecutive levels of
+    // one (output, l), and each thread reads its row-program tables once per chunk
     int lvs = 0;  // level slot: smallest power of two >= lev_tile
     while ((1 << lvs) < a.lev_tile) ++lvs;
-    const int ntask = a.n_out << (4 + lvs);
+    const int npair = a.n_out << lvs;
+    int R = 1;
+    while (R < 16 && npair * R * 2 <= kGemmThreads) R *= 2;
+    const int ispan = 16 / R;
     for (int c0 = 0; c0 < wk; c0 += 16) {
       float v[16];
       tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + c0, v);
@@ -621,19 +625,26 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_anal_gemm(SplitAnaArgs a) {
 #pragma unroll
       for (int i = 0; i < 16; ++i) xch[(kSplitRows + tid) * XS + i] = v[i];
       __syncthreads();
-      for (int task = tid; task < ntask; task += kGemmThreads) {
-        const int lv = task & ((1 << lvs) - 1), rest = task >> lvs;
-        const int i = rest & 15, o = rest >> 4;
-        const int kk = c0 + i, k = 2 * kk + par;
-        if (lv >= nlev || k >= nlm) continue;
-        const int base = lv * a.cols;
-        const int q = 4 * o;
-        const double re = cf[q] * (double)xch[(base + colx[q]) * XS + i] +
-                          cf[q + 1] * (double)xch[(base + colx[q + 1]) * XS + i];
-        const double im = cf[q + 2] * (double)xch[(base + colx[q + 2]) * XS + i] +
-                          cf[q + 3] * (double)xch[(base + colx[q + 3]) * XS + i];
-        const double sc = a.ops[2 * o].scale ? osc[kk] : 1.0;
-        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] = make_double2(sc * re, sc * im);
+      for (int pr = tid / R; pr < npair; pr += kGemmThreads / R) {
+        const int lv = pr & ((1 << lvs) - 1), o = pr >> lvs;
+        if (lv >= nlev) continue;
+        const int q = 4 * o, base = lv * a.cols;
+        const double fr0 = cf[q], fr1 = cf[q + 1], fi0 = cf[q + 2], fi1 = cf[q + 3];
+        const float* xr0 = xch + (base + colx[q]) * XS;
+        const float* xr1 = xch + (base + colx[q + 1]) * XS;
+        const float* xi0 = xch + (base + colx[q + 2]) * XS;
+        const float* xi1 = xch + (base + colx[q + 3]) * XS;
+        const bool scaled = a.ops[2 * o].scale;
+        double2* dst = a.out[o] + a.out_col0 + lev0 + lv;
+        const int i0 = (tid & (R - 1)) * ispan;
+        for (int ii = 0; ii < ispan; ++ii) {
+          const int i = i0 + ii, kk = c0 + i, k = 2 * kk + par;
+          if (k >= nlm) break;
+          const double re = fr0 * (double)xr0[i] + fr1 * (double)xr1[i];
+          const double im = fi0 * (double)xi0[i] + fi1 * (double)xi1[i];
+          const double sc = scaled ? osc[kk] : 1.0;
+          dst[(int64_t)(ls + k) * a.ld] = make_double2(sc * re, sc * im);
+        }
       }
       __syncthreads();
     }
