@@ -247,6 +247,14 @@ MT_API int mt_nl_anel(const mt_plan* plan, int n_r, const mt_anel_in* in,
                const mt_anel_out* out, const mt_anel_stage_params* p, double* dtrkc,
                double* dthkc, void* work, size_t work_bytes, void* stream);
 
+/* Self-test of the device-side failure detection (no reference counterpart):
+ * one CTA waits on an mbarrier that nothing completes, gives up after
+ * `spins` polls, writes 99 to the device int *status (which the caller zeroes
+ * first) and returns, so the context stays usable.  The tensor-core kernels
+ * use the same bounded wait (2^22 polls) and report their own codes in the
+ * first int of their workspace. */
+MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
+
 /* Thread-local message for the last non-zero status. */
 MT_API const char* mt_last_error(void);
 

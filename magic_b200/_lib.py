@@ -105,6 +105,7 @@ _PROTOS = {
     "mt_nl_anel_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "mt_nl_anel": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(AnelIn), C.POINTER(AnelOut),
                              C.POINTER(AnelStageParams), _dp, _dp, _dp, C.c_size_t, _dp]),
+    "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }
 

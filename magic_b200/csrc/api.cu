@@ -1289,4 +1289,10 @@ int mt_nl_anel(const mt_plan* p, int n_r, const mt_anel_in* in, const mt_anel_ou
                    : nl_anel_split_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
 }
 
+int mt_selftest_wait_timeout(int* status, long long spins, void* stream) {
+  MT_REQUIRE(status && spins > 0 && spins <= (1LL << 30), MT_ERR_ARG,
+             "status pointer and 0 < spins <= 2^30 required");
+  return launch_selftest_wait(status, (long)spins, (cudaStream_t)stream);
+}
+
 }  // extern "C"

@@ -682,6 +682,28 @@ size_t synth_split_image_bytes(int nrows, int64_t total_chunks) {
   return (size_t)((nrows + kSplitRows - 1) / kSplitRows) * (size_t)total_chunks * 2 * kImgChunk;
 }
 
+// Self-test of the bounded waits: every thread waits on a barrier that no one
+// arrives on, gives up after `spins` polls, records code 99 and returns.
+__global__ void k_selftest_wait(int* status, long spins) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_n(&bar, 0, &abort_flag, status, 99, spins);
+  __syncthreads();
+  if (threadIdx.x == 0 && ok) atomicCAS(status, 0, -1);  // a wait that nothing ends returned true
+}
+
+int launch_selftest_wait(int* status, long spins, cudaStream_t st) {
+  k_selftest_wait<<<1, 64, 0, st>>>(status, spins);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st) {
   const int ntiles = (a.n_lev + a.lev_tile - 1) / a.lev_tile;
   const int nchj = (a.t.nhs + kSplitKC - 1) / kSplitKC;

@@ -61,6 +61,7 @@ struct SplitAnaArgs {
 int launch_synth_split(const SplitSynArgs& a, cudaStream_t st);
 size_t synth_split_image_bytes(int nrows, int64_t total_chunks);
 int launch_anal_split(const SplitAnaArgs& a, cudaStream_t st);
+int launch_selftest_wait(int* status, long spins, cudaStream_t st);
 size_t anal_split_image_bytes(int n_m, int nhs, int n_lev, int lev_tile);
 
 struct NlSplitArgs {

@@ -43,12 +43,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// Bounded wait for the phase with the given parity.  Returns false on timeout
-// or when another thread of the CTA already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          int* err, int code) {
+// Bounded wait for the phase with the given parity, at most `spins` polls.
+// Returns false on timeout (after raising the CTA's abort flag and recording
+// `code` in *err) or when another thread of the CTA already aborted.
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity,
+                                            volatile int* abort_flag, int* err, int code,
+                                            long spins) {
   const uint32_t a = smem_u32(bar);
-  for (long it = 0; it < kWaitSpins; ++it) {
+  for (long it = 0; it < spins; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -62,6 +64,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   *abort_flag = 1;
   if (err) atomicCAS(err, 0, code);
   return false;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          int* err, int code) {
+  return mbar_wait_n(bar, parity, abort_flag, err, code, kWaitSpins);
 }
 
 // Bounded wait used only to drain a CTA's own bulk copies before it exits:

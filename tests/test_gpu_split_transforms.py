@@ -100,3 +100,32 @@ def test_split_roundtrip_sht_benchmark_config():
                ((t2 - T)[lpos].abs().max() / T.abs().max()).item())
     print(f"split round trip: scalar {e_s:.1e}, Q {e_q:.1e}, S/T {e_st:.1e}")
     assert e_s < 1e-5 and e_q < 1e-5 and e_st < 1e-5
+
+
+@pytest.mark.parametrize("name", ["sht_l16", "sht_l32m4", "sht_l64"])
+def test_reference_signature_module_split(name):
+    """The module-level drop-in (magic_b200.sht, reference signatures) on a
+    split-precision plan against the reference's own golden outputs: 1-D and
+    batched inputs, every helper, relative error below 2e-5."""
+    import magic_b200
+    from magic_b200 import sht
+    from conftest import load_golden, rel_err
+
+    z = load_golden(name)
+    magic_b200.configure({"l_max": int(z["l_max"]), "minc": int(z["minc"]), "precision": "split"})
+    try:
+        tol = 2e-5
+        assert rel_err(npy(sht.pol_to_curlr_spat(cu(z["Q"]))), z["curlr"]) < tol
+        dt, dp = sht.torpol_to_dphspat(cu(z["S"][:, 0]), cu(z["T"][:, 0]))
+        assert rel_err(npy(dt), z["dph_t"]) < tol and rel_err(npy(dp), z["dph_p"]) < tol
+        cr, ct, cp = sht.torpol_to_curl_spat(cu(z["or2"]), cu(z["Bl"]), cu(z["ddB"]),
+                                             cu(z["J"]), cu(z["dJ"]))
+        assert rel_err(npy(cr), z["curl_r"]) < tol
+        assert rel_err(npy(ct), z["curl_t"]) < tol and rel_err(npy(cp), z["curl_p"]) < tol
+        vt, vp = sht.sphtor_to_spat(cu(z["S"][:, 0]), cu(z["T"][:, 0]))
+        assert rel_err(npy(vt), z["sphtor_t"]) < tol and rel_err(npy(vp), z["sphtor_p"]) < tol
+        q, s, t = sht.spat_to_qst(cu(z["grid"][0]), cu(z["vt"][0]), cu(z["vp"][0]))
+        assert rel_err(npy(q), z["qst_q"]) < tol
+        assert rel_err(npy(s), z["qst_s"]) < tol and rel_err(npy(t), z["qst_t"]) < tol
+    finally:
+        magic_b200.configure({})
