@@ -513,7 +513,7 @@ def main():
                 "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
-                "gpu_launches": (5 if split else 6) * args.steps,
+                "gpu_launches": 6 * args.steps,  # split: 2 packs, 2 GEMMs, phi, Courant; fp64: 2 + 1 + 2 + 1
                 "kernel_ms": part_ms, "sht_tflops": sht_tflops,
                 "roofline": roof}
         if world == 1 and not args.no_cpu:
