@@ -232,6 +232,20 @@ def cpu_stage_sample(n_levels=5, seed=0):
                       f"table build {build_s:.1f} s excluded"}
 
 
+def max_over_ranks(x, dist, device):
+    """The largest per-rank value (a step time) over all ranks; x itself with one rank."""
+    if dist is None:
+        return x
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def job_steps_per_s(world, ms_max):
+    """Whole-job throughput of `world` replicas whose slowest one needs ms_max per step."""
+    return world * 1000.0 / ms_max
+
+
 def run_anel(args, rank, world):
     """Optional line: the fused anelastic stage at the anelastic benchmark
     resolution (l_max = 383, n_theta = 576, n_phi = 1152, n_r = 129, hydrodynamic,
@@ -375,12 +389,8 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = t.item()
-    value = world * 1000.0 / ms
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
+    value = job_steps_per_s(world, ms)
 
     # --- per-kernel times: same work, each part bracketed by events on the same stream
     parts = {1: "legendre_synthesis", 2: "phi_fft_products", 4: "legendre_analysis"}
@@ -457,11 +467,7 @@ def main():
     b_ev.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = a_ev.elapsed_time(b_ev) / k_e2e
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
+    e2e_ms = max_over_ranks(a_ev.elapsed_time(b_ev) / k_e2e, dist, dev)
 
     # --- roofline of the dominant kernel
     peaks, src = measured_peaks()
@@ -510,7 +516,7 @@ def main():
                 "dtype": "bf16x3/f32" if split else "f64", "data": "synthetic",
                 "config": workload_config(args.precision),
                 "clocks": clocks.summary(),
-                "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "steps/s",
+                "e2e": {"value": job_steps_per_s(world, e2e_ms), "unit": "steps/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
                 "gpu_launches": 6 * args.steps,  # split: 2 packs, 2 GEMMs, phi, Courant; fp64: 2 + 1 + 2 + 1
