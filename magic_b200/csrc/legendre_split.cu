@@ -44,49 +44,47 @@ __device__ __forceinline__ double coef_value(int code, double m) {
   }
 }
 
-// Three bf16 planes of a float: hi = bf16(v), mid = bf16(v - hi), lo = v - hi - mid.
-// A float has 24 significant bits, so hi + mid + lo == v exactly (no underflow).
-__device__ __forceinline__ void split3f(float v, __nv_bfloat16& h, __nv_bfloat16& m,
-                                       __nv_bfloat16& l) {
-  h = __float2bfloat16_rn(v);
-  float r = v - __bfloat162float(h);
-  m = __float2bfloat16_rn(r);
-  l = __float2bfloat16_rn(r - __bfloat162float(m));
+// Three bf16 planes of two floats (packed pairs, first value in the low
+// half): hi = bf16(v), mid = bf16(v - hi), lo = bf16(v - hi - mid).  A float
+// has 24 significant bits, so hi + mid + lo == v exactly (no underflow).
+__device__ __forceinline__ void split3f2(float v0, float v1, uint32_t& h, uint32_t& m,
+                                        uint32_t& l) {
+  const __nv_bfloat162 bh = __floats2bfloat162_rn(v0, v1);
+  const float2 fh = __bfloat1622float2(bh);
+  const float r0 = v0 - fh.x, r1 = v1 - fh.y;
+  const __nv_bfloat162 bm = __floats2bfloat162_rn(r0, r1);
+  const float2 fm = __bfloat1622float2(bm);
+  const __nv_bfloat162 bl = __floats2bfloat162_rn(r0 - fm.x, r1 - fm.y);
+  h = *reinterpret_cast<const uint32_t*>(&bh);
+  m = *reinterpret_cast<const uint32_t*>(&bm);
+  l = *reinterpret_cast<const uint32_t*>(&bl);
 }
 
 // Write 16 consecutive K values of one row as 3 planes into an A tile.
 __device__ __forceinline__ void put_row16(uint8_t* tile, int row, const float (&v)[16]) {
-  __nv_bfloat16 q[3][16];
+  uint32_t w[3][8];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) split3f(v[i], q[0][i], q[1][i], q[2][i]);
+  for (int i = 0; i < 8; ++i) split3f2(v[2 * i], v[2 * i + 1], w[0][i], w[1][i], w[2][i]);
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
-      uint4 w;
-      w.x = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 0]);
-      w.y = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 2]);
-      w.z = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 4]);
-      w.w = *reinterpret_cast<uint32_t*>(&q[s][8 * half + 6]);
-      *reinterpret_cast<uint4*>(tile + s * (kSplitRows * 32) + core_off(row, 8 * half)) = w;
+      const uint4 q = make_uint4(w[s][4 * half], w[s][4 * half + 1], w[s][4 * half + 2],
+                                 w[s][4 * half + 3]);
+      *reinterpret_cast<uint4*>(tile + s * (kSplitRows * 32) + core_off(row, 8 * half)) = q;
     }
   }
 }
 
 // Write K values 8 half .. 8 half + 7 of one row as 3 planes into an A tile.
 __device__ __forceinline__ void put_row8(uint8_t* tile, int row, int half, const float (&v)[8]) {
-  __nv_bfloat16 q[3][8];
+  uint32_t w[3][4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) split3f(v[i], q[0][i], q[1][i], q[2][i]);
+  for (int i = 0; i < 4; ++i) split3f2(v[2 * i], v[2 * i + 1], w[0][i], w[1][i], w[2][i]);
 #pragma unroll
-  for (int s = 0; s < 3; ++s) {
-    uint4 w;
-    w.x = *reinterpret_cast<uint32_t*>(&q[s][0]);
-    w.y = *reinterpret_cast<uint32_t*>(&q[s][2]);
-    w.z = *reinterpret_cast<uint32_t*>(&q[s][4]);
-    w.w = *reinterpret_cast<uint32_t*>(&q[s][6]);
-    *reinterpret_cast<uint4*>(tile + s * (kSplitRows * 32) + core_off(row, 8 * half)) = w;
-  }
+  for (int s = 0; s < 3; ++s)
+    *reinterpret_cast<uint4*>(tile + s * (kSplitRows * 32) + core_off(row, 8 * half)) =
+        make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
 }
 
 // 16-byte global -> shared copy; src_bytes = 0 zero-fills (no global read).
