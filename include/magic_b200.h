@@ -253,6 +253,62 @@ MT_API int mt_nl_anel(const mt_plan* plan, int n_r, const mt_anel_in* in,
  * first) and returns, so the context stays usable.  The tensor-core kernels
  * use the same bounded wait (2^22 polls) and report their own codes in the
  * first int of their workspace. */
+/* ---- radial operators ---------------------------------------------------
+ * A real n_r x n_r matrix D applied along the radial axis of complex rows:
+ * out[b][j] = sum_k D[j][k] in[b][k] for b < nrows, rows of n_r complex
+ * values with strides ld_in / ld_out (complex units; the reference's
+ * (lm_max, n_r_max) spectral arrays are nrows = lm_max rows, ld = n_r_max).
+ * Replaces magic_torch/radial_derivatives.py:29-68 (get_dr, get_ddr, get_dddr:
+ * dense Chebyshev or banded finite-difference matrices) and
+ * magic_torch/cosine_transform.py:18-45 (costf, the self-inverse DCT-I).
+ * mt_radial_op_create copies D (HOST pointer, row-major) to the current
+ * device and keeps only each row's nonzero band, so a banded matrix costs its
+ * band only.  Operators are read-only after creation. */
+typedef struct mt_radial_op mt_radial_op;
+MT_API int mt_radial_op_create(int n_r, const double* D_host, mt_radial_op** op);
+MT_API int mt_radial_op_create_dct1(int n_r, mt_radial_op** op);
+MT_API int mt_radial_op_destroy(mt_radial_op* op);
+MT_API int mt_radial_op_bandwidth(const mt_radial_op* op);
+MT_API int mt_radial_apply(const mt_radial_op* op, int nrows, const double* in, int64_t ld_in,
+                           double* out, int64_t ld_out, void* stream);
+/* two operators on one input in one pass (get_ddr: D1 and D2) */
+MT_API int mt_radial_apply2(const mt_radial_op* op1, const mt_radial_op* op2, int nrows,
+                            const double* in, int64_t ld_in, double* out1, double* out2,
+                            int64_t ld_out, void* stream);
+
+/* ---- explicit time-derivative terms ----------------------------------------
+ * Step 4 of the radial loop (magic_torch/step_time.py:1139-1176): the
+ * nonlinear and Coriolis terms of get_td (magic_torch/get_td.py:58-308:
+ * get_dwdt or get_dwdt_double_curl, get_dzdt, get_dpdt, get_dsdt,
+ * get_dxidt, get_dbdt) completed by the finish_exp radial derivatives
+ * (update_wp.py:371-385, update_s.py:191-210, update_xi.py:183-202,
+ * update_b.py:514-528) with the operator D1.  Inputs: the spectral
+ * nonlinear products of the stage (mt_bouss_out / mt_anel_out names) and the
+ * velocity potentials, all (lm_max, n_r) complex with row stride `ld`;
+ * outputs likewise.  dpdt is written only without the double-curl form (may
+ * be null); ddw and dz are read only with it.  Values at the boundary levels
+ * are those of the reference (zero before finish_exp, then plus or2 D1 of
+ * the auxiliary). */
+typedef struct {
+  const double *Advr, *Advt, *Advp, *VSr, *VSt, *VxBr, *VxBt, *VxBp, *VXir, *VXit;
+  const double *w, *dw, *ddw, *z, *dz;
+  int64_t ld;
+} mt_td_in;
+
+typedef struct {
+  double *dwdt, *dzdt, *dpdt, *dsdt, *dxidt, *dbdt, *djdt;
+  int64_t ld;
+} mt_td_out;
+
+typedef struct {
+  const double *r, *or1, *or2, *or4, *orho1, *beta; /* (n_r) device */
+  double CorFac;
+  int l_double_curl, l_heat, l_mag, l_chem, l_anel;
+} mt_td_params;
+
+MT_API int mt_get_td(const mt_plan* plan, int n_r, const mt_td_in* in, const mt_td_out* out,
+                     const mt_td_params* p, const mt_radial_op* D1, void* stream);
+
 MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
 
 /* Thread-local message for the last non-zero status. */

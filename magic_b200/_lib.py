@@ -76,6 +76,22 @@ class AnelStageParams(C.Structure):
                [("l_mag", C.c_int), ("l_chem", C.c_int), ("cour_mode", C.c_int)]
 
 
+class TdIn(C.Structure):
+    _fields_ = [(n, _dp) for n in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp",
+                                   "VXir", "VXit", "w", "dw", "ddw", "z", "dz")] + [("ld", _i64)]
+
+
+class TdOut(C.Structure):
+    _fields_ = [(n, _dp) for n in ("dwdt", "dzdt", "dpdt", "dsdt", "dxidt", "dbdt",
+                                   "djdt")] + [("ld", _i64)]
+
+
+class TdParams(C.Structure):
+    _fields_ = [(n, _dp) for n in ("r", "or1", "or2", "or4", "orho1", "beta")] + \
+               [("CorFac", C.c_double)] + \
+               [(n, C.c_int) for n in ("l_double_curl", "l_heat", "l_mag", "l_chem", "l_anel")]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "mt_plan_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
@@ -105,6 +121,15 @@ _PROTOS = {
     "mt_nl_anel_workspace": (C.c_size_t, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "mt_nl_anel": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(AnelIn), C.POINTER(AnelOut),
                              C.POINTER(AnelStageParams), _dp, _dp, _dp, C.c_size_t, _dp]),
+    "mt_radial_op_create": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
+    "mt_radial_op_create_dct1": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "mt_radial_op_destroy": (C.c_int, [C.c_void_p]),
+    "mt_radial_op_bandwidth": (C.c_int, [C.c_void_p]),
+    "mt_radial_apply": (C.c_int, [C.c_void_p, C.c_int, _dp, _i64, _dp, _i64, _dp]),
+    "mt_radial_apply2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, _dp, _i64, _dp, _dp, _i64,
+                                   _dp]),
+    "mt_get_td": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TdIn), C.POINTER(TdOut),
+                            C.POINTER(TdParams), C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }

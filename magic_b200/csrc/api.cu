@@ -47,11 +47,6 @@ static int check_plan(const mt_plan* p) {
   return MT_OK;
 }
 
-#define MT_TRY(expr)              \
-  do {                            \
-    int _rc = (expr);             \
-    if (_rc != MT_OK) return _rc; \
-  } while (0)
 
 static size_t fourier_bytes(const mt_plan* p, int64_t ncols) {
   return (size_t)p->n_m * p->n_theta * ncols * sizeof(double2);

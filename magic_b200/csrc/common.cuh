@@ -30,6 +30,12 @@ void set_error(const std::string& msg);
     }                                                                              \
   } while (0)
 
+#define MT_TRY(expr)              \
+  do {                            \
+    int _rc = (expr);             \
+    if (_rc != MT_OK) return _rc; \
+  } while (0)
+
 constexpr int kMaxFftStages = 24;
 
 // Device-side view of the horizontal tables, passed by value to kernels.

@@ -1,0 +1,434 @@
+// Radial operators and the spectral explicit terms of a time step (FP64).
+//
+// Radial operator: a real n_r x n_r matrix D applied along the radial axis of
+// complex (row, n_r) arrays, out[row][j] = sum_k D[j][k] in[row][k]
+// (magic_torch/radial_derivatives.py:29-68: get_dr / get_ddr / get_dddr with
+// the dense Chebyshev or the banded finite-difference matrices;
+// magic_torch/cosine_transform.py:18-45: the self-inverse DCT-I, which is the
+// same operation with the DCT-I matrix).  Each matrix row keeps only its
+// nonzero band: W values starting at column k0[j] (W = widest band, rows
+// shifted left so k0[j] + W <= n_r, padding zero), stored band-transposed,
+// vals[kk * n_r + j] = D[j][k0[j] + kk], so the 32 lanes of a warp (32
+// consecutive output levels) read 32 consecutive values.  A dense Chebyshev
+// matrix has W = n_r; the fourth-order finite-difference ones W = 5.
+//
+// Explicit terms: one warp per lm row assembles the Coriolis and nonlinear
+// terms of get_td (magic_torch/get_td.py:58-308) level by level, keeps the
+// finish_exp auxiliaries (dVxVhLM, dVSrLM, dVXirLM, dVxBhLM) and the partial
+// terms in warp-private shared memory, applies D1 along the row and writes
+// the finished terms (update_wp.py:371-385, update_s.py:191-210,
+// update_xi.py:183-202, update_b.py:514-528).  The l -+ 1 couplings read the
+// neighbouring rows lm -+ 1 of the same m block (m-major order).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+struct mt_radial_op {
+  int n_r = 0, W = 0, device = 0;
+  int* k0 = nullptr;       // (n_r) first column of each row's band
+  double* vals = nullptr;  // (W, n_r) band-transposed values
+};
+
+namespace mt {
+
+namespace {
+
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return {a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ double2 c_scale(double s, double2 a) { return {s * a.x, s * a.y}; }
+// i m x
+__device__ __forceinline__ double2 c_im(double m, double2 a) { return {-m * a.y, m * a.x}; }
+__device__ __forceinline__ double2 c_fma(double s, double2 a, double2 acc) {
+  return {fma(s, a.x, acc.x), fma(s, a.y, acc.y)};
+}
+
+struct OpView {
+  int n_r, W;
+  const int* k0;
+  const double* vals;
+};
+
+// (D f)[j] for one row f staged in shared memory
+__device__ __forceinline__ double2 op_row(const OpView& op, const double2* f, int j) {
+  const int k0 = __ldg(op.k0 + j);
+  double2 acc = {0.0, 0.0};
+  for (int kk = 0; kk < op.W; ++kk) acc = c_fma(__ldg(op.vals + (int64_t)kk * op.n_r + j), f[k0 + kk], acc);
+  return acc;
+}
+
+struct ApplyArgs {
+  OpView op[2];
+  int nop, nrows;
+  const double2* in;
+  int64_t ld_in;
+  double2* out[2];
+  int64_t ld_out;
+};
+
+// one warp per row: stage the row, then every lane forms its output levels
+__global__ void k_radial_apply(ApplyArgs a) {
+  extern __shared__ double2 rowbuf[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int n_r = a.op[0].n_r;
+  double2* f = rowbuf + (int64_t)wib * n_r;
+  const int wpb = blockDim.x >> 5;
+  for (int row = blockIdx.x * wpb + wib; row < a.nrows; row += gridDim.x * wpb) {
+    const double2* src = a.in + (int64_t)row * a.ld_in;
+    for (int j = lane; j < n_r; j += 32) f[j] = src[j];
+    __syncwarp();
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+      if (o >= a.nop) break;
+      double2* dst = a.out[o] + (int64_t)row * a.ld_out;
+      for (int j = lane; j < n_r; j += 32) dst[j] = op_row(a.op[o], f, j);
+    }
+    __syncwarp();
+  }
+}
+
+struct TdArgs {
+  int n_r, l_max, minc, n_m;
+  const int* lstart;
+  const double2 *Advr, *Advt, *Advp, *VSr, *VSt, *VxBr, *VxBt, *VxBp, *VXir, *VXit;
+  const double2 *w, *dw, *ddw, *z, *dz;
+  int64_t ld_in;
+  double2 *dwdt, *dzdt, *dpdt, *dsdt, *dxidt, *dbdt, *djdt;
+  int64_t ld_out;
+  const double *r, *or1, *or2, *or4, *orho1, *beta;
+  double CorFac;
+  int double_curl, heat, mag, chem, anel;
+  OpView D1;
+};
+
+// sqrt((l+m)(l-m)/((2l-1)(2l+1))) for l > 0 (magic_torch/horizontal_data.py:91-100)
+__device__ __forceinline__ double clm_d(double l, double m) {
+  return l > 0.0 ? sqrt((l + m) * (l - m) / ((2.0 * l - 1.0) * (2.0 * l + 1.0))) : 0.0;
+}
+
+// warp-private shared memory per row: 4 auxiliaries + 4 partial terms
+constexpr int kTdBufs = 8;
+
+__global__ void k_get_td(TdArgs a) {
+  extern __shared__ double2 tdbuf[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const int n_r = a.n_r;
+  const int mc = blockIdx.y, m = mc * a.minc;
+  const int l = m + blockIdx.x * wpb + wib;
+  if (l > a.l_max) return;
+  const int lm = a.lstart[mc] + (l - m);
+  double2* buf = tdbuf + (int64_t)wib * kTdBufs * n_r;
+  double2 *xVh = buf, *xVS = buf + n_r, *xVX = buf + 2 * n_r, *xVB = buf + 3 * n_r;
+  double2 *pW = buf + 4 * n_r, *pS = buf + 5 * n_r, *pX = buf + 6 * n_r, *pJ = buf + 7 * n_r;
+
+  // horizontal coefficients of this (l, m) (magic_torch/horizontal_data.py:103-130)
+  const double lf = (double)l, mf = (double)m;
+  const double c_l = clm_d(lf, mf), c_lp1 = clm_d(lf + 1.0, mf);
+  const double dLh = lf * (lf + 1.0);
+  const double dTh1S = (lf + 1.0) * c_l, dTh1A = lf * c_lp1;
+  const double dTh2S = (lf - 1.0) * c_l, dTh2A = (lf + 2.0) * c_lp1;
+  const double dTh3S = (lf - 1.0) * (lf + 1.0) * c_l, dTh3A = lf * (lf + 2.0) * c_lp1;
+  const double dTh4S = dTh1S * (lf - 1.0) * lf, dTh4A = dTh1A * (lf + 1.0) * (lf + 2.0);
+  // l+1 neighbour (masked at l_max) and l-1 neighbour (self, zero coefficient, at l = m)
+  const bool hasA = l < a.l_max;
+  const int64_t rowA = (int64_t)(hasA ? lm + 1 : lm) * a.ld_in;
+  const int64_t rowS = (int64_t)(l > m ? lm - 1 : lm) * a.ld_in;
+  const int64_t row = (int64_t)lm * a.ld_in;
+  const double mA = hasA ? 1.0 : 0.0;
+  const double cf2 = 2.0 * a.CorFac;
+  auto ldA = [&](const double2* f, int j) {
+    const double2 v = f[rowA + j];
+    return double2{mA * v.x, mA * v.y};
+  };
+
+  for (int j = lane; j < n_r; j += 32) {
+    const bool bnd = j == 0 || j == n_r - 1;
+    const double or1 = a.or1[j], or2 = a.or2[j], or4 = a.or4[j], r = a.r[j];
+    const double orho1 = a.orho1[j], beta = a.beta[j];
+    const double2 w = a.w[row + j], dw = a.dw[row + j], z = a.z[row + j];
+    const double2 zA = ldA(a.z, j), zS = a.z[rowS + j];
+    // toroidal velocity (get_td.py:151-181)
+    {
+      const double2 dwA = ldA(a.dw, j), dwS = a.dw[rowS + j];
+      const double2 wA = ldA(a.w, j), wS = a.w[rowS + j];
+      double2 cor = c_im(mf, z);
+      cor = c_add(cor, c_scale(dTh3A, dwA));
+      cor = c_add(cor, c_scale(or1 * dTh4A, wA));
+      cor = c_add(cor, c_scale(dTh3S, dwS));
+      cor = c_sub(cor, c_scale(or1 * dTh4S, wS));
+      const double2 v = c_add(c_scale(dLh, a.Advp[row + j]), c_scale(cf2 * or2, cor));
+      a.dzdt[(int64_t)lm * a.ld_out + j] = bnd ? double2{0.0, 0.0} : v;
+    }
+    if (a.double_curl) {
+      // get_td.py:88-148
+      double2 v;
+      if (lm == 0) {
+        v = c_add(c_scale(or2, a.Advr[row + j]), c_scale(cf2 * or1 * dTh2A, zA));
+      } else {
+        const double2 ddw = a.ddw[row + j], dz = a.dz[row + j];
+        const double2 dzA = ldA(a.dz, j), dzS = a.dz[rowS + j];
+        double2 t = c_add(c_scale(-1.0, ddw), c_scale(beta, dw));
+        t = c_add(t, c_scale((beta * or1 + or2) * dLh, w));
+        double2 in = c_im(mf, t);
+        in = c_add(in, c_scale(dTh3A, c_sub(dzA, c_scale(beta, zA))));
+        in = c_add(in, c_scale(dTh3S, c_sub(dzS, c_scale(beta, zS))));
+        in = c_add(in, c_scale(or1, c_sub(c_scale(dTh4A, zA), c_scale(dTh4S, zS))));
+        v = c_add(c_scale(dLh * or4 * orho1, a.Advr[row + j]), c_scale(cf2 * or2 * orho1, in));
+      }
+      pW[j] = bnd ? double2{0.0, 0.0} : v;
+      xVh[j] = bnd ? double2{0.0, 0.0} : c_scale(-orho1 * (r * r) * dLh, a.Advt[row + j]);
+    } else {
+      // get_td.py:58-85 and 184-213
+      double2 cor = c_im(mf, dw);
+      cor = c_add(cor, c_scale(dTh2A, zA));
+      cor = c_sub(cor, c_scale(dTh2S, zS));
+      const double2 v = c_add(c_scale(or2, a.Advr[row + j]), c_scale(cf2 * or1, cor));
+      a.dwdt[(int64_t)lm * a.ld_out + j] = bnd ? double2{0.0, 0.0} : v;
+      double2 cp = c_scale(-1.0, c_im(mf, c_add(dw, c_scale(or1 * dLh, w))));
+      cp = c_add(cp, c_scale(dTh3A, zA));
+      cp = c_add(cp, c_scale(dTh3S, zS));
+      const double2 p = c_add(c_scale(-dLh, a.Advt[row + j]), c_scale(cf2 * or2, cp));
+      if (a.dpdt) a.dpdt[(int64_t)lm * a.ld_out + j] = bnd ? double2{0.0, 0.0} : p;
+    }
+    if (a.heat) {
+      pS[j] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VSt[row + j]);
+      xVS[j] = bnd ? double2{0.0, 0.0} : a.VSr[row + j];
+    }
+    if (a.chem) {
+      pX[j] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VXit[row + j]);
+      xVX[j] = bnd ? double2{0.0, 0.0} : a.VXir[row + j];
+    }
+    if (a.mag) {
+      a.dbdt[(int64_t)lm * a.ld_out + j] =
+          bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VxBp[row + j]);
+      pJ[j] = bnd ? double2{0.0, 0.0} : c_scale(dLh * or4, a.VxBr[row + j]);
+      const double2 h = c_scale(-dLh, a.VxBt[row + j]);
+      xVB[j] = (lm == 0 && bnd) ? double2{0.0, 0.0} : c_scale(r * r, h);
+    }
+  }
+  __syncwarp();
+  // finish_exp: the radial derivative of each auxiliary along this row
+  for (int j = lane; j < n_r; j += 32) {
+    const double or2 = a.or2[j], orho1 = a.orho1[j];
+    const int64_t o = (int64_t)lm * a.ld_out + j;
+    if (a.double_curl) a.dwdt[o] = c_add(pW[j], c_scale(or2, op_row(a.D1, xVh, j)));
+    if (a.heat) {
+      double2 v = c_sub(pS[j], c_scale(or2, op_row(a.D1, xVS, j)));
+      a.dsdt[o] = a.anel ? c_scale(orho1, v) : v;
+    }
+    if (a.chem) {
+      double2 v = c_sub(pX[j], c_scale(or2, op_row(a.D1, xVX, j)));
+      a.dxidt[o] = a.anel ? c_scale(orho1, v) : v;
+    }
+    if (a.mag) a.djdt[o] = c_add(pJ[j], c_scale(or2, op_row(a.D1, xVB, j)));
+  }
+}
+
+OpView view(const mt_radial_op* op) { return OpView{op->n_r, op->W, op->k0, op->vals}; }
+
+int check_op(const mt_radial_op* op) {
+  MT_REQUIRE(op && op->vals, MT_ERR_ARG, "null radial operator");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == op->device, MT_ERR_ARG,
+             "radial operator used on a different device than it was built on");
+  return MT_OK;
+}
+
+constexpr size_t kRadialSmemBudget = 96 * 1024;
+
+}  // namespace
+
+}  // namespace mt
+
+using namespace mt;
+
+extern "C" {
+
+int mt_radial_op_create(int n_r, const double* D, mt_radial_op** out) {
+  MT_REQUIRE(out && D && n_r >= 2 && n_r <= 4096, MT_ERR_ARG, "bad radial operator argument");
+  *out = nullptr;
+  // band of every row: first and last nonzero column
+  std::vector<int> first(n_r), last(n_r);
+  int W = 1;
+  for (int j = 0; j < n_r; ++j) {
+    int f = -1, l = -1;
+    for (int k = 0; k < n_r; ++k) {
+      MT_REQUIRE(std::isfinite(D[(size_t)j * n_r + k]), MT_ERR_ARG, "radial operator not finite");
+      if (D[(size_t)j * n_r + k] != 0.0) {
+        if (f < 0) f = k;
+        l = k;
+      }
+    }
+    if (f < 0) f = l = std::min(j, n_r - 1);
+    first[j] = f;
+    last[j] = l;
+    W = std::max(W, l - f + 1);
+  }
+  std::vector<int> k0(n_r);
+  std::vector<double> vals((size_t)W * n_r, 0.0);
+  for (int j = 0; j < n_r; ++j) {
+    k0[j] = std::min(first[j], n_r - W);  // keep k0 + W <= n_r; the extra columns are zero
+    for (int kk = 0; kk < W; ++kk) vals[(size_t)kk * n_r + j] = D[(size_t)j * n_r + k0[j] + kk];
+  }
+  mt_radial_op* op = new mt_radial_op();
+  op->n_r = n_r;
+  op->W = W;
+  auto fail = [&](int rc) {
+    if (op->k0) cudaFree(op->k0);
+    if (op->vals) cudaFree(op->vals);
+    delete op;
+    return rc;
+  };
+  if (cudaGetDevice(&op->device) != cudaSuccess) return fail((set_error("cudaGetDevice failed"), MT_ERR_CUDA));
+  if (cudaMalloc(&op->k0, n_r * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&op->vals, vals.size() * sizeof(double)) != cudaSuccess ||
+      cudaMemcpy(op->k0, k0.data(), n_r * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(op->vals, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+          cudaSuccess)
+    return fail((set_error("radial operator allocation or upload failed"), MT_ERR_CUDA));
+  *out = op;
+  return MT_OK;
+}
+
+int mt_radial_op_create_dct1(int n_r, mt_radial_op** out) {
+  MT_REQUIRE(n_r >= 2 && n_r <= 4096, MT_ERR_ARG, "bad DCT-I length");
+  // y[k] = (f[0] + (-1)^k f[N] + 2 sum_{j=1}^{N-1} f[j] cos(j k pi / N)) / sqrt(2 N)
+  const int N = n_r - 1;
+  const double s = 1.0 / std::sqrt(2.0 * N);
+  std::vector<double> C((size_t)n_r * n_r);
+  for (int k = 0; k < n_r; ++k)
+    for (int j = 0; j < n_r; ++j) {
+      double v;
+      if (j == 0) v = 1.0;
+      else if (j == N) v = (k & 1) ? -1.0 : 1.0;
+      else v = 2.0 * std::cos(M_PI * (double)((int64_t)j * k % (2 * N)) / N);
+      C[(size_t)k * n_r + j] = v * s;
+    }
+  return mt_radial_op_create(n_r, C.data(), out);
+}
+
+int mt_radial_op_destroy(mt_radial_op* op) {
+  if (!op) return MT_OK;
+  if (op->k0) cudaFree(op->k0);
+  if (op->vals) cudaFree(op->vals);
+  delete op;
+  return MT_OK;
+}
+
+int mt_radial_op_bandwidth(const mt_radial_op* op) { return op ? op->W : 0; }
+
+static int radial_apply_n(const mt_radial_op* const* ops, int nop, int nrows, const double* in,
+                          int64_t ld_in, double* const* out, int64_t ld_out, void* stream) {
+  for (int o = 0; o < nop; ++o) {
+    MT_TRY(check_op(ops[o]));
+    MT_REQUIRE(ops[o]->n_r == ops[0]->n_r, MT_ERR_ARG, "radial operators of different sizes");
+    MT_REQUIRE(out[o], MT_ERR_ARG, "null radial output");
+  }
+  const int n_r = ops[0]->n_r;
+  MT_REQUIRE(in && nrows >= 0 && ld_in >= n_r && ld_out >= n_r, MT_ERR_ARG,
+             "bad radial apply argument");
+  if (nrows == 0) return MT_OK;
+  ApplyArgs a{};
+  for (int o = 0; o < nop; ++o) {
+    a.op[o] = view(ops[o]);
+    a.out[o] = (double2*)out[o];
+  }
+  a.nop = nop;
+  a.nrows = nrows;
+  a.in = (const double2*)in;
+  a.ld_in = ld_in;
+  a.ld_out = ld_out;
+  const size_t per_warp = (size_t)n_r * sizeof(double2);
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, kRadialSmemBudget / per_warp));
+  MT_REQUIRE(per_warp <= 200 * 1024, MT_ERR_UNSUPPORTED, "radial row too long for shared memory");
+  const size_t sm = wpb * per_warp;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_radial_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+  int dev = 0, nsm = 148;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_CHECK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = (int)std::min<int64_t>((nrows + wpb - 1) / wpb, (int64_t)nsm * 16);
+  k_radial_apply<<<blocks, 32 * wpb, sm, (cudaStream_t)stream>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int mt_radial_apply(const mt_radial_op* op, int nrows, const double* in, int64_t ld_in,
+                    double* out, int64_t ld_out, void* stream) {
+  const mt_radial_op* ops[1] = {op};
+  double* outs[1] = {out};
+  return radial_apply_n(ops, 1, nrows, in, ld_in, outs, ld_out, stream);
+}
+
+int mt_radial_apply2(const mt_radial_op* op1, const mt_radial_op* op2, int nrows,
+                     const double* in, int64_t ld_in, double* out1, double* out2,
+                     int64_t ld_out, void* stream) {
+  const mt_radial_op* ops[2] = {op1, op2};
+  double* outs[2] = {out1, out2};
+  return radial_apply_n(ops, 2, nrows, in, ld_in, outs, ld_out, stream);
+}
+
+int mt_get_td(const mt_plan* p, int n_r, const mt_td_in* in, const mt_td_out* out,
+              const mt_td_params* q, const mt_radial_op* D1, void* stream) {
+  MT_REQUIRE(p && in && out && q, MT_ERR_ARG, "null argument");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == p->device, MT_ERR_ARG, "plan used on a different device than it was built on");
+  MT_REQUIRE(n_r >= 3 && in->ld >= n_r && out->ld >= n_r, MT_ERR_ARG, "bad radial size or stride");
+  MT_REQUIRE(q->r && q->or1 && q->or2 && q->or4 && q->orho1 && q->beta, MT_ERR_ARG,
+             "null radial profile");
+  MT_REQUIRE(in->w && in->dw && in->z && in->Advr && in->Advt && in->Advp && out->dwdt &&
+                 out->dzdt,
+             MT_ERR_ARG, "null velocity field or output");
+  const bool need_d1 = q->l_double_curl || q->l_heat || q->l_chem || q->l_mag;
+  if (need_d1) {
+    MT_TRY(check_op(D1));
+    MT_REQUIRE(D1->n_r == n_r, MT_ERR_ARG, "D1 size differs from n_r");
+  }
+  if (q->l_double_curl) MT_REQUIRE(in->ddw && in->dz, MT_ERR_ARG, "double curl needs ddw and dz");
+  if (q->l_heat) MT_REQUIRE(in->VSr && in->VSt && out->dsdt, MT_ERR_ARG, "heat terms missing");
+  if (q->l_chem) MT_REQUIRE(in->VXir && in->VXit && out->dxidt, MT_ERR_ARG, "composition terms missing");
+  if (q->l_mag)
+    MT_REQUIRE(in->VxBr && in->VxBt && in->VxBp && out->dbdt && out->djdt, MT_ERR_ARG,
+               "induction terms missing");
+  TdArgs a{};
+  a.n_r = n_r;
+  a.l_max = p->l_max;
+  a.minc = p->minc;
+  a.n_m = p->n_m;
+  a.lstart = p->d_lstart;
+  auto c = [](const double* x) { return (const double2*)x; };
+  a.Advr = c(in->Advr); a.Advt = c(in->Advt); a.Advp = c(in->Advp);
+  a.VSr = c(in->VSr); a.VSt = c(in->VSt);
+  a.VxBr = c(in->VxBr); a.VxBt = c(in->VxBt); a.VxBp = c(in->VxBp);
+  a.VXir = c(in->VXir); a.VXit = c(in->VXit);
+  a.w = c(in->w); a.dw = c(in->dw); a.ddw = c(in->ddw); a.z = c(in->z); a.dz = c(in->dz);
+  a.ld_in = in->ld;
+  auto d = [](double* x) { return (double2*)x; };
+  a.dwdt = d(out->dwdt); a.dzdt = d(out->dzdt); a.dpdt = d(out->dpdt); a.dsdt = d(out->dsdt);
+  a.dxidt = d(out->dxidt); a.dbdt = d(out->dbdt); a.djdt = d(out->djdt);
+  a.ld_out = out->ld;
+  a.r = q->r; a.or1 = q->or1; a.or2 = q->or2; a.or4 = q->or4; a.orho1 = q->orho1; a.beta = q->beta;
+  a.CorFac = q->CorFac;
+  a.double_curl = q->l_double_curl != 0;
+  a.heat = q->l_heat != 0;
+  a.chem = q->l_chem != 0;
+  a.mag = q->l_mag != 0;
+  a.anel = q->l_anel != 0;
+  if (need_d1) a.D1 = view(D1);
+  else a.D1 = OpView{n_r, 0, nullptr, nullptr};
+  const size_t per_warp = (size_t)kTdBufs * n_r * sizeof(double2);
+  MT_REQUIRE(per_warp <= 200 * 1024, MT_ERR_UNSUPPORTED, "n_r too large for the explicit-term kernel");
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, kRadialSmemBudget / per_warp));
+  const size_t sm = wpb * per_warp;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_get_td, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const dim3 grid((p->l_max + 1 + wpb - 1) / wpb, p->n_m);
+  k_get_td<<<grid, 32 * wpb, sm, (cudaStream_t)stream>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+}  // extern "C"

@@ -310,6 +310,52 @@ class Plan:
                             _ptr(dth), _ptr(work), work.numel(), self._stream()))
         return out, dtr, dth
 
+    def get_td(self, ins, prof, CorFac, D1, l_double_curl=False, l_heat=True, l_mag=True,
+               l_chem=False, l_anel=False, out=None):
+        """Explicit time-derivative terms of one step (magic_torch/step_time.py:1139-1176):
+        get_dwdt or get_dwdt_double_curl, get_dzdt, get_dpdt, get_dsdt, get_dxidt and
+        get_dbdt (magic_torch/get_td.py:58-308) completed by finish_exp_pol, _entropy,
+        _comp and _mag (update_wp.py:371-385, update_s.py:191-210, update_xi.py:183-202,
+        update_b.py:514-528), in one launch.
+
+        ``ins``: dict of (lm_max, n_r) complex128 arrays Advr, Advt, Advp, w, dw, z (plus
+        ddw, dz for the double-curl form; VSr, VSt if l_heat; VxBr, VxBt, VxBp if l_mag;
+        VXir, VXit if l_chem).  ``prof``: r, or1, or2, or4, orho1, beta over n_r.
+        ``D1``: the first-derivative RadialOp.  Returns a dict dwdt, dzdt (+ dpdt without
+        the double-curl form, dsdt, dxidt, dbdt, djdt as enabled)."""
+        n_r = ins["w"].shape[1]
+        need = ["Advr", "Advt", "Advp", "w", "dw", "z"]
+        need += ["ddw", "dz"] if l_double_curl else []
+        need += ["VSr", "VSt"] if l_heat else []
+        need += ["VxBr", "VxBt", "VxBp"] if l_mag else []
+        need += ["VXir", "VXit"] if l_chem else []
+        src = {}
+        for k in need:
+            x = ins[k]
+            if x.shape != (self.lm_max, n_r) or x.dtype != _CD or x.device != self.device:
+                raise ValueError(f"ins[{k}]: expected ({self.lm_max}, {n_r}) complex128")
+            src[k] = x.contiguous()
+        onames = ["dwdt", "dzdt"] + ([] if l_double_curl else ["dpdt"]) + \
+            (["dsdt"] if l_heat else []) + (["dxidt"] if l_chem else []) + \
+            (["dbdt", "djdt"] if l_mag else [])
+        if out is None:
+            out = {k: torch.empty(self.lm_max, n_r, dtype=_CD, device=self.device)
+                   for k in onames}
+        keep = {k: self._prof(prof[k], n_r) for k in ("r", "or1", "or2", "or4", "orho1", "beta")}
+        ti = _lib.TdIn(*[src[k].data_ptr() if k in src else None for k in
+                         ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp", "VXir",
+                          "VXit", "w", "dw", "ddw", "z", "dz")], n_r)
+        to = _lib.TdOut(*[out[k].data_ptr() if k in out else None for k in
+                          ("dwdt", "dzdt", "dpdt", "dsdt", "dxidt", "dbdt", "djdt")],
+                        out["dwdt"].stride(0))
+        tp = _lib.TdParams(*[keep[k].data_ptr() for k in ("r", "or1", "or2", "or4", "orho1",
+                                                          "beta")],
+                           float(CorFac), int(l_double_curl), int(l_heat), int(l_mag),
+                           int(l_chem), int(l_anel))
+        check(_lib.lib().mt_get_td(self._h, n_r, C.byref(ti), C.byref(to), C.byref(tp),
+                                   D1._h if D1 is not None else None, self._stream()))
+        return out
+
     def nl_anel_workspace(self, n_r, l_mag=True, l_chem=False):
         return _lib.lib().mt_nl_anel_workspace(self._h, int(n_r), int(l_mag), int(l_chem))
 

@@ -174,6 +174,68 @@ def worker_nl(name, ref):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+TD_CONFIGS = {
+    # spectral explicit terms (get_td + finish_exp), radial derivatives, DCT-I
+    "td_cheb": {"l_max": 8, "minc": 1, "n_r_max": 9, "mode": 0},
+    "td_fd_anel": {"l_max": 16, "minc": 2, "n_r_max": 12, "radial_scheme": "FD",
+                   "fd_order": 4, "fd_order_bound": 2, "strat": 5.0, "polind": 2.0,
+                   "g0": 0.0, "g1": 0.0, "g2": 1.0, "mode": 0, "ek": 1e-4, "ra": 3e6},
+}
+
+
+def worker_td(name, ref):
+    cfg = dict(TD_CONFIGS[name], device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, blocking, radial_functions as rf, pre_calculations as pc
+    from magic_torch import get_td as gt, radial_derivatives as rd
+    from magic_torch.radial_scheme import r as r_grid
+    from magic_torch.cosine_transform import costf
+    from magic_torch.update_s import finish_exp_entropy
+    from magic_torch.update_wp import finish_exp_pol
+    from magic_torch.update_b import finish_exp_mag
+    from magic_torch.update_xi import finish_exp_comp
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))
+    n = lambda x: x.detach().cpu().numpy()
+    rng = np.random.default_rng(321)
+    N, lm = params.n_r_max, params.lm_max
+    l_of = n(blocking.st_lm2l)
+    out = dict(n_r_max=N, l_max=params.l_max, minc=params.minc, lm_max=lm,
+               l_anel=int(bool(params.l_anel)), l_double_curl=int(bool(params.l_double_curl)),
+               r=n(r_grid), or1=n(rf.or1), or2=n(rf.or2), or4=n(rf.or4), orho1=n(rf.orho1),
+               beta=n(rf.beta), CorFac=float(pc.CorFac), lm2l=l_of, lm2m=n(blocking.st_lm2m),
+               D1=n(rd._D1_real), D2=n(rd._D2_real))
+    names = ["Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp", "VXir", "VXit",
+             "w", "dw", "ddw", "z", "dz", "f"]
+    ins = {k: _spec(rng, lm, l_of, N) for k in names}
+    out.update({"in_" + k: v for k, v in ins.items()})
+    T = {k: t(v) for k, v in ins.items()}
+    out["dwdt"] = n(gt.get_dwdt(T["Advr"], T["dw"], T["z"]))
+    dwdt_dc, dVxVh = gt.get_dwdt_double_curl(T["Advr"], T["Advt"], T["w"], T["dw"], T["ddw"],
+                                             T["z"], T["dz"])
+    out["dwdt_dc"] = n(dwdt_dc)
+    out["dVxVh"] = n(dVxVh)
+    out["dwdt_dc_fin"] = n(finish_exp_pol(dwdt_dc.clone(), dVxVh))
+    out["dzdt"] = n(gt.get_dzdt(T["Advp"], T["w"], T["dw"], T["z"]))
+    out["dpdt"] = n(gt.get_dpdt(T["Advt"], T["w"], T["dw"], T["z"]))
+    ds, dVSr = gt.get_dsdt(T["VSt"], T["VSr"])
+    out["dsdt_part"] = n(ds)
+    out["dsdt"] = n(finish_exp_entropy(ds.clone(), dVSr))
+    dx, dVXir = gt.get_dxidt(T["VXit"], T["VXir"])
+    out["dxidt"] = n(finish_exp_comp(dx.clone(), dVXir))
+    db, dj, dVxBh = gt.get_dbdt(T["VxBr"], T["VxBt"], T["VxBp"])
+    out["dbdt"] = n(db)
+    out["djdt_part"] = n(dj)
+    out["djdt"] = n(finish_exp_mag(dj.clone(), dVxBh))
+    out["dr_f"] = n(rd.get_dr(T["f"]))
+    d1, d2 = rd.get_ddr(T["f"])
+    out["ddr_f1"], out["ddr_f2"] = n(d1), n(d2)
+    out["costf_f"] = n(costf(T["f"]))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
@@ -181,10 +243,15 @@ def main():
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     if a.worker:
-        (worker_sht if a.worker in SHT_CONFIGS else worker_nl)(a.worker, a.ref)
+        if a.worker in SHT_CONFIGS:
+            worker_sht(a.worker, a.ref)
+        elif a.worker in TD_CONFIGS:
+            worker_td(a.worker, a.ref)
+        else:
+            worker_nl(a.worker, a.ref)
         return
     env = dict(os.environ, TORCHDYNAMO_DISABLE="1", MAGIC_DEVICE="cpu")
-    names = list(SHT_CONFIGS) + list(NL_CONFIGS)
+    names = list(SHT_CONFIGS) + list(NL_CONFIGS) + list(TD_CONFIGS)
     if a.only:
         names = [x for x in names if x in a.only.split(",")]
     for name in names:

@@ -55,7 +55,8 @@ def test_struct_layouts_match_header(libpath, tmp_path):
                "mt_anel_params": _lib.AnelParams, "mt_courant_params": _lib.CourantParams,
                "mt_bouss_in": _lib.BoussIn, "mt_bouss_out": _lib.BoussOut,
                "mt_bouss_params": _lib.BoussParams, "mt_anel_in": _lib.AnelIn,
-               "mt_anel_out": _lib.AnelOut, "mt_anel_stage_params": _lib.AnelStageParams}
+               "mt_anel_out": _lib.AnelOut, "mt_anel_stage_params": _lib.AnelStageParams,
+               "mt_td_in": _lib.TdIn, "mt_td_out": _lib.TdOut, "mt_td_params": _lib.TdParams}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
              "int main(void){"]
     for cname, py in structs.items():
@@ -87,6 +88,23 @@ def test_plan_create_rejects_bad_arguments(libpath):
     assert L.mt_plan_create(ctypes.byref(desc), ctypes.byref(h)) == 3  # unsupported precision
     assert L.mt_plan_destroy(None) == 0
     assert L.mt_transform_workspace(None, 4, 1) == 0
+
+
+def test_radial_op_rejects_bad_arguments(libpath):
+    """Argument checks of the radial-operator constructor run before any device call."""
+    from magic_b200 import _lib
+
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    D = (ctypes.c_double * 4)(1.0, 0.0, 0.0, 1.0)
+    assert L.mt_radial_op_create(1, D, ctypes.byref(h)) == 1
+    assert L.mt_radial_op_create(2, None, ctypes.byref(h)) == 1
+    bad = (ctypes.c_double * 4)(1.0, float("nan"), 0.0, 1.0)
+    assert L.mt_radial_op_create(2, bad, ctypes.byref(h)) == 1
+    assert b"finite" in L.mt_last_error()
+    assert L.mt_radial_op_create_dct1(1, ctypes.byref(h)) == 1
+    assert L.mt_radial_op_destroy(None) == 0
+    assert L.mt_radial_op_bandwidth(None) == 0
 
 
 def test_no_cpu_fallback_without_gpu(libpath):

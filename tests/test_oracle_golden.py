@@ -139,3 +139,53 @@ def test_courant():
     for case, ch, new in zip(z["dtc_cases"], z["dtc_changed"], z["dtc_new"]):
         c2, n2 = onl.dt_courant(*case)
         assert c2 == bool(ch) and n2 == new
+
+
+def _td_setup(name):
+    z = load_golden(name)
+    g = {k: z[k] for k in ("lm2l", "lm2m", "r", "or1", "or2", "or4", "orho1", "beta")}
+    g.update(l_max=int(z["l_max"]), CorFac=float(z["CorFac"]), l_anel=int(z["l_anel"]))
+    ins = {k[3:]: z[k] for k in z if k.startswith("in_")}
+    return z, g, ins
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_td_oracle(name):
+    """get_td + finish_exp restated in numpy against the reference's own outputs, in both
+    poloidal forms (standard with dpdt, double curl with beta and 1/rho), plus the
+    radial derivatives and the DCT-I."""
+    from oracle import td
+
+    z, g, ins = _td_setup(name)
+    for dc in (0, 1):
+        g["l_double_curl"] = dc
+        o = td.get_td(g, ins, z["D1"])
+        if dc:
+            assert rel_err(o["dwdt"], z["dwdt_dc_fin"]) < 1e-14
+        else:
+            assert rel_err(o["dwdt"], z["dwdt"]) < 1e-14
+            assert rel_err(o["dpdt"], z["dpdt"]) < 1e-14
+        for k in ("dzdt", "dsdt", "dxidt", "dbdt", "djdt"):
+            assert rel_err(o[k], z[k]) < 1e-14, k
+    assert rel_err(td.radial_apply(z["D1"], z["in_f"]), z["dr_f"]) < 1e-14
+    assert rel_err(td.radial_apply(z["D1"], z["in_f"]), z["ddr_f1"]) < 1e-14
+    assert rel_err(td.radial_apply(z["D2"], z["in_f"]), z["ddr_f2"]) < 1e-14
+    C = td.dct1_matrix(int(z["n_r_max"]))
+    assert rel_err(td.radial_apply(C, z["in_f"]), z["costf_f"]) < 1e-14
+    assert np.abs(C @ C - np.eye(C.shape[0])).max() < 1e-13  # self-inverse
+
+
+def test_radial_scheme_builders():
+    """The library's host-side Chebyshev and finite-difference builders reproduce the
+    reference's grids and derivative matrices."""
+    from magic_b200 import radial as R
+
+    z = load_golden("td_cheb")
+    r, D1, D2, _ = R.cheb_matrices(int(z["n_r_max"]))
+    assert rel_err(r, z["r"]) < 1e-15
+    assert rel_err(D1, z["D1"]) < 1e-13 and rel_err(D2, z["D2"]) < 1e-13
+    z = load_golden("td_fd_anel")
+    r = R.fd_grid(int(z["n_r_max"]))
+    assert rel_err(r, z["r"]) < 1e-15
+    D = R.fd_matrices(r, 4, 2)
+    assert rel_err(D[0], z["D1"]) < 1e-13 and rel_err(D[1], z["D2"]) < 1e-13
