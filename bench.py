@@ -299,6 +299,87 @@ def run_anel(args, rank, world):
                           "clocks": clocks.summary()}), flush=True)
 
 
+def run_td(args, rank, world):
+    """Optional line: the explicit time-derivative terms of one step (get_td with the
+    double-curl poloidal form + finish_exp radial derivatives, FP64) at l_max = 255 on
+    the 97-level fourth-order finite-difference grid, MHD, device-timed with inputs
+    resident; roofline against HBM (every input array read once, every output written
+    once)."""
+    from magic_b200 import Plan
+    from magic_b200.profiles import boussinesq_profiles
+    from magic_b200.radial import RadialScheme
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n_r = args.levels
+    plan = Plan(L_MAX, 1, device=dev)
+    sch = RadialScheme(n_r, "FD", fd_order=4, fd_order_bound=2, device=dev)
+    g = torch.Generator(device="cpu").manual_seed(rank)
+    ins_names = ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp",
+                 "w", "dw", "ddw", "z", "dz")
+    ins = {k: torch.randn(plan.lm_max, n_r, dtype=torch.complex128, generator=g).to(dev)
+           for k in ins_names}
+    bp = boussinesq_profiles(n_r, L_MAX, device=dev)
+    r = torch.as_tensor(sch.r, device=dev)
+    prof = dict(r=r, or1=1.0 / r, or2=1.0 / r ** 2, or4=1.0 / r ** 4, orho1=bp["orho1"],
+                beta=torch.zeros(n_r, dtype=torch.float64, device=dev))
+    out = None
+
+    def step():
+        nonlocal out
+        out = plan.get_td(ins, prof, 1e5, sch.D1, l_double_curl=True, l_heat=True, l_mag=True,
+                          out=out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    arrays = len(ins_names) + len(out)
+    byts = arrays * plan.lm_max * n_r * 16
+    peaks, src = measured_peaks()
+    ach = byts / (ms * 1e-3) / 1e9
+    line = {"metric": "explicit-term assemblies/s (get_td + finish_exp) @lmax=255, 1 B200",
+            "value": 1000.0 / ms, "unit": "calls/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "get_td double-curl + finish_exp, MHD, FD4 radial scheme",
+                       "l_max": L_MAX, "n_r": n_r, "arrays_in": len(ins_names),
+                       "arrays_out": len(out), "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "traffic": None,
+                         "algorithmic_bytes": byts, "peak_source": src},
+            "gpu_launches": args.steps, "clocks": clocks.summary()}
+    if rank == 0 and not args.no_cpu:
+        import numpy as np
+
+        from oracle import td as otd
+
+        sub = 3  # orders m < 3 of the same levels: a bounded CPU sample
+        rows = int(np.sum(plan.lm2m < sub))
+        h = {k: v[:rows].cpu().numpy() for k, v in ins.items()}
+        gg = dict(lm2l=plan.lm2l[:rows], lm2m=plan.lm2m[:rows], l_max=L_MAX, CorFac=1e5,
+                  l_anel=0, l_double_curl=1, **{k: v.cpu().numpy() for k, v in prof.items()})
+        t0, reps = time.perf_counter(), 0
+        while time.perf_counter() - t0 < 3.0:
+            otd.get_td(gg, h, sch.D1m)
+            reps += 1
+        dt = (time.perf_counter() - t0) / reps
+        line["cpu_baseline"] = {"value": rows / plan.lm_max / dt, "unit": "calls/s", "cores": 1,
+                                "kind": "port",
+                                "sample": f"numpy oracle on the {rows} lm rows with m < {sub} "
+                                          f"({reps} repeats, 3 s), scaled to all lm_max rows"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -325,9 +406,10 @@ def main():
     ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
-    ap.add_argument("--workload", default="bouss", choices=["bouss", "anel"],
+    ap.add_argument("--workload", default="bouss", choices=["bouss", "anel", "td"],
                     help="bouss: the headline Boussinesq MHD stage; anel: the fused anelastic "
-                         "stage at l_max=383 (extra line, split precision)")
+                         "stage at l_max=383 (extra line, split precision); td: the explicit "
+                         "time-derivative terms (get_td + finish_exp, FP64, extra line)")
     ap.add_argument("--levels", type=int, default=N_R,
                     help="radial levels (profiling runs use fewer than the 97 of the workload)")
     args = ap.parse_args()
@@ -341,6 +423,9 @@ def main():
         return
     if args.workload == "anel":
         run_anel(args, rank, world)
+        return
+    if args.workload == "td":
+        run_td(args, rank, world)
         return
 
     torch.cuda.set_device(local)

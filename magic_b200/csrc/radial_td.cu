@@ -12,11 +12,12 @@
 // consecutive output levels) read 32 consecutive values.  A dense Chebyshev
 // matrix has W = n_r; the fourth-order finite-difference ones W = 5.
 //
-// Explicit terms: one warp per lm row assembles the Coriolis and nonlinear
-// terms of get_td (magic_torch/get_td.py:58-308) level by level, keeps the
-// finish_exp auxiliaries (dVxVhLM, dVSrLM, dVXirLM, dVxBhLM) and the partial
-// terms in warp-private shared memory, applies D1 along the row and writes
-// the finished terms (update_wp.py:371-385, update_s.py:191-210,
+// Explicit terms: a CTA takes 8 consecutive lm rows of one m block (contiguous
+// in memory) and its threads stride over their (row, level) elements: the
+// Coriolis and nonlinear terms of get_td (magic_torch/get_td.py:58-308) go to
+// the outputs, the enabled finish_exp auxiliaries (dVxVhLM, dVSrLM, dVXirLM,
+// dVxBhLM) to shared memory; after one barrier the threads apply D1 along
+// each row and add the derivative terms (update_wp.py:371-385, update_s.py:191-210,
 // update_xi.py:183-202, update_b.py:514-528).  The l -+ 1 couplings read the
 // neighbouring rows lm -+ 1 of the same m block (m-major order).
 #include <algorithm>
@@ -99,6 +100,7 @@ struct TdArgs {
   const double *r, *or1, *or2, *or4, *orho1, *beta;
   double CorFac;
   int double_curl, heat, mag, chem, anel;
+  int naux;  // enabled auxiliaries, in the order double curl, heat, chem, mag
   OpView D1;
 };
 
@@ -107,122 +109,138 @@ __device__ __forceinline__ double clm_d(double l, double m) {
   return l > 0.0 ? sqrt((l + m) * (l - m) / ((2.0 * l - 1.0) * (2.0 * l + 1.0))) : 0.0;
 }
 
-// warp-private shared memory per row: 4 auxiliaries + 4 partial terms
-constexpr int kTdBufs = 8;
+constexpr int kTdRows = 8;       // consecutive lm rows (one m block) per CTA
+constexpr int kTdThreads = 256;
 
-__global__ void k_get_td(TdArgs a) {
+// CTA (row block x, order mc): rows l = m + kTdRows x .. of the m block, which
+// are contiguous in memory, so the threads stride over all (row, level)
+// elements of the block with fully coalesced loads.  Pass 1 writes the
+// partial terms and the enabled auxiliaries (shared memory); pass 2 adds
+// or2 D1 (auxiliary) along each row.
+__global__ void __launch_bounds__(kTdThreads, 4) k_get_td(TdArgs a) {
   extern __shared__ double2 tdbuf[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int wpb = blockDim.x >> 5;
   const int n_r = a.n_r;
   const int mc = blockIdx.y, m = mc * a.minc;
-  const int l = m + blockIdx.x * wpb + wib;
-  if (l > a.l_max) return;
-  const int lm = a.lstart[mc] + (l - m);
-  double2* buf = tdbuf + (int64_t)wib * kTdBufs * n_r;
-  double2 *xVh = buf, *xVS = buf + n_r, *xVX = buf + 2 * n_r, *xVB = buf + 3 * n_r;
-  double2 *pW = buf + 4 * n_r, *pS = buf + 5 * n_r, *pX = buf + 6 * n_r, *pJ = buf + 7 * n_r;
+  const int l0 = m + blockIdx.x * kTdRows;
+  if (l0 > a.l_max) return;
+  const int nrow = min(kTdRows, a.l_max + 1 - l0);
+  const int lm0 = a.lstart[mc] + (l0 - m);
+  const int nel = nrow * n_r;
+  const int span = kTdRows * n_r;  // one auxiliary array of the block
+  double2* xVh = tdbuf;
+  double2* xVS = xVh + (a.double_curl ? span : 0);
+  double2* xVX = xVS + (a.heat ? span : 0);
+  double2* xVB = xVX + (a.chem ? span : 0);
+  const double mf = (double)m, cf2 = 2.0 * a.CorFac;
+  const float rcp = 1.0f / (float)n_r;
 
-  // horizontal coefficients of this (l, m) (magic_torch/horizontal_data.py:103-130)
-  const double lf = (double)l, mf = (double)m;
-  const double c_l = clm_d(lf, mf), c_lp1 = clm_d(lf + 1.0, mf);
-  const double dLh = lf * (lf + 1.0);
-  const double dTh1S = (lf + 1.0) * c_l, dTh1A = lf * c_lp1;
-  const double dTh2S = (lf - 1.0) * c_l, dTh2A = (lf + 2.0) * c_lp1;
-  const double dTh3S = (lf - 1.0) * (lf + 1.0) * c_l, dTh3A = lf * (lf + 2.0) * c_lp1;
-  const double dTh4S = dTh1S * (lf - 1.0) * lf, dTh4A = dTh1A * (lf + 1.0) * (lf + 2.0);
-  // l+1 neighbour (masked at l_max) and l-1 neighbour (self, zero coefficient, at l = m)
-  const bool hasA = l < a.l_max;
-  const int64_t rowA = (int64_t)(hasA ? lm + 1 : lm) * a.ld_in;
-  const int64_t rowS = (int64_t)(l > m ? lm - 1 : lm) * a.ld_in;
-  const int64_t row = (int64_t)lm * a.ld_in;
-  const double mA = hasA ? 1.0 : 0.0;
-  const double cf2 = 2.0 * a.CorFac;
-  auto ldA = [&](const double2* f, int j) {
-    const double2 v = f[rowA + j];
-    return double2{mA * v.x, mA * v.y};
-  };
-
-  for (int j = lane; j < n_r; j += 32) {
+  for (int e = threadIdx.x; e < nel; e += kTdThreads) {
+    int rr = (int)((float)e * rcp);
+    rr -= (rr * n_r > e);
+    rr += ((rr + 1) * n_r <= e);
+    const int j = e - rr * n_r, l = l0 + rr, lm = lm0 + rr;
     const bool bnd = j == 0 || j == n_r - 1;
+    // horizontal coefficients of this (l, m) (magic_torch/horizontal_data.py:103-130)
+    const double lf = (double)l;
+    const double c_l = clm_d(lf, mf), c_lp1 = clm_d(lf + 1.0, mf);
+    const double dLh = lf * (lf + 1.0);
+    const double dTh1S = (lf + 1.0) * c_l, dTh1A = lf * c_lp1;
+    const double dTh2S = (lf - 1.0) * c_l, dTh2A = (lf + 2.0) * c_lp1;
+    const double dTh3S = (lf - 1.0) * (lf + 1.0) * c_l, dTh3A = lf * (lf + 2.0) * c_lp1;
+    const double dTh4S = dTh1S * (lf - 1.0) * lf, dTh4A = dTh1A * (lf + 1.0) * (lf + 2.0);
+    // l+1 neighbour (masked at l_max) and l-1 neighbour (self, zero coefficient, at l = m)
+    const bool hasA = l < a.l_max;
+    const int64_t row = (int64_t)lm * a.ld_in + j;
+    const int64_t rowA = hasA ? row + a.ld_in : row;
+    const int64_t rowS = l > m ? row - a.ld_in : row;
+    const double mA = hasA ? 1.0 : 0.0;
+    const int64_t o = (int64_t)lm * a.ld_out + j;
     const double or1 = a.or1[j], or2 = a.or2[j], or4 = a.or4[j], r = a.r[j];
     const double orho1 = a.orho1[j], beta = a.beta[j];
-    const double2 w = a.w[row + j], dw = a.dw[row + j], z = a.z[row + j];
-    const double2 zA = ldA(a.z, j), zS = a.z[rowS + j];
+    const double2 w = a.w[row], dw = a.dw[row], z = a.z[row];
+    const double2 zA = c_scale(mA, a.z[rowA]), zS = a.z[rowS];
     // toroidal velocity (get_td.py:151-181)
     {
-      const double2 dwA = ldA(a.dw, j), dwS = a.dw[rowS + j];
-      const double2 wA = ldA(a.w, j), wS = a.w[rowS + j];
+      const double2 dwA = c_scale(mA, a.dw[rowA]), dwS = a.dw[rowS];
+      const double2 wA = c_scale(mA, a.w[rowA]), wS = a.w[rowS];
       double2 cor = c_im(mf, z);
       cor = c_add(cor, c_scale(dTh3A, dwA));
       cor = c_add(cor, c_scale(or1 * dTh4A, wA));
       cor = c_add(cor, c_scale(dTh3S, dwS));
       cor = c_sub(cor, c_scale(or1 * dTh4S, wS));
-      const double2 v = c_add(c_scale(dLh, a.Advp[row + j]), c_scale(cf2 * or2, cor));
-      a.dzdt[(int64_t)lm * a.ld_out + j] = bnd ? double2{0.0, 0.0} : v;
+      const double2 v = c_add(c_scale(dLh, a.Advp[row]), c_scale(cf2 * or2, cor));
+      a.dzdt[o] = bnd ? double2{0.0, 0.0} : v;
     }
     if (a.double_curl) {
       // get_td.py:88-148
       double2 v;
       if (lm == 0) {
-        v = c_add(c_scale(or2, a.Advr[row + j]), c_scale(cf2 * or1 * dTh2A, zA));
+        v = c_add(c_scale(or2, a.Advr[row]), c_scale(cf2 * or1 * dTh2A, zA));
       } else {
-        const double2 ddw = a.ddw[row + j], dz = a.dz[row + j];
-        const double2 dzA = ldA(a.dz, j), dzS = a.dz[rowS + j];
+        const double2 ddw = a.ddw[row];
+        const double2 dzA = c_scale(mA, a.dz[rowA]), dzS = a.dz[rowS];
         double2 t = c_add(c_scale(-1.0, ddw), c_scale(beta, dw));
         t = c_add(t, c_scale((beta * or1 + or2) * dLh, w));
         double2 in = c_im(mf, t);
         in = c_add(in, c_scale(dTh3A, c_sub(dzA, c_scale(beta, zA))));
         in = c_add(in, c_scale(dTh3S, c_sub(dzS, c_scale(beta, zS))));
         in = c_add(in, c_scale(or1, c_sub(c_scale(dTh4A, zA), c_scale(dTh4S, zS))));
-        v = c_add(c_scale(dLh * or4 * orho1, a.Advr[row + j]), c_scale(cf2 * or2 * orho1, in));
+        v = c_add(c_scale(dLh * or4 * orho1, a.Advr[row]), c_scale(cf2 * or2 * orho1, in));
       }
-      pW[j] = bnd ? double2{0.0, 0.0} : v;
-      xVh[j] = bnd ? double2{0.0, 0.0} : c_scale(-orho1 * (r * r) * dLh, a.Advt[row + j]);
+      a.dwdt[o] = bnd ? double2{0.0, 0.0} : v;
+      xVh[e] = bnd ? double2{0.0, 0.0} : c_scale(-orho1 * (r * r) * dLh, a.Advt[row]);
     } else {
       // get_td.py:58-85 and 184-213
       double2 cor = c_im(mf, dw);
       cor = c_add(cor, c_scale(dTh2A, zA));
       cor = c_sub(cor, c_scale(dTh2S, zS));
-      const double2 v = c_add(c_scale(or2, a.Advr[row + j]), c_scale(cf2 * or1, cor));
-      a.dwdt[(int64_t)lm * a.ld_out + j] = bnd ? double2{0.0, 0.0} : v;
-      double2 cp = c_scale(-1.0, c_im(mf, c_add(dw, c_scale(or1 * dLh, w))));
-      cp = c_add(cp, c_scale(dTh3A, zA));
-      cp = c_add(cp, c_scale(dTh3S, zS));
-      const double2 p = c_add(c_scale(-dLh, a.Advt[row + j]), c_scale(cf2 * or2, cp));
-      if (a.dpdt) a.dpdt[(int64_t)lm * a.ld_out + j] = bnd ? double2{0.0, 0.0} : p;
+      const double2 v = c_add(c_scale(or2, a.Advr[row]), c_scale(cf2 * or1, cor));
+      a.dwdt[o] = bnd ? double2{0.0, 0.0} : v;
+      if (a.dpdt) {
+        double2 cp = c_scale(-1.0, c_im(mf, c_add(dw, c_scale(or1 * dLh, w))));
+        cp = c_add(cp, c_scale(dTh3A, zA));
+        cp = c_add(cp, c_scale(dTh3S, zS));
+        const double2 p = c_add(c_scale(-dLh, a.Advt[row]), c_scale(cf2 * or2, cp));
+        a.dpdt[o] = bnd ? double2{0.0, 0.0} : p;
+      }
     }
     if (a.heat) {
-      pS[j] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VSt[row + j]);
-      xVS[j] = bnd ? double2{0.0, 0.0} : a.VSr[row + j];
+      a.dsdt[o] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VSt[row]);
+      xVS[e] = bnd ? double2{0.0, 0.0} : a.VSr[row];
     }
     if (a.chem) {
-      pX[j] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VXit[row + j]);
-      xVX[j] = bnd ? double2{0.0, 0.0} : a.VXir[row + j];
+      a.dxidt[o] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VXit[row]);
+      xVX[e] = bnd ? double2{0.0, 0.0} : a.VXir[row];
     }
     if (a.mag) {
-      a.dbdt[(int64_t)lm * a.ld_out + j] =
-          bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VxBp[row + j]);
-      pJ[j] = bnd ? double2{0.0, 0.0} : c_scale(dLh * or4, a.VxBr[row + j]);
-      const double2 h = c_scale(-dLh, a.VxBt[row + j]);
-      xVB[j] = (lm == 0 && bnd) ? double2{0.0, 0.0} : c_scale(r * r, h);
+      a.dbdt[o] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VxBp[row]);
+      a.djdt[o] = bnd ? double2{0.0, 0.0} : c_scale(dLh * or4, a.VxBr[row]);
+      const double2 h = c_scale(-dLh, a.VxBt[row]);
+      xVB[e] = (lm == 0 && bnd) ? double2{0.0, 0.0} : c_scale(r * r, h);
     }
   }
-  __syncwarp();
-  // finish_exp: the radial derivative of each auxiliary along this row
-  for (int j = lane; j < n_r; j += 32) {
+  if (a.naux == 0) return;
+  __syncthreads();
+  // finish_exp: the radial derivative of each auxiliary along its row, added to
+  // the partial term this thread wrote above (same element, same thread)
+  for (int e = threadIdx.x; e < nel; e += kTdThreads) {
+    int rr = (int)((float)e * rcp);
+    rr -= (rr * n_r > e);
+    rr += ((rr + 1) * n_r <= e);
+    const int j = e - rr * n_r;
+    const int64_t o = (int64_t)(lm0 + rr) * a.ld_out + j;
+    const int base = rr * n_r;
     const double or2 = a.or2[j], orho1 = a.orho1[j];
-    const int64_t o = (int64_t)lm * a.ld_out + j;
-    if (a.double_curl) a.dwdt[o] = c_add(pW[j], c_scale(or2, op_row(a.D1, xVh, j)));
+    if (a.double_curl) a.dwdt[o] = c_add(a.dwdt[o], c_scale(or2, op_row(a.D1, xVh + base, j)));
     if (a.heat) {
-      double2 v = c_sub(pS[j], c_scale(or2, op_row(a.D1, xVS, j)));
+      double2 v = c_sub(a.dsdt[o], c_scale(or2, op_row(a.D1, xVS + base, j)));
       a.dsdt[o] = a.anel ? c_scale(orho1, v) : v;
     }
     if (a.chem) {
-      double2 v = c_sub(pX[j], c_scale(or2, op_row(a.D1, xVX, j)));
+      double2 v = c_sub(a.dxidt[o], c_scale(or2, op_row(a.D1, xVX + base, j)));
       a.dxidt[o] = a.anel ? c_scale(orho1, v) : v;
     }
-    if (a.mag) a.djdt[o] = c_add(pJ[j], c_scale(or2, op_row(a.D1, xVB, j)));
+    if (a.mag) a.djdt[o] = c_add(a.djdt[o], c_scale(or2, op_row(a.D1, xVB + base, j)));
   }
 }
 
@@ -420,13 +438,12 @@ int mt_get_td(const mt_plan* p, int n_r, const mt_td_in* in, const mt_td_out* ou
   a.anel = q->l_anel != 0;
   if (need_d1) a.D1 = view(D1);
   else a.D1 = OpView{n_r, 0, nullptr, nullptr};
-  const size_t per_warp = (size_t)kTdBufs * n_r * sizeof(double2);
-  MT_REQUIRE(per_warp <= 200 * 1024, MT_ERR_UNSUPPORTED, "n_r too large for the explicit-term kernel");
-  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, kRadialSmemBudget / per_warp));
-  const size_t sm = wpb * per_warp;
+  a.naux = (int)a.double_curl + (int)a.heat + (int)a.chem + (int)a.mag;
+  const size_t sm = (size_t)a.naux * kTdRows * n_r * sizeof(double2);
+  MT_REQUIRE(sm <= 200 * 1024, MT_ERR_UNSUPPORTED, "n_r too large for the explicit-term kernel");
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_get_td, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const dim3 grid((p->l_max + 1 + wpb - 1) / wpb, p->n_m);
-  k_get_td<<<grid, 32 * wpb, sm, (cudaStream_t)stream>>>(a);
+  const dim3 grid((p->l_max + 1 + kTdRows - 1) / kTdRows, p->n_m);
+  k_get_td<<<grid, kTdThreads, sm, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

@@ -77,8 +77,9 @@ def get_td(g, ins, D1):
     (update_b.py:514-528).
 
     g: dict with lm2l, lm2m, l_max, r, or1, or2, or4, orho1, beta, CorFac, l_anel,
-    l_double_curl.  ins: Advr, Advt, Advp, VSr, VSt, VxBr, VxBt, VxBp, VXir, VXit,
-    w, dw, ddw, z, dz (lm_max, n_r) complex.  Returns a dict of outputs.
+    l_double_curl.  ins: Advr, Advt, Advp, w, dw, ddw, z, dz (lm_max, n_r) complex,
+    plus VSr, VSt / VXir, VXit / VxBr, VxBt, VxBp for the entropy / composition /
+    induction terms (each group only when present).  Returns a dict of outputs.
     """
     h = lm_arrays(g["lm2l"], g["lm2m"])
     S, A, mA = neighbours(g["lm2l"], g["lm2m"], g["l_max"])
@@ -135,6 +136,8 @@ def get_td(g, ins, D1):
     out["dzdt"] = bnd0(dzdt)
     # get_td.py:216-237 + update_s.py:191-210 (and the composition twin)
     for part, radial, name in (("VSt", "VSr", "dsdt"), ("VXit", "VXir", "dxidt")):
+        if part not in ins:
+            continue
         d = bnd0(dLh * ins[part])
         q = bnd0(ins[radial].copy())
         res = d - or2 * radial_apply(D1, q)
@@ -142,6 +145,8 @@ def get_td(g, ins, D1):
             res = orho1 * res
         out[name] = res
     # get_td.py:266-308 + update_b.py:514-528
+    if "VxBp" not in ins:
+        return out
     out["dbdt"] = bnd0(dLh * ins["VxBp"])
     dj = bnd0(dLh * or4 * ins["VxBr"])
     dVxBh = -dLh * ins["VxBt"] * r2
