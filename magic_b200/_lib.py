@@ -92,6 +92,13 @@ class TdParams(C.Structure):
                [(n, C.c_int) for n in ("l_double_curl", "l_heat", "l_mag", "l_chem", "l_anel")]
 
 
+class ScalarUpdate(C.Structure):
+    _fields_ = [(n, _dp) for n in ("s", "ds", "old", "impl", "expl0", "expl1", "top", "bot")] + \
+               [("ld", _i64)] + \
+               [(n, C.c_double) for n in ("w_old", "w_impl", "w_expl0", "w_expl1", "opr")] + \
+               [(n, _dp) for n in ("hdif", "kappa", "d1c", "or2")]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "mt_plan_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
@@ -130,6 +137,10 @@ _PROTOS = {
                                    _dp]),
     "mt_get_td": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TdIn), C.POINTER(TdOut),
                             C.POINTER(TdParams), C.c_void_p, _dp]),
+    "mt_lop_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
+    "mt_lop_destroy": (C.c_int, [C.c_void_p]),
+    "mt_update_scalar": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ScalarUpdate), C.c_void_p,
+                                   C.c_void_p, C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }

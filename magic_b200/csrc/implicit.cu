@@ -1,0 +1,194 @@
+// Implicit (IMEX) update of a scalar field: entropy or composition (FP64).
+//
+// Replaces magic_torch/update_s.py:213-271 (updateS; updateXi,
+// update_xi.py:208-262, has the same form) with the CNAB2 right-hand side of
+// time_scheme.py:82-96 and the history rotation of time_scheme.py:130-143.
+//
+// The per-degree solve is an operator set (mt_lop): one dense n_r x n_r
+// matrix per l, built on the host as the inverse of the reference's
+// preconditioned LHS (update_s.py:67-134); for the Chebyshev scheme the
+// DCT-I back to grid values and the Chebyshev truncation are folded in
+// (M_l = C T A_l^-1).  Matrices are stored transposed, MT[l][k][j], so the 32
+// lanes of a warp (32 consecutive output levels j) read consecutive values.
+//
+// k_update_scalar: CTA = (degree l, chunk of orders m), one warp per lm row:
+//   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1, rows 0 and
+//   n_r - 1 replaced by the boundary values; expl1 <- expl0 (rotation);
+//   s = M_l rhs, imaginary part dropped for m = 0; old <- s;
+//   ds = D1 s, d2s = D2 s;
+//   impl <- opr hdif_l kappa (d2s + d1c ds - l(l+1) or2 s).
+// Rows of one l share M_l through L1 (the CTA's warps and co-resident CTAs).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "radial_op.cuh"
+
+struct mt_lop {
+  int n_l = 0, n_r = 0, device = 0;
+  double* mt = nullptr;  // (n_l, n_r, n_r) transposed: mt[(l * n_r + k) * n_r + j] = M_l[j][k]
+};
+
+namespace mt {
+
+namespace {
+
+constexpr int kUsWarps = 8;
+
+struct UsArgs {
+  int n_r, l_max, minc, n_m;
+  const int* lstart;
+  double2 *s, *ds, *old, *impl, *expl0, *expl1;
+  const double2 *top, *bot;
+  int64_t ld;
+  double w_old, w_impl, w_expl0, w_expl1, opr;
+  const double *hdif, *kappa, *d1c, *or2;
+  const double* mt;
+  OpView D1, D2;
+};
+
+__global__ void __launch_bounds__(32 * kUsWarps) k_update_scalar(UsArgs a) {
+  extern __shared__ double2 usbuf[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int n_r = a.n_r, l = blockIdx.x;
+  const int mc = blockIdx.y * kUsWarps + wib, m = mc * a.minc;
+  if (mc >= a.n_m || m > l) return;
+  const int64_t row = (int64_t)(a.lstart[mc] + (l - m)) * a.ld;
+  double2* rhs = usbuf + (int64_t)wib * 2 * n_r;
+  double2* x = rhs + n_r;
+  const double2 zero = {0.0, 0.0};
+  const int lm = a.lstart[mc] + (l - m);
+  for (int k = lane; k < n_r; k += 32) {
+    const double2 o = a.old[row + k], im = a.impl[row + k];
+    const double2 e0 = a.expl0[row + k], e1 = a.expl1[row + k];
+    double2 v;
+    v.x = a.w_old * o.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
+    v.y = a.w_old * o.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
+    if (k == 0) v = a.top ? a.top[lm] : zero;
+    if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
+    rhs[k] = v;
+    a.expl1[row + k] = e0;
+  }
+  __syncwarp();
+  const double* M = a.mt + (int64_t)l * n_r * n_r;
+  for (int j = lane; j < n_r; j += 32) {
+    double2 acc = zero;
+    for (int k = 0; k < n_r; ++k) {
+      const double c = __ldg(M + (int64_t)k * n_r + j);
+      acc.x = fma(c, rhs[k].x, acc.x);
+      acc.y = fma(c, rhs[k].y, acc.y);
+    }
+    if (m == 0) acc.y = 0.0;
+    x[j] = acc;
+    a.s[row + j] = acc;
+    a.old[row + j] = acc;
+  }
+  __syncwarp();
+  const double dL = (double)l * (l + 1.0), ch = a.opr * a.hdif[l];
+  for (int j = lane; j < n_r; j += 32) {
+    const double2 d1 = op_row(a.D1, x, j), d2 = op_row(a.D2, x, j);
+    a.ds[row + j] = d1;
+    const double c1 = a.d1c[j], c0 = dL * a.or2[j], kap = ch * a.kappa[j];
+    a.impl[row + j] = double2{kap * (d2.x + c1 * d1.x - c0 * x[j].x),
+                              kap * (d2.y + c1 * d1.y - c0 * x[j].y)};
+  }
+}
+
+int check_lop(const mt_lop* op) {
+  MT_REQUIRE(op && op->mt, MT_ERR_ARG, "null per-degree operator");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == op->device, MT_ERR_ARG,
+             "per-degree operator used on a different device than it was built on");
+  return MT_OK;
+}
+
+}  // namespace
+
+}  // namespace mt
+
+using namespace mt;
+
+extern "C" {
+
+int mt_lop_create(int n_l, int n_r, const double* M, mt_lop** out) {
+  MT_REQUIRE(out && M && n_l >= 1 && n_r >= 2 && n_r <= 1024, MT_ERR_ARG,
+             "bad per-degree operator argument");
+  *out = nullptr;
+  const size_t per = (size_t)n_r * n_r;
+  std::vector<double> t(per * n_l);
+  for (int l = 0; l < n_l; ++l)
+    for (int j = 0; j < n_r; ++j)
+      for (int k = 0; k < n_r; ++k) {
+        const double v = M[l * per + (size_t)j * n_r + k];
+        MT_REQUIRE(std::isfinite(v), MT_ERR_ARG, "per-degree operator not finite");
+        t[l * per + (size_t)k * n_r + j] = v;
+      }
+  mt_lop* op = new mt_lop();
+  op->n_l = n_l;
+  op->n_r = n_r;
+  if (cudaGetDevice(&op->device) != cudaSuccess ||
+      cudaMalloc(&op->mt, t.size() * sizeof(double)) != cudaSuccess ||
+      cudaMemcpy(op->mt, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+    if (op->mt) cudaFree(op->mt);
+    delete op;
+    set_error("per-degree operator allocation or upload failed");
+    return MT_ERR_CUDA;
+  }
+  *out = op;
+  return MT_OK;
+}
+
+int mt_lop_destroy(mt_lop* op) {
+  if (!op) return MT_OK;
+  if (op->mt) cudaFree(op->mt);
+  delete op;
+  return MT_OK;
+}
+
+int mt_update_scalar(const mt_plan* p, int n_r, const mt_scalar_update* u, const mt_lop* solve,
+                     const mt_radial_op* D1, const mt_radial_op* D2, void* stream) {
+  MT_REQUIRE(p && u, MT_ERR_ARG, "null argument");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == p->device, MT_ERR_ARG, "plan used on a different device than it was built on");
+  MT_TRY(check_lop(solve));
+  MT_TRY(check_radial_op(D1));
+  MT_TRY(check_radial_op(D2));
+  MT_REQUIRE(solve->n_r == n_r && radial_op_size(D1) == n_r && radial_op_size(D2) == n_r,
+             MT_ERR_ARG, "operator sizes differ from n_r");
+  MT_REQUIRE(solve->n_l == p->l_max + 1, MT_ERR_ARG, "solve operators must cover l = 0..l_max");
+  MT_REQUIRE(n_r >= 3 && u->ld >= n_r, MT_ERR_ARG, "bad radial size or stride");
+  MT_REQUIRE(u->s && u->ds && u->old && u->impl && u->expl0 && u->expl1, MT_ERR_ARG,
+             "null field or time array");
+  MT_REQUIRE(u->hdif && u->kappa && u->d1c && u->or2, MT_ERR_ARG, "null coefficient array");
+  UsArgs a{};
+  a.n_r = n_r;
+  a.l_max = p->l_max;
+  a.minc = p->minc;
+  a.n_m = p->n_m;
+  a.lstart = p->d_lstart;
+  auto d = [](double* x) { return (double2*)x; };
+  a.s = d(u->s); a.ds = d(u->ds); a.old = d(u->old); a.impl = d(u->impl);
+  a.expl0 = d(u->expl0); a.expl1 = d(u->expl1);
+  a.top = (const double2*)u->top;
+  a.bot = (const double2*)u->bot;
+  a.ld = u->ld;
+  a.w_old = u->w_old; a.w_impl = u->w_impl; a.w_expl0 = u->w_expl0; a.w_expl1 = u->w_expl1;
+  a.opr = u->opr;
+  a.hdif = u->hdif; a.kappa = u->kappa; a.d1c = u->d1c; a.or2 = u->or2;
+  a.mt = solve->mt;
+  a.D1 = radial_op_view(D1);
+  a.D2 = radial_op_view(D2);
+  const size_t sm = (size_t)kUsWarps * 2 * n_r * sizeof(double2);
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_scalar,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const dim3 grid(p->l_max + 1, (p->n_m + kUsWarps - 1) / kUsWarps);
+  k_update_scalar<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+}  // extern "C"

@@ -24,13 +24,7 @@
 #include <cmath>
 #include <vector>
 
-#include "common.cuh"
-
-struct mt_radial_op {
-  int n_r = 0, W = 0, device = 0;
-  int* k0 = nullptr;       // (n_r) first column of each row's band
-  double* vals = nullptr;  // (W, n_r) band-transposed values
-};
+#include "radial_op.cuh"
 
 namespace mt {
 
@@ -41,23 +35,6 @@ __device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return {a.x - b
 __device__ __forceinline__ double2 c_scale(double s, double2 a) { return {s * a.x, s * a.y}; }
 // i m x
 __device__ __forceinline__ double2 c_im(double m, double2 a) { return {-m * a.y, m * a.x}; }
-__device__ __forceinline__ double2 c_fma(double s, double2 a, double2 acc) {
-  return {fma(s, a.x, acc.x), fma(s, a.y, acc.y)};
-}
-
-struct OpView {
-  int n_r, W;
-  const int* k0;
-  const double* vals;
-};
-
-// (D f)[j] for one row f staged in shared memory
-__device__ __forceinline__ double2 op_row(const OpView& op, const double2* f, int j) {
-  const int k0 = __ldg(op.k0 + j);
-  double2 acc = {0.0, 0.0};
-  for (int kk = 0; kk < op.W; ++kk) acc = c_fma(__ldg(op.vals + (int64_t)kk * op.n_r + j), f[k0 + kk], acc);
-  return acc;
-}
 
 struct ApplyArgs {
   OpView op[2];
@@ -244,9 +221,12 @@ __global__ void __launch_bounds__(kTdThreads, 4) k_get_td(TdArgs a) {
   }
 }
 
-OpView view(const mt_radial_op* op) { return OpView{op->n_r, op->W, op->k0, op->vals}; }
 
-int check_op(const mt_radial_op* op) {
+constexpr size_t kRadialSmemBudget = 96 * 1024;
+
+}  // namespace
+
+int check_radial_op(const mt_radial_op* op) {
   MT_REQUIRE(op && op->vals, MT_ERR_ARG, "null radial operator");
   int dev = -1;
   MT_CHECK_CUDA(cudaGetDevice(&dev));
@@ -254,10 +234,6 @@ int check_op(const mt_radial_op* op) {
              "radial operator used on a different device than it was built on");
   return MT_OK;
 }
-
-constexpr size_t kRadialSmemBudget = 96 * 1024;
-
-}  // namespace
 
 }  // namespace mt
 
@@ -341,7 +317,7 @@ int mt_radial_op_bandwidth(const mt_radial_op* op) { return op ? op->W : 0; }
 static int radial_apply_n(const mt_radial_op* const* ops, int nop, int nrows, const double* in,
                           int64_t ld_in, double* const* out, int64_t ld_out, void* stream) {
   for (int o = 0; o < nop; ++o) {
-    MT_TRY(check_op(ops[o]));
+    MT_TRY(check_radial_op(ops[o]));
     MT_REQUIRE(ops[o]->n_r == ops[0]->n_r, MT_ERR_ARG, "radial operators of different sizes");
     MT_REQUIRE(out[o], MT_ERR_ARG, "null radial output");
   }
@@ -351,7 +327,7 @@ static int radial_apply_n(const mt_radial_op* const* ops, int nop, int nrows, co
   if (nrows == 0) return MT_OK;
   ApplyArgs a{};
   for (int o = 0; o < nop; ++o) {
-    a.op[o] = view(ops[o]);
+    a.op[o] = radial_op_view(ops[o]);
     a.out[o] = (double2*)out[o];
   }
   a.nop = nop;
@@ -403,7 +379,7 @@ int mt_get_td(const mt_plan* p, int n_r, const mt_td_in* in, const mt_td_out* ou
              MT_ERR_ARG, "null velocity field or output");
   const bool need_d1 = q->l_double_curl || q->l_heat || q->l_chem || q->l_mag;
   if (need_d1) {
-    MT_TRY(check_op(D1));
+    MT_TRY(check_radial_op(D1));
     MT_REQUIRE(D1->n_r == n_r, MT_ERR_ARG, "D1 size differs from n_r");
   }
   if (q->l_double_curl) MT_REQUIRE(in->ddw && in->dz, MT_ERR_ARG, "double curl needs ddw and dz");
@@ -436,7 +412,7 @@ int mt_get_td(const mt_plan* p, int n_r, const mt_td_in* in, const mt_td_out* ou
   a.chem = q->l_chem != 0;
   a.mag = q->l_mag != 0;
   a.anel = q->l_anel != 0;
-  if (need_d1) a.D1 = view(D1);
+  if (need_d1) a.D1 = radial_op_view(D1);
   else a.D1 = OpView{n_r, 0, nullptr, nullptr};
   a.naux = (int)a.double_curl + (int)a.heat + (int)a.chem + (int)a.mag;
   const size_t sm = (size_t)a.naux * kTdRows * n_r * sizeof(double2);

@@ -38,6 +38,25 @@ def cheb_grid(n_r, radratio=0.35):
     return 0.5 * (r_cmb - r_icb) * x + 0.5 * (r_icb + r_cmb), x
 
 
+def cheb_polynomials(n_r, radratio=0.35):
+    """(rMat, drMat, d2rMat): T_n(x_i) and its first two r-derivatives at the
+    Gauss-Lobatto points (magic_torch/chebyshev.py:62-110)."""
+    _, x = cheb_grid(n_r, radratio)
+    r_cmb = 1.0 / (1.0 - radratio)
+    drx = 2.0 / (r_cmb - (r_cmb - 1.0))
+    T = np.zeros((n_r, n_r))
+    dT = np.zeros((n_r, n_r))
+    d2T = np.zeros((n_r, n_r))
+    T[:, 0] = 1.0
+    T[:, 1] = x
+    dT[:, 1] = drx
+    for c in range(2, n_r):
+        T[:, c] = 2.0 * x * T[:, c - 1] - T[:, c - 2]
+        dT[:, c] = 2.0 * drx * T[:, c - 1] + 2.0 * x * dT[:, c - 1] - dT[:, c - 2]
+        d2T[:, c] = 4.0 * drx * dT[:, c - 1] + 2.0 * x * d2T[:, c - 1] - d2T[:, c - 2]
+    return T, dT, d2T
+
+
 def cheb_matrices(n_r, radratio=0.35, n_cheb=None):
     """(r, D1, D2, D3): D_k = d^k rMat . rMat^-1 with rMat[i, n] = T_n(x_i) and the
     derivative columns from the three-term recurrence with the linear map
@@ -271,10 +290,20 @@ class RadialScheme:
 
     def __init__(self, n_r, scheme="chebyshev", radratio=0.35, n_cheb=None, fd_order=2,
                  fd_order_bound=2, fd_stretch=0.3, fd_ratio=0.1, device=None):
-        if scheme.upper() == "FD":
+        self.n_r = n_r
+        self.chebyshev = scheme.upper() != "FD"
+        self.n_cheb = n_r if (n_cheb is None or not self.chebyshev) else min(n_cheb, n_r)
+        if not self.chebyshev:
             self.r = fd_grid(n_r, radratio, fd_stretch, fd_ratio)
             mats = fd_matrices(self.r, fd_order, fd_order_bound)[:3]
+            # grid-point unknowns: rMat = I, rnorm = boundary_fac = 1
+            # (magic_torch/finite_differences.py:296-300)
+            self.rMat, self.drMat, self.d2rMat = np.eye(n_r), mats[0], mats[1]
+            self.rnorm, self.boundary_fac = 1.0, 1.0
         else:
             self.r, *mats = cheb_matrices(n_r, radratio, n_cheb)
+            self.rMat, self.drMat, self.d2rMat = cheb_polynomials(n_r, radratio)
+            # Chebyshev-coefficient unknowns (magic_torch/chebyshev.py:47-52)
+            self.rnorm, self.boundary_fac = math.sqrt(2.0 / (n_r - 1)), 0.5
         self.D1m, self.D2m, self.D3m = mats
         self.D1, self.D2, self.D3 = (RadialOp(M, device=device) for M in mats)

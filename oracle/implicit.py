@@ -1,0 +1,72 @@
+"""CPU restatement (numpy, FP64) of the implicit update of a scalar field
+(entropy; composition has the same form) with the CNAB2 scheme.  Test
+infrastructure only: the library never imports this module.
+
+Pinned against the reference's own updateS outputs (tests/golden/td_*.npz).
+"""
+
+import numpy as np
+
+from oracle.td import dct1_matrix
+
+
+def cnab2_weights(dt1, dt2, alpha=0.6):
+    """wimp, wimp_lin, wexp of CNAB2 (magic_torch/time_scheme.py:56-73)."""
+    return ([1.0], [alpha * dt1, (1.0 - alpha) * dt1],
+            [(1.0 + 0.5 * dt1 / dt2) * dt1, -0.5 * dt1 * dt1 / dt2])
+
+
+def s_matrix(l, mats, prof, wimp_lin0, opr, hdif_l, n_cheb):
+    """Entropy LHS of degree l (magic_torch/update_s.py:67-134): rows 1..N-2 are
+    rnorm (rMat - wimp opr hdif kappa (d2rMat + (beta + dLtemp0 + 2/r + dLkappa) drMat
+    - l(l+1)/r^2 rMat)), rows 0 and N-1 the Dirichlet rows rnorm rMat, Chebyshev
+    columns >= n_cheb zeroed in those rows, columns 0 and N-1 scaled by boundary_fac."""
+    rMat, drMat, d2rMat, rnorm, bfac = mats
+    N = rMat.shape[0]
+    d1c = (prof["beta"] + prof["dLtemp0"] + 2.0 * prof["or1"] + prof["dLkappa"])[:, None]
+    dL = float(l * (l + 1))
+    dat = rnorm * (rMat - wimp_lin0 * opr * hdif_l * prof["kappa"][:, None] * (
+        d2rMat + d1c * drMat - dL * prof["or2"][:, None] * rMat))
+    dat[0, :] = rnorm * rMat[0, :]
+    dat[N - 1, :] = rnorm * rMat[N - 1, :]
+    if n_cheb < N:
+        dat[0, n_cheb:] = 0.0
+        dat[N - 1, n_cheb:] = 0.0
+    dat[:, 0] *= bfac
+    dat[:, N - 1] *= bfac
+    return dat
+
+
+def update_s(g, mats, prof, st, weights, opr, hdif, tops, bots, D1, D2, chebyshev, n_cheb):
+    """One updateS (magic_torch/update_s.py:213-271): CNAB2 right-hand side
+    (time_scheme.py:82-96) with the boundary values in rows 0 and N-1, a solve per
+    degree l (row-preconditioned LU), m = 0 coefficients made real, the DCT-I to
+    grid values (Chebyshev only), then ds, d2s and the implicit term
+    opr hdif kappa (d2s + (beta + dLtemp0 + 2/r + dLkappa) ds - l(l+1)/r^2 s).
+
+    st: dict old, impl, expl0, expl1 ((lm_max, N) complex).  Returns s, ds, impl,
+    old, expl1 after the update (expl0 is left for the next explicit stage)."""
+    wimp, wimp_lin, wexp = weights
+    N = st["old"].shape[1]
+    rhs = wimp[0] * st["old"] + wimp_lin[1] * st["impl"] + wexp[0] * st["expl0"] \
+        + wexp[1] * st["expl1"]
+    rhs[:, 0] = tops
+    rhs[:, N - 1] = bots
+    x = np.empty_like(rhs)
+    for l in range(g["l_max"] + 1):
+        rows = np.nonzero(g["lm2l"] == l)[0]
+        dat = s_matrix(l, mats, prof, wimp_lin[0], opr, hdif[l], n_cheb)
+        fac = 1.0 / np.abs(dat).max(axis=1)
+        x[rows] = np.linalg.solve(fac[:, None] * dat, (fac[None, :] * rhs[rows]).T).T
+    m0 = g["lm2m"] == 0
+    x[m0] = x[m0].real
+    if chebyshev:
+        if n_cheb < N:
+            x[:, n_cheb:] = 0.0
+        x = x @ dct1_matrix(N).T
+    ds, d2s = x @ D1.T, x @ D2.T
+    d1c = prof["beta"] + prof["dLtemp0"] + 2.0 * prof["or1"] + prof["dLkappa"]
+    dLh = (g["lm2l"] * (g["lm2l"] + 1.0))[:, None]
+    impl = opr * hdif[g["lm2l"]][:, None] * prof["kappa"][None, :] * (
+        d2s + d1c[None, :] * ds - dLh * prof["or2"][None, :] * x)
+    return dict(s=x, ds=ds, impl=impl, old=x.copy(), expl1=st["expl0"].copy())

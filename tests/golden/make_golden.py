@@ -198,7 +198,8 @@ def worker_td(name, ref):
     from magic_torch.update_b import finish_exp_mag
     from magic_torch.update_xi import finish_exp_comp
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a))
-    n = lambda x: x.detach().cpu().numpy()
+    # copies: updateS later overwrites its time arrays in place
+    n = lambda x: x.detach().cpu().numpy().copy()
     rng = np.random.default_rng(321)
     N, lm = params.n_r_max, params.lm_max
     l_of = n(blocking.st_lm2l)
@@ -233,6 +234,35 @@ def worker_td(name, ref):
     d1, d2 = rd.get_ddr(T["f"])
     out["ddr_f1"], out["ddr_f2"] = n(d1), n(d2)
     out["costf_f"] = n(costf(T["f"]))
+    # one implicit entropy update (magic_torch/update_s.py:67-271) with CNAB2
+    # weights from two different time steps
+    from magic_torch.time_scheme import tscheme
+    from magic_torch import update_s as us, dt_fields as dtf, horizontal_data as hd
+    from magic_torch import radial_functions as rf2
+    tscheme.dt[0] = 1e-4
+    tscheme.dt[1] = 1.3e-4
+    tscheme.set_weights()
+    us.build_s_matrices(tscheme.wimp_lin[0].item())
+    ta = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+    ta.old[:, :, 0] = t(_spec(rng, lm, l_of, N))
+    ta.impl[:, :, 0] = t(_spec(rng, lm, l_of, N))
+    ta.expl[:, :, 0] = t(_spec(rng, lm, l_of, N))
+    ta.expl[:, :, 1] = t(_spec(rng, lm, l_of, N))
+    out.update(s_old=n(ta.old[:, :, 0]), s_impl=n(ta.impl[:, :, 0]),
+               s_expl0=n(ta.expl[:, :, 0]), s_expl1=n(ta.expl[:, :, 1]),
+               wimp=n(tscheme.wimp), wimp_lin=n(tscheme.wimp_lin), wexp=n(tscheme.wexp),
+               opr=float(pc.opr), hdif_S=n(hd.hdif_S), kappa=n(rf2.kappa),
+               dLtemp0=n(rf2.dLtemp0), dLkappa=n(rf2.dLkappa), bots=n(us._bots),
+               tops=n(us._tops), n_cheb_max=int(params.n_cheb_max))
+    from magic_torch import radial_scheme as rs
+    out.update(rMat=n(rs.rMat), drMat=n(rs.drMat), d2rMat=n(rs.d2rMat),
+               rnorm=float(rs.rnorm), boundary_fac=float(rs.boundary_fac),
+               chebyshev=int(params.radial_scheme != "FD"))
+    s_new = torch.zeros(lm, N, dtype=torch.complex128)
+    ds_new = torch.zeros_like(s_new)
+    us.updateS(s_new, ds_new, ta, tscheme)
+    out.update(s_new=n(s_new), ds_new=n(ds_new), s_impl_new=n(ta.impl[:, :, 0]),
+               s_old_new=n(ta.old[:, :, 0]), s_expl1_new=n(ta.expl[:, :, 1]))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

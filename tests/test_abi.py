@@ -56,7 +56,8 @@ def test_struct_layouts_match_header(libpath, tmp_path):
                "mt_bouss_in": _lib.BoussIn, "mt_bouss_out": _lib.BoussOut,
                "mt_bouss_params": _lib.BoussParams, "mt_anel_in": _lib.AnelIn,
                "mt_anel_out": _lib.AnelOut, "mt_anel_stage_params": _lib.AnelStageParams,
-               "mt_td_in": _lib.TdIn, "mt_td_out": _lib.TdOut, "mt_td_params": _lib.TdParams}
+               "mt_td_in": _lib.TdIn, "mt_td_out": _lib.TdOut, "mt_td_params": _lib.TdParams,
+               "mt_scalar_update": _lib.ScalarUpdate}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
              "int main(void){"]
     for cname, py in structs.items():
@@ -105,6 +106,11 @@ def test_radial_op_rejects_bad_arguments(libpath):
     assert L.mt_radial_op_create_dct1(1, ctypes.byref(h)) == 1
     assert L.mt_radial_op_destroy(None) == 0
     assert L.mt_radial_op_bandwidth(None) == 0
+    M = (ctypes.c_double * 8)(*([1.0] * 8))
+    assert L.mt_lop_create(0, 2, M, ctypes.byref(h)) == 1
+    bad = (ctypes.c_double * 8)(*([1.0] * 7 + [float("inf")]))
+    assert L.mt_lop_create(2, 2, bad, ctypes.byref(h)) == 1
+    assert L.mt_lop_destroy(None) == 0
 
 
 def test_no_cpu_fallback_without_gpu(libpath):

@@ -189,3 +189,60 @@ def test_radial_scheme_builders():
     assert rel_err(r, z["r"]) < 1e-15
     D = R.fd_matrices(r, 4, 2)
     assert rel_err(D[0], z["D1"]) < 1e-13 and rel_err(D[1], z["D2"]) < 1e-13
+
+
+def _s_case(name):
+    z = load_golden(name)
+    g = dict(lm2l=z["lm2l"], lm2m=z["lm2m"], l_max=int(z["l_max"]))
+    prof = {k: z[k] for k in ("or1", "or2", "beta", "dLtemp0", "dLkappa", "kappa")}
+    mats = (z["rMat"], z["drMat"], z["d2rMat"], float(z["rnorm"]), float(z["boundary_fac"]))
+    st = dict(old=z["s_old"].copy(), impl=z["s_impl"].copy(), expl0=z["s_expl0"].copy(),
+              expl1=z["s_expl1"].copy())
+    return z, g, prof, mats, st
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_update_s_oracle(name):
+    """The implicit entropy update restated in numpy (per-l LU solves) against the
+    reference's updateS (Chebyshev with the DCT-I; FD4 anelastic, where the reference
+    uses a pivoted banded LU)."""
+    from oracle import implicit as oi
+
+    z, g, prof, mats, st = _s_case(name)
+    w = (z["wimp"], z["wimp_lin"], z["wexp"])
+    o = oi.update_s(g, mats, prof, st, w, float(z["opr"]), z["hdif_S"], z["tops"], z["bots"],
+                    z["D1"], z["D2"], bool(z["chebyshev"]), int(z["n_cheb_max"]))
+    assert rel_err(o["s"], z["s_new"]) < 1e-14
+    assert rel_err(o["ds"], z["ds_new"]) < 1e-14
+    assert rel_err(o["impl"], z["s_impl_new"]) < 1e-14
+    assert rel_err(o["old"], z["s_old_new"]) < 1e-14
+    assert rel_err(o["expl1"], z["s_expl1_new"]) == 0.0
+    ref_w = oi.cnab2_weights(1e-4, 1.3e-4)
+    assert np.allclose(ref_w[1], z["wimp_lin"], rtol=1e-15) and np.allclose(ref_w[2], z["wexp"],
+                                                                            rtol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_scalar_solve_operators(name):
+    """The library's host builder of the per-degree solve operators (inverse of the
+    preconditioned LHS, DCT-I folded in for Chebyshev), applied in numpy, reproduces
+    the reference's new field."""
+    from types import SimpleNamespace
+
+    from magic_b200 import implicit as I
+
+    z = load_golden(name)
+    sch = SimpleNamespace(n_r=int(z["n_r_max"]), chebyshev=bool(z["chebyshev"]),
+                          n_cheb=int(z["n_cheb_max"]), rMat=z["rMat"], drMat=z["drMat"],
+                          d2rMat=z["d2rMat"], rnorm=float(z["rnorm"]),
+                          boundary_fac=float(z["boundary_fac"]))
+    d1c = z["beta"] + z["dLtemp0"] + 2 * z["or1"] + z["dLkappa"]
+    w = I.cnab2_weights(1e-4, 1.3e-4)
+    M = I.scalar_solve_operators(sch, int(z["l_max"]), w[1], float(z["opr"]), z["hdif_S"],
+                                 z["kappa"], d1c, z["or2"])
+    rhs = w[0] * z["s_old"] + w[2] * z["s_impl"] + w[3] * z["s_expl0"] + w[4] * z["s_expl1"]
+    rhs[:, 0] = z["tops"]
+    rhs[:, -1] = z["bots"]
+    x = np.stack([M[l] @ rhs[i] for i, l in enumerate(z["lm2l"])])
+    x[z["lm2m"] == 0] = x[z["lm2m"] == 0].real
+    assert rel_err(x, z["s_new"]) < 1e-13
