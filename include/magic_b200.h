@@ -309,36 +309,42 @@ typedef struct {
 MT_API int mt_get_td(const mt_plan* plan, int n_r, const mt_td_in* in, const mt_td_out* out,
                      const mt_td_params* p, const mt_radial_op* D1, void* stream);
 
-/* ---- implicit update of a scalar field ----------------------------------
- * One CNAB2 step of the entropy equation (magic_torch/update_s.py:213-271
- * updateS; composition, update_xi.py updateXi, has the same form):
+/* ---- implicit update of a field with a per-degree solve ------------------
+ * One CNAB2 step of an equation whose implicit operator is a radial
+ * operator per degree l: entropy (magic_torch/update_s.py:213-271 updateS),
+ * composition (update_xi.py updateXi), toroidal velocity (update_z.py:333-505
+ * updateZ without inner-core rotation or angular-momentum correction):
  *   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1
  *         (time_scheme.py:82-96), rows 0 and n_r-1 = top / bot values;
- *   s = M_l rhs per degree l (m = 0 coefficients real), old <- s,
- *   expl1 <- expl0 (time_scheme.py:130-143), ds = D1 s,
- *   impl <- opr hdif_l kappa (D2 s + d1c ds - l(l+1) or2 s).
+ *   x = M_l rhs per degree l (m = 0 coefficients real), dx = D1 x,
+ *   expl1 <- expl0 (time_scheme.py:130-143),
+ *   old  <- so_l[l] so_r[r] x,
+ *   impl <- ia_l[l] ia_r[r] (D2 x + ib_r[r] dx - (ic_r[r] + ic_l[l] ic_r2[r]) x).
+ * Entropy: so = 1, ia = opr hdif_l kappa, ib = beta + dLtemp0 + 2/r + dLkappa,
+ * ic_r = 0, ic_l ic_r2 = l(l+1)/r^2; toroidal velocity: so = l(l+1)/r^2,
+ * ia = hdif_l l(l+1)/r^2 visc, ib = dLvisc - beta, ic_r = the l-independent
+ * part, ic_l ic_r2 = l(l+1)/r^2 (magic_b200.implicit builds both).
  * M_l: the per-degree solve operators (mt_lop: one dense n_r x n_r matrix per
- * l = 0..l_max, HOST pointer, row-major; the inverse of the LHS of
- * update_s.py:67-134, with the DCT-I to grid values folded in for the
- * Chebyshev scheme; magic_b200.implicit builds them).  All (lm_max, n_r)
- * complex arrays share the row stride ld; top/bot are (lm_max) complex or
- * NULL (zero); hdif (l_max+1), kappa, d1c = beta + dLtemp0 + 2/r + dLkappa,
- * or2 (n_r) are device arrays. */
+ * l = 0..l_max, HOST pointer, row-major; the inverse of the reference's LHS,
+ * with the DCT-I to grid values folded in for the Chebyshev scheme).  All
+ * (lm_max, n_r) complex arrays share the row stride ld; top/bot are
+ * (lm_max) complex or NULL (zero); the coefficient arrays are device arrays,
+ * *_l of l_max+1 and *_r of n_r values; so_l/so_r NULL mean 1, ic_r NULL 0. */
 typedef struct mt_lop mt_lop;
 MT_API int mt_lop_create(int n_l, int n_r, const double* M_host, mt_lop** op);
 MT_API int mt_lop_destroy(mt_lop* op);
 
 typedef struct {
-  double *s, *ds, *old, *impl, *expl0, *expl1;
+  double *x, *dx, *old, *impl, *expl0, *expl1;
   const double *top, *bot;
   int64_t ld;
-  double w_old, w_impl, w_expl0, w_expl1, opr;
-  const double *hdif, *kappa, *d1c, *or2;
-} mt_scalar_update;
+  double w_old, w_impl, w_expl0, w_expl1;
+  const double *so_l, *so_r, *ia_l, *ia_r, *ib_r, *ic_r, *ic_l, *ic_r2;
+} mt_field_update;
 
-MT_API int mt_update_scalar(const mt_plan* plan, int n_r, const mt_scalar_update* u,
-                            const mt_lop* solve, const mt_radial_op* D1,
-                            const mt_radial_op* D2, void* stream);
+MT_API int mt_update_field(const mt_plan* plan, int n_r, const mt_field_update* u,
+                           const mt_lop* solve, const mt_radial_op* D1,
+                           const mt_radial_op* D2, void* stream);
 
 MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
 

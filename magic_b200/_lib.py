@@ -92,11 +92,12 @@ class TdParams(C.Structure):
                [(n, C.c_int) for n in ("l_double_curl", "l_heat", "l_mag", "l_chem", "l_anel")]
 
 
-class ScalarUpdate(C.Structure):
-    _fields_ = [(n, _dp) for n in ("s", "ds", "old", "impl", "expl0", "expl1", "top", "bot")] + \
+class FieldUpdate(C.Structure):
+    _fields_ = [(n, _dp) for n in ("x", "dx", "old", "impl", "expl0", "expl1", "top", "bot")] + \
                [("ld", _i64)] + \
-               [(n, C.c_double) for n in ("w_old", "w_impl", "w_expl0", "w_expl1", "opr")] + \
-               [(n, _dp) for n in ("hdif", "kappa", "d1c", "or2")]
+               [(n, C.c_double) for n in ("w_old", "w_impl", "w_expl0", "w_expl1")] + \
+               [(n, _dp) for n in ("so_l", "so_r", "ia_l", "ia_r", "ib_r", "ic_r", "ic_l",
+                                   "ic_r2")]
 
 
 # name -> (restype, argtypes)
@@ -139,8 +140,8 @@ _PROTOS = {
                             C.POINTER(TdParams), C.c_void_p, _dp]),
     "mt_lop_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
     "mt_lop_destroy": (C.c_int, [C.c_void_p]),
-    "mt_update_scalar": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ScalarUpdate), C.c_void_p,
-                                   C.c_void_p, C.c_void_p, _dp]),
+    "mt_update_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FieldUpdate), C.c_void_p,
+                                  C.c_void_p, C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }

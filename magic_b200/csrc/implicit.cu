@@ -1,8 +1,11 @@
-// Implicit (IMEX) update of a scalar field: entropy or composition (FP64).
+// Implicit (IMEX) update of a field whose implicit operator is a radial
+// operator per degree l (FP64): entropy, composition, toroidal velocity.
 //
 // Replaces magic_torch/update_s.py:213-271 (updateS; updateXi,
-// update_xi.py:208-262, has the same form) with the CNAB2 right-hand side of
-// time_scheme.py:82-96 and the history rotation of time_scheme.py:130-143.
+// update_xi.py:208-262, has the same form) and update_z.py:333-505 (updateZ
+// without inner-core rotation or angular-momentum correction) with the CNAB2
+// right-hand side of time_scheme.py:82-96 and the history rotation of
+// time_scheme.py:130-143.
 //
 // The per-degree solve is an operator set (mt_lop): one dense n_r x n_r
 // matrix per l, built on the host as the inverse of the reference's
@@ -11,12 +14,11 @@
 // (M_l = C T A_l^-1).  Matrices are stored transposed, MT[l][k][j], so the 32
 // lanes of a warp (32 consecutive output levels j) read consecutive values.
 //
-// k_update_scalar: CTA = (degree l, chunk of orders m), one warp per lm row:
+// k_update_field: CTA = (degree l, chunk of orders m), one warp per lm row:
 //   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1, rows 0 and
 //   n_r - 1 replaced by the boundary values; expl1 <- expl0 (rotation);
-//   s = M_l rhs, imaginary part dropped for m = 0; old <- s;
-//   ds = D1 s, d2s = D2 s;
-//   impl <- opr hdif_l kappa (d2s + d1c ds - l(l+1) or2 s).
+//   x = M_l rhs, imaginary part dropped for m = 0; dx = D1 x, d2x = D2 x;
+//   old <- so_l so_r x; impl <- ia_l ia_r (d2x + ib_r dx - (ic_r + ic_l ic_r2) x).
 // Rows of one l share M_l through L1 (the CTA's warps and co-resident CTAs).
 #include <algorithm>
 #include <cmath>
@@ -39,16 +41,16 @@ constexpr int kUsWarps = 8;
 struct UsArgs {
   int n_r, l_max, minc, n_m;
   const int* lstart;
-  double2 *s, *ds, *old, *impl, *expl0, *expl1;
+  double2 *x, *dx, *old, *impl, *expl0, *expl1;
   const double2 *top, *bot;
   int64_t ld;
-  double w_old, w_impl, w_expl0, w_expl1, opr;
-  const double *hdif, *kappa, *d1c, *or2;
+  double w_old, w_impl, w_expl0, w_expl1;
+  const double *so_l, *so_r, *ia_l, *ia_r, *ib_r, *ic_r, *ic_l, *ic_r2;
   const double* mt;
   OpView D1, D2;
 };
 
-__global__ void __launch_bounds__(32 * kUsWarps) k_update_scalar(UsArgs a) {
+__global__ void __launch_bounds__(32 * kUsWarps) k_update_field(UsArgs a) {
   extern __shared__ double2 usbuf[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int n_r = a.n_r, l = blockIdx.x;
@@ -81,17 +83,18 @@ __global__ void __launch_bounds__(32 * kUsWarps) k_update_scalar(UsArgs a) {
     }
     if (m == 0) acc.y = 0.0;
     x[j] = acc;
-    a.s[row + j] = acc;
-    a.old[row + j] = acc;
+    a.x[row + j] = acc;
   }
   __syncwarp();
-  const double dL = (double)l * (l + 1.0), ch = a.opr * a.hdif[l];
+  const double so_l = a.so_l ? a.so_l[l] : 1.0, ia_l = a.ia_l[l], ic_l = a.ic_l[l];
   for (int j = lane; j < n_r; j += 32) {
-    const double2 d1 = op_row(a.D1, x, j), d2 = op_row(a.D2, x, j);
-    a.ds[row + j] = d1;
-    const double c1 = a.d1c[j], c0 = dL * a.or2[j], kap = ch * a.kappa[j];
-    a.impl[row + j] = double2{kap * (d2.x + c1 * d1.x - c0 * x[j].x),
-                              kap * (d2.y + c1 * d1.y - c0 * x[j].y)};
+    const double2 d1 = op_row(a.D1, x, j), d2 = op_row(a.D2, x, j), v = x[j];
+    a.dx[row + j] = d1;
+    const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
+    a.old[row + j] = double2{so * v.x, so * v.y};
+    const double c1 = a.ib_r[j], c0 = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
+    const double ia = ia_l * a.ia_r[j];
+    a.impl[row + j] = double2{ia * (d2.x + c1 * d1.x - c0 * v.x), ia * (d2.y + c1 * d1.y - c0 * v.y)};
   }
 }
 
@@ -148,8 +151,8 @@ int mt_lop_destroy(mt_lop* op) {
   return MT_OK;
 }
 
-int mt_update_scalar(const mt_plan* p, int n_r, const mt_scalar_update* u, const mt_lop* solve,
-                     const mt_radial_op* D1, const mt_radial_op* D2, void* stream) {
+int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const mt_lop* solve,
+                    const mt_radial_op* D1, const mt_radial_op* D2, void* stream) {
   MT_REQUIRE(p && u, MT_ERR_ARG, "null argument");
   int dev = -1;
   MT_CHECK_CUDA(cudaGetDevice(&dev));
@@ -161,9 +164,10 @@ int mt_update_scalar(const mt_plan* p, int n_r, const mt_scalar_update* u, const
              MT_ERR_ARG, "operator sizes differ from n_r");
   MT_REQUIRE(solve->n_l == p->l_max + 1, MT_ERR_ARG, "solve operators must cover l = 0..l_max");
   MT_REQUIRE(n_r >= 3 && u->ld >= n_r, MT_ERR_ARG, "bad radial size or stride");
-  MT_REQUIRE(u->s && u->ds && u->old && u->impl && u->expl0 && u->expl1, MT_ERR_ARG,
+  MT_REQUIRE(u->x && u->dx && u->old && u->impl && u->expl0 && u->expl1, MT_ERR_ARG,
              "null field or time array");
-  MT_REQUIRE(u->hdif && u->kappa && u->d1c && u->or2, MT_ERR_ARG, "null coefficient array");
+  MT_REQUIRE(u->ia_l && u->ia_r && u->ib_r && u->ic_l && u->ic_r2, MT_ERR_ARG,
+             "null coefficient array");
   UsArgs a{};
   a.n_r = n_r;
   a.l_max = p->l_max;
@@ -171,22 +175,22 @@ int mt_update_scalar(const mt_plan* p, int n_r, const mt_scalar_update* u, const
   a.n_m = p->n_m;
   a.lstart = p->d_lstart;
   auto d = [](double* x) { return (double2*)x; };
-  a.s = d(u->s); a.ds = d(u->ds); a.old = d(u->old); a.impl = d(u->impl);
+  a.x = d(u->x); a.dx = d(u->dx); a.old = d(u->old); a.impl = d(u->impl);
   a.expl0 = d(u->expl0); a.expl1 = d(u->expl1);
   a.top = (const double2*)u->top;
   a.bot = (const double2*)u->bot;
   a.ld = u->ld;
   a.w_old = u->w_old; a.w_impl = u->w_impl; a.w_expl0 = u->w_expl0; a.w_expl1 = u->w_expl1;
-  a.opr = u->opr;
-  a.hdif = u->hdif; a.kappa = u->kappa; a.d1c = u->d1c; a.or2 = u->or2;
+  a.so_l = u->so_l; a.so_r = u->so_r; a.ia_l = u->ia_l; a.ia_r = u->ia_r; a.ib_r = u->ib_r;
+  a.ic_r = u->ic_r; a.ic_l = u->ic_l; a.ic_r2 = u->ic_r2;
   a.mt = solve->mt;
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   const size_t sm = (size_t)kUsWarps * 2 * n_r * sizeof(double2);
-  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_scalar,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_field, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
   const dim3 grid(p->l_max + 1, (p->n_m + kUsWarps - 1) / kUsWarps);
-  k_update_scalar<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
+  k_update_field<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

@@ -37,34 +37,100 @@ def _dct1(n):
     return Cm / np.sqrt(2.0 * N)
 
 
-def scalar_solve_operators(sch, l_max, wimp_lin0, opr, hdif, kappa, d1c, or2):
-    """(l_max+1, n_r, n_r) solve operators M_l of the scalar-field LHS
-    (magic_torch/update_s.py:67-134):
-        A_l = rnorm (rMat - wimp_lin0 opr hdif_l kappa (d2rMat + d1c drMat
-              - l(l+1) or2 rMat)),
-    Dirichlet rows 0 and n_r-1 (rnorm rMat, Chebyshev columns >= n_cheb dropped),
-    columns 0 and n_r-1 scaled by boundary_fac; M_l = A_l^-1 through the same row
-    scaling (1 / row max) the reference factorises with.  For the Chebyshev scheme
-    the truncation to n_cheb modes and the DCT-I to grid values are folded in."""
+def _inverse_ops(A, sch, zero_l0=False, identity_l0=False):
+    """M_l = A_l^-1 through the reference's row scaling (1 / row max), the
+    Chebyshev truncation and the DCT-I to grid values folded in; degree 0 zero or
+    the identity where the reference's solve does that."""
     N = sch.n_r
-    ls = np.arange(l_max + 1, dtype=np.float64)
-    dL = (ls * (ls + 1.0))[:, None, None]
-    op = sch.d2rMat[None] + d1c[None, :, None] * sch.drMat[None] - dL * or2[None, :, None] * sch.rMat[None]
-    A = sch.rnorm * (sch.rMat[None] - wimp_lin0 * opr * np.asarray(hdif)[:, None, None]
-                     * kappa[None, :, None] * op)
-    A[:, 0, :] = sch.rnorm * sch.rMat[0, :]
-    A[:, N - 1, :] = sch.rnorm * sch.rMat[N - 1, :]
+    if zero_l0 or identity_l0:
+        A = A.copy()
+        A[0] = np.eye(N)
+    fac = 1.0 / np.abs(A).max(axis=2)
+    M = np.linalg.inv(fac[:, :, None] * A) * fac[:, None, :]
+    if zero_l0:
+        M[0] = 0.0
+    if sch.chebyshev:
+        M[:, sch.n_cheb:, :] = 0.0
+        M = np.einsum("jk,lkn->ljn", _dct1(N), M)
+    return M
+
+
+def _bc_rows(A, sch, rows):
+    """Boundary rows (row index -> matrix row), the Chebyshev columns >= n_cheb
+    dropped in them, then columns 0 and n_r-1 scaled by boundary_fac."""
+    N = sch.n_r
+    for i, v in rows.items():
+        A[:, i, :] = v
     if sch.n_cheb < N:
         A[:, 0, sch.n_cheb:] = 0.0
         A[:, N - 1, sch.n_cheb:] = 0.0
     A[:, :, 0] *= sch.boundary_fac
     A[:, :, N - 1] *= sch.boundary_fac
-    fac = 1.0 / np.abs(A).max(axis=2)
-    M = np.linalg.inv(fac[:, :, None] * A) * fac[:, None, :]
-    if sch.chebyshev:
-        M[:, sch.n_cheb:, :] = 0.0
-        M = np.einsum("jk,lkn->ljn", _dct1(N), M)
-    return M
+    return A
+
+
+def scalar_solve_operators(sch, l_max, wimp_lin0, opr, hdif, kappa, d1c, or2):
+    """(l_max+1, n_r, n_r) solve operators M_l of the entropy / composition LHS
+    (magic_torch/update_s.py:67-134):
+        A_l = rnorm (rMat - wimp_lin0 opr hdif_l kappa (d2rMat + d1c drMat
+              - l(l+1) or2 rMat)),
+    Dirichlet rows 0 and n_r-1 (rnorm rMat)."""
+    ls = np.arange(l_max + 1, dtype=np.float64)
+    dL = (ls * (ls + 1.0))[:, None, None]
+    op = sch.d2rMat[None] + d1c[None, :, None] * sch.drMat[None] - dL * or2[None, :, None] * sch.rMat[None]
+    A = sch.rnorm * (sch.rMat[None] - wimp_lin0 * opr * np.asarray(hdif)[:, None, None]
+                     * kappa[None, :, None] * op)
+    N = sch.n_r
+    A = _bc_rows(A, sch, {0: sch.rnorm * sch.rMat[0], N - 1: sch.rnorm * sch.rMat[N - 1]})
+    return _inverse_ops(A, sch)
+
+
+def toroidal_solve_operators(sch, l_max, wimp_lin0, hdif, visc, beta, dbeta, dLvisc, or1, or2,
+                             ktopv=2, kbotv=2):
+    """(l_max+1, n_r, n_r) solve operators of the toroidal-velocity LHS
+    (magic_torch/update_z.py:89-240):
+        A_l = rnorm l(l+1) or2 (rMat - wimp_lin0 hdif_l visc (d2rMat + (dLvisc - beta) drMat
+              - (dLvisc beta + 2 dLvisc or1 + l(l+1) or2 + dbeta + 2 beta or1) rMat)),
+    boundary rows stress-free (k = 1: rnorm (drMat - (2 or1 + beta) rMat)) or no-slip
+    (rnorm rMat).  Degree 0: zero, except the identity of the banded finite-difference
+    solve (fd_order > 2)."""
+    N = sch.n_r
+    ls = np.arange(l_max + 1, dtype=np.float64)
+    dL = (ls * (ls + 1.0))[:, None, None]
+    c0 = (dLvisc * beta + 2.0 * dLvisc * or1)[None, :, None] + dL * or2[None, :, None] \
+        + (dbeta + 2.0 * beta * or1)[None, :, None]
+    op = sch.d2rMat[None] + (dLvisc - beta)[None, :, None] * sch.drMat[None] - c0 * sch.rMat[None]
+    A = sch.rnorm * dL * or2[None, :, None] * (
+        sch.rMat[None] - wimp_lin0 * np.asarray(hdif)[:, None, None] * visc[None, :, None] * op)
+    rows = {}
+    for i, k in ((0, ktopv), (N - 1, kbotv)):
+        rows[i] = (sch.rnorm * (sch.drMat[i] - (2.0 * or1[i] + beta[i]) * sch.rMat[i]) if k == 1
+                   else sch.rnorm * sch.rMat[i])
+    A = _bc_rows(A, sch, rows)
+    banded_l0 = (not sch.chebyshev) and getattr(sch, "fd_order", 2) > 2
+    return _inverse_ops(A, sch, zero_l0=not banded_l0, identity_l0=banded_l0)
+
+
+def entropy_coefficients(l_max, opr, hdif, kappa, d1c, or2):
+    """Coefficients of mt_update_field for entropy / composition
+    (magic_torch/update_s.py:262-270): old = s, impl = opr hdif kappa
+    (d2s + d1c ds - l(l+1) or2 s)."""
+    ls = np.arange(l_max + 1, dtype=np.float64)
+    return dict(so_l=None, so_r=None, ia_l=opr * np.asarray(hdif, dtype=np.float64), ia_r=kappa,
+                ib_r=d1c, ic_r=None, ic_l=ls * (ls + 1.0), ic_r2=or2)
+
+
+def toroidal_coefficients(l_max, hdif, visc, beta, dbeta, dLvisc, or1, or2):
+    """Coefficients of mt_update_field for the toroidal velocity
+    (magic_torch/update_z.py:37-47, 481-495): old = l(l+1) or2 z, impl = hdif l(l+1)
+    or2 visc (d2z + (dLvisc - beta) dz - (dLvisc beta + 2 dLvisc or1 + dbeta
+    + 2 beta or1 + l(l+1) or2) z)."""
+    ls = np.arange(l_max + 1, dtype=np.float64)
+    dLh = ls * (ls + 1.0)
+    return dict(so_l=dLh, so_r=or2, ia_l=np.asarray(hdif, dtype=np.float64) * dLh,
+                ia_r=or2 * visc, ib_r=dLvisc - beta,
+                ic_r=dLvisc * beta + 2.0 * dLvisc * or1 + dbeta + 2.0 * beta * or1,
+                ic_l=dLh, ic_r2=or2)
 
 
 class LOp:
@@ -93,26 +159,32 @@ class LOp:
             self._h = None
 
 
-def update_scalar(plan, sch, lop, s, ds, ta, weights, opr, hdif, kappa, d1c, or2, top=None,
-                  bot=None):
-    """One implicit step of a scalar field in place (magic_torch/update_s.py:213-271).
-
-    s, ds: (lm_max, n_r) complex128 outputs; ta: dict old, impl, expl0, expl1 of the
-    same shape (updated in place); weights: cnab2_weights(...); hdif (l_max+1),
-    kappa, d1c = beta + dLtemp0 + 2/r + dLkappa, or2 (n_r) real tensors on the device;
-    top / bot: (lm_max) complex boundary values or None (zero)."""
-    n_r = s.shape[1]
-    arrs = [s, ds, ta["old"], ta["impl"], ta["expl0"], ta["expl1"]]
-    for x in arrs:
-        if x.shape != s.shape or x.dtype != torch.complex128 or not x.is_contiguous():
+def update_field(plan, sch, lop, x, dx, ta, weights, coef, top=None, bot=None):
+    """One implicit step of a field in place (mt_update_field): x, dx (lm_max, n_r)
+    complex128 outputs; ta: dict old, impl, expl0, expl1 of the same shape (updated in
+    place); weights: cnab2_weights(...); coef: entropy_coefficients(...) or
+    toroidal_coefficients(...); top / bot: (lm_max) complex boundary values or None."""
+    n_r = x.shape[1]
+    arrs = [x, dx, ta["old"], ta["impl"], ta["expl0"], ta["expl1"]]
+    for a in arrs:
+        if a.shape != x.shape or a.dtype != torch.complex128 or not a.is_contiguous():
             raise ValueError("fields and time arrays must be contiguous (lm_max, n_r) complex128")
     w_old, _, w_impl, w_e0, w_e1 = weights
-    prof = [torch.as_tensor(v, dtype=torch.float64, device=s.device).contiguous()
-            for v in (hdif, kappa, d1c, or2)]
-    u = _lib.ScalarUpdate(*[x.data_ptr() for x in arrs],
-                          top.data_ptr() if top is not None else None,
-                          bot.data_ptr() if bot is not None else None, n_r,
-                          w_old, w_impl, w_e0, w_e1, float(opr), *[p.data_ptr() for p in prof])
-    st = C.c_void_p(torch.cuda.current_stream(s.device).cuda_stream)
-    check(_lib.lib().mt_update_scalar(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h,
-                                      st))
+    names = ("so_l", "so_r", "ia_l", "ia_r", "ib_r", "ic_r", "ic_l", "ic_r2")
+    dev = {k: (torch.as_tensor(coef[k], dtype=torch.float64, device=x.device).contiguous()
+               if coef.get(k) is not None else None) for k in names}
+    u = _lib.FieldUpdate(*[a.data_ptr() for a in arrs],
+                         top.data_ptr() if top is not None else None,
+                         bot.data_ptr() if bot is not None else None, n_r,
+                         w_old, w_impl, w_e0, w_e1,
+                         *[dev[k].data_ptr() if dev[k] is not None else None for k in names])
+    st = C.c_void_p(torch.cuda.current_stream(x.device).cuda_stream)
+    check(_lib.lib().mt_update_field(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h, st))
+
+
+def update_scalar(plan, sch, lop, s, ds, ta, weights, opr, hdif, kappa, d1c, or2, top=None,
+                  bot=None):
+    """One implicit entropy (or composition) step in place (magic_torch/update_s.py:213-271)."""
+    update_field(plan, sch, lop, s, ds, ta, weights,
+                 entropy_coefficients(plan.l_max, opr, hdif, np.asarray(kappa),
+                                      np.asarray(d1c), np.asarray(or2)), top=top, bot=bot)

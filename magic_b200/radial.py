@@ -292,6 +292,7 @@ class RadialScheme:
                  fd_order_bound=2, fd_stretch=0.3, fd_ratio=0.1, device=None):
         self.n_r = n_r
         self.chebyshev = scheme.upper() != "FD"
+        self.fd_order = fd_order
         self.n_cheb = n_r if (n_cheb is None or not self.chebyshev) else min(n_cheb, n_r)
         if not self.chebyshev:
             self.r = fd_grid(n_r, radratio, fd_stretch, fd_ratio)

@@ -70,3 +70,69 @@ def update_s(g, mats, prof, st, weights, opr, hdif, tops, bots, D1, D2, chebyshe
     impl = opr * hdif[g["lm2l"]][:, None] * prof["kappa"][None, :] * (
         d2s + d1c[None, :] * ds - dLh * prof["or2"][None, :] * x)
     return dict(s=x, ds=ds, impl=impl, old=x.copy(), expl1=st["expl0"].copy())
+
+
+def z_matrix(l, mats, prof, wimp_lin0, hdif_l, n_cheb, ktopv, kbotv):
+    """Toroidal-velocity LHS of degree l >= 1 (magic_torch/update_z.py:156-188):
+    rnorm l(l+1)/r^2 (rMat - wimp hdif visc (d2rMat + (dLvisc - beta) drMat
+    - (dLvisc beta + 2 dLvisc/r + l(l+1)/r^2 + dbeta + 2 beta/r) rMat)); boundary rows
+    stress-free (k = 1: rnorm (drMat - (2/r + beta) rMat)) or no-slip (rnorm rMat)."""
+    rMat, drMat, d2rMat, rnorm, bfac = mats
+    N = rMat.shape[0]
+    p = prof
+    dL = float(l * (l + 1))
+    c0 = (p["dLvisc"] * p["beta"] + 2.0 * p["dLvisc"] * p["or1"] + dL * p["or2"] + p["dbeta"]
+          + 2.0 * p["beta"] * p["or1"])[:, None]
+    dat = rnorm * dL * p["or2"][:, None] * (rMat - wimp_lin0 * hdif_l * p["visc"][:, None] * (
+        d2rMat + (p["dLvisc"] - p["beta"])[:, None] * drMat - c0 * rMat))
+    for row, k in ((0, ktopv), (N - 1, kbotv)):
+        if k == 1:
+            dat[row, :] = rnorm * (drMat[row, :] - (2.0 * p["or1"][row] + p["beta"][row]) * rMat[row, :])
+        else:
+            dat[row, :] = rnorm * rMat[row, :]
+    if n_cheb < N:
+        dat[0, n_cheb:] = 0.0
+        dat[N - 1, n_cheb:] = 0.0
+    dat[:, 0] *= bfac
+    dat[:, N - 1] *= bfac
+    return dat
+
+
+def update_z(g, mats, prof, st, weights, hdif, D1, D2, chebyshev, n_cheb, ktopv, kbotv, fd_order):
+    """One updateZ without inner-core rotation (magic_torch/update_z.py:333-505):
+    CNAB2 right-hand side with zero boundary rows, per-l solves (l = 0: zero on the
+    dense paths, the right-hand side itself on the banded finite-difference path,
+    fd_order > 2), m = 0 real, DCT-I (Chebyshev), dz, d2z; old = l(l+1)/r^2 z and
+    impl = hdif l(l+1)/r^2 visc (d2z + (dLvisc - beta) dz
+    - (dLvisc beta + 2 dLvisc/r + dbeta + 2 beta/r + l(l+1)/r^2) z)."""
+    wimp, wimp_lin, wexp = weights
+    N = st["old"].shape[1]
+    rhs = wimp[0] * st["old"] + wimp_lin[1] * st["impl"] + wexp[0] * st["expl0"] \
+        + wexp[1] * st["expl1"]
+    rhs[:, 0] = 0.0
+    rhs[:, N - 1] = 0.0
+    x = np.zeros_like(rhs)
+    for l in range(g["l_max"] + 1):
+        rows = np.nonzero(g["lm2l"] == l)[0]
+        if l == 0:
+            if not chebyshev and fd_order > 2:
+                x[rows] = rhs[rows]
+            continue
+        dat = z_matrix(l, mats, prof, wimp_lin[0], hdif[l], n_cheb, ktopv, kbotv)
+        fac = 1.0 / np.abs(dat).max(axis=1)
+        x[rows] = np.linalg.solve(fac[:, None] * dat, (fac[None, :] * rhs[rows]).T).T
+    m0 = g["lm2m"] == 0
+    x[m0] = x[m0].real
+    if chebyshev:
+        if n_cheb < N:
+            x[:, n_cheb:] = 0.0
+        x = x @ dct1_matrix(N).T
+    dz, d2z = x @ D1.T, x @ D2.T
+    p = prof
+    dLh = (g["lm2l"] * (g["lm2l"] + 1.0))[:, None]
+    z0 = (p["dLvisc"] * p["beta"] + 2.0 * p["dLvisc"] * p["or1"] + p["dbeta"]
+          + 2.0 * p["beta"] * p["or1"])[None, :]
+    or2 = p["or2"][None, :]
+    impl = hdif[g["lm2l"]][:, None] * dLh * or2 * p["visc"][None, :] * (
+        d2z + (p["dLvisc"] - p["beta"])[None, :] * dz - (z0 + dLh * or2) * x)
+    return dict(x=x, dx=dz, impl=impl, old=dLh * or2 * x, expl1=st["expl0"].copy())

@@ -176,7 +176,7 @@ def worker_nl(name, ref):
 
 TD_CONFIGS = {
     # spectral explicit terms (get_td + finish_exp), radial derivatives, DCT-I
-    "td_cheb": {"l_max": 8, "minc": 1, "n_r_max": 9, "mode": 0},
+    "td_cheb": {"l_max": 8, "minc": 1, "n_r_max": 9, "mode": 0, "ktopv": 1, "kbotv": 1},
     "td_fd_anel": {"l_max": 16, "minc": 2, "n_r_max": 12, "radial_scheme": "FD",
                    "fd_order": 4, "fd_order_bound": 2, "strat": 5.0, "polind": 2.0,
                    "g0": 0.0, "g1": 0.0, "g2": 1.0, "mode": 0, "ek": 1e-4, "ra": 3e6},
@@ -263,6 +263,22 @@ def worker_td(name, ref):
     us.updateS(s_new, ds_new, ta, tscheme)
     out.update(s_new=n(s_new), ds_new=n(ds_new), s_impl_new=n(ta.impl[:, :, 0]),
                s_old_new=n(ta.old[:, :, 0]), s_expl1_new=n(ta.expl[:, :, 1]))
+    # one implicit toroidal-velocity update (magic_torch/update_z.py:89-505)
+    from magic_torch import update_z as uz
+    uz.build_z_matrices(tscheme.wimp_lin[0].item())
+    tz = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+    for k, arr in (("old", tz.old), ("impl", tz.impl), ("expl0", tz.expl), ("expl1", tz.expl)):
+        v = _spec(rng, lm, l_of, N)
+        arr[:, :, 1 if k == "expl1" else 0] = t(v)
+        out["z_" + k] = v
+    out.update(visc=n(rf2.visc), dLvisc=n(rf2.dLvisc), dbeta=n(rf2.dbeta),
+               hdif_V=n(hd.hdif_V), ktopv=int(params.ktopv), kbotv=int(params.kbotv),
+               fd_order=int(getattr(params, "fd_order", 2)))
+    z_new = torch.zeros(lm, N, dtype=torch.complex128)
+    dz_new = torch.zeros_like(z_new)
+    uz.updateZ(z_new, dz_new, tz, tscheme)
+    out.update(z_new=n(z_new), dz_new=n(dz_new), z_impl_new=n(tz.impl[:, :, 0]),
+               z_old_new=n(tz.old[:, :, 0]), z_expl1_new=n(tz.expl[:, :, 1]))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

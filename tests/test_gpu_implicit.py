@@ -1,12 +1,16 @@
-"""Implicit update of a scalar field (CNAB2 right-hand side, per-degree solve,
-radial derivatives, next implicit term, history rotation) on the GPU in FP64:
-against the reference's own updateS outputs (tests/golden/td_*.npz) and
-against the numpy oracle for two consecutive steps at l_max = 127 / 65
-Chebyshev levels and l_max = 255 / 97 fourth-order finite-difference levels.
+"""Implicit field updates (CNAB2 right-hand side, per-degree solve, radial
+derivatives, next implicit term, history rotation) on the GPU in FP64, for the
+entropy and the toroidal velocity: against the reference's own updateS and
+updateZ outputs (tests/golden/td_*.npz) and against the numpy oracle for two
+consecutive steps at l_max = 127 / 65 Chebyshev levels and l_max = 255 / 97
+fourth-order finite-difference levels.
 
 Tolerance 1e-12 relative to each array's largest value: the GPU applies the
 inverse of each degree's matrix (with the DCT-I folded in for Chebyshev)
-where the reference and the oracle factorise and solve.
+where the reference and the oracle factorise and solve.  The implicit term is
+a second radial derivative of the new field: at 65 Chebyshev levels
+||D2||_inf ~ 1e7 amplifies those rounding-level differences, so it is held
+to 1e-11 (measured 1.9e-12).
 """
 
 import numpy as np
@@ -19,6 +23,7 @@ from oracle import implicit as oi
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
+TOL_IMPL = 1e-11
 cu = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()
 npy = lambda t: t.cpu().numpy()
 
@@ -97,7 +102,78 @@ def test_update_scalar_two_steps_vs_oracle(scheme, l_max, n_r):
         for k, got in (("s", s), ("ds", ds), ("impl", ta["impl"]), ("old", ta["old"]),
                        ("expl1", ta["expl1"])):
             e = rel_err(npy(got), ref[k])
-            assert e < TOL, (scheme, step, k, e)
+            assert e < (TOL_IMPL if k == "impl" else TOL), (scheme, step, k, e)
         # next step: the explicit stage would write a new expl0
         st = dict(old=ref["old"], impl=ref["impl"], expl0=spec(), expl1=ref["expl1"])
         ta["expl0"] = cu(st["expl0"])
+
+
+def _sch_from(z):
+    from types import SimpleNamespace
+
+    from magic_b200.radial import RadialOp
+
+    return SimpleNamespace(n_r=int(z["n_r_max"]), chebyshev=bool(z["chebyshev"]),
+                           n_cheb=int(z["n_cheb_max"]), rMat=z["rMat"], drMat=z["drMat"],
+                           d2rMat=z["d2rMat"], rnorm=float(z["rnorm"]),
+                           boundary_fac=float(z["boundary_fac"]), fd_order=int(z["fd_order"]),
+                           D1=RadialOp(z["D1"]), D2=RadialOp(z["D2"]))
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_update_toroidal_matches_reference(name):
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+
+    z = load_golden(name)
+    p = Plan(int(z["l_max"]), int(z["minc"]))
+    sch = _sch_from(z)
+    w = I.cnab2_weights(1e-4, 1.3e-4)
+    args = (z["hdif_V"], z["visc"], z["beta"], z["dbeta"], z["dLvisc"], z["or1"], z["or2"])
+    lop = I.LOp(I.toroidal_solve_operators(sch, p.l_max, w[1], *args, ktopv=int(z["ktopv"]),
+                                           kbotv=int(z["kbotv"])))
+    ta = {k: cu(z["z_" + k]) for k in ("old", "impl", "expl0", "expl1")}
+    x, dx = torch.empty_like(ta["old"]), torch.empty_like(ta["old"])
+    I.update_field(p, sch, lop, x, dx, ta, w, I.toroidal_coefficients(p.l_max, *args))
+    errs = dict(z=rel_err(npy(x), z["z_new"]), dz=rel_err(npy(dx), z["dz_new"]),
+                impl=rel_err(npy(ta["impl"]), z["z_impl_new"]),
+                old=rel_err(npy(ta["old"]), z["z_old_new"]),
+                expl1=rel_err(npy(ta["expl1"]), z["z_expl1_new"]))
+    print(name, {k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        assert v < TOL, (k, v)
+
+
+@pytest.mark.parametrize("scheme,l_max,n_r,k", [("chebyshev", 127, 65, 1), ("FD", 255, 97, 2)])
+def test_update_toroidal_vs_oracle(scheme, l_max, n_r, k):
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialScheme
+
+    p = Plan(l_max, 1)
+    fd = scheme == "FD"
+    sch = RadialScheme(n_r, scheme, fd_order=4 if fd else 2)
+    r = sch.r
+    prof = dict(or1=1.0 / r, or2=1.0 / r ** 2, beta=-0.3 / r if fd else np.zeros(n_r),
+                dbeta=0.3 / r ** 2 if fd else np.zeros(n_r), dLvisc=np.zeros(n_r),
+                visc=np.ones(n_r))
+    hdif = np.ones(l_max + 1)
+    rng = np.random.default_rng(7 * l_max)
+    amp = (p.lm2l + 1.0)[:, None] ** -1.5
+    st = {kk: (rng.standard_normal((p.lm_max, n_r)) + 1j * rng.standard_normal((p.lm_max, n_r)))
+          * amp for kk in ("old", "impl", "expl0", "expl1")}
+    ta = {kk: cu(v) for kk, v in st.items()}
+    w = I.cnab2_weights(1e-4, 1.2e-4)
+    args = (hdif, prof["visc"], prof["beta"], prof["dbeta"], prof["dLvisc"], prof["or1"],
+            prof["or2"])
+    lop = I.LOp(I.toroidal_solve_operators(sch, l_max, w[1], *args, ktopv=k, kbotv=k))
+    x, dx = torch.empty_like(ta["old"]), torch.empty_like(ta["old"])
+    I.update_field(p, sch, lop, x, dx, ta, w, I.toroidal_coefficients(l_max, *args))
+    g = dict(lm2l=p.lm2l, lm2m=p.lm2m, l_max=l_max)
+    mats = (sch.rMat, sch.drMat, sch.d2rMat, sch.rnorm, sch.boundary_fac)
+    ref = oi.update_z(g, mats, prof, st, ([w[0]], [w[1], w[2]], [w[3], w[4]]), hdif, sch.D1m,
+                      sch.D2m, sch.chebyshev, sch.n_cheb, k, k, sch.fd_order)
+    for kk, got in (("x", x), ("dx", dx), ("impl", ta["impl"]), ("old", ta["old"]),
+                    ("expl1", ta["expl1"])):
+        e = rel_err(npy(got), ref[kk])
+        assert e < (TOL_IMPL if kk == "impl" else TOL), (scheme, kk, e)

@@ -246,3 +246,46 @@ def test_scalar_solve_operators(name):
     x = np.stack([M[l] @ rhs[i] for i, l in enumerate(z["lm2l"])])
     x[z["lm2m"] == 0] = x[z["lm2m"] == 0].real
     assert rel_err(x, z["s_new"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_update_z_oracle(name):
+    """The toroidal-velocity update restated in numpy against the reference's updateZ
+    (Chebyshev with stress-free rows; FD4 anelastic with no-slip rows and the banded
+    solve's identity at l = 0)."""
+    from oracle import implicit as oi
+
+    z = load_golden(name)
+    g = dict(lm2l=z["lm2l"], lm2m=z["lm2m"], l_max=int(z["l_max"]))
+    prof = {k: z[k] for k in ("or1", "or2", "beta", "dbeta", "dLvisc", "visc")}
+    mats = (z["rMat"], z["drMat"], z["d2rMat"], float(z["rnorm"]), float(z["boundary_fac"]))
+    st = {k: z["z_" + k].copy() for k in ("old", "impl", "expl0", "expl1")}
+    o = oi.update_z(g, mats, prof, st, (z["wimp"], z["wimp_lin"], z["wexp"]), z["hdif_V"],
+                    z["D1"], z["D2"], bool(z["chebyshev"]), int(z["n_cheb_max"]),
+                    int(z["ktopv"]), int(z["kbotv"]), int(z["fd_order"]))
+    for k, ref in (("x", "z_new"), ("dx", "dz_new"), ("impl", "z_impl_new"),
+                   ("old", "z_old_new"), ("expl1", "z_expl1_new")):
+        assert rel_err(o[k], z[ref]) < 1e-14, k
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_toroidal_solve_operators(name):
+    from types import SimpleNamespace
+
+    from magic_b200 import implicit as I
+
+    z = load_golden(name)
+    sch = SimpleNamespace(n_r=int(z["n_r_max"]), chebyshev=bool(z["chebyshev"]),
+                          n_cheb=int(z["n_cheb_max"]), rMat=z["rMat"], drMat=z["drMat"],
+                          d2rMat=z["d2rMat"], rnorm=float(z["rnorm"]),
+                          boundary_fac=float(z["boundary_fac"]), fd_order=int(z["fd_order"]))
+    w = I.cnab2_weights(1e-4, 1.3e-4)
+    M = I.toroidal_solve_operators(sch, int(z["l_max"]), w[1], z["hdif_V"], z["visc"], z["beta"],
+                                   z["dbeta"], z["dLvisc"], z["or1"], z["or2"], int(z["ktopv"]),
+                                   int(z["kbotv"]))
+    rhs = w[0] * z["z_old"] + w[2] * z["z_impl"] + w[3] * z["z_expl0"] + w[4] * z["z_expl1"]
+    rhs[:, 0] = 0.0
+    rhs[:, -1] = 0.0
+    x = np.stack([M[l] @ rhs[i] for i, l in enumerate(z["lm2l"])])
+    x[z["lm2m"] == 0] = x[z["lm2m"] == 0].real
+    assert rel_err(x, z["z_new"]) < 1e-13
