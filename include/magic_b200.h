@@ -313,10 +313,13 @@ MT_API int mt_get_td(const mt_plan* plan, int n_r, const mt_td_in* in, const mt_
  * One CNAB2 step of an equation whose implicit operator is a radial
  * operator per degree l: entropy (magic_torch/update_s.py:213-271 updateS),
  * composition (update_xi.py updateXi), toroidal velocity (update_z.py:333-505
- * updateZ without inner-core rotation or angular-momentum correction):
+ * updateZ without inner-core rotation or angular-momentum correction), the
+ * poloidal and toroidal magnetic field with an insulating inner core
+ * (update_b.py:98-635 updateB, b and j each one call):
  *   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1
  *         (time_scheme.py:82-96), rows 0 and n_r-1 = top / bot values;
  *   x = M_l rhs per degree l (m = 0 coefficients real), dx = D1 x,
+ *   d2x = D2 x (stored when d2x is not NULL),
  *   expl1 <- expl0 (time_scheme.py:130-143),
  *   old  <- so_l[l] so_r[r] x,
  *   impl <- ia_l[l] ia_r[r] (D2 x + ib_r[r] dx - (ic_r[r] + ic_l[l] ic_r2[r]) x).
@@ -335,7 +338,7 @@ MT_API int mt_lop_create(int n_l, int n_r, const double* M_host, mt_lop** op);
 MT_API int mt_lop_destroy(mt_lop* op);
 
 typedef struct {
-  double *x, *dx, *old, *impl, *expl0, *expl1;
+  double *x, *dx, *d2x, *old, *impl, *expl0, *expl1; /* d2x may be NULL */
   const double *top, *bot;
   int64_t ld;
   double w_old, w_impl, w_expl0, w_expl1;

@@ -93,7 +93,8 @@ class TdParams(C.Structure):
 
 
 class FieldUpdate(C.Structure):
-    _fields_ = [(n, _dp) for n in ("x", "dx", "old", "impl", "expl0", "expl1", "top", "bot")] + \
+    _fields_ = [(n, _dp) for n in ("x", "dx", "d2x", "old", "impl", "expl0", "expl1", "top",
+                                   "bot")] + \
                [("ld", _i64)] + \
                [(n, C.c_double) for n in ("w_old", "w_impl", "w_expl0", "w_expl1")] + \
                [(n, _dp) for n in ("so_l", "so_r", "ia_l", "ia_r", "ib_r", "ic_r", "ic_l",

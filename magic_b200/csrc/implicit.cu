@@ -17,7 +17,8 @@
 // k_update_field: CTA = (degree l, chunk of orders m), one warp per lm row:
 //   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1, rows 0 and
 //   n_r - 1 replaced by the boundary values; expl1 <- expl0 (rotation);
-//   x = M_l rhs, imaginary part dropped for m = 0; dx = D1 x, d2x = D2 x;
+//   x = M_l rhs, imaginary part dropped for m = 0; dx = D1 x, d2x = D2 x
+//   (d2x stored when requested);
 //   old <- so_l so_r x; impl <- ia_l ia_r (d2x + ib_r dx - (ic_r + ic_l ic_r2) x).
 // Rows of one l share M_l through L1 (the CTA's warps and co-resident CTAs).
 #include <algorithm>
@@ -41,7 +42,7 @@ constexpr int kUsWarps = 8;
 struct UsArgs {
   int n_r, l_max, minc, n_m;
   const int* lstart;
-  double2 *x, *dx, *old, *impl, *expl0, *expl1;
+  double2 *x, *dx, *d2x, *old, *impl, *expl0, *expl1;
   const double2 *top, *bot;
   int64_t ld;
   double w_old, w_impl, w_expl0, w_expl1;
@@ -90,6 +91,7 @@ __global__ void __launch_bounds__(32 * kUsWarps) k_update_field(UsArgs a) {
   for (int j = lane; j < n_r; j += 32) {
     const double2 d1 = op_row(a.D1, x, j), d2 = op_row(a.D2, x, j), v = x[j];
     a.dx[row + j] = d1;
+    if (a.d2x) a.d2x[row + j] = d2;
     const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
     a.old[row + j] = double2{so * v.x, so * v.y};
     const double c1 = a.ib_r[j], c0 = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
@@ -175,7 +177,7 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.n_m = p->n_m;
   a.lstart = p->d_lstart;
   auto d = [](double* x) { return (double2*)x; };
-  a.x = d(u->x); a.dx = d(u->dx); a.old = d(u->old); a.impl = d(u->impl);
+  a.x = d(u->x); a.dx = d(u->dx); a.d2x = d(u->d2x); a.old = d(u->old); a.impl = d(u->impl);
   a.expl0 = d(u->expl0); a.expl1 = d(u->expl1);
   a.top = (const double2*)u->top;
   a.bot = (const double2*)u->bot;

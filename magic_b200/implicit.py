@@ -56,8 +56,9 @@ def _inverse_ops(A, sch, zero_l0=False, identity_l0=False):
 
 
 def _bc_rows(A, sch, rows):
-    """Boundary rows (row index -> matrix row), the Chebyshev columns >= n_cheb
-    dropped in them, then columns 0 and n_r-1 scaled by boundary_fac."""
+    """Boundary rows (row index -> matrix row, or one row per degree), the
+    Chebyshev columns >= n_cheb dropped in them, then columns 0 and n_r-1 scaled
+    by boundary_fac."""
     N = sch.n_r
     for i, v in rows.items():
         A[:, i, :] = v
@@ -111,6 +112,45 @@ def toroidal_solve_operators(sch, l_max, wimp_lin0, hdif, visc, beta, dbeta, dLv
     return _inverse_ops(A, sch, zero_l0=not banded_l0, identity_l0=banded_l0)
 
 
+def magnetic_solve_operators(sch, l_max, wimp_lin0, opm, hdif, lam, dLlam, or1, or2):
+    """(M_b, M_j): solve operators of the poloidal and toroidal magnetic field with
+    an insulating inner core and mantle (magic_torch/update_b.py:98-280):
+        bulk rows  rnorm l(l+1) or2 (rMat - wimp_lin0 opm lambda hdif_l (d2rMat
+                   [+ dLlambda drMat for j] - l(l+1) or2 rMat)),
+        b: rows rnorm (drMat + l or1 rMat) at the top and rnorm (drMat - (l+1) or1 rMat)
+           at the bottom (potential-field matching), j: Dirichlet rows rnorm rMat.
+    Degree 0: zero, except the identity of the banded finite-difference solve."""
+    N = sch.n_r
+    ls = np.arange(l_max + 1, dtype=np.float64)
+    dL = (ls * (ls + 1.0))[:, None, None]
+    hd = np.asarray(hdif, dtype=np.float64)[:, None, None]
+    base = sch.rnorm * dL * or2[None, :, None]
+    lap = dL * or2[None, :, None] * sch.rMat[None]
+    Ab = base * (sch.rMat[None] - wimp_lin0 * opm * lam[None, :, None] * hd
+                 * (sch.d2rMat[None] - lap))
+    Aj = base * (sch.rMat[None] - wimp_lin0 * opm * lam[None, :, None] * hd
+                 * (sch.d2rMat[None] + dLlam[None, :, None] * sch.drMat[None] - lap))
+    top = sch.rnorm * (sch.drMat[0][None] + ls[:, None] * or1[0] * sch.rMat[0][None])
+    bot = sch.rnorm * (sch.drMat[N - 1][None] - (ls[:, None] + 1.0) * or1[N - 1]
+                       * sch.rMat[N - 1][None])
+    Ab = _bc_rows(Ab, sch, {0: top, N - 1: bot})
+    Aj = _bc_rows(Aj, sch, {0: sch.rnorm * sch.rMat[0], N - 1: sch.rnorm * sch.rMat[N - 1]})
+    banded_l0 = (not sch.chebyshev) and getattr(sch, "fd_order", 2) > 2
+    return (_inverse_ops(Ab, sch, zero_l0=not banded_l0, identity_l0=banded_l0),
+            _inverse_ops(Aj, sch, zero_l0=not banded_l0, identity_l0=banded_l0))
+
+
+def magnetic_coefficients(l_max, opm, hdif, lam, dLlam, or2):
+    """Coefficients of mt_update_field for b and j (magic_torch/update_b.py:616-631):
+    old = l(l+1) or2 x; impl = opm lambda hdif l(l+1) or2 (d2x [+ dLlambda dx for j]
+    - l(l+1) or2 x)."""
+    ls = np.arange(l_max + 1, dtype=np.float64)
+    dLh = ls * (ls + 1.0)
+    ia_l = opm * np.asarray(hdif, dtype=np.float64) * dLh
+    common = dict(so_l=dLh, so_r=or2, ia_l=ia_l, ia_r=lam * or2, ic_r=None, ic_l=dLh, ic_r2=or2)
+    return dict(common, ib_r=np.zeros_like(or2)), dict(common, ib_r=dLlam)
+
+
 def entropy_coefficients(l_max, opr, hdif, kappa, d1c, or2):
     """Coefficients of mt_update_field for entropy / composition
     (magic_torch/update_s.py:262-270): old = s, impl = opr hdif kappa
@@ -159,11 +199,12 @@ class LOp:
             self._h = None
 
 
-def update_field(plan, sch, lop, x, dx, ta, weights, coef, top=None, bot=None):
-    """One implicit step of a field in place (mt_update_field): x, dx (lm_max, n_r)
-    complex128 outputs; ta: dict old, impl, expl0, expl1 of the same shape (updated in
-    place); weights: cnab2_weights(...); coef: entropy_coefficients(...) or
-    toroidal_coefficients(...); top / bot: (lm_max) complex boundary values or None."""
+def update_field(plan, sch, lop, x, dx, ta, weights, coef, top=None, bot=None, d2x=None):
+    """One implicit step of a field in place (mt_update_field): x, dx (and d2x when
+    given) (lm_max, n_r) complex128 outputs; ta: dict old, impl, expl0, expl1 of the
+    same shape (updated in place); weights: cnab2_weights(...); coef:
+    entropy_coefficients(...), toroidal_coefficients(...) or one of
+    magnetic_coefficients(...); top / bot: (lm_max) complex boundary values or None."""
     n_r = x.shape[1]
     arrs = [x, dx, ta["old"], ta["impl"], ta["expl0"], ta["expl1"]]
     for a in arrs:
@@ -173,7 +214,12 @@ def update_field(plan, sch, lop, x, dx, ta, weights, coef, top=None, bot=None):
     names = ("so_l", "so_r", "ia_l", "ia_r", "ib_r", "ic_r", "ic_l", "ic_r2")
     dev = {k: (torch.as_tensor(coef[k], dtype=torch.float64, device=x.device).contiguous()
                if coef.get(k) is not None else None) for k in names}
-    u = _lib.FieldUpdate(*[a.data_ptr() for a in arrs],
+    if d2x is not None and (d2x.shape != x.shape or d2x.dtype != torch.complex128
+                            or not d2x.is_contiguous()):
+        raise ValueError("d2x must be a contiguous (lm_max, n_r) complex128 array")
+    u = _lib.FieldUpdate(arrs[0].data_ptr(), arrs[1].data_ptr(),
+                         d2x.data_ptr() if d2x is not None else None,
+                         *[a.data_ptr() for a in arrs[2:]],
                          top.data_ptr() if top is not None else None,
                          bot.data_ptr() if bot is not None else None, n_r,
                          w_old, w_impl, w_e0, w_e1,

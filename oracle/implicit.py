@@ -136,3 +136,76 @@ def update_z(g, mats, prof, st, weights, hdif, D1, D2, chebyshev, n_cheb, ktopv,
     impl = hdif[g["lm2l"]][:, None] * dLh * or2 * p["visc"][None, :] * (
         d2z + (p["dLvisc"] - p["beta"])[None, :] * dz - (z0 + dLh * or2) * x)
     return dict(x=x, dx=dz, impl=impl, old=dLh * or2 * x, expl1=st["expl0"].copy())
+
+
+def b_matrices(l, mats, prof, wimp_lin0, opm, hdif_l, n_cheb):
+    """Poloidal (b) and toroidal (j) magnetic LHS of degree l >= 1 with an
+    insulating inner core (magic_torch/update_b.py:160-240): bulk rows
+    rnorm l(l+1)/r^2 (rMat - wimp opm lambda hdif (d2rMat [+ dLlambda drMat for j]
+    - l(l+1)/r^2 rMat)); b: rows rnorm (drMat + l/r rMat) at the top, rnorm (drMat
+    - (l+1)/r rMat) at the bottom; j: Dirichlet rows."""
+    rMat, drMat, d2rMat, rnorm, bfac = mats
+    N = rMat.shape[0]
+    p = prof
+    dL = float(l * (l + 1))
+    out = []
+    for with_dl in (False, True):
+        inner = d2rMat - dL * p["or2"][:, None] * rMat
+        if with_dl:
+            inner = inner + p["dLlambda"][:, None] * drMat
+        dat = rnorm * dL * p["or2"][:, None] * (
+            rMat - wimp_lin0 * opm * p["lambda_"][:, None] * hdif_l * inner)
+        if with_dl:
+            dat[0, :] = rnorm * rMat[0, :]
+            dat[N - 1, :] = rnorm * rMat[N - 1, :]
+        else:
+            dat[0, :] = rnorm * (drMat[0, :] + l * p["or1"][0] * rMat[0, :])
+            dat[N - 1, :] = rnorm * (drMat[N - 1, :] - (l + 1) * p["or1"][N - 1] * rMat[N - 1, :])
+        if n_cheb < N:
+            dat[0, n_cheb:] = 0.0
+            dat[N - 1, n_cheb:] = 0.0
+        dat[:, 0] *= bfac
+        dat[:, N - 1] *= bfac
+        out.append(dat)
+    return out
+
+
+def update_b(g, mats, prof, stb, stj, weights, opm, hdif, D1, D2, chebyshev, n_cheb, fd_order):
+    """One updateB with an insulating inner core (magic_torch/update_b.py:530-635):
+    both fields as update_z with their own matrices (degree 0 as there), old =
+    l(l+1)/r^2 x and impl = opm lambda hdif l(l+1)/r^2 (d2x [+ dLlambda dx for j]
+    - l(l+1)/r^2 x).  Returns the dicts of b and j (x, dx, d2x, impl, old, expl1)."""
+    wimp, wimp_lin, wexp = weights
+    N = stb["old"].shape[1]
+    res = []
+    for fi, st in enumerate((stb, stj)):
+        rhs = wimp[0] * st["old"] + wimp_lin[1] * st["impl"] + wexp[0] * st["expl0"] \
+            + wexp[1] * st["expl1"]
+        rhs[:, 0] = 0.0
+        rhs[:, N - 1] = 0.0
+        x = np.zeros_like(rhs)
+        for l in range(g["l_max"] + 1):
+            rows = np.nonzero(g["lm2l"] == l)[0]
+            if l == 0:
+                if not chebyshev and fd_order > 2:
+                    x[rows] = rhs[rows]
+                continue
+            dat = b_matrices(l, mats, prof, wimp_lin[0], opm, hdif[l], n_cheb)[fi]
+            fac = 1.0 / np.abs(dat).max(axis=1)
+            x[rows] = np.linalg.solve(fac[:, None] * dat, (fac[None, :] * rhs[rows]).T).T
+        m0 = g["lm2m"] == 0
+        x[m0] = x[m0].real
+        if chebyshev:
+            if n_cheb < N:
+                x[:, n_cheb:] = 0.0
+            x = x @ dct1_matrix(N).T
+        dx, d2x = x @ D1.T, x @ D2.T
+        dLh = (g["lm2l"] * (g["lm2l"] + 1.0))[:, None]
+        or2 = prof["or2"][None, :]
+        inner = d2x - dLh * or2 * x
+        if fi:
+            inner = inner + prof["dLlambda"][None, :] * dx
+        impl = opm * prof["lambda_"][None, :] * hdif[g["lm2l"]][:, None] * dLh * or2 * inner
+        res.append(dict(x=x, dx=dx, d2x=d2x, impl=impl, old=dLh * or2 * x,
+                        expl1=st["expl0"].copy()))
+    return res

@@ -279,6 +279,25 @@ def worker_td(name, ref):
     uz.updateZ(z_new, dz_new, tz, tscheme)
     out.update(z_new=n(z_new), dz_new=n(dz_new), z_impl_new=n(tz.impl[:, :, 0]),
                z_old_new=n(tz.old[:, :, 0]), z_expl1_new=n(tz.expl[:, :, 1]))
+    # one implicit magnetic update, insulating inner core (update_b.py:98-635)
+    from magic_torch import update_b as ub
+    ub.build_b_matrices(tscheme.wimp_lin[0].item())
+    tb = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+    tj = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+    for f, ta_ in (("b", tb), ("j", tj)):
+        for k in ("old", "impl", "expl0", "expl1"):
+            v = _spec(rng, lm, l_of, N)
+            (ta_.old if k == "old" else ta_.impl if k == "impl" else ta_.expl)[
+                :, :, 1 if k == "expl1" else 0] = t(v)
+            out[f + "_" + k] = v
+    out.update(opm=float(pc.opm), lambda_=n(rf2.lambda_), dLlambda=n(rf2.dLlambda),
+               hdif_B=n(hd.hdif_B))
+    bj = [torch.zeros(lm, N, dtype=torch.complex128) for _ in range(6)]
+    ub.updateB(*bj, tb, tj, tscheme)
+    for f, ta_, (x, dx, d2x) in (("b", tb, bj[:3]), ("j", tj, bj[3:])):
+        out.update({f + "_new": n(x), "d" + f + "_new": n(dx), "dd" + f + "_new": n(d2x),
+                    f + "_impl_new": n(ta_.impl[:, :, 0]), f + "_old_new": n(ta_.old[:, :, 0]),
+                    f + "_expl1_new": n(ta_.expl[:, :, 1])})
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

@@ -1,7 +1,7 @@
 """Implicit field updates (CNAB2 right-hand side, per-degree solve, radial
 derivatives, next implicit term, history rotation) on the GPU in FP64, for the
-entropy and the toroidal velocity: against the reference's own updateS and
-updateZ outputs (tests/golden/td_*.npz) and against the numpy oracle for two
+entropy, the toroidal velocity and the magnetic field: against the
+reference's own updateS, updateZ and updateB outputs (tests/golden/td_*.npz) and against the numpy oracle for two
 consecutive steps at l_max = 127 / 65 Chebyshev levels and l_max = 255 / 97
 fourth-order finite-difference levels.
 
@@ -177,3 +177,67 @@ def test_update_toroidal_vs_oracle(scheme, l_max, n_r, k):
                     ("expl1", ta["expl1"])):
         e = rel_err(npy(got), ref[kk])
         assert e < (TOL_IMPL if kk == "impl" else TOL), (scheme, kk, e)
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_update_magnetic_matches_reference(name):
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+
+    z = load_golden(name)
+    p = Plan(int(z["l_max"]), int(z["minc"]))
+    sch = _sch_from(z)
+    w = I.cnab2_weights(1e-4, 1.3e-4)
+    Mb, Mj = I.magnetic_solve_operators(sch, p.l_max, w[1], float(z["opm"]), z["hdif_B"],
+                                        z["lambda_"], z["dLlambda"], z["or1"], z["or2"])
+    cb, cj = I.magnetic_coefficients(p.l_max, float(z["opm"]), z["hdif_B"], z["lambda_"],
+                                     z["dLlambda"], z["or2"])
+    for f, M, c in (("b", Mb, cb), ("j", Mj, cj)):
+        ta = {k: cu(z[f + "_" + k]) for k in ("old", "impl", "expl0", "expl1")}
+        x, dx, d2x = (torch.empty_like(ta["old"]) for _ in range(3))
+        I.update_field(p, sch, I.LOp(M), x, dx, ta, w, c, d2x=d2x)
+        errs = dict(x=rel_err(npy(x), z[f + "_new"]), dx=rel_err(npy(dx), z["d" + f + "_new"]),
+                    d2x=rel_err(npy(d2x), z["dd" + f + "_new"]),
+                    impl=rel_err(npy(ta["impl"]), z[f + "_impl_new"]),
+                    old=rel_err(npy(ta["old"]), z[f + "_old_new"]),
+                    expl1=rel_err(npy(ta["expl1"]), z[f + "_expl1_new"]))
+        print(name, f, {k: f"{v:.1e}" for k, v in errs.items()})
+        for k, v in errs.items():
+            assert v < TOL, (f, k, v)
+
+
+@pytest.mark.parametrize("scheme,l_max,n_r", [("chebyshev", 127, 65), ("FD", 255, 97)])
+def test_update_magnetic_vs_oracle(scheme, l_max, n_r):
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialScheme
+
+    p = Plan(l_max, 1)
+    fd = scheme == "FD"
+    sch = RadialScheme(n_r, scheme, fd_order=4 if fd else 2)
+    r = sch.r
+    prof = dict(or1=1.0 / r, or2=1.0 / r ** 2, lambda_=np.ones(n_r),
+                dLlambda=0.2 / r if fd else np.zeros(n_r))
+    hdif, opm = np.ones(l_max + 1), 0.2
+    rng = np.random.default_rng(11 * l_max)
+    amp = (p.lm2l + 1.0)[:, None] ** -1.5
+    spec = lambda: (rng.standard_normal((p.lm_max, n_r))
+                    + 1j * rng.standard_normal((p.lm_max, n_r))) * amp
+    st = {f: {k: spec() for k in ("old", "impl", "expl0", "expl1")} for f in ("b", "j")}
+    w = I.cnab2_weights(1e-4, 1.2e-4)
+    Mb, Mj = I.magnetic_solve_operators(sch, l_max, w[1], opm, hdif, prof["lambda_"],
+                                        prof["dLlambda"], prof["or1"], prof["or2"])
+    cb, cj = I.magnetic_coefficients(l_max, opm, hdif, prof["lambda_"], prof["dLlambda"],
+                                     prof["or2"])
+    g = dict(lm2l=p.lm2l, lm2m=p.lm2m, l_max=l_max)
+    mats = (sch.rMat, sch.drMat, sch.d2rMat, sch.rnorm, sch.boundary_fac)
+    ref = oi.update_b(g, mats, prof, st["b"], st["j"], ([w[0]], [w[1], w[2]], [w[3], w[4]]),
+                      opm, hdif, sch.D1m, sch.D2m, sch.chebyshev, sch.n_cheb, sch.fd_order)
+    for f, M, c, o in (("b", Mb, cb, ref[0]), ("j", Mj, cj, ref[1])):
+        ta = {k: cu(v) for k, v in st[f].items()}
+        x, dx, d2x = (torch.empty_like(ta["old"]) for _ in range(3))
+        I.update_field(p, sch, I.LOp(M), x, dx, ta, w, c, d2x=d2x)
+        for k, got in (("x", x), ("dx", dx), ("d2x", d2x), ("impl", ta["impl"]),
+                       ("old", ta["old"]), ("expl1", ta["expl1"])):
+            e = rel_err(npy(got), o[k])
+            assert e < (TOL_IMPL if k in ("impl", "d2x") else TOL), (scheme, f, k, e)

@@ -289,3 +289,25 @@ def test_toroidal_solve_operators(name):
     x = np.stack([M[l] @ rhs[i] for i, l in enumerate(z["lm2l"])])
     x[z["lm2m"] == 0] = x[z["lm2m"] == 0].real
     assert rel_err(x, z["z_new"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["td_cheb", "td_fd_anel"])
+def test_update_b_oracle(name):
+    """The magnetic update (insulating inner core) restated in numpy against the
+    reference's updateB, both fields and their first and second derivatives."""
+    from oracle import implicit as oi
+
+    z = load_golden(name)
+    g = dict(lm2l=z["lm2l"], lm2m=z["lm2m"], l_max=int(z["l_max"]))
+    prof = {k: z[k] for k in ("or1", "or2", "lambda_", "dLlambda")}
+    mats = (z["rMat"], z["drMat"], z["d2rMat"], float(z["rnorm"]), float(z["boundary_fac"]))
+    st = {f: {k: z[f + "_" + k].copy() for k in ("old", "impl", "expl0", "expl1")}
+          for f in ("b", "j")}
+    ob, oj = oi.update_b(g, mats, prof, st["b"], st["j"], (z["wimp"], z["wimp_lin"], z["wexp"]),
+                         float(z["opm"]), z["hdif_B"], z["D1"], z["D2"], bool(z["chebyshev"]),
+                         int(z["n_cheb_max"]), int(z["fd_order"]))
+    for f, o in (("b", ob), ("j", oj)):
+        for k, ref in (("x", f + "_new"), ("dx", "d" + f + "_new"), ("d2x", "dd" + f + "_new"),
+                       ("impl", f + "_impl_new"), ("old", f + "_old_new"),
+                       ("expl1", f + "_expl1_new")):
+            assert rel_err(o[k], z[ref]) < 1e-14, (f, k)
