@@ -349,6 +349,35 @@ MT_API int mt_update_field(const mt_plan* plan, int n_r, const mt_field_update* 
                            const mt_lop* solve, const mt_radial_op* D1,
                            const mt_radial_op* D2, void* stream);
 
+/* ---- implicit update of the poloidal velocity, double-curl form ----------
+ * One CNAB2 step of magic_torch/update_w_doublecurl.py:393-483 (updateW, the
+ * finite-difference scheme) with the l = 0 pressure of update_wp.py:80-194:
+ *   rhs = CNAB2 combination + wimp_lin0 BuoFac l(l+1) or2 rgrav s on rows
+ *         2..n_r-3 (+ ChemFac ... xi), rows 0, 1, n_r-2, n_r-1 zero;
+ *   w = M_l rhs (degree 0 zero, m = 0 real), dw = D1 w, ddw = D2 w,
+ *   dddw = D1 ddw, ddddw = D2 ddw;
+ *   old  <- -l(l+1) or2 orho1 (ddw - beta dw - l(l+1) or2 w),
+ *   impl <- -hdif_l l(l+1) or2 visc orho1 (ddddw + c3 dddw + c2 ddw + c1 dw + c0 w)
+ *           + BuoFac l(l+1) or2 rgrav s (+ ChemFac ... xi), both zero at r_0, r_N-1,
+ *     c2 = c2n - 2 l(l+1) or2, c1 = c1n + l(l+1) c1d, c0 = l(l+1) or2 (c0n + l(l+1) or2);
+ *   expl1 <- expl0;
+ *   p(0,0) = P0 (0, rho0 BuoFac rgrav Re s00 + Re expl0_00 (+ chemistry), ...).
+ * s / xi: the entropy / composition of this step (after their own update).
+ * P0: the inverse of the l = 0 pressure matrix as a radial operator. */
+typedef struct {
+  double *w, *dw, *ddw, *old, *impl, *expl0, *expl1, *p; /* p: row (l, m) = (0, 0) only */
+  const double *s, *xi;                                   /* xi may be NULL */
+  int64_t ld;
+  double w_old, w_impl, w_expl0, w_expl1, wimp_lin0, BuoFac, ChemFac;
+  const double* hdif;                                     /* (l_max + 1) */
+  const double *or2, *orho1, *beta, *visc, *rgrav, *rho0; /* (n_r) */
+  const double *c3, *c2n, *c1n, *c1d, *c0n;               /* (n_r) */
+} mt_poloidal_update;
+
+MT_API int mt_update_poloidal(const mt_plan* plan, int n_r, const mt_poloidal_update* u,
+                              const mt_lop* solve, const mt_radial_op* D1,
+                              const mt_radial_op* D2, const mt_radial_op* P0, void* stream);
+
 MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
 
 /* Thread-local message for the last non-zero status. */

@@ -101,6 +101,15 @@ class FieldUpdate(C.Structure):
                                    "ic_r2")]
 
 
+class PoloidalUpdate(C.Structure):
+    _fields_ = [(n, _dp) for n in ("w", "dw", "ddw", "old", "impl", "expl0", "expl1", "p", "s",
+                                   "xi")] + [("ld", _i64)] + \
+               [(n, C.c_double) for n in ("w_old", "w_impl", "w_expl0", "w_expl1", "wimp_lin0",
+                                          "BuoFac", "ChemFac")] + \
+               [(n, _dp) for n in ("hdif", "or2", "orho1", "beta", "visc", "rgrav", "rho0", "c3",
+                                   "c2n", "c1n", "c1d", "c0n")]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "mt_plan_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
@@ -143,6 +152,8 @@ _PROTOS = {
     "mt_lop_destroy": (C.c_int, [C.c_void_p]),
     "mt_update_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FieldUpdate), C.c_void_p,
                                   C.c_void_p, C.c_void_p, _dp]),
+    "mt_update_poloidal": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PoloidalUpdate), C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }

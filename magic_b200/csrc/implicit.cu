@@ -1,5 +1,6 @@
-// Implicit (IMEX) update of a field whose implicit operator is a radial
-// operator per degree l (FP64): entropy, composition, toroidal velocity.
+// Implicit (IMEX) updates with a per-degree solve (FP64): entropy,
+// composition, toroidal velocity, magnetic field (k_update_field) and the
+// double-curl poloidal velocity with the l = 0 pressure (k_update_poloidal).
 //
 // Replaces magic_torch/update_s.py:213-271 (updateS; updateXi,
 // update_xi.py:208-262, has the same form) and update_z.py:333-505 (updateZ
@@ -100,6 +101,113 @@ __global__ void __launch_bounds__(32 * kUsWarps) k_update_field(UsArgs a) {
   }
 }
 
+struct PwArgs {
+  int n_r, l_max, minc, n_m;
+  const int* lstart;
+  double2 *w, *dw, *ddw, *old, *impl, *expl0, *expl1, *p;
+  const double2 *s, *xi;
+  int64_t ld;
+  double w_old, w_impl, w_expl0, w_expl1, wimp_lin0, BuoFac, ChemFac;
+  const double* hdif;
+  const double *or2, *orho1, *beta, *visc, *rgrav, *rho0, *c3, *c2n, *c1n, *c1d, *c0n;
+  const double* mt;
+  OpView D1, D2, P0;
+};
+
+// Double-curl poloidal update (magic_torch/update_w_doublecurl.py:393-483):
+// CTA = (degree l, chunk of orders m), one warp per lm row; the warp of
+// (l, m) = (0, 0) also solves the l = 0 pressure (update_wp.py:173-194).
+__global__ void __launch_bounds__(32 * kUsWarps) k_update_poloidal(PwArgs a) {
+  extern __shared__ double2 pwbuf[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int n_r = a.n_r, l = blockIdx.x;
+  const int mc = blockIdx.y * kUsWarps + wib, m = mc * a.minc;
+  if (mc >= a.n_m || m > l) return;
+  const int lm = a.lstart[mc] + (l - m);
+  const int64_t row = (int64_t)lm * a.ld;
+  double2* rhs = pwbuf + (int64_t)wib * 3 * n_r;
+  double2* x = rhs + n_r;
+  double2* dd = x + n_r;
+  const double2 zero = {0.0, 0.0};
+  const double dL = (double)l * (l + 1.0);
+  for (int k = lane; k < n_r; k += 32) {
+    const double2 o = a.old[row + k], im = a.impl[row + k];
+    const double2 e0 = a.expl0[row + k], e1 = a.expl1[row + k];
+    double2 v;
+    v.x = a.w_old * o.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
+    v.y = a.w_old * o.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
+    const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
+    const double2 sv = a.s[row + k];
+    v.x += gb * a.BuoFac * sv.x;
+    v.y += gb * a.BuoFac * sv.y;
+    if (a.xi) {
+      const double2 xv = a.xi[row + k];
+      v.x += gb * a.ChemFac * xv.x;
+      v.y += gb * a.ChemFac * xv.y;
+    }
+    if (k < 2 || k > n_r - 3 || l == 0) v = zero;
+    rhs[k] = v;
+    a.expl1[row + k] = e0;
+  }
+  __syncwarp();
+  const double* M = a.mt + (int64_t)l * n_r * n_r;
+  for (int j = lane; j < n_r; j += 32) {
+    double2 acc = zero;
+    for (int k = 0; k < n_r; ++k) {
+      const double c = __ldg(M + (int64_t)k * n_r + j);
+      acc.x = fma(c, rhs[k].x, acc.x);
+      acc.y = fma(c, rhs[k].y, acc.y);
+    }
+    if (m == 0) acc.y = 0.0;
+    x[j] = acc;
+    a.w[row + j] = acc;
+  }
+  __syncwarp();
+  for (int j = lane; j < n_r; j += 32) {
+    const double2 d2 = op_row(a.D2, x, j);
+    dd[j] = d2;
+    a.ddw[row + j] = d2;
+  }
+  __syncwarp();
+  const double hd = a.hdif[l];
+  for (int j = lane; j < n_r; j += 32) {
+    const double2 d1 = op_row(a.D1, x, j), d2 = dd[j];
+    const double2 d3 = op_row(a.D1, dd, j), d4 = op_row(a.D2, dd, j), v = x[j];
+    a.dw[row + j] = d1;
+    const bool bnd = j == 0 || j == n_r - 1;
+    const double or2 = a.or2[j], orho1 = a.orho1[j], beta = a.beta[j];
+    const double dLo = dL * or2;
+    const double fo = -dLo * orho1;
+    a.old[row + j] = bnd ? zero
+                         : double2{fo * (d2.x - beta * d1.x - dLo * v.x),
+                                   fo * (d2.y - beta * d1.y - dLo * v.y)};
+    const double c3 = a.c3[j], c2 = a.c2n[j] - 2.0 * dLo, c1 = a.c1n[j] + dL * a.c1d[j];
+    const double c0 = dLo * (a.c0n[j] + dLo);
+    const double fd = -hd * dLo * a.visc[j] * orho1;
+    const double gb = dLo * a.rgrav[j];
+    const double2 sv = a.s[row + j];
+    double2 im;
+    im.x = fd * (d4.x + c3 * d3.x + c2 * d2.x + c1 * d1.x + c0 * v.x) + a.BuoFac * gb * sv.x;
+    im.y = fd * (d4.y + c3 * d3.y + c2 * d2.y + c1 * d1.y + c0 * v.y) + a.BuoFac * gb * sv.y;
+    if (a.xi) {
+      const double2 xv = a.xi[row + j];
+      im.x += a.ChemFac * gb * xv.x;
+      im.y += a.ChemFac * gb * xv.y;
+    }
+    a.impl[row + j] = bnd ? zero : im;
+  }
+  if (l != 0 || m != 0 || !a.p) return;
+  // l = 0 pressure: P0 (0, rho0 BuoFac rgrav Re s + Re expl0 [+ chemistry])
+  __syncwarp();
+  for (int k = lane; k < n_r; k += 32) {
+    double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row + k].x + a.expl0[row + k].x;
+    if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row + k].x;
+    rhs[k] = double2{k == 0 ? 0.0 : v, 0.0};
+  }
+  __syncwarp();
+  for (int j = lane; j < n_r; j += 32) a.p[row + j] = double2{op_row(a.P0, rhs, j).x, 0.0};
+}
+
 int check_lop(const mt_lop* op) {
   MT_REQUIRE(op && op->mt, MT_ERR_ARG, "null per-degree operator");
   int dev = -1;
@@ -193,6 +301,57 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
                                      (int)sm));
   const dim3 grid(p->l_max + 1, (p->n_m + kUsWarps - 1) / kUsWarps);
   k_update_field<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
+                       const mt_lop* solve, const mt_radial_op* D1, const mt_radial_op* D2,
+                       const mt_radial_op* P0, void* stream) {
+  MT_REQUIRE(p && u, MT_ERR_ARG, "null argument");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == p->device, MT_ERR_ARG, "plan used on a different device than it was built on");
+  MT_TRY(check_lop(solve));
+  MT_TRY(check_radial_op(D1));
+  MT_TRY(check_radial_op(D2));
+  MT_TRY(check_radial_op(P0));
+  MT_REQUIRE(solve->n_r == n_r && radial_op_size(D1) == n_r && radial_op_size(D2) == n_r &&
+                 radial_op_size(P0) == n_r,
+             MT_ERR_ARG, "operator sizes differ from n_r");
+  MT_REQUIRE(solve->n_l == p->l_max + 1, MT_ERR_ARG, "solve operators must cover l = 0..l_max");
+  MT_REQUIRE(n_r >= 5 && u->ld >= n_r, MT_ERR_ARG, "bad radial size or stride");
+  MT_REQUIRE(u->w && u->dw && u->ddw && u->old && u->impl && u->expl0 && u->expl1 && u->s,
+             MT_ERR_ARG, "null field or time array");
+  MT_REQUIRE(u->hdif && u->or2 && u->orho1 && u->beta && u->visc && u->rgrav && u->rho0 &&
+                 u->c3 && u->c2n && u->c1n && u->c1d && u->c0n,
+             MT_ERR_ARG, "null coefficient array");
+  PwArgs a{};
+  a.n_r = n_r;
+  a.l_max = p->l_max;
+  a.minc = p->minc;
+  a.n_m = p->n_m;
+  a.lstart = p->d_lstart;
+  auto d = [](double* x) { return (double2*)x; };
+  a.w = d(u->w); a.dw = d(u->dw); a.ddw = d(u->ddw); a.old = d(u->old); a.impl = d(u->impl);
+  a.expl0 = d(u->expl0); a.expl1 = d(u->expl1); a.p = d(u->p);
+  a.s = (const double2*)u->s;
+  a.xi = (const double2*)u->xi;
+  a.ld = u->ld;
+  a.w_old = u->w_old; a.w_impl = u->w_impl; a.w_expl0 = u->w_expl0; a.w_expl1 = u->w_expl1;
+  a.wimp_lin0 = u->wimp_lin0; a.BuoFac = u->BuoFac; a.ChemFac = u->ChemFac;
+  a.hdif = u->hdif;
+  a.or2 = u->or2; a.orho1 = u->orho1; a.beta = u->beta; a.visc = u->visc; a.rgrav = u->rgrav;
+  a.rho0 = u->rho0; a.c3 = u->c3; a.c2n = u->c2n; a.c1n = u->c1n; a.c1d = u->c1d; a.c0n = u->c0n;
+  a.mt = solve->mt;
+  a.D1 = radial_op_view(D1);
+  a.D2 = radial_op_view(D2);
+  a.P0 = radial_op_view(P0);
+  const size_t sm = (size_t)kUsWarps * 3 * n_r * sizeof(double2);
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_poloidal,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const dim3 grid(p->l_max + 1, (p->n_m + kUsWarps - 1) / kUsWarps);
+  k_update_poloidal<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

@@ -151,6 +151,103 @@ def magnetic_coefficients(l_max, opm, hdif, lam, dLlam, or2):
     return dict(common, ib_r=np.zeros_like(or2)), dict(common, ib_r=dLlam)
 
 
+def _w_coefficient_profiles(prof):
+    """(c3, c2n, c1n, c1d, c0n) of the double-curl diffusion operator
+    (magic_torch/update_w_doublecurl.py:146-168): c2 = c2n - 2 l(l+1) or2,
+    c1 = c1n + l(l+1) c1d, c0 = l(l+1) or2 (c0n + l(l+1) or2)."""
+    dLv, ddLv, b, db, ddb, or1, or2 = (prof[k] for k in ("dLvisc", "ddLvisc", "beta", "dbeta",
+                                                          "ddbeta", "or1", "or2"))
+    c3 = 2.0 * (dLv - b)
+    c2n = ddLv - 2.0 * db + dLv ** 2 + b ** 2 - 3.0 * dLv * b - 2.0 * or1 * (dLv + b)
+    c1n = (-ddb - db * (2.0 * dLv - b + 2.0 * or1) - ddLv * (b + 2.0 * or1)
+           + b ** 2 * (dLv + 2.0 * or1) - b * (dLv ** 2 - 2.0 * or2)
+           - 2.0 * dLv * or1 * (dLv - or1))
+    c1d = 2.0 * (2.0 * or1 + b - dLv) * or2
+    c0n = (2.0 * db + ddLv + dLv ** 2 - (2.0 / 3.0) * b ** 2 + dLv * b
+           + 2.0 * or1 * (2.0 * dLv - b - 3.0 * or1))
+    return c3, c2n, c1n, c1d, c0n
+
+
+def poloidal_dc_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbotv=2):
+    """(l_max+1, n_r, n_r) solve operators of the double-curl poloidal LHS on
+    finite-difference grid values (magic_torch/update_w_doublecurl.py:67-300):
+    rows 2..n_r-3  -l(l+1) or2 orho1 (d2 - beta d - l(l+1) or2)
+                   + wimp_lin0 orho1 hdif_l visc l(l+1) or2 (d4 + c3 d3 + c2 d2 + c1 d + c0),
+    rows 0, n_r-1: w = 0; rows 1, n_r-2: dw = 0 (no-slip) or d2w - (2 or1 + beta) dw = 0
+    (stress-free) at the boundary.  Inverted through the reference's row, then column
+    scaling; degree 0 zero.  prof: or1, or2, beta, dbeta, ddbeta, visc, dLvisc,
+    ddLvisc, orho1 over n_r."""
+    if sch.chebyshev:
+        raise ValueError("the double-curl form is used with finite differences only")
+    N = sch.n_r
+    D = (np.eye(N), sch.D1m, sch.D2m, sch.D3m, sch.D4m)
+    c3, c2n, c1n, c1d, c0n = _w_coefficient_profiles(prof)
+    or1, or2, beta, orho1, visc = (prof[k] for k in ("or1", "or2", "beta", "orho1", "visc"))
+    M = np.zeros((l_max + 1, N, N))
+    b = slice(2, N - 2)
+    for l in range(1, l_max + 1):
+        dL = float(l * (l + 1))
+        dLo = dL * or2
+        old = (-dLo * orho1)[b, None] * (D[2][b] - beta[b, None] * D[1][b] - dLo[b, None] * D[0][b])
+        c2, c1, c0 = c2n - 2.0 * dLo, c1n + dL * c1d, dLo * (c0n + dLo)
+        imp = (orho1 * hdif[l] * visc * dLo)[b, None] * (
+            D[4][b] + c3[b, None] * D[3][b] + c2[b, None] * D[2][b] + c1[b, None] * D[1][b]
+            + c0[b, None] * D[0][b])
+        A = np.zeros((N, N))
+        A[b] = old + wimp_lin0 * imp
+        A[0], A[N - 1] = D[0][0], D[0][N - 1]
+        A[1] = (D[2][0] - (2.0 * or1[0] + beta[0]) * D[1][0]) if ktopv == 1 else D[1][0]
+        A[N - 2] = ((D[2][N - 1] - (2.0 * or1[N - 1] + beta[N - 1]) * D[1][N - 1])
+                    if kbotv == 1 else D[1][N - 1])
+        fr = 1.0 / np.abs(A).max(axis=1)
+        A = fr[:, None] * A
+        fc = 1.0 / np.abs(A).max(axis=0)
+        M[l] = fc[:, None] * np.linalg.inv(A * fc[None, :]) * fr[None, :]
+    return M
+
+
+def p0_inverse(sch, beta):
+    """Inverse of the l = 0 pressure matrix on finite-difference grid values
+    (magic_torch/update_wp.py:80-165): rows 1.. dp/dr - beta p with the last row the
+    first-order backward difference (entries beyond the band of half-width
+    fd_order/2 dropped), row 0 p = 0."""
+    N = sch.n_r
+    A = np.zeros((N, N))
+    A[1:] = sch.D1m[1:] - beta[1:, None] * np.eye(N)[1:]
+    delr = sch.r[N - 1] - sch.r[N - 2]
+    A[N - 1, N - 1] = 1.0 / delr - beta[N - 1]
+    A[N - 1, N - 2] = -1.0 / delr
+    A[N - 1, :N - 1 - sch.fd_order // 2] = 0.0
+    A[0] = np.eye(N)[0]
+    return np.linalg.inv(A)
+
+
+def update_poloidal_dc(plan, sch, lop, P0, w, dw, ddw, p, ta, weights, s, prof, hdif, BuoFac,
+                       xi=None, ChemFac=0.0):
+    """One double-curl poloidal step in place (mt_update_poloidal): w, dw, ddw outputs,
+    p (row (0, 0) written: the l = 0 pressure), ta: dict old, impl, expl0, expl1;
+    s / xi: this step's entropy / composition; prof: or1, or2, beta, dbeta, ddbeta,
+    visc, dLvisc, ddLvisc, orho1, rgrav, rho0 over n_r; P0: RadialOp of p0_inverse."""
+    n_r = w.shape[1]
+    arrs = [w, dw, ddw, ta["old"], ta["impl"], ta["expl0"], ta["expl1"], p, s]
+    for a in arrs + ([xi] if xi is not None else []):
+        if a.shape != w.shape or a.dtype != torch.complex128 or not a.is_contiguous():
+            raise ValueError("fields and time arrays must be contiguous (lm_max, n_r) complex128")
+    w_old, wimp_lin0, w_impl, w_e0, w_e1 = weights
+    c3, c2n, c1n, c1d, c0n = _w_coefficient_profiles(prof)
+    prof_arrays = [np.asarray(hdif, dtype=np.float64)] + [prof[k] for k in (
+        "or2", "orho1", "beta", "visc", "rgrav", "rho0")] + [c3, c2n, c1n, c1d, c0n]
+    dev = [torch.as_tensor(v, dtype=torch.float64, device=w.device).contiguous()
+           for v in prof_arrays]
+    u = _lib.PoloidalUpdate(*[a.data_ptr() for a in arrs],
+                            xi.data_ptr() if xi is not None else None, n_r,
+                            w_old, w_impl, w_e0, w_e1, wimp_lin0, float(BuoFac), float(ChemFac),
+                            *[d.data_ptr() for d in dev])
+    st = C.c_void_p(torch.cuda.current_stream(w.device).cuda_stream)
+    check(_lib.lib().mt_update_poloidal(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h,
+                                        P0._h, st))
+
+
 def entropy_coefficients(l_max, opr, hdif, kappa, d1c, or2):
     """Coefficients of mt_update_field for entropy / composition
     (magic_torch/update_s.py:262-270): old = s, impl = opr hdif kappa

@@ -296,7 +296,8 @@ class RadialScheme:
         self.n_cheb = n_r if (n_cheb is None or not self.chebyshev) else min(n_cheb, n_r)
         if not self.chebyshev:
             self.r = fd_grid(n_r, radratio, fd_stretch, fd_ratio)
-            mats = fd_matrices(self.r, fd_order, fd_order_bound)[:3]
+            allm = fd_matrices(self.r, fd_order, fd_order_bound)
+            mats, self.D4m = allm[:3], allm[3]
             # grid-point unknowns: rMat = I, rnorm = boundary_fac = 1
             # (magic_torch/finite_differences.py:296-300)
             self.rMat, self.drMat, self.d2rMat = np.eye(n_r), mats[0], mats[1]

@@ -209,3 +209,108 @@ def update_b(g, mats, prof, stb, stj, weights, opm, hdif, D1, D2, chebyshev, n_c
         res.append(dict(x=x, dx=dx, d2x=d2x, impl=impl, old=dLh * or2 * x,
                         expl1=st["expl0"].copy()))
     return res
+
+
+def _w_coefficients(prof, dL):
+    """c3, c2, c1, c0 of the double-curl diffusion operator
+    (magic_torch/update_w_doublecurl.py:137-190, 340-366)."""
+    p = prof
+    dLv, ddLv, b, db, ddb, or1, or2 = (p["dLvisc"], p["ddLvisc"], p["beta"], p["dbeta"],
+                                       p["ddbeta"], p["or1"], p["or2"])
+    c3 = 2.0 * (dLv - b)
+    c2 = ddLv - 2.0 * db + dLv ** 2 + b ** 2 - 3.0 * dLv * b - 2.0 * or1 * (dLv + b) \
+        - 2.0 * dL * or2
+    c1 = (-ddb - db * (2.0 * dLv - b + 2.0 * or1) - ddLv * (b + 2.0 * or1)
+          + b ** 2 * (dLv + 2.0 * or1) - b * (dLv ** 2 - 2.0 * or2)
+          - 2.0 * dLv * or1 * (dLv - or1) + 2.0 * (2.0 * or1 + b - dLv) * dL * or2)
+    c0 = dL * or2 * (2.0 * db + ddLv + dLv ** 2 - (2.0 / 3.0) * b ** 2 + dLv * b
+                     + 2.0 * or1 * (2.0 * dLv - b - 3.0 * or1) + dL * or2)
+    return c3, c2, c1, c0
+
+
+def w_matrix(l, mats, prof, wimp_lin0, hdif_l, ktopv, kbotv):
+    """Double-curl poloidal LHS of degree l >= 1 on finite-difference grid values
+    (magic_torch/update_w_doublecurl.py:137-260): rows 2..N-3
+    -l(l+1)/r^2/rho (d2 - beta d - l(l+1)/r^2) + wimp hdif visc l(l+1)/r^2/rho
+    (d4 + c3 d3 + c2 d2 + c1 d + c0); rows 0, N-1: w = 0; rows 1, N-2: dw = 0
+    (no-slip) or d2w - (2/r + beta) dw = 0 (stress-free) at the boundary."""
+    rMat, drMat, d2rMat, d3rMat, d4rMat = mats
+    N = rMat.shape[0]
+    p = prof
+    dL = float(l * (l + 1))
+    b = slice(2, N - 2)
+    c3, c2, c1, c0 = _w_coefficients(prof, dL)
+    dat = np.zeros((N, N))
+    old = (-dL * p["or2"] * p["orho1"])[b, None] * (
+        d2rMat[b] - p["beta"][b, None] * drMat[b] - dL * p["or2"][b, None] * rMat[b])
+    imp = (p["orho1"] * hdif_l * p["visc"] * dL * p["or2"])[b, None] * (
+        d4rMat[b] + c3[b, None] * d3rMat[b] + c2[b, None] * d2rMat[b] + c1[b, None] * drMat[b]
+        + c0[b, None] * rMat[b])
+    dat[b] = old + wimp_lin0 * imp
+    dat[0] = rMat[0]
+    dat[N - 1] = rMat[N - 1]
+    dat[1] = (d2rMat[0] - (2.0 * p["or1"][0] + p["beta"][0]) * drMat[0]) if ktopv == 1 else drMat[0]
+    dat[N - 2] = ((d2rMat[N - 1] - (2.0 * p["or1"][N - 1] + p["beta"][N - 1]) * drMat[N - 1])
+                  if kbotv == 1 else drMat[N - 1])
+    return dat
+
+
+def p0_matrix(mats, prof, r, fd_order):
+    """l = 0 pressure matrix on finite-difference grid values
+    (magic_torch/update_wp.py:80-140): rows 1.. dp/dr - beta p, last row the
+    first-order backward difference (entries outside the band of width
+    fd_order/2 dropped), row 0 the Dirichlet condition p = 0."""
+    rMat, drMat = mats[0], mats[1]
+    N = rMat.shape[0]
+    dat = np.zeros((N, N))
+    dat[1:] = drMat[1:] - prof["beta"][1:, None] * rMat[1:]
+    delr = r[N - 1] - r[N - 2]
+    dat[N - 1, N - 1] = 1.0 / delr - prof["beta"][N - 1]
+    dat[N - 1, N - 2] = -1.0 / delr
+    dat[N - 1, :N - 1 - fd_order // 2] = 0.0
+    dat[0] = rMat[0]
+    return dat
+
+
+def update_w(g, mats, prof, st, weights, hdif, D1, D2, s_new, BuoFac, r, fd_order,
+             ktopv, kbotv):
+    """One double-curl updateW on finite differences (magic_torch/update_w_doublecurl.py:
+    393-483): CNAB2 right-hand side plus wimp BuoFac l(l+1)/r^2 g s on rows 2..N-3,
+    four boundary rows zero, degree 0 zero, per-l solves, m = 0 real; dw, ddw,
+    dddw = D1 ddw, ddddw = D2 ddw; the l = 0 pressure from rho0 BuoFac g s00 +
+    Re expl0; old and impl as get_w_old / get_w_impl."""
+    wimp, wimp_lin, wexp = weights
+    N = st["old"].shape[1]
+    p = prof
+    dLh = (g["lm2l"] * (g["lm2l"] + 1.0))[:, None]
+    rhs = wimp[0] * st["old"] + wimp_lin[1] * st["impl"] + wexp[0] * st["expl0"] \
+        + wexp[1] * st["expl1"]
+    rhs[:, 2:N - 2] += wimp_lin[0] * BuoFac * dLh * (p["or2"] * p["rgrav"])[None, 2:N - 2] \
+        * s_new[:, 2:N - 2]
+    rhs[:, [0, 1, N - 2, N - 1]] = 0.0
+    x = np.zeros_like(rhs)
+    for l in range(1, g["l_max"] + 1):
+        rows = np.nonzero(g["lm2l"] == l)[0]
+        dat = w_matrix(l, mats, prof, wimp_lin[0], hdif[l], ktopv, kbotv)
+        fr = 1.0 / np.abs(dat).max(axis=1)  # row, then column scaling as the reference
+        dat = fr[:, None] * dat
+        fc = 1.0 / np.abs(dat).max(axis=0)
+        y = np.linalg.solve(dat * fc[None, :], (fr[None, :] * rhs[rows]).T).T
+        x[rows] = fc[None, :] * y
+    m0 = g["lm2m"] == 0
+    x[m0] = x[m0].real
+    dw, ddw = x @ D1.T, x @ D2.T
+    dddw, ddddw = ddw @ D1.T, ddw @ D2.T
+    p0_rhs = np.zeros(N)
+    p0_rhs[1:] = p["rho0"][1:] * BuoFac * p["rgrav"][1:] * s_new[0, 1:].real + st["expl0"][0, 1:].real
+    p0 = np.linalg.solve(p0_matrix(mats, prof, r, fd_order), p0_rhs)
+    or2 = p["or2"][None, :]
+    old = dLh * or2 * (-p["orho1"][None, :] * (ddw - p["beta"][None, :] * dw - dLh * or2 * x))
+    old[:, [0, -1]] = 0.0
+    c3, c2, c1, c0 = (np.broadcast_to(c, x.shape) for c in _w_coefficients(
+        {k: v[None, :] if np.ndim(v) else v for k, v in prof.items()}, dLh))
+    dif = -hdif[g["lm2l"]][:, None] * dLh * or2 * p["visc"][None, :] * p["orho1"][None, :] * (
+        ddddw + c3 * dddw + c2 * ddw + c1 * dw + c0 * x)
+    impl = dif + BuoFac * dLh * or2 * p["rgrav"][None, :] * s_new
+    impl[:, [0, -1]] = 0.0
+    return dict(x=x, dx=dw, d2x=ddw, impl=impl, old=old, expl1=st["expl0"].copy(), p0=p0)

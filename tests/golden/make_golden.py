@@ -298,6 +298,27 @@ def worker_td(name, ref):
         out.update({f + "_new": n(x), "d" + f + "_new": n(dx), "dd" + f + "_new": n(d2x),
                     f + "_impl_new": n(ta_.impl[:, :, 0]), f + "_old_new": n(ta_.old[:, :, 0]),
                     f + "_expl1_new": n(ta_.expl[:, :, 1])})
+    if params.l_double_curl:
+        # one double-curl poloidal update with the l = 0 pressure
+        # (magic_torch/update_w_doublecurl.py:67-483, update_wp.py:80-194)
+        from magic_torch import update_w_doublecurl as uw, update_wp as uwp
+        uw.build_w_matrices(tscheme.wimp_lin[0].item())
+        uwp.build_p0_matrix()
+        tw = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+        for k in ("old", "impl", "expl0", "expl1"):
+            v = _spec(rng, lm, l_of, N)
+            (tw.old if k == "old" else tw.impl if k == "impl" else tw.expl)[
+                :, :, 1 if k == "expl1" else 0] = t(v)
+            out["w_" + k] = v
+        out.update(rgrav=n(rf2.rgrav), rho0=n(rf2.rho0), ddbeta=n(rf2.ddbeta),
+                   ddLvisc=n(rf2.ddLvisc), BuoFac=float(pc.BuoFac), ChemFac=float(pc.ChemFac),
+                   d3rMat=n(rs.d3rMat), d4rMat=n(rs.d4rMat))
+        w_new, dw_new, ddw_new, p_new, dp_new = (torch.zeros(lm, N, dtype=torch.complex128)
+                                                 for _ in range(5))
+        uw.updateW(s_new.clone(), w_new, dw_new, ddw_new, tw, p_new, dp_new, tscheme)
+        out.update(w_new=n(w_new), dw_new=n(dw_new), ddw_new=n(ddw_new), p0_new=n(p_new[0]),
+                   w_impl_new=n(tw.impl[:, :, 0]), w_old_new=n(tw.old[:, :, 0]),
+                   w_expl1_new=n(tw.expl[:, :, 1]))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

@@ -241,3 +241,76 @@ def test_update_magnetic_vs_oracle(scheme, l_max, n_r):
                        ("old", ta["old"]), ("expl1", ta["expl1"])):
             e = rel_err(npy(got), o[k])
             assert e < (TOL_IMPL if k in ("impl", "d2x") else TOL), (scheme, f, k, e)
+
+
+WPROF = ("or1", "or2", "beta", "dbeta", "ddbeta", "visc", "dLvisc", "ddLvisc", "orho1", "rgrav",
+         "rho0")
+
+
+def _run_poloidal(p, sch, st, s_new, prof, hdif, BuoFac, w):
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialOp
+
+    lop = I.LOp(I.poloidal_dc_solve_operators(sch, p.l_max, w[1], hdif, prof))
+    P0 = RadialOp(I.p0_inverse(sch, prof["beta"]))
+    ta = {k: cu(v) for k, v in st.items()}
+    x, dx, d2x, pr = (torch.zeros_like(ta["old"]) for _ in range(4))
+    I.update_poloidal_dc(p, sch, lop, P0, x, dx, d2x, pr, ta, w, cu(s_new), prof, hdif, BuoFac)
+    return dict(x=x, dx=dx, d2x=d2x, impl=ta["impl"], old=ta["old"], expl1=ta["expl1"],
+                p0=pr[0].real)
+
+
+def test_update_poloidal_matches_reference():
+    from types import SimpleNamespace
+
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialOp
+
+    z = load_golden("td_fd_anel")
+    p = Plan(int(z["l_max"]), int(z["minc"]))
+    sch = SimpleNamespace(n_r=int(z["n_r_max"]), chebyshev=False, D1m=z["drMat"],
+                          D2m=z["d2rMat"], D3m=z["d3rMat"], D4m=z["d4rMat"], r=z["r"],
+                          fd_order=int(z["fd_order"]), D1=RadialOp(z["D1"]), D2=RadialOp(z["D2"]))
+    prof = {k: z[k] for k in WPROF}
+    st = {k: z["w_" + k] for k in ("old", "impl", "expl0", "expl1")}
+    o = _run_poloidal(p, sch, st, z["s_new"], prof, z["hdif_V"], float(z["BuoFac"]),
+                      I.cnab2_weights(1e-4, 1.3e-4))
+    errs = {k: rel_err(npy(o[k]), z[ref]) for k, ref in (
+        ("x", "w_new"), ("dx", "dw_new"), ("d2x", "ddw_new"), ("impl", "w_impl_new"),
+        ("old", "w_old_new"), ("expl1", "w_expl1_new"), ("p0", "p0_new"))}
+    print({k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        assert v < TOL, (k, v)
+
+
+def test_update_poloidal_vs_oracle():
+    """l_max = 255, 97 fourth-order finite-difference levels, anelastic-like profiles."""
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialScheme
+
+    l_max, n_r = 255, 97
+    p = Plan(l_max, 1)
+    sch = RadialScheme(n_r, "FD", fd_order=4)
+    r = sch.r
+    prof = dict(or1=1.0 / r, or2=1.0 / r ** 2, beta=-0.3 / r, dbeta=0.3 / r ** 2,
+                ddbeta=-0.6 / r ** 3, visc=np.ones(n_r), dLvisc=np.zeros(n_r),
+                ddLvisc=np.zeros(n_r), orho1=np.exp(-0.3 * (r[0] - r)), rgrav=r / r[0],
+                rho0=np.exp(0.3 * (r[0] - r)))
+    hdif, BuoFac = np.ones(l_max + 1), 1e3
+    rng = np.random.default_rng(3)
+    amp = (p.lm2l + 1.0)[:, None] ** -1.5
+    spec = lambda: (rng.standard_normal((p.lm_max, n_r))
+                    + 1j * rng.standard_normal((p.lm_max, n_r))) * amp
+    st = {k: spec() for k in ("old", "impl", "expl0", "expl1")}
+    s_new = spec()
+    w = I.cnab2_weights(1e-4, 1.2e-4)
+    o = _run_poloidal(p, sch, st, s_new, prof, hdif, BuoFac, w)
+    g = dict(lm2l=p.lm2l, lm2m=p.lm2m, l_max=l_max)
+    mats = (np.eye(n_r), sch.D1m, sch.D2m, sch.D3m, sch.D4m)
+    ref = oi.update_w(g, mats, prof, st, ([w[0]], [w[1], w[2]], [w[3], w[4]]), hdif, sch.D1m,
+                      sch.D2m, s_new, BuoFac, r, 4, 2, 2)
+    for k in ("x", "dx", "d2x", "impl", "old", "expl1", "p0"):
+        e = rel_err(npy(o[k]), ref[k])
+        assert e < (TOL_IMPL if k in ("impl", "old", "d2x") else TOL), (k, e)

@@ -311,3 +311,22 @@ def test_update_b_oracle(name):
                        ("impl", f + "_impl_new"), ("old", f + "_old_new"),
                        ("expl1", f + "_expl1_new")):
             assert rel_err(o[k], z[ref]) < 1e-14, (f, k)
+
+
+def test_update_w_oracle():
+    """The double-curl poloidal update with the l = 0 pressure restated in numpy
+    against the reference's updateW (FD4 anelastic, no-slip)."""
+    from oracle import implicit as oi
+
+    z = load_golden("td_fd_anel")
+    g = dict(lm2l=z["lm2l"], lm2m=z["lm2m"], l_max=int(z["l_max"]))
+    prof = {k: z[k] for k in ("or1", "or2", "beta", "dbeta", "ddbeta", "visc", "dLvisc",
+                              "ddLvisc", "orho1", "rgrav", "rho0")}
+    mats = (z["rMat"], z["drMat"], z["d2rMat"], z["d3rMat"], z["d4rMat"])
+    st = {k: z["w_" + k].copy() for k in ("old", "impl", "expl0", "expl1")}
+    o = oi.update_w(g, mats, prof, st, (z["wimp"], z["wimp_lin"], z["wexp"]), z["hdif_V"],
+                    z["D1"], z["D2"], z["s_new"], float(z["BuoFac"]), z["r"], int(z["fd_order"]),
+                    int(z["ktopv"]), int(z["kbotv"]))
+    for k, ref in (("x", "w_new"), ("dx", "dw_new"), ("d2x", "ddw_new"), ("impl", "w_impl_new"),
+                   ("old", "w_old_new"), ("expl1", "w_expl1_new"), ("p0", "p0_new")):
+        assert rel_err(o[k], z[ref]) < 1e-13, k
