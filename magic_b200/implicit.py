@@ -223,19 +223,20 @@ def p0_inverse(sch, beta):
 
 
 def update_poloidal_dc(plan, sch, lop, P0, w, dw, ddw, p, ta, weights, s, prof, hdif, BuoFac,
-                       xi=None, ChemFac=0.0):
+                       xi=None, ChemFac=0.0, wcoef=None):
     """One double-curl poloidal step in place (mt_update_poloidal): w, dw, ddw outputs,
     p (row (0, 0) written: the l = 0 pressure), ta: dict old, impl, expl0, expl1;
     s / xi: this step's entropy / composition; prof: or1, or2, beta, dbeta, ddbeta,
-    visc, dLvisc, ddLvisc, orho1, rgrav, rho0 over n_r; P0: RadialOp of p0_inverse."""
+    visc, dLvisc, ddLvisc, orho1, rgrav, rho0 over n_r (numpy or device arrays);
+    P0: RadialOp of p0_inverse; wcoef: precomputed _w_coefficient_profiles(prof)."""
     n_r = w.shape[1]
     arrs = [w, dw, ddw, ta["old"], ta["impl"], ta["expl0"], ta["expl1"], p, s]
     for a in arrs + ([xi] if xi is not None else []):
         if a.shape != w.shape or a.dtype != torch.complex128 or not a.is_contiguous():
             raise ValueError("fields and time arrays must be contiguous (lm_max, n_r) complex128")
     w_old, wimp_lin0, w_impl, w_e0, w_e1 = weights
-    c3, c2n, c1n, c1d, c0n = _w_coefficient_profiles(prof)
-    prof_arrays = [np.asarray(hdif, dtype=np.float64)] + [prof[k] for k in (
+    c3, c2n, c1n, c1d, c0n = wcoef if wcoef is not None else _w_coefficient_profiles(prof)
+    prof_arrays = [hdif] + [prof[k] for k in (
         "or2", "orho1", "beta", "visc", "rgrav", "rho0")] + [c3, c2n, c1n, c1d, c0n]
     dev = [torch.as_tensor(v, dtype=torch.float64, device=w.device).contiguous()
            for v in prof_arrays]

@@ -1,0 +1,206 @@
+"""One CNAB2 time step of the Boussinesq dynamo on the GPU.
+
+The reference's one_step (magic_torch/step_time.py:1574-1640) with its
+radial_loop (:931-1213) and lm_loop (:1478-1527), for the finite-difference
+radial scheme with the double-curl poloidal form, an insulating inner core
+and mantle, Boussinesq profiles, magnetic field on:
+
+    radial loop  mt_nl_bouss (input assembly, synthesis, phi FFT, get_nl
+                 products, Courant, analysis) then mt_get_td (explicit terms
+                 with finish_exp), written straight into each field's expl0;
+    lm loop      entropy (mt_update_field), toroidal velocity
+                 (mt_update_field), double-curl poloidal velocity and l = 0
+                 pressure (mt_update_poloidal), magnetic b and j
+                 (mt_update_field), in the reference's order S, Z, W, B.
+
+The time step is held fixed (the solve operators are built once for it); the
+Courant limits of every step are returned for the caller's dt control.
+Every launch is stream-ordered on the current stream; nothing synchronises.
+"""
+
+import math
+
+import numpy as np
+import torch
+
+from . import implicit as I
+from .plan import Plan
+from .radial import RadialOp, RadialScheme
+
+_CD = torch.complex128
+
+
+class BoussinesqStep:
+    def __init__(self, l_max, n_r, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
+                 precision="split", radratio=0.35, fd_order=4, fd_order_bound=2, ktopv=2,
+                 kbotv=2, device=None):
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        dev = self.device
+        self.plan = Plan(l_max, 1, precision=precision, device=dev)
+        self.sch = RadialScheme(n_r, "FD", radratio, fd_order=fd_order,
+                                fd_order_bound=fd_order_bound, device=dev)
+        self.l_max, self.n_r, self.lm_max = l_max, n_r, self.plan.lm_max
+        # physical prefactors (magic_torch/pre_calculations.py:13-41)
+        self.CorFac, self.LFfac = 1.0 / ek, 1.0 / (ek * prmag)
+        self.BuoFac, self.opr, self.opm = ra / pr, 1.0 / pr, 1.0 / prmag
+        r = self.sch.r
+        r_cmb = 1.0 / (1.0 - radratio)
+        dr = np.abs(np.diff(r))
+        delxr2 = np.empty(n_r)
+        delxr2[0], delxr2[-1] = dr[0] ** 2, dr[-1] ** 2
+        delxr2[1:-1] = np.minimum(dr[:-1], dr[1:]) ** 2
+        zeros, ones = np.zeros(n_r), np.ones(n_r)
+        hp = dict(r=r, or1=1.0 / r, or2=1.0 / r ** 2, or4=1.0 / r ** 4, orho1=ones,
+                  orho2=ones, beta=zeros, dbeta=zeros, ddbeta=zeros, visc=ones, dLvisc=zeros,
+                  ddLvisc=zeros, kappa=ones, dLkappa=zeros, dLtemp0=zeros, lambda_=ones,
+                  dLlambda=zeros, rgrav=r / r_cmb, rho0=ones, delxr2=delxr2,
+                  delxh2=r ** 2 / float(l_max * (l_max + 1)))
+        self.hprof = hp
+        t = lambda x: torch.as_tensor(np.asarray(x, dtype=np.float64), device=dev).contiguous()
+        self.prof = {k: t(v) for k, v in hp.items()}
+        hdif = np.ones(l_max + 1)
+        self.hdif = t(hdif)
+        # CNAB2 with a fixed step: solve operators for it, coefficients uploaded once
+        self.weights = I.cnab2_weights(dt, dt)
+        wl0 = self.weights[1]
+        d1c = hp["beta"] + hp["dLtemp0"] + 2.0 * hp["or1"] + hp["dLkappa"]
+        self.ops = dict(
+            s=I.LOp(I.scalar_solve_operators(self.sch, l_max, wl0, self.opr, hdif, hp["kappa"],
+                                             d1c, hp["or2"]), device=dev),
+            z=I.LOp(I.toroidal_solve_operators(self.sch, l_max, wl0, hdif, hp["visc"],
+                                               hp["beta"], hp["dbeta"], hp["dLvisc"], hp["or1"],
+                                               hp["or2"], ktopv, kbotv), device=dev),
+            w=I.LOp(I.poloidal_dc_solve_operators(self.sch, l_max, wl0, hdif, hp, ktopv, kbotv),
+                    device=dev))
+        Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif, hp["lambda_"],
+                                            hp["dLlambda"], hp["or1"], hp["or2"])
+        self.ops["b"], self.ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
+        self.P0 = RadialOp(I.p0_inverse(self.sch, hp["beta"]), device=dev)
+        dev_coef = lambda c: {k: (t(v) if v is not None else None) for k, v in c.items()}
+        self.coef = dict(s=dev_coef(I.entropy_coefficients(l_max, self.opr, hdif, hp["kappa"], d1c,
+                                                           hp["or2"])),
+                         z=dev_coef(I.toroidal_coefficients(l_max, hdif, hp["visc"], hp["beta"],
+                                                            hp["dbeta"], hp["dLvisc"], hp["or1"],
+                                                            hp["or2"])))
+        cb, cj = I.magnetic_coefficients(l_max, self.opm, hdif, hp["lambda_"], hp["dLlambda"],
+                                         hp["or2"])
+        self.coef["b"], self.coef["j"] = dev_coef(cb), dev_coef(cj)
+        self.wprof = {k: self.prof[k] for k in ("or1", "or2", "beta", "dbeta", "ddbeta", "visc",
+                                                "dLvisc", "ddLvisc", "orho1", "rgrav", "rho0")}
+        self.wcoef = tuple(t(c) for c in I._w_coefficient_profiles(hp))
+        # state: fields, their derivatives and the time arrays of each equation
+        z = lambda: torch.zeros(self.lm_max, n_r, dtype=_CD, device=dev)
+        self.f = {k: z() for k in ("w", "dw", "ddw", "z", "dz", "s", "ds", "b", "db", "ddb", "aj",
+                                   "dj", "ddj", "p")}
+        self.ta = {e: {k: z() for k in ("old", "impl", "expl0", "expl1")}
+                   for e in ("s", "z", "w", "b", "j")}
+        self.nl_out = {k: z() for k in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt",
+                                        "VxBp")}
+        self.work = torch.empty(self.plan.nl_bouss_workspace(n_r, True, False), dtype=torch.uint8,
+                                device=dev)
+        self.bots = torch.zeros(self.lm_max, dtype=_CD, device=dev)
+        self.bots[0] = math.sqrt(4.0 * math.pi)  # fixed entropy at the inner boundary, l = m = 0
+
+    def init_random(self, seed=0, amp=1e-4):
+        """Seeded random fields |c_lm| ~ amp (l+1)^-2 on the interior levels (m = 0
+        real), their radial derivatives, and the old / implicit time arrays built from
+        them as the reference's setup_initial_state does (step_time.py:398-600: old =
+        s, l(l+1)/r^2 z, the double-curl w term, l(l+1)/r^2 b and j; impl = each
+        equation's implicit operator applied to the fields)."""
+        from .radial import get_ddr
+
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        l = torch.as_tensor(self.plan.lm2l, dtype=torch.float64)
+        m0 = torch.as_tensor(self.plan.lm2m == 0)
+        for k in ("w", "z", "s", "b", "aj"):
+            c = torch.randn(self.lm_max, self.n_r, dtype=_CD, generator=g) * amp
+            c *= ((l + 1.0) ** -2)[:, None]
+            c[m0] = c[m0].real.to(_CD)
+            c[:, 0] = 0.0
+            c[:, -1] = 0.0
+            self.f[k].copy_(c.to(self.device))
+        f, P, D1, D2 = self.f, self.prof, self.sch.D1, self.sch.D2
+        second = {}
+        for k, d1, d2 in (("w", "dw", "ddw"), ("z", "dz", None), ("s", "ds", None),
+                          ("b", "db", "ddb"), ("aj", "dj", "ddj")):
+            a1, a2 = get_ddr(f[k], D1, D2)
+            f[d1].copy_(a1)
+            second[k] = a2
+            if d2:
+                f[d2].copy_(a2)
+        dL = (l * (l + 1.0)).to(self.device)[:, None]
+        row = lambda x: x[None, :]
+        hd = self.hdif[self.plan_l()][:, None]
+
+        def generic(key, x, dx, d2x):
+            c = self.coef[key]
+            so = (c["so_l"][self.plan_l()][:, None] * row(c["so_r"])) if c["so_l"] is not None \
+                else 1.0
+            ic = (row(c["ic_r"]) if c["ic_r"] is not None else 0.0) \
+                + c["ic_l"][self.plan_l()][:, None] * row(c["ic_r2"])
+            impl = c["ia_l"][self.plan_l()][:, None] * row(c["ia_r"]) * (
+                d2x + row(c["ib_r"]) * dx - ic * x)
+            self.ta[key]["old"].copy_(so * x)
+            self.ta[key]["impl"].copy_(impl)
+
+        generic("s", f["s"], f["ds"], second["s"])
+        generic("z", f["z"], f["dz"], second["z"])
+        generic("b", f["b"], f["db"], second["b"])
+        generic("j", f["aj"], f["dj"], second["aj"])
+        # double-curl poloidal terms (update_w_doublecurl.py:310-390)
+        dddw, ddddw = get_ddr(f["ddw"], D1, D2)
+        or2, orho1, beta = row(P["or2"]), row(P["orho1"]), row(P["beta"])
+        old = dL * or2 * (-orho1 * (f["ddw"] - beta * f["dw"] - dL * or2 * f["w"]))
+        c3, c2n, c1n, c1d, c0n = (row(c) for c in self.wcoef)
+        dLo = dL * or2
+        dif = -hd * dLo * row(P["visc"]) * orho1 * (
+            ddddw + c3 * dddw + (c2n - 2.0 * dLo) * f["ddw"] + (c1n + dL * c1d) * f["dw"]
+            + dLo * (c0n + dLo) * f["w"])
+        impl = dif + self.BuoFac * dLo * row(P["rgrav"]) * f["s"]
+        for x in (old, impl):
+            x[:, 0] = 0.0
+            x[:, -1] = 0.0
+        self.ta["w"]["old"].copy_(old)
+        self.ta["w"]["impl"].copy_(impl)
+
+    def plan_l(self):
+        if not hasattr(self, "_l_dev"):
+            self._l_dev = torch.as_tensor(self.plan.lm2l, dtype=torch.long, device=self.device)
+        return self._l_dev
+
+    def radial_loop(self):
+        """Explicit stage: nonlinear products and Courant limits, then the explicit
+        time derivatives into each equation's expl0 (step_time.py:931-1213)."""
+        f = self.f
+        fields = {k: f[k] for k in ("w", "dw", "ddw", "z", "dz", "s", "b", "db", "ddb", "aj",
+                                    "dj")}
+        out, dtr, dth = self.plan.nl_bouss(fields, self.prof, self.LFfac, 2.5, 1.0, self.opm,
+                                           l_mag=True, out=self.nl_out, work=self.work)
+        ins = dict(out, w=f["w"], dw=f["dw"], ddw=f["ddw"], z=f["z"], dz=f["dz"])
+        td_out = dict(dwdt=self.ta["w"]["expl0"], dzdt=self.ta["z"]["expl0"],
+                      dsdt=self.ta["s"]["expl0"], dbdt=self.ta["b"]["expl0"],
+                      djdt=self.ta["j"]["expl0"])
+        self.plan.get_td(ins, self.prof, self.CorFac, self.sch.D1, l_double_curl=True,
+                         l_heat=True, l_mag=True, out=td_out)
+        return dtr, dth
+
+    def lm_loop(self):
+        """Implicit solves S, Z, W, B (step_time.py:1478-1527)."""
+        f, ta, w = self.f, self.ta, self.weights
+        I.update_field(self.plan, self.sch, self.ops["s"], f["s"], f["ds"], ta["s"], w,
+                       self.coef["s"], bot=self.bots)
+        I.update_field(self.plan, self.sch, self.ops["z"], f["z"], f["dz"], ta["z"], w,
+                       self.coef["z"])
+        I.update_poloidal_dc(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"],
+                             f["ddw"], f["p"], ta["w"], w, f["s"], self.wprof, self.hdif,
+                             self.BuoFac, wcoef=self.wcoef)
+        I.update_field(self.plan, self.sch, self.ops["b"], f["b"], f["db"], ta["b"], w,
+                       self.coef["b"], d2x=f["ddb"])
+        I.update_field(self.plan, self.sch, self.ops["j"], f["aj"], f["dj"], ta["j"], w,
+                       self.coef["j"], d2x=f["ddj"])
+
+    def step(self):
+        dtr, dth = self.radial_loop()
+        self.lm_loop()
+        return dtr, dth
