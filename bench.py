@@ -380,6 +380,65 @@ def run_td(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_step(args, rank, world):
+    """Optional line: whole CNAB2 time steps of the Boussinesq MHD dynamo at
+    l_max = 255 on the 97-level fourth-order finite-difference grid (radial loop
+    with the fused nonlinear stage and the explicit terms, implicit solves of S, Z,
+    W with the l = 0 pressure, B), device-timed with the state resident; the same
+    steps with the FP64 stage beside them."""
+    from magic_b200.step import BoussinesqStep
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    res = {}
+    for prec in ("split", "fp64"):
+        st = BoussinesqStep(L_MAX, args.levels, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
+                            precision=prec, device=dev)
+        st.init_random(seed=rank, amp=1e-4)
+        for _ in range(args.warmup):
+            st.step()
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        with ClockSampler(dev) as clocks:
+            e[0].record()
+            for _ in range(args.steps):
+                st.step()
+            e[1].record()
+            torch.cuda.synchronize()
+        ms = e[0].elapsed_time(e[1]) / args.steps
+        # radial loop / implicit solves split, same work bracketed by events
+        rl, lm = 0.0, 0.0
+        for _ in range(args.steps):
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record()
+            st.radial_loop()
+            b.record()
+            st.lm_loop()
+            c.record()
+            torch.cuda.synchronize()
+            rl += a.elapsed_time(b)
+            lm += b.elapsed_time(c)
+        res[prec] = dict(ms=ms, radial_loop_ms=rl / args.steps, implicit_ms=lm / args.steps,
+                         clocks=clocks.summary())
+        del st
+        torch.cuda.empty_cache()
+    if rank == 0:
+        sp, fp = res["split"], res["fp64"]
+        print(json.dumps({
+            "metric": "IMEX steps/s @lmax=255 (whole CNAB2 step), 1 B200", "value": 1000.0 / sp["ms"],
+            "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sp["ms"], "higher_is_better": True, "dtype": "bf16x3/f32 stage, f64 rest",
+            "data": "synthetic",
+            "config": {"workload": "Boussinesq MHD dynamo step, FD4 double curl, CNAB2, dt fixed",
+                       "l_max": L_MAX, "n_theta": 384, "n_phi": 768, "n_r": args.levels,
+                       "l2": "state larger than L2"},
+            "fp64_stage_steps_per_s": 1000.0 / fp["ms"], "split_over_fp64": fp["ms"] / sp["ms"],
+            "breakdown_ms": {p: {k: res[p][k] for k in ("radial_loop_ms", "implicit_ms")}
+                             for p in res},
+            "clocks": sp["clocks"]}), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -406,10 +465,11 @@ def main():
     ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
-    ap.add_argument("--workload", default="bouss", choices=["bouss", "anel", "td"],
+    ap.add_argument("--workload", default="bouss", choices=["bouss", "anel", "td", "step"],
                     help="bouss: the headline Boussinesq MHD stage; anel: the fused anelastic "
                          "stage at l_max=383 (extra line, split precision); td: the explicit "
-                         "time-derivative terms (get_td + finish_exp, FP64, extra line)")
+                         "time-derivative terms (get_td + finish_exp, FP64, extra line); "
+                         "step: whole CNAB2 time steps, split and FP64 stage (extra line)")
     ap.add_argument("--levels", type=int, default=N_R,
                     help="radial levels (profiling runs use fewer than the 97 of the workload)")
     args = ap.parse_args()
@@ -426,6 +486,9 @@ def main():
         return
     if args.workload == "td":
         run_td(args, rank, world)
+        return
+    if args.workload == "step":
+        run_step(args, rank, world)
         return
 
     torch.cuda.set_device(local)
