@@ -15,13 +15,16 @@
 // (M_l = C T A_l^-1).  Matrices are stored transposed, MT[l][k][j], so the 32
 // lanes of a warp (32 consecutive output levels j) read consecutive values.
 //
-// k_update_field: CTA = (degree l, chunk of orders m), one warp per lm row:
+// k_update_field: CTA = (4 orders m, degree l); every thread owns output
+// levels j and works on all 4 rows, so each matrix coefficient is loaded once
+// per CTA and applied to 4 right-hand sides broadcast from shared memory:
 //   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1, rows 0 and
 //   n_r - 1 replaced by the boundary values; expl1 <- expl0 (rotation);
 //   x = M_l rhs, imaginary part dropped for m = 0; dx = D1 x, d2x = D2 x
 //   (d2x stored when requested);
 //   old <- so_l so_r x; impl <- ia_l ia_r (d2x + ib_r dx - (ic_r + ic_l ic_r2) x).
-// Rows of one l share M_l through L1 (the CTA's warps and co-resident CTAs).
+// The radial derivatives of the 4 rows share their coefficients the same way;
+// consecutive CTAs hold the same degree, so M_l is reused through L1 / L2.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -38,7 +41,45 @@ namespace mt {
 
 namespace {
 
-constexpr int kUsWarps = 8;
+constexpr int kUsRows = 4;       // orders m (rows of one degree l) per CTA
+constexpr int kUsThreads = 128;  // output levels j = thread, thread + 128, ...
+
+// acc[r] = (M_l f_r)[j] for the CTA's rows r: every coefficient M_l[j][k]
+// (transposed storage: consecutive j contiguous) is loaded once and applied
+// to all rows, whose values are broadcast from shared memory.
+__device__ __forceinline__ void solve_rows(const double* __restrict__ M, int n_r,
+                                           const double2* f, int j,
+                                           double2 (&acc)[kUsRows]) {
+#pragma unroll
+  for (int r = 0; r < kUsRows; ++r) acc[r] = double2{0.0, 0.0};
+#pragma unroll 8
+  for (int k = 0; k < n_r; ++k) {
+    const double c = __ldg(M + (int64_t)k * n_r + j);
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      const double2 v = f[r * n_r + k];
+      acc[r].x = fma(c, v.x, acc[r].x);
+      acc[r].y = fma(c, v.y, acc[r].y);
+    }
+  }
+}
+
+// acc[r] = (D f_r)[j] for a banded radial operator, coefficients shared by the rows
+__device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int n_r, int j,
+                                        double2 (&acc)[kUsRows]) {
+  const int k0 = __ldg(op.k0 + j);
+#pragma unroll
+  for (int r = 0; r < kUsRows; ++r) acc[r] = double2{0.0, 0.0};
+  for (int kk = 0; kk < op.W; ++kk) {
+    const double c = __ldg(op.vals + (int64_t)kk * op.n_r + j);
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      const double2 v = f[r * n_r + k0 + kk];
+      acc[r].x = fma(c, v.x, acc[r].x);
+      acc[r].y = fma(c, v.y, acc[r].y);
+    }
+  }
+}
 
 struct UsArgs {
   int n_r, l_max, minc, n_m;
@@ -52,52 +93,76 @@ struct UsArgs {
   OpView D1, D2;
 };
 
-__global__ void __launch_bounds__(32 * kUsWarps) k_update_field(UsArgs a) {
+// rows of this CTA (grid x = chunk of orders, y = degree l): orders
+// mc = chunk * kUsRows + r with m <= l
+__device__ __forceinline__ int cta_rows(int l, int minc, int n_m) {
+  const int mc0 = blockIdx.x * kUsRows;
+  int n = 0;
+  for (int r = 0; r < kUsRows; ++r) {
+    const int mc = mc0 + r;
+    if (mc < n_m && mc * minc <= l) n = r + 1;
+  }
+  return n;
+}
+
+__global__ void __launch_bounds__(kUsThreads) k_update_field(UsArgs a) {
   extern __shared__ double2 usbuf[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int n_r = a.n_r, l = blockIdx.x;
-  const int mc = blockIdx.y * kUsWarps + wib, m = mc * a.minc;
-  if (mc >= a.n_m || m > l) return;
-  const int64_t row = (int64_t)(a.lstart[mc] + (l - m)) * a.ld;
-  double2* rhs = usbuf + (int64_t)wib * 2 * n_r;
-  double2* x = rhs + n_r;
+  const int n_r = a.n_r, l = blockIdx.y;
+  const int nrow = cta_rows(l, a.minc, a.n_m);
+  if (nrow == 0) return;
+  const int mc0 = blockIdx.x * kUsRows;
+  double2* rhs = usbuf;                  // [kUsRows][n_r]
+  double2* x = usbuf + kUsRows * n_r;    // [kUsRows][n_r]
   const double2 zero = {0.0, 0.0};
-  const int lm = a.lstart[mc] + (l - m);
-  for (int k = lane; k < n_r; k += 32) {
-    const double2 o = a.old[row + k], im = a.impl[row + k];
-    const double2 e0 = a.expl0[row + k], e1 = a.expl1[row + k];
-    double2 v;
-    v.x = a.w_old * o.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
-    v.y = a.w_old * o.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
-    if (k == 0) v = a.top ? a.top[lm] : zero;
-    if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
-    rhs[k] = v;
-    a.expl1[row + k] = e0;
-  }
-  __syncwarp();
-  const double* M = a.mt + (int64_t)l * n_r * n_r;
-  for (int j = lane; j < n_r; j += 32) {
-    double2 acc = zero;
-    for (int k = 0; k < n_r; ++k) {
-      const double c = __ldg(M + (int64_t)k * n_r + j);
-      acc.x = fma(c, rhs[k].x, acc.x);
-      acc.y = fma(c, rhs[k].y, acc.y);
+  auto lm_of = [&](int r) { return a.lstart[mc0 + r] + (l - (mc0 + r) * a.minc); };
+  for (int r = 0; r < kUsRows; ++r) {
+    const int lm = r < nrow ? lm_of(r) : 0;
+    for (int k = threadIdx.x; k < n_r; k += kUsThreads) {
+      double2 v = zero;
+      if (r < nrow) {
+        const int64_t o = (int64_t)lm * a.ld + k;
+        const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
+        a.expl1[o] = e0;
+        v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
+        v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
+        if (k == 0) v = a.top ? a.top[lm] : zero;
+        if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
+      }
+      rhs[r * n_r + k] = v;
     }
-    if (m == 0) acc.y = 0.0;
-    x[j] = acc;
-    a.x[row + j] = acc;
   }
-  __syncwarp();
+  __syncthreads();
+  const double* M = a.mt + (int64_t)l * n_r * n_r;
+  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
+    double2 acc[kUsRows];
+    solve_rows(M, n_r, rhs, j, acc);
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      if (mc0 + r == 0) acc[r].y = 0.0;  // m = 0
+      x[r * n_r + j] = acc[r];
+      if (r < nrow) a.x[(int64_t)lm_of(r) * a.ld + j] = acc[r];
+    }
+  }
+  __syncthreads();
   const double so_l = a.so_l ? a.so_l[l] : 1.0, ia_l = a.ia_l[l], ic_l = a.ic_l[l];
-  for (int j = lane; j < n_r; j += 32) {
-    const double2 d1 = op_row(a.D1, x, j), d2 = op_row(a.D2, x, j), v = x[j];
-    a.dx[row + j] = d1;
-    if (a.d2x) a.d2x[row + j] = d2;
+  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
+    double2 d1[kUsRows], d2[kUsRows];
+    op_rows(a.D1, x, n_r, j, d1);
+    op_rows(a.D2, x, n_r, j, d2);
     const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
-    a.old[row + j] = double2{so * v.x, so * v.y};
     const double c1 = a.ib_r[j], c0 = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
     const double ia = ia_l * a.ia_r[j];
-    a.impl[row + j] = double2{ia * (d2.x + c1 * d1.x - c0 * v.x), ia * (d2.y + c1 * d1.y - c0 * v.y)};
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      if (r >= nrow) break;
+      const int64_t o = (int64_t)lm_of(r) * a.ld + j;
+      const double2 v = x[r * n_r + j];
+      a.dx[o] = d1[r];
+      if (a.d2x) a.d2x[o] = d2[r];
+      a.old[o] = double2{so * v.x, so * v.y};
+      a.impl[o] = double2{ia * (d2[r].x + c1 * d1[r].x - c0 * v.x),
+                          ia * (d2[r].y + c1 * d1[r].y - c0 * v.y)};
+    }
   }
 }
 
@@ -115,97 +180,112 @@ struct PwArgs {
 };
 
 // Double-curl poloidal update (magic_torch/update_w_doublecurl.py:393-483):
-// CTA = (degree l, chunk of orders m), one warp per lm row; the warp of
-// (l, m) = (0, 0) also solves the l = 0 pressure (update_wp.py:173-194).
-__global__ void __launch_bounds__(32 * kUsWarps) k_update_poloidal(PwArgs a) {
+// CTA = (chunk of kUsRows orders m, degree l); the CTA holding (l, m) = (0, 0)
+// also solves the l = 0 pressure (update_wp.py:173-194).
+__global__ void __launch_bounds__(kUsThreads) k_update_poloidal(PwArgs a) {
   extern __shared__ double2 pwbuf[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int n_r = a.n_r, l = blockIdx.x;
-  const int mc = blockIdx.y * kUsWarps + wib, m = mc * a.minc;
-  if (mc >= a.n_m || m > l) return;
-  const int lm = a.lstart[mc] + (l - m);
-  const int64_t row = (int64_t)lm * a.ld;
-  double2* rhs = pwbuf + (int64_t)wib * 3 * n_r;
-  double2* x = rhs + n_r;
-  double2* dd = x + n_r;
+  const int n_r = a.n_r, l = blockIdx.y;
+  const int nrow = cta_rows(l, a.minc, a.n_m);
+  if (nrow == 0) return;
+  const int mc0 = blockIdx.x * kUsRows;
+  double2* rhs = pwbuf;
+  double2* x = pwbuf + kUsRows * n_r;
+  double2* dd = pwbuf + 2 * kUsRows * n_r;
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
-  for (int k = lane; k < n_r; k += 32) {
-    const double2 o = a.old[row + k], im = a.impl[row + k];
-    const double2 e0 = a.expl0[row + k], e1 = a.expl1[row + k];
-    double2 v;
-    v.x = a.w_old * o.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
-    v.y = a.w_old * o.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
-    const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
-    const double2 sv = a.s[row + k];
-    v.x += gb * a.BuoFac * sv.x;
-    v.y += gb * a.BuoFac * sv.y;
-    if (a.xi) {
-      const double2 xv = a.xi[row + k];
-      v.x += gb * a.ChemFac * xv.x;
-      v.y += gb * a.ChemFac * xv.y;
+  auto lm_of = [&](int r) { return a.lstart[mc0 + r] + (l - (mc0 + r) * a.minc); };
+  for (int r = 0; r < kUsRows; ++r) {
+    const int64_t row = r < nrow ? (int64_t)lm_of(r) * a.ld : 0;
+    for (int k = threadIdx.x; k < n_r; k += kUsThreads) {
+      double2 v = zero;
+      if (r < nrow) {
+        const int64_t o = row + k;
+        const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
+        a.expl1[o] = e0;
+        v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
+        v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
+        const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
+        const double2 sv = a.s[o];
+        v.x += gb * a.BuoFac * sv.x;
+        v.y += gb * a.BuoFac * sv.y;
+        if (a.xi) {
+          const double2 xv = a.xi[o];
+          v.x += gb * a.ChemFac * xv.x;
+          v.y += gb * a.ChemFac * xv.y;
+        }
+        if (k < 2 || k > n_r - 3 || l == 0) v = zero;
+      }
+      rhs[r * n_r + k] = v;
     }
-    if (k < 2 || k > n_r - 3 || l == 0) v = zero;
-    rhs[k] = v;
-    a.expl1[row + k] = e0;
   }
-  __syncwarp();
+  __syncthreads();
   const double* M = a.mt + (int64_t)l * n_r * n_r;
-  for (int j = lane; j < n_r; j += 32) {
-    double2 acc = zero;
-    for (int k = 0; k < n_r; ++k) {
-      const double c = __ldg(M + (int64_t)k * n_r + j);
-      acc.x = fma(c, rhs[k].x, acc.x);
-      acc.y = fma(c, rhs[k].y, acc.y);
+  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
+    double2 acc[kUsRows];
+    solve_rows(M, n_r, rhs, j, acc);
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      if (mc0 + r == 0) acc[r].y = 0.0;
+      x[r * n_r + j] = acc[r];
+      if (r < nrow) a.w[(int64_t)lm_of(r) * a.ld + j] = acc[r];
     }
-    if (m == 0) acc.y = 0.0;
-    x[j] = acc;
-    a.w[row + j] = acc;
   }
-  __syncwarp();
-  for (int j = lane; j < n_r; j += 32) {
-    const double2 d2 = op_row(a.D2, x, j);
-    dd[j] = d2;
-    a.ddw[row + j] = d2;
+  __syncthreads();
+  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
+    double2 d2[kUsRows];
+    op_rows(a.D2, x, n_r, j, d2);
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      dd[r * n_r + j] = d2[r];
+      if (r < nrow) a.ddw[(int64_t)lm_of(r) * a.ld + j] = d2[r];
+    }
   }
-  __syncwarp();
+  __syncthreads();
   const double hd = a.hdif[l];
-  for (int j = lane; j < n_r; j += 32) {
-    const double2 d1 = op_row(a.D1, x, j), d2 = dd[j];
-    const double2 d3 = op_row(a.D1, dd, j), d4 = op_row(a.D2, dd, j), v = x[j];
-    a.dw[row + j] = d1;
+  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
+    double2 d1[kUsRows], d3[kUsRows], d4[kUsRows];
+    op_rows(a.D1, x, n_r, j, d1);
+    op_rows(a.D1, dd, n_r, j, d3);
+    op_rows(a.D2, dd, n_r, j, d4);
     const bool bnd = j == 0 || j == n_r - 1;
     const double or2 = a.or2[j], orho1 = a.orho1[j], beta = a.beta[j];
-    const double dLo = dL * or2;
-    const double fo = -dLo * orho1;
-    a.old[row + j] = bnd ? zero
-                         : double2{fo * (d2.x - beta * d1.x - dLo * v.x),
-                                   fo * (d2.y - beta * d1.y - dLo * v.y)};
+    const double dLo = dL * or2, fo = -dLo * orho1;
     const double c3 = a.c3[j], c2 = a.c2n[j] - 2.0 * dLo, c1 = a.c1n[j] + dL * a.c1d[j];
     const double c0 = dLo * (a.c0n[j] + dLo);
-    const double fd = -hd * dLo * a.visc[j] * orho1;
-    const double gb = dLo * a.rgrav[j];
-    const double2 sv = a.s[row + j];
-    double2 im;
-    im.x = fd * (d4.x + c3 * d3.x + c2 * d2.x + c1 * d1.x + c0 * v.x) + a.BuoFac * gb * sv.x;
-    im.y = fd * (d4.y + c3 * d3.y + c2 * d2.y + c1 * d1.y + c0 * v.y) + a.BuoFac * gb * sv.y;
-    if (a.xi) {
-      const double2 xv = a.xi[row + j];
-      im.x += a.ChemFac * gb * xv.x;
-      im.y += a.ChemFac * gb * xv.y;
+    const double fd = -hd * dLo * a.visc[j] * orho1, gb = dLo * a.rgrav[j];
+#pragma unroll
+    for (int r = 0; r < kUsRows; ++r) {
+      if (r >= nrow) break;
+      const int64_t o = (int64_t)lm_of(r) * a.ld + j;
+      const double2 v = x[r * n_r + j], e2 = dd[r * n_r + j];
+      a.dw[o] = d1[r];
+      a.old[o] = bnd ? zero
+                     : double2{fo * (e2.x - beta * d1[r].x - dLo * v.x),
+                               fo * (e2.y - beta * d1[r].y - dLo * v.y)};
+      const double2 sv = a.s[o];
+      double2 im;
+      im.x = fd * (d4[r].x + c3 * d3[r].x + c2 * e2.x + c1 * d1[r].x + c0 * v.x) + a.BuoFac * gb * sv.x;
+      im.y = fd * (d4[r].y + c3 * d3[r].y + c2 * e2.y + c1 * d1[r].y + c0 * v.y) + a.BuoFac * gb * sv.y;
+      if (a.xi) {
+        const double2 xv = a.xi[o];
+        im.x += a.ChemFac * gb * xv.x;
+        im.y += a.ChemFac * gb * xv.y;
+      }
+      a.impl[o] = bnd ? zero : im;
     }
-    a.impl[row + j] = bnd ? zero : im;
   }
-  if (l != 0 || m != 0 || !a.p) return;
-  // l = 0 pressure: P0 (0, rho0 BuoFac rgrav Re s + Re expl0 [+ chemistry])
-  __syncwarp();
-  for (int k = lane; k < n_r; k += 32) {
-    double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row + k].x + a.expl0[row + k].x;
-    if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row + k].x;
+  if (l != 0 || mc0 != 0 || !a.p) return;
+  // l = 0 pressure: P0 (0, rho0 BuoFac rgrav Re s + Re expl0 [+ chemistry]); row (0, 0)
+  __syncthreads();
+  const int64_t row0 = (int64_t)lm_of(0) * a.ld;
+  for (int k = threadIdx.x; k < n_r; k += kUsThreads) {
+    double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.expl0[row0 + k].x;
+    if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
     rhs[k] = double2{k == 0 ? 0.0 : v, 0.0};
   }
-  __syncwarp();
-  for (int j = lane; j < n_r; j += 32) a.p[row + j] = double2{op_row(a.P0, rhs, j).x, 0.0};
+  __syncthreads();
+  for (int j = threadIdx.x; j < n_r; j += kUsThreads)
+    a.p[row0 + j] = double2{op_row(a.P0, rhs, j).x, 0.0};
 }
 
 int check_lop(const mt_lop* op) {
@@ -296,11 +376,11 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.mt = solve->mt;
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
-  const size_t sm = (size_t)kUsWarps * 2 * n_r * sizeof(double2);
+  const size_t sm = (size_t)2 * kUsRows * n_r * sizeof(double2);
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_field, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-  const dim3 grid(p->l_max + 1, (p->n_m + kUsWarps - 1) / kUsWarps);
-  k_update_field<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
+  const dim3 grid((p->n_m + kUsRows - 1) / kUsRows, p->l_max + 1);
+  k_update_field<<<grid, kUsThreads, sm, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
@@ -347,11 +427,11 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);
-  const size_t sm = (size_t)kUsWarps * 3 * n_r * sizeof(double2);
+  const size_t sm = (size_t)3 * kUsRows * n_r * sizeof(double2);
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_poloidal,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const dim3 grid(p->l_max + 1, (p->n_m + kUsWarps - 1) / kUsWarps);
-  k_update_poloidal<<<grid, 32 * kUsWarps, sm, (cudaStream_t)stream>>>(a);
+  const dim3 grid((p->n_m + kUsRows - 1) / kUsRows, p->l_max + 1);
+  k_update_poloidal<<<grid, kUsThreads, sm, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
