@@ -12,19 +12,21 @@
 // matrix per l, built on the host as the inverse of the reference's
 // preconditioned LHS (update_s.py:67-134); for the Chebyshev scheme the
 // DCT-I back to grid values and the Chebyshev truncation are folded in
-// (M_l = C T A_l^-1).  Matrices are stored transposed, MT[l][k][j], so the 32
-// lanes of a warp (32 consecutive output levels j) read consecutive values.
+// (M_l = C T A_l^-1).  Matrices are stored transposed, MT[l][k][j], with the
+// j stride rounded up to even, so consecutive threads read consecutive
+// 16-byte level pairs (j, j + 1).
 //
-// k_update_field: CTA = (4 orders m, degree l); every thread owns output
-// levels j and works on all 4 rows, so each matrix coefficient is loaded once
-// per CTA and applied to 4 right-hand sides broadcast from shared memory:
+// k_update_field: CTA = (16 orders m of one degree l); thread = (group of 4
+// orders, pair of output levels j, j + 1), a 4 x 2 complex register tile:
 //   rhs = w_old old + w_impl impl + w_expl0 expl0 + w_expl1 expl1, rows 0 and
 //   n_r - 1 replaced by the boundary values; expl1 <- expl0 (rotation);
 //   x = M_l rhs, imaginary part dropped for m = 0; dx = D1 x, d2x = D2 x
 //   (d2x stored when requested);
 //   old <- so_l so_r x; impl <- ia_l ia_r (d2x + ib_r dx - (ic_r + ic_l ic_r2) x).
-// The radial derivatives of the 4 rows share their coefficients the same way;
-// consecutive CTAs hold the same degree, so M_l is reused through L1 / L2.
+// M_l streams through shared memory in chunks of 16 rows k (double-buffered
+// cp.async, overlapping the right-hand-side loads and the products), each
+// coefficient pair feeding 16 FMAs.  For n_r > 256 a wide variant (4 orders
+// per CTA, coefficients read from L2) keeps shared memory bounded.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -33,47 +35,128 @@
 #include "radial_op.cuh"
 
 struct mt_lop {
-  int n_l = 0, n_r = 0, device = 0;
-  double* mt = nullptr;  // (n_l, n_r, n_r) transposed: mt[(l * n_r + k) * n_r + j] = M_l[j][k]
+  int n_l = 0, n_r = 0, ldm = 0, device = 0;  // ldm: n_r rounded up to even
+  double* mt = nullptr;  // (n_l, n_r, ldm) transposed: mt[(l * n_r + k) * ldm + j] = M_l[j][k]
 };
 
 namespace mt {
 
 namespace {
 
-constexpr int kUsRows = 4;       // orders m (rows of one degree l) per CTA
-constexpr int kUsThreads = 128;  // output levels j = thread, thread + 128, ...
+constexpr int kRows = 4;           // orders m per thread
+constexpr int kKc = 16;            // solve-matrix rows k per staged chunk
+constexpr int kStagedMaxR = 256;   // largest n_r on the shared-memory path
+constexpr int kMaxThreads = 512;   // 4 groups x 128 level pairs; wide: 512 pairs
 
-// acc[r] = (M_l f_r)[j] for the CTA's rows r: every coefficient M_l[j][k]
-// (transposed storage: consecutive j contiguous) is loaded once and applied
-// to all rows, whose values are broadcast from shared memory.
-__device__ __forceinline__ void solve_rows(const double* __restrict__ M, int n_r,
-                                           const double2* f, int j,
-                                           double2 (&acc)[kUsRows]) {
+template <bool kStaged>
+struct Tile {
+  static constexpr int kGroups = kStaged ? 4 : 1;  // row groups per CTA
+  static constexpr int kCtaRows = kGroups * kRows;
+};
+
+// thread = (row group rg: rows rg * kRows .. + kRows - 1, level pair jp: j = 2 jp, 2 jp + 1)
+struct Slot {
+  int rg, jp;
+  bool active;
+};
+template <bool kStaged>
+__device__ __forceinline__ Slot slot_of(int n_r) {
+  const int n_jp = (n_r + 1) >> 1;
+  Slot s;
+  s.jp = threadIdx.x % n_jp;
+  s.rg = threadIdx.x / n_jp;
+  s.active = s.rg < Tile<kStaged>::kGroups;
+  return s;
+}
+
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// rows k of chunk c of M_l (row stride ldm, even, so every 16-byte piece is
+// aligned) into a shared buffer of kKc x ldm doubles; one commit group
+__device__ __forceinline__ void stage_chunk(const double* Ml, int n_r, int ldm, int c,
+                                            double* buf) {
+  const int k0 = c * kKc, nk = min(kKc, n_r - k0);
+  const int nv = nk * ldm / 2;
+  const double2* src = (const double2*)(Ml + (int64_t)k0 * ldm);
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) cpa16(buf + 2 * i, src + i);
+  cpa_commit();
+}
+
+// acc[r][h] += m.h * f_r[k] for the thread's 4 rows (broadcast from shared memory)
+__device__ __forceinline__ void fma_rows(double2 m, const double2* fr, int n_r, int k,
+                                         double2 (&acc)[kRows][2]) {
 #pragma unroll
-  for (int r = 0; r < kUsRows; ++r) acc[r] = double2{0.0, 0.0};
+  for (int r = 0; r < kRows; ++r) {
+    const double2 v = fr[r * n_r + k];
+    acc[r][0].x = fma(m.x, v.x, acc[r][0].x);
+    acc[r][0].y = fma(m.x, v.y, acc[r][0].y);
+    acc[r][1].x = fma(m.y, v.x, acc[r][1].x);
+    acc[r][1].y = fma(m.y, v.y, acc[r][1].y);
+  }
+}
+
+// acc[r][h] = (M_l f_{rg kRows + r})[2 jp + h].  Staged: chunk 0 was issued by
+// the caller; every thread of the CTA must call this (barriers inside), and
+// the call ends with a barrier.  Wide: M_l read from global memory.
+template <bool kStaged>
+__device__ __forceinline__ void solve_tile(const double* __restrict__ Ml, int n_r, int ldm,
+                                           const double2* f, double* mbuf, const Slot& s,
+                                           double2 (&acc)[kRows][2]) {
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) acc[r][0] = acc[r][1] = double2{0.0, 0.0};
+  const double2* fr = f + s.rg * kRows * n_r;
+  if constexpr (!kStaged) {
+    if (!s.active) return;
+    const double* mp = Ml + 2 * s.jp;
 #pragma unroll 8
-  for (int k = 0; k < n_r; ++k) {
-    const double c = __ldg(M + (int64_t)k * n_r + j);
+    for (int k = 0; k < n_r; ++k)
+      fma_rows(__ldg((const double2*)(mp + (int64_t)k * ldm)), fr, n_r, k, acc);
+  } else {
+    const int nch = (n_r + kKc - 1) / kKc;
+    for (int c = 0; c < nch; ++c) {
+      if (c + 1 < nch) {
+        stage_chunk(Ml, n_r, ldm, c + 1, mbuf + ((c + 1) & 1) * kKc * ldm);
+        cpa_wait<1>();
+      } else {
+        cpa_wait<0>();
+      }
+      __syncthreads();
+      if (s.active) {
+        const double* mp = mbuf + (c & 1) * kKc * ldm + 2 * s.jp;
+        const double2* fc = fr + c * kKc;
+        const int nk = n_r - c * kKc;
+        if (nk >= kKc) {
 #pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
-      const double2 v = f[r * n_r + k];
-      acc[r].x = fma(c, v.x, acc[r].x);
-      acc[r].y = fma(c, v.y, acc[r].y);
+          for (int kk = 0; kk < kKc; ++kk)
+            fma_rows(*(const double2*)(mp + kk * ldm), fc, n_r, kk, acc);
+        } else {
+          for (int kk = 0; kk < nk; ++kk)
+            fma_rows(*(const double2*)(mp + kk * ldm), fc, n_r, kk, acc);
+        }
+      }
+      __syncthreads();
     }
   }
 }
 
 // acc[r] = (D f_r)[j] for a banded radial operator, coefficients shared by the rows
 __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int n_r, int j,
-                                        double2 (&acc)[kUsRows]) {
+                                        double2 (&acc)[kRows]) {
   const int k0 = __ldg(op.k0 + j);
 #pragma unroll
-  for (int r = 0; r < kUsRows; ++r) acc[r] = double2{0.0, 0.0};
+  for (int r = 0; r < kRows; ++r) acc[r] = double2{0.0, 0.0};
   for (int kk = 0; kk < op.W; ++kk) {
     const double c = __ldg(op.vals + (int64_t)kk * op.n_r + j);
 #pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
+    for (int r = 0; r < kRows; ++r) {
       const double2 v = f[r * n_r + k0 + kk];
       acc[r].x = fma(c, v.x, acc[r].x);
       acc[r].y = fma(c, v.y, acc[r].y);
@@ -82,7 +165,7 @@ __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int 
 }
 
 struct UsArgs {
-  int n_r, l_max, minc, n_m;
+  int n_r, ldm, l_max, minc, n_m;
   const int* lstart;
   double2 *x, *dx, *d2x, *old, *impl, *expl0, *expl1;
   const double2 *top, *bot;
@@ -93,70 +176,81 @@ struct UsArgs {
   OpView D1, D2;
 };
 
-// rows of this CTA (grid x = chunk of orders, y = degree l): orders
-// mc = chunk * kUsRows + r with m <= l
-__device__ __forceinline__ int cta_rows(int l, int minc, int n_m) {
-  const int mc0 = blockIdx.x * kUsRows;
-  int n = 0;
-  for (int r = 0; r < kUsRows; ++r) {
-    const int mc = mc0 + r;
-    if (mc < n_m && mc * minc <= l) n = r + 1;
-  }
-  return n;
+// number of valid rows of the CTA starting at order index mc0: mc < n_m, m <= l
+__device__ __forceinline__ int cta_rows(int mc0, int rows, int l, int minc, int n_m) {
+  int n = min(rows, n_m - mc0);
+  if (n <= 0) return 0;
+  return max(0, min(n, l / minc - mc0 + 1));
 }
 
-__global__ void __launch_bounds__(kUsThreads) k_update_field(UsArgs a) {
-  extern __shared__ double2 usbuf[];
-  const int n_r = a.n_r, l = blockIdx.y;
-  const int nrow = cta_rows(l, a.minc, a.n_m);
+template <bool kStaged>
+__global__ void __launch_bounds__(kMaxThreads) k_update_field(UsArgs a) {
+  constexpr int kCtaRows = Tile<kStaged>::kCtaRows;
+  extern __shared__ __align__(16) double2 usbuf[];
+  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * kCtaRows;
+  const int nrow = cta_rows(mc0, kCtaRows, l, a.minc, a.n_m);
   if (nrow == 0) return;
-  const int mc0 = blockIdx.x * kUsRows;
-  double2* rhs = usbuf;                  // [kUsRows][n_r]
-  double2* x = usbuf + kUsRows * n_r;    // [kUsRows][n_r]
+  double2* f = usbuf;                                // [kCtaRows][n_r]: rhs, then x
+  double* mbuf = (double*)(usbuf + kCtaRows * n_r);  // staged: [2][kKc][ldm]
+  const double* Ml = a.mt + (int64_t)l * n_r * ldm;
+  if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
   const double2 zero = {0.0, 0.0};
-  auto lm_of = [&](int r) { return a.lstart[mc0 + r] + (l - (mc0 + r) * a.minc); };
-  for (int r = 0; r < kUsRows; ++r) {
-    const int lm = r < nrow ? lm_of(r) : 0;
-    for (int k = threadIdx.x; k < n_r; k += kUsThreads) {
-      double2 v = zero;
-      if (r < nrow) {
-        const int64_t o = (int64_t)lm * a.ld + k;
-        const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
-        a.expl1[o] = e0;
-        v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
-        v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
-        if (k == 0) v = a.top ? a.top[lm] : zero;
-        if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
-      }
-      rhs[r * n_r + k] = v;
+  auto lm_of = [&](int row) { return __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc); };
+  for (int idx = threadIdx.x; idx < kCtaRows * n_r; idx += blockDim.x) {
+    const int row = idx / n_r, k = idx - row * n_r;
+    double2 v = zero;
+    if (row < nrow) {
+      const int lm = lm_of(row);
+      const int64_t o = (int64_t)lm * a.ld + k;
+      const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
+      a.expl1[o] = e0;
+      v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
+      v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
+      if (k == 0) v = a.top ? a.top[lm] : zero;
+      if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
     }
+    f[idx] = v;
   }
   __syncthreads();
-  const double* M = a.mt + (int64_t)l * n_r * n_r;
-  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
-    double2 acc[kUsRows];
-    solve_rows(M, n_r, rhs, j, acc);
+  const Slot s = slot_of<kStaged>(n_r);
+  double2 acc[kRows][2];
+  solve_tile<kStaged>(Ml, n_r, ldm, f, mbuf, s, acc);
+  __syncthreads();
+  if (s.active) {
 #pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
-      if (mc0 + r == 0) acc[r].y = 0.0;  // m = 0
-      x[r * n_r + j] = acc[r];
-      if (r < nrow) a.x[(int64_t)lm_of(r) * a.ld + j] = acc[r];
+    for (int r = 0; r < kRows; ++r) {
+      const int row = s.rg * kRows + r;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = 2 * s.jp + h;
+        if (j >= n_r) continue;
+        double2 v = acc[r][h];
+        if (mc0 + row == 0) v.y = 0.0;  // m = 0
+        f[row * n_r + j] = v;
+        if (row < nrow) a.x[(int64_t)lm_of(row) * a.ld + j] = v;
+      }
     }
   }
   __syncthreads();
+  if (!s.active) return;
   const double so_l = a.so_l ? a.so_l[l] : 1.0, ia_l = a.ia_l[l], ic_l = a.ic_l[l];
-  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
-    double2 d1[kUsRows], d2[kUsRows];
-    op_rows(a.D1, x, n_r, j, d1);
-    op_rows(a.D2, x, n_r, j, d2);
+  const double2* fr = f + s.rg * kRows * n_r;
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    const int j = 2 * s.jp + h;
+    if (j >= n_r) break;
+    double2 d1[kRows], d2[kRows];
+    op_rows(a.D1, fr, n_r, j, d1);
+    op_rows(a.D2, fr, n_r, j, d2);
     const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
     const double c1 = a.ib_r[j], c0 = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
     const double ia = ia_l * a.ia_r[j];
 #pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
-      if (r >= nrow) break;
-      const int64_t o = (int64_t)lm_of(r) * a.ld + j;
-      const double2 v = x[r * n_r + j];
+    for (int r = 0; r < kRows; ++r) {
+      const int row = s.rg * kRows + r;
+      if (row >= nrow) break;
+      const int64_t o = (int64_t)lm_of(row) * a.ld + j;
+      const double2 v = fr[r * n_r + j];
       a.dx[o] = d1[r];
       if (a.d2x) a.d2x[o] = d2[r];
       a.old[o] = double2{so * v.x, so * v.y};
@@ -167,7 +261,7 @@ __global__ void __launch_bounds__(kUsThreads) k_update_field(UsArgs a) {
 }
 
 struct PwArgs {
-  int n_r, l_max, minc, n_m;
+  int n_r, ldm, l_max, minc, n_m;
   const int* lstart;
   double2 *w, *dw, *ddw, *old, *impl, *expl0, *expl1, *p;
   const double2 *s, *xi;
@@ -180,112 +274,158 @@ struct PwArgs {
 };
 
 // Double-curl poloidal update (magic_torch/update_w_doublecurl.py:393-483):
-// CTA = (chunk of kUsRows orders m, degree l); the CTA holding (l, m) = (0, 0)
-// also solves the l = 0 pressure (update_wp.py:173-194).
-__global__ void __launch_bounds__(kUsThreads) k_update_poloidal(PwArgs a) {
-  extern __shared__ double2 pwbuf[];
-  const int n_r = a.n_r, l = blockIdx.y;
-  const int nrow = cta_rows(l, a.minc, a.n_m);
+// same tiling as k_update_field; the CTA holding (l, m) = (0, 0) also solves
+// the l = 0 pressure (update_wp.py:173-194).
+template <bool kStaged>
+__global__ void __launch_bounds__(kMaxThreads) k_update_poloidal(PwArgs a) {
+  constexpr int kCtaRows = Tile<kStaged>::kCtaRows;
+  extern __shared__ __align__(16) double2 pwbuf[];
+  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * kCtaRows;
+  const int nrow = cta_rows(mc0, kCtaRows, l, a.minc, a.n_m);
   if (nrow == 0) return;
-  const int mc0 = blockIdx.x * kUsRows;
-  double2* rhs = pwbuf;
-  double2* x = pwbuf + kUsRows * n_r;
-  double2* dd = pwbuf + 2 * kUsRows * n_r;
+  double2* f = pwbuf;                      // [kCtaRows][n_r]: rhs, then w
+  double2* dd = pwbuf + kCtaRows * n_r;    // [kCtaRows][n_r]: D2 w
+  double* mbuf = (double*)(pwbuf + 2 * kCtaRows * n_r);
+  const double* Ml = a.mt + (int64_t)l * n_r * ldm;
+  if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
-  auto lm_of = [&](int r) { return a.lstart[mc0 + r] + (l - (mc0 + r) * a.minc); };
-  for (int r = 0; r < kUsRows; ++r) {
-    const int64_t row = r < nrow ? (int64_t)lm_of(r) * a.ld : 0;
-    for (int k = threadIdx.x; k < n_r; k += kUsThreads) {
-      double2 v = zero;
-      if (r < nrow) {
-        const int64_t o = row + k;
-        const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
-        a.expl1[o] = e0;
-        v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
-        v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
-        const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
-        const double2 sv = a.s[o];
-        v.x += gb * a.BuoFac * sv.x;
-        v.y += gb * a.BuoFac * sv.y;
-        if (a.xi) {
-          const double2 xv = a.xi[o];
-          v.x += gb * a.ChemFac * xv.x;
-          v.y += gb * a.ChemFac * xv.y;
-        }
-        if (k < 2 || k > n_r - 3 || l == 0) v = zero;
-      }
-      rhs[r * n_r + k] = v;
-    }
-  }
-  __syncthreads();
-  const double* M = a.mt + (int64_t)l * n_r * n_r;
-  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
-    double2 acc[kUsRows];
-    solve_rows(M, n_r, rhs, j, acc);
-#pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
-      if (mc0 + r == 0) acc[r].y = 0.0;
-      x[r * n_r + j] = acc[r];
-      if (r < nrow) a.w[(int64_t)lm_of(r) * a.ld + j] = acc[r];
-    }
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
-    double2 d2[kUsRows];
-    op_rows(a.D2, x, n_r, j, d2);
-#pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
-      dd[r * n_r + j] = d2[r];
-      if (r < nrow) a.ddw[(int64_t)lm_of(r) * a.ld + j] = d2[r];
-    }
-  }
-  __syncthreads();
-  const double hd = a.hdif[l];
-  for (int j = threadIdx.x; j < n_r; j += kUsThreads) {
-    double2 d1[kUsRows], d3[kUsRows], d4[kUsRows];
-    op_rows(a.D1, x, n_r, j, d1);
-    op_rows(a.D1, dd, n_r, j, d3);
-    op_rows(a.D2, dd, n_r, j, d4);
-    const bool bnd = j == 0 || j == n_r - 1;
-    const double or2 = a.or2[j], orho1 = a.orho1[j], beta = a.beta[j];
-    const double dLo = dL * or2, fo = -dLo * orho1;
-    const double c3 = a.c3[j], c2 = a.c2n[j] - 2.0 * dLo, c1 = a.c1n[j] + dL * a.c1d[j];
-    const double c0 = dLo * (a.c0n[j] + dLo);
-    const double fd = -hd * dLo * a.visc[j] * orho1, gb = dLo * a.rgrav[j];
-#pragma unroll
-    for (int r = 0; r < kUsRows; ++r) {
-      if (r >= nrow) break;
-      const int64_t o = (int64_t)lm_of(r) * a.ld + j;
-      const double2 v = x[r * n_r + j], e2 = dd[r * n_r + j];
-      a.dw[o] = d1[r];
-      a.old[o] = bnd ? zero
-                     : double2{fo * (e2.x - beta * d1[r].x - dLo * v.x),
-                               fo * (e2.y - beta * d1[r].y - dLo * v.y)};
+  auto lm_of = [&](int row) { return __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc); };
+  for (int idx = threadIdx.x; idx < kCtaRows * n_r; idx += blockDim.x) {
+    const int row = idx / n_r, k = idx - row * n_r;
+    double2 v = zero;
+    if (row < nrow) {
+      const int64_t o = (int64_t)lm_of(row) * a.ld + k;
+      const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
+      a.expl1[o] = e0;
+      v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
+      v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
+      const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
       const double2 sv = a.s[o];
-      double2 im;
-      im.x = fd * (d4[r].x + c3 * d3[r].x + c2 * e2.x + c1 * d1[r].x + c0 * v.x) + a.BuoFac * gb * sv.x;
-      im.y = fd * (d4[r].y + c3 * d3[r].y + c2 * e2.y + c1 * d1[r].y + c0 * v.y) + a.BuoFac * gb * sv.y;
+      v.x += gb * a.BuoFac * sv.x;
+      v.y += gb * a.BuoFac * sv.y;
       if (a.xi) {
         const double2 xv = a.xi[o];
-        im.x += a.ChemFac * gb * xv.x;
-        im.y += a.ChemFac * gb * xv.y;
+        v.x += gb * a.ChemFac * xv.x;
+        v.y += gb * a.ChemFac * xv.y;
       }
-      a.impl[o] = bnd ? zero : im;
+      if (k < 2 || k > n_r - 3 || l == 0) v = zero;
+    }
+    f[idx] = v;
+  }
+  __syncthreads();
+  const Slot s = slot_of<kStaged>(n_r);
+  double2 acc[kRows][2];
+  solve_tile<kStaged>(Ml, n_r, ldm, f, mbuf, s, acc);
+  __syncthreads();
+  if (s.active) {
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int row = s.rg * kRows + r;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = 2 * s.jp + h;
+        if (j >= n_r) continue;
+        double2 v = acc[r][h];
+        if (mc0 + row == 0) v.y = 0.0;
+        f[row * n_r + j] = v;
+        if (row < nrow) a.w[(int64_t)lm_of(row) * a.ld + j] = v;
+      }
+    }
+  }
+  __syncthreads();
+  const double2* fr = f + s.rg * kRows * n_r;
+  double2* dr = dd + s.rg * kRows * n_r;
+  if (s.active) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = 2 * s.jp + h;
+      if (j >= n_r) break;
+      double2 d2[kRows];
+      op_rows(a.D2, fr, n_r, j, d2);
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int row = s.rg * kRows + r;
+        dr[r * n_r + j] = d2[r];
+        if (row < nrow) a.ddw[(int64_t)lm_of(row) * a.ld + j] = d2[r];
+      }
+    }
+  }
+  __syncthreads();
+  if (s.active) {
+    const double hd = a.hdif[l];
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      const int j = 2 * s.jp + h;
+      if (j >= n_r) break;
+      double2 d1[kRows], d3[kRows], d4[kRows];
+      op_rows(a.D1, fr, n_r, j, d1);
+      op_rows(a.D1, dr, n_r, j, d3);
+      op_rows(a.D2, dr, n_r, j, d4);
+      const bool bnd = j == 0 || j == n_r - 1;
+      const double or2 = a.or2[j], orho1 = a.orho1[j], beta = a.beta[j];
+      const double dLo = dL * or2, fo = -dLo * orho1;
+      const double c3 = a.c3[j], c2 = a.c2n[j] - 2.0 * dLo, c1 = a.c1n[j] + dL * a.c1d[j];
+      const double c0 = dLo * (a.c0n[j] + dLo);
+      const double fd = -hd * dLo * a.visc[j] * orho1, gb = dLo * a.rgrav[j];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int row = s.rg * kRows + r;
+        if (row >= nrow) break;
+        const int64_t o = (int64_t)lm_of(row) * a.ld + j;
+        const double2 v = fr[r * n_r + j], e2 = dr[r * n_r + j];
+        a.dw[o] = d1[r];
+        a.old[o] = bnd ? zero
+                       : double2{fo * (e2.x - beta * d1[r].x - dLo * v.x),
+                                 fo * (e2.y - beta * d1[r].y - dLo * v.y)};
+        const double2 sv = a.s[o];
+        double2 im;
+        im.x = fd * (d4[r].x + c3 * d3[r].x + c2 * e2.x + c1 * d1[r].x + c0 * v.x) +
+               a.BuoFac * gb * sv.x;
+        im.y = fd * (d4[r].y + c3 * d3[r].y + c2 * e2.y + c1 * d1[r].y + c0 * v.y) +
+               a.BuoFac * gb * sv.y;
+        if (a.xi) {
+          const double2 xv = a.xi[o];
+          im.x += a.ChemFac * gb * xv.x;
+          im.y += a.ChemFac * gb * xv.y;
+        }
+        a.impl[o] = bnd ? zero : im;
+      }
     }
   }
   if (l != 0 || mc0 != 0 || !a.p) return;
   // l = 0 pressure: P0 (0, rho0 BuoFac rgrav Re s + Re expl0 [+ chemistry]); row (0, 0)
   __syncthreads();
   const int64_t row0 = (int64_t)lm_of(0) * a.ld;
-  for (int k = threadIdx.x; k < n_r; k += kUsThreads) {
+  for (int k = threadIdx.x; k < n_r; k += blockDim.x) {
     double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.expl0[row0 + k].x;
     if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
-    rhs[k] = double2{k == 0 ? 0.0 : v, 0.0};
+    f[k] = double2{k == 0 ? 0.0 : v, 0.0};
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < n_r; j += kUsThreads)
-    a.p[row0 + j] = double2{op_row(a.P0, rhs, j).x, 0.0};
+  for (int j = threadIdx.x; j < n_r; j += blockDim.x)
+    a.p[row0 + j] = double2{op_row(a.P0, f, j).x, 0.0};
+}
+
+// Launch shape of either tiling: threads = groups x level pairs (rounded to a
+// warp), shared memory = row buffers (+ the two staged matrix chunks).
+struct TileLaunch {
+  bool staged;
+  dim3 grid;
+  int threads;
+  size_t smem;
+};
+TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers) {
+  TileLaunch t;
+  t.staged = n_r <= kStagedMaxR;
+  const int groups = t.staged ? Tile<true>::kGroups : Tile<false>::kGroups;
+  const int rows = groups * kRows;
+  const int n_jp = (n_r + 1) / 2;
+  t.threads = (groups * n_jp + 31) / 32 * 32;
+  t.grid = dim3((n_m + rows - 1) / rows, l_max + 1);
+  t.smem = (size_t)row_buffers * rows * n_r * sizeof(double2) +
+           (t.staged ? (size_t)2 * kKc * ldm * sizeof(double) : 0);
+  return t;
 }
 
 int check_lop(const mt_lop* op) {
@@ -310,17 +450,20 @@ int mt_lop_create(int n_l, int n_r, const double* M, mt_lop** out) {
              "bad per-degree operator argument");
   *out = nullptr;
   const size_t per = (size_t)n_r * n_r;
-  std::vector<double> t(per * n_l);
+  const int ldm = n_r + (n_r & 1);
+  const size_t per_t = (size_t)n_r * ldm;
+  std::vector<double> t(per_t * n_l, 0.0);
   for (int l = 0; l < n_l; ++l)
     for (int j = 0; j < n_r; ++j)
       for (int k = 0; k < n_r; ++k) {
         const double v = M[l * per + (size_t)j * n_r + k];
         MT_REQUIRE(std::isfinite(v), MT_ERR_ARG, "per-degree operator not finite");
-        t[l * per + (size_t)k * n_r + j] = v;
+        t[l * per_t + (size_t)k * ldm + j] = v;
       }
   mt_lop* op = new mt_lop();
   op->n_l = n_l;
   op->n_r = n_r;
+  op->ldm = ldm;
   if (cudaGetDevice(&op->device) != cudaSuccess ||
       cudaMalloc(&op->mt, t.size() * sizeof(double)) != cudaSuccess ||
       cudaMemcpy(op->mt, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice) !=
@@ -360,6 +503,7 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
              "null coefficient array");
   UsArgs a{};
   a.n_r = n_r;
+  a.ldm = solve->ldm;
   a.l_max = p->l_max;
   a.minc = p->minc;
   a.n_m = p->n_m;
@@ -376,11 +520,10 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.mt = solve->mt;
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
-  const size_t sm = (size_t)2 * kUsRows * n_r * sizeof(double2);
-  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_field, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sm));
-  const dim3 grid((p->n_m + kUsRows - 1) / kUsRows, p->l_max + 1);
-  k_update_field<<<grid, kUsThreads, sm, (cudaStream_t)stream>>>(a);
+  const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1);
+  auto kern = t.staged ? k_update_field<true> : k_update_field<false>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
+  kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
@@ -408,6 +551,7 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
              MT_ERR_ARG, "null coefficient array");
   PwArgs a{};
   a.n_r = n_r;
+  a.ldm = solve->ldm;
   a.l_max = p->l_max;
   a.minc = p->minc;
   a.n_m = p->n_m;
@@ -427,11 +571,10 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);
-  const size_t sm = (size_t)3 * kUsRows * n_r * sizeof(double2);
-  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_poloidal,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const dim3 grid((p->n_m + kUsRows - 1) / kUsRows, p->l_max + 1);
-  k_update_poloidal<<<grid, kUsThreads, sm, (cudaStream_t)stream>>>(a);
+  const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 2);
+  auto kern = t.staged ? k_update_poloidal<true> : k_update_poloidal<false>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
+  kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

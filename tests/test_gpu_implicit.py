@@ -62,8 +62,11 @@ def test_update_scalar_matches_reference(name):
     assert rel_err(npy(ta["expl0"]), z["s_expl0"]) == 0.0  # left for the next explicit stage
 
 
-@pytest.mark.parametrize("scheme,l_max,n_r", [("chebyshev", 127, 65), ("FD", 255, 97)])
+@pytest.mark.parametrize("scheme,l_max,n_r", [("chebyshev", 127, 65), ("FD", 255, 97),
+                                               ("FD", 31, 289)])
 def test_update_scalar_two_steps_vs_oracle(scheme, l_max, n_r):
+    """Two consecutive steps against the oracle; 289 levels take the wide tiling
+    (n_r > 256: solve matrices read from L2 instead of staged in shared memory)."""
     from magic_b200 import Plan
     from magic_b200 import implicit as I
     from magic_b200.radial import RadialScheme
@@ -284,13 +287,19 @@ def test_update_poloidal_matches_reference():
         assert v < TOL, (k, v)
 
 
-def test_update_poloidal_vs_oracle():
-    """l_max = 255, 97 fourth-order finite-difference levels, anelastic-like profiles."""
+@pytest.mark.parametrize("l_max,n_r,scale", [(255, 97, 1.0), (16, 261, 50.0)])
+def test_update_poloidal_vs_oracle(l_max, n_r, scale):
+    """l_max = 255, 97 fourth-order finite-difference levels, anelastic-like
+    profiles; and l_max = 16 at 261 levels, the wide tiling (n_r > 256).  The
+    GPU applies the inverse of the fourth-order double-curl operator, whose
+    rounding error grows with its condition number (~ n_r^4): the tolerances
+    are scaled by 50 ~ (261 / 97)^4 there (a numpy restatement of the same
+    inverse-apply algorithm differs from the oracle by 8.0e-11 in impl and
+    4.3e-12 in dw at 261 levels)."""
     from magic_b200 import Plan
     from magic_b200 import implicit as I
     from magic_b200.radial import RadialScheme
 
-    l_max, n_r = 255, 97
     p = Plan(l_max, 1)
     sch = RadialScheme(n_r, "FD", fd_order=4)
     r = sch.r
@@ -313,4 +322,4 @@ def test_update_poloidal_vs_oracle():
                       sch.D2m, s_new, BuoFac, r, 4, 2, 2)
     for k in ("x", "dx", "d2x", "impl", "old", "expl1", "p0"):
         e = rel_err(npy(o[k]), ref[k])
-        assert e < (TOL_IMPL if k in ("impl", "old", "d2x") else TOL), (k, e)
+        assert e < scale * (TOL_IMPL if k in ("impl", "old", "d2x") else TOL), (k, e)
