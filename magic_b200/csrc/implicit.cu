@@ -46,12 +46,15 @@ namespace {
 constexpr int kRows = 4;           // orders m per thread
 constexpr int kKc = 16;            // solve-matrix rows k per staged chunk
 constexpr int kStagedMaxR = 256;   // largest n_r on the shared-memory path
-constexpr int kMaxThreads = 512;   // 4 groups x 128 level pairs; wide: 512 pairs
+constexpr int kStagedThreads = 256;
+constexpr int kWideThreads = 512;  // one group of up to 512 level pairs
 
-template <bool kStaged>
-struct Tile {
-  static constexpr int kGroups = kStaged ? 4 : 1;  // row groups per CTA
-  static constexpr int kCtaRows = kGroups * kRows;
+// staged: up to 4 row groups within 256 threads, kMinBlocks resident CTAs
+// per SM (the register cap); wide: one group
+template <bool kStaged, int kMinBlocks>
+struct Bounds {
+  static constexpr int kThreads = kStaged ? kStagedThreads : kWideThreads;
+  static constexpr int kBlocks = kStaged ? kMinBlocks : 1;
 };
 
 // thread = (row group rg: rows rg * kRows .. + kRows - 1, level pair jp: j = 2 jp, 2 jp + 1)
@@ -59,13 +62,12 @@ struct Slot {
   int rg, jp;
   bool active;
 };
-template <bool kStaged>
-__device__ __forceinline__ Slot slot_of(int n_r) {
+__device__ __forceinline__ Slot slot_of(int n_r, int groups) {
   const int n_jp = (n_r + 1) >> 1;
   Slot s;
   s.jp = threadIdx.x % n_jp;
   s.rg = threadIdx.x / n_jp;
-  s.active = s.rg < Tile<kStaged>::kGroups;
+  s.active = s.rg < groups;
   return s;
 }
 
@@ -165,7 +167,7 @@ __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int 
 }
 
 struct UsArgs {
-  int n_r, ldm, l_max, minc, n_m;
+  int n_r, ldm, l_max, minc, n_m, groups;
   const int* lstart;
   double2 *x, *dx, *d2x, *old, *impl, *expl0, *expl1;
   const double2 *top, *bot;
@@ -183,36 +185,85 @@ __device__ __forceinline__ int cta_rows(int mc0, int rows, int l, int minc, int 
   return max(0, min(n, l / minc - mc0 + 1));
 }
 
+// CNAB2 right-hand sides of the CTA's rows into f ([rows][n_r], zero for
+// rows past nrow), with expl1 <- expl0.  kLd elements per thread are loaded
+// before any store, so their HBM latencies overlap (the stores may alias the
+// next loads as far as the compiler knows).  The poloidal form adds
+// the buoyancy (and chemical) coupling and zeroes its boundary rows.
+template <bool kPol, int kLd, class A>
+__device__ __forceinline__ void build_rhs(const A& a, int l, int mc0, int rows, int nrow,
+                                          double2* f) {
+  const int n_r = a.n_r, total = rows * n_r;
+  const double2 zero = {0.0, 0.0};
+  const double dL = (double)l * (l + 1.0);
+  for (int base = threadIdx.x; base < total; base += kLd * blockDim.x) {
+    double2 ol[kLd], im[kLd], e0[kLd], e1[kLd], cs[kLd], cx[kLd];
+    int64_t off[kLd];
+#pragma unroll
+    for (int u = 0; u < kLd; ++u) {
+      const int idx = base + u * blockDim.x, row = idx / n_r;
+      off[u] = -1;
+      ol[u] = im[u] = e0[u] = e1[u] = cs[u] = cx[u] = zero;
+      if (idx < total && row < nrow) {
+        const int lm = __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc);
+        const int64_t o = (int64_t)lm * a.ld + (idx - row * n_r);
+        off[u] = o;
+        ol[u] = a.old[o];
+        im[u] = a.impl[o];
+        e0[u] = a.expl0[o];
+        e1[u] = a.expl1[o];
+        if constexpr (kPol) {
+          cs[u] = a.s[o];
+          if (a.xi) cx[u] = a.xi[o];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kLd; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx >= total) break;
+      const int row = idx / n_r, k = idx - row * n_r;
+      double2 v = zero;
+      if (off[u] >= 0) {
+        a.expl1[off[u]] = e0[u];
+        v.x = a.w_old * ol[u].x + a.w_impl * im[u].x + a.w_expl0 * e0[u].x + a.w_expl1 * e1[u].x;
+        v.y = a.w_old * ol[u].y + a.w_impl * im[u].y + a.w_expl0 * e0[u].y + a.w_expl1 * e1[u].y;
+        if constexpr (kPol) {
+          const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
+          v.x += gb * a.BuoFac * cs[u].x;
+          v.y += gb * a.BuoFac * cs[u].y;
+          if (a.xi) {
+            v.x += gb * a.ChemFac * cx[u].x;
+            v.y += gb * a.ChemFac * cx[u].y;
+          }
+          if (k < 2 || k > n_r - 3 || l == 0) v = zero;
+        } else {
+          const int lm = __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc);
+          if (k == 0) v = a.top ? a.top[lm] : zero;
+          if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
+        }
+      }
+      f[idx] = v;
+    }
+  }
+}
+
 template <bool kStaged>
-__global__ void __launch_bounds__(kMaxThreads) k_update_field(UsArgs a) {
-  constexpr int kCtaRows = Tile<kStaged>::kCtaRows;
+__global__ void __launch_bounds__(Bounds<kStaged, 3>::kThreads, Bounds<kStaged, 3>::kBlocks)
+    k_update_field(UsArgs a) {
   extern __shared__ __align__(16) double2 usbuf[];
-  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * kCtaRows;
-  const int nrow = cta_rows(mc0, kCtaRows, l, a.minc, a.n_m);
+  const int rows = a.groups * kRows;
+  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * rows;
+  const int nrow = cta_rows(mc0, rows, l, a.minc, a.n_m);
   if (nrow == 0) return;
-  double2* f = usbuf;                                // [kCtaRows][n_r]: rhs, then x
-  double* mbuf = (double*)(usbuf + kCtaRows * n_r);  // staged: [2][kKc][ldm]
+  double2* f = usbuf;                            // [rows][n_r]: rhs, then x
+  double* mbuf = (double*)(usbuf + rows * n_r);  // staged: [2][kKc][ldm]
   const double* Ml = a.mt + (int64_t)l * n_r * ldm;
   if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
-  const double2 zero = {0.0, 0.0};
   auto lm_of = [&](int row) { return __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc); };
-  for (int idx = threadIdx.x; idx < kCtaRows * n_r; idx += blockDim.x) {
-    const int row = idx / n_r, k = idx - row * n_r;
-    double2 v = zero;
-    if (row < nrow) {
-      const int lm = lm_of(row);
-      const int64_t o = (int64_t)lm * a.ld + k;
-      const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
-      a.expl1[o] = e0;
-      v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
-      v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
-      if (k == 0) v = a.top ? a.top[lm] : zero;
-      if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
-    }
-    f[idx] = v;
-  }
+  build_rhs<false, 3>(a, l, mc0, rows, nrow, f);
   __syncthreads();
-  const Slot s = slot_of<kStaged>(n_r);
+  const Slot s = slot_of(n_r, a.groups);
   double2 acc[kRows][2];
   solve_tile<kStaged>(Ml, n_r, ldm, f, mbuf, s, acc);
   __syncthreads();
@@ -261,7 +312,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_update_field(UsArgs a) {
 }
 
 struct PwArgs {
-  int n_r, ldm, l_max, minc, n_m;
+  int n_r, ldm, l_max, minc, n_m, groups;
   const int* lstart;
   double2 *w, *dw, *ddw, *old, *impl, *expl0, *expl1, *p;
   const double2 *s, *xi;
@@ -277,44 +328,24 @@ struct PwArgs {
 // same tiling as k_update_field; the CTA holding (l, m) = (0, 0) also solves
 // the l = 0 pressure (update_wp.py:173-194).
 template <bool kStaged>
-__global__ void __launch_bounds__(kMaxThreads) k_update_poloidal(PwArgs a) {
-  constexpr int kCtaRows = Tile<kStaged>::kCtaRows;
+__global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 2>::kBlocks)
+    k_update_poloidal(PwArgs a) {
   extern __shared__ __align__(16) double2 pwbuf[];
-  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * kCtaRows;
-  const int nrow = cta_rows(mc0, kCtaRows, l, a.minc, a.n_m);
+  const int rows = a.groups * kRows;
+  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * rows;
+  const int nrow = cta_rows(mc0, rows, l, a.minc, a.n_m);
   if (nrow == 0) return;
-  double2* f = pwbuf;                      // [kCtaRows][n_r]: rhs, then w
-  double2* dd = pwbuf + kCtaRows * n_r;    // [kCtaRows][n_r]: D2 w
-  double* mbuf = (double*)(pwbuf + 2 * kCtaRows * n_r);
+  double2* f = pwbuf;                  // [rows][n_r]: rhs, then w
+  double2* dd = pwbuf + rows * n_r;    // [rows][n_r]: D2 w
+  double* mbuf = (double*)(pwbuf + 2 * rows * n_r);
   const double* Ml = a.mt + (int64_t)l * n_r * ldm;
   if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
   auto lm_of = [&](int row) { return __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc); };
-  for (int idx = threadIdx.x; idx < kCtaRows * n_r; idx += blockDim.x) {
-    const int row = idx / n_r, k = idx - row * n_r;
-    double2 v = zero;
-    if (row < nrow) {
-      const int64_t o = (int64_t)lm_of(row) * a.ld + k;
-      const double2 ol = a.old[o], im = a.impl[o], e0 = a.expl0[o], e1 = a.expl1[o];
-      a.expl1[o] = e0;
-      v.x = a.w_old * ol.x + a.w_impl * im.x + a.w_expl0 * e0.x + a.w_expl1 * e1.x;
-      v.y = a.w_old * ol.y + a.w_impl * im.y + a.w_expl0 * e0.y + a.w_expl1 * e1.y;
-      const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
-      const double2 sv = a.s[o];
-      v.x += gb * a.BuoFac * sv.x;
-      v.y += gb * a.BuoFac * sv.y;
-      if (a.xi) {
-        const double2 xv = a.xi[o];
-        v.x += gb * a.ChemFac * xv.x;
-        v.y += gb * a.ChemFac * xv.y;
-      }
-      if (k < 2 || k > n_r - 3 || l == 0) v = zero;
-    }
-    f[idx] = v;
-  }
+  build_rhs<true, 2>(a, l, mc0, rows, nrow, f);
   __syncthreads();
-  const Slot s = slot_of<kStaged>(n_r);
+  const Slot s = slot_of(n_r, a.groups);
   double2 acc[kRows][2];
   solve_tile<kStaged>(Ml, n_r, ldm, f, mbuf, s, acc);
   __syncthreads();
@@ -368,6 +399,23 @@ __global__ void __launch_bounds__(kMaxThreads) k_update_poloidal(PwArgs a) {
       const double c3 = a.c3[j], c2 = a.c2n[j] - 2.0 * dLo, c1 = a.c1n[j] + dL * a.c1d[j];
       const double c0 = dLo * (a.c0n[j] + dLo);
       const double fd = -hd * dLo * a.visc[j] * orho1, gb = dLo * a.rgrav[j];
+      // couplings of all rows loaded before the stores, so the loads overlap
+      double2 cpl[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int row = s.rg * kRows + r;
+        cpl[r] = zero;
+        if (row < nrow) {
+          const int64_t o = (int64_t)lm_of(row) * a.ld + j;
+          const double2 sv = a.s[o];
+          cpl[r] = double2{a.BuoFac * gb * sv.x, a.BuoFac * gb * sv.y};
+          if (a.xi) {
+            const double2 xv = a.xi[o];
+            cpl[r].x += a.ChemFac * gb * xv.x;
+            cpl[r].y += a.ChemFac * gb * xv.y;
+          }
+        }
+      }
 #pragma unroll
       for (int r = 0; r < kRows; ++r) {
         const int row = s.rg * kRows + r;
@@ -378,17 +426,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_update_poloidal(PwArgs a) {
         a.old[o] = bnd ? zero
                        : double2{fo * (e2.x - beta * d1[r].x - dLo * v.x),
                                  fo * (e2.y - beta * d1[r].y - dLo * v.y)};
-        const double2 sv = a.s[o];
         double2 im;
-        im.x = fd * (d4[r].x + c3 * d3[r].x + c2 * e2.x + c1 * d1[r].x + c0 * v.x) +
-               a.BuoFac * gb * sv.x;
-        im.y = fd * (d4[r].y + c3 * d3[r].y + c2 * e2.y + c1 * d1[r].y + c0 * v.y) +
-               a.BuoFac * gb * sv.y;
-        if (a.xi) {
-          const double2 xv = a.xi[o];
-          im.x += a.ChemFac * gb * xv.x;
-          im.y += a.ChemFac * gb * xv.y;
-        }
+        im.x = fd * (d4[r].x + c3 * d3[r].x + c2 * e2.x + c1 * d1[r].x + c0 * v.x) + cpl[r].x;
+        im.y = fd * (d4[r].y + c3 * d3[r].y + c2 * e2.y + c1 * d1[r].y + c0 * v.y) + cpl[r].y;
         a.impl[o] = bnd ? zero : im;
       }
     }
@@ -411,6 +451,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_update_poloidal(PwArgs a) {
 // warp), shared memory = row buffers (+ the two staged matrix chunks).
 struct TileLaunch {
   bool staged;
+  int groups;
   dim3 grid;
   int threads;
   size_t smem;
@@ -418,10 +459,10 @@ struct TileLaunch {
 TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers) {
   TileLaunch t;
   t.staged = n_r <= kStagedMaxR;
-  const int groups = t.staged ? Tile<true>::kGroups : Tile<false>::kGroups;
-  const int rows = groups * kRows;
   const int n_jp = (n_r + 1) / 2;
-  t.threads = (groups * n_jp + 31) / 32 * 32;
+  t.groups = t.staged ? std::min(4, kStagedThreads / n_jp) : 1;
+  const int rows = t.groups * kRows;
+  t.threads = (t.groups * n_jp + 31) / 32 * 32;
   t.grid = dim3((n_m + rows - 1) / rows, l_max + 1);
   t.smem = (size_t)row_buffers * rows * n_r * sizeof(double2) +
            (t.staged ? (size_t)2 * kKc * ldm * sizeof(double) : 0);
@@ -521,6 +562,7 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1);
+  a.groups = t.groups;
   auto kern = t.staged ? k_update_field<true> : k_update_field<false>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
@@ -572,6 +614,7 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);
   const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 2);
+  a.groups = t.groups;
   auto kern = t.staged ? k_update_poloidal<true> : k_update_poloidal<false>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
