@@ -378,6 +378,30 @@ MT_API int mt_update_poloidal(const mt_plan* plan, int n_r, const mt_poloidal_up
                               const mt_lop* solve, const mt_radial_op* D1,
                               const mt_radial_op* D2, const mt_radial_op* P0, void* stream);
 
+/* ---- energy integrals of the outer core (FP64) ---------------------------
+ * magic_torch/output.py:101-180 (get_e_kin_full, get_e_mag_oc_full): with
+ * |x|^2 = Re^2 (m = 0) or 2 |x|^2 (m > 0) and L = l(l+1),
+ *   pol(lm, r) = cr[r] L (L or2[r] |pol|^2 + |dpol|^2),  tor(lm, r) = cr[r] L |tor|^2,
+ * out[0..3] = integral over r (weights rint[r]) of the sum over lm of pol
+ *             for all lm, m = 0, the equatorially symmetric lm, their m = 0 part;
+ * out[4..7] = the same for tor (the complementary parities);
+ * out[8..9] = sum over lm of l^2 (l+1) |pol(r = 0)|^2, all and m = 0 (magnetic
+ *             only; the caller scales by LFfac / (2 r_cmb)).
+ * Kinetic (magnetic = 0): pol = w, dpol = dw, tor = z, cr = orho1 / 2, symmetric
+ * parities pol (l+m) even, tor (l+m) odd; magnetic: b, db, aj, cr = LFfac / 2,
+ * the opposite parities.  rint: the radial rule as weights (n_r).  out: 10
+ * device doubles; work: mt_energy_workspace bytes of device memory. */
+typedef struct {
+  const double *pol, *dpol, *tor; /* (lm_max, n_r) complex, row stride ld */
+  int64_t ld;
+  const double *or2, *cr, *rint;  /* (n_r) device arrays */
+  int magnetic;
+} mt_energy_args;
+
+MT_API size_t mt_energy_workspace(const mt_plan* plan);
+MT_API int mt_energy(const mt_plan* plan, int n_r, const mt_energy_args* e, double* out,
+                     void* work, size_t work_bytes, void* stream);
+
 MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
 
 /* Thread-local message for the last non-zero status. */

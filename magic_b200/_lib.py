@@ -110,6 +110,11 @@ class PoloidalUpdate(C.Structure):
                                    "c2n", "c1n", "c1d", "c0n")]
 
 
+class EnergyArgs(C.Structure):
+    _fields_ = [(n, _dp) for n in ("pol", "dpol", "tor")] + [("ld", _i64)] + \
+               [(n, _dp) for n in ("or2", "cr", "rint")] + [("magnetic", C.c_int)]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "mt_plan_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
@@ -149,6 +154,9 @@ _PROTOS = {
     "mt_get_td": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TdIn), C.POINTER(TdOut),
                             C.POINTER(TdParams), C.c_void_p, _dp]),
     "mt_lop_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
+    "mt_energy_workspace": (C.c_size_t, [C.c_void_p]),
+    "mt_energy": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(EnergyArgs), _dp, _dp, C.c_size_t,
+                            _dp]),
     "mt_lop_destroy": (C.c_int, [C.c_void_p]),
     "mt_update_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FieldUpdate), C.c_void_p,
                                   C.c_void_p, C.c_void_p, _dp]),

@@ -273,6 +273,63 @@ def get_dddr(f, D1, D2, D3):
     return d1, d2, D3(f)
 
 
+def dct1_matrix(n_r):
+    """The self-inverse DCT-I of cosine_transform.py:18-45 as an n_r x n_r matrix:
+    y[k] = (f[0] + (-1)^k f[N] + 2 sum_{0<j<N} f[j] cos(pi j k / N)) / sqrt(2 N)."""
+    N = n_r - 1
+    k = np.arange(n_r)[:, None]
+    j = np.arange(n_r)[None, :]
+    C = 2.0 * np.cos(np.pi * j * k / N)
+    C[:, 0] = 1.0
+    C[:, N] = (-1.0) ** np.arange(n_r)
+    return C / np.sqrt(2.0 * N)
+
+
+def simpson_weights(r):
+    """Weights of the non-uniform Simpson rule of magic_torch/integration.py:73-121
+    (odd n_r: composite Simpson; even: the mean of the two Simpson sweeps closed by
+    a trapezoid at either end), integral = sum_r w[r] f[r], sign for r[0] = r_cmb."""
+    r = np.asarray(r, dtype=np.float64)
+    N = r.size
+    w = np.zeros(N)
+
+    def simpson(start, acc):
+        for n in range(start, N - 1, 2):
+            h1, h2 = r[n] - r[n - 1], r[n + 1] - r[n]
+            c = (h1 + h2) / 6.0
+            acc[n - 1] += c * (2.0 * h1 - h2) / h1
+            acc[n] += c * (h1 + h2) * (h1 + h2) / (h1 * h2)
+            acc[n + 1] += c * (2.0 * h2 - h1) / h2
+
+    if N % 2 == 1:
+        simpson(1, w)
+        return -w
+    w[0] += 0.5 * (r[1] - r[0])
+    w[1] += 0.5 * (r[1] - r[0])
+    simpson(2, w)
+    w[N - 1] += 0.5 * (r[N - 1] - r[N - 2])
+    w[N - 2] += 0.5 * (r[N - 1] - r[N - 2])
+    simpson(1, w)
+    return -0.5 * w
+
+
+def clenshaw_curtis_weights(n_r, radratio, rnorm, boundary_fac):
+    """Weights of the Chebyshev integration of magic_torch/integration.py:18-70:
+    DCT-I of f / drx (drx = 2 / (r_cmb - r_icb)), end coefficients times
+    boundary_fac, dotted with the Chebyshev integrals (1 for T_0, -1/((n+1)(n-1))
+    for even n > 0, 0 for odd n), times 2 rnorm."""
+    r_cmb = 1.0 / (1.0 - radratio)
+    r_icb = radratio / (1.0 - radratio)
+    drx = 2.0 / (r_cmb - r_icb)
+    ci = np.zeros(n_r)
+    ci[0] = 1.0
+    for n in range(2, n_r, 2):
+        ci[n] = -1.0 / ((n + 1) * (n - 1))
+    b = np.ones(n_r)
+    b[0] = b[-1] = boundary_fac
+    return 2.0 * rnorm / drx * ((ci * b) @ dct1_matrix(n_r))
+
+
 _DCT = {}
 
 
@@ -307,5 +364,9 @@ class RadialScheme:
             self.rMat, self.drMat, self.d2rMat = cheb_polynomials(n_r, radratio)
             # Chebyshev-coefficient unknowns (magic_torch/chebyshev.py:47-52)
             self.rnorm, self.boundary_fac = math.sqrt(2.0 / (n_r - 1)), 0.5
+        self.radratio = radratio
+        # radial integration rule as weights (magic_torch/integration.py:138)
+        self.rint = (clenshaw_curtis_weights(n_r, radratio, self.rnorm, self.boundary_fac)
+                     if self.chebyshev else simpson_weights(self.r))
         self.D1m, self.D2m, self.D3m = mats
         self.D1, self.D2, self.D3 = (RadialOp(M, device=device) for M in mats)

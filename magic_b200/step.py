@@ -61,25 +61,16 @@ class BoussinesqStep:
         self.prof = {k: t(v) for k, v in hp.items()}
         hdif = np.ones(l_max + 1)
         self.hdif = t(hdif)
-        # CNAB2 with a fixed step: solve operators for it, coefficients uploaded once
-        self.weights = I.cnab2_weights(dt, dt)
-        wl0 = self.weights[1]
+        self._hdif_np, self._ktopv, self._kbotv = hdif, ktopv, kbotv
         d1c = hp["beta"] + hp["dLtemp0"] + 2.0 * hp["or1"] + hp["dLkappa"]
-        self.ops = dict(
-            s=I.LOp(I.scalar_solve_operators(self.sch, l_max, wl0, self.opr, hdif, hp["kappa"],
-                                             d1c, hp["or2"]), device=dev),
-            z=I.LOp(I.toroidal_solve_operators(self.sch, l_max, wl0, hdif, hp["visc"],
-                                               hp["beta"], hp["dbeta"], hp["dLvisc"], hp["or1"],
-                                               hp["or2"], ktopv, kbotv), device=dev),
-            w=I.LOp(I.poloidal_dc_solve_operators(self.sch, l_max, wl0, hdif, hp, ktopv, kbotv),
-                    device=dev))
-        Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif, hp["lambda_"],
-                                            hp["dLlambda"], hp["or1"], hp["or2"])
-        self.ops["b"], self.ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
+        self._d1c = d1c
+        # CNAB2 weights and the per-degree solve operators of the current dt pair
+        self.dt = None
+        self.set_dt(dt, dt)
         self.P0 = RadialOp(I.p0_inverse(self.sch, hp["beta"]), device=dev)
         dev_coef = lambda c: {k: (t(v) if v is not None else None) for k, v in c.items()}
-        self.coef = dict(s=dev_coef(I.entropy_coefficients(l_max, self.opr, hdif, hp["kappa"], d1c,
-                                                           hp["or2"])),
+        self.coef = dict(s=dev_coef(I.entropy_coefficients(l_max, self.opr, hdif, hp["kappa"],
+                                                           self._d1c, hp["or2"])),
                          z=dev_coef(I.toroidal_coefficients(l_max, hdif, hp["visc"], hp["beta"],
                                                             hp["dbeta"], hp["dLvisc"], hp["or1"],
                                                             hp["or2"])))
@@ -101,6 +92,44 @@ class BoussinesqStep:
                                 device=dev)
         self.bots = torch.zeros(self.lm_max, dtype=_CD, device=dev)
         self.bots[0] = math.sqrt(4.0 * math.pi)  # fixed entropy at the inner boundary, l = m = 0
+
+    def set_dt(self, dt_new, dt_old):
+        """CNAB2 weights for the step dt_new after dt_old (time_scheme.py:56-73) and,
+        when the implicit weight changed, new solve operators (the reference's
+        build_all_matrices, step_time.py:1625-1627)."""
+        if self.dt == (float(dt_new), float(dt_old)):
+            return
+        self.dt = (float(dt_new), float(dt_old))
+        self.weights = I.cnab2_weights(*self.dt)
+        wl0 = self.weights[1]
+        if getattr(self, "_ops_wl0", None) == wl0:
+            return
+        hp, hdif, dev, l_max = self.hprof, self._hdif_np, self.device, self.l_max
+        self.ops = dict(
+            s=I.LOp(I.scalar_solve_operators(self.sch, l_max, wl0, self.opr, hdif, hp["kappa"],
+                                             self._d1c, hp["or2"]), device=dev),
+            z=I.LOp(I.toroidal_solve_operators(self.sch, l_max, wl0, hdif, hp["visc"],
+                                               hp["beta"], hp["dbeta"], hp["dLvisc"], hp["or1"],
+                                               hp["or2"], self._ktopv, self._kbotv), device=dev),
+            w=I.LOp(I.poloidal_dc_solve_operators(self.sch, l_max, wl0, hdif, hp, self._ktopv,
+                                                  self._kbotv), device=dev))
+        Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif, hp["lambda_"],
+                                            hp["dLlambda"], hp["or1"], hp["or2"])
+        self.ops["b"], self.ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
+        self._ops_wl0 = wl0
+
+    def energies(self):
+        """Kinetic and magnetic energies of the current state (EKin, EMagOC of
+        magic_torch/output.py:101-190), computed on the GPU in FP64."""
+        from .output import EnergyIntegrals
+
+        if not hasattr(self, "_energy"):
+            hp = self.hprof
+            self._energy = EnergyIntegrals(self.plan, hp["r"], hp["or2"], hp["orho1"],
+                                           self.sch.rint, self.LFfac)
+        f = self.f
+        return self._energy.kin(f["w"], f["dw"], f["z"]), self._energy.mag(f["b"], f["db"],
+                                                                           f["aj"])
 
     def init_random(self, seed=0, amp=1e-4):
         """Seeded random fields |c_lm| ~ amp (l+1)^-2 on the interior levels (m = 0

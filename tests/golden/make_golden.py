@@ -39,6 +39,23 @@ NL_CONFIGS = {
 }
 
 
+# whole CNAB2 steps of the finite-difference Boussinesq MHD dynamo
+# (fourth-order FD, double curl, insulating inner core, fixed entropy, no-slip)
+STEP_CONFIGS = {
+    "step_fd": {"l_max": 12, "minc": 1, "n_r_max": 13, "radial_scheme": "FD", "fd_order": 4,
+                "fd_order_bound": 2, "ek": 1e-3, "ra": 1e5, "pr": 1.0, "prmag": 5.0,
+                "dtmax": 1e-4, "mode": 0},
+}
+
+# energies of seeded spectra (output.py:101-180) and the radial rule
+ENERGY_CONFIGS = {
+    "energy_cheb": {"l_max": 8, "minc": 2, "n_r_max": 11, "prmag": 5.0, "ek": 1e-3},
+    "energy_fd": {"l_max": 12, "minc": 1, "n_r_max": 12, "radial_scheme": "FD", "fd_order": 4,
+                  "fd_order_bound": 2, "strat": 2.0, "polind": 2.0, "g0": 0.0, "g1": 0.0,
+                  "g2": 1.0, "mode": 0, "ek": 1e-4, "ra": 3e6},
+}
+
+
 def _spec(rng, lm_max, l_of_lm, B, decay=1.0):
     """Random complex spectrum with |c| ~ (l+1)^-decay."""
     amp = (l_of_lm.astype(np.float64) + 1.0) ** (-decay)
@@ -322,6 +339,107 @@ def worker_td(name, ref):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+def worker_energy(name, ref):
+    cfg = dict(ENERGY_CONFIGS[name], device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, blocking, radial_functions as rf, pre_calculations as pc
+    from magic_torch.radial_scheme import r as r_grid
+    from magic_torch.output import get_e_kin_full, get_e_mag_oc_full
+    from magic_torch.integration import rInt_R
+    n = lambda x: x.detach().cpu().numpy().copy()
+    rng = np.random.default_rng(99)
+    N, lm = params.n_r_max, params.lm_max
+    l_of = n(blocking.st_lm2l)
+    m_of = n(blocking.st_lm2m)
+    ins = {k: _spec(rng, lm, l_of, N) for k in ("w", "dw", "z", "b", "db", "aj")}
+    for k in ins:
+        ins[k][m_of == 0] = ins[k][m_of == 0].real
+    T = {k: torch.from_numpy(v) for k, v in ins.items()}
+    out = dict(n_r_max=N, l_max=params.l_max, minc=params.minc, lm_max=lm, lm2l=l_of, lm2m=m_of,
+               r=n(r_grid), or2=n(rf.or2), orho1=n(rf.orho1), LFfac=float(pc.LFfac),
+               radratio=float(params.radratio), chebyshev=int(params.radial_scheme != "FD"),
+               rint_w=n(rInt_R(torch.eye(N, dtype=torch.float64))),
+               e_kin=np.array(get_e_kin_full(T["w"], T["dw"], T["z"])),
+               e_mag=np.array(get_e_mag_oc_full(T["b"], T["db"], T["aj"])))
+    out.update({"in_" + k: v for k, v in ins.items()})
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def worker_step(name, ref):
+    """Reference state before and after two one_step calls, the reference's own
+    checkpoint dictionary layout (main.py:189-222), kinetic and magnetic
+    energies (output.py:101-180) and the radial integration weights."""
+    import json
+    import tempfile
+
+    cfg = dict(STEP_CONFIGS[name], device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, blocking, fields
+    from magic_torch.init_fields import initialize_fields
+    from magic_torch.step_time import setup_initial_state, one_step, initialize_dt
+    from magic_torch.main import save_checkpoint
+    from magic_torch.output import get_e_kin_full, get_e_mag_oc_full
+    from magic_torch.integration import rInt_R
+    from magic_torch.time_scheme import tscheme
+    n = lambda x: x.detach().cpu().numpy().copy()
+    N, lm = params.n_r_max, params.lm_max
+    initialize_fields()
+    # seeded perturbations on the interior levels (m = 0 real), so that every
+    # nonlinear and Coriolis term is active in the first step
+    g = torch.Generator().manual_seed(11)
+    m0 = blocking.st_lm2m == 0
+    for fld, amp in (("s_LMloc", 1e-3), ("w_LMloc", 1e-3), ("z_LMloc", 1e-3)):
+        c = torch.complex(torch.randn(lm, N, generator=g, dtype=torch.float64),
+                          torch.randn(lm, N, generator=g, dtype=torch.float64)) * amp
+        c[m0] = c[m0].real.to(c.dtype)
+        getattr(fields, fld)[:, 1:-1] += c[:, 1:-1]
+    setup_initial_state()
+    dt = float(cfg["dtmax"])
+    initialize_dt(dt)
+    out = dict(n_r_max=N, l_max=params.l_max, minc=params.minc, lm_max=lm, dt=dt,
+               ek=cfg["ek"], ra=cfg["ra"], pr=cfg["pr"], prmag=cfg["prmag"],
+               radratio=float(params.radratio), lm2l=n(blocking.st_lm2l),
+               lm2m=n(blocking.st_lm2m))
+    rint = rInt_R(torch.eye(N, dtype=torch.float64))
+    out["rint_w"] = n(rint)
+
+    def snapshot(tag, fields_only=None):
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "ck.pt")
+            save_checkpoint(path, 0, 0.0, {"tag": "golden"})
+            st = torch.load(path, weights_only=False)
+        if tag == "0":
+            out["ckpt_layout"] = json.dumps({k: (list(v.shape) if torch.is_tensor(v)
+                                                 else type(v).__name__)
+                                             for k, v in st.items()})
+        for k, v in st.items():
+            if not torch.is_tensor(v) or v.dim() < 2:
+                continue
+            if fields_only and k not in fields_only:
+                continue
+            out[tag + ":" + k] = n(v)
+        w, dw, z = fields.w_LMloc, fields.dw_LMloc, fields.z_LMloc
+        out[tag + ":e_kin"] = np.array(get_e_kin_full(w, dw, z))
+        out[tag + ":e_mag"] = np.array(get_e_mag_oc_full(fields.b_LMloc, fields.db_LMloc,
+                                                         fields.aj_LMloc))
+        out[tag + ":tscheme_dt"] = n(tscheme.dt)
+
+    snapshot("0")
+    for step in (1, 2):
+        dt_new = one_step(step, dt)
+        assert dt_new == dt, (dt_new, dt)
+        snapshot(str(step), fields_only=None if step == 2 else (
+            "fields.w_LMloc", "fields.z_LMloc", "fields.s_LMloc", "fields.b_LMloc",
+            "fields.aj_LMloc"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
@@ -333,11 +451,16 @@ def main():
             worker_sht(a.worker, a.ref)
         elif a.worker in TD_CONFIGS:
             worker_td(a.worker, a.ref)
+        elif a.worker in STEP_CONFIGS:
+            worker_step(a.worker, a.ref)
+        elif a.worker in ENERGY_CONFIGS:
+            worker_energy(a.worker, a.ref)
         else:
             worker_nl(a.worker, a.ref)
         return
     env = dict(os.environ, TORCHDYNAMO_DISABLE="1", MAGIC_DEVICE="cpu")
-    names = list(SHT_CONFIGS) + list(NL_CONFIGS) + list(TD_CONFIGS)
+    names = list(SHT_CONFIGS) + list(NL_CONFIGS) + list(TD_CONFIGS) + list(STEP_CONFIGS)
+    names += list(ENERGY_CONFIGS)
     if a.only:
         names = [x for x in names if x in a.only.split(",")]
     for name in names:

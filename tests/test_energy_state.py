@@ -1,0 +1,87 @@
+"""CPU checks of the energy oracle, the radial integration rules and the
+checkpoint layout, against the reference's own outputs
+(tests/golden/energy_*.npz, step_fd.npz)."""
+
+import json
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+from oracle import energy as oe
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("name", ["energy_cheb", "energy_fd"])
+def test_energy_oracle_matches_reference(name):
+    z = load_golden(name)
+    N = int(z["n_r_max"])
+    w = oe.cheb_weights(N, float(z["radratio"])) if z["chebyshev"] else oe.simps_weights(z["r"])
+    assert np.abs(w - z["rint_w"]).max() < 1e-15
+    ek = oe.e_kin_full(z["in_w"], z["in_dw"], z["in_z"], z["lm2l"], z["lm2m"], z["or2"],
+                       z["orho1"], w)
+    em = oe.e_mag_oc_full(z["in_b"], z["in_db"], z["in_aj"], z["lm2l"], z["lm2m"], z["or2"],
+                          float(z["LFfac"]), z["r"][0], w)
+    assert _rel(ek, z["e_kin"]) < 1e-15 and _rel(em, z["e_mag"]) < 1e-15
+
+
+@pytest.mark.parametrize("name", ["energy_cheb", "energy_fd"])
+def test_rint_weights_match_reference(name):
+    from magic_b200.radial import clenshaw_curtis_weights, simpson_weights
+
+    z = load_golden(name)
+    N = int(z["n_r_max"])
+    if z["chebyshev"]:
+        w = clenshaw_curtis_weights(N, float(z["radratio"]), np.sqrt(2.0 / (N - 1)), 0.5)
+    else:
+        w = simpson_weights(z["r"])
+    assert np.abs(w - z["rint_w"]).max() < 1e-15
+
+
+def test_energy_oracle_on_reference_steps():
+    """Energies of the reference's states before and after two steps."""
+    from magic_b200.radial import fd_grid
+
+    z = load_golden("step_fd")
+    N = int(z["n_r_max"])
+    r = fd_grid(N, float(z["radratio"]), 0.3, 0.1)
+    w = oe.simps_weights(r)
+    LFfac = 1.0 / (float(z["ek"]) * float(z["prmag"]))
+    for tag in ("0", "2"):
+        g = lambda k: z[f"{tag}:fields.{k}_LMloc"]
+        ek = oe.e_kin_full(g("w"), g("dw"), g("z"), z["lm2l"], z["lm2m"], 1.0 / r ** 2,
+                           np.ones(N), w)
+        em = oe.e_mag_oc_full(g("b"), g("db"), g("aj"), z["lm2l"], z["lm2m"], 1.0 / r ** 2,
+                              LFfac, r[0], w)
+        assert _rel(ek, z[tag + ":e_kin"]) < 1e-15
+        assert _rel(em, z[tag + ":e_mag"]) < 1e-15
+
+
+def test_checkpoint_layout_matches_reference():
+    """state_dict of a (host-side stand-in) step has the reference checkpoint's
+    keys, shapes and scalar types (magic_torch/main.py:189-222)."""
+    from magic_b200.state import state_dict
+
+    z = load_golden("step_fd")
+    lm, N = int(z["lm_max"]), int(z["n_r_max"])
+    zero = lambda: torch.zeros(lm, N, dtype=torch.complex128)
+    st = SimpleNamespace(
+        lm_max=lm, n_r=N, dt=(1e-4, 1e-4),
+        f={k: zero() for k in ("w", "dw", "ddw", "z", "dz", "s", "ds", "b", "db", "ddb", "aj",
+                               "dj", "ddj", "p")},
+        ta={e: {k: zero() for k in ("old", "impl", "expl0", "expl1")}
+            for e in ("s", "z", "w", "b", "j")})
+    d = state_dict(st, step=3, sim_time=0.5, cfg={"l_max": 12})
+    layout = json.loads(str(z["ckpt_layout"]))
+    assert set(d) == set(layout)
+    for k, v in layout.items():
+        if isinstance(v, list):
+            assert list(d[k].shape) == v, k
+        else:
+            assert type(d[k]).__name__ == v, k

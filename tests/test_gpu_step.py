@@ -52,3 +52,97 @@ def test_pure_diffusion_decays():
         a.step()
     torch.cuda.synchronize()
     assert _energy(a) < e0
+
+
+# ---- against the reference's own time steps -------------------------------
+
+STEP_FIELDS = ("w", "dw", "ddw", "z", "dz", "s", "ds", "b", "db", "ddb", "aj", "dj", "ddj")
+STEP_DT = {"s": "dsdt", "z": "dzdt", "w": "dwdt", "b": "dbdt", "j": "djdt"}
+
+
+def _golden_state(z, tag):
+    import numpy as np
+
+    return {k.split(":", 1)[1]: torch.as_tensor(np.ascontiguousarray(z[k]))
+            for k in z if k.startswith(tag + ":") and "." in k.split(":", 1)[1]} | {
+        "tscheme_dt": torch.as_tensor(z[tag + ":tscheme_dt"])}
+
+
+def _reference_run():
+    from conftest import load_golden
+    from magic_b200.state import load_state_dict
+    from magic_b200.step import BoussinesqStep
+
+    z = load_golden("step_fd")
+    st = BoussinesqStep(int(z["l_max"]), int(z["n_r_max"]), ek=float(z["ek"]), ra=float(z["ra"]),
+                        pr=float(z["pr"]), prmag=float(z["prmag"]), dt=float(z["dt"]),
+                        precision="fp64", radratio=float(z["radratio"]))
+    assert st.lm_max == int(z["lm_max"])
+    load_state_dict(st, _golden_state(z, "0"))
+    return z, st
+
+
+def test_two_steps_match_reference():
+    """Two whole CNAB2 steps (FP64 stage) from the reference's own initial state
+    (setup_initial_state after seeded perturbations of s, w and z) against the
+    reference's one_step results (tests/golden/step_fd.npz, l_max = 12, 13 FD4
+    levels, Ek 1e-3, Ra 1e5, Pm 5, dt 1e-4): every field the step evolves and
+    every time array, and the kinetic / magnetic energies.  Tolerance, relative
+    to each array's largest value: 1e-12 for the fields w, z, s, b, aj, the
+    l = 0 pressure and the energies (measured <= 4.3e-14); 1e-11 for the radial
+    derivatives and the time arrays (measured <= 1.5e-12 in the entropy's
+    implicit term): they apply D2 (and D4 through the double curl) to the new
+    fields of a state whose explicit terms reach 7e6."""
+    import numpy as np
+
+    z, st = _reference_run()
+    rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    st.step()
+    for k in ("w", "z", "s", "b", "aj"):
+        e = rel(st.f[k].cpu().numpy(), z[f"1:fields.{k}_LMloc"])
+        assert e < 1e-12, ("step 1", k, e)
+    st.step()
+    errs = {}
+    for k in STEP_FIELDS:
+        errs[k] = rel(st.f[k].cpu().numpy(), z[f"2:fields.{k}_LMloc"])
+    errs["p00"] = rel(st.f["p"][0].cpu().numpy(), z["2:fields.p_LMloc"][0])
+    for e, name in STEP_DT.items():
+        ta = st.ta[e]
+        errs[name + ".old"] = rel(ta["old"].cpu().numpy(), z[f"2:dt.{name}.old"][..., 0])
+        errs[name + ".impl"] = rel(ta["impl"].cpu().numpy(), z[f"2:dt.{name}.impl"][..., 0])
+        errs[name + ".expl0"] = rel(ta["expl0"].cpu().numpy(), z[f"2:dt.{name}.expl"][..., 0])
+        errs[name + ".expl1"] = rel(ta["expl1"].cpu().numpy(), z[f"2:dt.{name}.expl"][..., 1])
+    ek, em = st.energies()
+    errs["e_kin"] = rel(np.array(ek), z["2:e_kin"])
+    errs["e_mag"] = rel(np.array(em), z["2:e_mag"])
+    print({k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        tight = k in ("w", "z", "s", "b", "aj", "p00", "e_kin", "e_mag")
+        assert v < (1e-12 if tight else 1e-11), (k, v)
+
+
+def test_checkpoint_round_trip(tmp_path):
+    """save_checkpoint writes the reference's dictionary (main.py:189-222: the same
+    keys and shapes as the reference's own file) and load_checkpoint restores a
+    state that steps on identically."""
+    import json
+
+    from conftest import load_golden
+    from magic_b200.state import load_checkpoint, save_checkpoint
+
+    z, st = _reference_run()
+    st.step()
+    path = tmp_path / "ck.pt"
+    save_checkpoint(st, path, step=1, sim_time=1e-4, cfg={"l_max": 12})
+    saved = torch.load(path, weights_only=False)
+    layout = json.loads(str(load_golden("step_fd")["ckpt_layout"]))
+    assert set(saved) == set(layout)
+    for k, v in layout.items():
+        if isinstance(v, list):
+            assert list(saved[k].shape) == v, k
+    _, other = _reference_run()
+    assert load_checkpoint(other, path) == (1, 1e-4)
+    st.step()
+    other.step()
+    for k in STEP_FIELDS:
+        assert torch.equal(st.f[k], other.f[k]), k
