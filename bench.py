@@ -423,6 +423,7 @@ def run_step(args, rank, world):
                          clocks=clocks.summary())
         del st
         torch.cuda.empty_cache()
+    drift = measure_drift(args, dev, rank) if args.drift_steps > 0 else None
     if rank == 0:
         sp, fp = res["split"], res["fp64"]
         print(json.dumps({
@@ -436,7 +437,99 @@ def run_step(args, rank, world):
             "fp64_stage_steps_per_s": 1000.0 / fp["ms"], "split_over_fp64": fp["ms"] / sp["ms"],
             "breakdown_ms": {p: {k: res[p][k] for k in ("radial_loop_ms", "implicit_ms")}
                              for p in res},
-            "clocks": sp["clocks"]}), flush=True)
+            "clocks": sp["clocks"]} | ({"drift": drift} if drift else {})), flush=True)
+
+
+def run_serve(args, rank, world):
+    """Optional line: the ensemble stream (Poisson arrivals at 4 runs/s, l_max in
+    {32, 64, 85, 127}, n_r in {33, 49, 65}, Ek log-uniform [1e-4, 1e-3], Ra
+    log-uniform [1e5, 1e6], Pr 1, Pm 5, perturbation 1e-5, FD4 double-curl
+    Boussinesq MHD steps at dt 1e-4) served with continuous batching in split
+    precision: p50 / p99 per-step device latency and aggregate steps/s over the
+    serving wall time (value).  The same runs all arriving at once measure the
+    capacity.  Baseline: the FP64 stage one run at a time, eager: each run's
+    build time (host clock) and steps (device events) measured, then replayed
+    against the same arrival times (run i starts when it has arrived and run
+    i - 1 is done) for its stream wall time, and summed for its capacity."""
+    import dataclasses
+
+    from magic_b200.serve import EnsembleServer, latency_report, poisson_stream
+    from magic_b200.step import BoussinesqStep
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    specs = poisson_stream(args.serve_runs, rate=4.0, seed=rank, n_steps=args.serve_steps)
+    srv = EnsembleServer(device=dev)
+    with ClockSampler(dev) as clocks:
+        rep = latency_report(srv.serve(specs), srv.wall_s)
+    sat_specs = [dataclasses.replace(s, arrival=0.0) for s in specs]
+    srv = EnsembleServer(device=dev)
+    sat = latency_report(srv.serve(sat_specs), srv.wall_s)
+    finish, busy = 0.0, 0.0
+    for s in specs:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = BoussinesqStep(s.l_max, s.n_r, ek=s.ek, ra=s.ra, pr=s.pr, prmag=s.prmag, dt=s.dt,
+                            precision="fp64", device=dev)
+        st.init_random(seed=s.seed, amp=s.amp)
+        torch.cuda.synchronize()
+        build = time.perf_counter() - t0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(s.n_steps):
+            st.step()
+        e1.record()
+        torch.cuda.synchronize()
+        run_s = build + e0.elapsed_time(e1) / 1e3
+        finish = max(finish, s.arrival) + run_s
+        busy += run_s
+        del st
+    torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "ensemble aggregate steps/s (continuous batching), 1 B200",
+            "value": rep["steps_per_s"], "unit": "steps/s", "n_gpus": 1,
+            "higher_is_better": True, "p50_ms": rep["p50_ms"], "p99_ms": rep["p99_ms"],
+            "runs": rep["runs"], "steps": rep["steps"], "wall_s": rep["wall_s"],
+            "last_arrival_s": specs[-1].arrival,
+            "capacity": {"steps_per_s": sat["steps_per_s"], "p50_ms": sat["p50_ms"],
+                         "p99_ms": sat["p99_ms"], "wall_s": sat["wall_s"]},
+            "fp64_one_at_a_time": {"steps_per_s": rep["steps"] / finish, "wall_s": finish,
+                                   "capacity_steps_per_s": rep["steps"] / busy},
+            "dtype": "bf16x3/f32 stage, f64 rest", "data": "synthetic",
+            "config": {"workload": "ensemble stream: Poisson 4 runs/s, l_max 32-127, n_r 33-65, "
+                                   "FD4 Boussinesq MHD, dt 1e-4",
+                       "runs": args.serve_runs, "steps_per_run": args.serve_steps},
+            "clocks": clocks.summary()}), flush=True)
+
+
+def measure_drift(args, dev, rank):
+    """The split stage's drift from the FP64 stage: both run args.drift_steps whole
+    steps from the same seeded state; max over w, z, s, b, aj of |split - fp64| /
+    max |fp64| per field, and the largest relative difference of the four total
+    energies (kinetic / magnetic, poloidal / toroidal)."""
+    from magic_b200.step import BoussinesqStep
+
+    runs = []
+    for prec in ("fp64", "split"):
+        st = BoussinesqStep(L_MAX, args.levels, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
+                            precision=prec, device=dev)
+        st.init_random(seed=rank, amp=1e-4)
+        runs.append(st)
+    a, b = runs
+    for _ in range(args.drift_steps):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    fe = {k: ((a.f[k] - b.f[k]).abs().max() / a.f[k].abs().max()).item()
+          for k in ("w", "z", "s", "b", "aj")}
+    ea, eb = a.energies(), b.energies()
+    pairs = list(zip(ea[0][:2] + ea[1][:2], eb[0][:2] + eb[1][:2]))
+    return {"steps": args.drift_steps, "field_rel": fe, "field_rel_max": max(fe.values()),
+            "energy_rel_max": max(abs(x - y) / abs(x) for x, y in pairs),
+            "energies_fp64": {"e_kin_pol": ea[0][0], "e_kin_tor": ea[0][1],
+                              "e_mag_pol": ea[1][0], "e_mag_tor": ea[1][1]}}
 
 
 def run_reference(args, rank, world):
@@ -465,11 +558,18 @@ def main():
     ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
-    ap.add_argument("--workload", default="bouss", choices=["bouss", "anel", "td", "step"],
+    ap.add_argument("--workload", default="bouss",
+                    choices=["bouss", "anel", "td", "step", "serve"],
                     help="bouss: the headline Boussinesq MHD stage; anel: the fused anelastic "
                          "stage at l_max=383 (extra line, split precision); td: the explicit "
                          "time-derivative terms (get_td + finish_exp, FP64, extra line); "
-                         "step: whole CNAB2 time steps, split and FP64 stage (extra line)")
+                         "step: whole CNAB2 time steps, split and FP64 stage (extra line); "
+                         "serve: the ensemble stream, continuous batching (extra line)")
+    ap.add_argument("--serve-runs", type=int, default=64, help="serve: runs in the stream")
+    ap.add_argument("--serve-steps", type=int, default=200, help="serve: steps per run")
+    ap.add_argument("--drift-steps", type=int, default=0,
+                    help="step workload: also run both stages this many steps from one seeded "
+                         "state and report the split stage's drift from the FP64 one")
     ap.add_argument("--levels", type=int, default=N_R,
                     help="radial levels (profiling runs use fewer than the 97 of the workload)")
     args = ap.parse_args()
@@ -489,6 +589,9 @@ def main():
         return
     if args.workload == "step":
         run_step(args, rank, world)
+        return
+    if args.workload == "serve":
+        run_serve(args, rank, world)
         return
 
     torch.cuda.set_device(local)

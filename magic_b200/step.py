@@ -33,13 +33,21 @@ _CD = torch.complex128
 class BoussinesqStep:
     def __init__(self, l_max, n_r, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
                  precision="split", radratio=0.35, fd_order=4, fd_order_bound=2, ktopv=2,
-                 kbotv=2, device=None):
+                 kbotv=2, device=None, cache=None):
+        """cache: optional dict shared by several steps on one device; the read-only
+        parts that depend only on the grid and the dt pair (transform plan, radial
+        operators, per-degree solve operators) are taken from it or added to it, so
+        runs of the same shape share one resident copy."""
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         dev = self.device
-        self.plan = Plan(l_max, 1, precision=precision, device=dev)
-        self.sch = RadialScheme(n_r, "FD", radratio, fd_order=fd_order,
-                                fd_order_bound=fd_order_bound, device=dev)
+        self._cache = cache if cache is not None else {}
+        self._shape = (n_r, radratio, fd_order, fd_order_bound, str(dev))
+        self.plan = self._shared(("plan", l_max, precision, str(dev)),
+                                 lambda: Plan(l_max, 1, precision=precision, device=dev))
+        self.sch = self._shared(("sch",) + self._shape,
+                                lambda: RadialScheme(n_r, "FD", radratio, fd_order=fd_order,
+                                                     fd_order_bound=fd_order_bound, device=dev))
         self.l_max, self.n_r, self.lm_max = l_max, n_r, self.plan.lm_max
         # physical prefactors (magic_torch/pre_calculations.py:13-41)
         self.CorFac, self.LFfac = 1.0 / ek, 1.0 / (ek * prmag)
@@ -67,7 +75,8 @@ class BoussinesqStep:
         # CNAB2 weights and the per-degree solve operators of the current dt pair
         self.dt = None
         self.set_dt(dt, dt)
-        self.P0 = RadialOp(I.p0_inverse(self.sch, hp["beta"]), device=dev)
+        self.P0 = self._shared(("P0",) + self._shape,
+                               lambda: RadialOp(I.p0_inverse(self.sch, hp["beta"]), device=dev))
         dev_coef = lambda c: {k: (t(v) if v is not None else None) for k, v in c.items()}
         self.coef = dict(s=dev_coef(I.entropy_coefficients(l_max, self.opr, hdif, hp["kappa"],
                                                            self._d1c, hp["or2"])),
@@ -104,8 +113,18 @@ class BoussinesqStep:
         wl0 = self.weights[1]
         if getattr(self, "_ops_wl0", None) == wl0:
             return
+        key = ("ops", self.l_max, wl0, self.opr, self.opm, self._ktopv, self._kbotv) + self._shape
+        self.ops = self._shared(key, lambda: self._build_ops(wl0))
+        self._ops_wl0 = wl0
+
+    def _shared(self, key, build):
+        if key not in self._cache:
+            self._cache[key] = build()
+        return self._cache[key]
+
+    def _build_ops(self, wl0):
         hp, hdif, dev, l_max = self.hprof, self._hdif_np, self.device, self.l_max
-        self.ops = dict(
+        ops = dict(
             s=I.LOp(I.scalar_solve_operators(self.sch, l_max, wl0, self.opr, hdif, hp["kappa"],
                                              self._d1c, hp["or2"]), device=dev),
             z=I.LOp(I.toroidal_solve_operators(self.sch, l_max, wl0, hdif, hp["visc"],
@@ -115,8 +134,8 @@ class BoussinesqStep:
                                                   self._kbotv), device=dev))
         Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif, hp["lambda_"],
                                             hp["dLlambda"], hp["or1"], hp["or2"])
-        self.ops["b"], self.ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
-        self._ops_wl0 = wl0
+        ops["b"], ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
+        return ops
 
     def energies(self):
         """Kinetic and magnetic energies of the current state (EKin, EMagOC of
