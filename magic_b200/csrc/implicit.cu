@@ -35,7 +35,7 @@
 #include "radial_op.cuh"
 
 struct mt_lop {
-  int n_l = 0, n_r = 0, ldm = 0, device = 0;  // ldm: n_r rounded up to even
+  int n_l = 0, n_r = 0, ldm = 0, device = 0;  // ldm: j stride (>= n_r, multiple of 8)
   double* mt = nullptr;  // (n_l, n_r, ldm) transposed: mt[(l * n_r + k) * ldm + j] = M_l[j][k]
 };
 
@@ -56,6 +56,12 @@ struct Bounds {
   static constexpr int kThreads = kStaged ? kStagedThreads : kWideThreads;
   static constexpr int kBlocks = kStaged ? kMinBlocks : 1;
 };
+
+__device__ __forceinline__ void dmma_f64(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
 
 // thread = (row group rg: rows rg * kRows .. + kRows - 1, level pair jp: j = 2 jp, 2 jp + 1)
 struct Slot {
@@ -92,12 +98,13 @@ __device__ __forceinline__ void stage_chunk(const double* Ml, int n_r, int ldm, 
   cpa_commit();
 }
 
-// acc[r][h] += m.h * f_r[k] for the thread's 4 rows (broadcast from shared memory)
-__device__ __forceinline__ void fma_rows(double2 m, const double2* fr, int n_r, int k,
+// acc[r][h] += m.h * f_r[k] for the thread's 4 rows (row stride fs, broadcast
+// from shared memory)
+__device__ __forceinline__ void fma_rows(double2 m, const double2* fr, int fs, int k,
                                          double2 (&acc)[kRows][2]) {
 #pragma unroll
   for (int r = 0; r < kRows; ++r) {
-    const double2 v = fr[r * n_r + k];
+    const double2 v = fr[r * fs + k];
     acc[r][0].x = fma(m.x, v.x, acc[r][0].x);
     acc[r][0].y = fma(m.x, v.y, acc[r][0].y);
     acc[r][1].x = fma(m.y, v.x, acc[r][1].x);
@@ -105,52 +112,105 @@ __device__ __forceinline__ void fma_rows(double2 m, const double2* fr, int n_r, 
   }
 }
 
-// acc[r][h] = (M_l f_{rg kRows + r})[2 jp + h].  Staged: chunk 0 was issued by
-// the caller; every thread of the CTA must call this (barriers inside), and
-// the call ends with a barrier.  Wide: M_l read from global memory.
-template <bool kStaged>
-__device__ __forceinline__ void solve_tile(const double* __restrict__ Ml, int n_r, int ldm,
-                                           const double2* f, double* mbuf, const Slot& s,
-                                           double2 (&acc)[kRows][2]) {
+// Wide tiling: acc[r][h] = (M_l f_{rg kRows + r})[2 jp + h], M_l read from
+// global memory (L2) as 16-byte level pairs.
+__device__ __forceinline__ void solve_tile_wide(const double* __restrict__ Ml, int n_r, int ldm,
+                                                int fs, const double2* f, const Slot& s,
+                                                double2 (&acc)[kRows][2]) {
 #pragma unroll
   for (int r = 0; r < kRows; ++r) acc[r][0] = acc[r][1] = double2{0.0, 0.0};
-  const double2* fr = f + s.rg * kRows * n_r;
-  if constexpr (!kStaged) {
-    if (!s.active) return;
-    const double* mp = Ml + 2 * s.jp;
+  if (!s.active) return;
+  const double2* fr = f + s.rg * kRows * fs;
+  const double* mp = Ml + 2 * s.jp;
 #pragma unroll 8
-    for (int k = 0; k < n_r; ++k)
-      fma_rows(__ldg((const double2*)(mp + (int64_t)k * ldm)), fr, n_r, k, acc);
-  } else {
-    const int nch = (n_r + kKc - 1) / kKc;
-    for (int c = 0; c < nch; ++c) {
-      if (c + 1 < nch) {
-        stage_chunk(Ml, n_r, ldm, c + 1, mbuf + ((c + 1) & 1) * kKc * ldm);
-        cpa_wait<1>();
-      } else {
-        cpa_wait<0>();
-      }
-      __syncthreads();
-      if (s.active) {
-        const double* mp = mbuf + (c & 1) * kKc * ldm + 2 * s.jp;
-        const double2* fc = fr + c * kKc;
-        const int nk = n_r - c * kKc;
-        if (nk >= kKc) {
+  for (int k = 0; k < n_r; ++k)
+    fma_rows(__ldg((const double2*)(mp + (int64_t)k * ldm)), fr, fs, k, acc);
+}
+
+// Staged tiling on the FP64 tensor pipe (mma.sync m8n8k4 f64): the CTA's
+// right-hand sides as real rows (row 2 o + p = part p of order o; m-tile t =
+// row group t = orders 4 t .. 4 t + 3) times M_l^T (n-tile = 8 output levels),
+// K = the levels k in 4-wide steps.  M_l streams through shared memory in
+// chunks of kKc rows (chunk 0 issued by the caller before the right-hand
+// sides; double-buffered cp.async); warp w owns n-tiles w, w + nwarps, ...
+// (at most kNt) for every m-tile, so each B fragment feeds all m-tiles and each
+// A fragment all of the warp's n-tiles.  Padding: A is zero for k >= n_r, B for
+// rows past the chunk; M_l's columns past n_r are stored as zeros.  Every
+// thread of the CTA calls this (barriers inside).  The new field is written
+// back over the right-hand sides in f (row stride fs), imaginary parts of
+// m = 0 dropped.
+//
+// Fragments (PTX m8n8k4 .f64): A row-major 8x4, lane holds A[lane/4][lane%4];
+// B col-major 4x8, lane holds B[lane%4][lane/4]; C/D 8x8, lane holds
+// D[lane/4][2 (lane%4) + h], h = 0, 1.
+template <int kNt>
+__device__ __forceinline__ void solve_tile_dmma(const double* __restrict__ Ml, int n_r, int ldm,
+                                                int fs, double2* f, double* mbuf, int groups,
+                                                int mc0) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int nt_n = (n_r + 7) >> 3;
+  const int ar = lane >> 2, ac = lane & 3;
+  double acc[kNt][4][2];
 #pragma unroll
-          for (int kk = 0; kk < kKc; ++kk)
-            fma_rows(*(const double2*)(mp + kk * ldm), fc, n_r, kk, acc);
-        } else {
-          for (int kk = 0; kk < nk; ++kk)
-            fma_rows(*(const double2*)(mp + kk * ldm), fc, n_r, kk, acc);
+  for (int i = 0; i < kNt; ++i)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) acc[i][t][0] = acc[i][t][1] = 0.0;
+  double* fd = reinterpret_cast<double*>(f);
+  // A element of m-tile t at k: order 4 t + ar / 2, part ar % 2
+  const int a_off = (ar >> 1) * fs * 2 + (ar & 1);
+  const int nch = (n_r + kKc - 1) / kKc;
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) {
+      stage_chunk(Ml, n_r, ldm, c + 1, mbuf + ((c + 1) & 1) * kKc * ldm);
+      cpa_wait<1>();
+    } else {
+      cpa_wait<0>();
+    }
+    __syncthreads();
+    const double* mb = mbuf + (c & 1) * kKc * ldm;
+    const int k0 = c * kKc;
+#pragma unroll
+    for (int q = 0; q < kKc / 4; ++q) {
+      const int kk = 4 * q + ac, k = k0 + kk;
+      const bool kin = k < n_r;
+      double av[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        av[t] = (t < groups && kin) ? fd[a_off + (4 * t * fs + k) * 2] : 0.0;
+#pragma unroll
+      for (int i = 0; i < kNt; ++i) {
+        const int nt = warp + i * nwarp;
+        if (nt < nt_n) {
+          const double bv = kin ? mb[kk * ldm + 8 * nt + ar] : 0.0;
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+            if (t < groups) dmma_f64(acc[i][t], av[t], bv);
         }
       }
-      __syncthreads();
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < kNt; ++i) {
+    const int nt = warp + i * nwarp;
+    if (nt >= nt_n) continue;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (t >= groups) continue;
+      const int o = 4 * t + (ar >> 1), p = ar & 1;
+      const bool drop = p && mc0 + o == 0;  // m = 0: real
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = 8 * nt + 2 * ac + h;
+        if (j < n_r) fd[(o * fs + j) * 2 + p] = drop ? 0.0 : acc[i][t][h];
+      }
     }
   }
 }
 
-// acc[r] = (D f_r)[j] for a banded radial operator, coefficients shared by the rows
-__device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int n_r, int j,
+// acc[r] = (D f_r)[j] for a banded radial operator, coefficients shared by the
+// rows (row stride fs)
+__device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int fs, int j,
                                         double2 (&acc)[kRows]) {
   const int k0 = __ldg(op.k0 + j);
 #pragma unroll
@@ -159,7 +219,7 @@ __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int 
     const double c = __ldg(op.vals + (int64_t)kk * op.n_r + j);
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
-      const double2 v = f[r * n_r + k0 + kk];
+      const double2 v = f[r * fs + k0 + kk];
       acc[r].x = fma(c, v.x, acc[r].x);
       acc[r].y = fma(c, v.y, acc[r].y);
     }
@@ -167,7 +227,7 @@ __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int 
 }
 
 struct UsArgs {
-  int n_r, ldm, l_max, minc, n_m, groups;
+  int n_r, ldm, fs, l_max, minc, n_m, groups;
   const int* lstart;
   double2 *x, *dx, *d2x, *old, *impl, *expl0, *expl1;
   const double2 *top, *bot;
@@ -185,7 +245,7 @@ __device__ __forceinline__ int cta_rows(int mc0, int rows, int l, int minc, int 
   return max(0, min(n, l / minc - mc0 + 1));
 }
 
-// CNAB2 right-hand sides of the CTA's rows into f ([rows][n_r], zero for
+// CNAB2 right-hand sides of the CTA's rows into f ([rows][fs], zero for
 // rows past nrow), with expl1 <- expl0.  kLd elements per thread are loaded
 // before any store, so their HBM latencies overlap (the stores may alias the
 // next loads as far as the compiler knows).  The poloidal form adds
@@ -243,56 +303,90 @@ __device__ __forceinline__ void build_rhs(const A& a, int l, int mc0, int rows, 
           if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
         }
       }
-      f[idx] = v;
+      f[row * a.fs + k] = v;
     }
   }
 }
 
-template <bool kStaged>
-__global__ void __launch_bounds__(Bounds<kStaged, 3>::kThreads, Bounds<kStaged, 3>::kBlocks)
-    k_update_field(UsArgs a) {
-  extern __shared__ __align__(16) double2 usbuf[];
-  const int rows = a.groups * kRows;
-  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * rows;
-  const int nrow = cta_rows(mc0, rows, l, a.minc, a.n_m);
-  if (nrow == 0) return;
-  double2* f = usbuf;                            // [rows][n_r]: rhs, then x
-  double* mbuf = (double*)(usbuf + rows * n_r);  // staged: [2][kKc][ldm]
-  const double* Ml = a.mt + (int64_t)l * n_r * ldm;
-  if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
-  auto lm_of = [&](int row) { return __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc); };
-  build_rhs<false, 3>(a, l, mc0, rows, nrow, f);
-  __syncthreads();
-  const Slot s = slot_of(n_r, a.groups);
-  double2 acc[kRows][2];
-  solve_tile<kStaged>(Ml, n_r, ldm, f, mbuf, s, acc);
-  __syncthreads();
-  if (s.active) {
+// the new field of the CTA's rows into f (row stride fs) and out: staged
+// tiling on the tensor pipe, wide tiling with FMAs; returns after a barrier
+template <bool kStaged, int kNt>
+__device__ __forceinline__ void solve_rows_to(const double* __restrict__ Ml, int n_r, int ldm,
+                                              int fs, double2* f, double* mbuf, int groups,
+                                              int mc0, const Slot& s, int nrow,
+                                              double2* __restrict__ out, int64_t ld,
+                                              const int* lm) {
+  if constexpr (kStaged) {
+    solve_tile_dmma<kNt>(Ml, n_r, ldm, fs, f, mbuf, groups, mc0);
+    __syncthreads();
+    if (s.active) {
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int row = s.rg * kRows + r;
+      for (int r = 0; r < kRows; ++r) {
+        const int row = s.rg * kRows + r;
+        if (row >= nrow) break;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int j = 2 * s.jp + h;
-        if (j >= n_r) continue;
-        double2 v = acc[r][h];
-        if (mc0 + row == 0) v.y = 0.0;  // m = 0
-        f[row * n_r + j] = v;
-        if (row < nrow) a.x[(int64_t)lm_of(row) * a.ld + j] = v;
+        for (int h = 0; h < 2; ++h) {
+          const int j = 2 * s.jp + h;
+          if (j < n_r) out[(int64_t)lm[row] * ld + j] = f[row * fs + j];
+        }
+      }
+    }
+  } else {
+    double2 acc[kRows][2];
+    solve_tile_wide(Ml, n_r, ldm, fs, f, s, acc);
+    __syncthreads();
+    if (s.active) {
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        const int row = s.rg * kRows + r;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = 2 * s.jp + h;
+          if (j >= n_r) continue;
+          double2 v = acc[r][h];
+          if (mc0 + row == 0) v.y = 0.0;  // m = 0
+          f[row * fs + j] = v;
+          if (row < nrow) out[(int64_t)lm[row] * ld + j] = v;
+        }
       }
     }
   }
   __syncthreads();
+}
+
+template <bool kStaged, int kNt>
+__global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
+                                  Bounds<kStaged, kNt == 2 ? 3 : 2>::kBlocks)
+    k_update_field(UsArgs a) {
+  extern __shared__ __align__(16) double2 usbuf[];
+  __shared__ int lm_row[16];
+  const int rows = a.groups * kRows;
+  const int n_r = a.n_r, ldm = a.ldm, fs = a.fs, l = blockIdx.y, mc0 = blockIdx.x * rows;
+  const int nrow = cta_rows(mc0, rows, l, a.minc, a.n_m);
+  if (nrow == 0) return;
+  double2* f = usbuf;                           // [rows][fs]: rhs, then x
+  double* mbuf = (double*)(usbuf + rows * fs);  // staged: [2][kKc][ldm]
+  const double* Ml = a.mt + (int64_t)l * n_r * ldm;
+  if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
+  if (threadIdx.x < rows)
+    lm_row[threadIdx.x] = threadIdx.x < nrow
+        ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
+  build_rhs<false, 3>(a, l, mc0, rows, nrow, f);
+  __syncthreads();
+  const Slot s = slot_of(n_r, a.groups);
+  solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.x, a.ld,
+                              lm_row);
   if (!s.active) return;
+  auto lm_of = [&](int row) { return lm_row[row]; };
   const double so_l = a.so_l ? a.so_l[l] : 1.0, ia_l = a.ia_l[l], ic_l = a.ic_l[l];
-  const double2* fr = f + s.rg * kRows * n_r;
+  const double2* fr = f + s.rg * kRows * fs;
 #pragma unroll 1
   for (int h = 0; h < 2; ++h) {
     const int j = 2 * s.jp + h;
     if (j >= n_r) break;
     double2 d1[kRows], d2[kRows];
-    op_rows(a.D1, fr, n_r, j, d1);
-    op_rows(a.D2, fr, n_r, j, d2);
+    op_rows(a.D1, fr, fs, j, d1);
+    op_rows(a.D2, fr, fs, j, d2);
     const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
     const double c1 = a.ib_r[j], c0 = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
     const double ia = ia_l * a.ia_r[j];
@@ -301,7 +395,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 3>::kThreads, Bounds<kStaged, 
       const int row = s.rg * kRows + r;
       if (row >= nrow) break;
       const int64_t o = (int64_t)lm_of(row) * a.ld + j;
-      const double2 v = fr[r * n_r + j];
+      const double2 v = fr[r * fs + j];
       a.dx[o] = d1[r];
       if (a.d2x) a.d2x[o] = d2[r];
       a.old[o] = double2{so * v.x, so * v.y};
@@ -312,7 +406,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 3>::kThreads, Bounds<kStaged, 
 }
 
 struct PwArgs {
-  int n_r, ldm, l_max, minc, n_m, groups;
+  int n_r, ldm, fs, l_max, minc, n_m, groups;
   const int* lstart;
   double2 *w, *dw, *ddw, *old, *impl, *expl0, *expl1, *p;
   const double2 *s, *xi;
@@ -327,57 +421,44 @@ struct PwArgs {
 // Double-curl poloidal update (magic_torch/update_w_doublecurl.py:393-483):
 // same tiling as k_update_field; the CTA holding (l, m) = (0, 0) also solves
 // the l = 0 pressure (update_wp.py:173-194).
-template <bool kStaged>
+template <bool kStaged, int kNt>
 __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 2>::kBlocks)
     k_update_poloidal(PwArgs a) {
   extern __shared__ __align__(16) double2 pwbuf[];
+  __shared__ int lm_row[16];
   const int rows = a.groups * kRows;
-  const int n_r = a.n_r, ldm = a.ldm, l = blockIdx.y, mc0 = blockIdx.x * rows;
+  const int n_r = a.n_r, ldm = a.ldm, fs = a.fs, l = blockIdx.y, mc0 = blockIdx.x * rows;
   const int nrow = cta_rows(mc0, rows, l, a.minc, a.n_m);
   if (nrow == 0) return;
-  double2* f = pwbuf;                  // [rows][n_r]: rhs, then w
-  double2* dd = pwbuf + rows * n_r;    // [rows][n_r]: D2 w
-  double* mbuf = (double*)(pwbuf + 2 * rows * n_r);
+  double2* f = pwbuf;                 // [rows][fs]: rhs, then w
+  double2* dd = pwbuf + rows * fs;    // [rows][fs]: D2 w
+  double* mbuf = (double*)(pwbuf + 2 * rows * fs);
   const double* Ml = a.mt + (int64_t)l * n_r * ldm;
   if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
-  auto lm_of = [&](int row) { return __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc); };
+  if (threadIdx.x < rows)
+    lm_row[threadIdx.x] = threadIdx.x < nrow
+        ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
+  auto lm_of = [&](int row) { return lm_row[row]; };
   build_rhs<true, 2>(a, l, mc0, rows, nrow, f);
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
-  double2 acc[kRows][2];
-  solve_tile<kStaged>(Ml, n_r, ldm, f, mbuf, s, acc);
-  __syncthreads();
-  if (s.active) {
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      const int row = s.rg * kRows + r;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int j = 2 * s.jp + h;
-        if (j >= n_r) continue;
-        double2 v = acc[r][h];
-        if (mc0 + row == 0) v.y = 0.0;
-        f[row * n_r + j] = v;
-        if (row < nrow) a.w[(int64_t)lm_of(row) * a.ld + j] = v;
-      }
-    }
-  }
-  __syncthreads();
-  const double2* fr = f + s.rg * kRows * n_r;
-  double2* dr = dd + s.rg * kRows * n_r;
+  solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.w, a.ld,
+                              lm_row);
+  const double2* fr = f + s.rg * kRows * fs;
+  double2* dr = dd + s.rg * kRows * fs;
   if (s.active) {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int j = 2 * s.jp + h;
       if (j >= n_r) break;
       double2 d2[kRows];
-      op_rows(a.D2, fr, n_r, j, d2);
+      op_rows(a.D2, fr, fs, j, d2);
 #pragma unroll
       for (int r = 0; r < kRows; ++r) {
         const int row = s.rg * kRows + r;
-        dr[r * n_r + j] = d2[r];
+        dr[r * fs + j] = d2[r];
         if (row < nrow) a.ddw[(int64_t)lm_of(row) * a.ld + j] = d2[r];
       }
     }
@@ -390,9 +471,9 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
       const int j = 2 * s.jp + h;
       if (j >= n_r) break;
       double2 d1[kRows], d3[kRows], d4[kRows];
-      op_rows(a.D1, fr, n_r, j, d1);
-      op_rows(a.D1, dr, n_r, j, d3);
-      op_rows(a.D2, dr, n_r, j, d4);
+      op_rows(a.D1, fr, fs, j, d1);
+      op_rows(a.D1, dr, fs, j, d3);
+      op_rows(a.D2, dr, fs, j, d4);
       const bool bnd = j == 0 || j == n_r - 1;
       const double or2 = a.or2[j], orho1 = a.orho1[j], beta = a.beta[j];
       const double dLo = dL * or2, fo = -dLo * orho1;
@@ -421,7 +502,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
         const int row = s.rg * kRows + r;
         if (row >= nrow) break;
         const int64_t o = (int64_t)lm_of(row) * a.ld + j;
-        const double2 v = fr[r * n_r + j], e2 = dr[r * n_r + j];
+        const double2 v = fr[r * fs + j], e2 = dr[r * fs + j];
         a.dw[o] = d1[r];
         a.old[o] = bnd ? zero
                        : double2{fo * (e2.x - beta * d1[r].x - dLo * v.x),
@@ -451,7 +532,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
 // warp), shared memory = row buffers (+ the two staged matrix chunks).
 struct TileLaunch {
   bool staged;
-  int groups;
+  int groups, fs, nt;  // row groups, row stride of the shared rows, n-tiles per warp
   dim3 grid;
   int threads;
   size_t smem;
@@ -464,7 +545,12 @@ TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers) {
   const int rows = t.groups * kRows;
   t.threads = (t.groups * n_jp + 31) / 32 * 32;
   t.grid = dim3((n_m + rows - 1) / rows, l_max + 1);
-  t.smem = (size_t)row_buffers * rows * n_r * sizeof(double2) +
+  // staged: rows 4 (mod 8) double2 apart, so the 8 rows x 4 levels of an A
+  // fragment fall on distinct bank pairs (two wavefronts, the minimum)
+  t.fs = t.staged ? n_r + ((4 - n_r) & 7) : n_r;
+  const int nt_n = (n_r + 7) / 8, nwarp = t.threads / 32;
+  t.nt = nt_n <= 2 * nwarp ? 2 : 4;
+  t.smem = (size_t)row_buffers * rows * t.fs * sizeof(double2) +
            (t.staged ? (size_t)2 * kKc * ldm * sizeof(double) : 0);
   return t;
 }
@@ -491,7 +577,11 @@ int mt_lop_create(int n_l, int n_r, const double* M, mt_lop** out) {
              "bad per-degree operator argument");
   *out = nullptr;
   const size_t per = (size_t)n_r * n_r;
-  const int ldm = n_r + (n_r & 1);
+  // j stride: a multiple of 8 (the tensor-pipe n-tiles read whole 8-level
+  // groups), 8 (mod 16) so that the 4 k rows of a B fragment fall on distinct
+  // bank halves
+  int ldm = (n_r + 7) / 8 * 8;
+  if (ldm % 16 == 0) ldm += 8;
   const size_t per_t = (size_t)n_r * ldm;
   std::vector<double> t(per_t * n_l, 0.0);
   for (int l = 0; l < n_l; ++l)
@@ -562,8 +652,12 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1);
+  MT_REQUIRE(!t.staged || (n_r + 7) / 8 <= t.nt * (t.threads / 32), MT_ERR_ARG,
+             "tile shape does not cover n_r");
   a.groups = t.groups;
-  auto kern = t.staged ? k_update_field<true> : k_update_field<false>;
+  a.fs = t.fs;
+  auto kern = !t.staged ? k_update_field<false, 2>
+                        : (t.nt == 2 ? k_update_field<true, 2> : k_update_field<true, 4>);
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
@@ -614,8 +708,12 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);
   const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 2);
+  MT_REQUIRE(!t.staged || (n_r + 7) / 8 <= t.nt * (t.threads / 32), MT_ERR_ARG,
+             "tile shape does not cover n_r");
   a.groups = t.groups;
-  auto kern = t.staged ? k_update_poloidal<true> : k_update_poloidal<false>;
+  a.fs = t.fs;
+  auto kern = !t.staged ? k_update_poloidal<false, 2>
+                        : (t.nt == 2 ? k_update_poloidal<true, 2> : k_update_poloidal<true, 4>);
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
