@@ -251,22 +251,27 @@ __device__ __forceinline__ int cta_rows(int mc0, int rows, int l, int minc, int 
 // next loads as far as the compiler knows).  The poloidal form adds
 // the buoyancy (and chemical) coupling and zeroes its boundary rows.
 template <bool kPol, int kLd, class A>
-__device__ __forceinline__ void build_rhs(const A& a, int l, int mc0, int rows, int nrow,
-                                          double2* f) {
-  const int n_r = a.n_r, total = rows * n_r;
+__device__ __forceinline__ void build_rhs(const A& a, int l, int rows, int nrow,
+                                          const int* lm_row, double2* f) {
+  const int n_r = a.n_r;
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
-  for (int base = threadIdx.x; base < total; base += kLd * blockDim.x) {
+  // thread t takes elements t, t + T, ... of the rows x n_r block: (row, k)
+  // advances by (T / n_r rows, T % n_r levels) with a carry, no division
+  const int T = blockDim.x, dr = T / n_r, dk = T - dr * n_r;
+  int row = threadIdx.x / n_r, k = threadIdx.x - row * n_r;
+  while (row < rows) {
     double2 ol[kLd], im[kLd], e0[kLd], e1[kLd], cs[kLd], cx[kLd];
     int64_t off[kLd];
+    int rr[kLd], kq[kLd];
 #pragma unroll
     for (int u = 0; u < kLd; ++u) {
-      const int idx = base + u * blockDim.x, row = idx / n_r;
+      rr[u] = row;
+      kq[u] = k;
       off[u] = -1;
       ol[u] = im[u] = e0[u] = e1[u] = cs[u] = cx[u] = zero;
-      if (idx < total && row < nrow) {
-        const int lm = __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc);
-        const int64_t o = (int64_t)lm * a.ld + (idx - row * n_r);
+      if (row < nrow) {
+        const int64_t o = (int64_t)lm_row[row] * a.ld + k;
         off[u] = o;
         ol[u] = a.old[o];
         im[u] = a.impl[o];
@@ -277,33 +282,38 @@ __device__ __forceinline__ void build_rhs(const A& a, int l, int mc0, int rows, 
           if (a.xi) cx[u] = a.xi[o];
         }
       }
+      row += dr;
+      k += dk;
+      if (k >= n_r) {
+        k -= n_r;
+        ++row;
+      }
     }
 #pragma unroll
     for (int u = 0; u < kLd; ++u) {
-      const int idx = base + u * blockDim.x;
-      if (idx >= total) break;
-      const int row = idx / n_r, k = idx - row * n_r;
+      if (rr[u] >= rows) break;
+      const int kk = kq[u];
       double2 v = zero;
       if (off[u] >= 0) {
         a.expl1[off[u]] = e0[u];
         v.x = a.w_old * ol[u].x + a.w_impl * im[u].x + a.w_expl0 * e0[u].x + a.w_expl1 * e1[u].x;
         v.y = a.w_old * ol[u].y + a.w_impl * im[u].y + a.w_expl0 * e0[u].y + a.w_expl1 * e1[u].y;
         if constexpr (kPol) {
-          const double gb = a.wimp_lin0 * dL * a.or2[k] * a.rgrav[k];
+          const double gb = a.wimp_lin0 * dL * a.or2[kk] * a.rgrav[kk];
           v.x += gb * a.BuoFac * cs[u].x;
           v.y += gb * a.BuoFac * cs[u].y;
           if (a.xi) {
             v.x += gb * a.ChemFac * cx[u].x;
             v.y += gb * a.ChemFac * cx[u].y;
           }
-          if (k < 2 || k > n_r - 3 || l == 0) v = zero;
+          if (kk < 2 || kk > n_r - 3 || l == 0) v = zero;
         } else {
-          const int lm = __ldg(a.lstart + mc0 + row) + (l - (mc0 + row) * a.minc);
-          if (k == 0) v = a.top ? a.top[lm] : zero;
-          if (k == n_r - 1) v = a.bot ? a.bot[lm] : zero;
+          const int lm = lm_row[rr[u]];
+          if (kk == 0) v = a.top ? a.top[lm] : zero;
+          if (kk == n_r - 1) v = a.bot ? a.bot[lm] : zero;
         }
       }
-      f[row * a.fs + k] = v;
+      f[rr[u] * a.fs + kk] = v;
     }
   }
 }
@@ -371,7 +381,8 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
   if (threadIdx.x < rows)
     lm_row[threadIdx.x] = threadIdx.x < nrow
         ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
-  build_rhs<false, 3>(a, l, mc0, rows, nrow, f);
+  __syncthreads();
+  build_rhs<false, 3>(a, l, rows, nrow, lm_row, f);
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
   solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.x, a.ld,
@@ -441,7 +452,8 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
     lm_row[threadIdx.x] = threadIdx.x < nrow
         ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
   auto lm_of = [&](int row) { return lm_row[row]; };
-  build_rhs<true, 2>(a, l, mc0, rows, nrow, f);
+  __syncthreads();
+  build_rhs<true, 2>(a, l, rows, nrow, lm_row, f);
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
   solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.w, a.ld,
