@@ -85,3 +85,66 @@ def test_checkpoint_layout_matches_reference():
             assert list(d[k].shape) == v, k
         else:
             assert type(d[k]).__name__ == v, k
+
+
+class _FakeStep:
+    """Host-side stand-in with the state layout of BoussinesqStep."""
+
+    def __init__(self, lm=6, n_r=5):
+        from collections import namedtuple
+
+        from magic_b200.output import EKin, EMagOC
+
+        self.lm_max, self.n_r, self.dt, self.count = lm, n_r, (1e-4, 1e-4), 0
+        self.device = torch.device("cpu")
+        z = lambda: torch.zeros(lm, n_r, dtype=torch.complex128)
+        self.f = {k: z() for k in ("w", "dw", "ddw", "z", "dz", "s", "ds", "b", "db", "ddb",
+                                   "aj", "dj", "ddj", "p")}
+        self.ta = {e: {k: z() for k in ("old", "impl", "expl0", "expl1")}
+                   for e in ("s", "z", "w", "b", "j")}
+        self._EKin, self._EMag = EKin, EMagOC
+
+    def step(self):
+        self.count += 1
+        self.f["w"] += 1.0
+
+    def energies(self):
+        c = float(self.count)
+        return (self._EKin(*[c + 0.125 * i for i in range(8)]),
+                self._EMag(*[-c - 0.25 * i for i in range(12)]))
+
+    def set_dt(self, a, b):
+        self.dt = (a, b)
+
+
+def test_run_outputs_follow_the_reference_layout(tmp_path):
+    """log.csv columns and cadence, Fortran-format energy lines and checkpoint
+    names of magic_torch/main.py:385-886 and output.py:304-319."""
+    import csv
+
+    from magic_b200.run import LOG_COLUMNS, run
+    from magic_b200.state import load_state_dict
+
+    st = _FakeStep()
+    t = run(st, 7, str(tmp_path), tag="x", log_every=3, checkpoint_every=4)
+    assert t == pytest.approx(7e-4)
+    rows = list(csv.reader(open(tmp_path / "log.csv")))
+    assert rows[0] == LOG_COLUMNS
+    assert [int(r[0]) for r in rows[1:]] == [0, 3, 6, 7]
+    assert float(rows[2][2]) == 3.0 and float(rows[2][4]) == -3.0
+    ek = open(tmp_path / "e_kin.x").read().splitlines()
+    em = open(tmp_path / "e_mag_oc.x").read().splitlines()
+    assert len(ek) == 4 and all(len(x) == 20 + 8 * 16 for x in ek)
+    assert len(em) == 4 and all(len(x) == 20 + 12 * 16 for x in em)
+    assert float(ek[1][:20]) == pytest.approx(3e-4) and float(ek[1][20:36]) == 3.0
+    assert sorted(p.name for p in tmp_path.glob("checkpoint_*.pt")) == [
+        "checkpoint_000004.pt", "checkpoint_000007.pt"]
+    other = _FakeStep()
+    assert load_state_dict(other, torch.load(tmp_path / "checkpoint_000004.pt",
+                                             weights_only=False)) == (4, pytest.approx(4e-4))
+    assert torch.equal(other.f["w"], torch.full_like(other.f["w"], 4.0))
+    # a restart appends: no new header, no step-0 row
+    run(other, 9, str(tmp_path), tag="x", log_every=3, start_step=4, sim_time=4e-4)
+    rows = list(csv.reader(open(tmp_path / "log.csv")))
+    assert [r[0] for r in rows].count("step") == 1
+    assert [int(r[0]) for r in rows[1:]] == [0, 3, 6, 7, 6, 9]

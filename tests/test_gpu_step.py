@@ -172,3 +172,36 @@ def test_split_stage_drift_after_500_steps():
     print(fe, ee)
     assert max(fe.values()) < 2e-7, fe
     assert ee < 1e-6, ee
+
+
+def test_run_outputs_and_restart(tmp_path):
+    """magic_b200.run from the reference's initial state: the energies logged
+    after two steps equal the reference's (its e_kin / e_mag_oc after two
+    one_step calls, to 1e-12), and a run restarted from its step-2 checkpoint
+    ends bit for bit where the uninterrupted run ends."""
+    import csv
+
+    import numpy as np
+
+    from magic_b200.run import run
+    from magic_b200.state import load_checkpoint
+
+    z, st = _reference_run()
+    run(st, 4, str(tmp_path / "a"), log_every=1, checkpoint_every=2)
+    rows = list(csv.reader(open(tmp_path / "a" / "log.csv")))
+    r2 = rows[3]
+    assert int(r2[0]) == 2
+    ek_ref, em_ref = z["2:e_kin"], z["2:e_mag"]
+    assert abs(float(r2[2]) - ek_ref[0]) <= 1e-12 * abs(ek_ref[0])
+    assert abs(float(r2[3]) - ek_ref[1]) <= 1e-12 * abs(ek_ref[1])
+    assert abs(float(r2[4]) - em_ref[0]) <= 1e-12 * abs(em_ref[0])
+    assert abs(float(r2[5]) - em_ref[1]) <= 1e-12 * abs(em_ref[1])
+    line = open(tmp_path / "a" / "e_kin.gpu").read().splitlines()[2]
+    vals = np.array([float(line[20 + 16 * i:36 + 16 * i]) for i in range(8)])
+    assert np.abs(vals - ek_ref).max() <= 1e-7 * np.abs(ek_ref).max()   # ES16.8 digits
+    _, other = _reference_run()
+    step, t = load_checkpoint(other, tmp_path / "a" / "checkpoint_000002.pt")
+    assert step == 2
+    run(other, 4, str(tmp_path / "a"), log_every=1, start_step=2, sim_time=t)
+    for k in STEP_FIELDS:
+        assert torch.equal(st.f[k], other.f[k]), k
