@@ -33,8 +33,11 @@ _CD = torch.complex128
 class BoussinesqStep:
     def __init__(self, l_max, n_r, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
                  precision="split", radratio=0.35, fd_order=4, fd_order_bound=2, ktopv=2,
-                 kbotv=2, device=None, cache=None):
-        """cache: optional dict shared by several steps on one device; the read-only
+                 kbotv=2, device=None, cache=None, minc=1):
+        """minc: azimuthal symmetry (orders m = 0, minc, 2 minc, ...; the grid covers
+        one sector of 2 pi / minc).
+
+        cache: optional dict shared by several steps on one device; the read-only
         parts that depend only on the grid and the dt pair (transform plan, radial
         operators, per-degree solve operators) are taken from it or added to it, so
         runs of the same shape share one resident copy."""
@@ -43,8 +46,8 @@ class BoussinesqStep:
         dev = self.device
         self._cache = cache if cache is not None else {}
         self._shape = (n_r, radratio, fd_order, fd_order_bound, str(dev))
-        self.plan = self._shared(("plan", l_max, precision, str(dev)),
-                                 lambda: Plan(l_max, 1, precision=precision, device=dev))
+        self.plan = self._shared(("plan", l_max, minc, precision, str(dev)),
+                                 lambda: Plan(l_max, minc, precision=precision, device=dev))
         self.sch = self._shared(("sch",) + self._shape,
                                 lambda: RadialScheme(n_r, "FD", radratio, fd_order=fd_order,
                                                      fd_order_bound=fd_order_bound, device=dev))

@@ -47,6 +47,18 @@ STEP_CONFIGS = {
                 "dtmax": 1e-4, "mode": 0},
 }
 
+# 500 CNAB2 steps of the Boussinesq MHD dynamo at the sizes of the CPU-runnable
+# shell case (l_max 32, minc 4, 33 levels, Ek 1e-3, Ra 1e5, Pr 1, Pm 5, dt 1e-4,
+# the reference's initial fields: l = m = 4 entropy mode of amplitude 0.1 and
+# its dipolar poloidal field, init_b1 = 3, amp_b1 = 5) with seeded Gaussian
+# noise of amplitude 1e-5 on the entropy; the radial scheme is fourth-order FD
+# (double curl), the form the GPU time step implements.
+RUN_CONFIGS = {
+    "run_fd_l32m4": ({"l_max": 32, "minc": 4, "n_r_max": 33, "radial_scheme": "FD",
+                      "fd_order": 4, "fd_order_bound": 2, "ek": 1e-3, "ra": 1e5, "pr": 1.0,
+                      "prmag": 5.0, "dtmax": 1e-4, "mode": 0}, 500, 1e-5),
+}
+
 # energies of seeded spectra (output.py:101-180) and the radial rule
 ENERGY_CONFIGS = {
     "energy_cheb": {"l_max": 8, "minc": 2, "n_r_max": 11, "prmag": 5.0, "ek": 1e-3},
@@ -440,6 +452,62 @@ def worker_step(name, ref):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+def worker_run(name, ref):
+    """The reference's own initial state (initialize_fields + seeded entropy
+    noise + setup_initial_state, saved through save_checkpoint), its kinetic and
+    magnetic energies after every one_step call, and its fields after the last
+    step, all at a fixed dt (the run asserts that the Courant check never changed
+    it)."""
+    import tempfile
+
+    cfg, nsteps, noise = RUN_CONFIGS[name]
+    cfg = dict(cfg, device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, blocking, fields
+    from magic_torch.init_fields import initialize_fields
+    from magic_torch.step_time import setup_initial_state, one_step, initialize_dt
+    from magic_torch.main import save_checkpoint
+    from magic_torch.output import get_e_kin_full, get_e_mag_oc_full
+    from magic_torch.time_scheme import tscheme
+    n = lambda x: x.detach().cpu().numpy().copy()
+    N, lm = params.n_r_max, params.lm_max
+    initialize_fields()
+    g = torch.Generator().manual_seed(0)
+    m0 = blocking.st_lm2m == 0
+    c = torch.complex(torch.randn(lm, N, generator=g, dtype=torch.float64),
+                      torch.randn(lm, N, generator=g, dtype=torch.float64)) * noise
+    c[m0] = c[m0].real.to(c.dtype)
+    fields.s_LMloc[:, 1:-1] += c[:, 1:-1]
+    setup_initial_state()
+    dt = float(cfg["dtmax"])
+    initialize_dt(dt)
+    out = dict(n_r_max=N, l_max=params.l_max, minc=params.minc, lm_max=lm, dt=dt,
+               ek=cfg["ek"], ra=cfg["ra"], pr=cfg["pr"], prmag=cfg["prmag"],
+               radratio=float(params.radratio), steps=nsteps, noise=noise)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "ck.pt")
+        save_checkpoint(path, 0, 0.0, {"tag": "golden"})
+        st = torch.load(path, weights_only=False)
+    for k, v in st.items():
+        if torch.is_tensor(v) and v.dim() >= 2:
+            out["0:" + k] = n(v)
+    out["0:tscheme_dt"] = n(tscheme.dt)
+    ek_t, em_t = [], []
+    for step in range(1, nsteps + 1):
+        dt_new = one_step(step, dt)
+        assert dt_new == dt, (step, dt_new, dt)
+        ek_t.append(np.array(get_e_kin_full(fields.w_LMloc, fields.dw_LMloc, fields.z_LMloc)))
+        em_t.append(np.array(get_e_mag_oc_full(fields.b_LMloc, fields.db_LMloc,
+                                               fields.aj_LMloc)))
+    out["e_kin"], out["e_mag"] = np.stack(ek_t), np.stack(em_t)
+    for k in ("w", "z", "s", "p", "b", "aj"):
+        out[f"{nsteps}:{k}"] = n(getattr(fields, k + "_LMloc"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
@@ -453,6 +521,8 @@ def main():
             worker_td(a.worker, a.ref)
         elif a.worker in STEP_CONFIGS:
             worker_step(a.worker, a.ref)
+        elif a.worker in RUN_CONFIGS:
+            worker_run(a.worker, a.ref)
         elif a.worker in ENERGY_CONFIGS:
             worker_energy(a.worker, a.ref)
         else:
@@ -460,7 +530,7 @@ def main():
         return
     env = dict(os.environ, TORCHDYNAMO_DISABLE="1", MAGIC_DEVICE="cpu")
     names = list(SHT_CONFIGS) + list(NL_CONFIGS) + list(TD_CONFIGS) + list(STEP_CONFIGS)
-    names += list(ENERGY_CONFIGS)
+    names += list(ENERGY_CONFIGS) + list(RUN_CONFIGS)
     if a.only:
         names = [x for x in names if x in a.only.split(",")]
     for name in names:
