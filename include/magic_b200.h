@@ -378,6 +378,48 @@ MT_API int mt_update_poloidal(const mt_plan* plan, int n_r, const mt_poloidal_up
                               const mt_lop* solve, const mt_radial_op* D1,
                               const mt_radial_op* D2, const mt_radial_op* P0, void* stream);
 
+/* ---- implicit update of the poloidal velocity and pressure, standard form --
+ * One CNAB2 step of magic_torch/update_wp.py:387-531 (updateWP, the form the
+ * Chebyshev scheme uses) with the l = 0 pressure of update_wp.py:80-194:
+ *   rhs_w = CNAB2 combination of the w equation's time arrays
+ *           + wimp_lin0 BuoFac rho0 rgrav s (+ ChemFac ... xi) on rows 1..n_r-2,
+ *   rhs_p = CNAB2 combination of the p equation's time arrays on rows 1..n_r-2,
+ *   boundary rows zero; (w, p) = M_l (rhs_w, rhs_p) per degree l >= 1 (m = 0
+ *   real); w = 0 at l = 0 and p(0,0) = P0 (0, rho0 BuoFac rgrav Re s00
+ *   + Re expl0_w,00 (+ chemistry), ...);
+ *   dw = D1 w, ddw = D2 w, dddw = D3 w, dp = D1 p;
+ *   w:  old <- l(l+1) or2 w,
+ *       impl <- -dp + beta p + hdif_l l(l+1) or2 visc (ddw + (2 dLvisc - beta/3) dw
+ *               - (l(l+1) or2 + 4/3 (dbeta + dLvisc beta + (3 dLvisc + beta) or1)) w)
+ *               + BuoFac rho0 rgrav s (+ ChemFac rho0 rgrav xi);
+ *   p:  old <- -l(l+1) or2 dw,
+ *       impl <- l(l+1) or2 p + hdif_l visc l(l+1) or2 (-dddw + (beta - dLvisc) ddw
+ *               + (l(l+1) or2 + dLvisc beta + dbeta + 2 (dLvisc + beta) or1) dw
+ *               - l(l+1) or2 (2 or1 + 2/3 beta + dLvisc) w);
+ *   expl1 <- expl0 for both equations.
+ * solve: per-degree operators of size 2 n_r (mt_lop with n_r' = 2 n_r): the
+ * inverse of the reference's coupled 2n_r x 2n_r matrix (get_wpMat) with the
+ * Chebyshev truncation and the DCT-I to grid values of each block folded in;
+ * P0: the l = 0 pressure inverse likewise; s / xi: this step's entropy /
+ * composition (after their own update). */
+typedef struct {
+  double *w, *dw, *ddw, *p, *dp;
+  double *w_old, *w_impl, *w_expl0, *w_expl1;
+  double *p_old, *p_impl, *p_expl0, *p_expl1;
+  const double *s, *xi;                                    /* xi may be NULL */
+  int64_t ld;
+  double w_old_wt, w_impl_wt, w_expl0_wt, w_expl1_wt, wimp_lin0, BuoFac, ChemFac;
+  const double* hdif;                                      /* (l_max + 1) */
+  const double *or1, *or2, *beta, *dbeta, *visc, *dLvisc, *rgrav, *rho0; /* (n_r) */
+  int impl_interior; /* nonzero: both implicit terms zero at l = 0 and at the two boundary
+                        levels, as the reference's time step stores them (step_time.py:385-394,
+                        :538-545); zero: every entry, as updateWP alone */
+} mt_wp_update;
+
+MT_API int mt_update_wp(const mt_plan* plan, int n_r, const mt_wp_update* u, const mt_lop* solve,
+                        const mt_radial_op* D1, const mt_radial_op* D2, const mt_radial_op* D3,
+                        const mt_radial_op* P0, void* stream);
+
 /* ---- energy integrals of the outer core (FP64) ---------------------------
  * magic_torch/output.py:101-180 (get_e_kin_full, get_e_mag_oc_full): with
  * |x|^2 = Re^2 (m = 0) or 2 |x|^2 (m > 0) and L = l(l+1),

@@ -110,6 +110,16 @@ class PoloidalUpdate(C.Structure):
                                    "c2n", "c1n", "c1d", "c0n")]
 
 
+class WpUpdate(C.Structure):
+    _fields_ = [(n, _dp) for n in ("w", "dw", "ddw", "p", "dp", "w_old", "w_impl", "w_expl0",
+                                   "w_expl1", "p_old", "p_impl", "p_expl0", "p_expl1", "s",
+                                   "xi")] + [("ld", _i64)] + \
+               [(n, C.c_double) for n in ("w_old_wt", "w_impl_wt", "w_expl0_wt", "w_expl1_wt",
+                                          "wimp_lin0", "BuoFac", "ChemFac")] + \
+               [(n, _dp) for n in ("hdif", "or1", "or2", "beta", "dbeta", "visc", "dLvisc",
+                                   "rgrav", "rho0")] + [("impl_interior", C.c_int)]
+
+
 class EnergyArgs(C.Structure):
     _fields_ = [(n, _dp) for n in ("pol", "dpol", "tor")] + [("ld", _i64)] + \
                [(n, _dp) for n in ("or2", "cr", "rint")] + [("magnetic", C.c_int)]
@@ -162,6 +172,8 @@ _PROTOS = {
                                   C.c_void_p, C.c_void_p, _dp]),
     "mt_update_poloidal": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PoloidalUpdate), C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
+    "mt_update_wp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(WpUpdate), C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
     "mt_last_error": (C.c_char_p, []),
 }

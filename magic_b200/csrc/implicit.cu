@@ -567,6 +567,149 @@ TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers) {
   return t;
 }
 
+// ---------------------------------------------------------------------------
+// Standard-form poloidal update (magic_torch/update_wp.py:387-531): the w and
+// p equations are coupled through one 2 n_r x 2 n_r solve per degree.
+// CTA = (kWpRows orders m of one degree l); the rows' right-hand sides and
+// solutions sit in shared memory, each operator coefficient (read once per
+// CTA from L2 as MT[l][k][j], consecutive j across threads) feeds kWpRows
+// complex FMAs.  Derivatives with the radial operators D1, D2, D3.
+constexpr int kWpRows = 8;
+constexpr int kWpThreads = 256;
+
+struct WpArgs {
+  int n_r, ldm, l_max, minc, n_m;
+  const int* lstart;
+  double2 *w, *dw, *ddw, *p, *dp, *wo, *wi, *we0, *we1, *po, *pi, *pe0, *pe1;
+  const double2 *s, *xi;
+  int64_t ld;
+  double w_old, w_impl, w_expl0, w_expl1, wimp_lin0, BuoFac, ChemFac;
+  const double* hdif;
+  const double *or1, *or2, *beta, *dbeta, *visc, *dLvisc, *rgrav, *rho0;
+  int impl_interior;
+  const double* mt;
+  OpView D1, D2, D3, P0;
+};
+
+__global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
+  extern __shared__ __align__(16) double2 wpbuf[];
+  __shared__ int lm_row[kWpRows];
+  const int n_r = a.n_r, n2 = 2 * n_r, l = blockIdx.y, mc0 = blockIdx.x * kWpRows;
+  const int nrow = cta_rows(mc0, kWpRows, l, a.minc, a.n_m);
+  if (nrow == 0) return;
+  double2* f = wpbuf;                  // [kWpRows][n2]: right-hand sides
+  double2* x = wpbuf + kWpRows * n2;   // [kWpRows][n2]: w (0..n_r-1), p (n_r..)
+  if (threadIdx.x < kWpRows)
+    lm_row[threadIdx.x] = threadIdx.x < nrow
+        ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
+  __syncthreads();
+  const double2 zero = {0.0, 0.0};
+  const double dL = (double)l * (l + 1.0);
+  // CNAB2 right-hand sides and the rotation of both explicit histories
+  for (int e = threadIdx.x; e < kWpRows * n_r; e += blockDim.x) {
+    const int r = e / n_r, k = e - r * n_r;
+    double2 vw = zero, vp = zero;
+    if (r < nrow) {
+      const int64_t o = (int64_t)lm_row[r] * a.ld + k;
+      const double2 ow = a.wo[o], iw = a.wi[o], e0w = a.we0[o], e1w = a.we1[o];
+      const double2 op = a.po[o], ip = a.pi[o], e0p = a.pe0[o], e1p = a.pe1[o];
+      const double2 sv = a.s[o];
+      const double2 xv = a.xi ? a.xi[o] : zero;
+      a.we1[o] = e0w;
+      a.pe1[o] = e0p;
+      if (k > 0 && k < n_r - 1) {
+        const double gb = a.wimp_lin0 * a.rho0[k] * a.rgrav[k];
+        vw.x = a.w_old * ow.x + a.w_impl * iw.x + a.w_expl0 * e0w.x + a.w_expl1 * e1w.x +
+               gb * (a.BuoFac * sv.x + a.ChemFac * xv.x);
+        vw.y = a.w_old * ow.y + a.w_impl * iw.y + a.w_expl0 * e0w.y + a.w_expl1 * e1w.y +
+               gb * (a.BuoFac * sv.y + a.ChemFac * xv.y);
+        vp.x = a.w_old * op.x + a.w_impl * ip.x + a.w_expl0 * e0p.x + a.w_expl1 * e1p.x;
+        vp.y = a.w_old * op.y + a.w_impl * ip.y + a.w_expl0 * e0p.y + a.w_expl1 * e1p.y;
+      }
+    }
+    f[r * n2 + k] = vw;
+    f[r * n2 + n_r + k] = vp;
+  }
+  __syncthreads();
+  if (l == 0) {
+    // degree 0 (one row, (l, m) = (0, 0)): w = 0; the l = 0 pressure from its
+    // own right-hand side, built in f's first n_r entries (the expl0 loads
+    // above were of the same row)
+    const int64_t row0 = (int64_t)lm_row[0] * a.ld;
+    for (int k = threadIdx.x; k < n_r; k += blockDim.x) {
+      double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.we0[row0 + k].x;
+      if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
+      f[k] = double2{k == 0 ? 0.0 : v, 0.0};
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < n_r; j += blockDim.x) {
+      x[j] = zero;
+      x[n_r + j] = double2{op_row(a.P0, f, j).x, 0.0};
+    }
+  } else {
+    const double* Ml = a.mt + (int64_t)l * n2 * a.ldm;
+    for (int j = threadIdx.x; j < n2; j += blockDim.x) {
+      double2 acc[kWpRows];
+#pragma unroll
+      for (int r = 0; r < kWpRows; ++r) acc[r] = zero;
+#pragma unroll 4
+      for (int k = 0; k < n2; ++k) {
+        const double c = __ldg(Ml + (int64_t)k * a.ldm + j);
+#pragma unroll
+        for (int r = 0; r < kWpRows; ++r) {
+          const double2 v = f[r * n2 + k];
+          acc[r].x = fma(c, v.x, acc[r].x);
+          acc[r].y = fma(c, v.y, acc[r].y);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kWpRows; ++r) {
+        if (mc0 + r == 0) acc[r].y = 0.0;  // m = 0: real coefficients
+        x[r * n2 + j] = acc[r];
+      }
+    }
+  }
+  __syncthreads();
+  const double hd = a.hdif[l];
+  for (int e = threadIdx.x; e < nrow * n_r; e += blockDim.x) {
+    const int r = e / n_r, j = e - r * n_r;
+    const double2* xw = x + r * n2;
+    const double2* xp = xw + n_r;
+    const double2 w = xw[j], p = xp[j];
+    const double2 d1 = op_row(a.D1, xw, j), d2 = op_row(a.D2, xw, j);
+    const double2 d3 = op_row(a.D3, xw, j), dp = op_row(a.D1, xp, j);
+    const int64_t o = (int64_t)lm_row[r] * a.ld + j;
+    const double2 sv = a.s[o];
+    const double2 xv = a.xi ? a.xi[o] : zero;
+    const double or1 = a.or1[j], or2 = a.or2[j], beta = a.beta[j], dbeta = a.dbeta[j];
+    const double visc = a.visc[j], dLv = a.dLvisc[j];
+    const double dLo = dL * or2, rg = a.rho0[j] * a.rgrav[j];
+    const double fw = hd * dLo * visc;
+    const double cw1 = 2.0 * dLv - beta / 3.0;
+    const double cw0 = dLo + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1);
+    const double cp2 = beta - dLv;
+    const double cp1 = dLo + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1;
+    const double cp0 = dLo * (2.0 * or1 + 2.0 / 3.0 * beta + dLv);
+    a.w[o] = w;
+    a.dw[o] = d1;
+    a.ddw[o] = d2;
+    a.p[o] = p;
+    a.dp[o] = dp;
+    a.wo[o] = double2{dLo * w.x, dLo * w.y};
+    a.po[o] = double2{-dLo * d1.x, -dLo * d1.y};
+    double2 iw, ip;
+    iw.x = -dp.x + beta * p.x + fw * (d2.x + cw1 * d1.x - cw0 * w.x) +
+           rg * (a.BuoFac * sv.x + a.ChemFac * xv.x);
+    iw.y = -dp.y + beta * p.y + fw * (d2.y + cw1 * d1.y - cw0 * w.y) +
+           rg * (a.BuoFac * sv.y + a.ChemFac * xv.y);
+    ip.x = dLo * p.x + fw * (-d3.x + cp2 * d2.x + cp1 * d1.x - cp0 * w.x);
+    ip.y = dLo * p.y + fw * (-d3.y + cp2 * d2.y + cp1 * d1.y - cp0 * w.y);
+    if (a.impl_interior && (l == 0 || j == 0 || j == n_r - 1)) iw = ip = zero;
+    a.wi[o] = iw;
+    a.pi[o] = ip;
+  }
+}
+
 int check_lop(const mt_lop* op) {
   MT_REQUIRE(op && op->mt, MT_ERR_ARG, "null per-degree operator");
   int dev = -1;
@@ -728,6 +871,65 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
                         : (t.nt == 2 ? k_update_poloidal<true, 2> : k_update_poloidal<true, 4>);
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int mt_update_wp(const mt_plan* p, int n_r, const mt_wp_update* u, const mt_lop* solve,
+                 const mt_radial_op* D1, const mt_radial_op* D2, const mt_radial_op* D3,
+                 const mt_radial_op* P0, void* stream) {
+  MT_REQUIRE(p && u, MT_ERR_ARG, "null argument");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == p->device, MT_ERR_ARG, "plan used on a different device than it was built on");
+  MT_TRY(check_lop(solve));
+  MT_TRY(check_radial_op(D1));
+  MT_TRY(check_radial_op(D2));
+  MT_TRY(check_radial_op(D3));
+  MT_TRY(check_radial_op(P0));
+  MT_REQUIRE(solve->n_r == 2 * n_r && radial_op_size(D1) == n_r && radial_op_size(D2) == n_r &&
+                 radial_op_size(D3) == n_r && radial_op_size(P0) == n_r,
+             MT_ERR_ARG, "operator sizes differ from n_r (solve operators: 2 n_r)");
+  MT_REQUIRE(solve->n_l == p->l_max + 1, MT_ERR_ARG, "solve operators must cover l = 0..l_max");
+  MT_REQUIRE(n_r >= 3 && u->ld >= n_r, MT_ERR_ARG, "bad radial size or stride");
+  MT_REQUIRE(u->w && u->dw && u->ddw && u->p && u->dp && u->w_old && u->w_impl && u->w_expl0 &&
+                 u->w_expl1 && u->p_old && u->p_impl && u->p_expl0 && u->p_expl1 && u->s,
+             MT_ERR_ARG, "null field or time array");
+  MT_REQUIRE(u->hdif && u->or1 && u->or2 && u->beta && u->dbeta && u->visc && u->dLvisc &&
+                 u->rgrav && u->rho0,
+             MT_ERR_ARG, "null coefficient array");
+  const size_t smem = (size_t)2 * kWpRows * 2 * n_r * sizeof(double2);
+  MT_REQUIRE(smem <= 227 * 1024, MT_ERR_ARG, "n_r too large for the coupled update");
+  WpArgs a{};
+  a.n_r = n_r;
+  a.ldm = solve->ldm;
+  a.l_max = p->l_max;
+  a.minc = p->minc;
+  a.n_m = p->n_m;
+  a.lstart = p->d_lstart;
+  auto d = [](double* x) { return (double2*)x; };
+  a.w = d(u->w); a.dw = d(u->dw); a.ddw = d(u->ddw); a.p = d(u->p); a.dp = d(u->dp);
+  a.wo = d(u->w_old); a.wi = d(u->w_impl); a.we0 = d(u->w_expl0); a.we1 = d(u->w_expl1);
+  a.po = d(u->p_old); a.pi = d(u->p_impl); a.pe0 = d(u->p_expl0); a.pe1 = d(u->p_expl1);
+  a.s = (const double2*)u->s;
+  a.xi = (const double2*)u->xi;
+  a.ld = u->ld;
+  a.w_old = u->w_old_wt; a.w_impl = u->w_impl_wt; a.w_expl0 = u->w_expl0_wt;
+  a.w_expl1 = u->w_expl1_wt; a.wimp_lin0 = u->wimp_lin0; a.BuoFac = u->BuoFac;
+  a.ChemFac = u->ChemFac;
+  a.hdif = u->hdif;
+  a.or1 = u->or1; a.or2 = u->or2; a.beta = u->beta; a.dbeta = u->dbeta; a.visc = u->visc;
+  a.dLvisc = u->dLvisc; a.rgrav = u->rgrav; a.rho0 = u->rho0;
+  a.impl_interior = u->impl_interior;
+  a.mt = solve->mt;
+  a.D1 = radial_op_view(D1);
+  a.D2 = radial_op_view(D2);
+  a.D3 = radial_op_view(D3);
+  a.P0 = radial_op_view(P0);
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_wp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+  const dim3 grid((p->n_m + kWpRows - 1) / kWpRows, p->l_max + 1);
+  k_update_wp<<<grid, kWpThreads, smem, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

@@ -206,12 +206,91 @@ def poloidal_dc_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbot
     return M
 
 
+def wp_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbotv=2):
+    """(l_max+1, 2 n_r, 2 n_r) solve operators of the coupled (w, p) LHS of the
+    standard poloidal form on Chebyshev levels (magic_torch/update_wp.py:197-368,
+    get_wpMat): unknowns the Chebyshev coefficients of w (0..n_r-1) and p
+    (n_r..2n_r-1),
+      w rows 1..n_r-2  rnorm l(l+1) or2 (rMat - wimp hdif_l visc (d2rMat
+                       + (2 dLvisc - beta/3) drMat - (l(l+1) or2 + 4/3 (dLvisc beta
+                       + (3 dLvisc + beta) or1 + dbeta)) rMat))  |  rnorm wimp (drMat - beta rMat)
+      p rows           rnorm l(l+1) or2 (-drMat - wimp hdif_l visc (-d3rMat
+                       + (beta - dLvisc) d2rMat + (l(l+1) or2 + dbeta + dLvisc beta
+                       + 2 (dLvisc + beta) or1) drMat - l(l+1) or2 (2 or1 + dLvisc
+                       + 2/3 beta) rMat))  |  -rnorm wimp l(l+1) or2 rMat
+      boundary rows    w = 0 at both ends; dw = 0 (no-slip) or d2w - (2 or1 + beta) dw
+                       = 0 (stress-free) in rows n_r, 2n_r-1,
+    Chebyshev columns >= n_cheb dropped in the boundary rows, the first and last
+    column of each block scaled by boundary_fac; inverted through the reference's
+    row, then column scaling; the Chebyshev truncation and the DCT-I of each block
+    folded in, so the operators map the right-hand side to grid values; degree 0
+    zero.  prof: or1, or2, beta, dbeta, visc, dLvisc over n_r."""
+    if not sch.chebyshev:
+        raise ValueError("the standard (w, p) form is used with the Chebyshev scheme only")
+    N, nc = sch.n_r, sch.n_cheb
+    rMat, drMat, d2rMat, d3rMat, rn = sch.rMat, sch.drMat, sch.d2rMat, sch.d3rMat, sch.rnorm
+    col = lambda k: np.asarray(prof[k], dtype=np.float64)[:, None]
+    or1, or2, beta, dbeta, visc, dLv = (col(k) for k in ("or1", "or2", "beta", "dbeta", "visc",
+                                                         "dLvisc"))
+    b = slice(1, N - 1)
+    C2 = np.zeros((2 * N, 2 * N))
+    C2[:N, :N] = C2[N:, N:] = _dct1(N)
+    M = np.zeros((l_max + 1, 2 * N, 2 * N))
+    for l in range(1, l_max + 1):
+        dL, hl = float(l * (l + 1)), float(hdif[l])
+        A = np.zeros((2 * N, 2 * N))
+        A[b, :N] = rn * dL * or2[b] * (rMat[b] - wimp_lin0 * hl * visc[b] * (
+            d2rMat[b] + (2.0 * dLv[b] - beta[b] / 3.0) * drMat[b]
+            - (dL * or2[b] + 4.0 / 3.0 * (dLv[b] * beta[b] + (3.0 * dLv[b] + beta[b]) * or1[b]
+                                          + dbeta[b])) * rMat[b]))
+        A[b, N:] = rn * wimp_lin0 * (drMat[b] - beta[b] * rMat[b])
+        A[N + 1:2 * N - 1, :N] = rn * dL * or2[b] * (-drMat[b] - wimp_lin0 * hl * visc[b] * (
+            -d3rMat[b] + (beta[b] - dLv[b]) * d2rMat[b]
+            + (dL * or2[b] + dbeta[b] + dLv[b] * beta[b] + 2.0 * (dLv[b] + beta[b]) * or1[b])
+            * drMat[b]
+            - dL * or2[b] * (2.0 * or1[b] + dLv[b] + 2.0 / 3.0 * beta[b]) * rMat[b]))
+        A[N + 1:2 * N - 1, N:] = -rn * wimp_lin0 * dL * or2[b] * rMat[b]
+        A[0, :N], A[N - 1, :N] = rn * rMat[0], rn * rMat[N - 1]
+        for row, i, k in ((N, 0, ktopv), (2 * N - 1, N - 1, kbotv)):
+            A[row, :N] = rn * ((d2rMat[i] - (2.0 * or1[i, 0] + beta[i, 0]) * drMat[i]) if k == 1
+                               else drMat[i])
+        if nc < N:
+            for row in (0, N - 1, N, 2 * N - 1):
+                A[row, nc:N] = 0.0
+                A[row, N + nc:] = 0.0
+        for c in (0, N - 1, N, 2 * N - 1):
+            A[:, c] *= sch.boundary_fac
+        fr = 1.0 / np.abs(A).max(axis=1)
+        A = fr[:, None] * A
+        fc = 1.0 / np.abs(A).max(axis=0)
+        Minv = fc[:, None] * np.linalg.inv(A * fc[None, :]) * fr[None, :]
+        if nc < N:
+            Minv[nc:N] = 0.0
+            Minv[N + nc:] = 0.0
+        M[l] = C2 @ Minv
+    return M
+
+
 def p0_inverse(sch, beta):
-    """Inverse of the l = 0 pressure matrix on finite-difference grid values
-    (magic_torch/update_wp.py:80-165): rows 1.. dp/dr - beta p with the last row the
-    first-order backward difference (entries beyond the band of half-width
-    fd_order/2 dropped), row 0 p = 0."""
+    """Inverse of the l = 0 pressure matrix (magic_torch/update_wp.py:80-165),
+    Boussinesq row 0 (p = 0).  Finite differences: grid-value unknowns, rows 1..
+    dp/dr - beta p with the last row the first-order backward difference (entries
+    beyond the band of half-width fd_order/2 dropped).  Chebyshev: coefficient
+    unknowns, rows rnorm (drMat - beta rMat), row 0 rnorm rMat[0] (columns >= n_cheb
+    dropped), first and last column scaled by boundary_fac, with the truncation and
+    the DCT-I to grid values folded into the inverse."""
     N = sch.n_r
+    if sch.chebyshev:
+        A = np.zeros((N, N))
+        A[1:] = sch.rnorm * (sch.drMat[1:] - np.asarray(beta)[1:, None] * sch.rMat[1:])
+        A[0] = sch.rnorm * sch.rMat[0]
+        if sch.n_cheb < N:
+            A[0, sch.n_cheb:] = 0.0
+        A[:, 0] *= sch.boundary_fac
+        A[:, N - 1] *= sch.boundary_fac
+        Minv = np.linalg.inv(A)
+        Minv[sch.n_cheb:] = 0.0
+        return _dct1(N) @ Minv
     A = np.zeros((N, N))
     A[1:] = sch.D1m[1:] - beta[1:, None] * np.eye(N)[1:]
     delr = sch.r[N - 1] - sch.r[N - 2]
@@ -247,6 +326,34 @@ def update_poloidal_dc(plan, sch, lop, P0, w, dw, ddw, p, ta, weights, s, prof, 
     st = C.c_void_p(torch.cuda.current_stream(w.device).cuda_stream)
     check(_lib.lib().mt_update_poloidal(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h,
                                         P0._h, st))
+
+
+def update_wp(plan, sch, lop, P0, w, dw, ddw, p, dp, taw, tap, weights, s, prof, hdif,
+              BuoFac, xi=None, ChemFac=0.0, impl_interior=False):
+    """One standard-form poloidal step in place (mt_update_wp): w, dw, ddw, p, dp
+    outputs; taw / tap: dicts old, impl, expl0, expl1 of the w and p equations;
+    s / xi: this step's entropy / composition; prof: or1, or2, beta, dbeta, visc,
+    dLvisc, rgrav, rho0 over n_r (numpy or device arrays); lop: LOp of
+    wp_solve_operators; P0: RadialOp of p0_inverse.  impl_interior: zero both
+    implicit terms at l = 0 and at the boundary levels, as the reference's time
+    step does (step_time.py:385-394; updateWP alone keeps them; the solution
+    never reads those entries)."""
+    n_r = w.shape[1]
+    arrs = [w, dw, ddw, p, dp, taw["old"], taw["impl"], taw["expl0"], taw["expl1"], tap["old"],
+            tap["impl"], tap["expl0"], tap["expl1"], s]
+    for a in arrs + ([xi] if xi is not None else []):
+        if a.shape != w.shape or a.dtype != torch.complex128 or not a.is_contiguous():
+            raise ValueError("fields and time arrays must be contiguous (lm_max, n_r) complex128")
+    w_old, wimp_lin0, w_impl, w_e0, w_e1 = weights
+    dev = [torch.as_tensor(v, dtype=torch.float64, device=w.device).contiguous()
+           for v in [hdif] + [prof[k] for k in ("or1", "or2", "beta", "dbeta", "visc", "dLvisc",
+                                               "rgrav", "rho0")]]
+    u = _lib.WpUpdate(*[a.data_ptr() for a in arrs], xi.data_ptr() if xi is not None else None,
+                      n_r, w_old, w_impl, w_e0, w_e1, wimp_lin0, float(BuoFac), float(ChemFac),
+                      *[d.data_ptr() for d in dev], int(bool(impl_interior)))
+    st = C.c_void_p(torch.cuda.current_stream(w.device).cuda_stream)
+    check(_lib.lib().mt_update_wp(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h,
+                                  sch.D3._h, P0._h, st))
 
 
 def entropy_coefficients(l_max, opr, hdif, kappa, d1c, or2):

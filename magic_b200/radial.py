@@ -38,15 +38,17 @@ def cheb_grid(n_r, radratio=0.35):
     return 0.5 * (r_cmb - r_icb) * x + 0.5 * (r_icb + r_cmb), x
 
 
-def cheb_polynomials(n_r, radratio=0.35):
+def cheb_polynomials(n_r, radratio=0.35, third=False):
     """(rMat, drMat, d2rMat): T_n(x_i) and its first two r-derivatives at the
-    Gauss-Lobatto points (magic_torch/chebyshev.py:62-110)."""
+    Gauss-Lobatto points (magic_torch/chebyshev.py:62-110); with third=True also
+    d3rMat, the third derivatives."""
     _, x = cheb_grid(n_r, radratio)
     r_cmb = 1.0 / (1.0 - radratio)
     drx = 2.0 / (r_cmb - (r_cmb - 1.0))
     T = np.zeros((n_r, n_r))
     dT = np.zeros((n_r, n_r))
     d2T = np.zeros((n_r, n_r))
+    d3T = np.zeros((n_r, n_r))
     T[:, 0] = 1.0
     T[:, 1] = x
     dT[:, 1] = drx
@@ -54,7 +56,8 @@ def cheb_polynomials(n_r, radratio=0.35):
         T[:, c] = 2.0 * x * T[:, c - 1] - T[:, c - 2]
         dT[:, c] = 2.0 * drx * T[:, c - 1] + 2.0 * x * dT[:, c - 1] - dT[:, c - 2]
         d2T[:, c] = 4.0 * drx * dT[:, c - 1] + 2.0 * x * d2T[:, c - 1] - d2T[:, c - 2]
-    return T, dT, d2T
+        d3T[:, c] = 6.0 * drx * d2T[:, c - 1] + 2.0 * x * d3T[:, c - 1] - d3T[:, c - 2]
+    return (T, dT, d2T, d3T) if third else (T, dT, d2T)
 
 
 def cheb_matrices(n_r, radratio=0.35, n_cheb=None):
@@ -361,7 +364,8 @@ class RadialScheme:
             self.rnorm, self.boundary_fac = 1.0, 1.0
         else:
             self.r, *mats = cheb_matrices(n_r, radratio, n_cheb)
-            self.rMat, self.drMat, self.d2rMat = cheb_polynomials(n_r, radratio)
+            self.rMat, self.drMat, self.d2rMat, self.d3rMat = cheb_polynomials(n_r, radratio,
+                                                                                third=True)
             # Chebyshev-coefficient unknowns (magic_torch/chebyshev.py:47-52)
             self.rnorm, self.boundary_fac = math.sqrt(2.0 / (n_r - 1)), 0.5
         self.radratio = radratio

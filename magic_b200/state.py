@@ -9,8 +9,8 @@ for every time array ``dt.<name>.old`` / ``.impl`` ``(lm_max, n_r, 1)`` and
 previous one), plus the rotation-rate scalars ``dt.domega_{ic,ma}_dt.*``.
 The same dictionary is written and read here for a BoussinesqStep, so a run
 can be resumed by either implementation from the other's file.  Fields and
-time arrays this solver does not evolve (composition, dp, the rotation
-rates) are written as zeros and ignored on load.
+time arrays a step does not evolve (composition, the rotation rates; dp and
+dpdt in the double-curl form) are written as zeros and ignored on load.
 """
 
 import torch
@@ -22,11 +22,12 @@ DT_NAMES = ["dsdt", "dxidt", "dwdt", "dzdt", "dpdt", "dbdt", "djdt"]
 
 # reference field name -> BoussinesqStep.f key
 _FIELD_MAP = {"w_LMloc": "w", "dw_LMloc": "dw", "ddw_LMloc": "ddw", "z_LMloc": "z",
-              "dz_LMloc": "dz", "p_LMloc": "p", "s_LMloc": "s", "ds_LMloc": "ds",
+              "dz_LMloc": "dz", "p_LMloc": "p", "dp_LMloc": "dp", "s_LMloc": "s",
+              "ds_LMloc": "ds",
               "b_LMloc": "b", "db_LMloc": "db", "ddb_LMloc": "ddb", "aj_LMloc": "aj",
               "dj_LMloc": "dj", "ddj_LMloc": "ddj"}
 # reference time array -> BoussinesqStep.ta key
-_DT_MAP = {"dsdt": "s", "dwdt": "w", "dzdt": "z", "dbdt": "b", "djdt": "j"}
+_DT_MAP = {"dsdt": "s", "dwdt": "w", "dzdt": "z", "dpdt": "p", "dbdt": "b", "djdt": "j"}
 
 
 def state_dict(st, step=0, sim_time=0.0, cfg=None):
@@ -37,12 +38,12 @@ def state_dict(st, step=0, sim_time=0.0, cfg=None):
            "tscheme_dt": torch.tensor(st.dt, dtype=torch.float64)}
     for name in FIELD_NAMES:
         k = _FIELD_MAP.get(name)
-        out["fields." + name] = cpu(st.f[k]) if k else zero.clone()
+        out["fields." + name] = cpu(st.f[k]) if k in st.f else zero.clone()
     out["fields.omega_ic"] = 0.0
     out["fields.omega_ma"] = 0.0
     for name in DT_NAMES:
         e = _DT_MAP.get(name)
-        if e is None:
+        if e not in st.ta:
             old = impl = zero[..., None].clone()
             expl = torch.zeros(st.lm_max, st.n_r, 2, dtype=torch.complex128)
         else:
@@ -63,11 +64,15 @@ def load_state_dict(st, state):
     Returns (step, sim_time)."""
     shape = (st.lm_max, st.n_r)
     for name, k in _FIELD_MAP.items():
+        if k not in st.f:
+            continue
         v = state["fields." + name]
         if tuple(v.shape) != shape:
             raise ValueError(f"fields.{name}: shape {tuple(v.shape)}, expected {shape}")
         st.f[k].copy_(v.to(st.device, torch.complex128))
     for name, e in _DT_MAP.items():
+        if e not in st.ta:
+            continue
         ta = st.ta[e]
         expl = state[f"dt.{name}.expl"]
         if tuple(expl.shape) != shape + (2,):

@@ -2,15 +2,18 @@
 
 The reference's one_step (magic_torch/step_time.py:1574-1640) with its
 radial_loop (:931-1213) and lm_loop (:1478-1527), for the finite-difference
-radial scheme with the double-curl poloidal form, an insulating inner core
-and mantle, Boussinesq profiles, magnetic field on:
+radial scheme with the double-curl poloidal form or the Chebyshev scheme with
+the standard coupled (w, p) form (the reference ties the form to the scheme,
+params.py:143), an insulating inner core and mantle, Boussinesq profiles,
+magnetic field on:
 
     radial loop  mt_nl_bouss (input assembly, synthesis, phi FFT, get_nl
                  products, Courant, analysis) then mt_get_td (explicit terms
                  with finish_exp), written straight into each field's expl0;
     lm loop      entropy (mt_update_field), toroidal velocity
-                 (mt_update_field), double-curl poloidal velocity and l = 0
-                 pressure (mt_update_poloidal), magnetic b and j
+                 (mt_update_field), poloidal velocity and l = 0 pressure
+                 (mt_update_poloidal, double curl; mt_update_wp, standard
+                 form with the pressure of every degree), magnetic b and j
                  (mt_update_field), in the reference's order S, Z, W, B.
 
 The time step is held fixed (the solve operators are built once for it); the
@@ -33,9 +36,11 @@ _CD = torch.complex128
 class BoussinesqStep:
     def __init__(self, l_max, n_r, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
                  precision="split", radratio=0.35, fd_order=4, fd_order_bound=2, ktopv=2,
-                 kbotv=2, device=None, cache=None, minc=1):
+                 kbotv=2, device=None, cache=None, minc=1, radial_scheme="FD"):
         """minc: azimuthal symmetry (orders m = 0, minc, 2 minc, ...; the grid covers
-        one sector of 2 pi / minc).
+        one sector of 2 pi / minc).  radial_scheme: "FD" (fourth-order by default,
+        double-curl poloidal form) or "chebyshev" (n_r Gauss-Lobatto levels,
+        standard (w, p) form).
 
         cache: optional dict shared by several steps on one device; the read-only
         parts that depend only on the grid and the dt pair (transform plan, radial
@@ -45,11 +50,13 @@ class BoussinesqStep:
             "cuda", torch.cuda.current_device())
         dev = self.device
         self._cache = cache if cache is not None else {}
-        self._shape = (n_r, radratio, fd_order, fd_order_bound, str(dev))
+        self.std_form = radial_scheme.upper() != "FD"
+        self._shape = (n_r, radial_scheme.upper(), radratio, fd_order, fd_order_bound, str(dev))
         self.plan = self._shared(("plan", l_max, minc, precision, str(dev)),
                                  lambda: Plan(l_max, minc, precision=precision, device=dev))
         self.sch = self._shared(("sch",) + self._shape,
-                                lambda: RadialScheme(n_r, "FD", radratio, fd_order=fd_order,
+                                lambda: RadialScheme(n_r, radial_scheme, radratio,
+                                                     fd_order=fd_order,
                                                      fd_order_bound=fd_order_bound, device=dev))
         self.l_max, self.n_r, self.lm_max = l_max, n_r, self.plan.lm_max
         # physical prefactors (magic_torch/pre_calculations.py:13-41)
@@ -92,12 +99,14 @@ class BoussinesqStep:
         self.wprof = {k: self.prof[k] for k in ("or1", "or2", "beta", "dbeta", "ddbeta", "visc",
                                                 "dLvisc", "ddLvisc", "orho1", "rgrav", "rho0")}
         self.wcoef = tuple(t(c) for c in I._w_coefficient_profiles(hp))
+        self.wpprof = {k: self.prof[k] for k in ("or1", "or2", "beta", "dbeta", "visc", "dLvisc",
+                                                 "rgrav", "rho0")}
         # state: fields, their derivatives and the time arrays of each equation
         z = lambda: torch.zeros(self.lm_max, n_r, dtype=_CD, device=dev)
         self.f = {k: z() for k in ("w", "dw", "ddw", "z", "dz", "s", "ds", "b", "db", "ddb", "aj",
-                                   "dj", "ddj", "p")}
+                                   "dj", "ddj", "p") + (("dp",) if self.std_form else ())}
         self.ta = {e: {k: z() for k in ("old", "impl", "expl0", "expl1")}
-                   for e in ("s", "z", "w", "b", "j")}
+                   for e in ("s", "z", "w", "b", "j") + (("p",) if self.std_form else ())}
         self.nl_out = {k: z() for k in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt",
                                         "VxBp")}
         self.work = torch.empty(self.plan.nl_bouss_workspace(n_r, True, False), dtype=torch.uint8,
@@ -133,7 +142,9 @@ class BoussinesqStep:
             z=I.LOp(I.toroidal_solve_operators(self.sch, l_max, wl0, hdif, hp["visc"],
                                                hp["beta"], hp["dbeta"], hp["dLvisc"], hp["or1"],
                                                hp["or2"], self._ktopv, self._kbotv), device=dev),
-            w=I.LOp(I.poloidal_dc_solve_operators(self.sch, l_max, wl0, hdif, hp, self._ktopv,
+            w=I.LOp(I.wp_solve_operators(self.sch, l_max, wl0, hdif, hp, self._ktopv,
+                                         self._kbotv) if self.std_form else
+                    I.poloidal_dc_solve_operators(self.sch, l_max, wl0, hdif, hp, self._ktopv,
                                                   self._kbotv), device=dev))
         Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif, hp["lambda_"],
                                             hp["dLlambda"], hp["or1"], hp["or2"])
@@ -199,6 +210,9 @@ class BoussinesqStep:
         generic("z", f["z"], f["dz"], second["z"])
         generic("b", f["b"], f["db"], second["b"])
         generic("j", f["aj"], f["dj"], second["aj"])
+        if self.std_form:
+            self._init_wp_terms(dL, hd)
+            return
         # double-curl poloidal terms (update_w_doublecurl.py:310-390)
         dddw, ddddw = get_ddr(f["ddw"], D1, D2)
         or2, orho1, beta = row(P["or2"]), row(P["orho1"]), row(P["beta"])
@@ -214,6 +228,35 @@ class BoussinesqStep:
             x[:, -1] = 0.0
         self.ta["w"]["old"].copy_(old)
         self.ta["w"]["impl"].copy_(impl)
+
+    def _init_wp_terms(self, dL, hd):
+        """old and implicit terms of the standard-form w and p equations from the
+        current fields (step_time.py:491-545): dwdt.old = l(l+1) or2 w, dpdt.old =
+        -l(l+1) or2 dw, and the implicit operators of update_wp.py:492-531 (row 0
+        of the lm order is (l, m) = (0, 0))."""
+        f, P = self.f, self.prof
+        row = lambda x: x[None, :]
+        dddw = self.sch.D3(f["w"])
+        f["dp"].copy_(self.sch.D1(f["p"]))
+        or1, or2, beta, dbeta = (row(P[k]) for k in ("or1", "or2", "beta", "dbeta"))
+        visc, dLv = row(P["visc"]), row(P["dLvisc"])
+        dLo = dL * or2
+        w, dw, ddw, p, dp = f["w"], f["dw"], f["ddw"], f["p"], f["dp"]
+        dif = hd * dLo * visc * (ddw + (2.0 * dLv - beta / 3.0) * dw - (
+            dLo + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1)) * w)
+        self.ta["w"]["old"].copy_(dLo * w)
+        self.ta["w"]["impl"].copy_(-dp + beta * p + dif
+                                   + self.BuoFac * row(P["rho0"]) * row(P["rgrav"]) * f["s"])
+        self.ta["p"]["old"].copy_(-dLo * dw)
+        self.ta["p"]["impl"].copy_(dLo * p + hd * visc * dLo * (
+            -dddw + (beta - dLv) * ddw + (dLo + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1) * dw
+            - dLo * (2.0 * or1 + 2.0 / 3.0 * beta + dLv) * w))
+        # l = 0 and the boundary levels zero (step_time.py:538-545)
+        for e in ("w", "p"):
+            x = self.ta[e]["impl"]
+            x[0] = 0.0
+            x[:, 0] = 0.0
+            x[:, -1] = 0.0
 
     def plan_l(self):
         if not hasattr(self, "_l_dev"):
@@ -232,8 +275,10 @@ class BoussinesqStep:
         td_out = dict(dwdt=self.ta["w"]["expl0"], dzdt=self.ta["z"]["expl0"],
                       dsdt=self.ta["s"]["expl0"], dbdt=self.ta["b"]["expl0"],
                       djdt=self.ta["j"]["expl0"])
-        self.plan.get_td(ins, self.prof, self.CorFac, self.sch.D1, l_double_curl=True,
-                         l_heat=True, l_mag=True, out=td_out)
+        if self.std_form:
+            td_out["dpdt"] = self.ta["p"]["expl0"]
+        self.plan.get_td(ins, self.prof, self.CorFac, self.sch.D1,
+                         l_double_curl=not self.std_form, l_heat=True, l_mag=True, out=td_out)
         return dtr, dth
 
     def lm_loop(self):
@@ -243,9 +288,14 @@ class BoussinesqStep:
                        self.coef["s"], bot=self.bots)
         I.update_field(self.plan, self.sch, self.ops["z"], f["z"], f["dz"], ta["z"], w,
                        self.coef["z"])
-        I.update_poloidal_dc(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"],
-                             f["ddw"], f["p"], ta["w"], w, f["s"], self.wprof, self.hdif,
-                             self.BuoFac, wcoef=self.wcoef)
+        if self.std_form:
+            I.update_wp(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"], f["ddw"],
+                        f["p"], f["dp"], ta["w"], ta["p"], w, f["s"], self.wpprof, self.hdif,
+                        self.BuoFac, impl_interior=True)
+        else:
+            I.update_poloidal_dc(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"],
+                                 f["ddw"], f["p"], ta["w"], w, f["s"], self.wprof, self.hdif,
+                                 self.BuoFac, wcoef=self.wcoef)
         I.update_field(self.plan, self.sch, self.ops["b"], f["b"], f["db"], ta["b"], w,
                        self.coef["b"], d2x=f["ddb"])
         I.update_field(self.plan, self.sch, self.ops["j"], f["aj"], f["dj"], ta["j"], w,

@@ -314,3 +314,133 @@ def update_w(g, mats, prof, st, weights, hdif, D1, D2, s_new, BuoFac, r, fd_orde
     impl = dif + BuoFac * dLh * or2 * p["rgrav"][None, :] * s_new
     impl[:, [0, -1]] = 0.0
     return dict(x=x, dx=dw, d2x=ddw, impl=impl, old=old, expl1=st["expl0"].copy(), p0=p0)
+
+
+def wp_matrix(l, mats, d3rMat, prof, wimp_lin0, hdif_l, n_cheb, ktopv, kbotv):
+    """Coupled (w, p) LHS of degree l >= 1 in the standard poloidal form
+    (magic_torch/update_wp.py:197-329), unknowns the Chebyshev coefficients of w
+    (columns 0..N-1) and p (columns N..2N-1):
+      w rows 1..N-2   rnorm l(l+1) or2 (rMat - wimp hdif visc (d2rMat
+                      + (2 dLvisc - beta/3) drMat - (l(l+1) or2 + 4/3 (dLvisc beta
+                      + (3 dLvisc + beta) or1 + dbeta)) rMat)) | rnorm wimp (drMat - beta rMat)
+      p rows N+1..2N-2  rnorm l(l+1) or2 (-drMat - wimp hdif visc (-d3rMat
+                      + (beta - dLvisc) d2rMat + (l(l+1) or2 + dbeta + dLvisc beta
+                      + 2 (dLvisc + beta) or1) drMat - l(l+1) or2 (2 or1 + dLvisc
+                      + 2/3 beta) rMat)) | -rnorm wimp l(l+1) or2 rMat
+      rows 0, N-1     w = 0;  rows N, 2N-1  dw = 0 (no-slip) or d2w - (2 or1 + beta) dw = 0
+                      (stress-free) at the top / bottom,
+    Chebyshev columns >= n_cheb dropped in the four boundary rows, the first and
+    last column of each block scaled by boundary_fac."""
+    rMat, drMat, d2rMat, rnorm, bfac = mats
+    N = rMat.shape[0]
+    p = {k: np.asarray(v, dtype=np.float64)[:, None] for k, v in prof.items()
+         if np.ndim(v) == 1}
+    or1, or2, beta, dbeta, visc, dLv = (p[k] for k in ("or1", "or2", "beta", "dbeta", "visc",
+                                                       "dLvisc"))
+    dL = float(l * (l + 1))
+    b = slice(1, N - 1)
+    dat = np.zeros((2 * N, 2 * N))
+    dat[b, :N] = rnorm * dL * or2[b] * (rMat[b] - wimp_lin0 * hdif_l * visc[b] * (
+        d2rMat[b] + (2.0 * dLv[b] - beta[b] / 3.0) * drMat[b]
+        - (dL * or2[b] + 4.0 / 3.0 * (dLv[b] * beta[b] + (3.0 * dLv[b] + beta[b]) * or1[b]
+                                      + dbeta[b])) * rMat[b]))
+    dat[b, N:] = rnorm * wimp_lin0 * (drMat[b] - beta[b] * rMat[b])
+    dat[N + 1:2 * N - 1, :N] = rnorm * dL * or2[b] * (-drMat[b] - wimp_lin0 * hdif_l * visc[b] * (
+        -d3rMat[b] + (beta[b] - dLv[b]) * d2rMat[b]
+        + (dL * or2[b] + dbeta[b] + dLv[b] * beta[b] + 2.0 * (dLv[b] + beta[b]) * or1[b])
+        * drMat[b]
+        - dL * or2[b] * (2.0 * or1[b] + dLv[b] + 2.0 / 3.0 * beta[b]) * rMat[b]))
+    dat[N + 1:2 * N - 1, N:] = -rnorm * wimp_lin0 * dL * or2[b] * rMat[b]
+    dat[0, :N] = rnorm * rMat[0]
+    dat[N - 1, :N] = rnorm * rMat[N - 1]
+    o1, bt = prof["or1"], prof["beta"]
+    dat[N, :N] = rnorm * ((d2rMat[0] - (2.0 * o1[0] + bt[0]) * drMat[0]) if ktopv == 1
+                          else drMat[0])
+    dat[2 * N - 1, :N] = rnorm * ((d2rMat[N - 1] - (2.0 * o1[N - 1] + bt[N - 1]) * drMat[N - 1])
+                                  if kbotv == 1 else drMat[N - 1])
+    if n_cheb < N:
+        for row in (0, N - 1, N, 2 * N - 1):
+            dat[row, n_cheb:N] = 0.0
+            dat[row, N + n_cheb:] = 0.0
+    for c in (0, N - 1, N, 2 * N - 1):
+        dat[:, c] *= bfac
+    return dat
+
+
+def p0_matrix_cheb(mats, prof, n_cheb):
+    """l = 0 pressure matrix on Chebyshev coefficients, Boussinesq row 0
+    (magic_torch/update_wp.py:80-165): rows 1.. rnorm (drMat - beta rMat), row 0
+    the Dirichlet row rnorm rMat[0] with columns >= n_cheb dropped, the first and
+    last column scaled by boundary_fac."""
+    rMat, drMat, _, rnorm, bfac = mats
+    N = rMat.shape[0]
+    dat = np.zeros((N, N))
+    dat[1:] = rnorm * (drMat[1:] - prof["beta"][1:, None] * rMat[1:])
+    dat[0] = rnorm * rMat[0]
+    if n_cheb < N:
+        dat[0, n_cheb:] = 0.0
+    dat[:, 0] *= bfac
+    dat[:, N - 1] *= bfac
+    return dat
+
+
+def update_wp(g, mats, d3rMat, prof, stw, stp, weights, hdif, D1, D2, D3, s_new, BuoFac,
+              n_cheb, ktopv, kbotv):
+    """One standard-form updateWP on Chebyshev levels (magic_torch/update_wp.py:
+    387-531): CNAB2 right-hand sides of the w and p equations, plus
+    wimp BuoFac rho0 rgrav s on the interior w rows, boundary rows zero; a coupled
+    solve per degree l >= 1 (row, then column scaling, as the reference), m = 0
+    made real; the l = 0 pressure from rho0 BuoFac rgrav Re s00 + Re expl0_w;
+    Chebyshev truncation and the DCT-I to grid values; dw, ddw, dddw, dp; old and
+    implicit terms of both equations (update_wp.py:470-531).
+
+    stw, stp: dict old, impl, expl0, expl1 of the w and p equations."""
+    wimp, wimp_lin, wexp = weights
+    N = stw["old"].shape[1]
+    pr = prof
+    rhs_of = lambda st: (wimp[0] * st["old"] + wimp_lin[1] * st["impl"] + wexp[0] * st["expl0"]
+                         + wexp[1] * st["expl1"])
+    rw, rp = rhs_of(stw), rhs_of(stp)
+    rhs = np.zeros((rw.shape[0], 2 * N), dtype=np.complex128)
+    rhs[:, 1:N - 1] = rw[:, 1:N - 1] + wimp_lin[0] * BuoFac * (
+        pr["rho0"] * pr["rgrav"])[None, 1:N - 1] * s_new[:, 1:N - 1]
+    rhs[:, N + 1:2 * N - 1] = rp[:, 1:N - 1]
+    sol = np.zeros_like(rhs)
+    for l in range(1, g["l_max"] + 1):
+        rows = np.nonzero(g["lm2l"] == l)[0]
+        dat = wp_matrix(l, mats, d3rMat, prof, wimp_lin[0], hdif[l], n_cheb, ktopv, kbotv)
+        fr = 1.0 / np.abs(dat).max(axis=1)
+        dat = fr[:, None] * dat
+        fc = 1.0 / np.abs(dat).max(axis=0)
+        y = np.linalg.solve(dat * fc[None, :], (fr[None, :] * rhs[rows]).T).T
+        sol[rows] = fc[None, :] * y
+    m0 = g["lm2m"] == 0
+    sol[m0] = sol[m0].real
+    wc, pc = sol[:, :N].copy(), sol[:, N:].copy()
+    lm0 = int(np.nonzero((g["lm2l"] == 0) & m0)[0][0])
+    p0_rhs = np.zeros(N)
+    p0_rhs[1:] = pr["rho0"][1:] * BuoFac * pr["rgrav"][1:] * s_new[lm0, 1:].real \
+        + stw["expl0"][lm0, 1:].real
+    pc[lm0] = np.linalg.solve(p0_matrix_cheb(mats, prof, n_cheb), p0_rhs)
+    if n_cheb < N:
+        wc[:, n_cheb:] = 0.0
+        pc[:, n_cheb:] = 0.0
+    C = dct1_matrix(N)
+    w, p = wc @ C.T, pc @ C.T
+    dw, ddw, dddw, dp = w @ D1.T, w @ D2.T, w @ D3.T, p @ D1.T
+    dLh = (g["lm2l"] * (g["lm2l"] + 1.0))[:, None]
+    r1 = lambda k: np.asarray(pr[k], dtype=np.float64)[None, :]
+    or1, or2, beta, dbeta, visc, dLv = (r1(k) for k in ("or1", "or2", "beta", "dbeta", "visc",
+                                                        "dLvisc"))
+    hd = hdif[g["lm2l"]][:, None]
+    dif = hd * dLh * or2 * visc * (
+        ddw + (2.0 * dLv - beta / 3.0) * dw
+        - (dLh * or2 + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1)) * w)
+    w_impl = -dp + beta * p + dif + BuoFac * r1("rho0") * r1("rgrav") * s_new
+    p_impl = dLh * or2 * p + hd * visc * dLh * or2 * (
+        -dddw + (beta - dLv) * ddw
+        + (dLh * or2 + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1) * dw
+        - dLh * or2 * (2.0 * or1 + 2.0 / 3.0 * beta + dLv) * w)
+    return dict(w=w, dw=dw, ddw=ddw, p=p, dp=dp, w_old=dLh * or2 * w, w_impl=w_impl,
+                w_expl1=stw["expl0"].copy(), p_old=-dLh * or2 * dw, p_impl=p_impl,
+                p_expl1=stp["expl0"].copy())

@@ -39,9 +39,13 @@ NL_CONFIGS = {
 }
 
 
-# whole CNAB2 steps of the finite-difference Boussinesq MHD dynamo
-# (fourth-order FD, double curl, insulating inner core, fixed entropy, no-slip)
+# whole CNAB2 steps of the Boussinesq MHD dynamo (insulating inner core, fixed
+# entropy, no-slip): fourth-order FD with the double-curl form, and Chebyshev
+# levels with the standard form
 STEP_CONFIGS = {
+    # Chebyshev levels, standard (w, p) form, minc 4
+    "step_cheb": {"l_max": 32, "minc": 4, "n_r_max": 33, "ek": 1e-3, "ra": 1e5, "pr": 1.0,
+                  "prmag": 5.0, "dtmax": 5e-6, "mode": 0},
     "step_fd": {"l_max": 12, "minc": 1, "n_r_max": 13, "radial_scheme": "FD", "fd_order": 4,
                 "fd_order_bound": 2, "ek": 1e-3, "ra": 1e5, "pr": 1.0, "prmag": 5.0,
                 "dtmax": 1e-4, "mode": 0},
@@ -51,9 +55,12 @@ STEP_CONFIGS = {
 # shell case (l_max 32, minc 4, 33 levels, Ek 1e-3, Ra 1e5, Pr 1, Pm 5, dt 1e-4,
 # the reference's initial fields: l = m = 4 entropy mode of amplitude 0.1 and
 # its dipolar poloidal field, init_b1 = 3, amp_b1 = 5) with seeded Gaussian
-# noise of amplitude 1e-5 on the entropy; the radial scheme is fourth-order FD
-# (double curl), the form the GPU time step implements.
+# noise of amplitude 1e-5 on the entropy; on its 33 Chebyshev levels (standard
+# (w, p) form) and on 33 fourth-order FD levels (double-curl form).
 RUN_CONFIGS = {
+    # the shell case itself: 33 Chebyshev levels, standard (w, p) form
+    "run_cheb_l32m4": ({"l_max": 32, "minc": 4, "n_r_max": 33, "ek": 1e-3, "ra": 1e5,
+                        "pr": 1.0, "prmag": 5.0, "dtmax": 1e-4, "mode": 0}, 500, 1e-5),
     "run_fd_l32m4": ({"l_max": 32, "minc": 4, "n_r_max": 33, "radial_scheme": "FD",
                       "fd_order": 4, "fd_order_bound": 2, "ek": 1e-3, "ra": 1e5, "pr": 1.0,
                       "prmag": 5.0, "dtmax": 1e-4, "mode": 0}, 500, 1e-5),
@@ -348,6 +355,30 @@ def worker_td(name, ref):
         out.update(w_new=n(w_new), dw_new=n(dw_new), ddw_new=n(ddw_new), p0_new=n(p_new[0]),
                    w_impl_new=n(tw.impl[:, :, 0]), w_old_new=n(tw.old[:, :, 0]),
                    w_expl1_new=n(tw.expl[:, :, 1]))
+    else:
+        # one coupled (w, p) update in the standard form with the l = 0 pressure
+        # (magic_torch/update_wp.py:80-531)
+        from magic_torch import update_wp as uwp
+        uwp.build_wp_matrices(tscheme.wimp_lin[0].item())
+        uwp.build_p0_matrix()
+        tw = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+        tp = dtf.TimeArray(tscheme.nold, tscheme.nexp, tscheme.nimp)
+        for f, ta_ in (("wp_w", tw), ("wp_p", tp)):
+            for k in ("old", "impl", "expl0", "expl1"):
+                v = _spec(rng, lm, l_of, N)
+                (ta_.old if k == "old" else ta_.impl if k == "impl" else ta_.expl)[
+                    :, :, 1 if k == "expl1" else 0] = t(v)
+                out[f + "_" + k] = v
+        out.update(rgrav=n(rf2.rgrav), rho0=n(rf2.rho0), BuoFac=float(pc.BuoFac),
+                   d3rMat=n(rs.d3rMat), D3=n(rd._D3_real))
+        w_new, dw_new, ddw_new, p_new, dp_new = (torch.zeros(lm, N, dtype=torch.complex128)
+                                                 for _ in range(5))
+        uwp.updateWP(s_new.clone(), w_new, dw_new, ddw_new, tw, p_new, dp_new, tp, tscheme)
+        out.update({"wp_w_new": n(w_new), "wp_dw_new": n(dw_new), "wp_ddw_new": n(ddw_new),
+                    "wp_p_new": n(p_new), "wp_dp_new": n(dp_new)})
+        for f, ta_ in (("wp_w", tw), ("wp_p", tp)):
+            out.update({f + "_impl_new": n(ta_.impl[:, :, 0]), f + "_old_new": n(ta_.old[:, :, 0]),
+                        f + "_expl1_new": n(ta_.expl[:, :, 1])})
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

@@ -323,3 +323,104 @@ def test_update_poloidal_vs_oracle(l_max, n_r, scale):
     for k in ("x", "dx", "d2x", "impl", "old", "expl1", "p0"):
         e = rel_err(npy(o[k]), ref[k])
         assert e < scale * (TOL_IMPL if k in ("impl", "old", "d2x") else TOL), (k, e)
+
+
+WPPROF = ("or1", "or2", "beta", "dbeta", "visc", "dLvisc", "rgrav", "rho0")
+
+
+def _run_wp(p, sch, stw, stp, s_new, prof, hdif, BuoFac, w, ktopv, kbotv):
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialOp
+
+    lop = I.LOp(I.wp_solve_operators(sch, p.l_max, w[1], hdif, prof, ktopv, kbotv))
+    P0 = RadialOp(I.p0_inverse(sch, prof["beta"]))
+    taw = {k: cu(v) for k, v in stw.items()}
+    tap = {k: cu(v) for k, v in stp.items()}
+    shape = taw["old"].shape
+    out = {k: torch.full(shape, float("nan"), dtype=torch.complex128, device="cuda")
+           for k in ("w", "dw", "ddw", "p", "dp")}
+    I.update_wp(p, sch, lop, P0, out["w"], out["dw"], out["ddw"], out["p"], out["dp"], taw, tap,
+                w, cu(s_new), prof, hdif, BuoFac)
+    torch.cuda.synchronize()
+    res = {k: npy(v) for k, v in out.items()}
+    for f, ta in (("w", taw), ("p", tap)):
+        for k in ("old", "impl", "expl0", "expl1"):
+            res[f"{f}_{k}"] = npy(ta[k])
+    return res
+
+
+def test_update_wp_matches_reference():
+    """The standard-form coupled (w, p) update with the l = 0 pressure
+    (mt_update_wp) against the reference's own updateWP (tests/golden/td_cheb.npz:
+    l_max 8, 9 Chebyshev levels, stress-free rows): w, dw, ddw, p, dp and both
+    equations' old, implicit and rotated explicit terms.  The GPU applies the
+    inverse of the scaled coupled matrix with the DCT-I folded in (the reference
+    also applies a precomputed inverse, then the DCT-I)."""
+    from types import SimpleNamespace
+
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialOp
+
+    z = load_golden("td_cheb")
+    p = Plan(int(z["l_max"]), int(z["minc"]))
+    sch = SimpleNamespace(n_r=int(z["n_r_max"]), chebyshev=True, n_cheb=int(z["n_cheb_max"]),
+                          rMat=z["rMat"], drMat=z["drMat"], d2rMat=z["d2rMat"],
+                          d3rMat=z["d3rMat"], rnorm=float(z["rnorm"]),
+                          boundary_fac=float(z["boundary_fac"]), D1=RadialOp(z["D1"]),
+                          D2=RadialOp(z["D2"]), D3=RadialOp(z["D3"]))
+    prof = {k: z[k] for k in WPPROF}
+    stw = {k: z["wp_w_" + k] for k in ("old", "impl", "expl0", "expl1")}
+    stp = {k: z["wp_p_" + k] for k in ("old", "impl", "expl0", "expl1")}
+    o = _run_wp(p, sch, stw, stp, z["s_new"], prof, z["hdif_V"], float(z["BuoFac"]),
+                I.cnab2_weights(1e-4, 1.3e-4), int(z["ktopv"]), int(z["kbotv"]))
+    errs = {k: rel_err(o[k], z[f"wp_{k}_new"]) for k in ("w", "dw", "ddw", "p", "dp")}
+    for f in ("w", "p"):
+        for k in ("old", "impl", "expl1"):
+            errs[f"{f}_{k}"] = rel_err(o[f"{f}_{k}"], z[f"wp_{f}_{k}_new"])
+        assert rel_err(o[f"{f}_expl0"], z[f"wp_{f}_expl0"]) == 0.0
+    print({k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        assert v < (TOL_IMPL if k in ("ddw", "p_impl", "w_impl", "dw") else TOL), (k, v)
+
+
+@pytest.mark.parametrize("l_max,minc,n_r,ktopv", [(127, 1, 65, 2), (32, 4, 33, 1)])
+def test_update_wp_vs_oracle(l_max, minc, n_r, ktopv):
+    """l_max = 127 on 65 Chebyshev levels (no-slip) and l_max = 32, minc = 4 on 33
+    levels (stress-free) with anelastic-like profiles, against the oracle's LU
+    solves.  The coupled Chebyshev operator is far worse conditioned than the
+    scalar ones (its p rows carry d3rMat): the tolerances are relative to each
+    array's largest value, 1e-11 for the fields and 1e-10 for the terms that
+    apply D2 / D3 to the new w."""
+    from magic_b200 import Plan
+    from magic_b200 import implicit as I
+    from magic_b200.radial import RadialScheme
+
+    p = Plan(l_max, minc)
+    sch = RadialScheme(n_r, "chebyshev")
+    r = sch.r
+    prof = dict(or1=1.0 / r, or2=1.0 / r ** 2, beta=-0.3 / r, dbeta=0.3 / r ** 2,
+                visc=1.0 + 0.1 * r / r[0], dLvisc=0.1 / (r[0] + 0.1 * r), rgrav=r / r[0],
+                rho0=np.exp(0.3 * (r[0] - r)))
+    hdif, BuoFac = np.ones(l_max + 1), 1e3
+    rng = np.random.default_rng(5)
+    amp = (p.lm2l + 1.0)[:, None] ** -1.5
+    spec = lambda: (rng.standard_normal((p.lm_max, n_r))
+                    + 1j * rng.standard_normal((p.lm_max, n_r))) * amp
+    stw = {k: spec() for k in ("old", "impl", "expl0", "expl1")}
+    stp = {k: spec() for k in ("old", "impl", "expl0", "expl1")}
+    s_new = spec()
+    w = I.cnab2_weights(1e-4, 1.2e-4)
+    o = _run_wp(p, sch, stw, stp, s_new, prof, hdif, BuoFac, w, ktopv, ktopv)
+    g = dict(lm2l=p.lm2l, lm2m=p.lm2m, l_max=l_max)
+    mats = (sch.rMat, sch.drMat, sch.d2rMat, sch.rnorm, sch.boundary_fac)
+    ref = oi.update_wp(g, mats, sch.d3rMat, prof, {k: v.copy() for k, v in stw.items()},
+                       {k: v.copy() for k, v in stp.items()},
+                       ([w[0]], [w[1], w[2]], [w[3], w[4]]), hdif, sch.D1m, sch.D2m, sch.D3m,
+                       s_new, BuoFac, sch.n_cheb, ktopv, ktopv)
+    errs = {k: rel_err(o[k], ref[k]) for k in ("w", "dw", "ddw", "p", "dp", "w_old", "w_impl",
+                                                "w_expl1", "p_old", "p_impl", "p_expl1")}
+    print({k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        assert v < (1e-10 if k in ("ddw", "w_impl", "p_impl", "p_old", "dw", "dp") else 1e-11), \
+            (k, v)

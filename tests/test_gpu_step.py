@@ -68,15 +68,16 @@ def _golden_state(z, tag):
         "tscheme_dt": torch.as_tensor(z[tag + ":tscheme_dt"])}
 
 
-def _reference_run():
+def _reference_run(name="step_fd"):
     from conftest import load_golden
     from magic_b200.state import load_state_dict
     from magic_b200.step import BoussinesqStep
 
-    z = load_golden("step_fd")
+    z = load_golden(name)
     st = BoussinesqStep(int(z["l_max"]), int(z["n_r_max"]), ek=float(z["ek"]), ra=float(z["ra"]),
                         pr=float(z["pr"]), prmag=float(z["prmag"]), dt=float(z["dt"]),
-                        precision="fp64", radratio=float(z["radratio"]))
+                        precision="fp64", radratio=float(z["radratio"]), minc=int(z["minc"]),
+                        radial_scheme="chebyshev" if "cheb" in name else "FD")
     assert st.lm_max == int(z["lm_max"])
     load_state_dict(st, _golden_state(z, "0"))
     return z, st
@@ -119,6 +120,40 @@ def test_two_steps_match_reference():
     for k, v in errs.items():
         tight = k in ("w", "z", "s", "b", "aj", "p00", "e_kin", "e_mag")
         assert v < (1e-12 if tight else 1e-11), (k, v)
+
+
+def test_two_steps_match_reference_chebyshev():
+    """Two whole steps on Chebyshev levels with the standard (w, p) form from the
+    reference's own initial state (tests/golden/step_cheb.npz: l_max 32, minc 4,
+    33 levels, Ek 1e-3, Ra 1e5, Pm 5, dt 5e-6, seeded perturbations of s, w and
+    z): the fields (p and dp included), every time array (dpdt included) and the
+    energies against the reference's one_step results (its whole-step path, which
+    stores the w and p implicit terms as zero at l = 0 and at the boundaries).
+    Tolerance, relative to each array's largest value: 1e-12 for the fields and
+    the energies (measured <= 4.5e-13, in w), 1e-9 for the radial derivatives and
+    the time arrays (measured <= 2.0e-10, in ddb: the Chebyshev D2 at 33 levels
+    amplifies the fields' rounding-level differences ~1e5-fold)."""
+    import numpy as np
+
+    z, st = _reference_run("step_cheb")
+    rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    st.step()
+    st.step()
+    errs = {k: rel(st.f[k].cpu().numpy(), z[f"2:fields.{k}_LMloc"])
+            for k in STEP_FIELDS + ("p", "dp")}
+    for e, name in dict(STEP_DT, p="dpdt").items():
+        ta = st.ta[e]
+        errs[name + ".old"] = rel(ta["old"].cpu().numpy(), z[f"2:dt.{name}.old"][..., 0])
+        errs[name + ".impl"] = rel(ta["impl"].cpu().numpy(), z[f"2:dt.{name}.impl"][..., 0])
+        errs[name + ".expl0"] = rel(ta["expl0"].cpu().numpy(), z[f"2:dt.{name}.expl"][..., 0])
+        errs[name + ".expl1"] = rel(ta["expl1"].cpu().numpy(), z[f"2:dt.{name}.expl"][..., 1])
+    ek, em = st.energies()
+    errs["e_kin"] = rel(np.array(ek), z["2:e_kin"])
+    errs["e_mag"] = rel(np.array(em), z["2:e_mag"])
+    print({k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in errs.items():
+        tight = k in ("w", "z", "s", "b", "aj", "p", "e_kin", "e_mag")
+        assert v < (1e-12 if tight else 1e-9), (k, v)
 
 
 def test_checkpoint_round_trip(tmp_path):
@@ -207,28 +242,29 @@ def test_run_outputs_and_restart(tmp_path):
         assert torch.equal(st.f[k], other.f[k]), k
 
 
-def _reference_run500(precision):
+def _reference_run500(precision, name="run_fd_l32m4"):
     from conftest import load_golden
     from magic_b200.state import load_state_dict
     from magic_b200.step import BoussinesqStep
 
-    z = load_golden("run_fd_l32m4")
+    z = load_golden(name)
+    scheme = "chebyshev" if "cheb" in name else "FD"
     st = BoussinesqStep(int(z["l_max"]), int(z["n_r_max"]), ek=float(z["ek"]), ra=float(z["ra"]),
                         pr=float(z["pr"]), prmag=float(z["prmag"]), dt=float(z["dt"]),
                         precision=precision, radratio=float(z["radratio"]),
-                        minc=int(z["minc"]))
+                        minc=int(z["minc"]), radial_scheme=scheme)
     assert st.lm_max == int(z["lm_max"])
     load_state_dict(st, _golden_state(z, "0"))
     return z, st
 
 
-def _run500_errors(precision):
+def _run500_errors(precision, name="run_fd_l32m4"):
     """Fields after 500 steps (relative to each field's largest value) and the
     kinetic / magnetic energies of every step (relative to each energy's largest
     value over the run) against the reference's 500 one_step calls."""
     import numpy as np
 
-    z, st = _reference_run500(precision)
+    z, st = _reference_run500(precision, name)
     n = int(z["steps"])
     ek, em = [], []
     for _ in range(n):
@@ -238,8 +274,12 @@ def _run500_errors(precision):
         em.append(np.array(b))
     ek, em = np.stack(ek), np.stack(em)
     rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
-    fe = {k: rel(st.f[k].cpu().numpy(), z[f"{n}:{k}"]) for k in ("w", "z", "s", "b", "aj")}
+    keys = ("w", "z", "s", "b", "aj") + (("p",) if st.std_form else ())
+    fe = {k: rel(st.f[k].cpu().numpy(), z[f"{n}:{k}"]) for k in keys}
     ee = {}
+    growth = np.abs(ek[:, 0] - z["e_kin"][:, 0]) / np.abs(z["e_kin"][:, 0])
+    print("e_kin relative error at steps 1, 10, 100, 250, 500:",
+          [f"{growth[i]:.1e}" for i in (0, 9, 99, 249, 499)])
     for name, got, ref in (("e_kin", ek, z["e_kin"]), ("e_mag", em, z["e_mag"])):
         for c in range(ref.shape[1]):
             if np.abs(ref[:, c]).max() > 0:
@@ -270,6 +310,35 @@ def test_500_steps_match_reference_split():
     terms carry the FP32 phi stage's ~1e-7-1e-6 relative error every step, and
     the convecting flow (kinetic energy 0.44 -> 73 over the run) amplifies it."""
     fe, ee = _run500_errors("split")
+    print({k: f"{v:.1e}" for k, v in (fe | ee).items()})
+    assert max(fe.values()) < 3e-5, fe
+    assert max(ee.values()) < 5e-6, ee
+
+
+def test_500_steps_match_reference_chebyshev_fp64():
+    """The shell case as the reference runs it (tests/golden/run_cheb_l32m4.npz:
+    l_max 32, minc 4, 33 Chebyshev levels with the standard (w, p) form, Ek 1e-3,
+    Ra 1e5, Pr 1, Pm 5, dt 1e-4, the reference's initial fields and seeded entropy
+    noise 1e-5): 500 FP64 steps; the energies of every step within 1e-12 of the
+    reference's (measured <= 5.5e-13) and the fields (p included) after step 500
+    within 1e-11 (measured: z 4.4e-12, the others <= 7.3e-13).  The z figure
+    misses the 1e-12 target: the Chebyshev D2 turns the two implementations'
+    rounding-level differences into ~1e-10 relative differences of the
+    derivatives every step (two-step test), and the convecting flow carries them
+    into the fields.  For scale, the reference itself with its fields (not their
+    derivatives) perturbed by 1e-16 (relative) after every step ends 8.9e-14
+    away in z: the larger part of the difference enters through the derivative
+    arrays."""
+    fe, ee = _run500_errors("fp64", "run_cheb_l32m4")
+    print({k: f"{v:.1e}" for k, v in (fe | ee).items()})
+    assert max(fe.values()) < 1e-11, fe
+    assert max(ee.values()) < 1e-12, ee
+
+
+def test_500_steps_match_reference_chebyshev_split():
+    """The same Chebyshev run with the split-precision stage against the
+    reference's FP64 run (bounds as for the finite-difference run)."""
+    fe, ee = _run500_errors("split", "run_cheb_l32m4")
     print({k: f"{v:.1e}" for k, v in (fe | ee).items()})
     assert max(fe.values()) < 3e-5, fe
     assert max(ee.values()) < 5e-6, ee
