@@ -380,6 +380,37 @@ def run_td(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def fp64_plain_stage(args, dev, fields, prof, stream, dist):
+    """The same stage on an FP64 plan (the plain mode: FP64 DMMA Legendre
+    contractions and FP64 phi stage) with the same inputs, device-timed over the
+    same number of steps after the same warm-up; ms per stage, max over ranks."""
+    from magic_b200 import Plan
+
+    n_r = args.levels
+    plan = Plan(L_MAX, 1, precision="fp64", device=dev)
+    out = {k: torch.zeros(plan.lm_max, n_r, dtype=torch.complex128, device=dev) for k in OUTS}
+    work = torch.zeros(plan.nl_bouss_workspace(n_r, True, False), dtype=torch.uint8, device=dev)
+    step = lambda: plan.nl_bouss(fields, prof, LF, CF, AF, OPM, l_mag=True, l_chem=False,
+                                 out=out, work=work)
+    for _ in range(args.warmup):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
+    del plan, out, work
+    torch.cuda.empty_cache()
+    return ms
+
+
 def run_step(args, rank, world):
     """Optional line: whole CNAB2 time steps of the Boussinesq MHD dynamo at
     l_max = 255 on the 97-level fourth-order finite-difference grid (radial loop
@@ -443,8 +474,8 @@ def run_step(args, rank, world):
 def run_serve(args, rank, world):
     """Optional line: the ensemble stream (Poisson arrivals at 4 runs/s, l_max in
     {32, 64, 85, 127}, n_r in {33, 49, 65}, Ek log-uniform [1e-4, 1e-3], Ra
-    log-uniform [1e5, 1e6], Pr 1, Pm 5, perturbation 1e-5, FD4 double-curl
-    Boussinesq MHD steps at dt 1e-4) served with continuous batching in split
+    log-uniform [1e5, 1e6], Pr 1, Pm 5, perturbation 1e-5, Boussinesq MHD steps on
+    Chebyshev levels (standard (w, p) form) at dt 1e-4) served with continuous batching in split
     precision: p50 / p99 per-step device latency and aggregate steps/s over the
     serving wall time (value).  The same runs all arriving at once measure the
     capacity.  Baseline: the FP64 stage one run at a time, eager: each run's
@@ -471,7 +502,7 @@ def run_serve(args, rank, world):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         st = BoussinesqStep(s.l_max, s.n_r, ek=s.ek, ra=s.ra, pr=s.pr, prmag=s.prmag, dt=s.dt,
-                            precision="fp64", device=dev)
+                            precision="fp64", device=dev, radial_scheme=s.radial_scheme)
         st.init_random(seed=s.seed, amp=s.amp)
         torch.cuda.synchronize()
         build = time.perf_counter() - t0
@@ -499,7 +530,7 @@ def run_serve(args, rank, world):
                                    "capacity_steps_per_s": rep["steps"] / busy},
             "dtype": "bf16x3/f32 stage, f64 rest", "data": "synthetic",
             "config": {"workload": "ensemble stream: Poisson 4 runs/s, l_max 32-127, n_r 33-65, "
-                                   "FD4 Boussinesq MHD, dt 1e-4",
+                                   "Chebyshev Boussinesq MHD, dt 1e-4",
                        "runs": args.serve_runs, "steps_per_run": args.serve_steps},
             "clocks": clocks.summary()}), flush=True)
 
@@ -759,6 +790,7 @@ def main():
                                "(no FP64 entry in MEASURED_PEAKS.json)"}
     sht_tflops = (synth_f + anal_f) / ((part_ms["legendre_synthesis"] +
                                         part_ms["legendre_analysis"]) * 1e-3) / 1e12
+    plain = fp64_plain_stage(args, dev, fields, prof, stream, dist) if split else None
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
@@ -773,6 +805,12 @@ def main():
                 "gpu_launches": 6 * args.steps,  # split: 2 packs, 2 GEMMs, phi, Courant; fp64: 2 + 1 + 2 + 1
                 "kernel_ms": part_ms, "sht_tflops": sht_tflops,
                 "roofline": roof}
+        if plain is not None:
+            line["fp64_plain"] = {"value": job_steps_per_s(world, plain), "unit": "steps/s",
+                                  "ms_per_step": plain, "split_over_fp64": plain / ms,
+                                  "what": "the same stage on an FP64 plan (DMMA Legendre, "
+                                          "FP64 phi stage), same inputs, device-timed"}
+            line["gpu_launches"] += 6 * args.steps
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_stage_sample()
         print(json.dumps(line), flush=True)

@@ -44,6 +44,7 @@ class RunSpec:
     amp: float = 1e-5
     arrival: float = 0.0  # seconds after the start of serving
     precision: str = "split"
+    radial_scheme: str = "chebyshev"  # the reference's default; "FD": fourth-order FD
 
 
 @dataclass
@@ -57,7 +58,8 @@ class RunResult:
 
 
 def poisson_stream(n_runs=64, rate=4.0, seed=0, n_steps=200, precision="split",
-                   l_choices=(32, 64, 85, 127), nr_choices=(33, 49, 65)):
+                   l_choices=(32, 64, 85, 127), nr_choices=(33, 49, 65),
+                   radial_scheme="chebyshev"):
     """Seeded run stream: exponential inter-arrival times of mean 1 / rate,
     l_max and n_r uniform over the choices, Ekman log-uniform in [1e-4, 1e-3],
     Rayleigh log-uniform in [1e5, 1e6], Pr = 1, Pm = 5, perturbation 1e-5."""
@@ -70,7 +72,8 @@ def poisson_stream(n_runs=64, rate=4.0, seed=0, n_steps=200, precision="split",
                            n_r=int(rng.choice(nr_choices)),
                            ek=float(10.0 ** rng.uniform(-4.0, -3.0)),
                            ra=float(10.0 ** rng.uniform(5.0, 6.0)), n_steps=n_steps,
-                           seed=1000 + i, arrival=t, precision=precision))
+                           seed=1000 + i, arrival=t, precision=precision,
+                           radial_scheme=radial_scheme))
     return out
 
 
@@ -92,13 +95,14 @@ def footprint_estimate(spec):
     """Upper estimate of a run's device memory (bytes): 42 (lm_max, n_r) complex
     arrays (fields, time arrays, nonlinear outputs), the stage workspace
     (Fourier rows of 24 fields in FP64 and the split operand images), the
-    solve operators (5 (l_max + 1) n_r^2 doubles) and the transform tables."""
+    solve operators (at most 8 (l_max + 1) n_r^2 doubles: the coupled (w, p)
+    operators of the Chebyshev form are 2 n_r square) and the transform tables."""
     n_theta, n_phi, lm = _grid_sizes(spec.l_max)
     n_m = spec.l_max + 1
     arrays = 42 * lm * spec.n_r * 16
     fourier = 24 * spec.n_r * n_theta * n_m * 16
     images = (2 * 1.13e9 * (lm * spec.n_r) / (33024 * 97)) if spec.precision == "split" else 0
-    ops = 5 * (spec.l_max + 1) * spec.n_r * (spec.n_r + 1) * 8
+    ops = 8 * (spec.l_max + 1) * spec.n_r * (spec.n_r + 1) * 8
     tables = 8 * lm * (n_theta // 2) * 8
     return int(1.25 * (arrays + fourier + images + ops + tables)) + (64 << 20)
 
@@ -121,7 +125,8 @@ class GraphRunner:
         with torch.cuda.stream(self.stream):
             self.st = BoussinesqStep(spec.l_max, spec.n_r, ek=spec.ek, ra=spec.ra, pr=spec.pr,
                                      prmag=spec.prmag, dt=spec.dt, precision=spec.precision,
-                                     device=device, cache=cache)
+                                     device=device, cache=cache,
+                                     radial_scheme=spec.radial_scheme)
             self.st.init_random(seed=spec.seed, amp=spec.amp)
             self._launch(eager=True)
             if use_graph and spec.n_steps > 1:
