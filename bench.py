@@ -416,7 +416,9 @@ def run_step(args, rank, world):
     l_max = 255 on the 97-level fourth-order finite-difference grid (radial loop
     with the fused nonlinear stage and the explicit terms, implicit solves of S, Z,
     W with the l = 0 pressure, B), device-timed with the state resident; the same
-    steps with the FP64 stage beside them."""
+    steps with the FP64 stage beside them.  --step-lmax / --levels /
+    --step-scheme chebyshev time other shells (Chebyshev levels take the
+    standard (w, p) form)."""
     from magic_b200.step import BoussinesqStep
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -424,9 +426,10 @@ def run_step(args, rank, world):
     dev = torch.device("cuda", local)
     res = {}
     for prec in ("split", "fp64"):
-        st = BoussinesqStep(L_MAX, args.levels, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
-                            precision=prec, device=dev)
+        st = BoussinesqStep(args.step_lmax, args.levels, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0,
+                            dt=2e-7, precision=prec, device=dev, radial_scheme=args.step_scheme)
         st.init_random(seed=rank, amp=1e-4)
+        grid = (st.plan.n_theta_max, st.plan.n_phi_max)
         for _ in range(args.warmup):
             st.step()
         torch.cuda.synchronize()
@@ -458,13 +461,16 @@ def run_step(args, rank, world):
     if rank == 0:
         sp, fp = res["split"], res["fp64"]
         print(json.dumps({
-            "metric": "IMEX steps/s @lmax=255 (whole CNAB2 step), 1 B200", "value": 1000.0 / sp["ms"],
+            "metric": f"IMEX steps/s @lmax={args.step_lmax} (whole CNAB2 step), 1 B200",
+            "value": 1000.0 / sp["ms"],
             "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": sp["ms"], "higher_is_better": True, "dtype": "bf16x3/f32 stage, f64 rest",
             "data": "synthetic",
-            "config": {"workload": "Boussinesq MHD dynamo step, FD4 double curl, CNAB2, dt fixed",
-                       "l_max": L_MAX, "n_theta": 384, "n_phi": 768, "n_r": args.levels,
-                       "l2": "state larger than L2"},
+            "config": {"workload": "Boussinesq MHD dynamo step, " + (
+                           "FD4 double curl" if args.step_scheme == "FD" else
+                           "Chebyshev, standard (w, p) form") + ", CNAB2, dt fixed",
+                       "l_max": args.step_lmax, "n_theta": grid[0], "n_phi": grid[1],
+                       "n_r": args.levels, "l2": "state larger than L2"},
             "fp64_stage_steps_per_s": 1000.0 / fp["ms"], "split_over_fp64": fp["ms"] / sp["ms"],
             "breakdown_ms": {p: {k: res[p][k] for k in ("radial_loop_ms", "implicit_ms")}
                              for p in res},
@@ -535,6 +541,84 @@ def run_serve(args, rank, world):
             "clocks": clocks.summary()}), flush=True)
 
 
+def run_sht(args, rank, world):
+    """Optional line: the standalone SHT round trip (l_max = 127, n_theta = 192,
+    n_phi = 384, minc = 1) batched over 65 radial levels x (1 scalar + 2 torpol
+    vector fields) through the drop-in transforms: scal_to_spat -> scal_to_SH on
+    the 65 scalar columns; torpol_to_spat -> scal_to_SH (br) + spat_to_sphertor
+    (bt, bp) on the 130 vector columns.  |c_lm| = (l+1)^-2 with phases uniform
+    from seed 0 (m = 0 real).  Per mode (FP64 and split): device time per round
+    trip, SHT TFLOP/s with the flop convention F = 4 n_theta/2 lm_max per
+    scalar-equivalent contraction and column (18 F per level: 1 + 1 scalar,
+    2 x (3 + 1 + 4) vector), and the round trip's relative error against its
+    input (largest value of each array; S, T from l >= 1)."""
+    from magic_b200 import Plan
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L_SHT, LEV = 127, 65
+    res = {}
+    for prec in ("split", "fp64"):
+        plan = Plan(L_SHT, 1, precision=prec, device=dev)
+        l = torch.as_tensor(plan.lm2l, dtype=torch.float64)
+        m0 = torch.as_tensor(plan.lm2m == 0)
+        g = torch.Generator(device="cpu").manual_seed(0)
+
+        def spec(B):
+            ph = torch.rand(plan.lm_max, B, generator=g, dtype=torch.float64) * 2 * math.pi
+            c = torch.polar(((l + 1.0) ** -2)[:, None].expand(-1, B).contiguous(), ph)
+            c[m0] = c[m0].real.to(c.dtype)
+            return c.to(dev)
+
+        sc, Q, S, T = spec(LEV), spec(2 * LEV), spec(2 * LEV), spec(2 * LEV)
+
+        def round_trip():
+            sc2 = plan.scal_to_SH(plan.scal_to_spat(sc))
+            br, bt, bp = plan.torpol_to_spat(Q, S, T)
+            return sc2, plan.scal_to_SH(br), *plan.spat_to_sphertor(bt, bp)
+
+        for _ in range(args.warmup):
+            round_trip()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clocks:
+            e0.record()
+            for _ in range(args.steps):
+                out = round_trip()
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        lpos = (l > 0).to(dev)
+        rel = lambda a, b: float((a - b).abs().max() / b.abs().max())
+        errs = {"scalar": rel(out[0], sc), "Q": rel(out[1], Q),
+                "S": rel(out[2][lpos], S[lpos]), "T": rel(out[3][lpos], T[lpos])}
+        flops = LEV * 18 * 4.0 * plan.nhs * plan.lm_max
+        res[prec] = dict(ms=ms, tflops=flops / (ms * 1e-3) / 1e12, round_trip_rel_err=errs,
+                         clocks=clocks.summary())
+        del plan
+        torch.cuda.empty_cache()
+    if rank == 0:
+        sp, fp = res["split"], res["fp64"]
+        peaks, src = measured_peaks()
+        print(json.dumps({
+            "metric": "SHT round-trip TFLOP/s @lmax=127, 65 levels x (1 scalar + 2 torpol), 1 B200",
+            "value": sp["tflops"], "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sp["ms"], "higher_is_better": True,
+            "dtype": "bf16x3/f32", "data": "synthetic",
+            "config": {"workload": "SHT round trip through the drop-in transforms", "l_max": L_SHT,
+                       "n_theta": 192, "n_phi": 384, "levels": LEV,
+                       "columns": {"scalar": LEV, "torpol": 2 * LEV},
+                       "flops_per_round_trip": LEV * 18 * 4.0 * 96 * 8256,
+                       "l2": "grids 268 MB per round trip, larger than L2"},
+            "round_trip_rel_err": sp["round_trip_rel_err"],
+            "fp64": {"value": fp["tflops"], "ms_per_step": fp["ms"],
+                     "round_trip_rel_err": fp["round_trip_rel_err"]},
+            "split_over_fp64": fp["ms"] / sp["ms"],
+            "peak_bf16_tflops": peaks["bf16_tflops"], "peak_source": src,
+            "clocks": sp["clocks"]}), flush=True)
+
+
 def measure_drift(args, dev, rank):
     """The split stage's drift from the FP64 stage: both run args.drift_steps whole
     steps from the same seeded state; max over w, z, s, b, aj of |split - fp64| /
@@ -590,12 +674,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--workload", default="bouss",
-                    choices=["bouss", "anel", "td", "step", "serve"],
-                    help="bouss: the headline Boussinesq MHD stage; anel: the fused anelastic "
+                    choices=["bouss", "anel", "td", "step", "serve", "sht"],
+                    help="bouss: the headline Boussinesq MHD stage; sht: the standalone SHT "
+                         "round trip at l_max=127 (extra line); anel: the fused anelastic "
                          "stage at l_max=383 (extra line, split precision); td: the explicit "
                          "time-derivative terms (get_td + finish_exp, FP64, extra line); "
                          "step: whole CNAB2 time steps, split and FP64 stage (extra line); "
                          "serve: the ensemble stream, continuous batching (extra line)")
+    ap.add_argument("--step-lmax", type=int, default=L_MAX, help="step: l_max of the shell")
+    ap.add_argument("--step-scheme", default="FD", choices=["FD", "chebyshev"],
+                    help="step: radial scheme (FD4 double curl or Chebyshev standard form)")
     ap.add_argument("--serve-runs", type=int, default=64, help="serve: runs in the stream")
     ap.add_argument("--serve-steps", type=int, default=200, help="serve: steps per run")
     ap.add_argument("--drift-steps", type=int, default=0,
@@ -623,6 +711,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, rank, world)
+        return
+    if args.workload == "sht":
+        run_sht(args, rank, world)
         return
 
     torch.cuda.set_device(local)
