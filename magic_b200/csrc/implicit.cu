@@ -710,6 +710,127 @@ __global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
   }
 }
 
+// The same update with the coupled solve on the FP64 tensor pipe, for
+// 2 n_r <= 256: CTA = 16 orders (4 m-tiles) of one degree, 8 warps.  The
+// rows' right-hand sides (w part, then p part, row stride fs) are the A
+// operand of solve_tile_dmma with the 2 n_r x 2 n_r operator streamed
+// through shared memory in 16-row chunks; the solution overwrites them.
+// Derivatives: thread = (4-row group, level), each D coefficient serving 4 rows.
+constexpr int kWpDmmaThreads = 256;
+constexpr int kWpDmmaMaxR = 128;
+
+__global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, int fs) {
+  extern __shared__ __align__(16) double2 wpd[];
+  __shared__ int lm_row[4 * kRows];
+  constexpr int rows = 4 * kRows;
+  const int n_r = a.n_r, n2 = 2 * n_r, l = blockIdx.y, mc0 = blockIdx.x * rows;
+  const int nrow = cta_rows(mc0, rows, l, a.minc, a.n_m);
+  if (nrow == 0) return;
+  double2* f = wpd;                               // [rows][fs]
+  double* mbuf = (double*)(wpd + rows * fs);      // 2 staged chunks of the operator
+  const double* Ml = a.mt + (int64_t)l * n2 * a.ldm;
+  if (l > 0) stage_chunk(Ml, n2, a.ldm, 0, mbuf);
+  if (threadIdx.x < rows)
+    lm_row[threadIdx.x] = threadIdx.x < nrow
+        ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
+  __syncthreads();
+  const double2 zero = {0.0, 0.0};
+  const double dL = (double)l * (l + 1.0);
+  for (int e = threadIdx.x; e < rows * n_r; e += blockDim.x) {
+    const int r = e / n_r, k = e - r * n_r;
+    double2 vw = zero, vp = zero;
+    if (r < nrow) {
+      const int64_t o = (int64_t)lm_row[r] * a.ld + k;
+      const double2 ow = a.wo[o], iw = a.wi[o], e0w = a.we0[o], e1w = a.we1[o];
+      const double2 op = a.po[o], ip = a.pi[o], e0p = a.pe0[o], e1p = a.pe1[o];
+      const double2 sv = a.s[o];
+      const double2 xv = a.xi ? a.xi[o] : zero;
+      a.we1[o] = e0w;
+      a.pe1[o] = e0p;
+      if (k > 0 && k < n_r - 1) {
+        const double gb = a.wimp_lin0 * a.rho0[k] * a.rgrav[k];
+        vw.x = a.w_old * ow.x + a.w_impl * iw.x + a.w_expl0 * e0w.x + a.w_expl1 * e1w.x +
+               gb * (a.BuoFac * sv.x + a.ChemFac * xv.x);
+        vw.y = a.w_old * ow.y + a.w_impl * iw.y + a.w_expl0 * e0w.y + a.w_expl1 * e1w.y +
+               gb * (a.BuoFac * sv.y + a.ChemFac * xv.y);
+        vp.x = a.w_old * op.x + a.w_impl * ip.x + a.w_expl0 * e0p.x + a.w_expl1 * e1p.x;
+        vp.y = a.w_old * op.y + a.w_impl * ip.y + a.w_expl0 * e0p.y + a.w_expl1 * e1p.y;
+      }
+    }
+    f[r * fs + k] = vw;
+    f[r * fs + n_r + k] = vp;
+  }
+  __syncthreads();
+  if (l == 0) {
+    // degree 0, one row: w = 0, the l = 0 pressure from its own right-hand side
+    // (built in the row's p half, then solved into the w half and copied)
+    const int64_t row0 = (int64_t)lm_row[0] * a.ld;
+    for (int k = threadIdx.x; k < n_r; k += blockDim.x) {
+      double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.we0[row0 + k].x;
+      if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
+      f[n_r + k] = double2{k == 0 ? 0.0 : v, 0.0};
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < n_r; j += blockDim.x)
+      f[j] = double2{op_row(a.P0, f + n_r, j).x, 0.0};
+    __syncthreads();
+    for (int j = threadIdx.x; j < n_r; j += blockDim.x) {
+      f[n_r + j] = f[j];
+      f[j] = zero;
+    }
+  } else {
+    solve_tile_dmma<4>(Ml, n2, a.ldm, fs, f, mbuf, 4, mc0);
+  }
+  __syncthreads();
+  const double hd = a.hdif[l];
+  const int groups = (nrow + kRows - 1) / kRows;
+  for (int e = threadIdx.x; e < groups * n_r; e += blockDim.x) {
+    const int rg = e / n_r, j = e - rg * n_r;
+    const double2* xw = f + rg * kRows * fs;
+    double2 d1[kRows], d2[kRows], d3[kRows], dp[kRows];
+    op_rows(a.D1, xw, fs, j, d1);
+    op_rows(a.D2, xw, fs, j, d2);
+    op_rows(a.D3, xw, fs, j, d3);
+    op_rows(a.D1, xw + n_r, fs, j, dp);
+    const double or1 = a.or1[j], or2 = a.or2[j], beta = a.beta[j], dbeta = a.dbeta[j];
+    const double visc = a.visc[j], dLv = a.dLvisc[j];
+    const double dLo = dL * or2, rg0 = a.rho0[j] * a.rgrav[j];
+    const double fw = hd * dLo * visc;
+    const double cw1 = 2.0 * dLv - beta / 3.0;
+    const double cw0 = dLo + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1);
+    const double cp2 = beta - dLv;
+    const double cp1 = dLo + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1;
+    const double cp0 = dLo * (2.0 * or1 + 2.0 / 3.0 * beta + dLv);
+    const bool zero_impl = a.impl_interior && (l == 0 || j == 0 || j == n_r - 1);
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const int row = rg * kRows + r;
+      if (row >= nrow) break;
+      const double2 w = xw[r * fs + j], p = xw[r * fs + n_r + j];
+      const int64_t o = (int64_t)lm_row[row] * a.ld + j;
+      const double2 sv = a.s[o];
+      const double2 xv = a.xi ? a.xi[o] : zero;
+      a.w[o] = w;
+      a.dw[o] = d1[r];
+      a.ddw[o] = d2[r];
+      a.p[o] = p;
+      a.dp[o] = dp[r];
+      a.wo[o] = double2{dLo * w.x, dLo * w.y};
+      a.po[o] = double2{-dLo * d1[r].x, -dLo * d1[r].y};
+      double2 iw, ip;
+      iw.x = -dp[r].x + beta * p.x + fw * (d2[r].x + cw1 * d1[r].x - cw0 * w.x) +
+             rg0 * (a.BuoFac * sv.x + a.ChemFac * xv.x);
+      iw.y = -dp[r].y + beta * p.y + fw * (d2[r].y + cw1 * d1[r].y - cw0 * w.y) +
+             rg0 * (a.BuoFac * sv.y + a.ChemFac * xv.y);
+      ip.x = dLo * p.x + fw * (-d3[r].x + cp2 * d2[r].x + cp1 * d1[r].x - cp0 * w.x);
+      ip.y = dLo * p.y + fw * (-d3[r].y + cp2 * d2[r].y + cp1 * d1[r].y - cp0 * w.y);
+      if (zero_impl) iw = ip = zero;
+      a.wi[o] = iw;
+      a.pi[o] = ip;
+    }
+  }
+}
+
 int check_lop(const mt_lop* op) {
   MT_REQUIRE(op && op->mt, MT_ERR_ARG, "null per-degree operator");
   int dev = -1;
@@ -926,6 +1047,19 @@ int mt_update_wp(const mt_plan* p, int n_r, const mt_wp_update* u, const mt_lop*
   a.D2 = radial_op_view(D2);
   a.D3 = radial_op_view(D3);
   a.P0 = radial_op_view(P0);
+  if (n_r <= kWpDmmaMaxR) {
+    // tensor-pipe tiling: rows 4 (mod 8) double2 apart (conflict-free A
+    // fragments), the operator's 16-row chunks double-buffered
+    const int fs = 2 * n_r + ((4 - 2 * n_r) & 7);
+    const size_t sm = (size_t)4 * kRows * fs * sizeof(double2) +
+                      (size_t)2 * kKc * a.ldm * sizeof(double);
+    MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_wp_dmma,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const dim3 grid((p->n_m + 4 * kRows - 1) / (4 * kRows), p->l_max + 1);
+    k_update_wp_dmma<<<grid, kWpDmmaThreads, sm, (cudaStream_t)stream>>>(a, fs);
+    MT_CHECK_CUDA(cudaGetLastError());
+    return MT_OK;
+  }
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_wp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   const dim3 grid((p->n_m + kWpRows - 1) / kWpRows, p->l_max + 1);

@@ -384,14 +384,18 @@ def test_update_wp_matches_reference():
         assert v < (TOL_IMPL if k in ("ddw", "p_impl", "w_impl", "dw") else TOL), (k, v)
 
 
-@pytest.mark.parametrize("l_max,minc,n_r,ktopv", [(127, 1, 65, 2), (32, 4, 33, 1)])
-def test_update_wp_vs_oracle(l_max, minc, n_r, ktopv):
+@pytest.mark.parametrize("l_max,minc,n_r,ktopv,scale", [(127, 1, 65, 2, 1.0), (32, 4, 33, 1, 1.0),
+                                                         (16, 1, 129, 2, 1e2)])
+def test_update_wp_vs_oracle(l_max, minc, n_r, ktopv, scale):
     """l_max = 127 on 65 Chebyshev levels (no-slip) and l_max = 32, minc = 4 on 33
     levels (stress-free) with anelastic-like profiles, against the oracle's LU
-    solves.  The coupled Chebyshev operator is far worse conditioned than the
-    scalar ones (its p rows carry d3rMat): the tolerances are relative to each
+    solves (the tensor-pipe tiling, n_r <= 128); l_max = 16 on 129 levels takes
+    the FMA tiling.  The coupled Chebyshev operator is far worse conditioned than
+    the scalar ones (its p rows carry d3rMat): the tolerances are relative to each
     array's largest value, 1e-11 for the fields and 1e-10 for the terms that
-    apply D2 / D3 to the new w."""
+    apply D2 / D3 to the new w, scaled by 100 at 129 levels (the conditioning
+    grows ~ n_r^4 and the D3 norm ~ n_r^6; measured there: fields <= 5.0e-12,
+    ddw 6.9e-10, p_impl 3.4e-9)."""
     from magic_b200 import Plan
     from magic_b200 import implicit as I
     from magic_b200.radial import RadialScheme
@@ -422,5 +426,5 @@ def test_update_wp_vs_oracle(l_max, minc, n_r, ktopv):
                                                 "w_expl1", "p_old", "p_impl", "p_expl1")}
     print({k: f"{v:.1e}" for k, v in errs.items()})
     for k, v in errs.items():
-        assert v < (1e-10 if k in ("ddw", "w_impl", "p_impl", "p_old", "dw", "dp") else 1e-11), \
-            (k, v)
+        assert v < scale * (1e-10 if k in ("ddw", "w_impl", "p_impl", "p_old", "dw", "dp")
+                            else 1e-11), (k, v)
