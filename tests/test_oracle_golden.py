@@ -399,3 +399,42 @@ def test_wp_solve_operators():
     x[0, N:] = P0 @ p0_rhs
     assert rel_err(x[:, :N], z["wp_w_new"]) < 1e-12
     assert rel_err(x[:, N:], z["wp_p_new"]) < 1e-12
+
+
+def test_wp_solve_operators_truncated():
+    """With fewer Chebyshev modes than levels (n_cheb < n_r: boundary rows and the
+    solution truncated, update_wp.py:309-313, 465-468) the library's folded
+    operators reproduce the oracle's coupled solve on seeded right-hand sides."""
+    from types import SimpleNamespace
+
+    from magic_b200 import implicit as I
+    from magic_b200.radial import cheb_polynomials
+    from oracle import implicit as oi
+    from oracle.td import dct1_matrix
+
+    N, nc, l_max = 17, 14, 6
+    T, dT, d2T, d3T = cheb_polynomials(N, 0.35, third=True)
+    sch = SimpleNamespace(n_r=N, chebyshev=True, n_cheb=nc, rMat=T, drMat=dT, d2rMat=d2T,
+                          d3rMat=d3T, rnorm=np.sqrt(2.0 / (N - 1)), boundary_fac=0.5)
+    r = np.cos(np.pi * np.arange(N) / (N - 1)) * 0.5 + 1.5 / 1.3
+    prof = dict(or1=1.0 / r, or2=1.0 / r ** 2, beta=-0.2 / r, dbeta=0.2 / r ** 2,
+                visc=np.ones(N), dLvisc=np.zeros(N), rgrav=r, rho0=np.ones(N))
+    hdif = np.ones(l_max + 1)
+    wl0 = 0.6e-4
+    M = I.wp_solve_operators(sch, l_max, wl0, hdif, prof, 1, 2)
+    rng = np.random.default_rng(2)
+    mats = (T, dT, d2T, sch.rnorm, sch.boundary_fac)
+    C = dct1_matrix(N)
+    for l in (1, 3, l_max):
+        rhs = rng.standard_normal(2 * N) + 1j * rng.standard_normal(2 * N)
+        rhs[[0, N - 1, N, 2 * N - 1]] = 0.0
+        got = M[l] @ rhs
+        dat = oi.wp_matrix(l, mats, d3T, prof, wl0, 1.0, nc, 1, 2)
+        fr = 1.0 / np.abs(dat).max(axis=1)
+        dat = fr[:, None] * dat
+        fc = 1.0 / np.abs(dat).max(axis=0)
+        y = fc * np.linalg.solve(dat * fc[None, :], fr * rhs)
+        y[nc:N] = 0.0
+        y[N + nc:] = 0.0
+        ref = np.concatenate([C @ y[:N], C @ y[N:]])
+        assert rel_err(got, ref) < 1e-11, (l, rel_err(got, ref))
