@@ -900,8 +900,8 @@ def main():
             line["fp64_plain"] = {"value": job_steps_per_s(world, plain), "unit": "steps/s",
                                   "ms_per_step": plain, "split_over_fp64": plain / ms,
                                   "what": "the same stage on an FP64 plan (DMMA Legendre, "
-                                          "FP64 phi stage), same inputs, device-timed"}
-            line["gpu_launches"] += 6 * args.steps
+                                          "FP64 phi stage), same inputs, device-timed",
+                                  "gpu_launches": 6 * args.steps}
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_stage_sample()
         print(json.dumps(line), flush=True)
