@@ -42,9 +42,10 @@ def write_e_mag_oc_line(f, time_out, em):
 
 
 def run(st, n_steps, output_dir, tag="gpu", log_every=100, checkpoint_every=0, start_step=0,
-        sim_time=0.0, cfg=None, t_scale=1.0, clock=time.perf_counter):
+        sim_time=0.0, cfg=None, t_scale=1.0, clock=time.perf_counter, adaptive=False):
     """Steps st from start_step + 1 to n_steps (main.py:843-886); returns sim_time.
-    A restart (start_step > 0) appends to existing files and writes no step-0 row."""
+    A restart (start_step > 0) appends to existing files and writes no step-0 row.
+    adaptive: the Courant control of dt every step, as the reference's run loop."""
     os.makedirs(output_dir, exist_ok=True)
     mode = "a" if start_step > 0 else "w"
     log_path = os.path.join(output_dir, "log.csv")
@@ -71,7 +72,10 @@ def run(st, n_steps, output_dir, tag="gpu", log_every=100, checkpoint_every=0, s
             write_row(0, sim_time, 0.0, 0)
         t0 = clock()
         for n in range(start_step + 1, n_steps + 1):
-            st.step()
+            if adaptive:
+                st.step(adaptive=True)
+            else:
+                st.step()
             sim_time += st.dt[0]
             if n % log_every == 0 or n == n_steps:
                 if torch.cuda.is_available():

@@ -16,8 +16,9 @@ magnetic field on:
                  form with the pressure of every degree), magnetic b and j
                  (mt_update_field), in the reference's order S, Z, W, B.
 
-The time step is held fixed (the solve operators are built once for it); the
-Courant limits of every step are returned for the caller's dt control.
+By default the time step is held fixed (the solve operators are built once
+for it) and the Courant limits of every step are returned; step(adaptive=True)
+applies the reference's Courant control of dt instead.
 Every launch is stream-ordered on the current stream; nothing synchronises.
 """
 
@@ -84,6 +85,7 @@ class BoussinesqStep:
         self._d1c = d1c
         # CNAB2 weights and the per-degree solve operators of the current dt pair
         self.dt = None
+        self.dt_max = float(dt)  # the Courant control's upper bound (initialize_dt)
         self.set_dt(dt, dt)
         self.P0 = self._shared(("P0",) + self._shape,
                                lambda: RadialOp(I.p0_inverse(self.sch, hp["beta"]), device=dev))
@@ -301,7 +303,33 @@ class BoussinesqStep:
         I.update_field(self.plan, self.sch, self.ops["j"], f["aj"], f["dj"], ta["j"], w,
                        self.coef["j"], d2x=f["ddj"])
 
-    def step(self):
+    def courant_dt(self, dtr, dth):
+        """(changed, dt_new) of the reference's Courant control of dt
+        (magic_torch/courant.py:130-155) from the per-level limits of this step's
+        radial loop: dt_2 = min(0.75 min(dtr, dth), dt_max); a step above dt_max
+        falls to dt_max, a step above the limit to dt_2, a step below half the limit
+        (and below dt_max) rises to dt_2.  Reads the minima on the host (one
+        synchronisation, as the reference's .item())."""
+        dt = self.dt[0]
+        dt_min = min(float(dtr.min()), float(dth.min()))
+        dt_2 = min(0.5 * (1.0 / 2.0 + 1.0) * dt_min, self.dt_max)
+        if dt > self.dt_max:
+            return True, self.dt_max
+        if dt > dt_min:
+            return True, dt_2
+        if 2.0 * dt < dt_min and dt < self.dt_max:
+            return True, dt_2
+        return False, dt
+
+    def step(self, adaptive=False):
+        """One CNAB2 step.  adaptive: the reference's one_step order
+        (step_time.py:1602-1633): radial loop, Courant decision, dt history rolled
+        and the CNAB2 weights (and, when the step size changed, the solve
+        operators) renewed, then the lm loop; the default keeps dt fixed and never
+        synchronises."""
         dtr, dth = self.radial_loop()
+        if adaptive:
+            _, dt_new = self.courant_dt(dtr, dth)
+            self.set_dt(dt_new, self.dt[0])
         self.lm_loop()
         return dtr, dth

@@ -66,6 +66,15 @@ RUN_CONFIGS = {
                       "prmag": 5.0, "dtmax": 1e-4, "mode": 0}, 500, 1e-5),
 }
 
+# CNAB2 steps with the Courant control of dt (courant.py:130-155; one_step
+# changes dt and rebuilds the matrices when the limit requires): the shell case
+# on Chebyshev levels with dtmax 1e-4 and seeded perturbations of s, w and z of
+# 1e-3, where the first step already cuts dt
+ADAPT_CONFIGS = {
+    "adapt_cheb": ({"l_max": 32, "minc": 4, "n_r_max": 33, "ek": 1e-3, "ra": 1e5, "pr": 1.0,
+                    "prmag": 5.0, "dtmax": 1e-4, "mode": 0}, 30),
+}
+
 # energies of seeded spectra (output.py:101-180) and the radial rule
 ENERGY_CONFIGS = {
     "energy_cheb": {"l_max": 8, "minc": 2, "n_r_max": 11, "prmag": 5.0, "ek": 1e-3},
@@ -539,6 +548,62 @@ def worker_run(name, ref):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 
+def worker_adapt(name, ref):
+    """The reference's initial state (initialize_fields, seeded perturbations of
+    s, w and z as worker_step draws them, setup_initial_state), then one_step with
+    the Courant control: the dt of every step, the energies after every step and
+    the fields after the last."""
+    import tempfile
+
+    cfg, nsteps = ADAPT_CONFIGS[name]
+    cfg = dict(cfg, device="cpu", use_shtns=False)
+    sys.path.insert(0, ref)
+    from magic_torch.config import configure
+    configure(cfg)
+    import torch
+    from magic_torch import params, blocking, fields
+    from magic_torch.init_fields import initialize_fields
+    from magic_torch.step_time import setup_initial_state, one_step, initialize_dt
+    from magic_torch.main import save_checkpoint
+    from magic_torch.output import get_e_kin_full, get_e_mag_oc_full
+    from magic_torch.time_scheme import tscheme
+    n = lambda x: x.detach().cpu().numpy().copy()
+    N, lm = params.n_r_max, params.lm_max
+    initialize_fields()
+    g = torch.Generator().manual_seed(11)
+    m0 = blocking.st_lm2m == 0
+    for fld, amp in (("s_LMloc", 1e-3), ("w_LMloc", 1e-3), ("z_LMloc", 1e-3)):
+        c = torch.complex(torch.randn(lm, N, generator=g, dtype=torch.float64),
+                          torch.randn(lm, N, generator=g, dtype=torch.float64)) * amp
+        c[m0] = c[m0].real.to(c.dtype)
+        getattr(fields, fld)[:, 1:-1] += c[:, 1:-1]
+    setup_initial_state()
+    dt = float(cfg["dtmax"])
+    initialize_dt(dt)
+    out = dict(n_r_max=N, l_max=params.l_max, minc=params.minc, lm_max=lm, dtmax=dt,
+               ek=cfg["ek"], ra=cfg["ra"], pr=cfg["pr"], prmag=cfg["prmag"],
+               radratio=float(params.radratio), steps=nsteps)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "ck.pt")
+        save_checkpoint(path, 0, 0.0, {"tag": "golden"})
+        st = torch.load(path, weights_only=False)
+    for k, v in st.items():
+        if torch.is_tensor(v) and v.dim() >= 2:
+            out["0:" + k] = n(v)
+    out["0:tscheme_dt"] = n(tscheme.dt)
+    dts, ek_t, em_t = [], [], []
+    for step in range(1, nsteps + 1):
+        dt = one_step(step, dt)
+        dts.append(dt)
+        ek_t.append(np.array(get_e_kin_full(fields.w_LMloc, fields.dw_LMloc, fields.z_LMloc)))
+        em_t.append(np.array(get_e_mag_oc_full(fields.b_LMloc, fields.db_LMloc,
+                                               fields.aj_LMloc)))
+    out["dt"], out["e_kin"], out["e_mag"] = np.array(dts), np.stack(ek_t), np.stack(em_t)
+    for k in ("w", "z", "s", "p", "b", "aj"):
+        out[f"{nsteps}:{k}"] = n(getattr(fields, k + "_LMloc"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
@@ -554,6 +619,8 @@ def main():
             worker_step(a.worker, a.ref)
         elif a.worker in RUN_CONFIGS:
             worker_run(a.worker, a.ref)
+        elif a.worker in ADAPT_CONFIGS:
+            worker_adapt(a.worker, a.ref)
         elif a.worker in ENERGY_CONFIGS:
             worker_energy(a.worker, a.ref)
         else:
@@ -561,7 +628,7 @@ def main():
         return
     env = dict(os.environ, TORCHDYNAMO_DISABLE="1", MAGIC_DEVICE="cpu")
     names = list(SHT_CONFIGS) + list(NL_CONFIGS) + list(TD_CONFIGS) + list(STEP_CONFIGS)
-    names += list(ENERGY_CONFIGS) + list(RUN_CONFIGS)
+    names += list(ENERGY_CONFIGS) + list(RUN_CONFIGS) + list(ADAPT_CONFIGS)
     if a.only:
         names = [x for x in names if x in a.only.split(",")]
     for name in names:
