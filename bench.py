@@ -162,10 +162,11 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) of one launch of the phi-stage kernel from an ncu
-# capture of the same kernel at n_r = 17 (profiles/split_stage_kernels_l255_n17_ncu.md),
-# per Fourier row moved (13 fields x n_r in, 9 fields x (n_r - 2) out); traffic grows
+# full-set capture of the same kernel at l_max = 255, n_r = 17, per Fourier row moved (13 fields x n_r in, 9 fields x (n_r - 2) out); traffic grows
 # in proportion to the rows, so the full-size launch is scaled by its row count.
 NCU_PHI_TRAFFIC = {"split": (230.161408e6 + 104.267520e6) / (13 * 17 + 9 * 15)}
+# warp instructions of the same launch (smsp__inst_executed.sum), per Fourier row
+NCU_PHI_INST = {"split": 184287744.0 / (13 * 17 + 9 * 15)}
 
 
 def measured_peaks():
@@ -862,6 +863,19 @@ def main():
                 "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "algorithmic_bytes": byts,
                 "kernel": dom, "peak_source": src,
                 "traffic_source": "ncu dram bytes at n_r=17 scaled by rows" if per_row else None}
+        # the kernel is issue-bound, not HBM-bound: warp instructions per second
+        # against the SM partitions' issue peak (one warp instruction per clock
+        # per partition, 4 partitions per SM) at the clock sampled in the run
+        inst_row = NCU_PHI_INST.get(args.precision)
+        if inst_row:
+            props = torch.cuda.get_device_properties(dev)
+            mhz = clocks.summary().get("sm_mhz") or 1965.0
+            inst = inst_row * (13 * n_r + 9 * (n_r - 2))
+            rate = inst / (part_ms[dom] * 1e-3)
+            peak_issue = props.multi_processor_count * 4 * mhz * 1e6
+            roof["issue"] = {"warp_instructions": inst, "achieved": rate, "peak": peak_issue,
+                             "unit": "warp inst/s", "frac": rate / peak_issue,
+                             "source": "ncu smsp__inst_executed.sum at n_r=17 scaled by rows"}
     elif split:
         s_mma, a_mma = split_mma_flops(plan, n_r)
         fl = s_mma if dom == "legendre_synthesis" else a_mma

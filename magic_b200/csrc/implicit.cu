@@ -591,6 +591,86 @@ struct WpArgs {
   OpView D1, D2, D3, P0;
 };
 
+// CNAB2 right-hand sides of element o (level k) of both equations, with the
+// buoyancy coupling on the w rows and zero boundary rows, and the rotation
+// expl1 <- expl0 of both histories
+__device__ __forceinline__ void wp_rhs(const WpArgs& a, int64_t o, int k, double2& vw,
+                                       double2& vp) {
+  const double2 zero = {0.0, 0.0};
+  const double2 ow = a.wo[o], iw = a.wi[o], e0w = a.we0[o], e1w = a.we1[o];
+  const double2 op = a.po[o], ip = a.pi[o], e0p = a.pe0[o], e1p = a.pe1[o];
+  const double2 sv = a.s[o];
+  const double2 xv = a.xi ? a.xi[o] : zero;
+  a.we1[o] = e0w;
+  a.pe1[o] = e0p;
+  vw = vp = zero;
+  if (k > 0 && k < a.n_r - 1) {
+    const double gb = a.wimp_lin0 * a.rho0[k] * a.rgrav[k];
+    vw.x = a.w_old * ow.x + a.w_impl * iw.x + a.w_expl0 * e0w.x + a.w_expl1 * e1w.x +
+           gb * (a.BuoFac * sv.x + a.ChemFac * xv.x);
+    vw.y = a.w_old * ow.y + a.w_impl * iw.y + a.w_expl0 * e0w.y + a.w_expl1 * e1w.y +
+           gb * (a.BuoFac * sv.y + a.ChemFac * xv.y);
+    vp.x = a.w_old * op.x + a.w_impl * ip.x + a.w_expl0 * e0p.x + a.w_expl1 * e1p.x;
+    vp.y = a.w_old * op.y + a.w_impl * ip.y + a.w_expl0 * e0p.y + a.w_expl1 * e1p.y;
+  }
+}
+
+// right-hand side of the l = 0 pressure at level k (row (0, 0))
+__device__ __forceinline__ double wp_p0_rhs(const WpArgs& a, int64_t row0, int k) {
+  double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.we0[row0 + k].x;
+  if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
+  return k == 0 ? 0.0 : v;
+}
+
+// radial coefficients of the implicit terms at level j of degree l
+struct WpCoef {
+  double dLo, beta, fw, cw1, cw0, cp2, cp1, cp0, rg;
+  bool zero_impl;
+};
+__device__ __forceinline__ WpCoef wp_coef(const WpArgs& a, int l, int j) {
+  const double dL = (double)l * (l + 1.0);
+  const double or1 = a.or1[j], or2 = a.or2[j], beta = a.beta[j], dbeta = a.dbeta[j];
+  const double dLv = a.dLvisc[j];
+  WpCoef c;
+  c.dLo = dL * or2;
+  c.beta = beta;
+  c.fw = a.hdif[l] * c.dLo * a.visc[j];
+  c.cw1 = 2.0 * dLv - beta / 3.0;
+  c.cw0 = c.dLo + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1);
+  c.cp2 = beta - dLv;
+  c.cp1 = c.dLo + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1;
+  c.cp0 = c.dLo * (2.0 * or1 + 2.0 / 3.0 * beta + dLv);
+  c.rg = a.rho0[j] * a.rgrav[j];
+  c.zero_impl = a.impl_interior && (l == 0 || j == 0 || j == a.n_r - 1);
+  return c;
+}
+
+// new fields, derivatives, old and implicit terms of element o
+__device__ __forceinline__ void wp_store(const WpArgs& a, const WpCoef& c, int64_t o, double2 w,
+                                         double2 p, double2 d1, double2 d2, double2 d3,
+                                         double2 dp) {
+  const double2 zero = {0.0, 0.0};
+  const double2 sv = a.s[o];
+  const double2 xv = a.xi ? a.xi[o] : zero;
+  a.w[o] = w;
+  a.dw[o] = d1;
+  a.ddw[o] = d2;
+  a.p[o] = p;
+  a.dp[o] = dp;
+  a.wo[o] = double2{c.dLo * w.x, c.dLo * w.y};
+  a.po[o] = double2{-c.dLo * d1.x, -c.dLo * d1.y};
+  double2 iw, ip;
+  iw.x = -dp.x + c.beta * p.x + c.fw * (d2.x + c.cw1 * d1.x - c.cw0 * w.x) +
+         c.rg * (a.BuoFac * sv.x + a.ChemFac * xv.x);
+  iw.y = -dp.y + c.beta * p.y + c.fw * (d2.y + c.cw1 * d1.y - c.cw0 * w.y) +
+         c.rg * (a.BuoFac * sv.y + a.ChemFac * xv.y);
+  ip.x = c.dLo * p.x + c.fw * (-d3.x + c.cp2 * d2.x + c.cp1 * d1.x - c.cp0 * w.x);
+  ip.y = c.dLo * p.y + c.fw * (-d3.y + c.cp2 * d2.y + c.cp1 * d1.y - c.cp0 * w.y);
+  if (c.zero_impl) iw = ip = zero;
+  a.wi[o] = iw;
+  a.pi[o] = ip;
+}
+
 __global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
   extern __shared__ __align__(16) double2 wpbuf[];
   __shared__ int lm_row[kWpRows];
@@ -604,43 +684,19 @@ __global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
         ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
   __syncthreads();
   const double2 zero = {0.0, 0.0};
-  const double dL = (double)l * (l + 1.0);
-  // CNAB2 right-hand sides and the rotation of both explicit histories
   for (int e = threadIdx.x; e < kWpRows * n_r; e += blockDim.x) {
     const int r = e / n_r, k = e - r * n_r;
     double2 vw = zero, vp = zero;
-    if (r < nrow) {
-      const int64_t o = (int64_t)lm_row[r] * a.ld + k;
-      const double2 ow = a.wo[o], iw = a.wi[o], e0w = a.we0[o], e1w = a.we1[o];
-      const double2 op = a.po[o], ip = a.pi[o], e0p = a.pe0[o], e1p = a.pe1[o];
-      const double2 sv = a.s[o];
-      const double2 xv = a.xi ? a.xi[o] : zero;
-      a.we1[o] = e0w;
-      a.pe1[o] = e0p;
-      if (k > 0 && k < n_r - 1) {
-        const double gb = a.wimp_lin0 * a.rho0[k] * a.rgrav[k];
-        vw.x = a.w_old * ow.x + a.w_impl * iw.x + a.w_expl0 * e0w.x + a.w_expl1 * e1w.x +
-               gb * (a.BuoFac * sv.x + a.ChemFac * xv.x);
-        vw.y = a.w_old * ow.y + a.w_impl * iw.y + a.w_expl0 * e0w.y + a.w_expl1 * e1w.y +
-               gb * (a.BuoFac * sv.y + a.ChemFac * xv.y);
-        vp.x = a.w_old * op.x + a.w_impl * ip.x + a.w_expl0 * e0p.x + a.w_expl1 * e1p.x;
-        vp.y = a.w_old * op.y + a.w_impl * ip.y + a.w_expl0 * e0p.y + a.w_expl1 * e1p.y;
-      }
-    }
+    if (r < nrow) wp_rhs(a, (int64_t)lm_row[r] * a.ld + k, k, vw, vp);
     f[r * n2 + k] = vw;
     f[r * n2 + n_r + k] = vp;
   }
   __syncthreads();
   if (l == 0) {
     // degree 0 (one row, (l, m) = (0, 0)): w = 0; the l = 0 pressure from its
-    // own right-hand side, built in f's first n_r entries (the expl0 loads
-    // above were of the same row)
+    // own right-hand side, built in f's first n_r entries
     const int64_t row0 = (int64_t)lm_row[0] * a.ld;
-    for (int k = threadIdx.x; k < n_r; k += blockDim.x) {
-      double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.we0[row0 + k].x;
-      if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
-      f[k] = double2{k == 0 ? 0.0 : v, 0.0};
-    }
+    for (int k = threadIdx.x; k < n_r; k += blockDim.x) f[k] = double2{wp_p0_rhs(a, row0, k), 0.0};
     __syncthreads();
     for (int j = threadIdx.x; j < n_r; j += blockDim.x) {
       x[j] = zero;
@@ -670,43 +726,12 @@ __global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
     }
   }
   __syncthreads();
-  const double hd = a.hdif[l];
   for (int e = threadIdx.x; e < nrow * n_r; e += blockDim.x) {
     const int r = e / n_r, j = e - r * n_r;
     const double2* xw = x + r * n2;
     const double2* xp = xw + n_r;
-    const double2 w = xw[j], p = xp[j];
-    const double2 d1 = op_row(a.D1, xw, j), d2 = op_row(a.D2, xw, j);
-    const double2 d3 = op_row(a.D3, xw, j), dp = op_row(a.D1, xp, j);
-    const int64_t o = (int64_t)lm_row[r] * a.ld + j;
-    const double2 sv = a.s[o];
-    const double2 xv = a.xi ? a.xi[o] : zero;
-    const double or1 = a.or1[j], or2 = a.or2[j], beta = a.beta[j], dbeta = a.dbeta[j];
-    const double visc = a.visc[j], dLv = a.dLvisc[j];
-    const double dLo = dL * or2, rg = a.rho0[j] * a.rgrav[j];
-    const double fw = hd * dLo * visc;
-    const double cw1 = 2.0 * dLv - beta / 3.0;
-    const double cw0 = dLo + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1);
-    const double cp2 = beta - dLv;
-    const double cp1 = dLo + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1;
-    const double cp0 = dLo * (2.0 * or1 + 2.0 / 3.0 * beta + dLv);
-    a.w[o] = w;
-    a.dw[o] = d1;
-    a.ddw[o] = d2;
-    a.p[o] = p;
-    a.dp[o] = dp;
-    a.wo[o] = double2{dLo * w.x, dLo * w.y};
-    a.po[o] = double2{-dLo * d1.x, -dLo * d1.y};
-    double2 iw, ip;
-    iw.x = -dp.x + beta * p.x + fw * (d2.x + cw1 * d1.x - cw0 * w.x) +
-           rg * (a.BuoFac * sv.x + a.ChemFac * xv.x);
-    iw.y = -dp.y + beta * p.y + fw * (d2.y + cw1 * d1.y - cw0 * w.y) +
-           rg * (a.BuoFac * sv.y + a.ChemFac * xv.y);
-    ip.x = dLo * p.x + fw * (-d3.x + cp2 * d2.x + cp1 * d1.x - cp0 * w.x);
-    ip.y = dLo * p.y + fw * (-d3.y + cp2 * d2.y + cp1 * d1.y - cp0 * w.y);
-    if (a.impl_interior && (l == 0 || j == 0 || j == n_r - 1)) iw = ip = zero;
-    a.wi[o] = iw;
-    a.pi[o] = ip;
+    wp_store(a, wp_coef(a, l, j), (int64_t)lm_row[r] * a.ld + j, xw[j], xp[j],
+             op_row(a.D1, xw, j), op_row(a.D2, xw, j), op_row(a.D3, xw, j), op_row(a.D1, xp, j));
   }
 }
 
@@ -735,28 +760,10 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
         ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
   __syncthreads();
   const double2 zero = {0.0, 0.0};
-  const double dL = (double)l * (l + 1.0);
   for (int e = threadIdx.x; e < rows * n_r; e += blockDim.x) {
     const int r = e / n_r, k = e - r * n_r;
     double2 vw = zero, vp = zero;
-    if (r < nrow) {
-      const int64_t o = (int64_t)lm_row[r] * a.ld + k;
-      const double2 ow = a.wo[o], iw = a.wi[o], e0w = a.we0[o], e1w = a.we1[o];
-      const double2 op = a.po[o], ip = a.pi[o], e0p = a.pe0[o], e1p = a.pe1[o];
-      const double2 sv = a.s[o];
-      const double2 xv = a.xi ? a.xi[o] : zero;
-      a.we1[o] = e0w;
-      a.pe1[o] = e0p;
-      if (k > 0 && k < n_r - 1) {
-        const double gb = a.wimp_lin0 * a.rho0[k] * a.rgrav[k];
-        vw.x = a.w_old * ow.x + a.w_impl * iw.x + a.w_expl0 * e0w.x + a.w_expl1 * e1w.x +
-               gb * (a.BuoFac * sv.x + a.ChemFac * xv.x);
-        vw.y = a.w_old * ow.y + a.w_impl * iw.y + a.w_expl0 * e0w.y + a.w_expl1 * e1w.y +
-               gb * (a.BuoFac * sv.y + a.ChemFac * xv.y);
-        vp.x = a.w_old * op.x + a.w_impl * ip.x + a.w_expl0 * e0p.x + a.w_expl1 * e1p.x;
-        vp.y = a.w_old * op.y + a.w_impl * ip.y + a.w_expl0 * e0p.y + a.w_expl1 * e1p.y;
-      }
-    }
+    if (r < nrow) wp_rhs(a, (int64_t)lm_row[r] * a.ld + k, k, vw, vp);
     f[r * fs + k] = vw;
     f[r * fs + n_r + k] = vp;
   }
@@ -765,11 +772,8 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
     // degree 0, one row: w = 0, the l = 0 pressure from its own right-hand side
     // (built in the row's p half, then solved into the w half and copied)
     const int64_t row0 = (int64_t)lm_row[0] * a.ld;
-    for (int k = threadIdx.x; k < n_r; k += blockDim.x) {
-      double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.we0[row0 + k].x;
-      if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
-      f[n_r + k] = double2{k == 0 ? 0.0 : v, 0.0};
-    }
+    for (int k = threadIdx.x; k < n_r; k += blockDim.x)
+      f[n_r + k] = double2{wp_p0_rhs(a, row0, k), 0.0};
     __syncthreads();
     for (int j = threadIdx.x; j < n_r; j += blockDim.x)
       f[j] = double2{op_row(a.P0, f + n_r, j).x, 0.0};
@@ -782,7 +786,6 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
     solve_tile_dmma<4>(Ml, n2, a.ldm, fs, f, mbuf, 4, mc0);
   }
   __syncthreads();
-  const double hd = a.hdif[l];
   const int groups = (nrow + kRows - 1) / kRows;
   for (int e = threadIdx.x; e < groups * n_r; e += blockDim.x) {
     const int rg = e / n_r, j = e - rg * n_r;
@@ -792,41 +795,13 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
     op_rows(a.D2, xw, fs, j, d2);
     op_rows(a.D3, xw, fs, j, d3);
     op_rows(a.D1, xw + n_r, fs, j, dp);
-    const double or1 = a.or1[j], or2 = a.or2[j], beta = a.beta[j], dbeta = a.dbeta[j];
-    const double visc = a.visc[j], dLv = a.dLvisc[j];
-    const double dLo = dL * or2, rg0 = a.rho0[j] * a.rgrav[j];
-    const double fw = hd * dLo * visc;
-    const double cw1 = 2.0 * dLv - beta / 3.0;
-    const double cw0 = dLo + 4.0 / 3.0 * (dbeta + dLv * beta + (3.0 * dLv + beta) * or1);
-    const double cp2 = beta - dLv;
-    const double cp1 = dLo + dLv * beta + dbeta + 2.0 * (dLv + beta) * or1;
-    const double cp0 = dLo * (2.0 * or1 + 2.0 / 3.0 * beta + dLv);
-    const bool zero_impl = a.impl_interior && (l == 0 || j == 0 || j == n_r - 1);
+    const WpCoef c = wp_coef(a, l, j);
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
       const int row = rg * kRows + r;
       if (row >= nrow) break;
-      const double2 w = xw[r * fs + j], p = xw[r * fs + n_r + j];
-      const int64_t o = (int64_t)lm_row[row] * a.ld + j;
-      const double2 sv = a.s[o];
-      const double2 xv = a.xi ? a.xi[o] : zero;
-      a.w[o] = w;
-      a.dw[o] = d1[r];
-      a.ddw[o] = d2[r];
-      a.p[o] = p;
-      a.dp[o] = dp[r];
-      a.wo[o] = double2{dLo * w.x, dLo * w.y};
-      a.po[o] = double2{-dLo * d1[r].x, -dLo * d1[r].y};
-      double2 iw, ip;
-      iw.x = -dp[r].x + beta * p.x + fw * (d2[r].x + cw1 * d1[r].x - cw0 * w.x) +
-             rg0 * (a.BuoFac * sv.x + a.ChemFac * xv.x);
-      iw.y = -dp[r].y + beta * p.y + fw * (d2[r].y + cw1 * d1[r].y - cw0 * w.y) +
-             rg0 * (a.BuoFac * sv.y + a.ChemFac * xv.y);
-      ip.x = dLo * p.x + fw * (-d3[r].x + cp2 * d2[r].x + cp1 * d1[r].x - cp0 * w.x);
-      ip.y = dLo * p.y + fw * (-d3[r].y + cp2 * d2[r].y + cp1 * d1[r].y - cp0 * w.y);
-      if (zero_impl) iw = ip = zero;
-      a.wi[o] = iw;
-      a.pi[o] = ip;
+      wp_store(a, c, (int64_t)lm_row[row] * a.ld + j, xw[r * fs + j], xw[r * fs + n_r + j],
+               d1[r], d2[r], d3[r], dp[r]);
     }
   }
 }
