@@ -34,6 +34,22 @@ from .radial import RadialOp, RadialScheme
 _CD = torch.complex128
 
 
+def dt_courant(dt, dt_max, dt_min):
+    """(changed, dt_new) of the reference's Courant control of dt
+    (magic_torch/courant.py:130-155) for the current step dt and the smallest
+    Courant limit dt_min over the levels: with dt_2 = min(0.75 dt_min, dt_max), a
+    step above dt_max falls to dt_max, a step above the limit to dt_2, and a step
+    below half the limit (and below dt_max) rises to dt_2."""
+    dt_2 = min(0.5 * (1.0 / 2.0 + 1.0) * dt_min, dt_max)
+    if dt > dt_max:
+        return True, dt_max
+    if dt > dt_min:
+        return True, dt_2
+    if 2.0 * dt < dt_min and dt < dt_max:
+        return True, dt_2
+    return False, dt
+
+
 class BoussinesqStep:
     def __init__(self, l_max, n_r, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
                  precision="split", radratio=0.35, fd_order=4, fd_order_bound=2, ktopv=2,
@@ -304,22 +320,10 @@ class BoussinesqStep:
                        self.coef["j"], d2x=f["ddj"])
 
     def courant_dt(self, dtr, dth):
-        """(changed, dt_new) of the reference's Courant control of dt
-        (magic_torch/courant.py:130-155) from the per-level limits of this step's
-        radial loop: dt_2 = min(0.75 min(dtr, dth), dt_max); a step above dt_max
-        falls to dt_max, a step above the limit to dt_2, a step below half the limit
-        (and below dt_max) rises to dt_2.  Reads the minima on the host (one
+        """(changed, dt_new) of the Courant control (dt_courant) from the per-level
+        limits of this step's radial loop.  Reads the minima on the host (one
         synchronisation, as the reference's .item())."""
-        dt = self.dt[0]
-        dt_min = min(float(dtr.min()), float(dth.min()))
-        dt_2 = min(0.5 * (1.0 / 2.0 + 1.0) * dt_min, self.dt_max)
-        if dt > self.dt_max:
-            return True, self.dt_max
-        if dt > dt_min:
-            return True, dt_2
-        if 2.0 * dt < dt_min and dt < self.dt_max:
-            return True, dt_2
-        return False, dt
+        return dt_courant(self.dt[0], self.dt_max, min(float(dtr.min()), float(dth.min())))
 
     def step(self, adaptive=False):
         """One CNAB2 step.  adaptive: the reference's one_step order

@@ -148,3 +148,30 @@ def test_run_outputs_follow_the_reference_layout(tmp_path):
     rows = list(csv.reader(open(tmp_path / "log.csv")))
     assert [r[0] for r in rows].count("step") == 1
     assert [int(r[0]) for r in rows[1:]] == [0, 3, 6, 7, 6, 9]
+
+
+def test_dt_courant_matches_oracle_and_reference_sequence():
+    """The time step's Courant control (magic_b200.step.dt_courant) takes the same
+    branch and value as the oracle's restatement of courant.py:130-155 on every
+    regime (above dt_max, above the limit, far below it, in the keep band), and
+    replays the reference's own dt sequence of tests/golden/adapt_cheb.npz: each
+    decision from the previous dt and dtmax lands on the reference's next dt when
+    fed the limit that decision implies (dt_min = dt_new / 0.75)."""
+    import numpy as np
+
+    from conftest import load_golden
+    from magic_b200.step import dt_courant
+    from oracle.nonlinear import dt_courant as ref_dt_courant
+
+    cases = [(2e-4, 1e-4, 5e-4), (1e-4, 1e-4, 5e-5), (1e-6, 1e-4, 5e-5), (1e-5, 1e-4, 1.5e-5),
+             (1e-4, 1e-4, 1e-3), (4e-5, 1e-4, 6e-5)]
+    for dt, dtmax, dmin in cases:
+        assert dt_courant(dt, dtmax, dmin) == ref_dt_courant(dt, dtmax, dmin, dmin), (dt, dmin)
+    z = load_golden("adapt_cheb")
+    dts, dtmax = [float(x) for x in z["dt"]], float(z["dtmax"])
+    prev = dtmax
+    for d in dts:
+        if d != prev and d < dtmax:
+            changed, new = dt_courant(prev, dtmax, d / 0.75)
+            assert changed and abs(new - d) <= 1e-15 * d, (prev, d, new)
+        prev = d
