@@ -55,7 +55,10 @@ enum mt_status {
 
 enum mt_precision {
   MT_PREC_FP64 = 0,       /* plain FP64 Legendre contractions (DMMA)        */
-  MT_PREC_SPLIT = 1       /* split-BF16 tcgen05 contractions, FP32 accumulate */
+  MT_PREC_SPLIT = 1,      /* split-BF16 tcgen05 contractions, FP32 accumulate */
+  MT_PREC_OZAKI = 2       /* fused stage: int8 digit planes on tcgen05 with
+                             exact int32 accumulation, FP64 phi stage (about
+                             1e-12 of scale); transforms as MT_PREC_FP64     */
 };
 
 /* Grid description.  n_theta_max / n_phi_max = 0 derive the reference's
@@ -104,12 +107,18 @@ MT_API int mt_scal_to_spat(const mt_plan* plan, const double* Slm, int64_t ld, i
  * mt_scal_to_spat, but the workspace is a fixed array of
  * MT_NOALLOC_SCRATCH_BYTES inside the library: every GPU that loads the
  * library holds it until the process exits.  B is limited to
- * n_m_max * n_theta_max * B * 16 <= MT_NOALLOC_SCRATCH_BYTES (about 10
- * columns at l_max = 255); larger B returns MT_ERR_WORKSPACE before any
- * launch.  The first call on a device looks up the array's device address
- * (no allocation); make that first call before any stream capture.  All calls
- * on a device share the array: calls that can overlap on the GPU (different
- * streams, different host threads) race and must be serialised by the caller. */
+ * mt_transform_workspace(plan, B, 1) <= MT_NOALLOC_SCRATCH_BYTES: for FP64
+ * plans that is n_m_max * n_theta_max * B * 16 bytes (about 10 columns at
+ * l_max = 255); split plans also keep their operand images there and allow
+ * fewer columns.  Larger B returns MT_ERR_WORKSPACE before any launch.  The
+ * first call on a device looks up the array's device address (no allocation);
+ * make that first call before any stream capture.  The address is kept per
+ * device ordinal for the life of the process, so a context reset on that
+ * device (cudaDeviceReset) requires a process restart before the next call.
+ * All calls on a device share the array: calls that can overlap on the GPU
+ * (different streams, different host threads) race and must be serialised by
+ * the caller.  With a split plan, a device-side wait that ran out is reported
+ * only through mt_noalloc_status (the array is not the caller's to read). */
 #define MT_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 MT_API int mt_scal_to_spat_noalloc(const mt_plan* plan, const double* Slm, int64_t ld, int B,
                                    double* grid, void* stream);
@@ -445,6 +454,26 @@ MT_API int mt_energy(const mt_plan* plan, int n_r, const mt_energy_args* e, doub
                      void* work, size_t work_bytes, void* stream);
 
 MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
+
+/* ---- device status of the split-precision kernels ----------------------- */
+
+/* The tcgen05 kernels of split-precision plans bound every wait on the tensor
+ * pipe and on their bulk copies.  A wait that runs out stops the CTA, and the
+ * kernel records a non-zero code in the first 4 bytes of the call's `work`
+ * buffer; the results of that call are then invalid (the entry point itself
+ * returned MT_OK: it does not synchronise).  The code stays there until the
+ * next call that reuses the buffer clears it.  mt_device_status copies it into
+ * *code after the work enqueued on `stream` so far has finished (it
+ * synchronises `stream`).  0 means every wait completed; FP64 plans never
+ * write the word (their kernels have no such waits) and always read 0 when
+ * the buffer was cleared by a split call or zero-initialised.  No counterpart
+ * in the reference (its bmm path has no device-side waits). */
+MT_API int mt_device_status(const void* work, int* code, void* stream);
+
+/* The same for the fixed scratch of mt_scal_to_spat_noalloc (the caller has
+ * no pointer to it): the code of the last allocation-free call on the current
+ * device. */
+MT_API int mt_noalloc_status(int* code, void* stream);
 
 /* Thread-local message for the last non-zero status. */
 MT_API const char* mt_last_error(void);

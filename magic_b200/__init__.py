@@ -9,6 +9,7 @@ libmagic_b200.so), driven from Python through ctypes on torch CUDA tensors.
 * ``Plan.nl_bouss``          the fused radial-loop nonlinear stage
 """
 
+from ._lib import MagicError  # noqa: F401
 from .config import configure, configure_from_reference  # noqa: F401
 from .plan import Plan  # noqa: F401
 

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libmagic_b200.so")
 MT_OK = 0
 MT_PREC_FP64 = 0
 MT_PREC_SPLIT = 1
+MT_PREC_OZAKI = 2
 
 _dp = C.c_void_p  # device pointer
 _i64 = C.c_int64
@@ -175,6 +176,8 @@ _PROTOS = {
     "mt_update_wp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(WpUpdate), C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
+    "mt_device_status": (C.c_int, [_dp, C.POINTER(C.c_int), _dp]),
+    "mt_noalloc_status": (C.c_int, [C.POINTER(C.c_int), _dp]),
     "mt_last_error": (C.c_char_p, []),
 }
 
@@ -208,3 +211,38 @@ def check(rc):
     if rc != MT_OK:
         msg = lib().mt_last_error().decode(errors="replace")
         raise MagicError(f"magic_b200 status {rc}: {msg}")
+
+
+# Codes the split-precision kernels record in the first int of their workspace
+# when a bounded wait runs out (the wait that gave up; see umma.cuh callers).
+DEVICE_STATUS = {
+    2: "synthesis GEMM epilogue: accumulator never became ready",
+    3: "synthesis GEMM loader: operand stage never freed",
+    4: "synthesis GEMM MMA issuer: operand copy never landed",
+    6: "synthesis GEMM MMA issuer: accumulator never drained",
+    12: "analysis GEMM epilogue: accumulators never became ready",
+    13: "analysis GEMM loader: operand stage never freed",
+    14: "analysis GEMM MMA issuer: operand copy never landed",
+    22: "digit synthesis GEMM epilogue: accumulators never became ready",
+    23: "digit synthesis GEMM loader: operand stage never freed",
+    24: "digit synthesis GEMM MMA issuer: operand copy never landed",
+    26: "digit synthesis GEMM MMA issuer: accumulators never drained",
+    32: "digit analysis GEMM epilogue: accumulators never became ready",
+    33: "digit analysis GEMM loader: operand stage never freed",
+    34: "digit analysis GEMM MMA issuer: operand copy never landed",
+    36: "digit analysis GEMM MMA issuer: accumulators never drained",
+    99: "self-test wait (nothing arrives by design)",
+}
+
+
+def describe_status(code):
+    """Text for a device status code (0 = every bounded wait completed)."""
+    if code == 0:
+        return "ok"
+    return DEVICE_STATUS.get(code, "a bounded tensor-pipe wait ran out") + f" (code {code})"
+
+
+def raise_device_status(code, what="split-precision call"):
+    if code != 0:
+        raise MagicError(f"magic_b200 device status after {what}: {describe_status(code)}; "
+                         "its results are invalid")

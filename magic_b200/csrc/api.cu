@@ -6,6 +6,7 @@
 
 #include "fourier.cuh"
 #include "legendre.cuh"
+#include "ozaki.cuh"
 #include "split_kernels.cuh"
 
 namespace mt {
@@ -198,8 +199,9 @@ int mt_plan_create(const mt_grid_desc* desc, mt_plan** out) {
   *out = nullptr;
   MT_REQUIRE(desc->l_max >= 1 && desc->minc >= 1 && desc->minc <= desc->l_max + 1, MT_ERR_ARG,
              "l_max >= 1 and 1 <= minc required");
-  MT_REQUIRE(desc->precision == MT_PREC_FP64 || desc->precision == MT_PREC_SPLIT,
-             MT_ERR_UNSUPPORTED, "precision must be MT_PREC_FP64 or MT_PREC_SPLIT");
+  MT_REQUIRE(desc->precision == MT_PREC_FP64 || desc->precision == MT_PREC_SPLIT ||
+                 desc->precision == MT_PREC_OZAKI,
+             MT_ERR_UNSUPPORTED, "precision must be MT_PREC_FP64, MT_PREC_SPLIT or MT_PREC_OZAKI");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("no CUDA device");
@@ -236,6 +238,7 @@ int mt_plan_create(const mt_grid_desc* desc, mt_plan** out) {
     return fail(MT_ERR_UNSUPPORTED, "n_phi_max too small for l_max/minc (modes alias)");
   int rc = build_tables(p);
   if (rc == MT_OK && p->precision == MT_PREC_SPLIT) rc = build_split_tables(p);
+  if (rc == MT_OK && p->precision == MT_PREC_OZAKI) rc = build_ozaki_tables(p);
   if (rc != MT_OK) {
     std::string keep = g_err;
     mt_plan_destroy(p);
@@ -253,6 +256,7 @@ int mt_plan_destroy(mt_plan* p) {
   for (void* q : ptrs)
     if (q) cudaFree(q);
   free_split_tables(p);
+  free_ozaki_tables(p);
   delete p;
   return MT_OK;
 }
@@ -369,7 +373,8 @@ int mt_scal_to_spat_noalloc(const mt_plan* p, const double* Slm, int64_t ld, int
   const size_t need = mt_transform_workspace(p, B, 1);
   MT_REQUIRE(need <= MT_NOALLOC_SCRATCH_BYTES, MT_ERR_WORKSPACE,
              "mt_scal_to_spat_noalloc: B too large for the fixed 16 MiB scratch "
-             "(need n_m_max * n_theta_max * B * 16 bytes); use mt_scal_to_spat with a workspace");
+             "(need mt_transform_workspace(plan, B, 1) bytes); use mt_scal_to_spat with a "
+             "workspace");
   void* work = nullptr;
   MT_TRY(noalloc_scratch(&work));
   return mt_scal_to_spat(p, Slm, ld, B, grid, work, MT_NOALLOC_SCRATCH_BYTES, stream);
@@ -860,6 +865,87 @@ static int ana_t_ops(RowOp* ops, int a, int b) {
   return 2;
 }
 
+// Source arrays, terms (recipes over them, step_time.py:980-1013) and the row
+// programs of the fused stage's synthesis, shared by the split and digit-split
+// argument blocks (fields arr, narr, term, ops).
+template <typename A>
+static void fill_bouss_synth(A& s, const mt_bouss_in* in, bool mag, bool chem) {
+  auto c = [](const double* x) { return (const double2*)x; };
+  int na = 0;
+  auto arr = [&](const double* ptr) {
+    s.arr[na] = c(ptr);
+    return na++;
+  };
+  int x = 0;
+  auto term = [&](int ia, int ib, int recipe) {
+    s.term[x].ia = (int8_t)ia;
+    s.term[x].ib = (int8_t)ib;
+    s.term[x].recipe = (int8_t)recipe;
+    s.term[x].pad = 0;
+    ++x;
+  };
+  if (mag) {
+    const int ib = arr(in->b), idb = arr(in->db), iaj = arr(in->aj), idj = arr(in->dj),
+              iddb = arr(in->ddb);
+    term(ib, 0, kDlh);
+    term(idb, 0, kRaw);
+    term(iaj, 0, kRaw);
+    term(iaj, 0, kDlh);
+    term(idj, 0, kRaw);
+    term(ib, iddb, kCurlT);
+  }
+  const int iw = arr(in->w), idw = arr(in->dw), iz = arr(in->z), idz = arr(in->dz),
+            iddw = arr(in->ddw), is = arr(in->s);
+  const int ixi = chem ? arr(in->xi) : 0;
+  term(iw, 0, kDlh);
+  term(idw, 0, kRaw);
+  term(iz, 0, kRaw);
+  term(iz, 0, kDlh);
+  term(idz, 0, kRaw);
+  term(iw, iddw, kCurlT);
+  const int xs = x;
+  term(is, 0, kRaw);
+  if (chem) term(ixi, 0, kRaw);
+  s.narr = na;
+  const int G = mag ? 4 : 2;
+  for (int g = 0; g < G; ++g) syn_group_ops(&s.ops[6 * g], 3 * g, 3 * g + 1, 3 * g + 2);
+  ana_scalar_ops(&s.ops[6 * G], xs);
+  if (chem) ana_scalar_ops(&s.ops[6 * G + 2], xs + 1);
+}
+
+// Spectral outputs of the fused stage and their row programs
+// (magic_torch/step_time.py:1066-1124); returns the number of outputs.
+template <typename A>
+static int fill_bouss_anal(A& a, const mt_bouss_out* out, bool mag, bool chem) {
+  int o = 0, r = 0;
+  r += ana_scalar_ops(&a.ops[r], 0);
+  a.out[o++] = (double2*)out->Advr;
+  r += ana_s_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advt;
+  r += ana_t_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advp;
+  r += ana_scalar_ops(&a.ops[r], 3);
+  a.out[o++] = (double2*)out->VSr;
+  r += ana_s_ops(&a.ops[r], 4, 5);
+  a.out[o++] = (double2*)out->VSt;
+  if (mag) {
+    r += ana_scalar_ops(&a.ops[r], 6);
+    a.out[o++] = (double2*)out->VxBr;
+    r += ana_s_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBt;
+    r += ana_t_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBp;
+  }
+  if (chem) {
+    const int x0 = mag ? 9 : 6;
+    r += ana_scalar_ops(&a.ops[r], x0);
+    a.out[o++] = (double2*)out->VXir;
+    r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
+    a.out[o++] = (double2*)out->VXit;
+  }
+  return o;
+}
+
 template <bool MAG, bool CHEM>
 static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
                             const mt_bouss_out* out, const mt_bouss_params* q, double* dtrkc,
@@ -873,7 +959,6 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
   float* Gs = (float*)(w + W.gs);
   unsigned long long* mx = (unsigned long long*)(w + W.mx);
   const int parts = q->parts ? q->parts : 7;
-  auto c = [](const double* x) { return (const double2*)x; };
   const int64_t fs_j = W.rows_syn, fs_c = (int64_t)p->nhs * fs_j, fs_m = 2 * fs_c;
   const int64_t g_j = W.rows_nl, g_h = (int64_t)p->nhs * g_j, g_m = 2 * g_h;
 
@@ -882,48 +967,8 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     SplitSynArgs s{};
     s.t = p->tab;
     s.s = split_tables(p);
-    // source arrays, then terms = recipes over them (step_time.py:980-1013)
-    int na = 0;
-    auto arr = [&](const double* ptr) {
-      s.arr[na] = c(ptr);
-      return na++;
-    };
-    int x = 0;
-    auto term = [&](int ia, int ib, int recipe) {
-      s.term[x].ia = (int8_t)ia;
-      s.term[x].ib = (int8_t)ib;
-      s.term[x].recipe = (int8_t)recipe;
-      s.term[x].pad = 0;
-      ++x;
-    };
-    if (MAG) {
-      const int ib = arr(in->b), idb = arr(in->db), iaj = arr(in->aj), idj = arr(in->dj),
-                iddb = arr(in->ddb);
-      term(ib, 0, kDlh);
-      term(idb, 0, kRaw);
-      term(iaj, 0, kRaw);
-      term(iaj, 0, kDlh);
-      term(idj, 0, kRaw);
-      term(ib, iddb, kCurlT);
-    }
-    const int iw = arr(in->w), idw = arr(in->dw), iz = arr(in->z), idz = arr(in->dz),
-              iddw = arr(in->ddw), is = arr(in->s);
-    const int ixi = CHEM ? arr(in->xi) : 0;
-    term(iw, 0, kDlh);
-    term(idw, 0, kRaw);
-    term(iz, 0, kRaw);
-    term(iz, 0, kDlh);
-    term(idz, 0, kRaw);
-    term(iw, iddw, kCurlT);
-    const int xs = x;
-    term(is, 0, kRaw);
-    if (CHEM) term(ixi, 0, kRaw);
-    s.narr = na;
+    fill_bouss_synth(s, in, MAG, CHEM);
     s.n_lev = n_r;
-    const int G = MAG ? 4 : 2;
-    for (int g = 0; g < G; ++g) syn_group_ops(&s.ops[6 * g], 3 * g, 3 * g + 1, 3 * g + 2);
-    ana_scalar_ops(&s.ops[6 * G], xs);
-    if (CHEM) ana_scalar_ops(&s.ops[6 * G + 2], xs + 1);
     s.ld = in->ld;
     s.or2 = q->or2;
     s.nrows = (int)W.rows_syn;
@@ -982,34 +1027,7 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
   a.g_j = g_j;
   a.g_level = W.g_level;
   a.n_lev = n_r - 2;
-  int o = 0, r = 0;
-  // output fields and their row programs (magic_torch/step_time.py:1066-1124)
-  r += ana_scalar_ops(&a.ops[r], 0);
-  a.out[o++] = (double2*)out->Advr;
-  r += ana_s_ops(&a.ops[r], 1, 2);
-  a.out[o++] = (double2*)out->Advt;
-  r += ana_t_ops(&a.ops[r], 1, 2);
-  a.out[o++] = (double2*)out->Advp;
-  r += ana_scalar_ops(&a.ops[r], 3);
-  a.out[o++] = (double2*)out->VSr;
-  r += ana_s_ops(&a.ops[r], 4, 5);
-  a.out[o++] = (double2*)out->VSt;
-  if (MAG) {
-    r += ana_scalar_ops(&a.ops[r], 6);
-    a.out[o++] = (double2*)out->VxBr;
-    r += ana_s_ops(&a.ops[r], 7, 8);
-    a.out[o++] = (double2*)out->VxBt;
-    r += ana_t_ops(&a.ops[r], 7, 8);
-    a.out[o++] = (double2*)out->VxBp;
-  }
-  if (CHEM) {
-    const int x0 = MAG ? 9 : 6;
-    r += ana_scalar_ops(&a.ops[r], x0);
-    a.out[o++] = (double2*)out->VXir;
-    r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
-    a.out[o++] = (double2*)out->VXit;
-  }
-  a.n_out = o;
+  a.n_out = fill_bouss_anal(a, out, MAG, CHEM);
   a.cols = 2 * nfo;
   a.lev_tile = kSplitRowsHost / a.cols;
   a.ld = out->ld;
@@ -1017,6 +1035,129 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
   a.aimg = (uint8_t*)(w + W.aimg);
   a.err = err;
   MT_TRY(launch_anal_split(a, st));
+  return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
+}
+
+// ---- digit-split (ozaki) fused stage ---------------------------------------
+
+struct OzWs {
+  size_t err, fs, gs, mx, rexs, rexa, aimg, total;
+  int64_t rows_syn, rows_pad_s, g_level, rows_pad_a;
+  int cols, lev_tile;
+};
+
+static OzWs oz_ws(const mt_plan* p, int n_r, int mag, int chem) {
+  OzWs w;
+  const int nfi = bouss_nfi(mag, chem), nfo = bouss_nfo(mag, chem);
+  w.rows_syn = (int64_t)n_r * 2 * nfi;
+  w.rows_pad_s = (w.rows_syn + 127) / 128 * 128;
+  w.g_level = 2 * nfo;  // doubles per level (even: 16-byte pieces)
+  w.cols = 2 * nfo;
+  w.lev_tile = 128 / w.cols;
+  w.rows_pad_a = (int64_t)((n_r - 2 + w.lev_tile - 1) / w.lev_tile) * 128;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t nm2 = (size_t)p->n_m * 2;
+  w.err = 0;
+  w.fs = 256;
+  w.gs = w.fs + al(nm2 * p->nhs * w.rows_syn * sizeof(double));
+  w.mx = w.gs + al(nm2 * p->nhs * (size_t)(n_r - 2) * w.g_level * sizeof(double));
+  w.rexs = w.mx + al(2 * (size_t)n_r * sizeof(unsigned long long));
+  w.rexa = w.rexs + al(nm2 * w.rows_pad_s * sizeof(int));
+  w.aimg = w.rexa + al(nm2 * w.rows_pad_a * sizeof(int));
+  const size_t syn = oz_syn_image_bytes((int)w.rows_syn, ozaki_syn_total_chunks(p));
+  const size_t ana = oz_ana_image_bytes(p->n_m, p->nhs, n_r - 2, w.lev_tile);
+  w.total = w.aimg + al(std::max(syn, ana));
+  return w;
+}
+
+template <bool MAG, bool CHEM>
+static int nl_bouss_ozaki_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
+                            const mt_bouss_out* out, const mt_bouss_params* q, double* dtrkc,
+                            double* dthkc, void* work, cudaStream_t st) {
+  const int nfi = bouss_nfi(MAG, CHEM);
+  const OzWs W = oz_ws(p, n_r, MAG, CHEM);
+  char* w = (char*)work;
+  int* err = (int*)(w + W.err);
+  double* Fs = (double*)(w + W.fs);
+  double* Gs = (double*)(w + W.gs);
+  unsigned long long* mx = (unsigned long long*)(w + W.mx);
+  const int parts = q->parts ? q->parts : 7;
+  const int64_t fs_j = W.rows_syn, fs_c = (int64_t)p->nhs * fs_j, fs_m = 2 * fs_c;
+  const int64_t g_j = (int64_t)(n_r - 2) * W.g_level, g_h = (int64_t)p->nhs * g_j, g_m = 2 * g_h;
+  if (parts & 1) {
+    MT_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    OzSynArgs s{};
+    s.t = p->tab;
+    s.z = ozaki_tables(p);
+    fill_bouss_synth(s, in, MAG, CHEM);
+    s.n_lev = n_r;
+    s.ld = in->ld;
+    s.or2 = q->or2;
+    s.nrows = (int)W.rows_syn;
+    s.row_per_level = 2 * nfi;
+    s.stg_lev = std::min(n_r, 127 / s.row_per_level + 2);
+    s.aimg = (uint8_t*)(w + W.aimg);
+    s.total_chunks = ozaki_syn_total_chunks(p);
+    s.rexp = (int*)(w + W.rexs);
+    s.rows_pad = W.rows_pad_s;
+    s.Fs = Fs;
+    s.fs_m = fs_m;
+    s.fs_c = fs_c;
+    s.fs_j = fs_j;
+    s.err = err;
+    MT_TRY(launch_oz_synth(s, st));
+  }
+  if (parts & 2) {
+    MT_CHECK_CUDA(cudaMemsetAsync(mx, 0, 2 * n_r * sizeof(unsigned long long), st));
+    NlBoussArgs nl{};
+    nl.t = p->tab;
+    nl.n_r = n_r;
+    nl.split_io = 1;
+    nl.Fs = Fs;
+    nl.fs_m = fs_m;
+    nl.fs_c = fs_c;
+    nl.fs_j = fs_j;
+    nl.Gs = Gs;
+    nl.g_m2 = g_m;
+    nl.g_h = g_h;
+    nl.g_j = g_j;
+    nl.g_level = W.g_level;
+    nl.or2 = q->or2;
+    nl.or4 = q->or4;
+    nl.orho1 = q->orho1;
+    nl.orho2 = q->orho2;
+    nl.delxr2 = q->delxr2;
+    nl.delxh2 = q->delxh2;
+    nl.LFfac = q->LFfac;
+    nl.cour_mode = MAG ? q->cour_mode : 0;
+    nl.cf2 = q->courfac * q->courfac;
+    nl.af2 = q->alffac * q->alffac;
+    double h = 0.5 * (1.0 + q->opm);
+    nl.valfac = h * h;
+    nl.vr2max = mx;
+    nl.vh2max = mx + n_r;
+    MT_TRY(launch_nl_bouss(MAG, CHEM, nl, st));
+  }
+  if (!(parts & 4)) return MT_OK;
+  OzAnaArgs a{};
+  a.t = p->tab;
+  a.z = ozaki_tables(p);
+  a.G = Gs;
+  a.g_m = g_m;
+  a.g_h = g_h;
+  a.g_j = g_j;
+  a.g_level = W.g_level;
+  a.n_lev = n_r - 2;
+  a.n_out = fill_bouss_anal(a, out, MAG, CHEM);
+  a.cols = W.cols;
+  a.lev_tile = W.lev_tile;
+  a.ld = out->ld;
+  a.out_col0 = 1;
+  a.aimg = (uint8_t*)(w + W.aimg);
+  a.rexp = (int*)(w + W.rexa);
+  a.rows_pad = W.rows_pad_a;
+  a.err = err;
+  MT_TRY(launch_oz_anal(a, st));
   return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
 }
 
@@ -1206,6 +1347,7 @@ extern "C" {
 size_t mt_nl_bouss_workspace(const mt_plan* p, int n_r, int l_mag, int l_chem) {
   if (!p || n_r < 3) return 0;
   if (p->precision == MT_PREC_SPLIT) return split_ws(p, n_r, l_mag, l_chem).total;
+  if (p->precision == MT_PREC_OZAKI) return oz_ws(p, n_r, l_mag, l_chem).total;
   size_t f = fourier_bytes(p, (int64_t)n_r * bouss_nfi(l_mag, l_chem));
   size_t g = fourier_bytes(p, (int64_t)(n_r - 2) * bouss_nfo(l_mag, l_chem));
   return f + g + 2 * (size_t)n_r * sizeof(unsigned long long) + 256;
@@ -1237,6 +1379,13 @@ int mt_nl_bouss(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt_bouss
                        : nl_bouss_split_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
     return q->l_chem ? nl_bouss_split_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
                      : nl_bouss_split_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+  }
+  if (p->precision == MT_PREC_OZAKI) {
+    if (q->l_mag)
+      return q->l_chem ? nl_bouss_ozaki_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                       : nl_bouss_ozaki_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+    return q->l_chem ? nl_bouss_ozaki_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                     : nl_bouss_ozaki_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
   }
   if (q->l_mag)
     return q->l_chem ? nl_bouss_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
@@ -1288,6 +1437,23 @@ int mt_selftest_wait_timeout(int* status, long long spins, void* stream) {
   MT_REQUIRE(status && spins > 0 && spins <= (1LL << 30), MT_ERR_ARG,
              "status pointer and 0 < spins <= 2^30 required");
   return launch_selftest_wait(status, (long)spins, (cudaStream_t)stream);
+}
+
+int mt_device_status(const void* work, int* code, void* stream) {
+  MT_REQUIRE(work && code, MT_ERR_ARG, "work and code pointers required");
+  cudaStream_t st = (cudaStream_t)stream;
+  int v = 0;
+  MT_CHECK_CUDA(cudaMemcpyAsync(&v, work, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MT_CHECK_CUDA(cudaStreamSynchronize(st));
+  *code = v;
+  return MT_OK;
+}
+
+int mt_noalloc_status(int* code, void* stream) {
+  MT_REQUIRE(code, MT_ERR_ARG, "code pointer required");
+  void* work = nullptr;
+  MT_TRY(noalloc_scratch(&work));
+  return mt_device_status(work, code, stream);
 }
 
 }  // extern "C"

@@ -75,6 +75,8 @@ struct mt_plan {
   mt::Tables tab;              // device pointers + sizes, ready for launches
   // split-precision operand planes (null in FP64 plans)
   void* split = nullptr;
+  // digit-split table images (MT_PREC_OZAKI plans only)
+  void* ozaki = nullptr;
 };
 
 namespace mt {

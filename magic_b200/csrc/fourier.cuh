@@ -42,6 +42,16 @@ struct NlBoussArgs {
   int cour_mode;     // 0 non-magnetic, 1 damped, 2 undamped
   double cf2, af2, valfac;  // courfac^2, alffac^2, (0.5 (1 + 1/Pm))^2
   unsigned long long *vr2max, *vh2max;  // (n_r) non-negative doubles as bits
+  // Digit-split (ozaki) stage layout, used when split_io is set: the synthesis
+  // delivers equatorially symmetric / antisymmetric FP64 rows
+  //   Fs[m][sym|asym][theta pair][level * 2 nfi + 2 f + re/im]
+  // and the analysis reads plain north / south FP64 rows
+  //   Gs[m][north|south][theta pair][(level - 1) * g_level + 2 f + re/im].
+  int split_io;
+  const double* Fs;
+  int64_t fs_m, fs_c, fs_j;
+  double* Gs;
+  int64_t g_m2, g_h, g_j, g_level;
 };
 
 int launch_nl_bouss(bool mag, bool chem, const NlBoussArgs& a, cudaStream_t st);

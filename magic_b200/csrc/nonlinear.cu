@@ -124,7 +124,7 @@ __device__ __forceinline__ void c2r_prepare_nl(cplx<R>* row, int H, const double
   }
 }
 
-template <bool MAG, bool CHEM>
+template <bool MAG, bool CHEM, bool SPLIT_IO>
 __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   using BF = BoussFields<MAG, CHEM>;
   constexpr int NFI = BF::NFI, NFO = BF::NFO;
@@ -140,12 +140,24 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   for (int i = threadIdx.x; i < NFI * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
   // half spectra of the NFI fields (one real field per buffer row)
-  const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
-  for (int e = threadIdx.x; e < M * NFI; e += blockDim.x) {
-    int k = e / NFI, f = e - k * NFI;
-    cp_async16(&buf[f * stride + pad16(k)], &Fr[k * a.f_m + f]);
+  if constexpr (SPLIT_IO) {
+    // north = sym + asym, south = sym - asym
+    const double hs = (row & 1) ? -1.0 : 1.0;
+    const double* fsym = a.Fs + (int64_t)(row >> 1) * a.fs_j + (int64_t)r * 2 * NFI;
+    for (int e = threadIdx.x; e < M * NFI; e += blockDim.x) {
+      int k = e / NFI, f = e - k * NFI;
+      const double2 sy = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m) + f);
+      const double2 as = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m + a.fs_c) + f);
+      buf[f * stride + pad16(k)] = {sy.x + hs * as.x, sy.y + hs * as.y};
+    }
+  } else {
+    const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
+    for (int e = threadIdx.x; e < M * NFI; e += blockDim.x) {
+      int k = e / NFI, f = e - k * NFI;
+      cp_async16(&buf[f * stride + pad16(k)], &Fr[k * a.f_m + f]);
+    }
+    cp_async_wait_all();
   }
-  cp_async_wait_all();
   __syncthreads();
   for (int f = threadIdx.x / 32; f < NFI; f += kNlThreads / 32)
     c2r_prepare_nl(buf + f * stride, H, t.twiddle, threadIdx.x % 32, 32);
@@ -203,7 +215,12 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   __syncthreads();
   fft_rows<false>(buf, buf + BF::NB * stride, NFO, H, stride, t.fft_radix, t.fft_nstages, tws);
   const double ws = t.wq[row] / N, wv = t.wq_v[row] / N;
-  double2* Gr = a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * NFO;
+  double2* Gr = SPLIT_IO
+                    ? reinterpret_cast<double2*>(a.Gs + (int64_t)(row & 1) * a.g_h +
+                                                 (int64_t)(row >> 1) * a.g_j +
+                                                 (int64_t)(r - 1) * a.g_level)
+                    : a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * NFO;
+  const int64_t gm = SPLIT_IO ? a.g_m2 / 2 : a.g_m;  // double2 stride between orders
   for (int e = threadIdx.x; e < M * NFO; e += blockDim.x) {
     int k = e / NFO, o = e - k * NFO;
     const cplx<double>* z = buf + o * stride;
@@ -211,16 +228,16 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
     // radial components (Advr, VSr, VxBr, VXir) are scalar analyses
     bool radial = (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
     double w = radial ? ws : wv;
-    Gr[k * a.g_m + o] = make_double2(w * X.x, w * X.y);
+    Gr[k * gm + o] = make_double2(w * X.x, w * X.y);
   }
 }
 
-template <bool MAG, bool CHEM>
+template <bool MAG, bool CHEM, bool SPLIT_IO>
 static int launch_nl_bouss_t(const NlBoussArgs& a, cudaStream_t st) {
   using BF = BoussFields<MAG, CHEM>;
   size_t sm = ((size_t)(BF::NB + kFftRowBatch) * padded_len(a.t.n_phi / 2) + a.t.n_phi / 2) *
               sizeof(double2);
-  auto kern = k_nl_bouss<MAG, CHEM>;
+  auto kern = k_nl_bouss<MAG, CHEM, SPLIT_IO>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 grid(a.t.n_theta, a.n_r);
   kern<<<grid, kNlThreads, sm, st>>>(a);
@@ -228,9 +245,18 @@ static int launch_nl_bouss_t(const NlBoussArgs& a, cudaStream_t st) {
   return MT_OK;
 }
 
+template <bool SPLIT_IO>
+static int launch_nl_bouss_io(bool mag, bool chem, const NlBoussArgs& a, cudaStream_t st) {
+  if (mag)
+    return chem ? launch_nl_bouss_t<true, true, SPLIT_IO>(a, st)
+                : launch_nl_bouss_t<true, false, SPLIT_IO>(a, st);
+  return chem ? launch_nl_bouss_t<false, true, SPLIT_IO>(a, st)
+              : launch_nl_bouss_t<false, false, SPLIT_IO>(a, st);
+}
+
 int launch_nl_bouss(bool mag, bool chem, const NlBoussArgs& a, cudaStream_t st) {
-  if (mag) return chem ? launch_nl_bouss_t<true, true>(a, st) : launch_nl_bouss_t<true, false>(a, st);
-  return chem ? launch_nl_bouss_t<false, true>(a, st) : launch_nl_bouss_t<false, false>(a, st);
+  return a.split_io ? launch_nl_bouss_io<true>(mag, chem, a, st)
+                    : launch_nl_bouss_io<false>(mag, chem, a, st);
 }
 
 __global__ void k_courant_finish(int n_r, const unsigned long long* vr2, const unsigned long long* vh2,

@@ -1,0 +1,992 @@
+// Digit-split ("ozaki") Legendre stage of the fused Boussinesq radial loop:
+// table digit images (plan time), the synthesis and analysis packing kernels
+// and the two persistent tcgen05 kind::i8 GEMMs (ozaki.cuh has the scheme).
+//
+// Orientation as in the bf16x3 kernels (legendre_split.cu): the data operand
+// is A (M = 128 rows per tile, one row per output real component), the table
+// is B (N = kOzSynN theta rows for the synthesis, kOzAnaN l rows for the
+// analysis), K runs over l (synthesis) or theta pairs (analysis) in chunks of
+// 32.  Row scales of A are found by the packing kernels in a first pass over
+// the whole K range of their block; column scales of B at plan time.
+#include <algorithm>
+#include <vector>
+
+#include "ozaki.cuh"
+#include "umma.cuh"
+
+namespace mt {
+
+// ------------------------------------------------------------- digits
+
+// Exponent e with |x| < 2^e for the largest magnitude x of a row (0 for 0).
+__device__ __forceinline__ int oz_exponent(double mx) {
+  int e = 0;
+  if (mx > 0.0) frexp(mx, &e);
+  return e;
+}
+
+// Six signed digits of v at scale 2^e (|v| < 2^e): d_i in [-64, 64].
+__device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzDigits]) {
+  double y = ldexp(v, 6 - e);
+#pragma unroll
+  for (int i = 0; i < kOzDigits; ++i) {
+    const double q = rint(y);
+    d[i] = (int8_t)(int)q;
+    y = (y - q) * 128.0;
+  }
+}
+
+// Instruction descriptor: kind::i8, s8 x s8 -> s32, A and B K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_s8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// 16 consecutive int32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+}
+
+// Named barrier over `n` threads that also ANDs a predicate across them, so
+// that all participants take the same branch afterwards.
+__device__ __forceinline__ bool bar_and(int id, int n, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n.reg .pred p, q;\nsetp.ne.u32 p, %1, 0;\nbar.red.and.pred q, %2, %3, p;\n"
+      "selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
+// sum_g 2^(-7 g) C_g for one accumulator column (exact terms, FP64 sum)
+__device__ __forceinline__ double oz_combine(const int (&c)[kOzGroups][16], int i) {
+  double v = (double)c[kOzGroups - 1][i];
+#pragma unroll
+  for (int g = kOzGroups - 2; g >= 0; --g) v = fma(v, 1.0 / 128.0, (double)c[g][i]);
+  return v;
+}
+
+// Issue the 21 digit-pair MMAs of one K chunk: group g = i + j into the
+// accumulator at tmem_acc + g * gcols.  `first`: the first chunk of an item,
+// whose first MMA per group overwrites the accumulator.
+__device__ __forceinline__ void oz_mma_chunk(uint32_t tmem_acc, uint32_t gcols, uint32_t sa,
+                                             uint32_t sb, uint32_t b_plane, uint32_t idesc,
+                                             bool first) {
+#pragma unroll
+  for (int g = 0; g < kOzGroups; ++g) {
+#pragma unroll
+    for (int i = 0; i <= g; ++i) {
+      const int j = g - i;
+      const uint64_t da = umma_desc(sa + (uint32_t)i * kOzAPlane, 128, 256);
+      const uint64_t db = umma_desc(sb + (uint32_t)j * b_plane, 128, 256);
+      umma_s8(tmem_acc + (uint32_t)g * gcols, da, db, idesc, (first && i == 0) ? 0u : 1u);
+    }
+  }
+}
+
+// ------------------------------------------------------ plan-time tables
+
+// Synthesis column exponents: block (m, combo), thread per theta: the largest
+// |P| over l - m of parity combo and |dP| over the other parity.
+__global__ void k_oz_syn_fexp(const double* __restrict__ plm, const double* __restrict__ dplm,
+                              const int* __restrict__ lstart, int l_max, int minc, int nhs,
+                              int nthw, int* fexp) {
+  const int mc = blockIdx.x >> 1, combo = blockIdx.x & 1;
+  const int nlm = l_max - mc * minc + 1;
+  const int ls = lstart[mc];
+  for (int th = threadIdx.x; th < nthw; th += blockDim.x) {
+    double mx = 0.0;
+    if (th < nhs)
+      for (int k = 0; k < nlm; ++k) {
+        const bool p_par = ((k & 1) == combo);  // P rows of parity combo, dP rows of the other
+        const double v = p_par ? plm[(int64_t)(ls + k) * nhs + th] : dplm[(int64_t)(ls + k) * nhs + th];
+        mx = fmax(mx, fabs(v));
+      }
+    fexp[((int64_t)mc * 2 + combo) * nthw + th] = oz_exponent(mx);
+  }
+}
+
+// Synthesis table digits: block ((m * 2 + q) * 2 + p) * nthtile + tau.
+__global__ void k_oz_syn_img(const double* __restrict__ plm, const double* __restrict__ dplm,
+                             const int* __restrict__ lstart, int l_max, int minc, int nhs,
+                             int nthtile, const int* __restrict__ fexp, int8_t* img,
+                             const int64_t* __restrict__ off) {
+  const int id = blockIdx.x;
+  const int tau = id % nthtile;
+  const int p = (id / nthtile) % 2;
+  const int q = (id / nthtile / 2) % 2;
+  const int mc = id / nthtile / 4;
+  const int nlm = l_max - mc * minc + 1;
+  const int nch = (split_nk(nlm, p) + kOzK - 1) / kOzK;
+  const int combo = q == 0 ? p : 1 - p;
+  const double* T = q == 0 ? plm : dplm;
+  const int ls = lstart[mc];
+  const int nthw = nthtile * kOzSynN;
+  int8_t* base = img + off[id];
+  const int per = kOzSynN * kOzK;
+  for (int e = threadIdx.x; e < nch * per; e += blockDim.x) {
+    const int c = e / per, rem = e - c * per;
+    const int r = rem / kOzK, kl = rem % kOzK;
+    const int k = 2 * (kOzK * c + kl) + p;
+    const int th = tau * kOzSynN + r;
+    const double v = (k < nlm && th < nhs) ? T[(int64_t)(ls + k) * nhs + th] : 0.0;
+    int8_t d[kOzDigits];
+    oz_digits(v, fexp[((int64_t)mc * 2 + combo) * nthw + th], d);
+    int8_t* cb = base + (int64_t)c * kOzSynBChunk;
+#pragma unroll
+    for (int s = 0; s < kOzDigits; ++s) cb[s * kOzSynBPlane + oz_off(r, kl)] = d[s];
+  }
+}
+
+// Analysis row exponents: block (m * 2 + q) * 2 + p, thread per l row: the
+// largest |T_l| over the theta pairs.
+__global__ void k_oz_ana_fexp(const double* __restrict__ plm, const double* __restrict__ dplm,
+                              const int* __restrict__ lstart, int l_max, int minc, int nhs,
+                              int nlt, int* fexp) {
+  const int id = blockIdx.x;
+  const int p = id % 2, q = (id / 2) % 2, mc = id / 4;
+  const int nlm = l_max - mc * minc + 1;
+  const double* T = q == 0 ? plm : dplm;
+  const int ls = lstart[mc];
+  for (int kk = threadIdx.x; kk < nlt * kOzAnaN; kk += blockDim.x) {
+    const int k = 2 * kk + p;
+    double mx = 0.0;
+    if (k < nlm)
+      for (int j = 0; j < nhs; ++j) mx = fmax(mx, fabs(T[(int64_t)(ls + k) * nhs + j]));
+    fexp[(int64_t)id * nlt * kOzAnaN + kk] = oz_exponent(mx);
+  }
+}
+
+// Analysis table digits: block ((m * 2 + q) * 2 + p) * nlt + lt.
+__global__ void k_oz_ana_img(const double* __restrict__ plm, const double* __restrict__ dplm,
+                             const int* __restrict__ lstart, int l_max, int minc, int nhs, int nlt,
+                             const int* __restrict__ fexp, int8_t* img,
+                             const int64_t* __restrict__ off) {
+  const int id = blockIdx.x;
+  const int lt = id % nlt;
+  const int tp = id / nlt;  // (m * 2 + q) * 2 + p
+  const int p = tp % 2, q = (tp / 2) % 2, mc = tp / 4;
+  const int nlm = l_max - mc * minc + 1;
+  const double* T = q == 0 ? plm : dplm;
+  const int ls = lstart[mc];
+  const int nchj = (nhs + kOzK - 1) / kOzK;
+  int8_t* base = img + off[id];
+  const int per = kOzAnaN * kOzK;
+  for (int e = threadIdx.x; e < nchj * per; e += blockDim.x) {
+    const int c = e / per, rem = e - c * per;
+    const int r = rem / kOzK, jl = rem % kOzK;
+    const int kk = lt * kOzAnaN + r, k = 2 * kk + p, j = kOzK * c + jl;
+    const double v = (k < nlm && j < nhs) ? T[(int64_t)(ls + k) * nhs + j] : 0.0;
+    int8_t d[kOzDigits];
+    oz_digits(v, fexp[(int64_t)tp * nlt * kOzAnaN + kk], d);
+    int8_t* cb = base + (int64_t)c * kOzAnaBChunk;
+#pragma unroll
+    for (int s = 0; s < kOzDigits; ++s) cb[s * kOzAnaBPlane + oz_off(r, jl)] = d[s];
+  }
+}
+
+struct OzStore {
+  OzTables t;
+  int8_t *syn = nullptr, *ana = nullptr;
+  int64_t *syn_off = nullptr, *ana_off = nullptr;
+  int *syn_fexp = nullptr, *ana_fexp = nullptr, *syn_prefix = nullptr;
+  std::vector<int> h_prefix;
+};
+
+int build_ozaki_tables(mt_plan* p) {
+  const int nhs = p->nhs, nm = p->n_m;
+  OzStore* S = new OzStore();
+  p->ozaki = S;
+  const int nthtile = (nhs + kOzSynN - 1) / kOzSynN;
+  const int nthw = nthtile * kOzSynN;
+  const int nlt = (split_nk(p->l_max + 1, 0) + kOzAnaN - 1) / kOzAnaN;
+  const int nchj = (nhs + kOzK - 1) / kOzK;
+  std::vector<int64_t> so((size_t)nm * 4 * nthtile), ao((size_t)nm * 4 * nlt);
+  int64_t pos = 0;
+  for (int mc = 0; mc < nm; ++mc) {
+    const int nlm = p->l_max - mc * p->minc + 1;
+    for (int q = 0; q < 2; ++q)
+      for (int par = 0; par < 2; ++par)
+        for (int tau = 0; tau < nthtile; ++tau) {
+          so[((mc * 2 + q) * 2 + par) * nthtile + tau] = pos;
+          pos += (int64_t)((split_nk(nlm, par) + kOzK - 1) / kOzK) * kOzSynBChunk;
+        }
+  }
+  const int64_t syn_bytes = pos;
+  pos = 0;
+  for (int mc = 0; mc < nm; ++mc)
+    for (int q = 0; q < 2; ++q)
+      for (int par = 0; par < 2; ++par)
+        for (int lt = 0; lt < nlt; ++lt) {
+          ao[((mc * 2 + q) * 2 + par) * nlt + lt] = pos;
+          pos += (int64_t)nchj * kOzAnaBChunk;
+        }
+  const int64_t ana_bytes = pos;
+  S->h_prefix.resize((size_t)nm * 2 + 1);
+  int acc = 0;
+  for (int mc = 0; mc < nm; ++mc)
+    for (int combo = 0; combo < 2; ++combo) {
+      S->h_prefix[mc * 2 + combo] = acc;
+      acc += oz_syn_nch(p->l_max - mc * p->minc + 1, combo);
+    }
+  S->h_prefix[(size_t)nm * 2] = acc;
+  MT_CHECK_CUDA(cudaMalloc(&S->syn, syn_bytes > 0 ? syn_bytes : 16));
+  MT_CHECK_CUDA(cudaMalloc(&S->ana, ana_bytes > 0 ? ana_bytes : 16));
+  MT_CHECK_CUDA(cudaMalloc(&S->syn_off, so.size() * sizeof(int64_t)));
+  MT_CHECK_CUDA(cudaMalloc(&S->ana_off, ao.size() * sizeof(int64_t)));
+  MT_CHECK_CUDA(cudaMalloc(&S->syn_fexp, (size_t)nm * 2 * nthw * sizeof(int)));
+  MT_CHECK_CUDA(cudaMalloc(&S->ana_fexp, (size_t)nm * 4 * nlt * kOzAnaN * sizeof(int)));
+  MT_CHECK_CUDA(cudaMalloc(&S->syn_prefix, S->h_prefix.size() * sizeof(int)));
+  MT_CHECK_CUDA(cudaMemcpy(S->syn_off, so.data(), so.size() * sizeof(int64_t),
+                           cudaMemcpyHostToDevice));
+  MT_CHECK_CUDA(cudaMemcpy(S->ana_off, ao.data(), ao.size() * sizeof(int64_t),
+                           cudaMemcpyHostToDevice));
+  MT_CHECK_CUDA(cudaMemcpy(S->syn_prefix, S->h_prefix.data(), S->h_prefix.size() * sizeof(int),
+                           cudaMemcpyHostToDevice));
+  k_oz_syn_fexp<<<nm * 2, 256>>>(p->d_plm, p->d_dplm, p->d_lstart, p->l_max, p->minc, nhs, nthw,
+                                 S->syn_fexp);
+  k_oz_syn_img<<<nm * 4 * nthtile, 256>>>(p->d_plm, p->d_dplm, p->d_lstart, p->l_max, p->minc,
+                                          nhs, nthtile, S->syn_fexp, S->syn, S->syn_off);
+  k_oz_ana_fexp<<<nm * 4, 256>>>(p->d_plm, p->d_dplm, p->d_lstart, p->l_max, p->minc, nhs, nlt,
+                                 S->ana_fexp);
+  k_oz_ana_img<<<nm * 4 * nlt, 256>>>(p->d_plm, p->d_dplm, p->d_lstart, p->l_max, p->minc, nhs,
+                                      nlt, S->ana_fexp, S->ana, S->ana_off);
+  MT_CHECK_CUDA(cudaGetLastError());
+  MT_CHECK_CUDA(cudaDeviceSynchronize());
+  S->t.nthtile = nthtile;
+  S->t.nlt = nlt;
+  S->t.syn = S->syn;
+  S->t.syn_off = S->syn_off;
+  S->t.syn_fexp = S->syn_fexp;
+  S->t.ana = S->ana;
+  S->t.ana_off = S->ana_off;
+  S->t.ana_fexp = S->ana_fexp;
+  S->t.syn_prefix = S->syn_prefix;
+  return MT_OK;
+}
+
+void free_ozaki_tables(mt_plan* p) {
+  OzStore* S = (OzStore*)p->ozaki;
+  if (!S) return;
+  void* ptrs[] = {S->syn, S->ana, S->syn_off, S->ana_off, S->syn_fexp, S->ana_fexp,
+                  S->syn_prefix};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete S;
+  p->ozaki = nullptr;
+}
+
+const OzTables& ozaki_tables(const mt_plan* p) { return ((OzStore*)p->ozaki)->t; }
+int ozaki_syn_total_chunks(const mt_plan* p) { return ((OzStore*)p->ozaki)->h_prefix.back(); }
+
+// ------------------------------------------------------------ synthesis
+
+constexpr int kOzPackThreads = 256;
+
+__host__ __device__ inline int oz_stage_pitch(int stg_lev) { return 2 * kOzK * stg_lev + 1; }
+__host__ __device__ inline size_t oz_syn_pack_smem(int narr, int stg_lev) {
+  return (size_t)narr * oz_stage_pitch(stg_lev) * 16 + 2 * kOzRows * sizeof(int);
+}
+
+__host__ __device__ inline int64_t oz_syn_img_chunk(int64_t total_chunks, int rt, int prefix, int c,
+                                                    int q) {
+  return (((int64_t)rt * total_chunks + prefix + c) * 2 + q);
+}
+
+__device__ __forceinline__ double oz_coef(int code, double m) {
+  switch (code) {
+    case 1: return 1.0;
+    case 2: return -1.0;
+    case 3: return m;
+    case 4: return -m;
+    case 5: return -m * m;
+    default: return 0.0;
+  }
+}
+
+__device__ __forceinline__ void cp16_zfill(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// k_oz_syn_pack: block (row tile rt, order m).  Thread = (table q, parity p,
+// row pair): rows 2 pr, 2 pr + 1 are the real and imaginary rows of one field.
+// Pass 0 walks every chunk of 2 kOzK values of l - m and finds the largest
+// |value| of each (row, combo); pass 1 walks them again and writes the six
+// digit planes of every chunk at the row's scale.
+__global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const Tables& t = a.t;
+  const int rt = blockIdx.x, mc = blockIdx.y;
+  const int m = mc * t.minc;
+  const int nlm = t.l_max - m + 1;
+  const int ls = t.lstart[mc];
+  const int tid = threadIdx.x;
+  const int lev0 = (rt * kOzRows) / a.row_per_level;
+  const int nlev = min(a.stg_lev, a.n_lev - lev0);
+  const int pitch = oz_stage_pitch(a.stg_lev);
+  double2* d = reinterpret_cast<double2*>(smem);
+  int* rexp_s = reinterpret_cast<int*>(smem + (size_t)a.narr * pitch * 16);  // [combo][row]
+  const int qp = tid >> 6, row0 = 2 * (tid & 63);
+  const int q = qp >> 1, p = qp & 1;
+  const int combo = q == 0 ? p : 1 - p;
+  const int nch_all = (nlm + 2 * kOzK - 1) / (2 * kOzK);
+  const int nch_combo = oz_syn_nch(nlm, combo);
+  const double dm = (double)m;
+  struct RowSrc {
+    int ia, ib, cpart;
+    double f, dl, o2, cw;
+    bool live;
+  } rs[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int R = rt * kOzRows + row0 + h;
+    rs[h].live = R < a.nrows;
+    const int lev = rs[h].live ? R / a.row_per_level : lev0;
+    const int qf = rs[h].live ? R - lev * a.row_per_level : 0;
+    const RowOp op = a.ops[qf];
+    const TermIx tm = a.term[q ? op.tD : op.tP];
+    rs[h].cpart = q ? op.cD : op.cP;
+    rs[h].f = rs[h].live ? oz_coef(q ? op.kD : op.kP, dm) : 0.0;
+    rs[h].dl = tm.recipe == kRaw ? 0.0 : 1.0;
+    rs[h].o2 = (tm.recipe == kCurlT && a.or2) ? a.or2[lev] : 1.0;
+    rs[h].cw = tm.recipe == kCurlT ? 1.0 : 0.0;
+    rs[h].ia = tm.ia * pitch + (lev - lev0);
+    rs[h].ib = tm.ib * pitch + (lev - lev0);
+  }
+  // value of row h at the i-th l - m of parity p in chunk c (staged)
+  auto value = [&](int h, int c, int i) -> double {
+    const int kk = 2 * i + p;  // l - m offset inside the staged chunk
+    const double l = (double)(m + 2 * kOzK * c + kk);
+    const double2 x = d[rs[h].ia + kk * a.stg_lev];
+    const double2 w = rs[h].cw != 0.0 ? d[rs[h].ib + kk * a.stg_lev] : make_double2(0.0, 0.0);
+    const double mul = rs[h].o2 * (1.0 + rs[h].dl * (l * (l + 1.0) - 1.0));
+    const double xa = rs[h].cpart ? x.y : x.x, xb = rs[h].cpart ? w.y : w.x;
+    return rs[h].f * (mul * xa - rs[h].cw * xb);
+  };
+  auto stage = [&](int c) {
+    __syncthreads();  // the staging buffer is free
+    for (int e = tid; e < 2 * kOzK * a.stg_lev; e += kOzPackThreads) {
+      const int kk = e / a.stg_lev, lvv = e - kk * a.stg_lev;
+      if (lvv >= nlev) continue;
+      const int k = 2 * kOzK * c + kk;
+      const int64_t off = (int64_t)(ls + min(k, nlm - 1)) * a.ld + lev0 + lvv;
+      const uint32_t bytes = k < nlm ? 16u : 0u;
+      for (int ia = 0; ia < a.narr; ++ia)
+        cp16_zfill(&d[ia * pitch + kk * a.stg_lev + lvv], a.arr[ia] + off, bytes);
+    }
+    cp_commit_wait_all();
+    __syncthreads();
+  };
+  // pass 0: row maxima per combo; each (row, combo) gets contributions from
+  // two threads (P of one parity, dP of the other), merged through shared memory
+  double mx[2] = {0.0, 0.0};
+  for (int c = 0; c < nch_all; ++c) {
+    stage(c);
+#pragma unroll 4
+    for (int i = 0; i < kOzK; ++i) {
+      mx[0] = fmax(mx[0], fabs(value(0, c, i)));
+      mx[1] = fmax(mx[1], fabs(value(1, c, i)));
+    }
+  }
+  unsigned long long* rmax = reinterpret_cast<unsigned long long*>(smem);  // reuses staging
+  __syncthreads();
+  for (int e = tid; e < 2 * kOzRows; e += kOzPackThreads) rmax[e] = 0ull;
+  __syncthreads();
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+    atomicMax(&rmax[combo * kOzRows + row0 + h], (unsigned long long)__double_as_longlong(mx[h]));
+  __syncthreads();
+  for (int e = tid; e < 2 * kOzRows; e += kOzPackThreads) {
+    const int e_ = oz_exponent(__longlong_as_double((long long)rmax[e]));
+    rexp_s[e] = e_;
+    const int cb = e / kOzRows, row = e % kOzRows;
+    a.rexp[((int64_t)mc * 2 + cb) * a.rows_pad + (int64_t)rt * kOzRows + row] = e_;
+  }
+  __syncthreads();
+  const int ex[2] = {rexp_s[combo * kOzRows + row0], rexp_s[combo * kOzRows + row0 + 1]};
+  // pass 1: digit planes
+  for (int c = 0; c < nch_all; ++c) {
+    stage(c);
+    if (c >= nch_combo) continue;
+    uint8_t* dst = a.aimg + oz_syn_img_chunk(a.total_chunks, rt,
+                                             a.z.syn_prefix[mc * 2 + combo], c, q) * kOzAChunk;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t w[kOzDigits][4];
+#pragma unroll
+        for (int i4 = 0; i4 < 4; ++i4) {
+#pragma unroll
+          for (int s = 0; s < kOzDigits; ++s) w[s][i4] = 0u;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            int8_t dg[kOzDigits];
+            oz_digits(value(h, c, 16 * half + 4 * i4 + b), ex[h], dg);
+#pragma unroll
+            for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
+          }
+        }
+#pragma unroll
+        for (int s = 0; s < kOzDigits; ++s)
+          *reinterpret_cast<uint4*>(dst + s * kOzAPlane + oz_off(row0 + h, 16 * half)) =
+              make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+      }
+    }
+  }
+}
+
+// Persistent synthesis GEMM: one CTA per SM walks the items (tile, combo,
+// theta tile, m) with a stride of gridDim.x.  Warp 0 lane 0 bulk-copies the A
+// digit chunk and the table digit chunk of every K step into a ring, warp 1
+// lane 0 issues the 21 digit-pair MMAs per step into the six group
+// accumulators (TMEM columns 64 g) and commits when the item's K loop ends,
+// warps 2-5 drain the accumulators (one TMEM lane per thread), form the FP64
+// values and store them into Fs, and hand the accumulators back.
+constexpr int kOzStages = 4;
+constexpr int kOzSynThreads = 64 + 128;
+
+struct OzSynSmem {
+  static constexpr uint32_t stage_bytes = kOzAChunk + kOzSynBChunk;
+  static constexpr uint32_t bar_off = kOzStages * stage_bytes;
+  // full/empty per stage, tfull, tempty, done, tmem slot, abort flag
+  static constexpr size_t total = bar_off + 8 * (2 * kOzStages + 3) + 16;
+};
+
+__global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const Tables& t = a.t;
+  const OzTables& z = a.z;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + OzSynSmem::bar_off);
+  uint64_t* empty = full + kOzStages;
+  uint64_t* tfull = empty + kOzStages;
+  uint64_t* tempty = tfull + 1;
+  uint64_t* done = tempty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  if (*(volatile int*)a.err) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = (a.nrows + kOzRows - 1) / kOzRows, ny = 2 * z.nthtile;
+  const int nitems = ntiles * ny * t.n_m;
+  const int nthw = z.nthtile * kOzSynN;
+  struct Item {
+    int rt, combo, tau, mc, nch_t[2];
+  };
+  auto decode = [&](int item) {
+    Item it;
+    it.rt = item % ntiles;
+    const int r = item / ntiles, y = r % ny;
+    it.mc = r / ny;
+    it.combo = y & 1;
+    it.tau = y >> 1;
+    const int nlm = t.l_max - it.mc * t.minc + 1;
+    it.nch_t[0] = (split_nk(nlm, it.combo) + kOzK - 1) / kOzK;
+    it.nch_t[1] = (split_nk(nlm, 1 - it.combo) + kOzK - 1) / kOzK;
+    return it;
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < kOzStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(tfull, 1);
+    mbar_init(tempty, 128);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int g = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+        const Item it = decode(item);
+        const uint8_t* aimg =
+            a.aimg + oz_syn_img_chunk(a.total_chunks, it.rt, z.syn_prefix[it.mc * 2 + it.combo],
+                                      0, 0) * kOzAChunk;
+        const int8_t* img[2];
+        for (int q = 0; q < 2; ++q)
+          img[q] = z.syn + z.syn_off[((it.mc * 2 + q) * 2 + (q ? 1 - it.combo : it.combo)) *
+                                         z.nthtile + it.tau];
+        const int nch = max(it.nch_t[0], it.nch_t[1]);
+        for (int c = 0; c < nch && ok; ++c) {
+          for (int q = 0; q < 2; ++q) {
+            if (c >= it.nch_t[q]) continue;
+            const int s = g % kOzStages;
+            if (g >= kOzStages &&
+                !mbar_wait(&empty[s], ((g / kOzStages) - 1) & 1, abort_flag, a.err, 23)) {
+              ok = false;
+              break;
+            }
+            uint8_t* stg = smem + s * OzSynSmem::stage_bytes;
+            mbar_expect_tx(&full[s], OzSynSmem::stage_bytes);
+            bulk_g2s(stg, aimg + (int64_t)(2 * c + q) * kOzAChunk, kOzAChunk, &full[s]);
+            bulk_g2s(stg + kOzAChunk, img[q] + (int64_t)c * kOzSynBChunk, kOzSynBChunk, &full[s]);
+            ++g;
+          }
+        }
+      }
+      for (int k = max(0, g - kOzStages); k < g; ++k)
+        mbar_drain(&full[k % kOzStages], (k / kOzStages) & 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_s8(kOzRows, kOzSynN);
+      int g = 0, n = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x, ++n) {
+        const Item it = decode(item);
+        if (n >= 1 && !mbar_wait(tempty, (n - 1) & 1, abort_flag, a.err, 26)) break;
+        tc_fence_after();
+        const int nch = max(it.nch_t[0], it.nch_t[1]);
+        bool first = true;
+        for (int c = 0; c < nch && ok; ++c) {
+          for (int q = 0; q < 2; ++q) {
+            if (c >= it.nch_t[q]) continue;
+            const int s = g % kOzStages;
+            if (!mbar_wait(&full[s], (g / kOzStages) & 1, abort_flag, a.err, 24)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(smem + s * OzSynSmem::stage_bytes);
+            oz_mma_chunk(tbase, kOzSynN, sa, sa + kOzAChunk, kOzSynBPlane, idesc, first);
+            first = false;
+            umma_commit(&empty[s]);
+            ++g;
+          }
+        }
+        if (ok) umma_commit(tfull);
+      }
+      umma_commit(done);
+    }
+  } else {
+    // epilogue: warps 2-5 own TMEM lane quarters (warp % 4)
+    const int quarter = warp & 3;
+    const int R0 = quarter * 32 + lane;
+    int n = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++n) {
+      const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 22);
+      if (!__all_sync(0xffffffffu, ok && !*abort_flag)) break;
+      tc_fence_after();
+      const Item it = decode(item);
+      const int R = it.rt * kOzRows + R0;
+      const int er = R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + it.combo) * a.rows_pad + R] : 0;
+      const int* fe = z.syn_fexp + ((int64_t)it.mc * 2 + it.combo) * nthw + it.tau * kOzSynN;
+      double* out = a.Fs + (int64_t)it.mc * a.fs_m + (int64_t)it.combo * a.fs_c;
+      const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < kOzSynN; c0 += 16) {
+        int cg[kOzGroups][16];
+#pragma unroll
+        for (int g = 0; g < kOzGroups; ++g) tmem_ld16_i32(taddr + g * kOzSynN + c0, cg[g]);
+        if (R < a.nrows) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int th = it.tau * kOzSynN + c0 + i;
+            if (th < t.nhs)
+              out[(int64_t)th * a.fs_j + R] = ldexp(oz_combine(cg, i), er + __ldg(&fe[c0 + i]) - 12);
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(tempty);
+    }
+  }
+  __syncwarp();
+  if (warp == 1) mbar_drain(done, 0);  // no MMA may still write TMEM at dealloc
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tbase, 512);
+  }
+}
+
+size_t oz_syn_image_bytes(int nrows, int64_t total_chunks) {
+  return (size_t)((nrows + kOzRows - 1) / kOzRows) * (size_t)total_chunks * 2 * kOzAChunk;
+}
+
+int launch_oz_synth(const OzSynArgs& a, cudaStream_t st) {
+  const int ntiles = (a.nrows + kOzRows - 1) / kOzRows;
+  const size_t pack_sm = std::max(oz_syn_pack_smem(a.narr, a.stg_lev),
+                                  (size_t)2 * kOzRows * 8 + 2 * kOzRows * sizeof(int));
+  MT_REQUIRE(pack_sm <= 220 * 1024, MT_ERR_UNSUPPORTED, "digit pack staging too large");
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_syn_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pack_sm));
+  k_oz_syn_pack<<<dim3(ntiles, a.t.n_m), kOzPackThreads, pack_sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  const size_t sm = OzSynSmem::total;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_synth_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+  int dev = 0, nsm = 148;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_CHECK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int nitems = ntiles * 2 * a.z.nthtile * a.t.n_m;
+  k_oz_synth_gemm<<<std::min(nitems, nsm), kOzSynThreads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+// -------------------------------------------------------------- analysis
+//
+// k_oz_ana_pack: block (tile rt, order m); thread = (fold, row): fold 0 is
+// north + south, fold 1 north - south of the raw Fourier column (level lv,
+// column col) of the tile.  Pass 0 finds the row's largest |value| over all
+// theta pairs, pass 1 writes the digit planes of every chunk of kOzK pairs.
+// k_oz_anal_gemm (persistent; item = tile, output parity, l tile, m)
+// accumulates acc0 = fold_par . P and acc1 = fold_(1-par) . dP in six groups
+// each, and its epilogue forms each output component as
+// coef(kP) acc0[colP] + coef(kD) acc1[colD] (the row program) through an
+// FP64 exchange buffer in shared memory.
+
+__host__ __device__ inline int64_t oz_ana_img_chunk(int n_m, int nchj, int rt, int mc, int fold,
+                                                    int c) {
+  return (((int64_t)rt * n_m + mc) * 2 + fold) * nchj + c;
+}
+
+__global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_ana_pack(OzAnaArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const Tables& t = a.t;
+  const int rt = blockIdx.x, mc = blockIdx.y;
+  const int nchj = (t.nhs + kOzK - 1) / kOzK;
+  const int tid = threadIdx.x;
+  const int lev0 = rt * a.lev_tile;
+  const int nlev = min(a.lev_tile, a.n_lev - lev0);
+  const int gl = (int)a.g_level;
+  const int rowlen = a.lev_tile * gl;  // doubles per staged (hemisphere, theta pair)
+  double* d = reinterpret_cast<double*>(smem);
+  const int fold = tid >> 7, row = tid & 127;
+  const int lv = row / a.cols, col = row - lv * a.cols;
+  const bool live = lv < nlev;
+  const double sg = fold ? -1.0 : 1.0;
+  const double* nrow = d + lv * gl + col;
+  auto stage = [&](int c) {
+    __syncthreads();
+    const double* gm = a.G + (int64_t)mc * a.g_m + (int64_t)lev0 * gl;
+    const int cpl = nlev * gl / 2;  // 16-byte pieces per (hemisphere, theta pair)
+    for (int hj = tid >> 5; hj < 2 * kOzK; hj += kOzPackThreads / 32) {
+      const int h = hj / kOzK, j = kOzK * c + hj % kOzK;
+      const double* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j;
+      const uint32_t bytes = j < t.nhs ? 16u : 0u;
+      for (int p2 = tid & 31; p2 < cpl; p2 += 32)
+        cp16_zfill(d + hj * rowlen + 2 * p2, src + 2 * p2, bytes);
+    }
+    cp_commit_wait_all();
+    __syncthreads();
+  };
+  auto value = [&](int i) -> double {
+    return live ? nrow[i * rowlen] + sg * nrow[(kOzK + i) * rowlen] : 0.0;
+  };
+  double mx = 0.0;
+  for (int c = 0; c < nchj; ++c) {
+    stage(c);
+#pragma unroll 8
+    for (int i = 0; i < kOzK; ++i) mx = fmax(mx, fabs(value(i)));
+  }
+  const int ex = oz_exponent(mx);
+  a.rexp[((int64_t)mc * 2 + fold) * a.rows_pad + (int64_t)rt * kOzRows + row] = ex;
+  for (int c = 0; c < nchj; ++c) {
+    stage(c);
+    uint8_t* dst = a.aimg + oz_ana_img_chunk(t.n_m, nchj, rt, mc, fold, c) * kOzAChunk;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      uint32_t w[kOzDigits][4];
+#pragma unroll
+      for (int i4 = 0; i4 < 4; ++i4) {
+#pragma unroll
+        for (int s = 0; s < kOzDigits; ++s) w[s][i4] = 0u;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          int8_t dg[kOzDigits];
+          oz_digits(value(16 * half + 4 * i4 + b), ex, dg);
+#pragma unroll
+          for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < kOzDigits; ++s)
+        *reinterpret_cast<uint4*>(dst + s * kOzAPlane + oz_off(row, 16 * half)) =
+            make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+    }
+  }
+}
+
+constexpr int kOzAnaThreads = 64 + 128;
+constexpr int kOzXS = kOzAnaN + 1;  // padded exchange row (doubles)
+
+struct OzAnaSmem {
+  static constexpr uint32_t stage_bytes = kOzAChunk + kOzAnaBChunk;
+  static constexpr uint32_t xch_off = kOzStages * stage_bytes;
+  static constexpr uint32_t xch_bytes = 2 * kOzRows * kOzXS * 8;
+  static constexpr uint32_t tab_off = xch_off + xch_bytes;  // row-program tables
+  static constexpr uint32_t tab_bytes = 64 * 8 + 64 * 4 + kOzAnaN * 8 + 16;
+  static constexpr uint32_t bar_off = (tab_off + tab_bytes + 15) & ~15u;
+  static constexpr size_t total = bar_off + 8 * (2 * kOzStages + 3) + 16;
+};
+
+__global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const Tables& t = a.t;
+  const OzTables& z = a.z;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + OzAnaSmem::bar_off);
+  uint64_t* empty = full + kOzStages;
+  uint64_t* tfull = empty + kOzStages;
+  uint64_t* tempty = tfull + 1;
+  uint64_t* done = tempty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  if (*(volatile int*)a.err) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nchj = (t.nhs + kOzK - 1) / kOzK;
+  const int ntiles = (a.n_lev + a.lev_tile - 1) / a.lev_tile;
+  const int ny = 2 * z.nlt;
+  const int nitems = ntiles * ny * t.n_m;
+  struct Item {
+    int rt, par, lt, mc, nk;
+    bool live;
+  };
+  auto decode = [&](int item) {
+    Item it;
+    it.rt = item % ntiles;
+    const int r = item / ntiles, y = r % ny;
+    it.mc = r / ny;
+    it.par = y & 1;
+    it.lt = y >> 1;
+    const int nlm = t.l_max - it.mc * t.minc + 1;
+    it.nk = split_nk(nlm, it.par);
+    it.live = it.lt * kOzAnaN < it.nk;
+    return it;
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < kOzStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(tfull, 1);
+    mbar_init(tempty, 128);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int g = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+        const Item it = decode(item);
+        if (!it.live) continue;
+        const uint8_t* aimg[2];
+        const int8_t* img[2];
+        for (int q = 0; q < 2; ++q) {
+          const int fold = q ? 1 - it.par : it.par;
+          aimg[q] = a.aimg + oz_ana_img_chunk(t.n_m, nchj, it.rt, it.mc, fold, 0) * kOzAChunk;
+          img[q] = z.ana + z.ana_off[((it.mc * 2 + q) * 2 + it.par) * z.nlt + it.lt];
+        }
+        for (int c = 0; c < nchj && ok; ++c) {
+          for (int q = 0; q < 2; ++q) {
+            const int s = g % kOzStages;
+            if (g >= kOzStages &&
+                !mbar_wait(&empty[s], ((g / kOzStages) - 1) & 1, abort_flag, a.err, 33)) {
+              ok = false;
+              break;
+            }
+            uint8_t* stg = smem + s * OzAnaSmem::stage_bytes;
+            mbar_expect_tx(&full[s], OzAnaSmem::stage_bytes);
+            bulk_g2s(stg, aimg[q] + (int64_t)c * kOzAChunk, kOzAChunk, &full[s]);
+            bulk_g2s(stg + kOzAChunk, img[q] + (int64_t)c * kOzAnaBChunk, kOzAnaBChunk, &full[s]);
+            ++g;
+          }
+        }
+      }
+      for (int k = max(0, g - kOzStages); k < g; ++k)
+        mbar_drain(&full[k % kOzStages], (k / kOzStages) & 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_s8(kOzRows, kOzAnaN);
+      int g = 0, n = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+        const Item it = decode(item);
+        if (!it.live) continue;
+        if (n >= 1 && !mbar_wait(tempty, (n - 1) & 1, abort_flag, a.err, 36)) break;
+        tc_fence_after();
+        for (int c = 0; c < nchj && ok; ++c) {
+          for (int q = 0; q < 2; ++q) {
+            const int s = g % kOzStages;
+            if (!mbar_wait(&full[s], (g / kOzStages) & 1, abort_flag, a.err, 34)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(smem + s * OzAnaSmem::stage_bytes);
+            oz_mma_chunk(tbase + (uint32_t)(q * kOzGroups * kOzAnaN), kOzAnaN, sa, sa + kOzAChunk,
+                         kOzAnaBPlane, idesc, c == 0);
+            umma_commit(&empty[s]);
+            ++g;
+          }
+        }
+        if (ok) umma_commit(tfull);
+        ++n;
+      }
+      umma_commit(done);
+    }
+  } else {
+    // epilogue: warps 2-5, thread e = tid - 64 owns TMEM lane R0 = 32 (warp % 4) + lane
+    const int e = tid - 64;
+    const int quarter = warp & 3;
+    const int R0 = quarter * 32 + lane;
+    double* xch = reinterpret_cast<double*>(smem + OzAnaSmem::xch_off);  // [2][128][kOzXS]
+    double* cf = reinterpret_cast<double*>(smem + OzAnaSmem::tab_off);   // [64]
+    int* colx = reinterpret_cast<int*>(cf + 64);                        // [64]
+    double* osc = reinterpret_cast<double*>(colx + 64);                 // [kOzAnaN]
+    int n = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+      const Item it = decode(item);
+      if (!it.live) continue;
+      const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 32);
+      ++n;
+      // all four epilogue warps agree, since they meet at named barriers below
+      if (!bar_and(1, 128, ok && !*abort_flag)) break;
+      tc_fence_after();
+      const int m = it.mc * t.minc;
+      const int nlm = t.l_max - m + 1;
+      const int ls = t.lstart[it.mc];
+      const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16);
+      const int Rg = it.rt * kOzRows + R0;
+#pragma unroll 1
+      for (int q = 0; q < 2; ++q) {
+        const int fold = q ? 1 - it.par : it.par;
+        const int er = a.rexp[((int64_t)it.mc * 2 + fold) * a.rows_pad + Rg];
+        const int* fe = z.ana_fexp + ((int64_t)(it.mc * 2 + q) * 2 + it.par) * z.nlt * kOzAnaN +
+                        it.lt * kOzAnaN;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kOzAnaN; c0 += 16) {
+          int cg[kOzGroups][16];
+#pragma unroll
+          for (int g = 0; g < kOzGroups; ++g)
+            tmem_ld16_i32(taddr + (uint32_t)((q * kOzGroups + g) * kOzAnaN + c0), cg[g]);
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            xch[(q * kOzRows + R0) * kOzXS + c0 + i] =
+                ldexp(oz_combine(cg, i), er + __ldg(&fe[c0 + i]) - 12);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(tempty);  // the accumulators are free for the next item's MMAs
+      // row-program tables of this item
+      const double dm = (double)m;
+      for (int r = e; r < 2 * a.n_out; r += 128) {
+        const RowOp op = a.ops[r];
+        cf[2 * r] = oz_coef(op.kP, dm);
+        cf[2 * r + 1] = oz_coef(op.kD, dm);
+        colx[2 * r] = 2 * op.tP + op.cP;
+        colx[2 * r + 1] = kOzRows + 2 * op.tD + op.cD;
+      }
+      for (int i = e; i < kOzAnaN; i += 128) {
+        const double l = (double)(m + 2 * (it.lt * kOzAnaN + i) + it.par);
+        osc[i] = l > 0.0 ? 1.0 / (l * (l + 1.0)) : 0.0;
+      }
+      asm volatile("bar.sync 1, 128;\n" ::: "memory");
+      const int lev0 = it.rt * a.lev_tile;
+      const int nlev = min(a.lev_tile, a.n_lev - lev0);
+      const int nel = a.n_out * a.lev_tile * kOzAnaN;
+      for (int x = e; x < nel; x += 128) {
+        const int lv = x % a.lev_tile, rest = x / a.lev_tile;
+        const int i = rest % kOzAnaN, o = rest / kOzAnaN;
+        const int kk = it.lt * kOzAnaN + i, k = 2 * kk + it.par;
+        if (lv >= nlev || kk >= it.nk || k >= nlm) continue;
+        const int base = lv * a.cols;
+        const int r4 = 4 * o;
+        const double re = cf[r4] * xch[(base + colx[r4]) * kOzXS + i] +
+                          cf[r4 + 1] * xch[(base + colx[r4 + 1]) * kOzXS + i];
+        const double im = cf[r4 + 2] * xch[(base + colx[r4 + 2]) * kOzXS + i] +
+                          cf[r4 + 3] * xch[(base + colx[r4 + 3]) * kOzXS + i];
+        const double sc = a.ops[2 * o].scale ? osc[i] : 1.0;
+        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] = make_double2(sc * re, sc * im);
+      }
+      asm volatile("bar.sync 1, 128;\n" ::: "memory");  // exchange buffer free again
+    }
+  }
+  __syncwarp();
+  if (warp == 1) mbar_drain(done, 0);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tbase, 512);
+  }
+}
+
+size_t oz_ana_image_bytes(int n_m, int nhs, int n_lev, int lev_tile) {
+  const int ntiles = (n_lev + lev_tile - 1) / lev_tile;
+  return (size_t)ntiles * n_m * 2 * ((nhs + kOzK - 1) / kOzK) * kOzAChunk;
+}
+
+int launch_oz_anal(const OzAnaArgs& a, cudaStream_t st) {
+  const int ntiles = (a.n_lev + a.lev_tile - 1) / a.lev_tile;
+  MT_REQUIRE(a.cols * a.lev_tile <= kOzRows && a.g_level % 2 == 0, MT_ERR_ARG,
+             "analysis tile layout");
+  const size_t pack_sm = (size_t)2 * kOzK * a.lev_tile * a.g_level * sizeof(double);
+  MT_REQUIRE(pack_sm <= 220 * 1024, MT_ERR_UNSUPPORTED, "digit pack staging too large");
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_ana_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pack_sm));
+  k_oz_ana_pack<<<dim3(ntiles, a.t.n_m), kOzPackThreads, pack_sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  const size_t sm = OzAnaSmem::total;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_anal_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+  int dev = 0, nsm = 148;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_CHECK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int nitems = ntiles * 2 * a.z.nlt * a.t.n_m;
+  k_oz_anal_gemm<<<std::min(nitems, nsm), kOzAnaThreads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+}  // namespace mt

@@ -9,13 +9,14 @@ theta rows).  Every call enqueues on the current torch CUDA stream and does not
 synchronise the host.
 """
 
+import collections
 import ctypes as C
 
 import numpy as np
 import torch
 
 from . import _lib
-from ._lib import MagicError, check
+from ._lib import MagicError, check, raise_device_status
 
 _CD = torch.complex128
 _RD = torch.float64
@@ -25,8 +26,55 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
 
+class _StatusWatch:
+    """Non-blocking check of the split kernels' device status.  After each call
+    the status word of its workspace (first int, written by a bounded tensor-pipe
+    wait that ran out) is copied on the same stream into a pinned host slot, and
+    an event marks when it has landed; poll() raises MagicError for the first
+    landed non-zero code.  Nothing is recorded while the stream is being captured
+    into a CUDA graph (the caller reads the word after replays instead)."""
+
+    SLOTS = 4096
+
+    def __init__(self):
+        self.host = torch.zeros(self.SLOTS, dtype=torch.int32).pin_memory()
+        self.pending = collections.deque()
+        self.next = 0
+
+    def record(self, work, what):
+        if torch.cuda.is_current_stream_capturing():
+            return
+        self.poll()
+        if len(self.pending) >= self.SLOTS:
+            self.poll(block=True)
+        stream = torch.cuda.current_stream(work.device)
+        slot = self.next
+        self.next = (self.next + 1) % self.SLOTS
+        self.host[slot:slot + 1].copy_(work[:4].view(torch.int32), non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self.pending.append((slot, ev, what))
+
+    def poll(self, block=False):
+        while self.pending:
+            slot, ev, what = self.pending[0]
+            if block:
+                ev.synchronize()
+            elif not ev.query():
+                return
+            self.pending.popleft()
+            code = int(self.host[slot])
+            if code:
+                self.pending.clear()
+                raise_device_status(code, what)
+
+
 class Plan:
-    """Tables and entry points for one (l_max, minc) grid on one CUDA device."""
+    """Tables and entry points for one (l_max, minc) grid on one CUDA device.
+
+    Split-precision plans watch the device status of every call (see
+    ``poll_status``): a bounded wait on the tensor pipe that ran out is raised
+    as MagicError by the next call on the plan, or by ``poll_status``."""
 
     def __init__(self, l_max, minc=1, precision="fp64", device=None, n_theta_max=0,
                  n_phi_max=0):
@@ -37,7 +85,8 @@ class Plan:
             raise ValueError("magic_b200 plans live on CUDA devices")
         self.device = dev if dev.index is not None else torch.device(
             "cuda", torch.cuda.current_device())
-        prec = {"fp64": _lib.MT_PREC_FP64, "split": _lib.MT_PREC_SPLIT}[precision]
+        prec = {"fp64": _lib.MT_PREC_FP64, "split": _lib.MT_PREC_SPLIT,
+                "ozaki": _lib.MT_PREC_OZAKI}[precision]
         self.precision = precision
         L = _lib.lib()
         desc = _lib.GridDesc(int(l_max), int(minc), int(n_theta_max), int(n_phi_max), prec)
@@ -76,6 +125,29 @@ class Plan:
         self.grid_idx = gi.to(self.device)
         sin_g = torch.sin(th[self.grid_idx])
         self.O_sin_theta_E2_grid = 1.0 / sin_g ** 2
+        self._status = _StatusWatch() if precision != "fp64" else None
+
+    # ------------------------------------------------------ device status
+    def poll_status(self, block=False):
+        """Raise MagicError if a split-precision call on this plan recorded a
+        device-side timeout.  block=False only looks at calls that have already
+        finished; block=True waits for every call made so far."""
+        if self._status is not None:
+            self._status.poll(block)
+
+    def device_status(self, work):
+        """Status word of the call that last used ``work`` (synchronises the
+        current stream): 0, or the code of the bounded wait that ran out."""
+        code = C.c_int(0)
+        check(_lib.lib().mt_device_status(_ptr(work), C.byref(code), self._stream()))
+        return code.value
+
+    def _watch(self, work, what, fused=False):
+        """Record the status word of a call that cleared it: every call of a split
+        plan; on digit-split (ozaki) plans only the fused stage (their transforms
+        run the FP64 kernels, which leave the word alone)."""
+        if self._status is not None and (fused or self.precision == "split"):
+            self._status.record(work, what)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -135,6 +207,7 @@ class Plan:
         ws = self._work(L.mt_transform_workspace(self._h, B, 1))
         check(L.mt_scal_to_spat(self._h, _ptr(X), X.stride(0), B, _ptr(out), _ptr(ws),
                                 ws.numel(), self._stream()))
+        self._watch(ws, "scal_to_spat")
         return out[0] if one else out
 
     def scal_to_SH(self, sc, lcut=None):
@@ -145,6 +218,7 @@ class Plan:
         ws = self._work(L.mt_transform_workspace(self._h, B, 1))
         check(L.mt_scal_to_SH(self._h, _ptr(g), B, _ptr(out), B, _ptr(ws), ws.numel(),
                               self._stream()))
+        self._watch(ws, "scal_to_SH")
         return out[:, 0] if one else out
 
     def torpol_to_spat(self, Qlm, Slm, Tlm, lcut=None):
@@ -162,6 +236,7 @@ class Plan:
         ws = self._work(L.mt_transform_workspace(self._h, B, 3))
         check(L.mt_torpol_to_spat(self._h, _ptr(Q), _ptr(S), _ptr(T), Q.stride(0), B,
                                   *[_ptr(o) for o in outs], _ptr(ws), ws.numel(), self._stream()))
+        self._watch(ws, "torpol_to_spat")
         return tuple(o[0] for o in outs) if one else tuple(outs)
 
     def spat_to_sphertor(self, vt, vp, lcut=None):
@@ -176,6 +251,7 @@ class Plan:
         ws = self._work(L.mt_transform_workspace(self._h, B, 2))
         check(L.mt_spat_to_sphertor(self._h, _ptr(gt), _ptr(gp), B, _ptr(S), _ptr(T), B,
                                     _ptr(ws), ws.numel(), self._stream()))
+        self._watch(ws, "spat_to_sphertor")
         return (S[:, 0], T[:, 0]) if one else (S, T)
 
     def _grad(self, Slm, scale_dlh):
@@ -187,6 +263,7 @@ class Plan:
         ws = self._work(L.mt_transform_workspace(self._h, B, 2))
         check(L.mt_scal_to_grad_spat(self._h, _ptr(X), X.stride(0), B, int(scale_dlh), _ptr(gt),
                                      _ptr(gp), _ptr(ws), ws.numel(), self._stream()))
+        self._watch(ws, "scal_to_grad_spat")
         return (gt[0], gp[0]) if one else (gt, gp)
 
     def scal_to_grad_spat(self, Slm, lcut=None):
@@ -308,6 +385,7 @@ class Plan:
             work = self._work(need)
         check(L.mt_nl_bouss(self._h, n_r, C.byref(bi), C.byref(bo), C.byref(bp), _ptr(dtr),
                             _ptr(dth), _ptr(work), work.numel(), self._stream()))
+        self._watch(work, "nl_bouss", fused=True)
         return out, dtr, dth
 
     def get_td(self, ins, prof, CorFac, D1, l_double_curl=False, l_heat=True, l_mag=True,
@@ -356,14 +434,96 @@ class Plan:
                                    D1._h if D1 is not None else None, self._stream()))
         return out
 
+    def _nl_anel_composed(self, fields, prof, LFfac, ViscHeatFac, OhmLossFac, courfac, alffac,
+                          opm, l_mag, l_chem, damp, out):
+        """FP64 plans: the anelastic nonlinear stage composed, as the reference's
+        radial_loop_anel composes it (step_time.py:1233-1474), from the FP64 transform
+        kernels, mt_get_nl_anel and mt_courant, with the grids in device memory:
+        s, xi and the magnetic field on every level; velocity, its radial, theta and
+        phi derivatives and cvr on the bulk levels (zero on both boundaries); forward
+        transforms of the bulk levels; Courant steps from the zero-boundary velocity."""
+        n_r = fields["w"].shape[1]
+        for k in ["w", "dw", "ddw", "z", "dz", "s"] + (["b", "db", "ddb", "aj", "dj"] if l_mag
+                                                       else []) + (["xi"] if l_chem else []):
+            x = fields[k]
+            if x.shape != (self.lm_max, n_r) or x.dtype != _CD or x.device != self.device:
+                raise ValueError(f"fields[{k}]: expected ({self.lm_max}, {n_r}) complex128")
+        if n_r < 3:
+            raise MagicError("nl_anel needs n_r >= 3")
+        shape = (n_r, self.n_theta_max, self.n_phi_max)
+        zeros = lambda: torch.zeros(shape, dtype=_RD, device=self.device)
+        d = self.dLh.unsqueeze(1)
+        o2 = self._prof(prof["or2"], n_r).unsqueeze(0)
+        sc = self.scal_to_spat(fields["s"])
+        xic = self.scal_to_spat(fields["xi"]) if l_chem else zeros()
+        if l_mag:
+            br, bt, bp = self.torpol_to_spat(d * fields["b"], fields["db"], fields["aj"])
+            cbr, cbt, cbp = self.torpol_to_spat(d * fields["aj"], fields["dj"],
+                                                o2 * d * fields["b"] - fields["ddb"])
+        else:
+            br, bt, bp, cbr, cbt, cbp = (zeros() for _ in range(6))
+        bk = slice(1, n_r - 1)
+        wb, dwb, ddwb, zb, dzb = (fields[k][:, bk] for k in ("w", "dw", "ddw", "z", "dz"))
+
+        def bulk(*grids):
+            res = []
+            for x in grids:
+                a = zeros()
+                a[bk] = x
+                res.append(a)
+            return res
+
+        vr, vt, vp = bulk(*self.torpol_to_spat(d * wb, dwb, zb))
+        dvrdr, dvtdr, dvpdr = bulk(*self.torpol_to_spat(d * dwb, ddwb, dzb))
+        (cvr,) = bulk(self.scal_to_spat(d * zb))
+        dvrdt, dvrdp = bulk(*self.pol_to_grad_spat(wb))
+        ph = self.dPhi.unsqueeze(1)
+        _, gt, gp = self.torpol_to_spat(torch.zeros_like(dwb), ph * dwb, ph * zb)
+        ost = self.O_sin_theta_E2_grid.unsqueeze(1)
+        dvtdp, dvpdp = bulk(gt * ost, gp * ost)
+        nl = self.get_nl_anel([vr, vt, vp, dvrdr, dvtdr, dvpdr, dvrdt, dvrdp, dvtdp, dvpdp, cvr,
+                               sc, xic, br, bt, bp, cbr, cbt, cbp], prof, LFfac, ViscHeatFac,
+                              OhmLossFac, l_mag)
+        Advr, Advt, Advp, VSr, VSt, VSp, VxBr, VxBt, VxBp, VXir, VXit, VXip, heat = nl
+        onames = ["Advr", "Advt", "Advp", "VSr", "VSt"] + (["VxBr", "VxBt", "VxBp"] if l_mag
+                                                           else []) + \
+            (["VXir", "VXit"] if l_chem else []) + ["heat"]
+        if out is None:
+            out = {k: torch.zeros(self.lm_max, n_r, dtype=_CD, device=self.device) for k in onames}
+
+        def put(name, x):
+            out[name][:, 0] = 0.0
+            out[name][:, -1] = 0.0
+            out[name][:, bk] = x
+
+        put("Advr", self.scal_to_SH(Advr[bk]))
+        put("VSr", self.scal_to_SH(VSr[bk]))
+        S, T = self.spat_to_sphertor(Advt[bk], Advp[bk])
+        put("Advt", S)
+        put("Advp", T)
+        put("VSt", self.spat_to_sphertor(VSt[bk], VSp[bk])[0])
+        if l_mag:
+            put("VxBr", self.scal_to_SH(VxBr[bk]))
+            S, T = self.spat_to_sphertor(VxBt[bk], VxBp[bk])
+            put("VxBt", S)
+            put("VxBp", T)
+        if l_chem:
+            put("VXir", self.scal_to_SH(VXir[bk]))
+            put("VXit", self.spat_to_sphertor(VXit[bk], VXip[bk])[0])
+        put("heat", self.scal_to_SH(heat[bk]))
+        dtr, dth = self.courant(vr, vt, vp, br if l_mag else None, bt, bp, prof, courfac, alffac,
+                                LFfac, opm, damp=damp)
+        return out, dtr, dth
+
     def nl_anel_workspace(self, n_r, l_mag=True, l_chem=False):
         return _lib.lib().mt_nl_anel_workspace(self._h, int(n_r), int(l_mag), int(l_chem))
 
     def nl_anel(self, fields, prof, LFfac, ViscHeatFac, OhmLossFac, courfac, alffac, opm,
                 l_mag=True, l_chem=False, damp=True, out=None, work=None):
-        """Fused anelastic nonlinear stage (magic_torch/step_time.py:1215-1475: transforms,
-        get_nl_anel with viscous and Ohmic heating, forward transforms, CFL); split-precision
-        plans only.
+        """Anelastic nonlinear stage (magic_torch/step_time.py:1215-1475: transforms,
+        get_nl_anel with viscous and Ohmic heating, forward transforms, CFL): fused into
+        the tcgen05 pack/GEMM and FP32 phi kernels on split-precision plans, composed
+        from the FP64 kernels on FP64 and digit-split (ozaki) plans.
 
         ``fields``: dict of spectral (lm_max, n_r) complex128 arrays w, dw, ddw, z, dz, s
         (+ b, db, ddb, aj, dj if l_mag, xi if l_chem).  ``prof``: r, or1, or2, or4, beta,
@@ -373,10 +533,13 @@ class Plan:
         """
         w = fields["w"]
         n_r = w.shape[1]
+        if self.precision in ("fp64", "ozaki"):
+            return self._nl_anel_composed(fields, prof, LFfac, ViscHeatFac, OhmLossFac, courfac,
+                                          alffac, opm, l_mag, l_chem, damp, out)
         L = _lib.lib()
         need = L.mt_nl_anel_workspace(self._h, n_r, int(l_mag), int(l_chem))
         if need == 0:
-            raise MagicError("nl_anel needs a precision='split' plan and n_r >= 3")
+            raise MagicError("nl_anel needs n_r >= 3")
         names = ["w", "dw", "ddw", "z", "dz", "s"] + (["b", "db", "ddb", "aj", "dj"] if l_mag
                                                        else []) + (["xi"] if l_chem else [])
         ins = {}
@@ -409,4 +572,5 @@ class Plan:
             work = self._work(need)
         check(L.mt_nl_anel(self._h, n_r, C.byref(ai), C.byref(ao), C.byref(ap), _ptr(dtr),
                            _ptr(dth), _ptr(work), work.numel(), self._stream()))
+        self._watch(work, "nl_anel")
         return out, dtr, dth

@@ -144,6 +144,10 @@ class GraphRunner:
             else:
                 self.st.step()
             e1.record()
+            if self.graph is not None and not eager:
+                # a replay bypasses the plan's per-call watch: read the stage's
+                # device status word after it, on the run's stream
+                self.st.plan._watch(self.st.work, "nl_bouss (graph replay)", fused=True)
         self.inflight.append((e0, e1))
         self.launched += 1
 
@@ -154,6 +158,7 @@ class GraphRunner:
         return len(self.inflight)
 
     def poll(self):
+        self.st.plan.poll_status()
         while self.inflight and self.inflight[0][1].query():
             e0, e1 = self.inflight.pop(0)
             self.latencies_ms.append(e0.elapsed_time(e1))
@@ -165,6 +170,7 @@ class GraphRunner:
         from .state import state_dict
 
         self.stream.synchronize()
+        self.st.plan.poll_status(block=True)
         res = RunResult(self.spec, energies=self.st.energies(),
                         latencies_ms=list(self.latencies_ms))
         if keep_state:

@@ -124,3 +124,24 @@ def test_no_cpu_fallback_without_gpu(libpath):
 
     with pytest.raises(RuntimeError):
         Plan(16)
+
+
+def test_device_status_codes_decode():
+    from magic_b200 import MagicError, _lib
+
+    assert _lib.describe_status(0) == "ok"
+    assert "code 4" in _lib.describe_status(4)
+    assert "synthesis" in _lib.describe_status(4)
+    assert "code 12345" in _lib.describe_status(12345)
+    _lib.raise_device_status(0)
+    with pytest.raises(MagicError, match="invalid"):
+        _lib.raise_device_status(14, "nl_bouss")
+
+
+def test_device_status_rejects_null_arguments(libpath):
+    from magic_b200 import _lib
+
+    L = _lib.lib()
+    code = ctypes.c_int(0)
+    assert L.mt_device_status(None, ctypes.byref(code), None) != 0
+    assert L.mt_noalloc_status(None, None) != 0

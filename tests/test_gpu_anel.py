@@ -79,12 +79,34 @@ def test_split_anel_stage_matches_oracle(l_max, minc, N, l_mag, l_chem):
     assert np.abs(dh.cpu().numpy() - rdh).max() / np.abs(rdh).max() < 1e-5
 
 
-def test_anel_requires_split_plan():
-    from magic_b200 import Plan
-    from magic_b200._lib import MagicError
+FP64_CASES = [(16, 1, 5, True, False), (32, 4, 6, True, True), (383, 1, 3, True, False)]
 
-    p = Plan(16, 1)
-    with pytest.raises(MagicError):
-        p.nl_anel({k: torch.zeros(p.lm_max, 4, dtype=torch.complex128, device="cuda")
-                   for k in ["w", "dw", "ddw", "z", "dz", "s"]}, {}, 1.0, 0.0, 0.0, 1.0, 1.0, 1.0,
-                  l_mag=False)
+
+@pytest.mark.parametrize("l_max,minc,N,l_mag,l_chem", FP64_CASES)
+def test_fp64_anel_stage_matches_oracle(l_max, minc, N, l_mag, l_chem):
+    """FP64 plans compose the anelastic stage from the FP64 kernels; the l_max = 383
+    case is the anelastic configuration's horizontal grid (n_phi = 1152).  Tolerance
+    1e-12 of each output's scale (the vector pair's for S/T)."""
+    from magic_b200 import Plan
+
+    g = og.Grid(l_max, minc)
+    p = Plan(l_max, minc)
+    rng = np.random.default_rng(11 * l_max + N)
+    f = _fields(g, N, rng, l_mag, l_chem)
+    prof = ostage.anel_profiles(N, l_max=l_max)
+    LF, vhf, ohm, cf, af, opm = 200.0, 0.3, 0.2, 2.5, 1.0, 0.2
+    ref, rdt, rdh = ostage.nl_anel_stage(g, f, prof, LF, vhf, ohm, cf, af, opm, l_mag, l_chem)
+    cu = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()
+    out, dt, dh = p.nl_anel({k: cu(v) for k, v in f.items()}, {k: cu(v) for k, v in prof.items()},
+                            LF, vhf, ohm, cf, af, opm, l_mag=l_mag, l_chem=l_chem)
+    torch.cuda.synchronize()
+    assert set(out) == set(ref)
+    for k in ref:
+        got = out[k].cpu().numpy()
+        assert np.all(got[:, 0] == 0) and np.all(got[:, -1] == 0), k
+        scale = np.abs(ref[k]).max()
+        if k in PAIR:
+            scale = max(scale, np.abs(ref[PAIR[k]]).max())
+        assert np.abs(got - ref[k]).max() / scale < 1e-12, k
+    assert np.abs(dt.cpu().numpy() - rdt).max() / np.abs(rdt).max() < 1e-12
+    assert np.abs(dh.cpu().numpy() - rdh).max() / np.abs(rdh).max() < 1e-12

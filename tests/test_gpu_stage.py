@@ -18,6 +18,10 @@ CASES = [
     (20, 1, 6, False, True),
     (16, 1, 4, False, False),
     (63, 1, 9, True, False),
+    # the benchmark's horizontal grid (n_theta 384, n_phi 768) and the largest
+    # (n_phi 1152), on a few levels
+    (255, 1, 3, True, False),
+    (383, 1, 3, False, False),
 ]
 
 

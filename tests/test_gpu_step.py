@@ -347,6 +347,50 @@ def test_500_steps_match_reference_chebyshev_split():
     assert max(ee.values()) < 5e-6, ee
 
 
+def test_500_steps_match_reference_ozaki():
+    """The same 500 finite-difference steps with the digit-split (ozaki) stage:
+    int8 digit planes on the tcgen05 integer pipe with exact accumulation and an
+    FP64 phi stage.  Bounds: the north star's 1e-7 on the fields and 1e-9 on the
+    energies of every step, against the reference's FP64 run."""
+    fe, ee = _run500_errors("ozaki")
+    print({k: f"{v:.1e}" for k, v in (fe | ee).items()})
+    assert max(fe.values()) < 1e-7, fe
+    assert max(ee.values()) < 1e-9, ee
+
+
+def test_500_steps_match_reference_chebyshev_ozaki():
+    """The Chebyshev run with the digit-split stage (bounds 1e-7 and 1e-9)."""
+    fe, ee = _run500_errors("ozaki", "run_cheb_l32m4")
+    print({k: f"{v:.1e}" for k, v in (fe | ee).items()})
+    assert max(fe.values()) < 1e-7, fe
+    assert max(ee.values()) < 1e-9, ee
+
+
+def test_ozaki_stage_drift_after_500_steps():
+    """500 steps at l_max = 255 on 97 FD4 levels with the digit-split and the FP64
+    stage from one seeded state: fields within 1e-7 and total energies within
+    1e-9 of the FP64-stage run."""
+    from magic_b200.step import BoussinesqStep
+
+    runs = []
+    for prec in ("fp64", "ozaki"):
+        st = BoussinesqStep(255, 97, precision=prec)
+        st.init_random(seed=0, amp=1e-4)
+        runs.append(st)
+    a, b = runs
+    for _ in range(500):
+        a.step()
+        b.step()
+    b.plan.poll_status(block=True)
+    fe = {k: ((a.f[k] - b.f[k]).abs().max() / a.f[k].abs().max()).item()
+          for k in ("w", "z", "s", "b", "aj")}
+    ea, eb = a.energies(), b.energies()
+    ee = max(abs(x - y) / abs(x) for x, y in zip(ea[0][:2] + ea[1][:2], eb[0][:2] + eb[1][:2]))
+    print(fe, ee)
+    assert max(fe.values()) < 1e-7, fe
+    assert ee < 1e-9, ee
+
+
 def test_courant_dt_control_matches_reference():
     """Steps with the reference's Courant control of dt (step(adaptive=True)) from
     the reference's own initial state (tests/golden/adapt_cheb.npz: l_max 32,
