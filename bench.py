@@ -768,6 +768,8 @@ def run_serve(args, rank, world):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    from magic_b200.serve import BatchedEnsembleServer
+
     specs = poisson_stream(args.serve_runs, rate=4.0, seed=rank, n_steps=args.serve_steps)
     srv = EnsembleServer(device=dev)
     with ClockSampler(dev) as clocks:
@@ -775,6 +777,19 @@ def run_serve(args, rank, world):
     sat_specs = [dataclasses.replace(s, arrival=0.0) for s in specs]
     srv = EnsembleServer(device=dev)
     sat = latency_report(srv.serve(sat_specs), srv.wall_s)
+    # cross-run batching: one fused stage per resolution group per step, in the
+    # split mode and in the digit-split mode that meets the precision bounds
+    batched = {}
+    for prec in ("split", "ozaki"):
+        for name, ss in (("stream", specs), ("capacity", sat_specs)):
+            bsrv = BatchedEnsembleServer(device=dev)
+            res = bsrv.serve([dataclasses.replace(s, precision=prec) for s in ss])
+            r = latency_report(res, bsrv.wall_s)
+            r["kernels_per_run_step"] = (sum(g.kernel_launches for g in bsrv.groups.values()) /
+                                         max(1, r["steps"]))
+            r["group_steps"] = sum(g.launches for g in bsrv.groups.values())
+            batched[f"{prec}_{name}"] = r
+        torch.cuda.empty_cache()
     finish, busy = 0.0, 0.0
     for s in specs:
         torch.cuda.synchronize()
@@ -806,6 +821,8 @@ def run_serve(args, rank, world):
                          "p99_ms": sat["p99_ms"], "wall_s": sat["wall_s"]},
             "fp64_one_at_a_time": {"steps_per_s": rep["steps"] / finish, "wall_s": finish,
                                    "capacity_steps_per_s": rep["steps"] / busy},
+            "kernels_per_run_step": 12,
+            "batched": batched,
             "dtype": "bf16x3/f32 stage, f64 rest", "data": "synthetic",
             "config": {"workload": "ensemble stream: Poisson 4 runs/s, l_max 32-127, n_r 33-65, "
                                    "Chebyshev Boussinesq MHD, dt 1e-4",

@@ -208,6 +208,9 @@ typedef struct {
                  1 Legendre synthesis, 2 phi FFT + products + Courant maxima,
                  4 Legendre analysis + Courant steps (lets a caller time or
                  overlap the three launches individually)                     */
+  const double* LFfac_r; /* (n_r) per-level Lorentz factor in place of LFfac, or
+                            NULL; lets one call serve the levels of several runs
+                            with different Ekman or magnetic Prandtl numbers    */
 } mt_bouss_params;
 
 MT_API size_t mt_nl_bouss_workspace(const mt_plan* plan, int n_r, int l_mag, int l_chem);
@@ -454,6 +457,25 @@ MT_API int mt_energy(const mt_plan* plan, int n_r, const mt_energy_args* e, doub
                      void* work, size_t work_bytes, void* stream);
 
 MT_API int mt_selftest_wait_timeout(int* status, long long spins, void* stream);
+
+/* ---- cross-run batching ------------------------------------------------- */
+
+/* One block copy of complex (re, im double) columns: for every row i < n_rows,
+ * dst[i * dst_ld + dst_col0 + j] = src[i * src_ld + src_col0 + j], j < n_cols
+ * (strides and offsets in complex elements).  src and dst are device pointers;
+ * the array of copies itself lives in device memory. */
+typedef struct {
+  const double* src;
+  double* dst;
+  int64_t src_ld, dst_ld;
+  int src_col0, dst_col0, n_cols, pad;
+} mt_level_copy;
+
+/* All copies in one launch on `stream` (no counterpart in the reference, which
+ * runs one simulation per process): gathers the radial levels of several runs
+ * of one resolution into the batch arrays of one mt_nl_bouss call, and
+ * scatters the outputs back.  Copies must not overlap each other. */
+MT_API int mt_copy_levels(int n_rows, const mt_level_copy* copies, int n_copies, void* stream);
 
 /* ---- device status of the split-precision kernels ----------------------- */
 

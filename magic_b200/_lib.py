@@ -56,7 +56,7 @@ class BoussParams(C.Structure):
     _fields_ = [(n, _dp) for n in ("or2", "or4", "orho1", "orho2", "delxr2", "delxh2")] + \
                [("LFfac", C.c_double), ("courfac", C.c_double), ("alffac", C.c_double),
                 ("opm", C.c_double), ("l_mag", C.c_int), ("l_chem", C.c_int),
-                ("cour_mode", C.c_int), ("parts", C.c_int)]
+                ("cour_mode", C.c_int), ("parts", C.c_int), ("LFfac_r", _dp)]
 
 
 class AnelIn(C.Structure):
@@ -121,6 +121,12 @@ class WpUpdate(C.Structure):
                                    "rgrav", "rho0")] + [("impl_interior", C.c_int)]
 
 
+class LevelCopy(C.Structure):
+    _fields_ = [("src", _dp), ("dst", _dp), ("src_ld", _i64), ("dst_ld", _i64),
+                ("src_col0", C.c_int), ("dst_col0", C.c_int), ("n_cols", C.c_int),
+                ("pad", C.c_int)]
+
+
 class EnergyArgs(C.Structure):
     _fields_ = [(n, _dp) for n in ("pol", "dpol", "tor")] + [("ld", _i64)] + \
                [(n, _dp) for n in ("or2", "cr", "rint")] + [("magnetic", C.c_int)]
@@ -176,6 +182,7 @@ _PROTOS = {
     "mt_update_wp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(WpUpdate), C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "mt_selftest_wait_timeout": (C.c_int, [_dp, C.c_longlong, _dp]),
+    "mt_copy_levels": (C.c_int, [C.c_int, _dp, C.c_int, _dp]),
     "mt_device_status": (C.c_int, [_dp, C.POINTER(C.c_int), _dp]),
     "mt_noalloc_status": (C.c_int, [C.POINTER(C.c_int), _dp]),
     "mt_last_error": (C.c_char_p, []),

@@ -729,6 +729,7 @@ static int nl_bouss_t(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt
   nl.delxr2 = q->delxr2;
   nl.delxh2 = q->delxh2;
   nl.LFfac = q->LFfac;
+  nl.LFfac_r = q->LFfac_r;
   nl.cour_mode = MAG ? q->cour_mode : 0;
   nl.cf2 = q->courfac * q->courfac;
   nl.af2 = q->alffac * q->alffac;
@@ -1004,6 +1005,7 @@ static int nl_bouss_split_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     nl.delxr2 = q->delxr2;
     nl.delxh2 = q->delxh2;
     nl.LFfac = q->LFfac;
+    nl.LFfac_r = q->LFfac_r;
     nl.cour_mode = MAG ? q->cour_mode : 0;
     nl.cf2 = q->courfac * q->courfac;
     nl.af2 = q->alffac * q->alffac;
@@ -1129,6 +1131,7 @@ static int nl_bouss_ozaki_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
     nl.delxr2 = q->delxr2;
     nl.delxh2 = q->delxh2;
     nl.LFfac = q->LFfac;
+    nl.LFfac_r = q->LFfac_r;
     nl.cour_mode = MAG ? q->cour_mode : 0;
     nl.cf2 = q->courfac * q->courfac;
     nl.af2 = q->alffac * q->alffac;

@@ -21,7 +21,7 @@ BUILD = os.path.join(ROOT, "_build")
 SOURCES = ["api.cu", "tables.cu", "legendre_f64.cu", "fourier.cu", "nonlinear.cu",
            "split_tables.cu", "legendre_split.cu", "nl_split.cu", "split_transforms.cu",
            "nl_anel_split.cu", "radial_td.cu",
-           "implicit.cu", "energy.cu", "ozaki.cu"]
+           "implicit.cu", "energy.cu", "ozaki.cu", "batch.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -39,6 +39,7 @@ struct NlBoussArgs {
   int64_t g_m, g_row;
   const double *or2, *or4, *orho1, *orho2, *delxr2, *delxh2;
   double LFfac;
+  const double* LFfac_r;  // per-level Lorentz factor, or null (LFfac everywhere)
   int cour_mode;     // 0 non-magnetic, 1 damped, 2 undamped
   double cf2, af2, valfac;  // courfac^2, alffac^2, (0.5 (1 + 1/Pm))^2
   unsigned long long *vr2max, *vh2max;  // (n_r) non-negative doubles as bits

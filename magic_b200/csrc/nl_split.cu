@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(kNlSplitThreads) k_nl_bouss_split(NlSplitArgs 
   const float or2 = (float)a.or2[r], or4 = (float)a.or4[r], ost2 = (float)t.ost2[row];
   const double orho1 = a.orho1[r], orho2 = a.orho2[r];
   const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
+  const double LFd = a.LFfac_r ? a.LFfac_r[r] : a.LFfac;
   double mr = 0.0, mh = 0.0;
   for (int i = threadIdx.x; i < H; i += blockDim.x) {
     cplx<float> zin[NFI];
@@ -148,11 +149,11 @@ __global__ void __launch_bounds__(kNlSplitThreads) k_nl_bouss_split(NlSplitArgs 
       if constexpr (CHEM) fi.xi = v(iv + 7);
       double vr2, vh2;
       courant_point_f(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, a.or2[r], a.or4[r],
-                      orho1, orho2, t.ost2[row], a.LFfac, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+                      orho1, orho2, t.ost2[row], LFd, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
       mr = fmax(mr, vr2);
       mh = fmax(mh, vh2);
       float o[12];
-      bouss_point_f(fi, or2, or4, ost2, (float)a.LFfac, MAG, o);
+      bouss_point_f(fi, or2, or4, ost2, (float)LFd, MAG, o);
 #pragma unroll
       for (int q = 0; q < 6; ++q) out[h][q] = o[q];
       if constexpr (MAG) { out[h][6] = o[6]; out[h][7] = o[7]; out[h][8] = o[8]; }
@@ -237,7 +238,8 @@ __global__ void __maxnreg__(72)
   const float or2 = (float)a.or2[r], or4 = (float)a.or4[r], ost2 = (float)t.ost2[row];
   const float orho1 = (float)a.orho1[r], orho2 = (float)a.orho2[r];
   const float valri2 = (float)(a.valfac / a.delxr2[r]), valhi2 = (float)(a.valfac / a.delxh2[r]);
-  const float LF = (float)a.LFfac, cf2 = (float)a.cf2, af2 = (float)a.af2;
+  const float LF = (float)(a.LFfac_r ? a.LFfac_r[r] : a.LFfac), cf2 = (float)a.cf2,
+              af2 = (float)a.af2;
   float mr = 0.f, mh = 0.f;
   for (int i = tid; i < H; i += T) {
     const int si = hw_swz<Q>(i);

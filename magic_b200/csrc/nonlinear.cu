@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "fft.cuh"
+#include "fft_w64.cuh"
 #include "fourier.cuh"
 
 namespace mt {
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
   const double orho1 = a.orho1[r], orho2 = a.orho2[r];
   const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
+  const double LF = a.LFfac_r ? a.LFfac_r[r] : a.LFfac;
   double mr = 0.0, mh = 0.0;
   for (int i = threadIdx.x; i < H; i += blockDim.x) {
     cplx<double> zin[NFI];
@@ -190,11 +192,11 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
       if constexpr (CHEM) fi.xi = v(iv + 7);
       double vr2, vh2;
       courant_point(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, or2, or4, orho1, orho2,
-                    ost2, a.LFfac, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+                    ost2, LF, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
       mr = fmax(mr, vr2);
       mh = fmax(mh, vh2);
       BoussOut o;
-      bouss_point(fi, or2, or4, ost2, a.LFfac, MAG, o);
+      bouss_point(fi, or2, or4, ost2, LF, MAG, o);
 #pragma unroll
       for (int q = 0; q < 6; ++q) out[h][q] = o.o[q];
       if constexpr (MAG) { out[h][6] = o.o[6]; out[h][7] = o.o[7]; out[h][8] = o.o[8]; }
@@ -232,8 +234,150 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   }
 }
 
+// The same stage for n_phi = 64 Q (Q in 4, 8, 12, 16) with warp FFTs
+// (fft_w64.cuh): every field row is transformed by one warp, so between the
+// block-wide phases (load, inverse FFTs, products, forward FFTs, store) rows
+// proceed independently, and two CTAs of 7 warps share an SM.
+constexpr int kNlW64Threads = 224;
+
+template <bool MAG, bool CHEM, bool SPLIT_IO, int Q>
+__global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a) {
+  using BF = BoussFields<MAG, CHEM>;
+  constexpr int NFI = BF::NFI, NFO = BF::NFO, H = 32 * Q, S = padded_len(H);
+  constexpr int NW = kNlW64Threads / 32;
+  extern __shared__ double smem[];
+  __shared__ double red[32];
+  cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);  // NB rows, S apart
+  cplx<double>* twH = buf + BF::NB * S;                       // exp(-2 pi i n / H)
+  cplx<double>* twN = twH + H;                                // exp(-2 pi i k / (2 H))
+  const Tables& t = a.t;
+  const int M = t.n_m;
+  const int row = blockIdx.x, r = blockIdx.y;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < H; i += kNlW64Threads) {
+    const double2 wn = __ldg(&t.twiddle[i]), wh = __ldg(&t.twiddle[2 * i]);
+    twN[i] = {wn.x, wn.y};
+    twH[i] = {wh.x, wh.y};
+  }
+  // half spectra of the NFI fields; wavenumbers k >= n_m are zero
+  if constexpr (SPLIT_IO) {
+    const double hs = (row & 1) ? -1.0 : 1.0;  // north = sym + asym, south = sym - asym
+    const double* fsym = a.Fs + (int64_t)(row >> 1) * a.fs_j + (int64_t)r * 2 * NFI;
+    for (int e = tid; e < M * NFI; e += kNlW64Threads) {
+      const int k = e / NFI, f = e - k * NFI;
+      const double2 sy = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m) + f);
+      const double2 as = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m + a.fs_c) + f);
+      buf[f * S + pad16(k)] = {sy.x + hs * as.x, sy.y + hs * as.y};
+    }
+  } else {
+    const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
+    for (int e = tid; e < M * NFI; e += kNlW64Threads) {
+      const int k = e / NFI, f = e - k * NFI;
+      const double2 x = __ldg(&Fr[k * a.f_m + f]);
+      buf[f * S + pad16(k)] = {x.x, x.y};
+    }
+  }
+  for (int e = tid; e < NFI * (H - M); e += kNlW64Threads) {
+    const int f = e / (H - M), k = M + e % (H - M);
+    buf[f * S + pad16(k)] = {0.0, 0.0};
+  }
+  __syncthreads();
+  for (int f = warp; f < NFI; f += NW) w64_row_fft<Q, true, true>(buf + f * S, lane, twH, twN);
+  __syncthreads();
+
+  const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
+  const double orho1 = a.orho1[r], orho2 = a.orho2[r];
+  const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
+  const double LF = a.LFfac_r ? a.LFfac_r[r] : a.LFfac;
+  double mr = 0.0, mh = 0.0;
+  for (int i = tid; i < H; i += kNlW64Threads) {
+    const int si = pad16(i);
+    cplx<double> zin[NFI];
+#pragma unroll
+    for (int f = 0; f < NFI; ++f) zin[f] = buf[f * S + si];
+    double out[2][NFO];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {  // grid points 2i and 2i+1
+      auto v = [&](int f) { return h ? zin[f].y : zin[f].x; };
+      BoussIn fi;
+      constexpr int iv = BF::IV;
+      if constexpr (MAG) {
+        fi.br = v(0); fi.bt = v(1); fi.bp = v(2); fi.cbr = v(3); fi.cbt = v(4); fi.cbp = v(5);
+      } else {
+        fi.br = fi.bt = fi.bp = fi.cbr = fi.cbt = fi.cbp = 0.0;
+      }
+      fi.vr = v(iv); fi.vt = v(iv + 1); fi.vp = v(iv + 2);
+      fi.cvr = v(iv + 3); fi.cvt = v(iv + 4); fi.cvp = v(iv + 5);
+      fi.s = v(iv + 6);
+      fi.xi = 0.0;
+      if constexpr (CHEM) fi.xi = v(iv + 7);
+      double vr2, vh2;
+      courant_point(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, or2, or4, orho1, orho2,
+                    ost2, LF, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+      mr = fmax(mr, vr2);
+      mh = fmax(mh, vh2);
+      BoussOut o;
+      bouss_point(fi, or2, or4, ost2, LF, MAG, o);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) out[h][q] = o.o[q];
+      if constexpr (MAG) { out[h][6] = o.o[6]; out[h][7] = o.o[7]; out[h][8] = o.o[8]; }
+      if constexpr (CHEM) {
+        constexpr int c = MAG ? 9 : 6;
+        out[h][c] = o.o[9]; out[h][c + 1] = o.o[10]; out[h][c + 2] = o.o[11];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NFO; ++q) buf[q * S + si] = {out[0][q], out[1][q]};
+  }
+  double vmr = block_max(mr, red);
+  if (tid == 0) atomic_max_pos(&a.vr2max[r], vmr);
+  double vmh = block_max(mh, red);
+  if (tid == 0) atomic_max_pos(&a.vh2max[r], vmh);
+  if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
+  __syncthreads();
+  for (int f = warp; f < NFO; f += NW) w64_row_fft<Q, false, false>(buf + f * S, lane, twH, twN);
+  __syncthreads();
+  const double ws = t.wq[row] / (2 * H), wv = t.wq_v[row] / (2 * H);
+  double2* Gr = SPLIT_IO
+                    ? reinterpret_cast<double2*>(a.Gs + (int64_t)(row & 1) * a.g_h +
+                                                 (int64_t)(row >> 1) * a.g_j +
+                                                 (int64_t)(r - 1) * a.g_level)
+                    : a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * NFO;
+  const int64_t gm = SPLIT_IO ? a.g_m2 / 2 : a.g_m;  // double2 stride between orders
+  for (int e = tid; e < M * NFO; e += kNlW64Threads) {
+    const int k = e / NFO, o = e - k * NFO;
+    const cplx<double>* z = buf + o * S;
+    const cplx<double> X = r2c_post_d(z[pad16(k)], z[pad16((H - k) % H)], twN[k]);
+    const bool radial = (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
+    const double w = radial ? ws : wv;
+    Gr[k * gm + o] = make_double2(w * X.x, w * X.y);
+  }
+}
+
+template <bool MAG, bool CHEM, bool SPLIT_IO, int Q>
+static int launch_nl_bouss_w64(const NlBoussArgs& a, cudaStream_t st) {
+  using BF = BoussFields<MAG, CHEM>;
+  constexpr int H = 32 * Q;
+  const size_t sm = ((size_t)BF::NB * padded_len(H) + 2 * H) * sizeof(double2);
+  auto kern = k_nl_bouss_w64<MAG, CHEM, SPLIT_IO, Q>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
+  dim3 grid(a.t.n_theta, a.n_r);
+  kern<<<grid, kNlW64Threads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
 template <bool MAG, bool CHEM, bool SPLIT_IO>
 static int launch_nl_bouss_t(const NlBoussArgs& a, cudaStream_t st) {
+  switch (a.t.n_phi) {
+    case 256: return launch_nl_bouss_w64<MAG, CHEM, SPLIT_IO, 4>(a, st);
+    case 512: return launch_nl_bouss_w64<MAG, CHEM, SPLIT_IO, 8>(a, st);
+    case 768: return launch_nl_bouss_w64<MAG, CHEM, SPLIT_IO, 12>(a, st);
+    case 1024: return launch_nl_bouss_w64<MAG, CHEM, SPLIT_IO, 16>(a, st);
+    default: break;
+  }
   using BF = BoussFields<MAG, CHEM>;
   size_t sm = ((size_t)(BF::NB + kFftRowBatch) * padded_len(a.t.n_phi / 2) + a.t.n_phi / 2) *
               sizeof(double2);

@@ -73,6 +73,7 @@ struct NlSplitArgs {
   int64_t g_m, g_h, g_j, g_level;
   const double *or2, *or4, *orho1, *orho2, *delxr2, *delxh2;
   double LFfac;
+  const double* LFfac_r;  // per-level Lorentz factor, or null (LFfac everywhere)
   int cour_mode;
   double cf2, af2, valfac;
   unsigned long long *vr2max, *vh2max;

@@ -343,13 +343,14 @@ class Plan:
         return _lib.lib().mt_nl_bouss_workspace(self._h, int(n_r), int(l_mag), int(l_chem))
 
     def nl_bouss(self, fields, prof, LFfac, courfac, alffac, opm, l_mag=True, l_chem=False,
-                 damp=True, out=None, work=None, parts=0):
+                 damp=True, out=None, work=None, parts=0, LFfac_r=None):
         """Fused Boussinesq nonlinear stage (magic_torch/step_time.py:931-1213, steps 1-3 + CFL).
 
         ``fields``: dict of spectral (lm_max, n_r) complex128 arrays w, dw, ddw, z, dz, s
         (+ b, db, ddb, aj, dj if l_mag, xi if l_chem).  ``prof``: or2, or4, orho1, orho2,
         delxr2, delxh2 over the n_r levels.  Returns (outputs dict, dtrkc, dthkc); outputs
-        are (lm_max, n_r) with boundary columns zero.
+        are (lm_max, n_r) with boundary columns zero.  LFfac_r: optional per-level
+        Lorentz factor replacing LFfac (levels of several runs in one call).
         """
         w = fields["w"]
         n_r = w.shape[1]
@@ -374,9 +375,15 @@ class Plan:
         bo = _lib.BoussOut(*[out[k].data_ptr() if k in out else None for k in
                              ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp",
                               "VXir", "VXit")], out["Advr"].stride(0))
+        lf_r = None
+        if LFfac_r is not None:
+            lf_r = self._prof(LFfac_r, n_r)
+            if lf_r.numel() != n_r:
+                raise ValueError(f"LFfac_r: expected {n_r} per-level values")
         bp = _lib.BoussParams(*[k.data_ptr() for k in keep.values()], float(LFfac),
                               float(courfac), float(alffac), float(opm), int(l_mag),
-                              int(l_chem), (1 if damp else 2) if l_mag else 0, int(parts))
+                              int(l_chem), (1 if damp else 2) if l_mag else 0, int(parts),
+                              lf_r.data_ptr() if lf_r is not None else None)
         dtr = torch.empty(n_r, dtype=_RD, device=self.device)
         dth = torch.empty_like(dtr)
         L = _lib.lib()

@@ -127,8 +127,7 @@ class BoussinesqStep:
                    for e in ("s", "z", "w", "b", "j") + (("p",) if self.std_form else ())}
         self.nl_out = {k: z() for k in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt",
                                         "VxBp")}
-        self.work = torch.empty(self.plan.nl_bouss_workspace(n_r, True, False), dtype=torch.uint8,
-                                device=dev)
+        self._work = None  # the stage workspace, allocated at the first own stage
         self.bots = torch.zeros(self.lm_max, dtype=_CD, device=dev)
         self.bots[0] = math.sqrt(4.0 * math.pi)  # fixed entropy at the inner boundary, l = m = 0
 
@@ -281,15 +280,39 @@ class BoussinesqStep:
             self._l_dev = torch.as_tensor(self.plan.lm2l, dtype=torch.long, device=self.device)
         return self._l_dev
 
+    @property
+    def work(self):
+        """Workspace of this step's own fused stage (runs whose stage is shared
+        with other runs never allocate it)."""
+        if self._work is None:
+            self._work = torch.empty(self.plan.nl_bouss_workspace(self.n_r, True, False),
+                                     dtype=torch.uint8, device=self.device)
+        return self._work
+
+    STAGE_INPUTS = ("w", "dw", "ddw", "z", "dz", "s", "b", "db", "ddb", "aj", "dj")
+    STAGE_OUTPUTS = ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp")
+
     def radial_loop(self):
         """Explicit stage: nonlinear products and Courant limits, then the explicit
         time derivatives into each equation's expl0 (step_time.py:931-1213)."""
+        dtr, dth = self.nonlinear_stage()
+        self.explicit_terms()
+        return dtr, dth
+
+    def nonlinear_stage(self):
+        """The fused nonlinear stage of the radial loop into self.nl_out; returns
+        the per-level Courant steps (dtrkc, dthkc)."""
         f = self.f
-        fields = {k: f[k] for k in ("w", "dw", "ddw", "z", "dz", "s", "b", "db", "ddb", "aj",
-                                    "dj")}
-        out, dtr, dth = self.plan.nl_bouss(fields, self.prof, self.LFfac, 2.5, 1.0, self.opm,
-                                           l_mag=True, out=self.nl_out, work=self.work)
-        ins = dict(out, w=f["w"], dw=f["dw"], ddw=f["ddw"], z=f["z"], dz=f["dz"])
+        fields = {k: f[k] for k in self.STAGE_INPUTS}
+        _, dtr, dth = self.plan.nl_bouss(fields, self.prof, self.LFfac, 2.5, 1.0, self.opm,
+                                         l_mag=True, out=self.nl_out, work=self.work)
+        return dtr, dth
+
+    def explicit_terms(self):
+        """get_td + finish_exp from self.nl_out (whoever filled it: this step's own
+        stage, or a stage shared by several runs) into each equation's expl0."""
+        f = self.f
+        ins = dict(self.nl_out, w=f["w"], dw=f["dw"], ddw=f["ddw"], z=f["z"], dz=f["dz"])
         td_out = dict(dwdt=self.ta["w"]["expl0"], dzdt=self.ta["z"]["expl0"],
                       dsdt=self.ta["s"]["expl0"], dbdt=self.ta["b"]["expl0"],
                       djdt=self.ta["j"]["expl0"])
@@ -297,7 +320,6 @@ class BoussinesqStep:
             td_out["dpdt"] = self.ta["p"]["expl0"]
         self.plan.get_td(ins, self.prof, self.CorFac, self.sch.D1,
                          l_double_curl=not self.std_form, l_heat=True, l_mag=True, out=td_out)
-        return dtr, dth
 
     def lm_loop(self):
         """Implicit solves S, Z, W, B (step_time.py:1478-1527)."""

@@ -53,3 +53,30 @@ def test_graph_steps_equal_eager_steps():
     g, _ = _serve([A], use_graph=True)
     e, _ = _serve([A], use_graph=False)
     _same(g[3].state, e[3].state)
+
+
+@pytest.mark.parametrize("precision", ["split", "ozaki", "fp64"])
+def test_batched_result_same_alone_and_in_the_mix(precision):
+    """Cross-run batching: runs of one l_max share one fused stage per step (their
+    levels side by side, per-level Lorentz factor), joining and leaving the group
+    as they arrive and finish; each run's final state equals, bit for bit, its
+    state when served alone (every stage kernel works per level and per row)."""
+    import dataclasses
+
+    from magic_b200.serve import BatchedEnsembleServer, EnsembleServer
+
+    specs = [dataclasses.replace(s, precision=precision) for s in
+             (_spec(0, 32, 33, steps=10), _spec(1, 32, 49, arrival=0.0, steps=14),
+              _spec(2, 64, 33, arrival=0.0, steps=9), _spec(3, 32, 33, arrival=0.001, steps=7))]
+    alone = {}
+    for s in specs:
+        srv = EnsembleServer(budget_bytes=40 << 30)
+        alone[s.run_id] = srv.serve([s], keep_state=True)[0]
+    bsrv = BatchedEnsembleServer(budget_bytes=40 << 30)
+    mix = {r.spec.run_id: r for r in bsrv.serve(specs, keep_state=True)}
+    assert sorted(mix) == [0, 1, 2, 3]
+    g32 = bsrv.groups[(32, precision, 5.0)]
+    assert g32.launches < sum(s.n_steps for s in specs if s.l_max == 32)  # steps were shared
+    for i, r in mix.items():
+        assert len(r.latencies_ms) == r.spec.n_steps
+        _same(alone[i].state, r.state)

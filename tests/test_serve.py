@@ -116,3 +116,95 @@ def test_footprint_grows_with_size():
     small = RunSpec(run_id=0, l_max=32, n_r=33, ek=1e-3, ra=1e5)
     big = RunSpec(run_id=1, l_max=127, n_r=65, ek=1e-3, ra=1e5)
     assert footprint_estimate(big) > 8 * footprint_estimate(small)
+
+
+class FakeGroup:
+    """Stand-in GroupRunner: a group step takes `step_s` of virtual time after
+    the previous one; membership changes only when drained, as in GroupRunner."""
+    clock = None
+    step_s = 1e-3
+    created = []
+
+    def __init__(self, key, device, cache, use_graph=True, depth=8):
+        self.key, self.depth = key, depth
+        self.members, self.waiting, self.finish_times = [], [], []
+        self.steps_with = []  # member run ids of every group step
+        FakeGroup.created.append(self)
+
+    def add(self, spec, admitted_s=0.0):
+        self.waiting.append(spec)
+
+    def _inflight(self):
+        return sum(1 for t in self.finish_times if t > self.clock())
+
+    def drained(self):
+        return self._inflight() == 0
+
+    def active(self):
+        return bool(self.members or self.waiting)
+
+    def can_launch(self):
+        return (bool(self.members) and not self.waiting and self._inflight() < self.depth
+                and all(m[1] < m[0].n_steps for m in self.members))
+
+    def launch(self):
+        start = max([self.clock()] + self.finish_times[-1:])
+        self.finish_times.append(start + self.step_s)
+        for m in self.members:
+            m[1] += 1
+        self.steps_with.append(tuple(m[0].run_id for m in self.members))
+
+    def poll(self):
+        pass
+
+    def retire(self, keep_state=False):
+        if not self.drained():
+            return []
+        done = [m for m in self.members if m[1] >= m[0].n_steps]
+        for m in done:
+            self.members.remove(m)
+        out = [RunResult(m[0], latencies_ms=[self.step_s * 1e3] * m[0].n_steps) for m in done]
+        self.members += [[s, 0] for s in self.waiting]
+        self.waiting = []
+        return out
+
+
+def test_batched_server_groups_runs_and_admits_between_steps():
+    from magic_b200.serve import BatchedEnsembleServer, group_key
+
+    clock = Clock()
+    FakeGroup.clock, FakeGroup.created = clock, []
+    specs = [RunSpec(run_id=i, l_max=32 if i % 2 else 64, n_r=33, ek=1e-3 * (1 + i), ra=1e5,
+                     n_steps=10 + i, arrival=0.003 * i) for i in range(8)]
+    srv = BatchedEnsembleServer(device="cpu", budget_bytes=10 ** 9, max_active=8,
+                                group_runner=FakeGroup, footprint=lambda s: 100)
+    res = srv.serve(specs, clock=clock, sleep=clock.sleep)
+    assert [r.spec.run_id for r in res] == list(range(8))
+    # two resolution groups; every step of a group holds runs of that l_max only
+    assert {g.key for g in FakeGroup.created} == {group_key(specs[0]), group_key(specs[1])}
+    by_id = {s.run_id: s for s in specs}
+    for g in FakeGroup.created:
+        for ids in g.steps_with:
+            assert {by_id[i].l_max for i in ids} == {g.key[0]}
+    # every run took exactly its steps, and some group steps served several runs at once
+    counts = {i: 0 for i in by_id}
+    for g in FakeGroup.created:
+        for ids in g.steps_with:
+            for i in ids:
+                counts[i] += 1
+    assert counts == {i: by_id[i].n_steps for i in by_id}
+    assert max(len(ids) for g in FakeGroup.created for ids in g.steps_with) >= 2
+    admits = {rid: t for t, ev, rid in srv.log if ev == "admit"}
+    for s in specs:
+        assert admits[s.run_id] >= s.arrival
+
+
+def test_group_key_separates_precision_and_pm():
+    from magic_b200.serve import group_key
+
+    a = RunSpec(run_id=0, l_max=32, n_r=33, ek=1e-3, ra=1e5)
+    b = RunSpec(run_id=1, l_max=32, n_r=49, ek=5e-4, ra=3e5)
+    c = RunSpec(run_id=2, l_max=32, n_r=33, ek=1e-3, ra=1e5, prmag=2.0)
+    d = RunSpec(run_id=3, l_max=32, n_r=33, ek=1e-3, ra=1e5, precision="fp64")
+    assert group_key(a) == group_key(b)
+    assert len({group_key(x) for x in (a, c, d)}) == 3
