@@ -80,6 +80,30 @@ def split_mma_flops(plan, n_r):
     return syn, ana
 
 
+def ozaki_mma_ops(plan, n_r, nfi=13, nfo=9):
+    """Dense int8 tensor-pipe operations the digit-split kernels issue per stage:
+    21 digit-pair MMAs per K chunk of 32, M = 128 rows per tile, N = 64 theta rows
+    (synthesis) or 32 l rows (analysis), padded tiles included."""
+    kk, rows = 32, 128
+    nhs = plan.nhs
+    nthtile = -(-nhs // 64)
+    tiles_s = -(-(n_r * 2 * nfi) // rows)
+    lev_tile = rows // (2 * nfo)
+    tiles_a = -(-(n_r - 2) // lev_tile)
+    nchj = -(-nhs // kk)
+    nk = lambda nlm, p: (nlm + 1 - p) // 2
+    syn = ana = 0.0
+    for mc in range(plan.n_m_max):
+        nlm = plan.l_max - mc * plan.minc + 1
+        for combo in (0, 1):
+            steps = -(-nk(nlm, combo) // kk) + -(-nk(nlm, 1 - combo) // kk)
+            syn += tiles_s * nthtile * steps * 21 * 2.0 * rows * 64 * kk
+        for par in (0, 1):
+            nlt = -(-nk(nlm, par) // 32)
+            ana += tiles_a * nlt * nchj * 2 * 21 * 2.0 * rows * 32 * kk
+    return syn, ana
+
+
 def synth_inputs(plan, n_r, device, seed=0):
     g = torch.Generator(device="cpu").manual_seed(seed)
     l = torch.as_tensor(plan.lm2l, dtype=torch.float64)
@@ -692,6 +716,17 @@ def run_step(args, rank, world):
                 "frac": ach / pk, "traffic": None, "kernel": dom,
                 "flops": "dense bf16 MMA FLOPs issued (6 plane products, padded tiles)",
                 "peak_source": f"{src} bf16_tflops (burst)"}
+    elif prec == "ozaki":
+        s_mma, a_mma = ozaki_mma_ops(plan, n_r)
+        fl = s_mma if dom == "legendre_synthesis" else a_mma
+        pk = 2.0 * peaks["bf16_tflops"]
+        ach = fl / (parts[dom] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TOP/s",
+                "frac": ach / pk, "traffic": None, "kernel": dom,
+                "flops": "dense int8 MMA operations issued (21 digit pairs per K chunk, "
+                         "padded tiles; the pack kernel's time is included in the part)",
+                "peak_source": f"2 x {src} bf16_tflops (burst): B200's dense int8 rate is "
+                               "twice its bf16 rate"}
     else:
         synth_f, anal_f = flops_per_step(plan.nhs, plan.lm_max, n_r)
         fl = synth_f if dom == "legendre_synthesis" else anal_f
@@ -707,8 +742,10 @@ def run_step(args, rank, world):
     del st, state, host, host_back
     torch.cuda.empty_cache()
 
-    # --- the plain FP64 path: the same steps with the FP64 stage
+    # --- the plain FP64 path: the same steps with the FP64 stage; and the
+    # bf16x3 / FP32 split stage (fastest, ~1e-6 of scale per stage)
     plain = None
+    other = {}
     if prec != "fp64":
         sf = build("fp64")
         plain_ms = timed_steps(sf, args.steps)
@@ -719,13 +756,27 @@ def run_step(args, rank, world):
                  "kernel_ms": part_times(sf)}
         del sf
         torch.cuda.empty_cache()
+    for alt in ("split",):
+        if alt == prec or args.no_alt:
+            continue
+        sa = build(alt)
+        alt_ms = timed_steps(sa, args.steps)
+        other[alt] = {"value": job_steps_per_s(world, alt_ms), "unit": "steps/s",
+                      "ms_per_step": alt_ms,
+                      "what": "the same whole steps with the bf16x3 / FP32-accumulate split "
+                              "stage and FP32 phi stage (~1e-6 of scale per stage)",
+                      "kernel_ms": part_times(sa)}
+        del sa
+        torch.cuda.empty_cache()
     drift = measure_drift(args, dev, rank) if args.drift_steps > 0 else None
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": ("bf16x3/f32 stage, f64 solves" if split else "f64"),
+                "dtype": {"split": "bf16x3/f32 stage, f64 solves",
+                          "ozaki": "int8 digit planes (exact int32 accumulation, f64 combine), "
+                                   "f64 phi stage and solves"}.get(prec, "f64"),
                 "data": "synthetic", "config": step_workload_config(args, prec),
                 "clocks": clocks.summary(),
                 "e2e": {"value": job_steps_per_s(world, e2e_ms), "unit": "steps/s",
@@ -739,6 +790,8 @@ def run_step(args, rank, world):
                 "kernel_ms": parts, "sht_tflops": sht_tflops, "roofline": roof}
         if plain is not None:
             line["fp64_plain"] = plain
+        for k, v in other.items():
+            line[f"{k}_stage"] = v
         if drift:
             line["drift"] = drift
         if world == 1 and not args.no_cpu:
@@ -969,7 +1022,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="split", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="ozaki", choices=["fp64", "split", "ozaki"],
+                    help="stage precision of the timed steps: ozaki (digit-split tensor-core "
+                         "Legendre + FP64 phi stage, the mode that meets the precision bounds), "
+                         "split (bf16x3 / FP32), fp64")
+    ap.add_argument("--no-alt", action="store_true", help="skip the alternative split leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--workload", default="step",
@@ -1185,6 +1242,15 @@ def main():
                 "frac": ach / pk, "traffic": None, "kernel": dom,
                 "flops": "dense bf16 MMA FLOPs issued (6 plane products, padded tiles)",
                 "peak_source": f"{src} bf16_tflops (burst)"}
+    elif args.precision == "ozaki":
+        s_mma, a_mma = ozaki_mma_ops(plan, n_r)
+        fl = s_mma if dom == "legendre_synthesis" else a_mma
+        pk = 2.0 * peaks["bf16_tflops"]
+        ach = fl / (part_ms[dom] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TOP/s",
+                "frac": ach / pk, "traffic": None, "kernel": dom,
+                "flops": "dense int8 MMA operations issued (21 digit pairs per K chunk)",
+                "peak_source": f"2 x {src} bf16_tflops (burst)"}
     else:
         fl = synth_f if dom == "legendre_synthesis" else anal_f
         pk = dgemm_peak(dev) if rank == 0 else float("nan")
@@ -1195,13 +1261,15 @@ def main():
                                "(no FP64 entry in MEASURED_PEAKS.json)"}
     sht_tflops = (synth_f + anal_f) / ((part_ms["legendre_synthesis"] +
                                         part_ms["legendre_analysis"]) * 1e-3) / 1e12
-    plain = fp64_plain_stage(args, dev, fields, prof, stream, dist) if split else None
+    plain = (fp64_plain_stage(args, dev, fields, prof, stream, dist)
+             if args.precision != "fp64" else None)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "bf16x3/f32" if split else "f64", "data": "synthetic",
+                "dtype": {"split": "bf16x3/f32", "ozaki": "int8 digits/f64"}.get(
+                    args.precision, "f64"), "data": "synthetic",
                 "config": workload_config(args.precision),
                 "clocks": clocks.summary(),
                 "e2e": {"value": job_steps_per_s(world, e2e_ms), "unit": "steps/s",

@@ -347,6 +347,20 @@ MT_API int mt_get_td(const mt_plan* plan, int n_r, const mt_td_in* in, const mt_
  * *_l of l_max+1 and *_r of n_r values; so_l/so_r NULL mean 1, ic_r NULL 0. */
 typedef struct mt_lop mt_lop;
 MT_API int mt_lop_create(int n_l, int n_r, const double* M_host, mt_lop** op);
+
+/* Banded form of the per-degree solve (replaces the dense inverse where the
+ * reference factorises: finite differences of order > 2, magic_torch/
+ * update_s.py:95-104, update_z.py:119-127, update_b.py:127-131,
+ * update_w_doublecurl.py:106-125): A_host holds, per l = 0..n_l-1, the
+ * preconditioned n_r x n_r LHS (row-major, zero outside kl sub- and ku
+ * super-diagonals); fac_row (and fac_col, or NULL) the scalings of the solve,
+ * (n_l, n_r) row-major.  Each matrix is factored on the host with pivoted
+ * banded LU (algebra.py:371-457, LINPACK dgbfa order) and the updates then
+ * solve fac_col * U^-1 L^-1 P (fac_row * rhs) on the GPU in the reference's
+ * dgbsl order (algebra.py:460-510).  Used by mt_update_field and
+ * mt_update_poloidal; mt_update_wp needs the dense form. */
+MT_API int mt_lop_create_band(int n_l, int n_r, int kl, int ku, const double* A_host,
+                              const double* fac_row, const double* fac_col, mt_lop** op);
 MT_API int mt_lop_destroy(mt_lop* op);
 
 typedef struct {

@@ -174,6 +174,9 @@ _PROTOS = {
     "mt_energy_workspace": (C.c_size_t, [C.c_void_p]),
     "mt_energy": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(EnergyArgs), _dp, _dp, C.c_size_t,
                             _dp]),
+    "mt_lop_create_band": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_void_p)]),
     "mt_lop_destroy": (C.c_int, [C.c_void_p]),
     "mt_update_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FieldUpdate), C.c_void_p,
                                   C.c_void_p, C.c_void_p, _dp]),

@@ -37,6 +37,13 @@
 struct mt_lop {
   int n_l = 0, n_r = 0, ldm = 0, device = 0;  // ldm: j stride (>= n_r, multiple of 8)
   double* mt = nullptr;  // (n_l, n_r, ldm) transposed: mt[(l * n_r + k) * ldm + j] = M_l[j][k]
+  // banded form (mt null): pivoted LU factors of the preconditioned matrices in
+  // band storage, (n_l, 2 kl + ku + 1, n_r) row-major, 1-based pivots (n_l, n_r),
+  // and the row / column scalings (n_l, n_r) of the solve (fc may be null)
+  int kl = 0, ku = 0;
+  double* abd = nullptr;
+  int* piv = nullptr;
+  double *fr = nullptr, *fc = nullptr;
 };
 
 namespace mt {
@@ -226,8 +233,74 @@ __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int 
   }
 }
 
+// Band factors of a banded per-degree operator set (null abd: dense form).
+struct BandView {
+  const double* abd;
+  const int* piv;
+  const double *fr, *fc;
+  int kl, ku;
+};
+
+// Pivoted banded LU solve of the CTA's rows in shared memory (the reference's
+// solve_band_real, magic_torch/algebra.py:460-510, LINPACK dgbsl order, with
+// the row and column scalings of banded_solve_by_l, :672-728): thread t <
+// 2 nrow solves part t % 2 of row t / 2 in place (row stride fs); products and
+// sums are rounded separately (no contraction), as the reference computes
+// them.  m = 0 keeps only the real part.  Ends with a barrier.
+__device__ __forceinline__ void band_solve_rows(const BandView& b, int l, int n_r, int fs,
+                                                double2* f, int nrow, int mc0) {
+  const int t = threadIdx.x;
+  if (t < 2 * nrow) {
+    const int row = t >> 1, part = t & 1;
+    double* x = reinterpret_cast<double*>(f + row * fs) + part;  // level k at x[2 k]
+    const int kl = b.kl, ku = b.ku, m = kl + ku + 1;
+    const double* abd = b.abd + (int64_t)l * (2 * kl + ku + 1) * n_r;  // abd[i n_r + j]
+    const int* piv = b.piv + (int64_t)l * n_r;
+    const double* fr = b.fr + (int64_t)l * n_r;
+    for (int k = 0; k < n_r; ++k) x[2 * k] = __dmul_rn(fr[k], x[2 * k]);
+    for (int k = 1; k <= n_r - 1 && kl != 0; ++k) {  // L y = P (fr rhs), 1-based k
+      const int lm = min(kl, n_r - k), lp = piv[k - 1];
+      if (lp != k) {
+        const double tv = x[2 * (k - 1)];
+        x[2 * (k - 1)] = x[2 * (lp - 1)];
+        x[2 * (lp - 1)] = tv;
+      }
+      const double xk = x[2 * (k - 1)];
+      for (int i = 1; i <= lm; ++i)
+        x[2 * (k - 1 + i)] =
+            __dadd_rn(x[2 * (k - 1 + i)], __dmul_rn(xk, abd[(m - 1 + i) * n_r + (k - 1)]));
+    }
+    for (int k = n_r; k >= 1; --k) {  // U x = y
+      x[2 * (k - 1)] = __ddiv_rn(x[2 * (k - 1)], abd[(m - 1) * n_r + (k - 1)]);
+      const int lm = min(k, m) - 1, la = m - lm, lb = k - lm;
+      const double tv = -x[2 * (k - 1)];
+      for (int i = 0; i < lm; ++i)
+        x[2 * (lb - 1 + i)] =
+            __dadd_rn(x[2 * (lb - 1 + i)], __dmul_rn(tv, abd[(la - 1 + i) * n_r + (k - 1)]));
+    }
+    if (b.fc) {
+      const double* fc = b.fc + (int64_t)l * n_r;
+      for (int k = 0; k < n_r; ++k) x[2 * k] = __dmul_rn(fc[k], x[2 * k]);
+    }
+    if (part == 1 && mc0 + row == 0)
+      for (int k = 0; k < n_r; ++k) x[2 * k] = 0.0;
+  }
+  __syncthreads();
+}
+
+// the solved rows (band form) from shared memory to the field's global array
+__device__ __forceinline__ void store_rows(const double2* f, int fs, int n_r, int nrow,
+                                           const int* lm, double2* __restrict__ out, int64_t ld) {
+  for (int e = threadIdx.x; e < nrow * n_r; e += blockDim.x) {
+    const int row = e / n_r, j = e - row * n_r;
+    out[(int64_t)lm[row] * ld + j] = f[row * fs + j];
+  }
+  __syncthreads();
+}
+
 struct UsArgs {
   int n_r, ldm, fs, l_max, minc, n_m, groups;
+  BandView band;
   const int* lstart;
   double2 *x, *dx, *d2x, *old, *impl, *expl0, *expl1;
   const double2 *top, *bot;
@@ -376,8 +449,10 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
   if (nrow == 0) return;
   double2* f = usbuf;                           // [rows][fs]: rhs, then x
   double* mbuf = (double*)(usbuf + rows * fs);  // staged: [2][kKc][ldm]
-  const double* Ml = a.mt + (int64_t)l * n_r * ldm;
-  if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
+  const bool band = a.band.abd != nullptr;
+  const double* Ml = band ? nullptr : a.mt + (int64_t)l * n_r * ldm;
+  if constexpr (kStaged)
+    if (!band) stage_chunk(Ml, n_r, ldm, 0, mbuf);
   if (threadIdx.x < rows)
     lm_row[threadIdx.x] = threadIdx.x < nrow
         ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
@@ -385,8 +460,13 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
   build_rhs<false, 3>(a, l, rows, nrow, lm_row, f);
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
-  solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.x, a.ld,
-                              lm_row);
+  if (band) {
+    band_solve_rows(a.band, l, n_r, fs, f, nrow, mc0);
+    store_rows(f, fs, n_r, nrow, lm_row, a.x, a.ld);
+  } else {
+    solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.x, a.ld,
+                                lm_row);
+  }
   if (!s.active) return;
   auto lm_of = [&](int row) { return lm_row[row]; };
   const double so_l = a.so_l ? a.so_l[l] : 1.0, ia_l = a.ia_l[l], ic_l = a.ic_l[l];
@@ -418,6 +498,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
 
 struct PwArgs {
   int n_r, ldm, fs, l_max, minc, n_m, groups;
+  BandView band;
   const int* lstart;
   double2 *w, *dw, *ddw, *old, *impl, *expl0, *expl1, *p;
   const double2 *s, *xi;
@@ -444,8 +525,10 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
   double2* f = pwbuf;                 // [rows][fs]: rhs, then w
   double2* dd = pwbuf + rows * fs;    // [rows][fs]: D2 w
   double* mbuf = (double*)(pwbuf + 2 * rows * fs);
-  const double* Ml = a.mt + (int64_t)l * n_r * ldm;
-  if constexpr (kStaged) stage_chunk(Ml, n_r, ldm, 0, mbuf);
+  const bool band = a.band.abd != nullptr;
+  const double* Ml = band ? nullptr : a.mt + (int64_t)l * n_r * ldm;
+  if constexpr (kStaged)
+    if (!band) stage_chunk(Ml, n_r, ldm, 0, mbuf);
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
   if (threadIdx.x < rows)
@@ -456,8 +539,13 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
   build_rhs<true, 2>(a, l, rows, nrow, lm_row, f);
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
-  solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.w, a.ld,
-                              lm_row);
+  if (band) {
+    band_solve_rows(a.band, l, n_r, fs, f, nrow, mc0);
+    store_rows(f, fs, n_r, nrow, lm_row, a.w, a.ld);
+  } else {
+    solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.w, a.ld,
+                                lm_row);
+  }
   const double2* fr = f + s.rg * kRows * fs;
   double2* dr = dd + s.rg * kRows * fs;
   if (s.active) {
@@ -807,7 +895,7 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
 }
 
 int check_lop(const mt_lop* op) {
-  MT_REQUIRE(op && op->mt, MT_ERR_ARG, "null per-degree operator");
+  MT_REQUIRE(op && (op->mt || op->abd), MT_ERR_ARG, "null per-degree operator");
   int dev = -1;
   MT_CHECK_CUDA(cudaGetDevice(&dev));
   MT_REQUIRE(dev == op->device, MT_ERR_ARG,
@@ -861,8 +949,123 @@ int mt_lop_create(int n_l, int n_r, const double* M, mt_lop** out) {
 
 int mt_lop_destroy(mt_lop* op) {
   if (!op) return MT_OK;
-  if (op->mt) cudaFree(op->mt);
+  void* ptrs[] = {op->mt, op->abd, op->piv, op->fr, op->fc};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
   delete op;
+  return MT_OK;
+}
+
+// Pivoted banded LU factorisation of one band matrix in place (the reference's
+// prepare_band, magic_torch/algebra.py:371-457, a port of LINPACK dgbfa with
+// partial pivoting; 1-based indices as there): abd (nb x n, row-major, diagonal
+// in row kl + ku), pivots 1-based.  Returns 0 or the 1-based singular column.
+static int band_factor(double* abd, int n, int kl, int ku, int* pivot) {
+  const double kZeroTol = 1.0e-15;
+  const int m = kl + ku + 1;
+  auto A = [&](int i, int j) -> double& { return abd[(size_t)(i - 1) * n + (j - 1)]; };
+  int info = 0;
+  const int j0 = ku + 2, j1 = std::min(n, m) - 1;
+  for (int jz = j0; jz <= j1; ++jz)
+    for (int i = m + 1 - jz; i <= kl; ++i) A(i, jz) = 0.0;
+  int jz = j1, ju = 0;
+  for (int k = 1; k <= n - 1; ++k) {
+    const int kp1 = k + 1;
+    ++jz;
+    if (jz <= n)
+      for (int i = 1; i <= kl; ++i) A(i, jz) = 0.0;
+    const int lm = std::min(kl, n - k);
+    int lrel = 0;
+    double best = std::fabs(A(m, k));
+    for (int i = 1; i <= lm; ++i)
+      if (std::fabs(A(m + i, k)) > best) {
+        best = std::fabs(A(m + i, k));
+        lrel = i;
+      }
+    int l = lrel + m;
+    pivot[k - 1] = l + k - m;
+    if (std::fabs(A(l, k)) > kZeroTol) {
+      if (l != m) std::swap(A(l, k), A(m, k));
+      const double t = -1.0 / A(m, k);
+      for (int i = 1; i <= lm; ++i) A(m + i, k) *= t;
+      ju = std::min(std::max(ju, ku + pivot[k - 1]), n);
+      int mm = m;
+      for (int j = kp1; j <= ju; ++j) {
+        --l;
+        --mm;
+        const double tt = A(l, j);
+        if (l != mm) {
+          A(l, j) = A(mm, j);
+          A(mm, j) = tt;
+        }
+        for (int i = 1; i <= lm; ++i) A(mm + i, j) += tt * A(m + i, k);
+      }
+    } else {
+      info = k;
+    }
+  }
+  pivot[n - 1] = n;
+  if (std::fabs(A(m, n)) <= kZeroTol) info = n;
+  return info;
+}
+
+int mt_lop_create_band(int n_l, int n_r, int kl, int ku, const double* A, const double* fac_row,
+                       const double* fac_col, mt_lop** out) {
+  MT_REQUIRE(out && A && fac_row && n_l >= 1 && n_r >= 2 && n_r <= 1024 && kl >= 0 && ku >= 0 &&
+                 kl < n_r && ku < n_r && kl <= 16 && ku <= 16,
+             MT_ERR_ARG, "bad banded per-degree operator argument");
+  *out = nullptr;
+  const int nb = 2 * kl + ku + 1;
+  const size_t per = (size_t)n_r * n_r, perb = (size_t)nb * n_r;
+  std::vector<double> abd(perb * n_l, 0.0);
+  std::vector<int> piv((size_t)n_l * n_r, 0);
+  for (int l = 0; l < n_l; ++l) {
+    const double* Al = A + l * per;
+    double amax = 0.0;
+    for (size_t e = 0; e < per; ++e) {
+      MT_REQUIRE(std::isfinite(Al[e]), MT_ERR_ARG, "banded operator not finite");
+      amax = std::max(amax, std::fabs(Al[e]));
+    }
+    double* b = abd.data() + l * perb;
+    for (int j = 0; j < n_r; ++j)
+      for (int i = 0; i < n_r; ++i) {
+        const double v = Al[(size_t)i * n_r + j];
+        if (i < j - ku || i > j + kl) {
+          MT_REQUIRE(std::fabs(v) <= 1e-14 * amax, MT_ERR_ARG,
+                     "banded operator has entries outside its band");
+        } else {
+          b[(size_t)(kl + ku + i - j) * n_r + j] = v;
+        }
+      }
+    MT_REQUIRE(band_factor(b, n_r, kl, ku, piv.data() + (size_t)l * n_r) == 0, MT_ERR_ARG,
+               "banded operator is singular");
+  }
+  mt_lop* op = new mt_lop();
+  op->n_l = n_l;
+  op->n_r = n_r;
+  op->ldm = n_r;
+  op->kl = kl;
+  op->ku = ku;
+  const size_t nf = (size_t)n_l * n_r;
+  bool ok = cudaGetDevice(&op->device) == cudaSuccess &&
+            cudaMalloc(&op->abd, abd.size() * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&op->piv, piv.size() * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&op->fr, nf * sizeof(double)) == cudaSuccess &&
+            (!fac_col || cudaMalloc(&op->fc, nf * sizeof(double)) == cudaSuccess);
+  ok = ok &&
+       cudaMemcpy(op->abd, abd.data(), abd.size() * sizeof(double), cudaMemcpyHostToDevice) ==
+           cudaSuccess &&
+       cudaMemcpy(op->piv, piv.data(), piv.size() * sizeof(int), cudaMemcpyHostToDevice) ==
+           cudaSuccess &&
+       cudaMemcpy(op->fr, fac_row, nf * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+       (!fac_col ||
+        cudaMemcpy(op->fc, fac_col, nf * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess);
+  if (!ok) {
+    mt_lop_destroy(op);
+    set_error("banded operator allocation or upload failed");
+    return MT_ERR_CUDA;
+  }
+  *out = op;
   return MT_OK;
 }
 
@@ -900,6 +1103,7 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.so_l = u->so_l; a.so_r = u->so_r; a.ia_l = u->ia_l; a.ia_r = u->ia_r; a.ib_r = u->ib_r;
   a.ic_r = u->ic_r; a.ic_l = u->ic_l; a.ic_r2 = u->ic_r2;
   a.mt = solve->mt;
+  a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku};
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1);
@@ -955,6 +1159,7 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.or2 = u->or2; a.orho1 = u->orho1; a.beta = u->beta; a.visc = u->visc; a.rgrav = u->rgrav;
   a.rho0 = u->rho0; a.c3 = u->c3; a.c2n = u->c2n; a.c1n = u->c1n; a.c1d = u->c1d; a.c0n = u->c0n;
   a.mt = solve->mt;
+  a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku};
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);
@@ -983,6 +1188,7 @@ int mt_update_wp(const mt_plan* p, int n_r, const mt_wp_update* u, const mt_lop*
   MT_TRY(check_radial_op(D2));
   MT_TRY(check_radial_op(D3));
   MT_TRY(check_radial_op(P0));
+  MT_REQUIRE(solve->mt, MT_ERR_ARG, "the coupled (w, p) update takes a dense operator set");
   MT_REQUIRE(solve->n_r == 2 * n_r && radial_op_size(D1) == n_r && radial_op_size(D2) == n_r &&
                  radial_op_size(D3) == n_r && radial_op_size(P0) == n_r,
              MT_ERR_ARG, "operator sizes differ from n_r (solve operators: 2 n_r)");

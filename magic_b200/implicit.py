@@ -37,11 +37,42 @@ def _dct1(n):
     return Cm / np.sqrt(2.0 * N)
 
 
+class Band:
+    """Preconditioned per-degree LHS for a pivoted banded LU solve: A (n_l, n_r,
+    n_r) with kl sub- and ku super-diagonals, the row scaling fr (n_l, n_r) and
+    the column scaling fc (or None) of the solve x = fc U^-1 L^-1 P (fr rhs)."""
+
+    def __init__(self, A, fr, fc, kl, ku):
+        self.A, self.fr, self.fc, self.kl, self.ku = A, fr, fc, int(kl), int(ku)
+
+
+def _banded(sch):
+    """The reference factorises instead of inverting on finite-difference grids of
+    order > 2 (magic_torch/update_s.py:95-104 and the same test in update_z.py,
+    update_b.py, update_w_doublecurl.py)."""
+    return (not sch.chebyshev) and getattr(sch, "fd_order", 2) > 2
+
+
+def _band_width(sch):
+    """kl = ku of the S, Z, B and J matrices on such grids: max(fd_order / 2,
+    fd_order_bound) (update_s.py:101, update_z.py:125, update_b.py:129)."""
+    return max(sch.fd_order // 2, getattr(sch, "fd_order_bound", 2))
+
+
 def _inverse_ops(A, sch, zero_l0=False, identity_l0=False):
     """M_l = A_l^-1 through the reference's row scaling (1 / row max), the
     Chebyshev truncation and the DCT-I to grid values folded in; degree 0 zero or
-    the identity where the reference's solve does that."""
+    the identity where the reference's solve does that.  On finite-difference
+    grids of order > 2 the row-scaled matrices are returned for a banded LU
+    solve instead (Band)."""
     N = sch.n_r
+    if _banded(sch):
+        A = A.copy()
+        if zero_l0 or identity_l0:
+            A[0] = np.eye(N)
+        fac = 1.0 / np.abs(A).max(axis=2)
+        kl = _band_width(sch)
+        return Band(fac[:, :, None] * A, fac, None, kl, kl)
     if zero_l0 or identity_l0:
         A = A.copy()
         A[0] = np.eye(N)
@@ -183,7 +214,11 @@ def poloidal_dc_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbot
     D = (np.eye(N), sch.D1m, sch.D2m, sch.D3m, sch.D4m)
     c3, c2n, c1n, c1d, c0n = _w_coefficient_profiles(prof)
     or1, or2, beta, orho1, visc = (prof[k] for k in ("or1", "or2", "beta", "orho1", "visc"))
+    banded = _banded(sch)
     M = np.zeros((l_max + 1, N, N))
+    if banded:  # degree 0: the identity (update_w_doublecurl.py:136-139)
+        M[0] = np.eye(N)
+        FR, FC = np.ones((l_max + 1, N)), np.ones((l_max + 1, N))
     b = slice(2, N - 2)
     for l in range(1, l_max + 1):
         dL = float(l * (l + 1))
@@ -202,7 +237,14 @@ def poloidal_dc_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbot
         fr = 1.0 / np.abs(A).max(axis=1)
         A = fr[:, None] * A
         fc = 1.0 / np.abs(A).max(axis=0)
-        M[l] = fc[:, None] * np.linalg.inv(A * fc[None, :]) * fr[None, :]
+        if banded:
+            M[l], FR[l], FC[l] = A * fc[None, :], fr, fc
+        else:
+            M[l] = fc[:, None] * np.linalg.inv(A * fc[None, :]) * fr[None, :]
+    if banded:
+        # n_bands = max(fd_order + 3, 2 fd_order_bound + 3) (update_w_doublecurl.py:111-117)
+        kl = (max(sch.fd_order + 3, 2 * getattr(sch, "fd_order_bound", 2) + 3) - 1) // 2
+        return Band(M, FR, FC, kl, kl)
     return M
 
 
@@ -379,19 +421,35 @@ def toroidal_coefficients(l_max, hdif, visc, beta, dbeta, dLvisc, or1, or2):
 
 
 class LOp:
-    """Per-degree operator set on the GPU (mt_lop): one dense n_r x n_r matrix per l."""
+    """Per-degree operator set on the GPU (mt_lop): one dense n_r x n_r matrix per l
+    (an inverse, applied as a product), or a Band (pivoted banded LU factors,
+    solved in the reference's order)."""
 
     def __init__(self, M, device=None):
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        h = C.c_void_p()
+        if isinstance(M, Band):
+            A = np.ascontiguousarray(np.asarray(M.A, dtype=np.float64))
+            fr = np.ascontiguousarray(np.asarray(M.fr, dtype=np.float64))
+            fc = (np.ascontiguousarray(np.asarray(M.fc, dtype=np.float64)) if M.fc is not None
+                  else None)
+            self.n_l, self.n_r = A.shape[0], A.shape[1]
+            self.banded = True
+            with torch.cuda.device(self.device):
+                check(_lib.lib().mt_lop_create_band(self.n_l, self.n_r, M.kl, M.ku, dp(A), dp(fr),
+                                                    dp(fc) if fc is not None else None,
+                                                    C.byref(h)))
+            self._h = h
+            return
         M = np.ascontiguousarray(np.asarray(M, dtype=np.float64))
         if M.ndim != 3 or M.shape[1] != M.shape[2]:
             raise ValueError("expected (n_l, n_r, n_r) matrices")
         self.n_l, self.n_r = M.shape[0], M.shape[1]
-        self.device = torch.device(device) if device is not None else torch.device(
-            "cuda", torch.cuda.current_device())
-        h = C.c_void_p()
+        self.banded = False
         with torch.cuda.device(self.device):
-            check(_lib.lib().mt_lop_create(self.n_l, self.n_r,
-                                           M.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h)))
+            check(_lib.lib().mt_lop_create(self.n_l, self.n_r, dp(M), C.byref(h)))
         self._h = h
 
     def __del__(self):

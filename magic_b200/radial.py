@@ -353,6 +353,7 @@ class RadialScheme:
         self.n_r = n_r
         self.chebyshev = scheme.upper() != "FD"
         self.fd_order = fd_order
+        self.fd_order_bound = fd_order_bound
         self.n_cheb = n_r if (n_cheb is None or not self.chebyshev) else min(n_cheb, n_r)
         if not self.chebyshev:
             self.r = fd_grid(n_r, radratio, fd_stretch, fd_ratio)

@@ -10,6 +10,97 @@ import numpy as np
 from oracle.td import dct1_matrix
 
 
+def band_factor(A, kl, ku):
+    """Pivoted banded LU of the dense matrix A (zero outside kl sub- and ku
+    super-diagonals), in band storage abd[kl + ku + i - j, j] = A[i, j]: the
+    reference's dense_to_band_storage and prepare_band (magic_torch/algebra.py:
+    642-670, 371-457, a port of LINPACK dgbfa; 1-based indices as there).
+    Returns (abd, pivot) with 1-based pivots."""
+    n = A.shape[0]
+    nb = 2 * kl + ku + 1
+    abd = np.zeros((nb, n))
+    for j in range(n):
+        for i in range(max(0, j - ku), min(n, j + kl + 1)):
+            abd[kl + ku + i - j, j] = A[i, j]
+    m = kl + ku + 1
+    piv = np.zeros(n, dtype=np.int64)
+    a = lambda i, j: (i - 1, j - 1)
+    for jz in range(ku + 2, min(n, m) - 1 + 1):
+        for i in range(m + 1 - jz, kl + 1):
+            abd[a(i, jz)] = 0.0
+    jz, ju = min(n, m) - 1, 0
+    for k in range(1, n):
+        jz += 1
+        if jz <= n:
+            for i in range(1, kl + 1):
+                abd[a(i, jz)] = 0.0
+        lm = min(kl, n - k)
+        col = np.abs(abd[m - 1:m + lm, k - 1])
+        l = int(np.argmax(col)) + m
+        piv[k - 1] = l + k - m
+        if abs(abd[a(l, k)]) > 1.0e-15:
+            if l != m:
+                abd[a(l, k)], abd[a(m, k)] = abd[a(m, k)], abd[a(l, k)]
+            t = -1.0 / abd[a(m, k)]
+            abd[m:m + lm, k - 1] *= t
+            ju = min(max(ju, ku + int(piv[k - 1])), n)
+            mm = m
+            for j in range(k + 1, ju + 1):
+                l -= 1
+                mm -= 1
+                t = abd[a(l, j)]
+                if l != mm:
+                    abd[a(l, j)] = abd[a(mm, j)]
+                    abd[a(mm, j)] = t
+                abd[mm:mm + lm, j - 1] += t * abd[m:m + lm, k - 1]
+        else:
+            raise np.linalg.LinAlgError(f"singular band matrix at column {k}")
+    piv[n - 1] = n
+    return abd, piv
+
+
+def band_solve(abd, piv, kl, ku, rhs):
+    """solve_band_real (magic_torch/algebra.py:460-510, LINPACK dgbsl order) for the
+    columns of rhs (n, ncol), real or complex."""
+    x = np.array(rhs, dtype=rhs.dtype, copy=True)
+    n = x.shape[0]
+    m = kl + ku + 1
+    if kl:
+        for k in range(1, n):
+            lm = min(kl, n - k)
+            l = int(piv[k - 1])
+            if l != k:
+                x[[k - 1, l - 1]] = x[[l - 1, k - 1]]
+            x[k:k + lm] += x[k - 1:k] * abd[m:m + lm, k - 1:k]
+    for k in range(n, 0, -1):
+        x[k - 1] = x[k - 1] / abd[m - 1, k - 1]
+        lm = min(k, m) - 1
+        la, lb = m - lm, k - lm
+        if lm > 0:
+            t = -x[k - 1:k]
+            x[lb - 1:lb - 1 + lm] += t * abd[la - 1:la - 1 + lm, k - 1:k]
+    return x
+
+
+def _solve(dat, rhs, fac_row, fac_col=None, band=None):
+    """Rows rhs (count, n) of one degree through the preconditioned matrix dat:
+    np.linalg.solve, or the reference's banded LU (band = (kl, ku)) where it
+    factorises (finite differences of order > 2, banded_solve_by_l,
+    magic_torch/algebra.py:672-728)."""
+    b = fac_row[None, :] * rhs
+    if band is None:
+        y = np.linalg.solve(dat, b.T).T
+    else:
+        abd, piv = band_factor(dat, *band)
+        y = band_solve(abd, piv, band[0], band[1], b.T).T
+    return y if fac_col is None else fac_col[None, :] * y
+
+
+def _bw(fd_order, fd_order_bound):
+    """Band width kl = ku of the S, Z, B and J matrices (update_s.py:97-104)."""
+    return max(fd_order // 2, fd_order_bound)
+
+
 def cnab2_weights(dt1, dt2, alpha=0.6):
     """wimp, wimp_lin, wexp of CNAB2 (magic_torch/time_scheme.py:56-73)."""
     return ([1.0], [alpha * dt1, (1.0 - alpha) * dt1],
@@ -37,7 +128,8 @@ def s_matrix(l, mats, prof, wimp_lin0, opr, hdif_l, n_cheb):
     return dat
 
 
-def update_s(g, mats, prof, st, weights, opr, hdif, tops, bots, D1, D2, chebyshev, n_cheb):
+def update_s(g, mats, prof, st, weights, opr, hdif, tops, bots, D1, D2, chebyshev, n_cheb,
+             fd_order=2, fd_order_bound=2):
     """One updateS (magic_torch/update_s.py:213-271): CNAB2 right-hand side
     (time_scheme.py:82-96) with the boundary values in rows 0 and N-1, a solve per
     degree l (row-preconditioned LU), m = 0 coefficients made real, the DCT-I to
@@ -53,11 +145,12 @@ def update_s(g, mats, prof, st, weights, opr, hdif, tops, bots, D1, D2, chebyshe
     rhs[:, 0] = tops
     rhs[:, N - 1] = bots
     x = np.empty_like(rhs)
+    band = None if chebyshev or fd_order <= 2 else (_bw(fd_order, fd_order_bound),) * 2
     for l in range(g["l_max"] + 1):
         rows = np.nonzero(g["lm2l"] == l)[0]
         dat = s_matrix(l, mats, prof, wimp_lin[0], opr, hdif[l], n_cheb)
         fac = 1.0 / np.abs(dat).max(axis=1)
-        x[rows] = np.linalg.solve(fac[:, None] * dat, (fac[None, :] * rhs[rows]).T).T
+        x[rows] = _solve(fac[:, None] * dat, rhs[rows], fac, band=band)
     m0 = g["lm2m"] == 0
     x[m0] = x[m0].real
     if chebyshev:
@@ -98,7 +191,8 @@ def z_matrix(l, mats, prof, wimp_lin0, hdif_l, n_cheb, ktopv, kbotv):
     return dat
 
 
-def update_z(g, mats, prof, st, weights, hdif, D1, D2, chebyshev, n_cheb, ktopv, kbotv, fd_order):
+def update_z(g, mats, prof, st, weights, hdif, D1, D2, chebyshev, n_cheb, ktopv, kbotv, fd_order,
+             fd_order_bound=2):
     """One updateZ without inner-core rotation (magic_torch/update_z.py:333-505):
     CNAB2 right-hand side with zero boundary rows, per-l solves (l = 0: zero on the
     dense paths, the right-hand side itself on the banded finite-difference path,
@@ -120,7 +214,8 @@ def update_z(g, mats, prof, st, weights, hdif, D1, D2, chebyshev, n_cheb, ktopv,
             continue
         dat = z_matrix(l, mats, prof, wimp_lin[0], hdif[l], n_cheb, ktopv, kbotv)
         fac = 1.0 / np.abs(dat).max(axis=1)
-        x[rows] = np.linalg.solve(fac[:, None] * dat, (fac[None, :] * rhs[rows]).T).T
+        band = None if chebyshev or fd_order <= 2 else (_bw(fd_order, fd_order_bound),) * 2
+        x[rows] = _solve(fac[:, None] * dat, rhs[rows], fac, band=band)
     m0 = g["lm2m"] == 0
     x[m0] = x[m0].real
     if chebyshev:
@@ -170,7 +265,8 @@ def b_matrices(l, mats, prof, wimp_lin0, opm, hdif_l, n_cheb):
     return out
 
 
-def update_b(g, mats, prof, stb, stj, weights, opm, hdif, D1, D2, chebyshev, n_cheb, fd_order):
+def update_b(g, mats, prof, stb, stj, weights, opm, hdif, D1, D2, chebyshev, n_cheb, fd_order,
+             fd_order_bound=2):
     """One updateB with an insulating inner core (magic_torch/update_b.py:530-635):
     both fields as update_z with their own matrices (degree 0 as there), old =
     l(l+1)/r^2 x and impl = opm lambda hdif l(l+1)/r^2 (d2x [+ dLlambda dx for j]
@@ -192,7 +288,8 @@ def update_b(g, mats, prof, stb, stj, weights, opm, hdif, D1, D2, chebyshev, n_c
                 continue
             dat = b_matrices(l, mats, prof, wimp_lin[0], opm, hdif[l], n_cheb)[fi]
             fac = 1.0 / np.abs(dat).max(axis=1)
-            x[rows] = np.linalg.solve(fac[:, None] * dat, (fac[None, :] * rhs[rows]).T).T
+            band = None if chebyshev or fd_order <= 2 else (_bw(fd_order, fd_order_bound),) * 2
+            x[rows] = _solve(fac[:, None] * dat, rhs[rows], fac, band=band)
         m0 = g["lm2m"] == 0
         x[m0] = x[m0].real
         if chebyshev:
@@ -279,6 +376,9 @@ def update_w(g, mats, prof, st, weights, hdif, D1, D2, s_new, BuoFac, r, fd_orde
     four boundary rows zero, degree 0 zero, per-l solves, m = 0 real; dw, ddw,
     dddw = D1 ddw, ddddw = D2 ddw; the l = 0 pressure from rho0 BuoFac g s00 +
     Re expl0; old and impl as get_w_old / get_w_impl."""
+    # n_bands = max(fd_order + 3, 2 fd_order_bound + 3) (update_w_doublecurl.py:111-117);
+    # banded LU where the reference factorises (fd_order > 2)
+    wband = None if fd_order <= 2 else ((max(fd_order + 3, 2 * 2 + 3) - 1) // 2,) * 2
     wimp, wimp_lin, wexp = weights
     N = st["old"].shape[1]
     p = prof
@@ -295,8 +395,7 @@ def update_w(g, mats, prof, st, weights, hdif, D1, D2, s_new, BuoFac, r, fd_orde
         fr = 1.0 / np.abs(dat).max(axis=1)  # row, then column scaling as the reference
         dat = fr[:, None] * dat
         fc = 1.0 / np.abs(dat).max(axis=0)
-        y = np.linalg.solve(dat * fc[None, :], (fr[None, :] * rhs[rows]).T).T
-        x[rows] = fc[None, :] * y
+        x[rows] = _solve(dat * fc[None, :], rhs[rows], fr, fc, band=wband)
     m0 = g["lm2m"] == 0
     x[m0] = x[m0].real
     dw, ddw = x @ D1.T, x @ D2.T

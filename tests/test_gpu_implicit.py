@@ -5,12 +5,14 @@ reference's own updateS, updateZ and updateB outputs (tests/golden/td_*.npz) and
 consecutive steps at l_max = 127 / 65 Chebyshev levels and l_max = 255 / 97
 fourth-order finite-difference levels.
 
-Tolerance 1e-12 relative to each array's largest value: the GPU applies the
-inverse of each degree's matrix (with the DCT-I folded in for Chebyshev)
-where the reference and the oracle factorise and solve.  The implicit term is
-a second radial derivative of the new field: at 65 Chebyshev levels
-||D2||_inf ~ 1e7 amplifies those rounding-level differences, so it is held
-to 1e-11 (measured 1.9e-12).
+Tolerance 1e-12 relative to each array's largest value.  On Chebyshev and
+second-order finite-difference levels the GPU applies the inverse of each
+degree's matrix (with the DCT-I folded in for Chebyshev), as the reference
+does there; on finite differences of order > 2 it solves with the pivoted
+banded LU factors, in the reference's dgbsl order (the oracle restates the
+same factorisation).  The implicit term is a second radial derivative of the
+new field: at 65 Chebyshev levels ||D2||_inf ~ 1e7 amplifies rounding-level
+differences, so it is held to 1e-11 (measured 1.9e-12).
 """
 
 import numpy as np
@@ -41,8 +43,8 @@ def test_update_scalar_matches_reference(name):
     sch = SimpleNamespace(n_r=int(z["n_r_max"]), chebyshev=bool(z["chebyshev"]),
                           n_cheb=int(z["n_cheb_max"]), rMat=z["rMat"], drMat=z["drMat"],
                           d2rMat=z["d2rMat"], rnorm=float(z["rnorm"]),
-                          boundary_fac=float(z["boundary_fac"]), D1=RadialOp(z["D1"]),
-                          D2=RadialOp(z["D2"]))
+                          boundary_fac=float(z["boundary_fac"]), fd_order=int(z["fd_order"]),
+                          D1=RadialOp(z["D1"]), D2=RadialOp(z["D2"]))
     d1c = z["beta"] + z["dLtemp0"] + 2 * z["or1"] + z["dLkappa"]
     w = I.cnab2_weights(1e-4, 1.3e-4)
     lop = I.LOp(I.scalar_solve_operators(sch, p.l_max, w[1], float(z["opr"]), z["hdif_S"],
@@ -101,7 +103,7 @@ def test_update_scalar_two_steps_vs_oracle(scheme, l_max, n_r):
         I.update_scalar(p, sch, lop, s, ds, ta, w, opr, hdif, prof["kappa"], d1c, prof["or2"],
                         top=cu(tops), bot=cu(bots))
         ref = oi.update_s(g, mats, prof, st, ([w[0]], [w[1], w[2]], [w[3], w[4]]), opr, hdif,
-                          tops, bots, sch.D1m, sch.D2m, sch.chebyshev, sch.n_cheb)
+                          tops, bots, sch.D1m, sch.D2m, sch.chebyshev, sch.n_cheb, sch.fd_order)
         for k, got in (("s", s), ("ds", ds), ("impl", ta["impl"]), ("old", ta["old"]),
                        ("expl1", ta["expl1"])):
             e = rel_err(npy(got), ref[k])
@@ -287,15 +289,15 @@ def test_update_poloidal_matches_reference():
         assert v < TOL, (k, v)
 
 
-@pytest.mark.parametrize("l_max,n_r,scale", [(255, 97, 1.0), (16, 261, 50.0)])
+@pytest.mark.parametrize("l_max,n_r,scale", [(255, 97, 1.0), (16, 129, 1.0), (16, 261, 1.0)])
 def test_update_poloidal_vs_oracle(l_max, n_r, scale):
     """l_max = 255, 97 fourth-order finite-difference levels, anelastic-like
-    profiles; and l_max = 16 at 261 levels, the wide tiling (n_r > 256).  The
-    GPU applies the inverse of the fourth-order double-curl operator, whose
-    rounding error grows with its condition number (~ n_r^4): the tolerances
-    are scaled by 50 ~ (261 / 97)^4 there (a numpy restatement of the same
-    inverse-apply algorithm differs from the oracle by 8.0e-11 in impl and
-    4.3e-12 in dw at 261 levels)."""
+    profiles; and l_max = 16 at 261 levels, the wide tiling (n_r > 256).  GPU
+    and oracle both solve the fourth-order double-curl operator with its pivoted
+    banded LU factors (the reference's algorithm on these grids), so they agree
+    to 1e-12 (1e-11 for the terms with D2 of the new field) at both sizes;
+    the dense inverse the GPU applied before differed from the factorised solve
+    by 2.6e-12 at 97 levels and 8e-11 at 261 (conditioning ~ n_r^4)."""
     from magic_b200 import Plan
     from magic_b200 import implicit as I
     from magic_b200.radial import RadialScheme

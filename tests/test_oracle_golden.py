@@ -211,7 +211,8 @@ def test_update_s_oracle(name):
     z, g, prof, mats, st = _s_case(name)
     w = (z["wimp"], z["wimp_lin"], z["wexp"])
     o = oi.update_s(g, mats, prof, st, w, float(z["opr"]), z["hdif_S"], z["tops"], z["bots"],
-                    z["D1"], z["D2"], bool(z["chebyshev"]), int(z["n_cheb_max"]))
+                    z["D1"], z["D2"], bool(z["chebyshev"]), int(z["n_cheb_max"]),
+                    int(z["fd_order"]))
     assert rel_err(o["s"], z["s_new"]) < 1e-14
     assert rel_err(o["ds"], z["ds_new"]) < 1e-14
     assert rel_err(o["impl"], z["s_impl_new"]) < 1e-14
@@ -286,7 +287,17 @@ def test_toroidal_solve_operators(name):
     rhs = w[0] * z["z_old"] + w[2] * z["z_impl"] + w[3] * z["z_expl0"] + w[4] * z["z_expl1"]
     rhs[:, 0] = 0.0
     rhs[:, -1] = 0.0
-    x = np.stack([M[l] @ rhs[i] for i, l in enumerate(z["lm2l"])])
+    if isinstance(M, I.Band):  # finite differences of order > 2: the banded LU solve
+        from oracle import implicit as oi
+
+        x = np.zeros_like(rhs)
+        for l in range(int(z["l_max"]) + 1):
+            rows = np.nonzero(z["lm2l"] == l)[0]
+            abd, piv = oi.band_factor(M.A[l], M.kl, M.ku)
+            y = oi.band_solve(abd, piv, M.kl, M.ku, (M.fr[l][None, :] * rhs[rows]).T).T
+            x[rows] = y if M.fc is None else M.fc[l][None, :] * y
+    else:
+        x = np.stack([M[l] @ rhs[i] for i, l in enumerate(z["lm2l"])])
     x[z["lm2m"] == 0] = x[z["lm2m"] == 0].real
     assert rel_err(x, z["z_new"]) < 1e-13
 
