@@ -8,8 +8,11 @@ For them the library offers one entry point whose workspace is a fixed
 check it against the workspace-taking mt_scal_to_spat (1e-12 relative, the
 FP64 tolerance of the other tests) on two calls in a row, the second with
 different data so leftovers of the first call would show, and check that an
-oversized batch is refused before any launch.  This file is collected last
-so a failure here comes after every other test has run.
+oversized batch is refused before any launch.  Split-precision plans keep
+their operand images in the same array, so their limit is lower (the
+workspace query gives it); their device status is read with
+mt_noalloc_status.  This file is collected last so a failure here comes after
+every other test has run.
 """
 
 import ctypes
@@ -63,6 +66,44 @@ def test_noalloc_refuses_oversized_batch():
     Slm = _spec(plan, B, 3)
     out = torch.empty(B, plan.n_theta_max, plan.n_phi_max, dtype=torch.float64, device="cuda")
     L = _lib.lib()
+    rc = L.mt_scal_to_spat_noalloc(plan._h, ctypes.c_void_p(Slm.data_ptr()), Slm.stride(0), B,
+                                   ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 4  # MT_ERR_WORKSPACE
+    assert b"16 MiB" in L.mt_last_error()
+
+
+def test_noalloc_split_plan_matches_and_reports_status():
+    """A split-precision plan keeps its operand images in the same fixed array;
+    the allocation-free call gives the same grids as the workspace-taking call
+    (same kernels, so to FP64 rounding of the same arithmetic), and its device
+    status, which only mt_noalloc_status can read, is 0."""
+    from magic_b200 import Plan, _lib
+
+    plan = Plan(63, precision="split")
+    L = _lib.lib()
+    for seed, B in ((4, 2), (5, 3)):
+        assert L.mt_transform_workspace(plan._h, B, 1) <= 16 << 20
+        Slm = _spec(plan, B, seed)
+        ref = plan.scal_to_spat(Slm)
+        got = _noalloc(plan, Slm)
+        code = ctypes.c_int(-1)
+        _lib.check(L.mt_noalloc_status(ctypes.byref(code),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        assert code.value == 0
+        err = (got - ref).abs().max().item() / ref.abs().max().item()
+        assert err < 1e-12, err
+
+
+def test_noalloc_split_plan_refuses_oversized_batch():
+    from magic_b200 import Plan, _lib
+
+    plan = Plan(63, precision="split")
+    L = _lib.lib()
+    B = 1
+    while L.mt_transform_workspace(plan._h, B, 1) <= 16 << 20:
+        B += 1
+    Slm = _spec(plan, B, 6)
+    out = torch.empty(B, plan.n_theta_max, plan.n_phi_max, dtype=torch.float64, device="cuda")
     rc = L.mt_scal_to_spat_noalloc(plan._h, ctypes.c_void_p(Slm.data_ptr()), Slm.stride(0), B,
                                    ctypes.c_void_p(out.data_ptr()), None)
     assert rc == 4  # MT_ERR_WORKSPACE
