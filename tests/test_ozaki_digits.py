@@ -1,0 +1,82 @@
+"""The digit-split (ozaki) contraction of the fused stage, restated in numpy on
+the CPU: six signed 7-bit digits per value at a power-of-two scale shared by a
+row (data) or a column (table), the 21 digit pairs with i + j <= 5 summed by
+weight group exactly in integers (as the int32 TMEM accumulators of
+tcgen05.mma kind::i8 sum them), combined in FP64.  Checks the digit range
+and the exactness of the decomposition, that every group sum fits int32 with
+a wide margin, and that the synthesis- and analysis-shaped Legendre
+contractions of the l_max = 255 grid are accurate to ~1e-12 of their scale
+(the FP64 oracle tables and the benchmark's spectral decay)."""
+
+import numpy as np
+import pytest
+
+from oracle import grid as og
+
+D, G = 6, 6  # digits per operand, weight groups kept (i + j <= 5)
+
+
+def digits(x, axis):
+    """(digit planes, exponents): x = 2^(e - 6) sum_i d_i 2^(-7 i) + O(2^(e - 42)),
+    e per row (axis = 1) or column (axis = 0), |x| < 2^e."""
+    mx = np.abs(x).max(axis=axis, keepdims=True)
+    e = np.where(mx > 0, np.frexp(mx)[1], 0)
+    y = np.ldexp(x, 6 - e)
+    ds = []
+    for _ in range(D):
+        q = np.rint(y)
+        ds.append(q.astype(np.int64))
+        y = (y - q) * 128.0
+    return ds, e
+
+
+def contract(A, B):
+    da, ea = digits(A, 1)
+    db, eb = digits(B, 0)
+    out = np.zeros((A.shape[0], B.shape[1]))
+    groups = []
+    for g in range(G):
+        C = np.zeros(out.shape, dtype=np.int64)
+        for i in range(g + 1):
+            C += da[i] @ db[g - i]  # exact integer sums, as the int32 accumulators
+        groups.append(C)
+    for g in range(G - 1, -1, -1):
+        out = out / 128.0 + groups[g]
+    return np.ldexp(out, ea + eb - 12), groups, (da, db)
+
+
+def test_digits_are_small_and_reconstruct():
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((8, 300)) * np.exp(rng.uniform(-30, 30, (8, 1)))
+    ds, e = digits(x, 1)
+    for d in ds:
+        assert np.abs(d).max() <= 64
+    back = sum(np.ldexp(d.astype(np.float64), -7 * i) for i, d in enumerate(ds))
+    err = np.abs(np.ldexp(back, e - 6) - x) / np.ldexp(1.0, e)
+    assert err.max() <= 2.0 ** -41
+
+
+@pytest.mark.parametrize("kind", ["synthesis", "analysis"])
+def test_contraction_accuracy_at_lmax_255(kind):
+    g = og.Grid(255)
+    rng = np.random.default_rng(1)
+    worst, lim = 0.0, 0
+    for m in (0, 17, 64, 128, 200, 250):
+        rows = np.nonzero(g.lm2m == m)[0]
+        l = g.lm2l[rows]
+        if kind == "synthesis":
+            # rows: scaled spectra over l (the row programs' l(l+1) included)
+            A = rng.standard_normal((16, len(rows))) * (1e-4 * (l + 1.0) ** -2 * l * (l + 1))
+            B = g.Plm[rows]
+        else:
+            # rows: weighted Fourier rows of a vector product over theta (1/sin^2)
+            th = g.theta_ord[:g.NHS]
+            c = rng.standard_normal((16, len(rows))) * (1e-4 * (l + 1.0) ** -2)
+            A = (c @ g.dPlm[rows]) * (g.gauss[:g.NHS] / np.sin(th) ** 2)
+            B = g.Plm[rows].T
+        ref = A @ B
+        got, groups, _ = contract(A, B)
+        worst = max(worst, np.abs(got - ref).max() / np.abs(ref).max())
+        lim = max(lim, max(int(np.abs(c).max()) for c in groups))
+    assert worst < 2e-11, worst
+    assert lim < 2 ** 28  # int32 accumulators with >= 8 bits of margin at this K
