@@ -35,8 +35,14 @@ def configure_from_reference():
     import magic_torch.params as P
     import magic_torch.pre_calculations as pc
     import magic_torch.radial_functions as rf
+    import magic_torch.radial_scheme as rs
 
-    cfg = dict(l_max=P.l_max, minc=P.minc, LFfac=pc.LFfac)
+    # get_nl_anel reads r from radial_scheme and ViscHeatFac / OhmLossFac from
+    # radial_functions (magic_torch/get_nl_anel.py:14-16); courant_check reads
+    # LFfac and opm (magic_torch/courant.py:12-14)
+    cfg = dict(l_max=P.l_max, minc=P.minc, LFfac=float(pc.LFfac), opm=float(pc.opm),
+               ViscHeatFac=float(rf.ViscHeatFac), OhmLossFac=float(rf.OhmLossFac),
+               r=rs.r)
     for k in ("or1", "or2", "or4", "orho1", "orho2", "beta", "otemp1", "visc", "lambda_",
               "delxr2", "delxh2"):
         cfg[k] = getattr(rf, k)
