@@ -300,11 +300,14 @@ MT_API int mt_radial_apply2(const mt_radial_op* op1, const mt_radial_op* op2, in
  * outputs likewise.  dpdt is written only without the double-curl form (may
  * be null); ddw and dz are read only with it.  Values at the boundary levels
  * are those of the reference (zero before finish_exp, then plus or2 D1 of
- * the auxiliary). */
+ * the auxiliary).  heat (may be NULL): the spectral viscous / Ohmic heating of
+ * the anelastic stage (mt_anel_out heat), added to the entropy's partial term
+ * before finish_exp (step_time.py:1452-1455, get_td.f90:485,499). */
 typedef struct {
   const double *Advr, *Advt, *Advp, *VSr, *VSt, *VxBr, *VxBt, *VxBp, *VXir, *VXit;
   const double *w, *dw, *ddw, *z, *dz;
   int64_t ld;
+  const double* heat;
 } mt_td_in;
 
 typedef struct {
@@ -374,6 +377,35 @@ typedef struct {
 MT_API int mt_update_field(const mt_plan* plan, int n_r, const mt_field_update* u,
                            const mt_lop* solve, const mt_radial_op* D1,
                            const mt_radial_op* D2, void* stream);
+
+/* ---- angular-momentum corrections of the toroidal velocity ---------------
+ * With stress-free boundaries the reference removes, after each toroidal
+ * solve, the outer core's axial (l_correct_AMz) and equatorial
+ * (l_correct_AMe) angular momentum (magic_torch/update_z.py:446-475, with
+ * get_angular_moment :301-331 and the constants of pre_calculations.py:
+ * 60-101).  For the row (l, m) = (1, 0):
+ *   AM_z = 8/3 pi y10 sum_r rint r^2 Re z,  y10 = sqrt(3/pi)/2,
+ *   c = (AM_z - am_start) / (c_moi_oc y10);
+ * then for (1, 1) (when the plan holds m = 1), from the corrected state:
+ *   AM_x = 16/3 pi y11 sum_r rint r^2 Re z,  AM_y = -16/3 pi y11 sum_r rint r^2 Im z,
+ *   c = (AM_x - i AM_y) / (2 y11 c_moi_oc),  y11 = sqrt(1.5/pi)/2;
+ * each correction subtracts c am_z from z, c am_dz from dz and c am_d2z from
+ * d2z (when stored), and the same linear change from the old and implicit
+ * terms that mt_update_field wrote with the coefficients of u (so the result
+ * equals recomputing them from the corrected fields).  u: the toroidal
+ * velocity's mt_field_update of this step, already applied. */
+typedef struct {
+  const double* rint;                   /* (n_r) weights of the radial integral */
+  const double* r;                      /* (n_r) radii */
+  const double *am_z, *am_dz, *am_d2z;  /* (n_r) rho0 r^2, rho0 (2 r + beta r^2),
+                                           rho0 (2 + 4 beta r + (dbeta + beta^2) r^2) */
+  double c_moi_oc;                      /* 8/3 pi sum_r rint r^4 rho0 */
+  double am_start;                      /* axial angular momentum to hold (0: fresh start) */
+  int axial, equatorial;
+} mt_am_correction;
+
+MT_API int mt_correct_am(const mt_plan* plan, int n_r, const mt_field_update* u,
+                         const mt_am_correction* c, void* stream);
 
 /* ---- implicit update of the poloidal velocity, double-curl form ----------
  * One CNAB2 step of magic_torch/update_w_doublecurl.py:393-483 (updateW, the

@@ -79,7 +79,8 @@ class AnelStageParams(C.Structure):
 
 class TdIn(C.Structure):
     _fields_ = [(n, _dp) for n in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp",
-                                   "VXir", "VXit", "w", "dw", "ddw", "z", "dz")] + [("ld", _i64)]
+                                   "VXir", "VXit", "w", "dw", "ddw", "z", "dz")] + [("ld", _i64),
+                                                                                   ("heat", _dp)]
 
 
 class TdOut(C.Structure):
@@ -100,6 +101,12 @@ class FieldUpdate(C.Structure):
                [(n, C.c_double) for n in ("w_old", "w_impl", "w_expl0", "w_expl1")] + \
                [(n, _dp) for n in ("so_l", "so_r", "ia_l", "ia_r", "ib_r", "ic_r", "ic_l",
                                    "ic_r2")]
+
+
+class AmCorrection(C.Structure):
+    _fields_ = [(n, _dp) for n in ("rint", "r", "am_z", "am_dz", "am_d2z")] + \
+               [(n, C.c_double) for n in ("c_moi_oc", "am_start")] + \
+               [(n, C.c_int) for n in ("axial", "equatorial")]
 
 
 class PoloidalUpdate(C.Structure):
@@ -180,6 +187,8 @@ _PROTOS = {
     "mt_lop_destroy": (C.c_int, [C.c_void_p]),
     "mt_update_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FieldUpdate), C.c_void_p,
                                   C.c_void_p, C.c_void_p, _dp]),
+    "mt_correct_am": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FieldUpdate),
+                                C.POINTER(AmCorrection), _dp]),
     "mt_update_poloidal": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PoloidalUpdate), C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "mt_update_wp": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(WpUpdate), C.c_void_p,

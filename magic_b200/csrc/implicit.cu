@@ -254,9 +254,9 @@ __device__ __forceinline__ void band_solve_rows(const BandView& b, int l, int n_
     const int row = t >> 1, part = t & 1;
     double* x = reinterpret_cast<double*>(f + row * fs) + part;  // level k at x[2 k]
     const int kl = b.kl, ku = b.ku, m = kl + ku + 1;
-    const double* abd = b.abd + (int64_t)l * (2 * kl + ku + 1) * n_r;  // abd[i n_r + j]
-    const int* piv = b.piv + (int64_t)l * n_r;
-    const double* fr = b.fr + (int64_t)l * n_r;
+    const double* abd = b.abd;  // degree l's factors (stage_band), abd[i n_r + j]
+    const int* piv = b.piv;
+    const double* fr = b.fr;
     for (int k = 0; k < n_r; ++k) x[2 * k] = __dmul_rn(fr[k], x[2 * k]);
     for (int k = 1; k <= n_r - 1 && kl != 0; ++k) {  // L y = P (fr rhs), 1-based k
       const int lm = min(kl, n_r - k), lp = piv[k - 1];
@@ -278,14 +278,38 @@ __device__ __forceinline__ void band_solve_rows(const BandView& b, int l, int n_
         x[2 * (lb - 1 + i)] =
             __dadd_rn(x[2 * (lb - 1 + i)], __dmul_rn(tv, abd[(la - 1 + i) * n_r + (k - 1)]));
     }
-    if (b.fc) {
-      const double* fc = b.fc + (int64_t)l * n_r;
-      for (int k = 0; k < n_r; ++k) x[2 * k] = __dmul_rn(fc[k], x[2 * k]);
-    }
+    if (b.fc)
+      for (int k = 0; k < n_r; ++k) x[2 * k] = __dmul_rn(b.fc[k], x[2 * k]);
     if (part == 1 && mc0 + row == 0)
       for (int k = 0; k < n_r; ++k) x[2 * k] = 0.0;
   }
   __syncthreads();
+}
+
+// Shared-memory bytes of one degree's band factors: abd ((2 kl + ku + 1) x n_r),
+// fr and fc (n_r each), piv (n_r ints), 16-byte aligned.
+__host__ __device__ inline size_t band_smem_bytes(int kl, int ku, int n_r) {
+  const size_t d = (size_t)(2 * kl + ku + 1 + 2) * n_r * sizeof(double);
+  return (d + (size_t)n_r * sizeof(int) + 15) / 16 * 16;
+}
+
+// Copy degree l's band factors into shared memory (all threads; the caller
+// synchronises before the solve reads them) and return a view of the copy,
+// so that the sequential solve reads shared memory instead of global memory.
+__device__ __forceinline__ BandView stage_band(const BandView& b, int l, int n_r, double* sm) {
+  const int nb = (2 * b.kl + b.ku + 1) * n_r;
+  double* abd = sm;
+  double* fr = abd + nb;
+  double* fc = fr + n_r;
+  int* piv = reinterpret_cast<int*>(fc + n_r);
+  const double* gabd = b.abd + (int64_t)l * nb;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) abd[i] = gabd[i];
+  for (int i = threadIdx.x; i < n_r; i += blockDim.x) {
+    fr[i] = b.fr[(int64_t)l * n_r + i];
+    if (b.fc) fc[i] = b.fc[(int64_t)l * n_r + i];
+    piv[i] = b.piv[(int64_t)l * n_r + i];
+  }
+  return BandView{abd, piv, fr, b.fc ? fc : nullptr, b.kl, b.ku};
 }
 
 // the solved rows (band form) from shared memory to the field's global array
@@ -453,6 +477,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
   const double* Ml = band ? nullptr : a.mt + (int64_t)l * n_r * ldm;
   if constexpr (kStaged)
     if (!band) stage_chunk(Ml, n_r, ldm, 0, mbuf);
+  const BandView bv = band ? stage_band(a.band, l, n_r, mbuf) : a.band;
   if (threadIdx.x < rows)
     lm_row[threadIdx.x] = threadIdx.x < nrow
         ? a.lstart[mc0 + threadIdx.x] + (l - (mc0 + threadIdx.x) * a.minc) : 0;
@@ -461,7 +486,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
   if (band) {
-    band_solve_rows(a.band, l, n_r, fs, f, nrow, mc0);
+    band_solve_rows(bv, l, n_r, fs, f, nrow, mc0);
     store_rows(f, fs, n_r, nrow, lm_row, a.x, a.ld);
   } else {
     solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.x, a.ld,
@@ -529,6 +554,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
   const double* Ml = band ? nullptr : a.mt + (int64_t)l * n_r * ldm;
   if constexpr (kStaged)
     if (!band) stage_chunk(Ml, n_r, ldm, 0, mbuf);
+  const BandView bv = band ? stage_band(a.band, l, n_r, mbuf) : a.band;
   const double2 zero = {0.0, 0.0};
   const double dL = (double)l * (l + 1.0);
   if (threadIdx.x < rows)
@@ -540,7 +566,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
   if (band) {
-    band_solve_rows(a.band, l, n_r, fs, f, nrow, mc0);
+    band_solve_rows(bv, l, n_r, fs, f, nrow, mc0);
     store_rows(f, fs, n_r, nrow, lm_row, a.w, a.ld);
   } else {
     solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.w, a.ld,
@@ -637,7 +663,8 @@ struct TileLaunch {
   int threads;
   size_t smem;
 };
-TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers) {
+TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers,
+                       size_t band_bytes) {
   TileLaunch t;
   t.staged = n_r <= kStagedMaxR;
   const int n_jp = (n_r + 1) / 2;
@@ -650,8 +677,10 @@ TileLaunch tile_launch(int n_r, int ldm, int l_max, int n_m, int row_buffers) {
   t.fs = t.staged ? n_r + ((4 - n_r) & 7) : n_r;
   const int nt_n = (n_r + 7) / 8, nwarp = t.threads / 32;
   t.nt = nt_n <= 2 * nwarp ? 2 : 4;
+  // after the row buffers: the staged solve-matrix chunks, or a degree's band
+  // factors (band_bytes, nonzero on the banded path)
   t.smem = (size_t)row_buffers * rows * t.fs * sizeof(double2) +
-           (t.staged ? (size_t)2 * kKc * ldm * sizeof(double) : 0);
+           (band_bytes ? band_bytes : t.staged ? (size_t)2 * kKc * ldm * sizeof(double) : 0);
   return t;
 }
 
@@ -894,6 +923,95 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
   }
 }
 
+// Angular-momentum corrections after the toroidal update (update_z.py:446-475).
+struct AmArgs {
+  int n_r;
+  int lm10, lm11;          // rows of (l, m) = (1, 0) and (1, 1); lm11 < 0: no m = 1
+  double2 *x, *dx, *d2x, *old, *impl;
+  int64_t ld;
+  const double *so_l, *so_r, *ia_l, *ia_r, *ib_r, *ic_r, *ic_l, *ic_r2;
+  const double *rint, *r, *am_z, *am_dz, *am_d2z;
+  double c_moi_oc, am_start;
+  int axial, equatorial;
+};
+
+constexpr int kAmThreads = 256;
+
+// sum over the block of (a, b); every thread gets the totals
+__device__ __forceinline__ double2 am_block_sum(double a, double b, double2* red) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = double2{a, b};
+  __syncthreads();
+  double2 t{0.0, 0.0};
+  for (int w = 0; w < kAmThreads / 32; ++w) {
+    t.x += red[w].x;
+    t.y += red[w].y;
+  }
+  return t;
+}
+
+// subtract corr * (am_z, am_dz, am_d2z) from row lm of x, dx, d2x and the
+// matching change from its old and implicit terms (degree l = 1)
+__device__ void am_apply(const AmArgs& a, int lm, double2 corr) {
+  const double so_l = a.so_l ? a.so_l[1] : 1.0;
+  const double ia_l = a.ia_l[1], ic_l = a.ic_l[1];
+  for (int j = threadIdx.x; j < a.n_r; j += kAmThreads) {
+    const int64_t o = (int64_t)lm * a.ld + j;
+    const double pz = a.am_z[j], pd = a.am_dz[j], pdd = a.am_d2z[j];
+    a.x[o].x -= pz * corr.x;
+    a.x[o].y -= pz * corr.y;
+    a.dx[o].x -= pd * corr.x;
+    a.dx[o].y -= pd * corr.y;
+    if (a.d2x) {
+      a.d2x[o].x -= pdd * corr.x;
+      a.d2x[o].y -= pdd * corr.y;
+    }
+    const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
+    const double ic = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
+    const double im = ia_l * a.ia_r[j] * (pdd + a.ib_r[j] * pd - ic * pz);
+    a.old[o].x -= so * pz * corr.x;
+    a.old[o].y -= so * pz * corr.y;
+    a.impl[o].x -= im * corr.x;
+    a.impl[o].y -= im * corr.y;
+  }
+}
+
+// one CTA: the axial correction of (1, 0), then the equatorial one of (1, 1)
+__global__ void __launch_bounds__(kAmThreads) k_correct_am(AmArgs a) {
+  __shared__ double2 red[kAmThreads / 32];
+  const double pi = 3.14159265358979323846;
+  const double fac = 8.0 / 3.0 * pi;                 // update_z.py:322
+  const double y10 = 0.5 * sqrt(3.0 / pi);           // pre_calculations.py:63
+  const double y11 = 0.5 * sqrt(1.5 / pi);           // pre_calculations.py:92
+  if (a.axial) {
+    double s = 0.0;
+    for (int j = threadIdx.x; j < a.n_r; j += kAmThreads)
+      s += a.rint[j] * a.r[j] * a.r[j] * a.x[(int64_t)a.lm10 * a.ld + j].x;
+    const double tot = am_block_sum(s, 0.0, red).x;
+    const double am_z = fac * y10 * tot;
+    am_apply(a, a.lm10, double2{(am_z - a.am_start) / (a.c_moi_oc * y10), 0.0});
+  }
+  if (a.equatorial && a.lm11 >= 0) {
+    __syncthreads();
+    double sr = 0.0, si = 0.0;
+    for (int j = threadIdx.x; j < a.n_r; j += kAmThreads) {
+      const double w = a.rint[j] * a.r[j] * a.r[j];
+      const double2 z = a.x[(int64_t)a.lm11 * a.ld + j];
+      sr += w * z.x;
+      si += w * z.y;
+    }
+    const double2 tot = am_block_sum(sr, si, red);
+    const double am_x = 2.0 * fac * y11 * tot.x, am_y = -2.0 * fac * y11 * tot.y;
+    const double den = 2.0 * y11 * a.c_moi_oc;
+    am_apply(a, a.lm11, double2{am_x / den, -am_y / den});
+  }
+}
+
 int check_lop(const mt_lop* op) {
   MT_REQUIRE(op && (op->mt || op->abd), MT_ERR_ARG, "null per-degree operator");
   int dev = -1;
@@ -1106,7 +1224,8 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku};
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
-  const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1);
+  const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1,
+                                   solve->abd ? band_smem_bytes(solve->kl, solve->ku, n_r) : 0);
   MT_REQUIRE(!t.staged || (n_r + 7) / 8 <= t.nt * (t.threads / 32), MT_ERR_ARG,
              "tile shape does not cover n_r");
   a.groups = t.groups;
@@ -1115,6 +1234,38 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
                         : (t.nt == 2 ? k_update_field<true, 2> : k_update_field<true, 4>);
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   kern<<<t.grid, t.threads, t.smem, (cudaStream_t)stream>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int mt_correct_am(const mt_plan* p, int n_r, const mt_field_update* u, const mt_am_correction* c,
+                  void* stream) {
+  MT_REQUIRE(p && u && c, MT_ERR_ARG, "null argument");
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev == p->device, MT_ERR_ARG, "plan used on a different device than it was built on");
+  MT_REQUIRE(p->l_max >= 1 && n_r >= 3 && u->ld >= n_r, MT_ERR_ARG, "bad size or stride");
+  MT_REQUIRE(u->x && u->dx && u->old && u->impl && u->ia_l && u->ia_r && u->ib_r && u->ic_l &&
+                 u->ic_r2,
+             MT_ERR_ARG, "null field, time array or coefficient");
+  MT_REQUIRE(c->rint && c->r && c->am_z && c->am_dz && c->am_d2z && c->c_moi_oc != 0.0,
+             MT_ERR_ARG, "null radial profile or zero moment of inertia");
+  if (!c->axial && !c->equatorial) return MT_OK;
+  AmArgs a{};
+  a.n_r = n_r;
+  a.lm10 = 1;                                   // m = 0 block, l = 1
+  a.lm11 = p->minc == 1 ? p->l_max + 1 : -1;    // m = 1 block starts after l = 0..l_max
+  auto d = [](double* x) { return (double2*)x; };
+  a.x = d(u->x); a.dx = d(u->dx); a.d2x = d(u->d2x); a.old = d(u->old); a.impl = d(u->impl);
+  a.ld = u->ld;
+  a.so_l = u->so_l; a.so_r = u->so_r; a.ia_l = u->ia_l; a.ia_r = u->ia_r; a.ib_r = u->ib_r;
+  a.ic_r = u->ic_r; a.ic_l = u->ic_l; a.ic_r2 = u->ic_r2;
+  a.rint = c->rint; a.r = c->r; a.am_z = c->am_z; a.am_dz = c->am_dz; a.am_d2z = c->am_d2z;
+  a.c_moi_oc = c->c_moi_oc;
+  a.am_start = c->am_start;
+  a.axial = c->axial != 0;
+  a.equatorial = c->equatorial != 0;
+  k_correct_am<<<1, kAmThreads, 0, (cudaStream_t)stream>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }
@@ -1163,7 +1314,8 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);
-  const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 2);
+  const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 2,
+                                   solve->abd ? band_smem_bytes(solve->kl, solve->ku, n_r) : 0);
   MT_REQUIRE(!t.staged || (n_r + 7) / 8 <= t.nt * (t.threads / 32), MT_ERR_ARG,
              "tile shape does not cover n_r");
   a.groups = t.groups;

@@ -71,6 +71,7 @@ struct TdArgs {
   const int* lstart;
   const double2 *Advr, *Advt, *Advp, *VSr, *VSt, *VxBr, *VxBt, *VxBp, *VXir, *VXit;
   const double2 *w, *dw, *ddw, *z, *dz;
+  const double2* heatTerms;  // anelastic viscous / Ohmic heating, or null
   int64_t ld_in;
   double2 *dwdt, *dzdt, *dpdt, *dsdt, *dxidt, *dbdt, *djdt;
   int64_t ld_out;
@@ -182,7 +183,9 @@ __global__ void __launch_bounds__(kTdThreads, 4) k_get_td(TdArgs a) {
       }
     }
     if (a.heat) {
-      a.dsdt[o] = bnd ? double2{0.0, 0.0} : c_scale(dLh, a.VSt[row]);
+      double2 ds = c_scale(dLh, a.VSt[row]);
+      if (a.heatTerms) ds = c_add(ds, a.heatTerms[row]);  // step_time.py:1452-1455
+      a.dsdt[o] = bnd ? double2{0.0, 0.0} : ds;
       xVS[e] = bnd ? double2{0.0, 0.0} : a.VSr[row];
     }
     if (a.chem) {
@@ -400,6 +403,7 @@ int mt_get_td(const mt_plan* p, int n_r, const mt_td_in* in, const mt_td_out* ou
   a.VxBr = c(in->VxBr); a.VxBt = c(in->VxBt); a.VxBp = c(in->VxBp);
   a.VXir = c(in->VXir); a.VXit = c(in->VXit);
   a.w = c(in->w); a.dw = c(in->dw); a.ddw = c(in->ddw); a.z = c(in->z); a.dz = c(in->dz);
+  a.heatTerms = q->l_heat ? c(in->heat) : nullptr;
   a.ld_in = in->ld;
   auto d = [](double* x) { return (double2*)x; };
   a.dwdt = d(out->dwdt); a.dzdt = d(out->dzdt); a.dpdt = d(out->dpdt); a.dsdt = d(out->dsdt);

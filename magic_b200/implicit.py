@@ -10,6 +10,7 @@ explicit history itself (expl1 <- expl0) and stores the new field as ``old``.
 """
 
 import ctypes as C
+import math
 
 import numpy as np
 import torch
@@ -489,6 +490,41 @@ def update_field(plan, sch, lop, x, dx, ta, weights, coef, top=None, bot=None, d
                          *[dev[k].data_ptr() if dev[k] is not None else None for k in names])
     st = C.c_void_p(torch.cuda.current_stream(x.device).cuda_stream)
     check(_lib.lib().mt_update_field(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h, st))
+
+
+def am_profiles(r, rho0, beta, dbeta, rint):
+    """Profiles of the angular-momentum corrections (magic_torch/update_z.py:57-64):
+    am_z = rho0 r^2, am_dz = rho0 (2 r + r^2 beta), am_d2z = rho0 (2 + 4 beta r
+    + (dbeta + beta^2) r^2), and the outer core's moment of inertia c_moi_oc =
+    8/3 pi int r^4 rho0 dr (pre_calculations.py:94-98) with the radial rule rint."""
+    r, rho0, beta, dbeta, rint = (np.asarray(x, dtype=np.float64)
+                                  for x in (r, rho0, beta, dbeta, rint))
+    r2 = r * r
+    return dict(am_z=rho0 * r2, am_dz=rho0 * (2.0 * r + r2 * beta),
+                am_d2z=rho0 * (2.0 + 4.0 * beta * r + dbeta * r2 + beta * beta * r2),
+                c_moi_oc=8.0 / 3.0 * math.pi * float(np.dot(rint, r2 * r2 * rho0)))
+
+
+def correct_am(plan, z, dz, ta, coef, am, d2z=None):
+    """The angular-momentum corrections after the toroidal update (mt_correct_am,
+    magic_torch/update_z.py:446-475): z, dz (d2z) and the old / implicit terms in
+    ta of the rows (l, m) = (1, 0) and (1, 1), in place.  coef: the toroidal
+    coefficients the update used; am: device profiles rint, r, am_z, am_dz, am_d2z
+    (am_profiles) and c_moi_oc, am_start, axial, equatorial."""
+    n_r = z.shape[1]
+    names = ("so_l", "so_r", "ia_l", "ia_r", "ib_r", "ic_r", "ic_l", "ic_r2")
+    ptr = lambda x: x.data_ptr() if x is not None else None
+    for a in (z, dz, ta["old"], ta["impl"]):
+        if a.shape != z.shape or a.dtype != torch.complex128 or not a.is_contiguous():
+            raise ValueError("fields and time arrays must be contiguous (lm_max, n_r) complex128")
+    u = _lib.FieldUpdate(z.data_ptr(), dz.data_ptr(), ptr(d2z), ta["old"].data_ptr(),
+                         ta["impl"].data_ptr(), None, None, None, None, n_r, 0.0, 0.0, 0.0, 0.0,
+                         *[ptr(coef.get(k)) for k in names])
+    c = _lib.AmCorrection(*[am[k].data_ptr() for k in ("rint", "r", "am_z", "am_dz", "am_d2z")],
+                          float(am["c_moi_oc"]), float(am["am_start"]), int(am["axial"]),
+                          int(am["equatorial"]))
+    st = C.c_void_p(torch.cuda.current_stream(z.device).cuda_stream)
+    check(_lib.lib().mt_correct_am(plan._h, n_r, C.byref(u), C.byref(c), st))
 
 
 def update_scalar(plan, sch, lop, s, ds, ta, weights, opr, hdif, kappa, d1c, or2, top=None,

@@ -405,7 +405,8 @@ class Plan:
 
         ``ins``: dict of (lm_max, n_r) complex128 arrays Advr, Advt, Advp, w, dw, z (plus
         ddw, dz for the double-curl form; VSr, VSt if l_heat; VxBr, VxBt, VxBp if l_mag;
-        VXir, VXit if l_chem).  ``prof``: r, or1, or2, or4, orho1, beta over n_r.
+        VXir, VXit if l_chem; optionally heat, the anelastic stage's spectral heating,
+        added to the entropy term).  ``prof``: r, or1, or2, or4, orho1, beta over n_r.
         ``D1``: the first-derivative RadialOp.  Returns a dict dwdt, dzdt (+ dpdt without
         the double-curl form, dsdt, dxidt, dbdt, djdt as enabled)."""
         n_r = ins["w"].shape[1]
@@ -414,6 +415,7 @@ class Plan:
         need += ["VSr", "VSt"] if l_heat else []
         need += ["VxBr", "VxBt", "VxBp"] if l_mag else []
         need += ["VXir", "VXit"] if l_chem else []
+        need += ["heat"] if l_heat and ins.get("heat") is not None else []
         src = {}
         for k in need:
             x = ins[k]
@@ -429,7 +431,8 @@ class Plan:
         keep = {k: self._prof(prof[k], n_r) for k in ("r", "or1", "or2", "or4", "orho1", "beta")}
         ti = _lib.TdIn(*[src[k].data_ptr() if k in src else None for k in
                          ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt", "VxBp", "VXir",
-                          "VXit", "w", "dw", "ddw", "z", "dz")], n_r)
+                          "VXit", "w", "dw", "ddw", "z", "dz")], n_r,
+                        src["heat"].data_ptr() if "heat" in src else None)
         to = _lib.TdOut(*[out[k].data_ptr() if k in out else None for k in
                           ("dwdt", "dzdt", "dpdt", "dsdt", "dxidt", "dbdt", "djdt")],
                         out["dwdt"].stride(0))

@@ -51,6 +51,10 @@ def dt_courant(dt, dt_max, dt_min):
 
 
 class BoussinesqStep:
+    l_mag = True        # magnetic field on (subclasses may turn it off)
+    l_anel = False      # anelastic background and terms
+    am = None           # angular-momentum corrections of z (AnelasticStep)
+
     def __init__(self, l_max, n_r, ek=1e-5, ra=3e8, pr=1.0, prmag=1.0, dt=2e-7,
                  precision="split", radratio=0.35, fd_order=4, fd_order_bound=2, ktopv=2,
                  kbotv=2, device=None, cache=None, minc=1, radial_scheme="FD"):
@@ -68,7 +72,8 @@ class BoussinesqStep:
         dev = self.device
         self._cache = cache if cache is not None else {}
         self.std_form = radial_scheme.upper() != "FD"
-        self._shape = (n_r, radial_scheme.upper(), radratio, fd_order, fd_order_bound, str(dev))
+        self._shape = (n_r, radial_scheme.upper(), radratio, fd_order, fd_order_bound, str(dev)) \
+            + self._background_key()
         self.plan = self._shared(("plan", l_max, minc, precision, str(dev)),
                                  lambda: Plan(l_max, minc, precision=precision, device=dev))
         self.sch = self._shared(("sch",) + self._shape,
@@ -89,8 +94,9 @@ class BoussinesqStep:
         hp = dict(r=r, or1=1.0 / r, or2=1.0 / r ** 2, or4=1.0 / r ** 4, orho1=ones,
                   orho2=ones, beta=zeros, dbeta=zeros, ddbeta=zeros, visc=ones, dLvisc=zeros,
                   ddLvisc=zeros, kappa=ones, dLkappa=zeros, dLtemp0=zeros, lambda_=ones,
-                  dLlambda=zeros, rgrav=r / r_cmb, rho0=ones, delxr2=delxr2,
+                  dLlambda=zeros, rgrav=r / r_cmb, rho0=ones, otemp1=ones, delxr2=delxr2,
                   delxh2=r ** 2 / float(l_max * (l_max + 1)))
+        hp.update(self._background(r, radratio, ek=ek, ra=ra, pr=pr, prmag=prmag))
         self.hprof = hp
         t = lambda x: torch.as_tensor(np.asarray(x, dtype=np.float64), device=dev).contiguous()
         self.prof = {k: t(v) for k, v in hp.items()}
@@ -111,9 +117,10 @@ class BoussinesqStep:
                          z=dev_coef(I.toroidal_coefficients(l_max, hdif, hp["visc"], hp["beta"],
                                                             hp["dbeta"], hp["dLvisc"], hp["or1"],
                                                             hp["or2"])))
-        cb, cj = I.magnetic_coefficients(l_max, self.opm, hdif, hp["lambda_"], hp["dLlambda"],
-                                         hp["or2"])
-        self.coef["b"], self.coef["j"] = dev_coef(cb), dev_coef(cj)
+        if self.l_mag:
+            cb, cj = I.magnetic_coefficients(l_max, self.opm, hdif, hp["lambda_"],
+                                             hp["dLlambda"], hp["or2"])
+            self.coef["b"], self.coef["j"] = dev_coef(cb), dev_coef(cj)
         self.wprof = {k: self.prof[k] for k in ("or1", "or2", "beta", "dbeta", "ddbeta", "visc",
                                                 "dLvisc", "ddLvisc", "orho1", "rgrav", "rho0")}
         self.wcoef = tuple(t(c) for c in I._w_coefficient_profiles(hp))
@@ -121,12 +128,14 @@ class BoussinesqStep:
                                                  "rgrav", "rho0")}
         # state: fields, their derivatives and the time arrays of each equation
         z = lambda: torch.zeros(self.lm_max, n_r, dtype=_CD, device=dev)
-        self.f = {k: z() for k in ("w", "dw", "ddw", "z", "dz", "s", "ds", "b", "db", "ddb", "aj",
-                                   "dj", "ddj", "p") + (("dp",) if self.std_form else ())}
+        mag = self.l_mag
+        self.f = {k: z() for k in ("w", "dw", "ddw", "z", "dz", "s", "ds", "p")
+                  + (("b", "db", "ddb", "aj", "dj", "ddj") if mag else ())
+                  + (("dp",) if self.std_form else ())}
         self.ta = {e: {k: z() for k in ("old", "impl", "expl0", "expl1")}
-                   for e in ("s", "z", "w", "b", "j") + (("p",) if self.std_form else ())}
-        self.nl_out = {k: z() for k in ("Advr", "Advt", "Advp", "VSr", "VSt", "VxBr", "VxBt",
-                                        "VxBp")}
+                   for e in ("s", "z", "w") + (("b", "j") if mag else ())
+                   + (("p",) if self.std_form else ())}
+        self.nl_out = {k: z() for k in self.stage_outputs()}
         self._work = None  # the stage workspace, allocated at the first own stage
         self.bots = torch.zeros(self.lm_max, dtype=_CD, device=dev)
         self.bots[0] = math.sqrt(4.0 * math.pi)  # fixed entropy at the inner boundary, l = m = 0
@@ -146,6 +155,18 @@ class BoussinesqStep:
         self.ops = self._shared(key, lambda: self._build_ops(wl0))
         self._ops_wl0 = wl0
 
+    def _background_key(self):
+        """Parameters of the radial background beyond the grid (cache key part)."""
+        return ()
+
+    def _background(self, r, radratio, **phys):
+        """Radial profiles replacing the Boussinesq ones (none here)."""
+        return {}
+
+    def stage_outputs(self):
+        """Spectral outputs of this step's nonlinear stage."""
+        return self.STAGE_OUTPUTS
+
     def _shared(self, key, build):
         if key not in self._cache:
             self._cache[key] = build()
@@ -163,9 +184,11 @@ class BoussinesqStep:
                                          self._kbotv) if self.std_form else
                     I.poloidal_dc_solve_operators(self.sch, l_max, wl0, hdif, hp, self._ktopv,
                                                   self._kbotv), device=dev))
-        Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif, hp["lambda_"],
-                                            hp["dLlambda"], hp["or1"], hp["or2"])
-        ops["b"], ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
+        if self.l_mag:
+            Mb, Mj = I.magnetic_solve_operators(self.sch, l_max, wl0, self.opm, hdif,
+                                                hp["lambda_"], hp["dLlambda"], hp["or1"],
+                                                hp["or2"])
+            ops["b"], ops["j"] = I.LOp(Mb, device=dev), I.LOp(Mj, device=dev)
         return ops
 
     def energies(self):
@@ -178,8 +201,10 @@ class BoussinesqStep:
             self._energy = EnergyIntegrals(self.plan, hp["r"], hp["or2"], hp["orho1"],
                                            self.sch.rint, self.LFfac)
         f = self.f
-        return self._energy.kin(f["w"], f["dw"], f["z"]), self._energy.mag(f["b"], f["db"],
-                                                                           f["aj"])
+        kin = self._energy.kin(f["w"], f["dw"], f["z"])
+        if not self.l_mag:
+            return kin, np.zeros(12)
+        return kin, self._energy.mag(f["b"], f["db"], f["aj"])
 
     def init_random(self, seed=0, amp=1e-4):
         """Seeded random fields |c_lm| ~ amp (l+1)^-2 on the interior levels (m = 0
@@ -194,6 +219,8 @@ class BoussinesqStep:
         m0 = torch.as_tensor(self.plan.lm2m == 0)
         for k in ("w", "z", "s", "b", "aj"):
             c = torch.randn(self.lm_max, self.n_r, dtype=_CD, generator=g) * amp
+            if k not in self.f:
+                continue
             c *= ((l + 1.0) ** -2)[:, None]
             c[m0] = c[m0].real.to(_CD)
             c[:, 0] = 0.0
@@ -203,6 +230,8 @@ class BoussinesqStep:
         second = {}
         for k, d1, d2 in (("w", "dw", "ddw"), ("z", "dz", None), ("s", "ds", None),
                           ("b", "db", "ddb"), ("aj", "dj", "ddj")):
+            if k not in f:
+                continue
             a1, a2 = get_ddr(f[k], D1, D2)
             f[d1].copy_(a1)
             second[k] = a2
@@ -225,8 +254,9 @@ class BoussinesqStep:
 
         generic("s", f["s"], f["ds"], second["s"])
         generic("z", f["z"], f["dz"], second["z"])
-        generic("b", f["b"], f["db"], second["b"])
-        generic("j", f["aj"], f["dj"], second["aj"])
+        if self.l_mag:
+            generic("b", f["b"], f["db"], second["b"])
+            generic("j", f["aj"], f["dj"], second["aj"])
         if self.std_form:
             self._init_wp_terms(dL, hd)
             return
@@ -314,12 +344,14 @@ class BoussinesqStep:
         f = self.f
         ins = dict(self.nl_out, w=f["w"], dw=f["dw"], ddw=f["ddw"], z=f["z"], dz=f["dz"])
         td_out = dict(dwdt=self.ta["w"]["expl0"], dzdt=self.ta["z"]["expl0"],
-                      dsdt=self.ta["s"]["expl0"], dbdt=self.ta["b"]["expl0"],
-                      djdt=self.ta["j"]["expl0"])
+                      dsdt=self.ta["s"]["expl0"])
+        if self.l_mag:
+            td_out.update(dbdt=self.ta["b"]["expl0"], djdt=self.ta["j"]["expl0"])
         if self.std_form:
             td_out["dpdt"] = self.ta["p"]["expl0"]
         self.plan.get_td(ins, self.prof, self.CorFac, self.sch.D1,
-                         l_double_curl=not self.std_form, l_heat=True, l_mag=True, out=td_out)
+                         l_double_curl=not self.std_form, l_heat=True, l_mag=self.l_mag,
+                         l_anel=self.l_anel, out=td_out)
 
     def lm_loop(self):
         """Implicit solves S, Z, W, B (step_time.py:1478-1527)."""
@@ -328,6 +360,8 @@ class BoussinesqStep:
                        self.coef["s"], bot=self.bots)
         I.update_field(self.plan, self.sch, self.ops["z"], f["z"], f["dz"], ta["z"], w,
                        self.coef["z"])
+        if self.am is not None:
+            I.correct_am(self.plan, f["z"], f["dz"], ta["z"], self.coef["z"], self.am)
         if self.std_form:
             I.update_wp(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"], f["ddw"],
                         f["p"], f["dp"], ta["w"], ta["p"], w, f["s"], self.wpprof, self.hdif,
@@ -336,6 +370,8 @@ class BoussinesqStep:
             I.update_poloidal_dc(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"],
                                  f["ddw"], f["p"], ta["w"], w, f["s"], self.wprof, self.hdif,
                                  self.BuoFac, wcoef=self.wcoef)
+        if not self.l_mag:
+            return
         I.update_field(self.plan, self.sch, self.ops["b"], f["b"], f["db"], ta["b"], w,
                        self.coef["b"], d2x=f["ddb"])
         I.update_field(self.plan, self.sch, self.ops["j"], f["aj"], f["dj"], ta["j"], w,
@@ -358,4 +394,90 @@ class BoussinesqStep:
             _, dt_new = self.courant_dt(dtr, dth)
             self.set_dt(dt_new, self.dt[0])
         self.lm_loop()
+        return dtr, dth
+
+
+class AnelasticStep(BoussinesqStep):
+    """One CNAB2 step of anelastic convection on the GPU: the reference's one_step
+    (magic_torch/step_time.py:1574-1640) with radial_loop_anel (:1215-1475) and
+    lm_loop (:1478-1527) under l_anel, on the polytropic background of
+    magic_torch/radial_functions.py:70-165 (magic_b200.profiles.polytropic_background).
+
+    radial loop  the anelastic nonlinear stage (Plan.nl_anel: the 18-19 grid
+                 fields of the non-curl advection, get_nl_anel with viscous and
+                 Ohmic heating, forward transforms, Courant), then mt_get_td with
+                 the anelastic entropy finish (1/rho0) and the heating added to
+                 the entropy's explicit term (step_time.py:1452-1455);
+    lm loop      entropy (kappa, beta + dLtemp0 + 2/r), toroidal velocity (with
+                 the density and viscosity terms of update_z.py:40-47), then the
+                 angular-momentum corrections of stress-free runs
+                 (update_z.py:446-475, mt_correct_am), the poloidal velocity and
+                 pressure with the anelastic (w, p) operators, magnetic field
+                 when l_mag.
+
+    Defaults are the reference's anelastic benchmark setup (configs/
+    hydro_bench_anel_modal.yaml): 5 density scale heights, polytropic index
+    2, gravity ~ 1/r^2, no magnetic field, stress-free boundaries with both
+    angular-momentum corrections, Chebyshev levels (standard (w, p) form).
+    The reference factorises the anelastic (w, p) matrices with LU
+    (update_wp.py:239-352); this step applies the inverse of the same scaled
+    matrices (the two agree to 2e-14 at 33 levels, 1.7e-11 at 129)."""
+
+    def __init__(self, l_max, n_r, ek=1e-4, ra=3e6, pr=1.0, prmag=5.0, dt=1e-6, strat=5.0,
+                 polind=2.0, g0=0.0, g1=0.0, g2=1.0, l_mag=False, ktopv=1, kbotv=1,
+                 l_correct_AMz=True, l_correct_AMe=True, precision="fp64", radratio=0.35,
+                 radial_scheme="chebyshev", fd_order=4, fd_order_bound=2, device=None,
+                 cache=None, minc=1):
+        self.l_mag = bool(l_mag)
+        self.l_anel = True
+        self._anel = dict(strat=float(strat), polind=float(polind), g0=float(g0),
+                          g1=float(g1), g2=float(g2))
+        super().__init__(l_max, n_r, ek=ek, ra=ra, pr=pr, prmag=prmag, dt=dt,
+                         precision=precision, radratio=radratio, fd_order=fd_order,
+                         fd_order_bound=fd_order_bound, ktopv=ktopv, kbotv=kbotv, device=device,
+                         cache=cache, minc=minc, radial_scheme=radial_scheme)
+        self.ViscHeatFac = float(self._bg["ViscHeatFac"])
+        self.OhmLossFac = float(self._bg["OhmLossFac"])
+        if l_correct_AMz or l_correct_AMe:
+            hp = self.hprof
+            prof = I.am_profiles(hp["r"], hp["rho0"], hp["beta"], hp["dbeta"], self.sch.rint)
+            t = lambda x: torch.as_tensor(np.asarray(x, dtype=np.float64),
+                                          device=self.device).contiguous()
+            self.am = dict({k: t(v) for k, v in prof.items() if k != "c_moi_oc"},
+                           rint=t(self.sch.rint), r=t(hp["r"]), c_moi_oc=prof["c_moi_oc"],
+                           am_start=0.0, axial=bool(l_correct_AMz),
+                           equatorial=bool(l_correct_AMe))
+
+    def _background_key(self):
+        return ("anel",) + tuple(self._anel.values())
+
+    def _background(self, r, radratio, ek, ra, pr, prmag):
+        from .profiles import polytropic_background
+
+        self._bg = polytropic_background(r, radratio, pr=pr, ra=ra, ek=ek, prmag=prmag,
+                                         l_mag=self.l_mag, **self._anel)
+        return {k: self._bg[k] for k in ("rgrav", "rho0", "beta", "dbeta", "ddbeta", "dLtemp0",
+                                         "orho1", "orho2", "otemp1")}
+
+    def stage_outputs(self):
+        return ("Advr", "Advt", "Advp", "VSr", "VSt") + (
+            ("VxBr", "VxBt", "VxBp") if self.l_mag else ()) + ("heat",)
+
+    @property
+    def work(self):
+        """Workspace of the fused (split-precision) anelastic stage; the FP64 and
+        digit-split plans compose the stage from the FP64 kernels and need none."""
+        if self._work is None:
+            n = self.plan.nl_anel_workspace(self.n_r, self.l_mag, False) \
+                if self.plan.precision == "split" else 0
+            self._work = torch.empty(max(int(n), 1), dtype=torch.uint8, device=self.device)
+        return self._work
+
+    def nonlinear_stage(self):
+        f = self.f
+        names = ("w", "dw", "ddw", "z", "dz", "s") + (
+            ("b", "db", "ddb", "aj", "dj") if self.l_mag else ())
+        _, dtr, dth = self.plan.nl_anel({k: f[k] for k in names}, self.prof, self.LFfac,
+                                        self.ViscHeatFac, self.OhmLossFac, 2.5, 1.0, self.opm,
+                                        l_mag=self.l_mag, out=self.nl_out, work=self.work)
         return dtr, dth

@@ -49,6 +49,15 @@ STEP_CONFIGS = {
     "step_fd": {"l_max": 12, "minc": 1, "n_r_max": 13, "radial_scheme": "FD", "fd_order": 4,
                 "fd_order_bound": 2, "ek": 1e-3, "ra": 1e5, "pr": 1.0, "prmag": 5.0,
                 "dtmax": 1e-4, "mode": 0},
+    # anelastic convection without magnetic field (the reference's anelastic
+    # benchmark setup, configs/hydro_bench_anel_modal.yaml, at a small size):
+    # polytropic background with 5 density scale heights, index 2, gravity
+    # ~ 1/r^2, stress-free boundaries with both angular-momentum corrections,
+    # Chebyshev levels, standard (w, p) form
+    "step_anel": {"l_max": 16, "minc": 1, "n_r_max": 17, "strat": 5.0, "polind": 2.0,
+                  "g0": 0.0, "g1": 0.0, "g2": 1.0, "mode": 1, "ek": 1e-3, "ra": 1.48638035e5,
+                  "pr": 1.0, "prmag": 5.0, "ktopv": 1, "kbotv": 1, "l_correct_AMz": True,
+                  "l_correct_AMe": True, "dtmax": 1e-4},
 }
 
 # 500 CNAB2 steps of the Boussinesq MHD dynamo at the sizes of the CPU-runnable
@@ -64,6 +73,14 @@ RUN_CONFIGS = {
     "run_fd_l32m4": ({"l_max": 32, "minc": 4, "n_r_max": 33, "radial_scheme": "FD",
                       "fd_order": 4, "fd_order_bound": 2, "ek": 1e-3, "ra": 1e5, "pr": 1.0,
                       "prmag": 5.0, "dtmax": 1e-4, "mode": 0}, 500, 1e-5),
+    # 100 steps of the anelastic setup of step_anel at l_max 32 on 33 Chebyshev
+    # levels from the benchmark's l = m = 19 entropy mode (init_s1 1919, amplitude
+    # 0.01) plus seeded noise of 1e-3 on the entropy
+    "run_anel_l32": ({"l_max": 32, "minc": 1, "n_r_max": 33, "strat": 5.0, "polind": 2.0,
+                      "g0": 0.0, "g1": 0.0, "g2": 1.0, "mode": 1, "ek": 1e-3,
+                      "ra": 1.48638035e5, "pr": 1.0, "prmag": 5.0, "ktopv": 1, "kbotv": 1,
+                      "l_correct_AMz": True, "l_correct_AMe": True, "init_s1": 1919,
+                      "amp_s1": 0.01, "dtmax": 1e-4}, 100, 1e-3),
 }
 
 # CNAB2 steps with the Courant control of dt (courant.py:130-155; one_step
@@ -460,6 +477,14 @@ def worker_step(name, ref):
                lm2m=n(blocking.st_lm2m))
     rint = rInt_R(torch.eye(N, dtype=torch.float64))
     out["rint_w"] = n(rint)
+    if params.l_anel:
+        # the anelastic background and the angular-momentum constants the step uses
+        from magic_torch import radial_functions as rf, pre_calculations as pc
+        from magic_torch.radial_scheme import r as r_grid
+        out.update(r=n(r_grid), rho0=n(rf.rho0), beta=n(rf.beta), dbeta=n(rf.dbeta),
+                   rgrav=n(rf.rgrav), dLtemp0=n(rf.dLtemp0), otemp1=n(rf.otemp1),
+                   ViscHeatFac=float(rf.ViscHeatFac), c_moi_oc=float(pc.c_moi_oc),
+                   cfg=json.dumps(cfg))
 
     def snapshot(tag, fields_only=None):
         with tempfile.TemporaryDirectory() as d:
@@ -527,6 +552,9 @@ def worker_run(name, ref):
     out = dict(n_r_max=N, l_max=params.l_max, minc=params.minc, lm_max=lm, dt=dt,
                ek=cfg["ek"], ra=cfg["ra"], pr=cfg["pr"], prmag=cfg["prmag"],
                radratio=float(params.radratio), steps=nsteps, noise=noise)
+    if params.l_anel:
+        import json
+        out["cfg"] = json.dumps(cfg)
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "ck.pt")
         save_checkpoint(path, 0, 0.0, {"tag": "golden"})

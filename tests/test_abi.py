@@ -57,7 +57,7 @@ def test_struct_layouts_match_header(libpath, tmp_path):
                "mt_bouss_params": _lib.BoussParams, "mt_anel_in": _lib.AnelIn,
                "mt_anel_out": _lib.AnelOut, "mt_anel_stage_params": _lib.AnelStageParams,
                "mt_td_in": _lib.TdIn, "mt_td_out": _lib.TdOut, "mt_td_params": _lib.TdParams,
-               "mt_field_update": _lib.FieldUpdate,
+               "mt_field_update": _lib.FieldUpdate, "mt_am_correction": _lib.AmCorrection,
                "mt_poloidal_update": _lib.PoloidalUpdate, "mt_level_copy": _lib.LevelCopy}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
              "int main(void){"]

@@ -1,0 +1,137 @@
+"""Whole CNAB2 steps of anelastic convection on the GPU
+(magic_b200.step.AnelasticStep) against the reference's own one_step with
+l_anel: the polytropic background of 5 density scale heights (index 2,
+gravity ~ 1/r^2), no magnetic field, stress-free boundaries with both
+angular-momentum corrections, Chebyshev levels (the reference's anelastic
+benchmark setup, configs/hydro_bench_anel_modal.yaml, at small sizes).
+
+Fixtures (tests/golden/make_golden.py): step_anel.npz, l_max 16 on 17
+levels, the reference's state before and after two steps from its own
+initial state with seeded perturbations of s, w and z (1e-3); and
+run_anel_l32.npz, l_max 32 on 33 levels, the l = m = 19 entropy mode of
+amplitude 0.01 plus seeded entropy noise of 1e-3, the kinetic energies after
+each of 100 steps and the fields after the last."""
+
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("w", "dw", "ddw", "z", "dz", "s", "ds", "p", "dp")
+DT_ARRAYS = {"s": "dsdt", "z": "dzdt", "w": "dwdt", "p": "dpdt"}
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _golden_state(z, tag):
+    st = {k.split(":", 1)[1]: torch.as_tensor(np.ascontiguousarray(z[k]))
+          for k in z if k.startswith(tag + ":") and "." in k.split(":", 1)[1]}
+    st["tscheme_dt"] = torch.as_tensor(z[tag + ":tscheme_dt"])
+    return st
+
+
+def _make(z, precision="fp64"):
+    from magic_b200.state import load_state_dict
+    from magic_b200.step import AnelasticStep
+
+    cfg = json.loads(str(z["cfg"]))
+    st = AnelasticStep(int(z["l_max"]), int(z["n_r_max"]), ek=cfg["ek"], ra=cfg["ra"],
+                       pr=cfg["pr"], prmag=cfg["prmag"], dt=float(z["dt"]), strat=cfg["strat"],
+                       polind=cfg["polind"], g0=cfg["g0"], g1=cfg["g1"], g2=cfg["g2"],
+                       ktopv=cfg["ktopv"], kbotv=cfg["kbotv"],
+                       l_correct_AMz=cfg["l_correct_AMz"], l_correct_AMe=cfg["l_correct_AMe"],
+                       precision=precision, minc=int(z["minc"]))
+    assert st.lm_max == int(z["lm_max"])
+    load_state_dict(st, _golden_state(z, "0"))
+    return st
+
+
+def test_two_anelastic_steps_match_reference():
+    """Every field and time array after two steps, and the kinetic energies.
+    Tolerances relative to each array's largest value: 1e-12 for the fields
+    and the energies, 1e-11 for the radial derivatives and time arrays (D2 and
+    D3 of the new fields)."""
+    z = load_golden("step_anel")
+    st = _make(z)
+    st.step()
+    torch.cuda.synchronize()
+    e1 = {k: _rel(st.f[k].cpu().numpy(), z[f"1:fields.{k}_LMloc"]) for k in ("w", "z", "s")}
+    st.step()
+    torch.cuda.synchronize()
+    errs = {k: _rel(st.f[k].cpu().numpy(), z[f"2:fields.{k}_LMloc"]) for k in FIELDS}
+    for e, name in DT_ARRAYS.items():
+        ta = st.ta[e]
+        errs[name + ".old"] = _rel(ta["old"].cpu().numpy(), z[f"2:dt.{name}.old"][..., 0])
+        errs[name + ".impl"] = _rel(ta["impl"].cpu().numpy(), z[f"2:dt.{name}.impl"][..., 0])
+        errs[name + ".expl0"] = _rel(ta["expl0"].cpu().numpy(), z[f"2:dt.{name}.expl"][..., 0])
+        errs[name + ".expl1"] = _rel(ta["expl1"].cpu().numpy(), z[f"2:dt.{name}.expl"][..., 1])
+    ek, _ = st.energies()
+    errs["e_kin"] = _rel(np.array(ek), z["2:e_kin"])
+    print("step 1", {k: f"{v:.1e}" for k, v in e1.items()})
+    print("step 2", {k: f"{v:.1e}" for k, v in errs.items()})
+    for k, v in e1.items():
+        assert v < 1e-12, ("step 1", k, v)
+    for k, v in errs.items():
+        tol = 1e-12 if k in ("w", "z", "s", "p", "e_kin") else 1e-11
+        assert v < tol, (k, v)
+
+
+def test_angular_momentum_is_removed():
+    """With both corrections on, the outer core's axial and equatorial angular
+    momentum after a step is the start value (zero) to rounding: the integrals
+    of r^2 z over the (1, 0) and (1, 1) rows vanish relative to the integrals
+    of |r^2 z| of those rows."""
+    z = load_golden("step_anel")
+    st = _make(z)
+    st.step()
+    torch.cuda.synchronize()
+    r = torch.as_tensor(st.hprof["r"], device=st.device)
+    w = torch.as_tensor(st.sch.rint, device=st.device) * r * r
+    for row in (1, st.l_max + 1):
+        zz = st.f["z"][row]
+        am = torch.abs((w * zz).sum()).item()
+        ref = (torch.abs(w) * torch.abs(zz)).sum().item()
+        assert am < 1e-13 * max(ref, 1e-300), (row, am, ref)
+
+
+def test_anelastic_run_matches_reference():
+    """100 steps of the l_max 32 case: the kinetic energies of every step and
+    the fields after the last (relative to each array's largest value)."""
+    z = load_golden("run_anel_l32")
+    st = _make(z)
+    ek_t = []
+    for _ in range(int(z["steps"])):
+        st.step()
+        ek_t.append(np.array(st.energies()[0]))
+    ek_t = np.stack(ek_t)
+    ref = z["e_kin"]
+    e_en = float((np.abs(ek_t - ref) / np.abs(ref).max(axis=0, keepdims=True).clip(1e-300)).max())
+    errs = {k: _rel(st.f[k].cpu().numpy(), z[f"{int(z['steps'])}:{k}"]) for k in ("w", "z", "s",
+                                                                                 "p")}
+    print("100 steps", f"energies {e_en:.1e}", {k: f"{v:.1e}" for k, v in errs.items()})
+    assert e_en < 1e-11, e_en
+    for k, v in errs.items():
+        assert v < 1e-11, (k, v)
+
+
+def test_split_stage_tracks_fp64_stage():
+    """The fused split-precision anelastic stage against the FP64 composition
+    over two steps from the reference's state (split per-stage error 4e-7 ...
+    2.2e-5 of scale)."""
+    z = load_golden("step_anel")
+    a, b = _make(z, "fp64"), _make(z, "split")
+    for _ in range(2):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    for k in ("w", "z", "s", "p"):
+        e = ((a.f[k] - b.f[k]).abs().max() / a.f[k].abs().max()).item()
+        print("split vs fp64", k, f"{e:.1e}")
+        assert e < 1e-4, (k, e)

@@ -295,7 +295,9 @@ def test_update_poloidal_vs_oracle(l_max, n_r, scale):
     profiles; and l_max = 16 at 261 levels, the wide tiling (n_r > 256).  GPU
     and oracle both solve the fourth-order double-curl operator with its pivoted
     banded LU factors (the reference's algorithm on these grids), so they agree
-    to 1e-12 (1e-11 for the terms with D2 of the new field) at both sizes;
+    to 1e-12 (1e-11 for the terms with D2 of the new field, and for dx at 261
+    levels, where D1 of the finest spacing amplifies the rounding of x: 7.2e-12
+    measured);
     the dense inverse the GPU applied before differed from the factorised solve
     by 2.6e-12 at 97 levels and 8e-11 at 261 (conditioning ~ n_r^4)."""
     from magic_b200 import Plan
@@ -324,7 +326,8 @@ def test_update_poloidal_vs_oracle(l_max, n_r, scale):
                       sch.D2m, s_new, BuoFac, r, 4, 2, 2)
     for k in ("x", "dx", "d2x", "impl", "old", "expl1", "p0"):
         e = rel_err(npy(o[k]), ref[k])
-        assert e < scale * (TOL_IMPL if k in ("impl", "old", "d2x") else TOL), (k, e)
+        loose = k in ("impl", "old", "d2x") or (k == "dx" and n_r > 256)
+        assert e < scale * (TOL_IMPL if loose else TOL), (k, e)
 
 
 WPPROF = ("or1", "or2", "beta", "dbeta", "visc", "dLvisc", "rgrav", "rho0")

@@ -57,14 +57,23 @@ def test_nl_bouss_matches_oracle(l_max, minc, N, l_mag, l_chem):
     # S and T of one vector field share its scale: T(Adv) cancels ~50x between
     # its two contributions for random fields, so errors are measured against
     # max(|S|, |T|) of the pair (both sides FP64, different summation order).
+    # Tolerance 1e-12 up to l_max 127; 4e-12 on the 384 x 768 and 576 x 1152
+    # grids, where each analysed coefficient sums ~3e5 products of mixed sign
+    # (measured: 1.2e-12 in Advt at (l, m) = (1, 0), l_max 255; rounding of
+    # the two summation orders, the twiddles being correctly rounded tables).
+    tol = 1e-12 if l_max <= 127 else 4e-12
     pair = {"Advt": "Advp", "Advp": "Advt", "VxBt": "VxBp", "VxBp": "VxBt"}
+    errs = {}
     for k in ref:
         got = out[k].cpu().numpy()
         assert np.all(got[:, 0] == 0) and np.all(got[:, -1] == 0), k
         scale = np.abs(ref[k]).max()
         if k in pair:
             scale = max(scale, np.abs(ref[pair[k]]).max())
-        assert np.abs(got - ref[k]).max() / scale < 1e-12, k
+        errs[k] = np.abs(got - ref[k]).max() / scale
+    print("fp64 stage errors", {k: f"{v:.1e}" for k, v in errs.items()})
+    for k, e in errs.items():
+        assert e < tol, (k, e)
     assert rel_err(dt.cpu().numpy(), rdt) < 1e-12
     assert rel_err(dh.cpu().numpy(), rdh) < 1e-12
 
