@@ -275,56 +275,86 @@ def job_steps_per_s(world, ms_max):
     return world * 1000.0 / ms_max
 
 
+def count_launches(fn):
+    """(this library's kernels, all kernels) launched by one call of fn, from the
+    CUDA activity of a torch profiler trace (library kernels live in namespace mt)."""
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    names = [e.name for e in prof.events() if e.device_type.name == "CUDA"
+             and not e.name.lower().startswith(("memcpy", "memset"))]
+    return sum(1 for n in names if "mt::" in n), len(names)
+
+
 def run_anel(args, rank, world):
-    """Optional line: the fused anelastic stage at the anelastic benchmark
-    resolution (l_max = 383, n_theta = 576, n_phi = 1152, n_r = 129, hydrodynamic,
-    split precision), device-timed with inputs resident."""
-    from magic_b200 import Plan
-    from magic_b200.profiles import anelastic_profiles
+    """Optional line: whole CNAB2 steps of anelastic convection at the anelastic
+    benchmark resolution (l_max = 383, n_theta = 576, n_phi = 1152, 129 Chebyshev
+    levels, standard (w, p) form; polytropic background with 5 density scale
+    heights and index 2, Ek 1e-4, Ra 3e6, Pr 1, no magnetic field, stress-free
+    boundaries with the angular-momentum corrections, dt 1e-6; seeded
+    perturbations |c_lm| ~ 1e-3 (l+1)^-2), through magic_b200.step.AnelasticStep:
+    the fused split-precision anelastic stage, beside the FP64 stage (composed
+    from the FP64 transform kernels as the reference composes it), both with the
+    same FP64 solves; device-timed with the state resident (2.9 GB of spectral
+    arrays, larger than L2)."""
+    from magic_b200.step import AnelasticStep
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     l_max, n_r = 383, args.levels if args.levels != N_R else 129
-    plan = Plan(l_max, 1, precision="split", device=dev)
-    g = torch.Generator(device="cpu").manual_seed(rank)
-    l = torch.as_tensor(plan.lm2l, dtype=torch.float64)
-    m0 = torch.as_tensor(plan.lm2m == 0)
-    fields = {}
-    for k in ("w", "dw", "ddw", "z", "dz", "s"):
-        ph = torch.rand(plan.lm_max, n_r, generator=g, dtype=torch.float64) * 2 * math.pi
-        c = torch.polar(1e-4 * (l + 1.0)[:, None] ** -2 * torch.ones(1, n_r, dtype=torch.float64), ph)
-        c[m0] = c[m0].real.to(c.dtype)
-        fields[k] = c.to(dev)
-    prof = anelastic_profiles(n_r, l_max, device=dev)
-    work = torch.empty(plan.nl_anel_workspace(n_r, False, False), dtype=torch.uint8, device=dev)
-    out = None
+    cache = {}
 
-    def step():
-        nonlocal out
-        out, _, _ = plan.nl_anel(fields, prof, 1.0, 0.3, 0.0, 2.5, 1.0, 1.0, l_mag=False,
-                                 out=out, work=work)
+    def build(prec):
+        st = AnelasticStep(l_max, n_r, ek=1e-4, ra=3e6, pr=1.0, dt=1e-6, precision=prec,
+                           device=dev, cache=cache)
+        st.init_random(seed=rank, amp=1e-3)
+        for _ in range(args.warmup):
+            st.step()
+        torch.cuda.synchronize()
+        return st
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev) as clocks:
+    def timed(st, nsteps, clocks=None):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(args.steps):
-            step()
+        for _ in range(nsteps):
+            st.step()
         e1.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+        return e0.elapsed_time(e1) / nsteps
+
+    st = build("split")
+    with ClockSampler(dev) as clocks:
+        ms = timed(st, args.steps)
+    ours, every = count_launches(lambda: st.step())
+    del st
+    torch.cuda.empty_cache()
+    st64 = build("fp64")
+    n64 = max(1, min(args.steps, 3))
+    ms64 = timed(st64, n64)
     if rank == 0:
-        print(json.dumps({"metric": "anelastic nonlinear stage steps/s @lmax=383, 1 B200",
+        print(json.dumps({"metric": "anelastic CNAB2 steps/s @lmax=383 vs FP64 stage, 1 B200",
                           "value": 1000.0 / ms, "unit": "steps/s", "n_gpus": 1,
                           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-                          "higher_is_better": True, "dtype": "bf16x3/f32", "data": "synthetic",
-                          "config": {"workload": "anelastic hydro radial-loop nonlinear stage "
-                                                 "(split)", "l_max": l_max, "n_theta": 576,
-                                     "n_phi": 1152, "n_r": n_r, "grid_fields_in": 12,
-                                     "spectral_out": 6},
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "bf16x3/f32 stage, f64 solves", "data": "synthetic",
+                          "config": {"workload": "anelastic convection, whole CNAB2 step "
+                                                 "(Chebyshev, standard (w, p) form, "
+                                                 "stress-free + AM corrections, split stage)",
+                                     "l_max": l_max, "n_theta": 576, "n_phi": 1152,
+                                     "n_r": n_r, "strat": 5.0, "polind": 2.0, "ek": 1e-4,
+                                     "ra": 3e6, "pr": 1.0, "dt": 1e-6, "l_mag": False,
+                                     "l2": "state larger than L2", "parallelism": "replicas"},
+                          "gpu_launches": ours * args.steps,
+                          "kernels_per_step": {"library": ours, "all": every},
+                          "fp64_stage": {"value": 1000.0 / ms64, "unit": "steps/s",
+                                         "ms_per_step": ms64, "steps": n64,
+                                         "speedup": ms64 / ms,
+                                         "what": "the same steps with the FP64 anelastic stage"},
                           "clocks": clocks.summary()}), flush=True)
 
 
@@ -1034,8 +1064,9 @@ def main():
                     help="step (headline): whole CNAB2 time steps at l_max=255, 97 FD4 levels, "
                          "beside the plain FP64 path; stage: the Boussinesq MHD nonlinear "
                          "stage alone (extra line); sht: the standalone SHT round trip at "
-                         "l_max=127 (extra line); anel: the fused anelastic stage at "
-                         "l_max=383 (extra line, split precision); td: the explicit "
+                         "l_max=127 (extra line); anel: whole anelastic CNAB2 steps at "
+                         "l_max=383, 129 Chebyshev levels (extra line, split and FP64 "
+                         "stages); td: the explicit "
                          "time-derivative terms (get_td + finish_exp, FP64, extra line); "
                          "serve: the ensemble stream, continuous batching (extra line)")
     ap.add_argument("--step-lmax", type=int, default=L_MAX, help="step: l_max of the shell")

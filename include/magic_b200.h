@@ -472,6 +472,9 @@ typedef struct {
   int impl_interior; /* nonzero: both implicit terms zero at l = 0 and at the two boundary
                         levels, as the reference's time step stores them (step_time.py:385-394,
                         :538-545); zero: every entry, as updateWP alone */
+  const double* p0_row0; /* (n_r) or NULL: row 0 of the l = 0 pressure right-hand side is
+                            sum_r p0_row0[r] Re s00[r] (the anelastic integral constraint,
+                            update_wp.py:416-421, with P0 built to match); NULL: 0 */
 } mt_wp_update;
 
 MT_API int mt_update_wp(const mt_plan* plan, int n_r, const mt_wp_update* u, const mt_lop* solve,

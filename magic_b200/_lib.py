@@ -125,7 +125,8 @@ class WpUpdate(C.Structure):
                [(n, C.c_double) for n in ("w_old_wt", "w_impl_wt", "w_expl0_wt", "w_expl1_wt",
                                           "wimp_lin0", "BuoFac", "ChemFac")] + \
                [(n, _dp) for n in ("hdif", "or1", "or2", "beta", "dbeta", "visc", "dLvisc",
-                                   "rgrav", "rho0")] + [("impl_interior", C.c_int)]
+                                   "rgrav", "rho0")] + [("impl_interior", C.c_int),
+                                                        ("p0_row0", _dp)]
 
 
 class LevelCopy(C.Structure):

@@ -704,6 +704,7 @@ struct WpArgs {
   const double* hdif;
   const double *or1, *or2, *beta, *dbeta, *visc, *dLvisc, *rgrav, *rho0;
   int impl_interior;
+  const double* p0_row0;
   const double* mt;
   OpView D1, D2, D3, P0;
 };
@@ -733,10 +734,17 @@ __device__ __forceinline__ void wp_rhs(const WpArgs& a, int64_t o, int k, double
 }
 
 // right-hand side of the l = 0 pressure at level k (row (0, 0))
+// (row 0: the anelastic integral constraint sum_r p0_row0[r] Re s00[r], or 0)
 __device__ __forceinline__ double wp_p0_rhs(const WpArgs& a, int64_t row0, int k) {
+  if (k == 0) {
+    double c = 0.0;
+    if (a.p0_row0)
+      for (int j = 0; j < a.n_r; ++j) c += a.p0_row0[j] * a.s[row0 + j].x;
+    return c;
+  }
   double v = a.rho0[k] * a.BuoFac * a.rgrav[k] * a.s[row0 + k].x + a.we0[row0 + k].x;
   if (a.xi) v += a.rho0[k] * a.ChemFac * a.rgrav[k] * a.xi[row0 + k].x;
-  return k == 0 ? 0.0 : v;
+  return v;
 }
 
 // radial coefficients of the implicit terms at level j of degree l
@@ -1375,6 +1383,7 @@ int mt_update_wp(const mt_plan* p, int n_r, const mt_wp_update* u, const mt_lop*
   a.or1 = u->or1; a.or2 = u->or2; a.beta = u->beta; a.dbeta = u->dbeta; a.visc = u->visc;
   a.dLvisc = u->dLvisc; a.rgrav = u->rgrav; a.rho0 = u->rho0;
   a.impl_interior = u->impl_interior;
+  a.p0_row0 = u->p0_row0;
   a.mt = solve->mt;
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);

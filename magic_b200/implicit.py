@@ -314,19 +314,59 @@ def wp_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbotv=2):
     return M
 
 
-def p0_inverse(sch, beta):
-    """Inverse of the l = 0 pressure matrix (magic_torch/update_wp.py:80-165),
-    Boussinesq row 0 (p = 0).  Finite differences: grid-value unknowns, rows 1..
-    dp/dr - beta p with the last row the first-order backward difference (entries
-    beyond the band of half-width fd_order/2 dropped).  Chebyshev: coefficient
-    unknowns, rows rnorm (drMat - beta rMat), row 0 rnorm rMat[0] (columns >= n_cheb
-    dropped), first and last column scaled by boundary_fac, with the truncation and
-    the DCT-I to grid values folded into the inverse."""
+def cheb_integral_kernel(N, rnorm):
+    """K[j, k] = rnorm (1/(1 - (k-j)^2) + 1/(1 - (k+j)^2)) / 2 for j + k even (terms
+    with a zero denominator dropped), else 0: the integral of T_j T_k over [-1, 1]
+    in the reference's Chebyshev normalisation (magic_torch/init_fields.py:88-105)."""
+    j = np.arange(N, dtype=np.float64)[:, None]
+    k = np.arange(N, dtype=np.float64)[None, :]
+    d1, d2 = 1.0 - (k - j) ** 2, 1.0 - (k + j) ** 2
+    with np.errstate(divide="ignore"):
+        s1 = np.where(d1 != 0, 1.0 / np.where(d1 != 0, d1, 1.0), 0.0)
+        s2 = np.where(d2 != 0, 1.0 / np.where(d2 != 0, d2, 1.0), 0.0)
+    return ((j + k) % 2 == 0) * (s1 + s2) * 0.5 * rnorm
+
+
+def p0_integral_constraint(sch, bg, ThExpNb=1.0):
+    """The anelastic l = 0 pressure's integral constraint on Chebyshev levels
+    (magic_torch/update_wp.py:31, 121-135, 416-421; used when ViscHeatFac ThExpNb
+    != 0): (row, rhs) with row the physical weights ThExpNb ViscHeatFac ogrun
+    alpha0 r^2 whose Chebyshev integral replaces the p = 0 row of the matrix
+    (ogrun = polind, alpha0 = 1 / temp0), and rhs the weights of the right-hand
+    side's row 0, int ThExpNb alpha0 temp0 rho0 r^2 Re s00 dr = sum rhs Re s00
+    (radial rule sch.rint).  None where the constraint is off (Boussinesq, or FD)."""
+    if not sch.chebyshev or bg["ViscHeatFac"] * ThExpNb == 0.0:
+        return None
+    r = np.asarray(sch.r, dtype=np.float64)
+    alpha0, temp0, rho0 = 1.0 / bg["temp0"], bg["temp0"], bg["rho0"]
+    ogrun = np.full_like(r, bg["polind"])
+    row = ThExpNb * bg["ViscHeatFac"] * ogrun * alpha0 * r * r
+    rhs = np.asarray(sch.rint) * ThExpNb * alpha0 * temp0 * rho0 * r * r
+    return row, rhs
+
+
+def p0_inverse(sch, beta, integ_row=None):
+    """Inverse of the l = 0 pressure matrix (magic_torch/update_wp.py:80-165).
+    Finite differences: grid-value unknowns, rows 1.. dp/dr - beta p with the last
+    row the first-order backward difference (entries beyond the band of half-width
+    fd_order/2 dropped), row 0 p = 0.  Chebyshev: coefficient unknowns, rows rnorm
+    (drMat - beta rMat); row 0 rnorm rMat[0] (p = 0 at the outer boundary) or, with
+    integ_row (p0_integral_constraint), the Chebyshev integral of integ_row p: K
+    applied to rnorm costf(integ_row) with its end values times boundary_fac;
+    columns >= n_cheb dropped in row 0, first and last column scaled by
+    boundary_fac, with the truncation and the DCT-I to grid values folded into
+    the inverse."""
     N = sch.n_r
     if sch.chebyshev:
         A = np.zeros((N, N))
         A[1:] = sch.rnorm * (sch.drMat[1:] - np.asarray(beta)[1:, None] * sch.rMat[1:])
-        A[0] = sch.rnorm * sch.rMat[0]
+        if integ_row is not None:
+            work = _dct1(N) @ np.asarray(integ_row, dtype=np.float64) * sch.rnorm
+            work[0] *= sch.boundary_fac
+            work[N - 1] *= sch.boundary_fac
+            A[0] = cheb_integral_kernel(N, sch.rnorm) @ work
+        else:
+            A[0] = sch.rnorm * sch.rMat[0]
         if sch.n_cheb < N:
             A[0, sch.n_cheb:] = 0.0
         A[:, 0] *= sch.boundary_fac
@@ -372,7 +412,7 @@ def update_poloidal_dc(plan, sch, lop, P0, w, dw, ddw, p, ta, weights, s, prof, 
 
 
 def update_wp(plan, sch, lop, P0, w, dw, ddw, p, dp, taw, tap, weights, s, prof, hdif,
-              BuoFac, xi=None, ChemFac=0.0, impl_interior=False):
+              BuoFac, xi=None, ChemFac=0.0, impl_interior=False, p0_row0=None):
     """One standard-form poloidal step in place (mt_update_wp): w, dw, ddw, p, dp
     outputs; taw / tap: dicts old, impl, expl0, expl1 of the w and p equations;
     s / xi: this step's entropy / composition; prof: or1, or2, beta, dbeta, visc,
@@ -380,7 +420,9 @@ def update_wp(plan, sch, lop, P0, w, dw, ddw, p, dp, taw, tap, weights, s, prof,
     wp_solve_operators; P0: RadialOp of p0_inverse.  impl_interior: zero both
     implicit terms at l = 0 and at the boundary levels, as the reference's time
     step does (step_time.py:385-394; updateWP alone keeps them; the solution
-    never reads those entries)."""
+    never reads those entries).  p0_row0: the anelastic integral constraint's
+    right-hand-side weights (p0_integral_constraint), with P0 built from the same
+    constraint; None: p = 0 at the outer boundary."""
     n_r = w.shape[1]
     arrs = [w, dw, ddw, p, dp, taw["old"], taw["impl"], taw["expl0"], taw["expl1"], tap["old"],
             tap["impl"], tap["expl0"], tap["expl1"], s]
@@ -393,7 +435,8 @@ def update_wp(plan, sch, lop, P0, w, dw, ddw, p, dp, taw, tap, weights, s, prof,
                                                "rgrav", "rho0")]]
     u = _lib.WpUpdate(*[a.data_ptr() for a in arrs], xi.data_ptr() if xi is not None else None,
                       n_r, w_old, w_impl, w_e0, w_e1, wimp_lin0, float(BuoFac), float(ChemFac),
-                      *[d.data_ptr() for d in dev], int(bool(impl_interior)))
+                      *[d.data_ptr() for d in dev], int(bool(impl_interior)),
+                      p0_row0.data_ptr() if p0_row0 is not None else None)
     st = C.c_void_p(torch.cuda.current_stream(w.device).cuda_stream)
     check(_lib.lib().mt_update_wp(plan._h, n_r, C.byref(u), lop._h, sch.D1._h, sch.D2._h,
                                   sch.D3._h, P0._h, st))

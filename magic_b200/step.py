@@ -109,8 +109,11 @@ class BoussinesqStep:
         self.dt = None
         self.dt_max = float(dt)  # the Courant control's upper bound (initialize_dt)
         self.set_dt(dt, dt)
+        pc = self._p0_constraint()
         self.P0 = self._shared(("P0",) + self._shape,
-                               lambda: RadialOp(I.p0_inverse(self.sch, hp["beta"]), device=dev))
+                               lambda: RadialOp(I.p0_inverse(self.sch, hp["beta"],
+                                                             pc[0] if pc else None), device=dev))
+        self.p0_row0 = t(pc[1]) if pc else None
         dev_coef = lambda c: {k: (t(v) if v is not None else None) for k, v in c.items()}
         self.coef = dict(s=dev_coef(I.entropy_coefficients(l_max, self.opr, hdif, hp["kappa"],
                                                            self._d1c, hp["or2"])),
@@ -162,6 +165,11 @@ class BoussinesqStep:
     def _background(self, r, radratio, **phys):
         """Radial profiles replacing the Boussinesq ones (none here)."""
         return {}
+
+    def _p0_constraint(self):
+        """(matrix row weights, right-hand-side weights) of an integral constraint
+        replacing p = 0 in the l = 0 pressure equation, or None."""
+        return None
 
     def stage_outputs(self):
         """Spectral outputs of this step's nonlinear stage."""
@@ -365,7 +373,7 @@ class BoussinesqStep:
         if self.std_form:
             I.update_wp(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"], f["ddw"],
                         f["p"], f["dp"], ta["w"], ta["p"], w, f["s"], self.wpprof, self.hdif,
-                        self.BuoFac, impl_interior=True)
+                        self.BuoFac, impl_interior=True, p0_row0=self.p0_row0)
         else:
             I.update_poloidal_dc(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"],
                                  f["ddw"], f["p"], ta["w"], w, f["s"], self.wprof, self.hdif,
@@ -412,8 +420,9 @@ class AnelasticStep(BoussinesqStep):
                  the density and viscosity terms of update_z.py:40-47), then the
                  angular-momentum corrections of stress-free runs
                  (update_z.py:446-475, mt_correct_am), the poloidal velocity and
-                 pressure with the anelastic (w, p) operators, magnetic field
-                 when l_mag.
+                 pressure with the anelastic (w, p) operators and, on Chebyshev
+                 levels, the integral constraint of the l = 0 pressure
+                 (update_wp.py:121-135, 416-421), magnetic field when l_mag.
 
     Defaults are the reference's anelastic benchmark setup (configs/
     hydro_bench_anel_modal.yaml): 5 density scale heights, polytropic index
@@ -458,6 +467,9 @@ class AnelasticStep(BoussinesqStep):
                                          l_mag=self.l_mag, **self._anel)
         return {k: self._bg[k] for k in ("rgrav", "rho0", "beta", "dbeta", "ddbeta", "dLtemp0",
                                          "orho1", "orho2", "otemp1")}
+
+    def _p0_constraint(self):
+        return I.p0_integral_constraint(self.sch, dict(self._bg, polind=self._anel["polind"]))
 
     def stage_outputs(self):
         return ("Advr", "Advt", "Advp", "VSr", "VSt") + (

