@@ -51,9 +51,9 @@ __device__ __forceinline__ void umma_s8(uint32_t tmem_d, uint64_t da, uint64_t d
       : "memory");
 }
 
-// 16 consecutive int32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
-  uint32_t r[16];
+// 16 consecutive int32 columns of this thread's TMEM lane, without the wait:
+// several loads are issued, then one tmem_wait_ld() makes their registers valid.
+__device__ __forceinline__ void tmem_ld16_i32_nowait(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
       "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
@@ -61,9 +61,25 @@ __device__ __forceinline__ void tmem_ld16_i32(uint32_t taddr, int (&v)[16]) {
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
         "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// v 2^s: one multiplication by the exact power of two when 2^s is a normal
+// double (the product rounds once, as ldexp does), ldexp otherwise.
+__device__ __forceinline__ double oz_scale(double v, int s) {
+  if (s >= -1022 && s <= 1023) return v * __longlong_as_double((long long)(s + 1023) << 52);
+  return ldexp(v, s);
+}
+
+// sum_g 2^(-7 g) C_g for one accumulator column from raw TMEM words
+__device__ __forceinline__ double oz_combine_u(const uint32_t (&c)[kOzGroups][16], int i) {
+  double v = (double)(int)c[kOzGroups - 1][i];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+  for (int g = kOzGroups - 2; g >= 0; --g) v = fma(v, 1.0 / 128.0, (double)(int)c[g][i]);
+  return v;
 }
 
 // Named barrier over `n` threads that also ANDs a predicate across them, so
@@ -77,14 +93,6 @@ __device__ __forceinline__ bool bar_and(int id, int n, bool v) {
       : "r"((uint32_t)v), "r"(id), "r"(n)
       : "memory");
   return r != 0;
-}
-
-// sum_g 2^(-7 g) C_g for one accumulator column (exact terms, FP64 sum)
-__device__ __forceinline__ double oz_combine(const int (&c)[kOzGroups][16], int i) {
-  double v = (double)c[kOzGroups - 1][i];
-#pragma unroll
-  for (int g = kOzGroups - 2; g >= 0; --g) v = fma(v, 1.0 / 128.0, (double)c[g][i]);
-  return v;
 }
 
 // Issue the 21 digit-pair MMAs of one K chunk: group g = i + j into the
@@ -471,7 +479,8 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
 // warps 2-5 drain the accumulators (one TMEM lane per thread), form the FP64
 // values and store them into Fs, and hand the accumulators back.
 constexpr int kOzStages = 4;
-constexpr int kOzSynThreads = 64 + 128;
+constexpr int kOzSynEpiWarps = 8;  // two per TMEM lane quarter, 32 columns each
+constexpr int kOzSynThreads = 64 + 32 * kOzSynEpiWarps;
 
 struct OzSynSmem {
   static constexpr uint32_t stage_bytes = kOzAChunk + kOzSynBChunk;
@@ -519,7 +528,7 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
       mbar_init(&empty[s], 1);
     }
     mbar_init(tfull, 1);
-    mbar_init(tempty, 128);
+    mbar_init(tempty, 32 * kOzSynEpiWarps);
     mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -596,8 +605,9 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
       umma_commit(done);
     }
   } else {
-    // epilogue: warps 2-5 own TMEM lane quarters (warp % 4)
-    const int quarter = warp & 3;
+    // epilogue: warps 2-9; warp w owns TMEM lane quarter w % 4 and the 32
+    // accumulator columns of half (w - 2) / 4
+    const int quarter = warp & 3, half = (warp - 2) >> 2;
     const int R0 = quarter * 32 + lane;
     int n = 0;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++n) {
@@ -607,21 +617,23 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
       const Item it = decode(item);
       const int R = it.rt * kOzRows + R0;
       const int er = R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + it.combo) * a.rows_pad + R] : 0;
-      const int* fe = z.syn_fexp + ((int64_t)it.mc * 2 + it.combo) * nthw + it.tau * kOzSynN;
+      // column exponents of this warp's 32 columns, one per lane, shared by shuffles
+      const int fe_l = __ldg(z.syn_fexp + ((int64_t)it.mc * 2 + it.combo) * nthw +
+                             it.tau * kOzSynN + 32 * half + lane);
       double* out = a.Fs + (int64_t)it.mc * a.fs_m + (int64_t)it.combo * a.fs_c;
-      const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16);
+      const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16) + 32 * half;
 #pragma unroll 1
-      for (int c0 = 0; c0 < kOzSynN; c0 += 16) {
-        int cg[kOzGroups][16];
+      for (int c0 = 0; c0 < 32; c0 += 16) {
+        uint32_t cg[kOzGroups][16];
 #pragma unroll
-        for (int g = 0; g < kOzGroups; ++g) tmem_ld16_i32(taddr + g * kOzSynN + c0, cg[g]);
-        if (R < a.nrows) {
+        for (int g = 0; g < kOzGroups; ++g) tmem_ld16_i32_nowait(taddr + g * kOzSynN + c0, cg[g]);
+        tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int th = it.tau * kOzSynN + c0 + i;
-            if (th < t.nhs)
-              out[(int64_t)th * a.fs_j + R] = ldexp(oz_combine(cg, i), er + __ldg(&fe[c0 + i]) - 12);
-          }
+        for (int i = 0; i < 16; ++i) {
+          const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
+          const int th = it.tau * kOzSynN + 32 * half + c0 + i;
+          if (R < a.nrows && th < t.nhs)
+            out[(int64_t)th * a.fs_j + R] = oz_scale(oz_combine_u(cg, i), er + fe - 12);
         }
       }
       tc_fence_before();
@@ -902,18 +914,22 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
       for (int q = 0; q < 2; ++q) {
         const int fold = q ? 1 - it.par : it.par;
         const int er = a.rexp[((int64_t)it.mc * 2 + fold) * a.rows_pad + Rg];
-        const int* fe = z.ana_fexp + ((int64_t)(it.mc * 2 + q) * 2 + it.par) * z.nlt * kOzAnaN +
-                        it.lt * kOzAnaN;
+        // the kOzAnaN (32) column exponents, one per lane, shared by shuffles
+        const int fe_l = __ldg(z.ana_fexp +
+                               ((int64_t)(it.mc * 2 + q) * 2 + it.par) * z.nlt * kOzAnaN +
+                               it.lt * kOzAnaN + lane);
 #pragma unroll 1
         for (int c0 = 0; c0 < kOzAnaN; c0 += 16) {
-          int cg[kOzGroups][16];
+          uint32_t cg[kOzGroups][16];
 #pragma unroll
           for (int g = 0; g < kOzGroups; ++g)
-            tmem_ld16_i32(taddr + (uint32_t)((q * kOzGroups + g) * kOzAnaN + c0), cg[g]);
+            tmem_ld16_i32_nowait(taddr + (uint32_t)((q * kOzGroups + g) * kOzAnaN + c0), cg[g]);
+          tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            xch[(q * kOzRows + R0) * kOzXS + c0 + i] =
-                ldexp(oz_combine(cg, i), er + __ldg(&fe[c0 + i]) - 12);
+          for (int i = 0; i < 16; ++i) {
+            const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
+            xch[(q * kOzRows + R0) * kOzXS + c0 + i] = oz_scale(oz_combine_u(cg, i), er + fe - 12);
+          }
         }
       }
       tc_fence_before();

@@ -345,6 +345,12 @@ def p0_integral_constraint(sch, bg, ThExpNb=1.0):
     return row, rhs
 
 
+def _lapack_inverse(A):
+    """FP64 inverse by torch.linalg.inv on the CPU, the routine the reference uses
+    for its l = 0 pressure matrix (magic_torch/update_wp.py:141-171)."""
+    return torch.linalg.inv(torch.from_numpy(np.ascontiguousarray(A, dtype=np.float64))).numpy()
+
+
 def p0_inverse(sch, beta, integ_row=None):
     """Inverse of the l = 0 pressure matrix (magic_torch/update_wp.py:80-165).
     Finite differences: grid-value unknowns, rows 1.. dp/dr - beta p with the last
@@ -355,7 +361,10 @@ def p0_inverse(sch, beta, integ_row=None):
     applied to rnorm costf(integ_row) with its end values times boundary_fac;
     columns >= n_cheb dropped in row 0, first and last column scaled by
     boundary_fac, with the truncation and the DCT-I to grid values folded into
-    the inverse."""
+    the inverse.  Inverted with the reference's own routine (torch.linalg.inv on
+    the CPU): with the integral row the matrix's condition number reaches ~5e8,
+    and two LAPACK inversions then differ by ~1e-10 in the hydrostatic p00,
+    while the same routine reproduces the reference's inverse exactly."""
     N = sch.n_r
     if sch.chebyshev:
         A = np.zeros((N, N))
@@ -371,7 +380,7 @@ def p0_inverse(sch, beta, integ_row=None):
             A[0, sch.n_cheb:] = 0.0
         A[:, 0] *= sch.boundary_fac
         A[:, N - 1] *= sch.boundary_fac
-        Minv = np.linalg.inv(A)
+        Minv = _lapack_inverse(A)
         Minv[sch.n_cheb:] = 0.0
         return _dct1(N) @ Minv
     A = np.zeros((N, N))
@@ -381,7 +390,7 @@ def p0_inverse(sch, beta, integ_row=None):
     A[N - 1, N - 2] = -1.0 / delr
     A[N - 1, :N - 1 - sch.fd_order // 2] = 0.0
     A[0] = np.eye(N)[0]
-    return np.linalg.inv(A)
+    return _lapack_inverse(A)
 
 
 def update_poloidal_dc(plan, sch, lop, P0, w, dw, ddw, p, ta, weights, s, prof, hdif, BuoFac,

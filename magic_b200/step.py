@@ -362,7 +362,11 @@ class BoussinesqStep:
                          l_anel=self.l_anel, out=td_out)
 
     def lm_loop(self):
-        """Implicit solves S, Z, W, B (step_time.py:1478-1527)."""
+        """Implicit solves S, Z, W, B (step_time.py:1478-1527).  The Boussinesq
+        standard form stores its implicit terms zero at l = 0 and on the boundary
+        levels, as the reference's fused lm loop does (:380-394); the anelastic
+        loop calls updateWP itself, which stores every entry (update_wp.py:
+        491-531; neither affects the solution)."""
         f, ta, w = self.f, self.ta, self.weights
         I.update_field(self.plan, self.sch, self.ops["s"], f["s"], f["ds"], ta["s"], w,
                        self.coef["s"], bot=self.bots)
@@ -373,7 +377,7 @@ class BoussinesqStep:
         if self.std_form:
             I.update_wp(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"], f["ddw"],
                         f["p"], f["dp"], ta["w"], ta["p"], w, f["s"], self.wpprof, self.hdif,
-                        self.BuoFac, impl_interior=True, p0_row0=self.p0_row0)
+                        self.BuoFac, impl_interior=not self.l_anel, p0_row0=self.p0_row0)
         else:
             I.update_poloidal_dc(self.plan, self.sch, self.ops["w"], self.P0, f["w"], f["dw"],
                                  f["ddw"], f["p"], ta["w"], w, f["s"], self.wprof, self.hdif,
