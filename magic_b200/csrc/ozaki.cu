@@ -74,12 +74,14 @@ __device__ __forceinline__ double oz_scale(double v, int s) {
   return ldexp(v, s);
 }
 
-// sum_g 2^(-7 g) C_g for one accumulator column from raw TMEM words
+// 2^35 sum_g 2^(-7 g) C_g for one accumulator column from raw TMEM words,
+// exact in int64 (|C_g| < 2^23, so the sum stays below 2^59), then rounded once
+// to FP64; callers scale by 2^(e - 35).
 __device__ __forceinline__ double oz_combine_u(const uint32_t (&c)[kOzGroups][16], int i) {
-  double v = (double)(int)c[kOzGroups - 1][i];
+  long long v = (int)c[0][i];
 #pragma unroll
-  for (int g = kOzGroups - 2; g >= 0; --g) v = fma(v, 1.0 / 128.0, (double)(int)c[g][i]);
-  return v;
+  for (int g = 1; g < kOzGroups; ++g) v = v * 128 + (int)c[g][i];
+  return (double)v;
 }
 
 // Named barrier over `n` threads that also ANDs a predicate across them, so
@@ -95,20 +97,28 @@ __device__ __forceinline__ bool bar_and(int id, int n, bool v) {
   return r != 0;
 }
 
-// Issue the 21 digit-pair MMAs of one K chunk: group g = i + j into the
-// accumulator at tmem_acc + g * gcols.  `first`: the first chunk of an item,
-// whose first MMA per group overwrites the accumulator.
-__device__ __forceinline__ void oz_mma_chunk(uint32_t tmem_acc, uint32_t gcols, uint32_t sa,
-                                             uint32_t sb, uint32_t b_plane, uint32_t idesc,
+// Issue the 21 digit-pair products of one K chunk: pair (i, j) accumulates
+// into group g = i + j at tmem_acc + g * NP (NP: MMA columns per table digit
+// plane).  The table's six digit planes lie one after another in shared
+// memory (NP rows of 32 bytes each, 8-row core groups 256 bytes apart), so the
+// planes j0 .. j0 + np - 1 form one operand of N = np * NP rows, and its
+// product with data plane i lands in groups i + j0 .. i + j0 + np - 1: eight
+// MMAs of up to 256 columns (NP = 64) or six (NP = 32) instead of 21, each
+// data plane read once per chunk.  `first`: the first chunk of an item, whose
+// i = 0 products (covering every group) overwrite the accumulators.
+template <int NP>
+__device__ __forceinline__ void oz_mma_chunk(uint32_t tmem_acc, uint32_t sa, uint32_t sb,
                                              bool first) {
+  constexpr int kMaxPlanes = 256 / NP;
 #pragma unroll
-  for (int g = 0; g < kOzGroups; ++g) {
+  for (int i = 0; i < kOzDigits; ++i) {
+    const uint64_t da = umma_desc(sa + (uint32_t)i * kOzAPlane, 128, 256);
 #pragma unroll
-    for (int i = 0; i <= g; ++i) {
-      const int j = g - i;
-      const uint64_t da = umma_desc(sa + (uint32_t)i * kOzAPlane, 128, 256);
-      const uint64_t db = umma_desc(sb + (uint32_t)j * b_plane, 128, 256);
-      umma_s8(tmem_acc + (uint32_t)g * gcols, da, db, idesc, (first && i == 0) ? 0u : 1u);
+    for (int j0 = 0; j0 < kOzDigits - i; j0 += kMaxPlanes) {
+      const int np = (kOzDigits - i - j0) < kMaxPlanes ? (kOzDigits - i - j0) : kMaxPlanes;
+      const uint64_t db = umma_desc(sb + (uint32_t)(j0 * NP * kOzK), 128, 256);
+      umma_s8(tmem_acc + (uint32_t)((i + j0) * NP), da, db, umma_idesc_s8(kOzRows, np * NP),
+              (first && i == 0) ? 0u : 1u);
     }
   }
 }
@@ -575,7 +585,6 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_s8(kOzRows, kOzSynN);
       int g = 0, n = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x, ++n) {
@@ -594,7 +603,7 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
             }
             tc_fence_after();
             const uint32_t sa = smem_u32(smem + s * OzSynSmem::stage_bytes);
-            oz_mma_chunk(tbase, kOzSynN, sa, sa + kOzAChunk, kOzSynBPlane, idesc, first);
+            oz_mma_chunk<kOzSynN>(tbase, sa, sa + kOzAChunk, first);
             first = false;
             umma_commit(&empty[s]);
             ++g;
@@ -633,7 +642,7 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
           const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
           const int th = it.tau * kOzSynN + 32 * half + c0 + i;
           if (R < a.nrows && th < t.nhs)
-            out[(int64_t)th * a.fs_j + R] = oz_scale(oz_combine_u(cg, i), er + fe - 12);
+            out[(int64_t)th * a.fs_j + R] = oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
         }
       }
       tc_fence_before();
@@ -859,7 +868,6 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_s8(kOzRows, kOzAnaN);
       int g = 0, n = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
@@ -876,8 +884,8 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
             }
             tc_fence_after();
             const uint32_t sa = smem_u32(smem + s * OzAnaSmem::stage_bytes);
-            oz_mma_chunk(tbase + (uint32_t)(q * kOzGroups * kOzAnaN), kOzAnaN, sa, sa + kOzAChunk,
-                         kOzAnaBPlane, idesc, c == 0);
+            oz_mma_chunk<kOzAnaN>(tbase + (uint32_t)(q * kOzGroups * kOzAnaN), sa,
+                                  sa + kOzAChunk, c == 0);
             umma_commit(&empty[s]);
             ++g;
           }
@@ -928,7 +936,7 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
-            xch[(q * kOzRows + R0) * kOzXS + c0 + i] = oz_scale(oz_combine_u(cg, i), er + fe - 12);
+            xch[(q * kOzRows + R0) * kOzXS + c0 + i] = oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
           }
         }
       }
