@@ -239,6 +239,7 @@ struct BandView {
   const int* piv;
   const double *fr, *fc;
   int kl, ku;
+  const double* rd;  // 1 / U's diagonal (staged copies only)
 };
 
 // Pivoted banded LU solve of the CTA's rows in shared memory (the reference's
@@ -287,9 +288,10 @@ __device__ __forceinline__ void band_solve_rows(const BandView& b, int l, int n_
 }
 
 // Shared-memory bytes of one degree's band factors: abd ((2 kl + ku + 1) x n_r),
-// fr and fc (n_r each), piv (n_r ints), 16-byte aligned.
+// fr, fc and the reciprocals of U's diagonal (n_r each), piv (n_r ints),
+// 16-byte aligned.
 __host__ __device__ inline size_t band_smem_bytes(int kl, int ku, int n_r) {
-  const size_t d = (size_t)(2 * kl + ku + 1 + 2) * n_r * sizeof(double);
+  const size_t d = (size_t)(2 * kl + ku + 1 + 3) * n_r * sizeof(double);
   return (d + (size_t)n_r * sizeof(int) + 15) / 16 * 16;
 }
 
@@ -301,15 +303,105 @@ __device__ __forceinline__ BandView stage_band(const BandView& b, int l, int n_r
   double* abd = sm;
   double* fr = abd + nb;
   double* fc = fr + n_r;
-  int* piv = reinterpret_cast<int*>(fc + n_r);
+  double* rd = fc + n_r;
+  int* piv = reinterpret_cast<int*>(rd + n_r);
   const double* gabd = b.abd + (int64_t)l * nb;
+  const int dg = (b.kl + b.ku) * n_r;  // row of U's diagonal
   for (int i = threadIdx.x; i < nb; i += blockDim.x) abd[i] = gabd[i];
   for (int i = threadIdx.x; i < n_r; i += blockDim.x) {
     fr[i] = b.fr[(int64_t)l * n_r + i];
     if (b.fc) fc[i] = b.fc[(int64_t)l * n_r + i];
     piv[i] = b.piv[(int64_t)l * n_r + i];
+    rd[i] = 1.0 / gabd[dg + i];
   }
-  return BandView{abd, piv, fr, b.fc ? fc : nullptr, b.kl, b.ku};
+  return BandView{abd, piv, fr, b.fc ? fc : nullptr, b.kl, b.ku, rd};
+}
+
+// x / d for U's diagonal entry d with r = 1/d: the product x r refined by one
+// residual step (Markstein's correction, q' = q + (x - q d) r), which gives the
+// correctly rounded quotient but in rare double-rounding cases; the refinement
+// replaces a full division on the solve's dependence chain.
+__device__ __forceinline__ double band_div(double x, double d, double r) {
+  const double q = __dmul_rn(x, r);
+  return fma(fma(-q, d, x), r, q);
+}
+
+// The solve of band_solve_rows for fixed half-bandwidths KL, KU with the
+// working entries of each row in registers: the forward sweep touches only
+// x[k-1 .. k-1+KL] at step k (the pivot row lies in that window), the
+// backward sweep only x[k-1-KL-KU .. k-1]; both windows slide along the row,
+// each entry read from and written to shared memory once per sweep.  Same
+// operations and order as band_solve_rows, except the division (band_div).
+template <int KL, int KU>
+__device__ __forceinline__ void band_solve_rows_w(const BandView& b, int n_r, int fs, double2* f,
+                                                  int nrow, int mc0) {
+  constexpr int M = KL + KU + 1, M1 = KL + KU;
+  const int t = threadIdx.x;
+  if (t < 2 * nrow) {
+    const int row = t >> 1, part = t & 1;
+    double* x = reinterpret_cast<double*>(f + row * fs) + part;  // level k at x[2 k]
+    const double* abd = b.abd;
+    double W[KL + 1];
+#pragma unroll
+    for (int q = 0; q <= KL; ++q) W[q] = q < n_r ? __dmul_rn(b.fr[q], x[2 * q]) : 0.0;
+    for (int k = 1; k <= n_r - 1; ++k) {  // L y = P (fr rhs), 1-based k
+      const int d = b.piv[k - 1] - k;     // 0 .. KL
+#pragma unroll
+      for (int q = 1; q <= KL; ++q)
+        if (d == q) {
+          const double tv = W[0];
+          W[0] = W[q];
+          W[q] = tv;
+        }
+      const double xk = W[0];
+      const int lm = min(KL, n_r - k);
+#pragma unroll
+      for (int i = 1; i <= KL; ++i)
+        if (i <= lm) W[i] = __dadd_rn(W[i], __dmul_rn(xk, abd[(M - 1 + i) * n_r + (k - 1)]));
+      x[2 * (k - 1)] = W[0];
+#pragma unroll
+      for (int q = 0; q < KL; ++q) W[q] = W[q + 1];
+      const int nx = k + KL;  // next entry entering the window
+      W[KL] = nx < n_r ? __dmul_rn(b.fr[nx], x[2 * nx]) : 0.0;
+    }
+    x[2 * (n_r - 1)] = W[0];
+    // U x = y: V[q] = x[k-1-M1+q], V[M1] the current entry
+    double V[M1 + 1];
+#pragma unroll
+    for (int q = 0; q <= M1; ++q) {
+      const int j = n_r - 1 - M1 + q;
+      V[q] = j >= 0 ? x[2 * j] : 0.0;
+    }
+    for (int k = n_r; k >= 1; --k) {
+      V[M1] = band_div(V[M1], abd[(M - 1) * n_r + (k - 1)], b.rd[k - 1]);
+      // b(lb + i) += t abd(la + i, k), i < lm = min(k, M) - 1, la = M - lm,
+      // lb = k - lm: entry x[k-1-lm+i] is V[q] with q = M1 - lm + i, and its
+      // coefficient row la - 1 + i is q itself
+      const int lm = min(k, M) - 1;
+      const double tv = -V[M1];
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q >= M1 - lm) V[q] = __dadd_rn(V[q], __dmul_rn(tv, abd[q * n_r + (k - 1)]));
+      x[2 * (k - 1)] = V[M1];
+#pragma unroll
+      for (int q = M1; q > 0; --q) V[q] = V[q - 1];
+      const int j = k - 2 - M1;
+      V[0] = j >= 0 ? x[2 * j] : 0.0;
+    }
+    if (b.fc)
+      for (int k = 0; k < n_r; ++k) x[2 * k] = __dmul_rn(b.fc[k], x[2 * k]);
+    if (part == 1 && mc0 + row == 0)
+      for (int k = 0; k < n_r; ++k) x[2 * k] = 0.0;
+  }
+  __syncthreads();
+}
+
+// dispatch on the half-bandwidths of the finite-difference operators
+__device__ __forceinline__ void band_solve(const BandView& b, int l, int n_r, int fs, double2* f,
+                                           int nrow, int mc0) {
+  if (b.rd && b.kl == 2 && b.ku == 2) band_solve_rows_w<2, 2>(b, n_r, fs, f, nrow, mc0);
+  else if (b.rd && b.kl == 3 && b.ku == 3) band_solve_rows_w<3, 3>(b, n_r, fs, f, nrow, mc0);
+  else band_solve_rows(b, l, n_r, fs, f, nrow, mc0);
 }
 
 // the solved rows (band form) from shared memory to the field's global array
@@ -486,7 +578,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
   if (band) {
-    band_solve_rows(bv, l, n_r, fs, f, nrow, mc0);
+    band_solve(bv, l, n_r, fs, f, nrow, mc0);
     store_rows(f, fs, n_r, nrow, lm_row, a.x, a.ld);
   } else {
     solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.x, a.ld,
@@ -566,7 +658,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, 2>::kThreads, Bounds<kStaged, 
   __syncthreads();
   const Slot s = slot_of(n_r, a.groups);
   if (band) {
-    band_solve_rows(bv, l, n_r, fs, f, nrow, mc0);
+    band_solve(bv, l, n_r, fs, f, nrow, mc0);
     store_rows(f, fs, n_r, nrow, lm_row, a.w, a.ld);
   } else {
     solve_rows_to<kStaged, kNt>(Ml, n_r, ldm, fs, f, mbuf, a.groups, mc0, s, nrow, a.w, a.ld,
@@ -1229,7 +1321,7 @@ int mt_update_field(const mt_plan* p, int n_r, const mt_field_update* u, const m
   a.so_l = u->so_l; a.so_r = u->so_r; a.ia_l = u->ia_l; a.ia_r = u->ia_r; a.ib_r = u->ib_r;
   a.ic_r = u->ic_r; a.ic_l = u->ic_l; a.ic_r2 = u->ic_r2;
   a.mt = solve->mt;
-  a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku};
+  a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku, nullptr};
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   const TileLaunch t = tile_launch(n_r, a.ldm, p->l_max, p->n_m, 1,
@@ -1318,7 +1410,7 @@ int mt_update_poloidal(const mt_plan* p, int n_r, const mt_poloidal_update* u,
   a.or2 = u->or2; a.orho1 = u->orho1; a.beta = u->beta; a.visc = u->visc; a.rgrav = u->rgrav;
   a.rho0 = u->rho0; a.c3 = u->c3; a.c2n = u->c2n; a.c1n = u->c1n; a.c1d = u->c1d; a.c0n = u->c0n;
   a.mt = solve->mt;
-  a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku};
+  a.band = BandView{solve->abd, solve->piv, solve->fr, solve->fc, solve->kl, solve->ku, nullptr};
   a.D1 = radial_op_view(D1);
   a.D2 = radial_op_view(D2);
   a.P0 = radial_op_view(P0);

@@ -260,21 +260,46 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
     twH[i] = {wh.x, wh.y};
   }
   // half spectra of the NFI fields; wavenumbers k >= n_m are zero
+  // (kLd elements per thread are loaded before any is stored, so their HBM
+  // latencies overlap)
+  constexpr int kLd = 4;
   if constexpr (SPLIT_IO) {
     const double hs = (row & 1) ? -1.0 : 1.0;  // north = sym + asym, south = sym - asym
     const double* fsym = a.Fs + (int64_t)(row >> 1) * a.fs_j + (int64_t)r * 2 * NFI;
-    for (int e = tid; e < M * NFI; e += kNlW64Threads) {
-      const int k = e / NFI, f = e - k * NFI;
-      const double2 sy = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m) + f);
-      const double2 as = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m + a.fs_c) + f);
-      buf[f * S + pad16(k)] = {sy.x + hs * as.x, sy.y + hs * as.y};
+    for (int e0 = tid; e0 < M * NFI; e0 += kLd * kNlW64Threads) {
+      double2 sy[kLd], as[kLd];
+#pragma unroll
+      for (int u = 0; u < kLd; ++u) {
+        const int e = e0 + u * kNlW64Threads;
+        if (e < M * NFI) {
+          const int k = e / NFI, f = e - k * NFI;
+          sy[u] = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m) + f);
+          as[u] = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m + a.fs_c) + f);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kLd; ++u) {
+        const int e = e0 + u * kNlW64Threads;
+        if (e < M * NFI) {
+          const int k = e / NFI, f = e - k * NFI;
+          buf[f * S + pad16(k)] = {sy[u].x + hs * as[u].x, sy[u].y + hs * as[u].y};
+        }
+      }
     }
   } else {
     const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
-    for (int e = tid; e < M * NFI; e += kNlW64Threads) {
-      const int k = e / NFI, f = e - k * NFI;
-      const double2 x = __ldg(&Fr[k * a.f_m + f]);
-      buf[f * S + pad16(k)] = {x.x, x.y};
+    for (int e0 = tid; e0 < M * NFI; e0 += kLd * kNlW64Threads) {
+      double2 x[kLd];
+#pragma unroll
+      for (int u = 0; u < kLd; ++u) {
+        const int e = e0 + u * kNlW64Threads;
+        if (e < M * NFI) x[u] = __ldg(&Fr[(e / NFI) * a.f_m + e % NFI]);
+      }
+#pragma unroll
+      for (int u = 0; u < kLd; ++u) {
+        const int e = e0 + u * kNlW64Threads;
+        if (e < M * NFI) buf[(e % NFI) * S + pad16(e / NFI)] = {x[u].x, x[u].y};
+      }
     }
   }
   for (int e = tid; e < NFI * (H - M); e += kNlW64Threads) {
