@@ -25,15 +25,23 @@ __device__ __forceinline__ int oz_exponent(double mx) {
   return e;
 }
 
-// Six signed digits of v at scale 2^e (|v| < 2^e): d_i in [-64, 64].
+// Six signed digits of v at scale 2^e (|v| < 2^e): Y = rint(v 2^(41 - e)),
+// |Y| <= 2^41, written in balanced base 128, Y = sum_i d_i 2^(7 (5 - i)) with
+// d_0 in [-64, 64] and d_1..d_5 in [-64, 63], so v = 2^(e - 6) sum_i d_i 2^(-7 i)
+// to 2^(e - 42).  Adding O = 64 sum_i 2^(7 (5 - i)) makes every base-128 digit
+// of Y + O non-negative (d_i = digit_i(Y + O) - 64), so the six digits come
+// from independent shifts of one integer.
+constexpr unsigned long long kOzDigitOffset =
+    64ull * ((1ull << 35) + (1ull << 28) + (1ull << 21) + (1ull << 14) + (1ull << 7) + 1ull);
+
+__device__ __forceinline__ double oz_scale(double v, int s);
+
 __device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzDigits]) {
-  double y = ldexp(v, 6 - e);
+  const long long Y = __double2ll_rn(oz_scale(v, 41 - e));
+  const unsigned long long U = (unsigned long long)Y + kOzDigitOffset;
+  d[0] = (int8_t)((int)(U >> 35) - 64);
 #pragma unroll
-  for (int i = 0; i < kOzDigits; ++i) {
-    const double q = rint(y);
-    d[i] = (int8_t)(int)q;
-    y = (y - q) * 128.0;
-  }
+  for (int i = 1; i < kOzDigits; ++i) d[i] = (int8_t)((int)((U >> (7 * (5 - i))) & 127u) - 64);
 }
 
 // Instruction descriptor: kind::i8, s8 x s8 -> s32, A and B K-major.
@@ -457,7 +465,7 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
                                              a.z.syn_prefix[mc * 2 + combo], c, q) * kOzAChunk;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-#pragma unroll
+#pragma unroll 1
       for (int half = 0; half < 2; ++half) {
         uint32_t w[kOzDigits][4];
 #pragma unroll
@@ -484,10 +492,11 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
 // Persistent synthesis GEMM: one CTA per SM walks the items (tile, combo,
 // theta tile, m) with a stride of gridDim.x.  Warp 0 lane 0 bulk-copies the A
 // digit chunk and the table digit chunk of every K step into a ring, warp 1
-// lane 0 issues the 21 digit-pair MMAs per step into the six group
-// accumulators (TMEM columns 64 g) and commits when the item's K loop ends,
-// warps 2-5 drain the accumulators (one TMEM lane per thread), form the FP64
-// values and store them into Fs, and hand the accumulators back.
+// lane 0 issues the digit-pair MMAs of every step (oz_mma_chunk: eight MMAs
+// covering the 21 pairs) into the six group accumulators (TMEM columns 64 g)
+// and commits when the item's K loop ends, warps 2-9 drain the accumulators
+// (one TMEM lane and 32 columns per thread), form the FP64 values and store
+// them into Fs, and hand the accumulators back.
 constexpr int kOzStages = 4;
 constexpr int kOzSynEpiWarps = 8;  // two per TMEM lane quarter, 32 columns each
 constexpr int kOzSynThreads = 64 + 32 * kOzSynEpiWarps;
