@@ -82,7 +82,8 @@ def split_mma_flops(plan, n_r):
 
 def ozaki_mma_ops(plan, n_r, nfi=13, nfo=9):
     """Dense int8 tensor-pipe operations the digit-split kernels issue per stage:
-    21 digit-pair MMAs per K chunk of 32, M = 128 rows per tile, N = 64 theta rows
+    21 digit-pair products per K chunk of 32 (issued as eight or six MMAs with the table
+    planes stacked along N), M = 128 rows per tile, N = 64 theta rows
     (synthesis) or 32 l rows (analysis), padded tiles included."""
     kk, rows = 32, 128
     nhs = plan.nhs
@@ -192,9 +193,12 @@ class ClockSampler:
 # DRAM bytes (read + write) of one launch of the phi-stage kernel from an ncu
 # full-set capture of the same kernel at l_max = 255, n_r = 17, per Fourier row moved (13 fields x n_r in, 9 fields x (n_r - 2) out); traffic grows
 # in proportion to the rows, so the full-size launch is scaled by its row count.
-NCU_PHI_TRAFFIC = {"split": (230.161408e6 + 104.267520e6) / (13 * 17 + 9 * 15)}
+NCU_PHI_TRAFFIC = {"split": (230.161408e6 + 104.267520e6) / (13 * 17 + 9 * 15),
+                   # the FP64 phi kernel of the digit-split stage (k_nl_bouss_w64)
+                   "ozaki": (386.640640e6 + 213.144320e6) / (13 * 17 + 9 * 15)}
 # warp instructions of the same launch (smsp__inst_executed.sum), per Fourier row
-NCU_PHI_INST = {"split": 184287744.0 / (13 * 17 + 9 * 15)}
+NCU_PHI_INST = {"split": 184287744.0 / (13 * 17 + 9 * 15),
+                "ozaki": 209892096.0 / (13 * 17 + 9 * 15)}
 
 
 def measured_peaks():
@@ -753,8 +757,9 @@ def run_step(args, rank, world):
         ach = fl / (parts[dom] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TOP/s",
                 "frac": ach / pk, "traffic": None, "kernel": dom,
-                "flops": "dense int8 MMA operations issued (21 digit pairs per K chunk, "
-                         "padded tiles; the pack kernel's time is included in the part)",
+                "flops": "dense int8 MMA operations issued (21 digit pairs per K chunk in "
+                         "eight stacked MMAs, padded tiles; the pack kernel's time is included "
+                         "in the part)",
                 "peak_source": f"2 x {src} bf16_tflops (burst): B200's dense int8 rate is "
                                "twice its bf16 rate"}
     else:
