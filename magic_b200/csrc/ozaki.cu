@@ -492,29 +492,34 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
 // Persistent synthesis GEMM: one CTA per SM walks the items (tile, combo,
 // theta tile, m) with a stride of gridDim.x.  Warp 0 lane 0 bulk-copies the A
 // digit chunk and the table digit chunk of every K step into a ring, warp 1
-// lane 0 issues the digit-pair MMAs of every step (oz_mma_chunk: eight MMAs
-// covering the 21 pairs) into the six group accumulators (TMEM columns 64 g)
-// and commits when the item's K loop ends, warps 2-9 drain the accumulators
-// (one TMEM lane and 32 columns per thread), form the FP64 values and store
-// them into Fs, and hand the accumulators back.
-constexpr int kOzStages = 4;
-constexpr int kOzSynEpiWarps = 8;  // two per TMEM lane quarter, 32 columns each
+// lane 0 issues the digit-pair MMAs of every step (oz_mma_chunk: six MMAs
+// covering the 21 pairs) into the six group accumulators (TMEM columns 32 g)
+// and commits when the item's K loop ends, warps 2-5 drain the accumulators
+// (one TMEM lane and the item's 32 columns per thread), form the FP64 values
+// and store them into Fs, and hand the accumulators back.
+constexpr int kOzStages = 4;     // analysis ring
+// Synthesis: two CTAs per SM, each with 256 TMEM columns (six groups of
+// kOzSynN = 32) and a 3-stage ring, so that one CTA's MMAs run while the
+// other drains its accumulators.
+constexpr int kOzSynStages = 3;
+constexpr int kOzSynEpiWarps = 4;  // one per TMEM lane quarter, all 32 columns
 constexpr int kOzSynThreads = 64 + 32 * kOzSynEpiWarps;
+constexpr int kOzSynTmemCols = 256;
 
 struct OzSynSmem {
   static constexpr uint32_t stage_bytes = kOzAChunk + kOzSynBChunk;
-  static constexpr uint32_t bar_off = kOzStages * stage_bytes;
+  static constexpr uint32_t bar_off = kOzSynStages * stage_bytes;
   // full/empty per stage, tfull, tempty, done, tmem slot, abort flag
-  static constexpr size_t total = bar_off + 8 * (2 * kOzStages + 3) + 16;
+  static constexpr size_t total = bar_off + 8 * (2 * kOzSynStages + 3) + 16;
 };
 
-__global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a) {
+__global__ void __launch_bounds__(kOzSynThreads, 2) k_oz_synth_gemm(OzSynArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   const Tables& t = a.t;
   const OzTables& z = a.z;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + OzSynSmem::bar_off);
-  uint64_t* empty = full + kOzStages;
-  uint64_t* tfull = empty + kOzStages;
+  uint64_t* empty = full + kOzSynStages;
+  uint64_t* tfull = empty + kOzSynStages;
   uint64_t* tempty = tfull + 1;
   uint64_t* done = tempty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
@@ -542,7 +547,7 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
   };
 
   if (tid == 0) {
-    for (int s = 0; s < kOzStages; ++s) {
+    for (int s = 0; s < kOzSynStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -552,7 +557,7 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 1) tmem_alloc(tmem_slot, 512);
+  if (warp == 1) tmem_alloc(tmem_slot, kOzSynTmemCols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -575,9 +580,9 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
         for (int c = 0; c < nch && ok; ++c) {
           for (int q = 0; q < 2; ++q) {
             if (c >= it.nch_t[q]) continue;
-            const int s = g % kOzStages;
-            if (g >= kOzStages &&
-                !mbar_wait(&empty[s], ((g / kOzStages) - 1) & 1, abort_flag, a.err, 23)) {
+            const int s = g % kOzSynStages;
+            if (g >= kOzSynStages &&
+                !mbar_wait(&empty[s], ((g / kOzSynStages) - 1) & 1, abort_flag, a.err, 23)) {
               ok = false;
               break;
             }
@@ -589,8 +594,8 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
           }
         }
       }
-      for (int k = max(0, g - kOzStages); k < g; ++k)
-        mbar_drain(&full[k % kOzStages], (k / kOzStages) & 1);
+      for (int k = max(0, g - kOzSynStages); k < g; ++k)
+        mbar_drain(&full[k % kOzSynStages], (k / kOzSynStages) & 1);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -605,8 +610,8 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
         for (int c = 0; c < nch && ok; ++c) {
           for (int q = 0; q < 2; ++q) {
             if (c >= it.nch_t[q]) continue;
-            const int s = g % kOzStages;
-            if (!mbar_wait(&full[s], (g / kOzStages) & 1, abort_flag, a.err, 24)) {
+            const int s = g % kOzSynStages;
+            if (!mbar_wait(&full[s], (g / kOzSynStages) & 1, abort_flag, a.err, 24)) {
               ok = false;
               break;
             }
@@ -623,8 +628,8 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
       umma_commit(done);
     }
   } else {
-    // epilogue: warps 2-9; warp w owns TMEM lane quarter w % 4 and the 32
-    // accumulator columns of half (w - 2) / 4
+    // epilogue: warps 2-5; warp w owns TMEM lane quarter w % 4 and the 32
+    // accumulator columns of half (w - 2) / 4 (0: all of them)
     const int quarter = warp & 3, half = (warp - 2) >> 2;
     const int R0 = quarter * 32 + lane;
     int n = 0;
@@ -664,7 +669,7 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tbase, 512);
+    tmem_dealloc(tbase, kOzSynTmemCols);
   }
 }
 
@@ -688,7 +693,7 @@ int launch_oz_synth(const OzSynArgs& a, cudaStream_t st) {
   MT_CHECK_CUDA(cudaGetDevice(&dev));
   MT_CHECK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int nitems = ntiles * 2 * a.z.nthtile * a.t.n_m;
-  k_oz_synth_gemm<<<std::min(nitems, nsm), kOzSynThreads, sm, st>>>(a);
+  k_oz_synth_gemm<<<std::min(nitems, 2 * nsm), kOzSynThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

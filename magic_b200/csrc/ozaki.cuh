@@ -34,7 +34,7 @@ constexpr int kOzDigits = 6;  // int8 digits per operand value
 constexpr int kOzGroups = 6;  // digit-weight groups kept: i + j <= 5
 constexpr int kOzK = 32;      // K per MMA and per operand chunk
 constexpr int kOzRows = 128;  // MMA M: data rows per tile
-constexpr int kOzSynN = 64;   // theta rows per synthesis tile (MMA N)
+constexpr int kOzSynN = 32;   // theta rows per synthesis tile (MMA N per table digit plane)
 constexpr int kOzAnaN = 32;   // l rows per analysis tile (MMA N)
 constexpr uint32_t kOzAPlane = kOzRows * kOzK;               // 4 KiB
 constexpr uint32_t kOzAChunk = kOzDigits * kOzAPlane;        // 24 KiB
