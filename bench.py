@@ -878,7 +878,7 @@ def run_serve(args, rank, world):
             r["group_steps"] = sum(g.launches for g in bsrv.groups.values())
             batched[f"{prec}_{name}"] = r
         torch.cuda.empty_cache()
-    finish, busy = 0.0, 0.0
+    finish, busy, steps_s, step_ms = 0.0, 0.0, 0.0, []
     for s in specs:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -893,11 +893,44 @@ def run_serve(args, rank, world):
             st.step()
         e1.record()
         torch.cuda.synchronize()
-        run_s = build + e0.elapsed_time(e1) / 1e3
+        dev_s = e0.elapsed_time(e1) / 1e3
+        run_s = build + dev_s
         finish = max(finish, s.arrival) + run_s
         busy += run_s
+        steps_s += dev_s
+        step_ms.append(1e3 * dev_s / s.n_steps)
         del st
     torch.cuda.empty_cache()
+    # accuracy of the serving precisions over whole runs: one spec of each l_max
+    # of the stream (its Ek, Ra, n_r, seed), all steps, against the same run with
+    # the FP64 stage: largest field difference over the largest field value, and
+    # the largest relative difference of the kinetic and magnetic energies
+    accuracy = {}
+    seen = {}
+    for s in specs:
+        seen.setdefault(s.l_max, s)
+    for l_max, s in sorted(seen.items()):
+        runs = {}
+        for prec in ("fp64", "split", "ozaki"):
+            st = BoussinesqStep(s.l_max, s.n_r, ek=s.ek, ra=s.ra, pr=s.pr, prmag=s.prmag,
+                                dt=s.dt, precision=prec, device=dev,
+                                radial_scheme=s.radial_scheme)
+            st.init_random(seed=s.seed, amp=s.amp)
+            for _ in range(s.n_steps):
+                st.step()
+            torch.cuda.synchronize()
+            ek, em = st.energies()
+            runs[prec] = ({k: st.f[k].clone() for k in ("w", "z", "s", "b", "aj")},
+                          [ek[0], ek[1], em[0], em[1]])
+            del st
+        ref_f, ref_e = runs["fp64"]
+        for prec in ("split", "ozaki"):
+            f, e = runs[prec]
+            fe = max(float((f[k] - ref_f[k]).abs().max() / ref_f[k].abs().max()) for k in f)
+            ee = max(abs(x - y) / abs(y) for x, y in zip(e, ref_e) if y != 0.0)
+            accuracy[f"{prec}_l{l_max}_n{s.n_r}"] = {"fields": fe, "energies": ee,
+                                                     "steps": s.n_steps}
+        torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps({
             "metric": "ensemble aggregate steps/s (continuous batching), 1 B200",
@@ -908,7 +941,11 @@ def run_serve(args, rank, world):
             "capacity": {"steps_per_s": sat["steps_per_s"], "p50_ms": sat["p50_ms"],
                          "p99_ms": sat["p99_ms"], "wall_s": sat["wall_s"]},
             "fp64_one_at_a_time": {"steps_per_s": rep["steps"] / finish, "wall_s": finish,
-                                   "capacity_steps_per_s": rep["steps"] / busy},
+                                   "capacity_steps_per_s": rep["steps"] / busy,
+                                   "steps_per_s_without_build": rep["steps"] / steps_s,
+                                   "run_mean_step_ms_p50": statistics.median(step_ms),
+                                   "run_mean_step_ms_max": max(step_ms)},
+            "accuracy_vs_fp64": accuracy,
             "kernels_per_run_step": 12,
             "batched": batched,
             "dtype": "bf16x3/f32 stage, f64 rest", "data": "synthetic",

@@ -62,17 +62,22 @@ def poisson_stream(n_runs=64, rate=4.0, seed=0, n_steps=200, precision="split",
                    radial_scheme="chebyshev"):
     """Seeded run stream: exponential inter-arrival times of mean 1 / rate,
     l_max and n_r uniform over the choices, Ekman log-uniform in [1e-4, 1e-3],
-    Rayleigh log-uniform in [1e5, 1e6], Pr = 1, Pm = 5, perturbation 1e-5."""
+    Rayleigh log-uniform in [1e5, 1e6], Pr = 1, Pm = 5, perturbation 1e-5.  The
+    time step is the largest of 1e-5, 2e-5, 5e-5, 1e-4 not above Ek / 10: the
+    Coriolis term is explicit in the CNAB2 scheme (get_td), so a stable dt
+    shrinks with Ek (1e-4 at Ek = 1e-3, as in the reference's shell case), and
+    runs of one dt share their solve operators."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(n_runs):
         t += rng.exponential(1.0 / rate)
-        out.append(RunSpec(run_id=i, l_max=int(rng.choice(l_choices)),
-                           n_r=int(rng.choice(nr_choices)),
-                           ek=float(10.0 ** rng.uniform(-4.0, -3.0)),
-                           ra=float(10.0 ** rng.uniform(5.0, 6.0)), n_steps=n_steps,
-                           seed=1000 + i, arrival=t, precision=precision,
+        l_max, n_r = int(rng.choice(l_choices)), int(rng.choice(nr_choices))
+        ek = float(10.0 ** rng.uniform(-4.0, -3.0))
+        ra = float(10.0 ** rng.uniform(5.0, 6.0))
+        dt = max([d for d in (1e-5, 2e-5, 5e-5, 1e-4) if d <= ek / 10.0] or [1e-5])
+        out.append(RunSpec(run_id=i, l_max=l_max, n_r=n_r, ek=ek, ra=ra, dt=dt,
+                           n_steps=n_steps, seed=1000 + i, arrival=t, precision=precision,
                            radial_scheme=radial_scheme))
     return out
 
