@@ -83,19 +83,55 @@ __device__ __forceinline__ cplx<double> r2c_post_d(cplx<double> Zk, cplx<double>
   return {0.5 * (F.x + t.y), 0.5 * (F.y - t.x)};
 }
 
-// In-place transform of one row (padded layout) by the calling warp.
-// twH[n] = exp(-2 pi i n / H), twN[k] = exp(-2 pi i k / (2 H)), n, k < H.
+// Twiddle tables of the passes in shared memory, each indexed by the
+// butterfly's position inside its span so that consecutive lanes read
+// consecutive entries (with w = exp(-2 pi i / H)):
+//   t2[r-1][jm] = w^(8 r jm), jm < Q;  t3[r-1][jm] = w^(2 r jm), jm < 4 Q;
+//   t4[j] = w^j, j < 16 Q;  twN[k] = exp(-2 pi i k / (2 H)), k < H.
+template <int Q>
+struct W64Tw {
+  const cplx<double>* t2;
+  const cplx<double>* t3;
+  const cplx<double>* t4;
+  const cplx<double>* twN;
+  static constexpr int kEntries = 3 * Q + 12 * Q + 16 * Q + 32 * Q;
+};
+
+// Fill the tables from the plan's exp(-2 pi i n / (2 H)) table (n < 2 H) at
+// `sm` (kEntries complex values); threads tid, tid + T, ... of the CTA.
+template <int Q>
+__device__ __forceinline__ W64Tw<Q> w64_twiddles(cplx<double>* sm, const double2* tw2h, int tid,
+                                                 int T) {
+  constexpr int H = 32 * Q;
+  cplx<double>* t2 = sm;
+  cplx<double>* t3 = t2 + 3 * Q;
+  cplx<double>* t4 = t3 + 12 * Q;
+  cplx<double>* tn = t4 + 16 * Q;
+  auto wH = [&](int e) {  // w^e = exp(-2 pi i e / H)
+    const double2 v = __ldg(&tw2h[(2 * e) % (2 * H)]);
+    return cplx<double>{v.x, v.y};
+  };
+  for (int i = tid; i < 3 * Q; i += T) t2[i] = wH(8 * (i / Q + 1) * (i % Q));
+  for (int i = tid; i < 12 * Q; i += T) t3[i] = wH(2 * (i / (4 * Q) + 1) * (i % (4 * Q)));
+  for (int i = tid; i < 16 * Q; i += T) t4[i] = wH(i);
+  for (int i = tid; i < H; i += T) {
+    const double2 v = __ldg(&tw2h[i]);
+    tn[i] = {v.x, v.y};
+  }
+  return W64Tw<Q>{t2, t3, t4, tn};
+}
+
+// In-place transform of one row (padded layout) by the calling warp, with the
+// twiddle tables of w64_twiddles.
 // PRE: the row holds the half spectrum X[0..H) of a real row of length 2 H and
 // the transform input is Z[k] = c2r_pre(X[k], X[H - k]) (Im X[0] dropped,
 // X[H] = 0); the result z[n] then carries x[2 n] + i x[2 n + 1].
 template <int Q, bool INV, bool PRE>
-__device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane,
-                                            const cplx<double>* __restrict__ twH,
-                                            const cplx<double>* __restrict__ twN) {
+__device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W64Tw<Q>& T) {
   constexpr int H = 32 * Q;
   static_assert(Q % 4 == 0, "radix-4 passes need Q / 4 butterflies per lane");
-  auto tw = [&](int e) {  // exp(-+ 2 pi i e / H), 0 <= e < H
-    cplx<double> w = twH[e];
+  const cplx<double>* __restrict__ twN = T.twN;
+  auto cj = [](cplx<double> w) {  // the inverse transform's conjugate twiddle
     if (INV) w.y = -w.y;
     return w;
   };
@@ -132,7 +168,7 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane,
     const int j = lane + 32 * it, jm = j % Q;
     cplx<double> u[4] = {v[4 * it], v[4 * it + 1], v[4 * it + 2], v[4 * it + 3]};
 #pragma unroll
-    for (int r = 1; r < 4; ++r) u[r] = cmul(u[r], tw(8 * r * jm));
+    for (int r = 1; r < 4; ++r) u[r] = cmul(u[r], cj(T.t2[(r - 1) * Q + jm]));
     dft_small<4, INV>(u);
     const int d = (j - jm) * 4 + jm;
 #pragma unroll
@@ -150,7 +186,7 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane,
     const int j = lane + 32 * it, jm = j % (4 * Q);
     cplx<double> u[4] = {v[4 * it], v[4 * it + 1], v[4 * it + 2], v[4 * it + 3]};
 #pragma unroll
-    for (int r = 1; r < 4; ++r) u[r] = cmul(u[r], tw(2 * r * jm));
+    for (int r = 1; r < 4; ++r) u[r] = cmul(u[r], cj(T.t3[(r - 1) * 4 * Q + jm]));
     dft_small<4, INV>(u);
     const int d = (j - jm) * 4 + jm;
 #pragma unroll
@@ -162,7 +198,7 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane,
 #pragma unroll
   for (int it = 0; it < Q / 2; ++it) {
     const int j = lane + 32 * it;
-    cplx<double> u[2] = {row[pad16(j)], cmul(row[pad16(j + 16 * Q)], tw(j))};
+    cplx<double> u[2] = {row[pad16(j)], cmul(row[pad16(j + 16 * Q)], cj(T.t4[j]))};
     dft_small<2, INV>(u);
     row[pad16(j)] = u[0];
     row[pad16(j + 16 * Q)] = u[1];

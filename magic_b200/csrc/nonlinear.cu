@@ -248,17 +248,13 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   extern __shared__ double smem[];
   __shared__ double red[32];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);  // NB rows, S apart
-  cplx<double>* twH = buf + BF::NB * S;                       // exp(-2 pi i n / H)
-  cplx<double>* twN = twH + H;                                // exp(-2 pi i k / (2 H))
+  cplx<double>* twsm = buf + BF::NB * S;                      // W64Tw<Q> tables
   const Tables& t = a.t;
   const int M = t.n_m;
   const int row = blockIdx.x, r = blockIdx.y;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int i = tid; i < H; i += kNlW64Threads) {
-    const double2 wn = __ldg(&t.twiddle[i]), wh = __ldg(&t.twiddle[2 * i]);
-    twN[i] = {wn.x, wn.y};
-    twH[i] = {wh.x, wh.y};
-  }
+  const W64Tw<Q> tw = w64_twiddles<Q>(twsm, t.twiddle, tid, kNlW64Threads);
+  const cplx<double>* twN = tw.twN;
   // half spectra of the NFI fields; wavenumbers k >= n_m are zero
   // (kLd elements per thread are loaded before any is stored, so their HBM
   // latencies overlap)
@@ -307,7 +303,7 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
     buf[f * S + pad16(k)] = {0.0, 0.0};
   }
   __syncthreads();
-  for (int f = warp; f < NFI; f += NW) w64_row_fft<Q, true, true>(buf + f * S, lane, twH, twN);
+  for (int f = warp; f < NFI; f += NW) w64_row_fft<Q, true, true>(buf + f * S, lane, tw);
   __syncthreads();
 
   const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
@@ -360,7 +356,7 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   if (tid == 0) atomic_max_pos(&a.vh2max[r], vmh);
   if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
   __syncthreads();
-  for (int f = warp; f < NFO; f += NW) w64_row_fft<Q, false, false>(buf + f * S, lane, twH, twN);
+  for (int f = warp; f < NFO; f += NW) w64_row_fft<Q, false, false>(buf + f * S, lane, tw);
   __syncthreads();
   const double ws = t.wq[row] / (2 * H), wv = t.wq_v[row] / (2 * H);
   double2* Gr = SPLIT_IO
@@ -383,7 +379,7 @@ template <bool MAG, bool CHEM, bool SPLIT_IO, int Q>
 static int launch_nl_bouss_w64(const NlBoussArgs& a, cudaStream_t st) {
   using BF = BoussFields<MAG, CHEM>;
   constexpr int H = 32 * Q;
-  const size_t sm = ((size_t)BF::NB * padded_len(H) + 2 * H) * sizeof(double2);
+  const size_t sm = ((size_t)BF::NB * padded_len(H) + W64Tw<Q>::kEntries) * sizeof(double2);
   auto kern = k_nl_bouss_w64<MAG, CHEM, SPLIT_IO, Q>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
