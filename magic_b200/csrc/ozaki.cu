@@ -34,10 +34,10 @@ __device__ __forceinline__ int oz_exponent(double mx) {
 constexpr unsigned long long kOzDigitOffset =
     64ull * ((1ull << 35) + (1ull << 28) + (1ull << 21) + (1ull << 14) + (1ull << 7) + 1ull);
 
-__device__ __forceinline__ double oz_scale(double v, int s);
+__device__ __forceinline__ double oz_scale_up(double v, int s);
 
 __device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzDigits]) {
-  const long long Y = __double2ll_rn(oz_scale(v, 41 - e));
+  const long long Y = __double2ll_rn(oz_scale_up(v, 41 - e));
   const unsigned long long U = (unsigned long long)Y + kOzDigitOffset;
   d[0] = (int8_t)((int)(U >> 35) - 64);
 #pragma unroll
@@ -75,21 +75,44 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-// v 2^s: one multiplication by the exact power of two when 2^s is a normal
-// double (the product rounds once, as ldexp does), ldexp otherwise.
-__device__ __forceinline__ double oz_scale(double v, int s) {
-  if (s >= -1022 && s <= 1023) return v * __longlong_as_double((long long)(s + 1023) << 52);
-  return ldexp(v, s);
+// v 2^s rounded once, as ldexp rounds it, without a library call.  For
+// -1022 <= s <= 1023 it is one multiplication by the exact power of two.  The
+// epilogues' exponents never exceed 1023; below -1022, v 2^(s + 1022) is exact
+// (v, an integer sum below 2^59, is far from the underflow range) and the
+// multiplication by 2^-1022 rounds once into the subnormals (for s < -2044 the
+// result is 0 either way).  The packs' exponents (41 - e for |v| < 2^e) are
+// at least -982, and exceed 1023 only for values below 2^-982, scaled by two
+// exact multiplications.
+__device__ __forceinline__ double oz_pow2(int s) {  // s in [-1022, 1023]
+  return __longlong_as_double((long long)(s + 1023) << 52);
+}
+
+__device__ __forceinline__ double oz_scale(double v, int s) {  // s <= 1023
+  if (s >= -1022) return v * oz_pow2(s);
+  return (v * oz_pow2(max(s + 1022, -1022))) * 0x1p-1022;
+}
+
+__device__ __forceinline__ double oz_scale_up(double v, int s) {  // s >= -1022
+  if (s <= 1023) return v * oz_pow2(s);
+  return (v * oz_pow2(min(s - 1023, 1023))) * 0x1p1023;
+}
+
+// Exact int32 -> double without a conversion instruction: the double whose
+// high word is 0x43300000 and low word w + 2^31 is 2^52 + w + 2^31.
+__device__ __forceinline__ double oz_i2d(uint32_t w) {
+  return __hiloint2double(0x43300000, (int)(w ^ 0x80000000u)) - 4503601774854144.0;
 }
 
 // 2^35 sum_g 2^(-7 g) C_g for one accumulator column from raw TMEM words,
-// exact in int64 (|C_g| < 2^23, so the sum stays below 2^59), then rounded once
-// to FP64; callers scale by 2^(e - 35).
+// rounded once to FP64: the halves P1 = (C0 2^7 + C1) 2^7 + C2 and
+// P2 = (C3 2^7 + C4) 2^7 + C5 are integers below 2^38, exact in FP64, and the
+// sum P1 2^21 + P2 (below 2^59) is rounded by the final fma alone; callers
+// scale by 2^(e - 35).
 __device__ __forceinline__ double oz_combine_u(const uint32_t (&c)[kOzGroups][16], int i) {
-  long long v = (int)c[0][i];
-#pragma unroll
-  for (int g = 1; g < kOzGroups; ++g) v = v * 128 + (int)c[g][i];
-  return (double)v;
+  static_assert(kOzGroups == 6, "two exact halves of three groups each");
+  const double p1 = fma(fma(oz_i2d(c[0][i]), 128.0, oz_i2d(c[1][i])), 128.0, oz_i2d(c[2][i]));
+  const double p2 = fma(fma(oz_i2d(c[3][i]), 128.0, oz_i2d(c[4][i])), 128.0, oz_i2d(c[5][i]));
+  return fma(p1, 2097152.0, p2);
 }
 
 // Named barrier over `n` threads that also ANDs a predicate across them, so

@@ -16,18 +16,58 @@ from oracle import grid as og
 D, G = 6, 6  # digits per operand, weight groups kept (i + j <= 5)
 
 
+OFFSET = 64 * sum(1 << (7 * (5 - i)) for i in range(D))  # 64 sum_i 2^(7 (5 - i))
+
+
 def digits(x, axis):
-    """(digit planes, exponents): x = 2^(e - 6) sum_i d_i 2^(-7 i) + O(2^(e - 42)),
-    e per row (axis = 1) or column (axis = 0), |x| < 2^e."""
+    """(digit planes, exponents) as the pack kernels form them: Y = rint(x 2^(41 - e))
+    (|Y| <= 2^41), written in balanced base 128 through the independent shifts of
+    Y + OFFSET (each base-128 digit minus 64), so x = 2^(e - 6) sum_i d_i 2^(-7 i)
+    to 2^(e - 42); e per row (axis = 1) or column (axis = 0), |x| < 2^e."""
     mx = np.abs(x).max(axis=axis, keepdims=True)
     e = np.where(mx > 0, np.frexp(mx)[1], 0)
-    y = np.ldexp(x, 6 - e)
-    ds = []
-    for _ in range(D):
-        q = np.rint(y)
-        ds.append(q.astype(np.int64))
-        y = (y - q) * 128.0
+    Y = np.rint(np.ldexp(x, 41 - e)).astype(np.int64)
+    U = Y + OFFSET
+    ds = [(U >> 35) - 64] + [((U >> (7 * (5 - i))) & 127) - 64 for i in range(1, D)]
     return ds, e
+
+
+def _pow2(k):
+    import struct
+
+    return struct.unpack("<d", struct.pack("<q", (k + 1023) << 52))[0]
+
+
+def oz_scale(v, s):
+    """v 2^s as the epilogues compute it (s <= 1023), for Python floats."""
+    if s >= -1022:
+        return v * _pow2(s)
+    return (v * _pow2(max(s + 1022, -1022))) * 2.0 ** -1022
+
+
+def oz_scale_up(v, s):
+    """v 2^s as the packs compute it (s >= -1022)."""
+    if s <= 1023:
+        return v * _pow2(s)
+    return (v * _pow2(min(s - 1023, 1023))) * 2.0 ** 1023
+
+
+def test_scaling_rounds_like_ldexp():
+    """The kernels' power-of-two scaling equals ldexp (one rounding) over the
+    exponents they use: digit extraction of values down to the subnormals, and
+    the epilogue's integer sums below 2^59 scaled into the subnormal range."""
+    import math
+    import random
+
+    rnd = random.Random(0)
+    for _ in range(100000):
+        e = rnd.randint(-1073, 1023)
+        v = rnd.uniform(-1.0, 1.0) * 2.0 ** e
+        if v != 0.0:
+            s = 41 - math.frexp(v)[1]
+            assert oz_scale_up(v, s) == math.ldexp(v, s)
+        w, t = float(rnd.randint(-2 ** 59, 2 ** 59)), rnd.randint(-2200, 60)
+        assert oz_scale(w, t) == math.ldexp(w, t)
 
 
 def contract(A, B):
