@@ -83,7 +83,7 @@ def _inverse_ops(A, sch, zero_l0=False, identity_l0=False):
         M[0] = 0.0
     if sch.chebyshev:
         M[:, sch.n_cheb:, :] = 0.0
-        M = np.einsum("jk,lkn->ljn", _dct1(N), M)
+        M = np.matmul(_dct1(N)[None], M)
     return M
 
 
@@ -278,39 +278,41 @@ def wp_solve_operators(sch, l_max, wimp_lin0, hdif, prof, ktopv=2, kbotv=2):
     b = slice(1, N - 1)
     C2 = np.zeros((2 * N, 2 * N))
     C2[:N, :N] = C2[N:, N:] = _dct1(N)
+    # every degree at once: (l_max, 2N, 2N) for l = 1 .. l_max, broadcast over l
+    ls = np.arange(1, l_max + 1, dtype=np.float64)
+    dL = (ls * (ls + 1.0))[:, None, None]
+    hl = np.asarray(hdif, dtype=np.float64)[1:l_max + 1, None, None]
+    A = np.zeros((l_max, 2 * N, 2 * N))
+    A[:, b, :N] = rn * dL * or2[b] * (rMat[b] - wimp_lin0 * hl * visc[b] * (
+        d2rMat[b] + (2.0 * dLv[b] - beta[b] / 3.0) * drMat[b]
+        - (dL * or2[b] + 4.0 / 3.0 * (dLv[b] * beta[b] + (3.0 * dLv[b] + beta[b]) * or1[b]
+                                      + dbeta[b])) * rMat[b]))
+    A[:, b, N:] = rn * wimp_lin0 * (drMat[b] - beta[b] * rMat[b])
+    A[:, N + 1:2 * N - 1, :N] = rn * dL * or2[b] * (-drMat[b] - wimp_lin0 * hl * visc[b] * (
+        -d3rMat[b] + (beta[b] - dLv[b]) * d2rMat[b]
+        + (dL * or2[b] + dbeta[b] + dLv[b] * beta[b] + 2.0 * (dLv[b] + beta[b]) * or1[b])
+        * drMat[b]
+        - dL * or2[b] * (2.0 * or1[b] + dLv[b] + 2.0 / 3.0 * beta[b]) * rMat[b]))
+    A[:, N + 1:2 * N - 1, N:] = -rn * wimp_lin0 * dL * or2[b] * rMat[b]
+    A[:, 0, :N], A[:, N - 1, :N] = rn * rMat[0], rn * rMat[N - 1]
+    for row, i, k in ((N, 0, ktopv), (2 * N - 1, N - 1, kbotv)):
+        A[:, row, :N] = rn * ((d2rMat[i] - (2.0 * or1[i, 0] + beta[i, 0]) * drMat[i]) if k == 1
+                              else drMat[i])
+    if nc < N:
+        for row in (0, N - 1, N, 2 * N - 1):
+            A[:, row, nc:N] = 0.0
+            A[:, row, N + nc:] = 0.0
+    for c in (0, N - 1, N, 2 * N - 1):
+        A[:, :, c] *= sch.boundary_fac
+    fr = 1.0 / np.abs(A).max(axis=2)
+    A = fr[:, :, None] * A
+    fc = 1.0 / np.abs(A).max(axis=1)
+    Minv = fc[:, :, None] * np.linalg.inv(A * fc[:, None, :]) * fr[:, None, :]
+    if nc < N:
+        Minv[:, nc:N] = 0.0
+        Minv[:, N + nc:] = 0.0
     M = np.zeros((l_max + 1, 2 * N, 2 * N))
-    for l in range(1, l_max + 1):
-        dL, hl = float(l * (l + 1)), float(hdif[l])
-        A = np.zeros((2 * N, 2 * N))
-        A[b, :N] = rn * dL * or2[b] * (rMat[b] - wimp_lin0 * hl * visc[b] * (
-            d2rMat[b] + (2.0 * dLv[b] - beta[b] / 3.0) * drMat[b]
-            - (dL * or2[b] + 4.0 / 3.0 * (dLv[b] * beta[b] + (3.0 * dLv[b] + beta[b]) * or1[b]
-                                          + dbeta[b])) * rMat[b]))
-        A[b, N:] = rn * wimp_lin0 * (drMat[b] - beta[b] * rMat[b])
-        A[N + 1:2 * N - 1, :N] = rn * dL * or2[b] * (-drMat[b] - wimp_lin0 * hl * visc[b] * (
-            -d3rMat[b] + (beta[b] - dLv[b]) * d2rMat[b]
-            + (dL * or2[b] + dbeta[b] + dLv[b] * beta[b] + 2.0 * (dLv[b] + beta[b]) * or1[b])
-            * drMat[b]
-            - dL * or2[b] * (2.0 * or1[b] + dLv[b] + 2.0 / 3.0 * beta[b]) * rMat[b]))
-        A[N + 1:2 * N - 1, N:] = -rn * wimp_lin0 * dL * or2[b] * rMat[b]
-        A[0, :N], A[N - 1, :N] = rn * rMat[0], rn * rMat[N - 1]
-        for row, i, k in ((N, 0, ktopv), (2 * N - 1, N - 1, kbotv)):
-            A[row, :N] = rn * ((d2rMat[i] - (2.0 * or1[i, 0] + beta[i, 0]) * drMat[i]) if k == 1
-                               else drMat[i])
-        if nc < N:
-            for row in (0, N - 1, N, 2 * N - 1):
-                A[row, nc:N] = 0.0
-                A[row, N + nc:] = 0.0
-        for c in (0, N - 1, N, 2 * N - 1):
-            A[:, c] *= sch.boundary_fac
-        fr = 1.0 / np.abs(A).max(axis=1)
-        A = fr[:, None] * A
-        fc = 1.0 / np.abs(A).max(axis=0)
-        Minv = fc[:, None] * np.linalg.inv(A * fc[None, :]) * fr[None, :]
-        if nc < N:
-            Minv[nc:N] = 0.0
-            Minv[N + nc:] = 0.0
-        M[l] = C2 @ Minv
+    M[1:] = np.matmul(C2[None], Minv)
     return M
 
 

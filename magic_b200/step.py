@@ -222,18 +222,21 @@ class BoussinesqStep:
         equation's implicit operator applied to the fields)."""
         from .radial import get_ddr
 
-        g = torch.Generator(device="cpu").manual_seed(seed)
-        l = torch.as_tensor(self.plan.lm2l, dtype=torch.float64)
-        m0 = torch.as_tensor(self.plan.lm2m == 0)
+        # drawn on the device (a CPU draw of these arrays dominated the build of a
+        # run); the same seed gives the same fields on a given device type
+        dev = self.device
+        g = torch.Generator(device=dev).manual_seed(seed)
+        decay = (torch.as_tensor(self.plan.lm2l, dtype=torch.float64, device=dev) + 1.0) ** -2
+        m0 = torch.as_tensor(self.plan.lm2m == 0, device=dev)
         for k in ("w", "z", "s", "b", "aj"):
-            c = torch.randn(self.lm_max, self.n_r, dtype=_CD, generator=g) * amp
+            c = torch.randn(self.lm_max, self.n_r, dtype=_CD, generator=g, device=dev) * amp
             if k not in self.f:
                 continue
-            c *= ((l + 1.0) ** -2)[:, None]
+            c *= decay[:, None]
             c[m0] = c[m0].real.to(_CD)
             c[:, 0] = 0.0
             c[:, -1] = 0.0
-            self.f[k].copy_(c.to(self.device))
+            self.f[k].copy_(c)
         f, P, D1, D2 = self.f, self.prof, self.sch.D1, self.sch.D2
         second = {}
         for k, d1, d2 in (("w", "dw", "ddw"), ("z", "dz", None), ("s", "ds", None),
@@ -245,7 +248,8 @@ class BoussinesqStep:
             second[k] = a2
             if d2:
                 f[d2].copy_(a2)
-        dL = (l * (l + 1.0)).to(self.device)[:, None]
+        l = torch.as_tensor(self.plan.lm2l, dtype=torch.float64, device=self.device)
+        dL = (l * (l + 1.0))[:, None]
         row = lambda x: x[None, :]
         hd = self.hdif[self.plan_l()][:, None]
 
