@@ -168,14 +168,15 @@ __device__ __forceinline__ int fdiv(int n, float rcp) {
 
 // One out-of-place Stockham stage over `nrows` rows of length H: src rows at
 // src + row * stride, dst rows at dst + row * stride (padded indexing).
-// tw: shared-memory table exp(-2 pi i n / H), n < H.
+// tw: this stage's twiddles in shared memory, tw[(r - 1) Ns + jm] =
+// exp(-2 pi i r jm / (Ns RADIX)) (fft_twiddles_to_smem), so that threads with
+// consecutive butterflies read consecutive entries.
 template <int RADIX, bool INV, typename R>
 __device__ __forceinline__ void fft_stage(const cplx<R>* __restrict__ src, cplx<R>* __restrict__ dst,
                                           int nrows, int H, int stride, int Ns,
                                           const cplx<R>* __restrict__ tw) {
   const int nbr = H / RADIX;
   const int total = nrows * nbr;
-  const int twstep = H / (Ns * RADIX);
   const float rcp_nbr = 1.0f / (float)nbr, rcp_ns = 1.0f / (float)Ns;
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
     const int row = fdiv(b, rcp_nbr), j = b - row * nbr;
@@ -187,7 +188,7 @@ __device__ __forceinline__ void fft_stage(const cplx<R>* __restrict__ src, cplx<
     if (jm > 0) {
 #pragma unroll
       for (int r = 1; r < RADIX; ++r) {
-        cplx<R> w = tw[r * jm * twstep];
+        cplx<R> w = tw[(r - 1) * Ns + jm];
         if (INV) w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
@@ -205,8 +206,8 @@ constexpr int kFftRowBatch = 7;  // rows per pass through the scratch buffer
 
 // Full transform of `nrows` rows (in place), ping-ponging each batch of at
 // most kFftRowBatch rows through `scratch` (kFftRowBatch * stride values).
-// Radices come from the plan (product H, each of 2, 3, 4, 5, 8); tw is the
-// shared-memory table exp(-2 pi i n/H), n < H (fft_twiddles_to_smem).
+// Radices come from the plan (product H, each of 2, 3, 4, 5, 8); tw holds the
+// stages' twiddle tables one after another (fft_twiddles_to_smem, H - 1 values).
 template <bool INV, typename R>
 __device__ __forceinline__ void fft_rows(cplx<R>* buf, cplx<R>* scratch, int nrows, int H,
                                          int stride, const int* radix, int nstages,
@@ -215,16 +216,18 @@ __device__ __forceinline__ void fft_rows(cplx<R>* buf, cplx<R>* scratch, int nro
     cplx<R>* a = buf + r0 * stride;
     cplx<R>* b = scratch;
     const int nr = min(kFftRowBatch, nrows - r0);
-    int Ns = 1;
+    int Ns = 1, off = 0;
     for (int s = 0; s < nstages; ++s) {
       int rad = radix[s];
+      const cplx<R>* tws = tw + off;
       switch (rad) {
-        case 8: fft_stage<8, INV>(a, b, nr, H, stride, Ns, tw); break;
-        case 4: fft_stage<4, INV>(a, b, nr, H, stride, Ns, tw); break;
-        case 3: fft_stage<3, INV>(a, b, nr, H, stride, Ns, tw); break;
-        case 2: fft_stage<2, INV>(a, b, nr, H, stride, Ns, tw); break;
-        default: fft_stage<5, INV>(a, b, nr, H, stride, Ns, tw); break;
+        case 8: fft_stage<8, INV>(a, b, nr, H, stride, Ns, tws); break;
+        case 4: fft_stage<4, INV>(a, b, nr, H, stride, Ns, tws); break;
+        case 3: fft_stage<3, INV>(a, b, nr, H, stride, Ns, tws); break;
+        case 2: fft_stage<2, INV>(a, b, nr, H, stride, Ns, tws); break;
+        default: fft_stage<5, INV>(a, b, nr, H, stride, Ns, tws); break;
       }
+      off += (rad - 1) * Ns;
       Ns *= rad;
       cplx<R>* t = a;
       a = b;
@@ -238,13 +241,25 @@ __device__ __forceinline__ void fft_rows(cplx<R>* buf, cplx<R>* scratch, int nro
   }
 }
 
-// H-point twiddles exp(-2 pi i n/H) = tw_N[2n] into shared memory (caller syncs).
+// The stages' twiddle tables of fft_rows into shared memory, one after another
+// (H - 1 values in all): stage s of radix R and span Ns (the product of the
+// earlier radices) gets exp(-2 pi i r jm / (Ns R)) at (r - 1) Ns + jm, r < R,
+// jm < Ns, read from the plan's table tw_N[n] = exp(-2 pi i n / (2 H)) at
+// n = 2 r jm H / (Ns R).  Caller syncs.
 template <typename R>
 __device__ __forceinline__ void fft_twiddles_to_smem(cplx<R>* tws, int H,
-                                                     const double2* __restrict__ tw_N) {
-  for (int n = threadIdx.x; n < H; n += blockDim.x) {
-    double2 w = __ldg(&tw_N[2 * n]);
-    tws[n] = {(R)w.x, (R)w.y};
+                                                     const double2* __restrict__ tw_N,
+                                                     const int* radix, int nstages) {
+  int Ns = 1, off = 0;
+  for (int s = 0; s < nstages; ++s) {
+    const int rad = radix[s], n = (rad - 1) * Ns, step = H / (Ns * rad);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int r = i / Ns + 1, jm = i - (r - 1) * Ns;
+      const double2 w = __ldg(&tw_N[2 * r * jm * step]);
+      tws[off + i] = {(R)w.x, (R)w.y};
+    }
+    off += n;
+    Ns *= rad;
   }
 }
 

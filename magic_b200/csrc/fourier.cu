@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fourier_to_grid(ToGridArgs a) {
   const int col0 = blockIdx.x * kColsPerCta;
   const int ncol = min(kColsPerCta, a.ncols - col0);
   cplx<double>* tws = buf + (kColsPerCta + kFftRowBatch) * stride;
-  fft_twiddles_to_smem(tws, H, t.twiddle);
+  fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   for (int i = threadIdx.x; i < ncol * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
   const double2* Fr = a.F + (int64_t)row * a.f_row + col0;
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kFftThreads) k_grid_to_fourier(ToFourierArgs a
   const int col0 = blockIdx.x * kColsPerCta;
   const int ncol = min(kColsPerCta, a.ncols - col0);
   cplx<double>* tws = buf + (kColsPerCta + kFftRowBatch) * stride;
-  fft_twiddles_to_smem(tws, H, t.twiddle);
+  fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   const float rcpH = 1.0f / (float)H;
   for (int e = threadIdx.x; e < ncol * H; e += blockDim.x) {
     int q = fdiv(e, rcpH), h = e - q * H;

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(Q > 0 ? AnelFields<MAG, CHEM>::THW : 256)
   cplx<float>* twN = tw3 + 12 * Q;
   cplx<float>* tws = buf + (NB + kFftRowBatch) * S;  // block FFT table (Q = 0)
   if constexpr (Q > 0) hw_twiddles_to_smem<Q>(tw2, tw3, twN, t.twiddle, tid, T);
-  else fft_twiddles_to_smem(tws, H, t.twiddle);
+  else fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   const float* fsym = a.Fs + (int64_t)j * a.fs_j + (int64_t)r * 2 * NFI;
 #pragma unroll 4
   for (int e = tid; e < NFI * M; e += T) {

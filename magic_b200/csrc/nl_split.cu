@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kNlSplitThreads) k_nl_bouss_split(NlSplitArgs 
   const int j = row >> 1;
   const float hs = (row & 1) ? -1.f : 1.f;  // north = sym + asym, south = sym - asym
   cplx<float>* tws = buf + (BF::NB + kFftRowBatch) * stride;
-  fft_twiddles_to_smem(tws, H, t.twiddle);
+  fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   for (int i = threadIdx.x; i < NFI * stride; i += blockDim.x) buf[i] = {0.f, 0.f};
   __syncthreads();
   const float* fsym = a.Fs + (int64_t)j * a.fs_j + (int64_t)r * 2 * NFI;

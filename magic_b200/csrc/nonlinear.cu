@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   const int stride = padded_len(H);
   const int row = blockIdx.x, r = blockIdx.y;
   cplx<double>* tws = buf + (BF::NB + kFftRowBatch) * stride;
-  fft_twiddles_to_smem(tws, H, t.twiddle);
+  fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   for (int i = threadIdx.x; i < NFI * stride; i += blockDim.x) buf[i] = {0.0, 0.0};
   __syncthreads();
   // half spectra of the NFI fields (one real field per buffer row)

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kPhiThreads) k_split_to_grid(SplitPhiArgs a) {
   cplx<float>* twN = tw3 + 12 * Q;
   cplx<float>* tws = buf + (kPhiRows + kFftRowBatch) * S;  // block FFT table (Q = 0)
   if constexpr (Q > 0) hw_twiddles_to_smem<Q>(tw2, tw3, twN, t.twiddle, tid, kPhiThreads);
-  else fft_twiddles_to_smem(tws, H, t.twiddle);
+  else fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   // rows r0 .. r0 + nrow of wavenumber k are contiguous in the synthesis output
   const float* fs = a.Fs + (int64_t)j * a.fs_j + 2 * r0;
   const float rcp = 1.0f / (float)nrow;
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(kPhiThreads) k_split_to_fourier(SplitPhiArgs a
   cplx<float>* twN = tw3 + 12 * Q;
   cplx<float>* tws = buf + (kPhiRows + kFftRowBatch) * S;
   if constexpr (Q > 0) hw_twiddles_to_smem<Q>(tw2, tw3, twN, t.twiddle, tid, kPhiThreads);
-  else fft_twiddles_to_smem(tws, H, t.twiddle);
+  else fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
   const int warp = tid >> 5, l32 = tid & 31;
   for (int q = warp; q < nrow; q += kPhiThreads / 32) {
     const int r = r0 + q, b = r / a.nf, f = r - b * a.nf;
