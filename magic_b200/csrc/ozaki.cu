@@ -739,51 +739,43 @@ __host__ __device__ inline int64_t oz_ana_img_chunk(int n_m, int nchj, int rt, i
 }
 
 __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_ana_pack(OzAnaArgs a) {
-  extern __shared__ __align__(16) uint8_t smem[];
   const Tables& t = a.t;
   const int rt = blockIdx.x, mc = blockIdx.y;
   const int nchj = (t.nhs + kOzK - 1) / kOzK;
   const int tid = threadIdx.x;
   const int lev0 = rt * a.lev_tile;
   const int nlev = min(a.lev_tile, a.n_lev - lev0);
-  const int gl = (int)a.g_level;
-  const int rowlen = a.lev_tile * gl;  // doubles per staged (hemisphere, theta pair)
-  double* d = reinterpret_cast<double*>(smem);
   const int fold = tid >> 7, row = tid & 127;
   const int lv = row / a.cols, col = row - lv * a.cols;
   const bool live = lv < nlev;
   const double sg = fold ? -1.0 : 1.0;
-  const double* nrow = d + lv * gl + col;
-  auto stage = [&](int c) {
-    __syncthreads();
-    const double* gm = a.G + (int64_t)mc * a.g_m + (int64_t)lev0 * gl;
-    const int cpl = nlev * gl / 2;  // 16-byte pieces per (hemisphere, theta pair)
-    for (int hj = tid >> 5; hj < 2 * kOzK; hj += kOzPackThreads / 32) {
-      const int h = hj / kOzK, j = kOzK * c + hj % kOzK;
-      const double* src = gm + (int64_t)h * a.g_h + (int64_t)min(j, t.nhs - 1) * a.g_j;
-      const uint32_t bytes = j < t.nhs ? 16u : 0u;
-      for (int p2 = tid & 31; p2 < cpl; p2 += 32)
-        cp16_zfill(d + hj * rowlen + 2 * p2, src + 2 * p2, bytes);
-    }
-    cp_commit_wait_all();
-    __syncthreads();
-  };
-  auto value = [&](int i) -> double {
-    return live ? nrow[i * rowlen] + sg * nrow[(kOzK + i) * rowlen] : 0.0;
+  // this thread's row of the north and south Fourier values: consecutive threads
+  // read consecutive columns of one theta pair (no staging: each value is read
+  // where it is used, kOzPackLd loads in flight per thread)
+  const double* nb = a.G + (int64_t)mc * a.g_m + (int64_t)(lev0 + (live ? lv : 0)) * a.g_level +
+                     col;
+  const double* sb = nb + a.g_h;
+  auto value = [&](int j) -> double {
+    return (live && j < t.nhs) ? __ldg(nb + (int64_t)j * a.g_j) + sg * __ldg(sb + (int64_t)j * a.g_j)
+                               : 0.0;
   };
   double mx = 0.0;
-  for (int c = 0; c < nchj; ++c) {
-    stage(c);
-#pragma unroll 8
-    for (int i = 0; i < kOzK; ++i) mx = fmax(mx, fabs(value(i)));
+  for (int j0 = 0; j0 < t.nhs; j0 += 16) {
+    double v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = value(j0 + i);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(v[i]));
   }
   const int ex = oz_exponent(mx);
   a.rexp[((int64_t)mc * 2 + fold) * a.rows_pad + (int64_t)rt * kOzRows + row] = ex;
   for (int c = 0; c < nchj; ++c) {
-    stage(c);
     uint8_t* dst = a.aimg + oz_ana_img_chunk(t.n_m, nchj, rt, mc, fold, c) * kOzAChunk;
-#pragma unroll
+#pragma unroll 1
     for (int half = 0; half < 2; ++half) {
+      double v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = value(kOzK * c + 16 * half + i);
       uint32_t w[kOzDigits][4];
 #pragma unroll
       for (int i4 = 0; i4 < 4; ++i4) {
@@ -792,7 +784,7 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_ana_pack(OzAnaArgs a) 
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
           int8_t dg[kOzDigits];
-          oz_digits(value(16 * half + 4 * i4 + b), ex, dg);
+          oz_digits(v[4 * i4 + b], ex, dg);
 #pragma unroll
           for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
         }
@@ -1032,11 +1024,7 @@ int launch_oz_anal(const OzAnaArgs& a, cudaStream_t st) {
   const int ntiles = (a.n_lev + a.lev_tile - 1) / a.lev_tile;
   MT_REQUIRE(a.cols * a.lev_tile <= kOzRows && a.g_level % 2 == 0, MT_ERR_ARG,
              "analysis tile layout");
-  const size_t pack_sm = (size_t)2 * kOzK * a.lev_tile * a.g_level * sizeof(double);
-  MT_REQUIRE(pack_sm <= 220 * 1024, MT_ERR_UNSUPPORTED, "digit pack staging too large");
-  MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_ana_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)pack_sm));
-  k_oz_ana_pack<<<dim3(ntiles, a.t.n_m), kOzPackThreads, pack_sm, st>>>(a);
+  k_oz_ana_pack<<<dim3(ntiles, a.t.n_m), kOzPackThreads, 0, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   const size_t sm = OzAnaSmem::total;
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_anal_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
