@@ -44,8 +44,8 @@ struct NlBoussArgs {
   double cf2, af2, valfac;  // courfac^2, alffac^2, (0.5 (1 + 1/Pm))^2
   unsigned long long *vr2max, *vh2max;  // (n_r) non-negative doubles as bits
   // Digit-split (ozaki) stage layout, used when split_io is set: the synthesis
-  // delivers equatorially symmetric / antisymmetric FP64 rows
-  //   Fs[m][sym|asym][theta pair][level * 2 nfi + 2 f + re/im]
+  // delivers north / south FP64 rows
+  //   Fs[m][north|south][theta pair][level * 2 nfi + 2 f + re/im]
   // and the analysis reads plain north / south FP64 rows
   //   Gs[m][north|south][theta pair][(level - 1) * g_level + 2 f + re/im].
   int split_io;

@@ -142,14 +142,13 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
   __syncthreads();
   // half spectra of the NFI fields (one real field per buffer row)
   if constexpr (SPLIT_IO) {
-    // north = sym + asym, south = sym - asym
-    const double hs = (row & 1) ? -1.0 : 1.0;
-    const double* fsym = a.Fs + (int64_t)(row >> 1) * a.fs_j + (int64_t)r * 2 * NFI;
+    // the synthesis wrote this hemisphere's row: [m][north|south][theta pair][row]
+    const double* frow = a.Fs + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
+                         (int64_t)r * 2 * NFI;
     for (int e = threadIdx.x; e < M * NFI; e += blockDim.x) {
       int k = e / NFI, f = e - k * NFI;
-      const double2 sy = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m) + f);
-      const double2 as = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m + a.fs_c) + f);
-      buf[f * stride + pad16(k)] = {sy.x + hs * as.x, sy.y + hs * as.y};
+      const double2 x = __ldg(reinterpret_cast<const double2*>(frow + k * a.fs_m) + f);
+      buf[f * stride + pad16(k)] = {x.x, x.y};
     }
   } else {
     const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
@@ -260,26 +259,22 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   // latencies overlap)
   constexpr int kLd = 4;
   if constexpr (SPLIT_IO) {
-    const double hs = (row & 1) ? -1.0 : 1.0;  // north = sym + asym, south = sym - asym
-    const double* fsym = a.Fs + (int64_t)(row >> 1) * a.fs_j + (int64_t)r * 2 * NFI;
-    for (int e0 = tid; e0 < M * NFI; e0 += kLd * kNlW64Threads) {
-      double2 sy[kLd], as[kLd];
+    // the synthesis wrote this hemisphere's row: [m][north|south][theta pair][row]
+    const double* frow = a.Fs + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
+                         (int64_t)r * 2 * NFI;
+    constexpr int kLd2 = 2 * kLd;
+    for (int e0 = tid; e0 < M * NFI; e0 += kLd2 * kNlW64Threads) {
+      double2 x[kLd2];
 #pragma unroll
-      for (int u = 0; u < kLd; ++u) {
+      for (int u = 0; u < kLd2; ++u) {
         const int e = e0 + u * kNlW64Threads;
-        if (e < M * NFI) {
-          const int k = e / NFI, f = e - k * NFI;
-          sy[u] = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m) + f);
-          as[u] = __ldg(reinterpret_cast<const double2*>(fsym + k * a.fs_m + a.fs_c) + f);
-        }
+        if (e < M * NFI)
+          x[u] = __ldg(reinterpret_cast<const double2*>(frow + (e / NFI) * a.fs_m) + e % NFI);
       }
 #pragma unroll
-      for (int u = 0; u < kLd; ++u) {
+      for (int u = 0; u < kLd2; ++u) {
         const int e = e0 + u * kNlW64Threads;
-        if (e < M * NFI) {
-          const int k = e / NFI, f = e - k * NFI;
-          buf[f * S + pad16(k)] = {sy[u].x + hs * as[u].x, sy[u].y + hs * as[u].y};
-        }
+        if (e < M * NFI) buf[(e % NFI) * S + pad16(e / NFI)] = {x[u].x, x[u].y};
       }
     }
   } else {

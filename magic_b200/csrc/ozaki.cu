@@ -512,31 +512,36 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
   }
 }
 
-// Persistent synthesis GEMM: one CTA per SM walks the items (tile, combo,
-// theta tile, m) with a stride of gridDim.x.  Warp 0 lane 0 bulk-copies the A
-// digit chunk and the table digit chunk of every K step into a ring, warp 1
-// lane 0 issues the digit-pair MMAs of every step (oz_mma_chunk: six MMAs
-// covering the 21 pairs) into the six group accumulators (TMEM columns 32 g)
-// and commits when the item's K loop ends, warps 2-5 drain the accumulators
-// (one TMEM lane and the item's 32 columns per thread), form the FP64 values
-// and store them into Fs, and hand the accumulators back.
 constexpr int kOzStages = 4;     // analysis ring
-// Synthesis: two CTAs per SM, each with 256 TMEM columns (six groups of
-// kOzSynN = 32) and a 3-stage ring, so that one CTA's MMAs run while the
-// other drains its accumulators.
+// Synthesis: one CTA per SM, six accumulator groups of kOzSynN = 64 columns
+// (384 of 512 TMEM columns), a 3-stage ring, and a shared-memory stash that
+// holds an item's symmetric half until its antisymmetric half is formed, so
+// that the epilogue writes the north (sym + asym) and south (sym - asym) rows.
 constexpr int kOzSynStages = 3;
-constexpr int kOzSynEpiWarps = 4;  // one per TMEM lane quarter, all 32 columns
+constexpr int kOzSynEpiWarps = 8;  // two per TMEM lane quarter, 32 columns each
 constexpr int kOzSynThreads = 64 + 32 * kOzSynEpiWarps;
-constexpr int kOzSynTmemCols = 256;
+constexpr int kOzSynTmemCols = 512;
 
 struct OzSynSmem {
   static constexpr uint32_t stage_bytes = kOzAChunk + kOzSynBChunk;
-  static constexpr uint32_t bar_off = kOzSynStages * stage_bytes;
+  static constexpr uint32_t stash_off = kOzSynStages * stage_bytes;
+  static constexpr uint32_t stash_bytes = kOzRows * kOzSynN * 8;  // [column][row] doubles
+  static constexpr uint32_t bar_off = stash_off + stash_bytes;
   // full/empty per stage, tfull, tempty, done, tmem slot, abort flag
   static constexpr size_t total = bar_off + 8 * (2 * kOzSynStages + 3) + 16;
 };
 
-__global__ void __launch_bounds__(kOzSynThreads, 2) k_oz_synth_gemm(OzSynArgs a) {
+// Persistent synthesis GEMM: one CTA per SM walks the items (tile, theta tile,
+// m) with a stride of gridDim.x; an item is two accumulations, the symmetric
+// (combo 0: P of even l - m, dP of odd) and the antisymmetric (combo 1) half.
+// Warp 0 lane 0 bulk-copies the A digit chunk and the table digit chunk of
+// every K step into the ring, warp 1 lane 0 issues the MMAs of every step
+// (oz_mma_chunk: eight MMAs covering the 21 digit pairs) into the six group
+// accumulators (TMEM columns 64 g) and commits at the end of each half, warps
+// 2-9 drain the accumulators (one TMEM lane and 32 columns per thread): the
+// symmetric half into the stash, then with the antisymmetric half the north
+// and south rows into Fs, handing the accumulators back after each half.
+__global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   const Tables& t = a.t;
   const OzTables& z = a.z;
@@ -547,26 +552,28 @@ __global__ void __launch_bounds__(kOzSynThreads, 2) k_oz_synth_gemm(OzSynArgs a)
   uint64_t* done = tempty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  double* stash = reinterpret_cast<double*>(smem + OzSynSmem::stash_off);
 
   if (*(volatile int*)a.err) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ntiles = (a.nrows + kOzRows - 1) / kOzRows, ny = 2 * z.nthtile;
-  const int nitems = ntiles * ny * t.n_m;
+  const int ntiles = (a.nrows + kOzRows - 1) / kOzRows;
+  const int nitems = ntiles * z.nthtile * t.n_m;
   const int nthw = z.nthtile * kOzSynN;
   struct Item {
-    int rt, combo, tau, mc, nch_t[2];
+    int rt, tau, mc, nlm;
   };
   auto decode = [&](int item) {
     Item it;
     it.rt = item % ntiles;
-    const int r = item / ntiles, y = r % ny;
-    it.mc = r / ny;
-    it.combo = y & 1;
-    it.tau = y >> 1;
-    const int nlm = t.l_max - it.mc * t.minc + 1;
-    it.nch_t[0] = (split_nk(nlm, it.combo) + kOzK - 1) / kOzK;
-    it.nch_t[1] = (split_nk(nlm, 1 - it.combo) + kOzK - 1) / kOzK;
+    const int r = item / ntiles;
+    it.tau = r % z.nthtile;
+    it.mc = r / z.nthtile;
+    it.nlm = t.l_max - it.mc * t.minc + 1;
     return it;
+  };
+  // K chunks of the table of kind q (0: P, 1: dP) in half `combo` of an item
+  auto nch_of = [&](const Item& it, int combo, int q) {
+    return (split_nk(it.nlm, q ? 1 - combo : combo) + kOzK - 1) / kOzK;
   };
 
   if (tid == 0) {
@@ -592,28 +599,32 @@ __global__ void __launch_bounds__(kOzSynThreads, 2) k_oz_synth_gemm(OzSynArgs a)
       bool ok = true;
       for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
         const Item it = decode(item);
-        const uint8_t* aimg =
-            a.aimg + oz_syn_img_chunk(a.total_chunks, it.rt, z.syn_prefix[it.mc * 2 + it.combo],
-                                      0, 0) * kOzAChunk;
-        const int8_t* img[2];
-        for (int q = 0; q < 2; ++q)
-          img[q] = z.syn + z.syn_off[((it.mc * 2 + q) * 2 + (q ? 1 - it.combo : it.combo)) *
-                                         z.nthtile + it.tau];
-        const int nch = max(it.nch_t[0], it.nch_t[1]);
-        for (int c = 0; c < nch && ok; ++c) {
-          for (int q = 0; q < 2; ++q) {
-            if (c >= it.nch_t[q]) continue;
-            const int s = g % kOzSynStages;
-            if (g >= kOzSynStages &&
-                !mbar_wait(&empty[s], ((g / kOzSynStages) - 1) & 1, abort_flag, a.err, 23)) {
-              ok = false;
-              break;
+        for (int combo = 0; combo < 2 && ok; ++combo) {
+          const uint8_t* aimg =
+              a.aimg + oz_syn_img_chunk(a.total_chunks, it.rt, z.syn_prefix[it.mc * 2 + combo],
+                                        0, 0) * kOzAChunk;
+          const int8_t* img[2];
+          for (int q = 0; q < 2; ++q)
+            img[q] = z.syn + z.syn_off[((it.mc * 2 + q) * 2 + (q ? 1 - combo : combo)) *
+                                           z.nthtile + it.tau];
+          const int nq[2] = {nch_of(it, combo, 0), nch_of(it, combo, 1)};
+          const int nch = max(nq[0], nq[1]);
+          for (int c = 0; c < nch && ok; ++c) {
+            for (int q = 0; q < 2; ++q) {
+              if (c >= nq[q]) continue;
+              const int s = g % kOzSynStages;
+              if (g >= kOzSynStages &&
+                  !mbar_wait(&empty[s], ((g / kOzSynStages) - 1) & 1, abort_flag, a.err, 23)) {
+                ok = false;
+                break;
+              }
+              uint8_t* stg = smem + s * OzSynSmem::stage_bytes;
+              mbar_expect_tx(&full[s], OzSynSmem::stage_bytes);
+              bulk_g2s(stg, aimg + (int64_t)(2 * c + q) * kOzAChunk, kOzAChunk, &full[s]);
+              bulk_g2s(stg + kOzAChunk, img[q] + (int64_t)c * kOzSynBChunk, kOzSynBChunk,
+                       &full[s]);
+              ++g;
             }
-            uint8_t* stg = smem + s * OzSynSmem::stage_bytes;
-            mbar_expect_tx(&full[s], OzSynSmem::stage_bytes);
-            bulk_g2s(stg, aimg + (int64_t)(2 * c + q) * kOzAChunk, kOzAChunk, &full[s]);
-            bulk_g2s(stg + kOzAChunk, img[q] + (int64_t)c * kOzSynBChunk, kOzSynBChunk, &full[s]);
-            ++g;
           }
         }
       }
@@ -624,66 +635,91 @@ __global__ void __launch_bounds__(kOzSynThreads, 2) k_oz_synth_gemm(OzSynArgs a)
     if (lane == 0) {
       int g = 0, n = 0;
       bool ok = true;
-      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x, ++n) {
+      for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
         const Item it = decode(item);
-        if (n >= 1 && !mbar_wait(tempty, (n - 1) & 1, abort_flag, a.err, 26)) break;
-        tc_fence_after();
-        const int nch = max(it.nch_t[0], it.nch_t[1]);
-        bool first = true;
-        for (int c = 0; c < nch && ok; ++c) {
-          for (int q = 0; q < 2; ++q) {
-            if (c >= it.nch_t[q]) continue;
-            const int s = g % kOzSynStages;
-            if (!mbar_wait(&full[s], (g / kOzSynStages) & 1, abort_flag, a.err, 24)) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t sa = smem_u32(smem + s * OzSynSmem::stage_bytes);
-            oz_mma_chunk<kOzSynN>(tbase, sa, sa + kOzAChunk, first);
-            first = false;
-            umma_commit(&empty[s]);
-            ++g;
+        for (int combo = 0; combo < 2 && ok; ++combo, ++n) {
+          if (n >= 1 && !mbar_wait(tempty, (n - 1) & 1, abort_flag, a.err, 26)) {
+            ok = false;
+            break;
           }
+          tc_fence_after();
+          const int nq[2] = {nch_of(it, combo, 0), nch_of(it, combo, 1)};
+          const int nch = max(nq[0], nq[1]);
+          bool first = true;
+          for (int c = 0; c < nch && ok; ++c) {
+            for (int q = 0; q < 2; ++q) {
+              if (c >= nq[q]) continue;
+              const int s = g % kOzSynStages;
+              if (!mbar_wait(&full[s], (g / kOzSynStages) & 1, abort_flag, a.err, 24)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              const uint32_t sa = smem_u32(smem + s * OzSynSmem::stage_bytes);
+              oz_mma_chunk<kOzSynN>(tbase, sa, sa + kOzAChunk, first);
+              first = false;
+              umma_commit(&empty[s]);
+              ++g;
+            }
+          }
+          if (ok) umma_commit(tfull);
         }
-        if (ok) umma_commit(tfull);
       }
       umma_commit(done);
     }
   } else {
-    // epilogue: warps 2-5; warp w owns TMEM lane quarter w % 4 and the 32
-    // accumulator columns of half (w - 2) / 4 (0: all of them)
+    // epilogue: warps 2-9; warp w owns TMEM lane quarter w % 4 and the 32
+    // accumulator columns of half (w - 2) / 4
     const int quarter = warp & 3, half = (warp - 2) >> 2;
     const int R0 = quarter * 32 + lane;
     int n = 0;
-    for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++n) {
-      const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 22);
-      if (!__all_sync(0xffffffffu, ok && !*abort_flag)) break;
-      tc_fence_after();
+    bool live = true;
+    for (int item = blockIdx.x; item < nitems && live; item += gridDim.x) {
       const Item it = decode(item);
       const int R = it.rt * kOzRows + R0;
-      const int er = R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + it.combo) * a.rows_pad + R] : 0;
-      // column exponents of this warp's 32 columns, one per lane, shared by shuffles
-      const int fe_l = __ldg(z.syn_fexp + ((int64_t)it.mc * 2 + it.combo) * nthw +
-                             it.tau * kOzSynN + 32 * half + lane);
-      double* out = a.Fs + (int64_t)it.mc * a.fs_m + (int64_t)it.combo * a.fs_c;
-      const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16) + 32 * half;
-#pragma unroll 1
-      for (int c0 = 0; c0 < 32; c0 += 16) {
-        uint32_t cg[kOzGroups][16];
-#pragma unroll
-        for (int g = 0; g < kOzGroups; ++g) tmem_ld16_i32_nowait(taddr + g * kOzSynN + c0, cg[g]);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
-          const int th = it.tau * kOzSynN + 32 * half + c0 + i;
-          if (R < a.nrows && th < t.nhs)
-            out[(int64_t)th * a.fs_j + R] = oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
+      double* north = a.Fs + (int64_t)it.mc * a.fs_m;
+      double* south = north + a.fs_c;
+      for (int combo = 0; combo < 2; ++combo, ++n) {
+        const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 22);
+        if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
+          live = false;
+          break;
         }
+        tc_fence_after();
+        const int er =
+            R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + combo) * a.rows_pad + R] : 0;
+        // column exponents of this warp's 32 columns, one per lane, shared by shuffles
+        const int fe_l = __ldg(z.syn_fexp + ((int64_t)it.mc * 2 + combo) * nthw +
+                               it.tau * kOzSynN + 32 * half + lane);
+        const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16) + 32 * half;
+#pragma unroll 1
+        for (int c0 = 0; c0 < 32; c0 += 16) {
+          uint32_t cg[kOzGroups][16];
+#pragma unroll
+          for (int g = 0; g < kOzGroups; ++g)
+            tmem_ld16_i32_nowait(taddr + g * kOzSynN + c0, cg[g]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
+            const int col = 32 * half + c0 + i;
+            const double v = oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
+            double* st = stash + col * kOzRows + R0;  // this thread's own entry
+            if (combo == 0) {
+              *st = v;
+            } else {
+              const int th = it.tau * kOzSynN + col;
+              if (R < a.nrows && th < t.nhs) {
+                const double sy = *st;
+                north[(int64_t)th * a.fs_j + R] = sy + v;
+                south[(int64_t)th * a.fs_j + R] = sy - v;
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(tempty);
       }
-      tc_fence_before();
-      mbar_arrive(tempty);
     }
   }
   __syncwarp();
@@ -715,8 +751,8 @@ int launch_oz_synth(const OzSynArgs& a, cudaStream_t st) {
   int dev = 0, nsm = 148;
   MT_CHECK_CUDA(cudaGetDevice(&dev));
   MT_CHECK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int nitems = ntiles * 2 * a.z.nthtile * a.t.n_m;
-  k_oz_synth_gemm<<<std::min(nitems, 2 * nsm), kOzSynThreads, sm, st>>>(a);
+  const int nitems = ntiles * a.z.nthtile * a.t.n_m;
+  k_oz_synth_gemm<<<std::min(nitems, nsm), kOzSynThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
 }

@@ -34,7 +34,7 @@ constexpr int kOzDigits = 6;  // int8 digits per operand value
 constexpr int kOzGroups = 6;  // digit-weight groups kept: i + j <= 5
 constexpr int kOzK = 32;      // K per MMA and per operand chunk
 constexpr int kOzRows = 128;  // MMA M: data rows per tile
-constexpr int kOzSynN = 32;   // theta rows per synthesis tile (MMA N per table digit plane)
+constexpr int kOzSynN = 64;   // theta rows per synthesis tile (MMA N per table digit plane)
 constexpr int kOzAnaN = 32;   // l rows per analysis tile (MMA N)
 constexpr uint32_t kOzAPlane = kOzRows * kOzK;               // 4 KiB
 constexpr uint32_t kOzAChunk = kOzDigits * kOzAPlane;        // 24 KiB
@@ -83,7 +83,7 @@ struct OzSynArgs {
   int64_t total_chunks;    // oz_syn_nch summed over (m, combo)
   int* rexp;               // row exponents [(m * 2 + combo) * rows_pad + row]
   int64_t rows_pad;        // tiles * kOzRows
-  double* Fs;              // [m][sym|asym][theta pair][row]
+  double* Fs;              // [m][north|south][theta pair][row]
   int64_t fs_m, fs_c, fs_j;
   int* err;
 };
