@@ -5,10 +5,21 @@
 // the row goes through four Stockham passes with the butterfly map of
 // fft_stage (fft.cuh):
 //   radix Q (span 1), radix 4 (span Q), radix 4 (span 4 Q), radix 2 (span 16 Q),
-// Q x 4 x 4 x 2 = H.  Between passes the row lives in shared memory at the
-// padded positions pad16(i) and only the warp synchronises (__syncwarp), so
-// rows of one CTA never wait for each other.  The radix-12 butterfly is a
-// two-factor DFT (12 = 4 x 3) with literal inner twiddles.
+// Q x 4 x 4 x 2 = H.  Between passes the row lives in shared memory and only
+// the warp synchronises (__syncwarp), so rows of one CTA never wait for each
+// other.  The radix-12 butterfly is a two-factor DFT (12 = 4 x 3) with
+// literal inner twiddles.
+//
+// Shared-memory layout of a row: element i sits at w64_pos<Q>(i).  A warp's
+// 16-byte accesses go to the banks a quarter warp at a time, eight slots per
+// pass over the 32 banks.  For Q = 4, 8, 12 each group of eight slots is
+// rotated by an amount that depends on the group, so that the stride-Q
+// scatter of the first pass (eight lanes whose indices agree modulo 8 in
+// pairs or all together) lands on distinct slots while every aligned run of
+// eight (the other passes' reads and writes) stays conflict-free; the
+// rotation of Q = 12 repeats every four groups, so that the stride-32 reads
+// keep constant address offsets.  For Q = 16 the stride-16 scatter is
+// conflict-free with one pad slot per 16 (i + i / 16).
 #pragma once
 
 #include "fft.cuh"
@@ -83,54 +94,118 @@ __device__ __forceinline__ cplx<double> r2c_post_d(cplx<double> Zk, cplx<double>
   return {0.5 * (F.x + t.y), 0.5 * (F.y - t.x)};
 }
 
-// Twiddle tables of the passes in shared memory, each indexed by the
-// butterfly's position inside its span so that consecutive lanes read
-// consecutive entries (with w = exp(-2 pi i / H)):
-//   t2[r-1][jm] = w^(8 r jm), jm < Q;  t3[r-1][jm] = w^(2 r jm), jm < 4 Q;
-//   t4[j] = w^j, j < 16 Q;  twN[k] = exp(-2 pi i k / (2 H)), k < H.
+// Rotation of slot group g of a row (see the file comment; Q = 4, 8, 12).
+template <int Q>
+__device__ __forceinline__ int w64_rot(int g) {
+  if constexpr (Q == 8) return g & 7;
+  else return g & 3;
+}
+
+// Shared-memory position of element i (< H) of a row.
+template <int Q>
+__device__ __forceinline__ int w64_pos(int i) {
+  if constexpr (Q == 16) return pad16(i);
+  else return (i & ~7) | ((i + w64_rot<Q>(i >> 3)) & 7);
+}
+
+// Slots of a row, plus one so that rows S apart start on different bank
+// quads (the load and store phases touch several rows in one warp access).
+template <int Q>
+__host__ __device__ constexpr int w64_row_stride() {
+  return Q == 16 ? padded_len(32 * Q) : 32 * Q + 1;
+}
+
+// exp(-2 pi i e / 16) (forward) or its conjugate, e < 8 a compile-time
+// constant after unrolling (cos/sin of multiples of 22.5 degrees).
+template <bool INV>
+__device__ __forceinline__ cplx<double> w16d(int e) {
+  const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;  // 22.5 deg
+  const double h = 0.70710678118654752440;
+  double c, s;
+  switch (e) {
+    case 0: c = 1.0; s = 0.0; break;
+    case 1: c = c1; s = s1; break;
+    case 2: c = h; s = h; break;
+    case 3: c = s1; s = c1; break;
+    case 4: c = 0.0; s = 1.0; break;
+    case 5: c = -s1; s = c1; break;
+    case 6: c = -h; s = h; break;
+    default: c = -c1; s = s1; break;
+  }
+  return {c, INV ? s : -s};
+}
+
+// exp(-2 pi i it / Q) (forward) for it < Q / 2: the factor between w^(lane)
+// and w^(lane + 32 it), w = exp(-2 pi i / H).
+template <int Q>
+__device__ __forceinline__ cplx<double> w64_root(int it) {
+  if constexpr (Q == 12) return w12d<false>(it);
+  else return w16d<false>(it * (16 / Q));
+}
+
+// Twiddle tables in shared memory, each read so that the eight lanes of a
+// quarter warp see eight distinct slots (w = exp(-2 pi i / H)):
+//   t2[p] = w^(8 (p % Q)), p < Q + 8: pass 2's w^(8 jm), jm = j % Q, read at
+//     p = (j & ~7) % Q + (j & 7) (the quarter's window of eight consecutive
+//     jm, unwrapped);
+//   t3[jm] = w^(2 jm), jm < 4 Q: pass 3's base twiddle;
+//   wl[l] = w^l, l < 32: pass 4's w^j = wl[lane] exp(-2 pi i it / Q);
+//   twN[k] = exp(-2 pi i k / (2 H)), k < H: the real-row pre/post-processing.
+// The butterflies raise the base twiddle u to u^2 and u^3 by complex
+// multiplication (one rounding each) instead of reading three tables.
 template <int Q>
 struct W64Tw {
   const cplx<double>* t2;
   const cplx<double>* t3;
-  const cplx<double>* t4;
+  const cplx<double>* wl;
   const cplx<double>* twN;
-  static constexpr int kEntries = 3 * Q + 12 * Q + 16 * Q + 32 * Q;
+  static constexpr int kEntries = (Q + 8) + 4 * Q + 32 + 32 * Q;
 };
 
 // Fill the tables from the plan's exp(-2 pi i n / (2 H)) table (n < 2 H) at
-// `sm` (kEntries complex values); threads tid, tid + T, ... of the CTA.
+// `sm` (kEntries complex values); threads tid, tid + T, ... of the CTA.  The
+// caller synchronises the CTA before the tables are read.
 template <int Q>
 __device__ __forceinline__ W64Tw<Q> w64_twiddles(cplx<double>* sm, const double2* tw2h, int tid,
                                                  int T) {
   constexpr int H = 32 * Q;
   cplx<double>* t2 = sm;
-  cplx<double>* t3 = t2 + 3 * Q;
-  cplx<double>* t4 = t3 + 12 * Q;
-  cplx<double>* tn = t4 + 16 * Q;
+  cplx<double>* t3 = t2 + (Q + 8);
+  cplx<double>* wl = t3 + 4 * Q;
+  cplx<double>* tn = wl + 32;
   auto wH = [&](int e) {  // w^e = exp(-2 pi i e / H)
     const double2 v = __ldg(&tw2h[(2 * e) % (2 * H)]);
     return cplx<double>{v.x, v.y};
   };
-  for (int i = tid; i < 3 * Q; i += T) t2[i] = wH(8 * (i / Q + 1) * (i % Q));
-  for (int i = tid; i < 12 * Q; i += T) t3[i] = wH(2 * (i / (4 * Q) + 1) * (i % (4 * Q)));
-  for (int i = tid; i < 16 * Q; i += T) t4[i] = wH(i);
+  for (int i = tid; i < Q + 8; i += T) t2[i] = wH(8 * (i % Q));
+  for (int i = tid; i < 4 * Q; i += T) t3[i] = wH(2 * i);
+  for (int i = tid; i < 32; i += T) wl[i] = wH(i);
   for (int i = tid; i < H; i += T) {
     const double2 v = __ldg(&tw2h[i]);
     tn[i] = {v.x, v.y};
   }
-  return W64Tw<Q>{t2, t3, t4, tn};
+  return W64Tw<Q>{t2, t3, wl, tn};
 }
 
-// In-place transform of one row (padded layout) by the calling warp, with the
-// twiddle tables of w64_twiddles.
-// PRE: the row holds the half spectrum X[0..H) of a real row of length 2 H and
-// the transform input is Z[k] = c2r_pre(X[k], X[H - k]) (Im X[0] dropped,
-// X[H] = 0); the result z[n] then carries x[2 n] + i x[2 n + 1].
-template <int Q, bool INV, bool PRE>
+// u[r] *= w^r (forward) or conj(w)^r (inverse), r = 1, 2, 3, from the base
+// twiddle w: the powers by complex multiplication, one rounding each.
+template <bool INV>
+__device__ __forceinline__ void twiddle3(cplx<double> (&u)[4], cplx<double> w) {
+  if (INV) w.y = -w.y;
+  u[1] = cmul(u[1], w);
+  const cplx<double> w2 = cmul(w, w);
+  u[2] = cmul(u[2], w2);
+  u[3] = cmul(u[3], cmul(w2, w));
+}
+
+// In-place transform of one row (layout w64_pos) by the calling warp, with
+// the twiddles of w64_twiddles.  The forward transform of the analysis takes
+// z[n] = x[2 n] + i x[2 n + 1]; the inverse of the synthesis takes the
+// pre-processed half spectrum Z[k] (c2r_pre_d), so that z[n] again carries
+// x[2 n] + i x[2 n + 1].
+template <int Q, bool INV>
 __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W64Tw<Q>& T) {
-  constexpr int H = 32 * Q;
   static_assert(Q % 4 == 0, "radix-4 passes need Q / 4 butterflies per lane");
-  const cplx<double>* __restrict__ twN = T.twN;
   auto cj = [](cplx<double> w) {  // the inverse transform's conjugate twiddle
     if (INV) w.y = -w.y;
     return w;
@@ -138,70 +213,58 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W
   cplx<double> v[Q];
   // pass 1: radix Q, span 1: butterfly `lane` reads x[lane + 32 r]
 #pragma unroll
-  for (int r = 0; r < Q; ++r) {
-    const int k = lane + 32 * r;
-    cplx<double> x = row[pad16(k)];
-    if constexpr (PRE) {
-      cplx<double> xc = row[pad16((H - k) % H)];
-      if (k == 0) {
-        x.y = 0.0;
-        xc = {0.0, 0.0};
-      }
-      x = c2r_pre_d(x, xc, twN[k]);
-    }
-    v[r] = x;
-  }
+  for (int r = 0; r < Q; ++r) v[r] = row[w64_pos<Q>(lane + 32 * r)];
   __syncwarp();
   dft_q_d<Q, INV>(v);
 #pragma unroll
-  for (int r = 0; r < Q; ++r) row[pad16(lane * Q + r)] = v[r];
+  for (int r = 0; r < Q; ++r) row[w64_pos<Q>(lane * Q + r)] = v[r];
   __syncwarp();
   // pass 2: radix 4, span Q: butterfly j reads x[j + 8 Q r], twiddle w^(8 r (j % Q))
   constexpr int NB4 = Q / 4;
 #pragma unroll
   for (int it = 0; it < NB4; ++it)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[pad16(lane + 32 * it + 8 * Q * r)];
+    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[w64_pos<Q>(lane + 32 * it + 8 * Q * r)];
   __syncwarp();
 #pragma unroll
   for (int it = 0; it < NB4; ++it) {
     const int j = lane + 32 * it, jm = j % Q;
     cplx<double> u[4] = {v[4 * it], v[4 * it + 1], v[4 * it + 2], v[4 * it + 3]};
-#pragma unroll
-    for (int r = 1; r < 4; ++r) u[r] = cmul(u[r], cj(T.t2[(r - 1) * Q + jm]));
+    twiddle3<INV>(u, T.t2[(j & ~7) % Q + (j & 7)]);
     dft_small<4, INV>(u);
     const int d = (j - jm) * 4 + jm;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) row[pad16(d + r * Q)] = u[r];
+    for (int r = 0; r < 4; ++r) row[w64_pos<Q>(d + r * Q)] = u[r];
   }
   __syncwarp();
   // pass 3: radix 4, span 4 Q: butterfly j reads x[j + 8 Q r], twiddle w^(2 r (j % 4Q))
 #pragma unroll
   for (int it = 0; it < NB4; ++it)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[pad16(lane + 32 * it + 8 * Q * r)];
+    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[w64_pos<Q>(lane + 32 * it + 8 * Q * r)];
   __syncwarp();
 #pragma unroll
   for (int it = 0; it < NB4; ++it) {
     const int j = lane + 32 * it, jm = j % (4 * Q);
     cplx<double> u[4] = {v[4 * it], v[4 * it + 1], v[4 * it + 2], v[4 * it + 3]};
-#pragma unroll
-    for (int r = 1; r < 4; ++r) u[r] = cmul(u[r], cj(T.t3[(r - 1) * 4 * Q + jm]));
+    twiddle3<INV>(u, T.t3[jm]);
     dft_small<4, INV>(u);
     const int d = (j - jm) * 4 + jm;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) row[pad16(d + r * 4 * Q)] = u[r];
+    for (int r = 0; r < 4; ++r) row[w64_pos<Q>(d + r * 4 * Q)] = u[r];
   }
   __syncwarp();
   // pass 4: radix 2, span 16 Q: butterfly j < 16 Q maps x[j], x[j + 16 Q] onto
   // themselves with twiddle w^j on the second input
+  const cplx<double> wl = T.wl[lane];
 #pragma unroll
   for (int it = 0; it < Q / 2; ++it) {
     const int j = lane + 32 * it;
-    cplx<double> u[2] = {row[pad16(j)], cmul(row[pad16(j + 16 * Q)], cj(T.t4[j]))};
+    const cplx<double> w = cj(it ? cmul(wl, w64_root<Q>(it)) : wl);
+    cplx<double> u[2] = {row[w64_pos<Q>(j)], cmul(row[w64_pos<Q>(j + 16 * Q)], w)};
     dft_small<2, INV>(u);
-    row[pad16(j)] = u[0];
-    row[pad16(j + 16 * Q)] = u[1];
+    row[w64_pos<Q>(j)] = u[0];
+    row[w64_pos<Q>(j + 16 * Q)] = u[1];
   }
   __syncwarp();
 }

@@ -236,13 +236,16 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
 // The same stage for n_phi = 64 Q (Q in 4, 8, 12, 16) with warp FFTs
 // (fft_w64.cuh): every field row is transformed by one warp, so between the
 // block-wide phases (load, inverse FFTs, products, forward FFTs, store) rows
-// proceed independently, and two CTAs of 7 warps share an SM.
+// proceed independently, and two CTAs of 7 warps share an SM.  The load
+// phase applies the real-row pre-processing: the thread of wavenumber pair
+// (k, H - k) reads both coefficients and writes Z[k] and Z[H - k], so the
+// inverse transforms read their rows once.
 constexpr int kNlW64Threads = 224;
 
 template <bool MAG, bool CHEM, bool SPLIT_IO, int Q>
 __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a) {
   using BF = BoussFields<MAG, CHEM>;
-  constexpr int NFI = BF::NFI, NFO = BF::NFO, H = 32 * Q, S = padded_len(H);
+  constexpr int NFI = BF::NFI, NFO = BF::NFO, H = 32 * Q, S = w64_row_stride<Q>();
   constexpr int NW = kNlW64Threads / 32;
   extern __shared__ double smem[];
   __shared__ double red[32];
@@ -254,51 +257,50 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const W64Tw<Q> tw = w64_twiddles<Q>(twsm, t.twiddle, tid, kNlW64Threads);
   const cplx<double>* twN = tw.twN;
-  // half spectra of the NFI fields; wavenumbers k >= n_m are zero
-  // (kLd elements per thread are loaded before any is stored, so their HBM
-  // latencies overlap)
-  constexpr int kLd = 4;
-  if constexpr (SPLIT_IO) {
-    // the synthesis wrote this hemisphere's row: [m][north|south][theta pair][row]
-    const double* frow = a.Fs + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
-                         (int64_t)r * 2 * NFI;
-    constexpr int kLd2 = 2 * kLd;
-    for (int e0 = tid; e0 < M * NFI; e0 += kLd2 * kNlW64Threads) {
-      double2 x[kLd2];
+  __syncthreads();  // twN is read by the load phase
+  // coefficient X[k] of field f (k < M) of this Fourier row
+  auto ldF = [&](int k, int f) -> double2 {
+    if constexpr (SPLIT_IO) {
+      // the synthesis wrote this hemisphere's row: [m][north|south][theta pair][row]
+      const double* frow = a.Fs + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
+                           (int64_t)r * 2 * NFI;
+      return __ldg(reinterpret_cast<const double2*>(frow + (int64_t)k * a.fs_m) + f);
+    } else {
+      return __ldg(&a.F[(int64_t)row * a.f_row + (int64_t)r * NFI + (int64_t)k * a.f_m + f]);
+    }
+  };
+  // pairs (k, H - k), k <= H / 2, of every input field: Z[k] = c2r_pre(X[k], X[H - k])
+  // and Z[H - k] = c2r_pre(X[H - k], X[k]) with X[k] = 0 for k >= M (and X[H] = 0);
+  // kLd pairs per thread are loaded before any is stored, so their HBM
+  // latencies overlap
+  constexpr int NP = H / 2 + 1, kLd = 4;
+  for (int e0 = tid; e0 < NP * NFI; e0 += kLd * kNlW64Threads) {
+    double2 xa[kLd], xb[kLd];
 #pragma unroll
-      for (int u = 0; u < kLd2; ++u) {
-        const int e = e0 + u * kNlW64Threads;
-        if (e < M * NFI)
-          x[u] = __ldg(reinterpret_cast<const double2*>(frow + (e / NFI) * a.fs_m) + e % NFI);
-      }
-#pragma unroll
-      for (int u = 0; u < kLd2; ++u) {
-        const int e = e0 + u * kNlW64Threads;
-        if (e < M * NFI) buf[(e % NFI) * S + pad16(e / NFI)] = {x[u].x, x[u].y};
+    for (int u = 0; u < kLd; ++u) {
+      const int e = e0 + u * kNlW64Threads, k = e / NFI, f = e - k * NFI;
+      xa[u] = make_double2(0.0, 0.0);
+      xb[u] = make_double2(0.0, 0.0);
+      if (e < NP * NFI) {
+        if (k < M) xa[u] = ldF(k, f);
+        if (k > 0 && H - k < M) xb[u] = ldF(H - k, f);
       }
     }
-  } else {
-    const double2* Fr = a.F + (int64_t)row * a.f_row + (int64_t)r * NFI;
-    for (int e0 = tid; e0 < M * NFI; e0 += kLd * kNlW64Threads) {
-      double2 x[kLd];
 #pragma unroll
-      for (int u = 0; u < kLd; ++u) {
-        const int e = e0 + u * kNlW64Threads;
-        if (e < M * NFI) x[u] = __ldg(&Fr[(e / NFI) * a.f_m + e % NFI]);
-      }
-#pragma unroll
-      for (int u = 0; u < kLd; ++u) {
-        const int e = e0 + u * kNlW64Threads;
-        if (e < M * NFI) buf[(e % NFI) * S + pad16(e / NFI)] = {x[u].x, x[u].y};
+    for (int u = 0; u < kLd; ++u) {
+      const int e = e0 + u * kNlW64Threads, k = e / NFI, f = e - k * NFI;
+      if (e < NP * NFI) {
+        cplx<double>* rowf = buf + f * S;
+        const cplx<double> w = twN[k];
+        const cplx<double> Xk = {xa[u].x, k ? xa[u].y : 0.0}, Xc = {xb[u].x, xb[u].y};
+        rowf[w64_pos<Q>(k)] = c2r_pre_d(Xk, Xc, w);
+        if (k > 0 && k < H / 2)  // exp(-2 pi i (H - k) / (2 H)) = -conj(w)
+          rowf[w64_pos<Q>(H - k)] = c2r_pre_d(Xc, Xk, cplx<double>{-w.x, w.y});
       }
     }
-  }
-  for (int e = tid; e < NFI * (H - M); e += kNlW64Threads) {
-    const int f = e / (H - M), k = M + e % (H - M);
-    buf[f * S + pad16(k)] = {0.0, 0.0};
   }
   __syncthreads();
-  for (int f = warp; f < NFI; f += NW) w64_row_fft<Q, true, true>(buf + f * S, lane, tw);
+  for (int f = warp; f < NFI; f += NW) w64_row_fft<Q, true>(buf + f * S, lane, tw);
   __syncthreads();
 
   const double or2 = a.or2[r], or4 = a.or4[r], ost2 = t.ost2[row];
@@ -307,7 +309,7 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   const double LF = a.LFfac_r ? a.LFfac_r[r] : a.LFfac;
   double mr = 0.0, mh = 0.0;
   for (int i = tid; i < H; i += kNlW64Threads) {
-    const int si = pad16(i);
+    const int si = w64_pos<Q>(i);
     cplx<double> zin[NFI];
 #pragma unroll
     for (int f = 0; f < NFI; ++f) zin[f] = buf[f * S + si];
@@ -351,7 +353,7 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   if (tid == 0) atomic_max_pos(&a.vh2max[r], vmh);
   if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
   __syncthreads();
-  for (int f = warp; f < NFO; f += NW) w64_row_fft<Q, false, false>(buf + f * S, lane, tw);
+  for (int f = warp; f < NFO; f += NW) w64_row_fft<Q, false>(buf + f * S, lane, tw);
   __syncthreads();
   const double ws = t.wq[row] / (2 * H), wv = t.wq_v[row] / (2 * H);
   double2* Gr = SPLIT_IO
@@ -363,7 +365,8 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   for (int e = tid; e < M * NFO; e += kNlW64Threads) {
     const int k = e / NFO, o = e - k * NFO;
     const cplx<double>* z = buf + o * S;
-    const cplx<double> X = r2c_post_d(z[pad16(k)], z[pad16((H - k) % H)], twN[k]);
+    const cplx<double> X =
+        r2c_post_d(z[w64_pos<Q>(k)], z[w64_pos<Q>((H - k) % H)], twN[k]);
     const bool radial = (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
     const double w = radial ? ws : wv;
     Gr[k * gm + o] = make_double2(w * X.x, w * X.y);
@@ -374,7 +377,7 @@ template <bool MAG, bool CHEM, bool SPLIT_IO, int Q>
 static int launch_nl_bouss_w64(const NlBoussArgs& a, cudaStream_t st) {
   using BF = BoussFields<MAG, CHEM>;
   constexpr int H = 32 * Q;
-  const size_t sm = ((size_t)BF::NB * padded_len(H) + W64Tw<Q>::kEntries) * sizeof(double2);
+  const size_t sm = ((size_t)BF::NB * w64_row_stride<Q>() + W64Tw<Q>::kEntries) * sizeof(double2);
   auto kern = k_nl_bouss_w64<MAG, CHEM, SPLIT_IO, Q>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
