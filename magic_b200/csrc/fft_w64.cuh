@@ -163,8 +163,9 @@ struct W64Tw {
 };
 
 // Fill the tables from the plan's exp(-2 pi i n / (2 H)) table (n < 2 H) at
-// `sm` (kEntries complex values); threads tid, tid + T, ... of the CTA.  The
-// caller synchronises the CTA before the tables are read.
+// `sm` (kEntries complex values) with asynchronous 16-byte copies issued by
+// threads tid, tid + T, ... of the CTA; the caller waits for its copies
+// (cp_async_wait_all) and synchronises the CTA before the tables are read.
 template <int Q>
 __device__ __forceinline__ W64Tw<Q> w64_twiddles(cplx<double>* sm, const double2* tw2h, int tid,
                                                  int T) {
@@ -173,17 +174,11 @@ __device__ __forceinline__ W64Tw<Q> w64_twiddles(cplx<double>* sm, const double2
   cplx<double>* t3 = t2 + (Q + 8);
   cplx<double>* wl = t3 + 4 * Q;
   cplx<double>* tn = wl + 32;
-  auto wH = [&](int e) {  // w^e = exp(-2 pi i e / H)
-    const double2 v = __ldg(&tw2h[(2 * e) % (2 * H)]);
-    return cplx<double>{v.x, v.y};
-  };
-  for (int i = tid; i < Q + 8; i += T) t2[i] = wH(8 * (i % Q));
-  for (int i = tid; i < 4 * Q; i += T) t3[i] = wH(2 * i);
-  for (int i = tid; i < 32; i += T) wl[i] = wH(i);
-  for (int i = tid; i < H; i += T) {
-    const double2 v = __ldg(&tw2h[i]);
-    tn[i] = {v.x, v.y};
-  }
+  auto wH = [&](int e) { return &tw2h[(2 * e) % (2 * H)]; };  // w^e = exp(-2 pi i e / H)
+  for (int i = tid; i < Q + 8; i += T) cp_async16(&t2[i], wH(8 * (i % Q)));
+  for (int i = tid; i < 4 * Q; i += T) cp_async16(&t3[i], wH(2 * i));
+  for (int i = tid; i < 32; i += T) cp_async16(&wl[i], wH(i));
+  for (int i = tid; i < H; i += T) cp_async16(&tn[i], &tw2h[i]);
   return W64Tw<Q>{t2, t3, wl, tn};
 }
 

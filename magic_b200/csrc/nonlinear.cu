@@ -89,6 +89,32 @@ __device__ __forceinline__ double block_max(double v, double* red) {
   return v;  // valid in thread 0
 }
 
+// Block-wide maxima of two values at once (one pass through `red`, >= 2 x 16
+// doubles); the results are valid in thread 0.
+__device__ __forceinline__ void block_max2(double& a, double& b, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  }
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[w] = a;
+    red[16 + w] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    a = threadIdx.x < nw ? red[threadIdx.x] : 0.0;
+    b = threadIdx.x < nw ? red[16 + threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+  }
+}
+
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
   v = v + 0.0;  // -0 -> +0: bit patterns of non-negative doubles order like integers
   atomicMax(a, (unsigned long long)__double_as_longlong(v));
@@ -236,11 +262,11 @@ __global__ void __launch_bounds__(kNlThreads) k_nl_bouss(NlBoussArgs a) {
 // The same stage for n_phi = 64 Q (Q in 4, 8, 12, 16) with warp FFTs
 // (fft_w64.cuh): every field row is transformed by one warp, so between the
 // block-wide phases (load, inverse FFTs, products, forward FFTs, store) rows
-// proceed independently, and two CTAs of 7 warps share an SM.  The load
-// phase applies the real-row pre-processing: the thread of wavenumber pair
-// (k, H - k) reads both coefficients and writes Z[k] and Z[H - k], so the
-// inverse transforms read their rows once.
-constexpr int kNlW64Threads = 224;
+// proceed independently, and two CTAs of 8 warps (128 registers a thread)
+// share an SM.  The load phase applies the real-row pre-processing: the
+// thread of wavenumber pair (k, H - k) reads both coefficients and writes
+// Z[k] and Z[H - k], so the inverse transforms read their rows once.
+constexpr int kNlW64Threads = 256;
 
 template <bool MAG, bool CHEM, bool SPLIT_IO, int Q>
 __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a) {
@@ -253,11 +279,13 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   cplx<double>* twsm = buf + BF::NB * S;                      // W64Tw<Q> tables
   const Tables& t = a.t;
   const int M = t.n_m;
-  const int row = blockIdx.x, r = blockIdx.y;
+  // levels run fastest through the grid: the CTAs resident at one time read
+  // (and write) whole runs of levels of a few theta rows, contiguous in HBM
+  const int row = blockIdx.y, r = blockIdx.x;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // twiddle tables: asynchronous copies, waited for before the first use
   const W64Tw<Q> tw = w64_twiddles<Q>(twsm, t.twiddle, tid, kNlW64Threads);
   const cplx<double>* twN = tw.twN;
-  __syncthreads();  // twN is read by the load phase
   // coefficient X[k] of field f (k < M) of this Fourier row
   auto ldF = [&](int k, int f) -> double2 {
     if constexpr (SPLIT_IO) {
@@ -272,13 +300,14 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   // pairs (k, H - k), k <= H / 2, of every input field: Z[k] = c2r_pre(X[k], X[H - k])
   // and Z[H - k] = c2r_pre(X[H - k], X[k]) with X[k] = 0 for k >= M (and X[H] = 0);
   // kLd pairs per thread are loaded before any is stored, so their HBM
-  // latencies overlap
-  constexpr int NP = H / 2 + 1, kLd = 4;
-  for (int e0 = tid; e0 < NP * NFI; e0 += kLd * kNlW64Threads) {
+  // latencies overlap (two rounds at n_phi = 768, the first also covering
+  // the twiddle copies)
+  constexpr int NP = H / 2 + 1, kLd = 6;
+  for (int e0 = 0; e0 < NP * NFI; e0 += kLd * kNlW64Threads) {
     double2 xa[kLd], xb[kLd];
 #pragma unroll
     for (int u = 0; u < kLd; ++u) {
-      const int e = e0 + u * kNlW64Threads, k = e / NFI, f = e - k * NFI;
+      const int e = e0 + u * kNlW64Threads + tid, k = e / NFI, f = e - k * NFI;
       xa[u] = make_double2(0.0, 0.0);
       xb[u] = make_double2(0.0, 0.0);
       if (e < NP * NFI) {
@@ -286,9 +315,13 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
         if (k > 0 && H - k < M) xb[u] = ldF(H - k, f);
       }
     }
+    if (e0 == 0) {  // (uniform) the tables are complete once every thread's copies are
+      cp_async_wait_all();
+      __syncthreads();
+    }
 #pragma unroll
     for (int u = 0; u < kLd; ++u) {
-      const int e = e0 + u * kNlW64Threads, k = e / NFI, f = e - k * NFI;
+      const int e = e0 + u * kNlW64Threads + tid, k = e / NFI, f = e - k * NFI;
       if (e < NP * NFI) {
         cplx<double>* rowf = buf + f * S;
         const cplx<double> w = twN[k];
@@ -347,10 +380,11 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
 #pragma unroll
     for (int q = 0; q < NFO; ++q) buf[q * S + si] = {out[0][q], out[1][q]};
   }
-  double vmr = block_max(mr, red);
-  if (tid == 0) atomic_max_pos(&a.vr2max[r], vmr);
-  double vmh = block_max(mh, red);
-  if (tid == 0) atomic_max_pos(&a.vh2max[r], vmh);
+  block_max2(mr, mh, red);
+  if (tid == 0) {
+    atomic_max_pos(&a.vr2max[r], mr);
+    atomic_max_pos(&a.vh2max[r], mh);
+  }
   if (r == 0 || r == a.n_r - 1) return;  // boundary levels: Courant only
   __syncthreads();
   for (int f = warp; f < NFO; f += NW) w64_row_fft<Q, false>(buf + f * S, lane, tw);
@@ -362,14 +396,31 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
                                                  (int64_t)(r - 1) * a.g_level)
                     : a.G + (int64_t)row * a.g_row + (int64_t)(r - 1) * NFO;
   const int64_t gm = SPLIT_IO ? a.g_m2 / 2 : a.g_m;  // double2 stride between orders
-  for (int e = tid; e < M * NFO; e += kNlW64Threads) {
-    const int k = e / NFO, o = e - k * NFO;
-    const cplx<double>* z = buf + o * S;
-    const cplx<double> X =
-        r2c_post_d(z[w64_pos<Q>(k)], z[w64_pos<Q>((H - k) % H)], twN[k]);
-    const bool radial = (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
-    const double w = radial ? ws : wv;
-    Gr[k * gm + o] = make_double2(w * X.x, w * X.y);
+  // kSt outputs per thread: their shared-memory reads are issued together
+  constexpr int kSt = 4;
+  for (int e0 = tid; e0 < M * NFO; e0 += kSt * kNlW64Threads) {
+    cplx<double> zk[kSt], zc[kSt], wn[kSt];
+#pragma unroll
+    for (int u = 0; u < kSt; ++u) {
+      const int e = e0 + u * kNlW64Threads, k = e / NFO, o = e - k * NFO;
+      if (e < M * NFO) {
+        const cplx<double>* z = buf + o * S;
+        zk[u] = z[w64_pos<Q>(k)];
+        zc[u] = z[w64_pos<Q>((H - k) % H)];
+        wn[u] = twN[k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kSt; ++u) {
+      const int e = e0 + u * kNlW64Threads, k = e / NFO, o = e - k * NFO;
+      if (e < M * NFO) {
+        const cplx<double> X = r2c_post_d(zk[u], zc[u], wn[u]);
+        const bool radial =
+            (o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == (MAG ? 9 : 6)));
+        const double w = radial ? ws : wv;
+        Gr[k * gm + o] = make_double2(w * X.x, w * X.y);
+      }
+    }
   }
 }
 
@@ -382,7 +433,7 @@ static int launch_nl_bouss_w64(const NlBoussArgs& a, cudaStream_t st) {
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
-  dim3 grid(a.t.n_theta, a.n_r);
+  dim3 grid(a.n_r, a.t.n_theta);
   kern<<<grid, kNlW64Threads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   return MT_OK;
