@@ -759,10 +759,12 @@ int launch_oz_synth(const OzSynArgs& a, cudaStream_t st) {
 
 // -------------------------------------------------------------- analysis
 //
-// k_oz_ana_pack: block (tile rt, order m); thread = (fold, row): fold 0 is
-// north + south, fold 1 north - south of the raw Fourier column (level lv,
-// column col) of the tile.  Pass 0 finds the row's largest |value| over all
-// theta pairs, pass 1 writes the digit planes of every chunk of kOzK pairs.
+// k_oz_ana_pack<RB>: block (RB rows of tile rt, order m).  The block's raw
+// Fourier values (north and south, every theta pair) are read from HBM once
+// into shared memory, [hemisphere][theta pair][row]; each row then yields
+// both folds, fold 0 north + south and fold 1 north - south: pass 0 finds
+// each (row, fold)'s largest |value| over all theta pairs, pass 1 writes the
+// digit planes of every chunk of kOzK pairs from shared memory.
 // k_oz_anal_gemm (persistent; item = tile, output parity, l tile, m)
 // accumulates acc0 = fold_par . P and acc1 = fold_(1-par) . dP in six groups
 // each, and its epilogue forms each output component as
@@ -774,62 +776,105 @@ __host__ __device__ inline int64_t oz_ana_img_chunk(int n_m, int nchj, int rt, i
   return (((int64_t)rt * n_m + mc) * 2 + fold) * nchj + c;
 }
 
+// rows per analysis-pack block: the largest of 32, 16, 8 whose staging buffer
+// (2 x nhs x RB doubles) lets two blocks share an SM
+inline int oz_ana_pack_rows(int nhs) {
+  for (int rb = 32; rb > 8; rb >>= 1)
+    if ((size_t)2 * nhs * rb * 8 <= 110 * 1024) return rb;
+  return 8;
+}
+inline size_t oz_ana_pack_smem(int nhs, int rb) {
+  return (size_t)2 * nhs * rb * 8 + (size_t)2 * (kOzPackThreads + rb) * 8;
+}
+
+template <int RB>
 __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_ana_pack(OzAnaArgs a) {
+  extern __shared__ __align__(16) double stg[];  // [hemisphere][theta pair][row]
+  constexpr int NG = kOzPackThreads / RB;        // theta-pair groups of the load pass
   const Tables& t = a.t;
-  const int rt = blockIdx.x, mc = blockIdx.y;
-  const int nchj = (t.nhs + kOzK - 1) / kOzK;
+  const int nhs = t.nhs;
+  const int rt = blockIdx.x / (kOzRows / RB), rq = blockIdx.x % (kOzRows / RB);
+  const int mc = blockIdx.y;
+  const int nchj = (nhs + kOzK - 1) / kOzK;
   const int tid = threadIdx.x;
+  double* red = stg + (size_t)2 * nhs * RB;  // [fold][group][row] partial maxima
+  double* exs = red + 2 * kOzPackThreads;    // [fold][row] exponents (as doubles)
   const int lev0 = rt * a.lev_tile;
   const int nlev = min(a.lev_tile, a.n_lev - lev0);
-  const int fold = tid >> 7, row = tid & 127;
-  const int lv = row / a.cols, col = row - lv * a.cols;
-  const bool live = lv < nlev;
-  const double sg = fold ? -1.0 : 1.0;
-  // this thread's row of the north and south Fourier values: consecutive threads
-  // read consecutive columns of one theta pair (no staging: each value is read
-  // where it is used, kOzPackLd loads in flight per thread)
-  const double* nb = a.G + (int64_t)mc * a.g_m + (int64_t)(lev0 + (live ? lv : 0)) * a.g_level +
-                     col;
-  const double* sb = nb + a.g_h;
-  auto value = [&](int j) -> double {
-    return (live && j < t.nhs) ? __ldg(nb + (int64_t)j * a.g_j) + sg * __ldg(sb + (int64_t)j * a.g_j)
-                               : 0.0;
-  };
-  double mx = 0.0;
-  for (int j0 = 0; j0 < t.nhs; j0 += 16) {
-    double v[16];
+  // load pass: thread (row rr, group g) reads theta pairs g, g + NG, ...;
+  // consecutive threads read consecutive rows of one theta pair
+  {
+    const int rr = tid % RB, g = tid / RB;
+    const int R = rq * RB + rr, lv = R / a.cols, col = R - lv * a.cols;
+    const bool live = lv < nlev;
+    const double* nb = a.G + (int64_t)mc * a.g_m + (int64_t)(lev0 + (live ? lv : 0)) * a.g_level +
+                       col;
+    double m0 = 0.0, m1 = 0.0;
+    constexpr int kB = 8;
+    for (int j0 = g; j0 < nhs; j0 += kB * NG) {
+      double vn[kB], vs[kB];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = value(j0 + i);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(v[i]));
-  }
-  const int ex = oz_exponent(mx);
-  a.rexp[((int64_t)mc * 2 + fold) * a.rows_pad + (int64_t)rt * kOzRows + row] = ex;
-  for (int c = 0; c < nchj; ++c) {
-    uint8_t* dst = a.aimg + oz_ana_img_chunk(t.n_m, nchj, rt, mc, fold, c) * kOzAChunk;
-#pragma unroll 1
-    for (int half = 0; half < 2; ++half) {
-      double v[16];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = value(kOzK * c + 16 * half + i);
-      uint32_t w[kOzDigits][4];
-#pragma unroll
-      for (int i4 = 0; i4 < 4; ++i4) {
-#pragma unroll
-        for (int s = 0; s < kOzDigits; ++s) w[s][i4] = 0u;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          int8_t dg[kOzDigits];
-          oz_digits(v[4 * i4 + b], ex, dg);
-#pragma unroll
-          for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
+      for (int u = 0; u < kB; ++u) {
+        const int j = j0 + u * NG;
+        vn[u] = vs[u] = 0.0;
+        if (live && j < nhs) {
+          vn[u] = __ldg(nb + (int64_t)j * a.g_j);
+          vs[u] = __ldg(nb + a.g_h + (int64_t)j * a.g_j);
         }
       }
 #pragma unroll
-      for (int s = 0; s < kOzDigits; ++s)
-        *reinterpret_cast<uint4*>(dst + s * kOzAPlane + oz_off(row, 16 * half)) =
-            make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+      for (int u = 0; u < kB; ++u) {
+        const int j = j0 + u * NG;
+        if (j < nhs) {
+          stg[(size_t)j * RB + rr] = vn[u];
+          stg[(size_t)(nhs + j) * RB + rr] = vs[u];
+        }
+        m0 = fmax(m0, fabs(vn[u] + vs[u]));
+        m1 = fmax(m1, fabs(vn[u] - vs[u]));
+      }
     }
+    red[g * RB + rr] = m0;
+    red[(NG + g) * RB + rr] = m1;
+  }
+  __syncthreads();
+  if (tid < 2 * RB) {
+    const int fold = tid / RB, rr = tid % RB;
+    double mx = 0.0;
+    for (int g = 0; g < NG; ++g) mx = fmax(mx, red[(fold * NG + g) * RB + rr]);
+    const int ex = oz_exponent(mx);
+    exs[tid] = (double)ex;
+    a.rexp[((int64_t)mc * 2 + fold) * a.rows_pad + (int64_t)rt * kOzRows + rq * RB + rr] = ex;
+  }
+  __syncthreads();
+  // digit pass: task (row rr, fold, half chunk hc of 16 theta pairs)
+  const int ntask = RB * 2 * 2 * nchj;
+  for (int task = tid; task < ntask; task += kOzPackThreads) {
+    const int rr = task % RB, rest = task / RB;
+    const int fold = rest & 1, hc = rest >> 1;
+    const double sg = fold ? -1.0 : 1.0;
+    const int ex = (int)exs[fold * RB + rr];
+    uint32_t w[kOzDigits][4];
+#pragma unroll
+    for (int i4 = 0; i4 < 4; ++i4) {
+#pragma unroll
+      for (int s = 0; s < kOzDigits; ++s) w[s][i4] = 0u;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int j = 16 * hc + 4 * i4 + b;
+        const double v =
+            j < nhs ? stg[(size_t)j * RB + rr] + sg * stg[(size_t)(nhs + j) * RB + rr] : 0.0;
+        int8_t dg[kOzDigits];
+        oz_digits(v, ex, dg);
+#pragma unroll
+        for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
+      }
+    }
+    uint8_t* dst =
+        a.aimg + oz_ana_img_chunk(t.n_m, nchj, rt, mc, fold, hc >> 1) * kOzAChunk;
+#pragma unroll
+    for (int s = 0; s < kOzDigits; ++s)
+      *reinterpret_cast<uint4*>(dst + s * kOzAPlane + oz_off(rq * RB + rr, 16 * (hc & 1))) =
+          make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
   }
 }
 
@@ -1060,7 +1105,11 @@ int launch_oz_anal(const OzAnaArgs& a, cudaStream_t st) {
   const int ntiles = (a.n_lev + a.lev_tile - 1) / a.lev_tile;
   MT_REQUIRE(a.cols * a.lev_tile <= kOzRows && a.g_level % 2 == 0, MT_ERR_ARG,
              "analysis tile layout");
-  k_oz_ana_pack<<<dim3(ntiles, a.t.n_m), kOzPackThreads, 0, st>>>(a);
+  const int rb = oz_ana_pack_rows(a.t.nhs);
+  const size_t psm = oz_ana_pack_smem(a.t.nhs, rb);
+  auto pack = rb == 32 ? k_oz_ana_pack<32> : rb == 16 ? k_oz_ana_pack<16> : k_oz_ana_pack<8>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(pack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+  pack<<<dim3(ntiles * (kOzRows / rb), a.t.n_m), kOzPackThreads, psm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());
   const size_t sm = OzAnaSmem::total;
   MT_CHECK_CUDA(cudaFuncSetAttribute(k_oz_anal_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
