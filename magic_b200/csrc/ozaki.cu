@@ -35,6 +35,7 @@ constexpr unsigned long long kOzDigitOffset =
     64ull * ((1ull << 35) + (1ull << 28) + (1ull << 21) + (1ull << 14) + (1ull << 7) + 1ull);
 
 __device__ __forceinline__ double oz_scale_up(double v, int s);
+__device__ __forceinline__ double oz_pow2(int s);
 
 __device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzDigits]) {
   const long long Y = __double2ll_rn(oz_scale_up(v, 41 - e));
@@ -42,6 +43,51 @@ __device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzDigits
   d[0] = (int8_t)((int)(U >> 35) - 64);
 #pragma unroll
   for (int i = 1; i < kOzDigits; ++i) d[i] = (int8_t)((int)((U >> (7 * (5 - i))) & 127u) - 64);
+}
+
+// The pack kernels' form of the same digits, four values to a 32-bit word
+// per digit plane.  One fma forms T = 1.5 2^52 + O + rint(v 2^(41 - e)): the
+// product v 2^(41 - e) is exact, |rint(..)| <= 2^41, and the fma's single
+// rounding to the integer grid of [2^52, 2^53) is rint's with ties to even,
+// 1.5 2^52 + O being an even integer; the mantissa of T is then 2^51 + U
+// (U = Y + O < 2^43): U mod 2^32 is T's low word and U / 2^32 the low bits of
+// its high word, so the six base-128 fields x_i of U need only 32-bit shifts
+// (x_0 <= 128 takes eight bits).  oz_put_digits puts byte b of w[i]:
+// d_0 = x_0 - 64 directly, x_1 .. x_5 raw; oz_bias_bytes then subtracts 64 from
+// each byte of a word of raw fields (all below 128) without borrows.
+__device__ __forceinline__ double oz_digit_word(double v, int e) {
+  constexpr double kC = 6755399441055744.0 + (double)kOzDigitOffset;
+  const int s = 41 - e;
+  if (s <= 1023) return fma(v, oz_pow2(s), kC);
+  return fma(v * oz_pow2(min(s - 1023, 1023)), 0x1p1023, kC);
+}
+
+__device__ __forceinline__ void oz_put_digits(double v, int e, int b, uint32_t (&w)[kOzDigits]) {
+  const double T = oz_digit_word(v, e);
+  const uint32_t lo = (uint32_t)__double2loint(T), hi = (uint32_t)__double2hiint(T);
+  const int sh = 8 * b;
+  w[0] |= (((hi >> 3) + 192u) & 0xFFu) << sh;
+  w[1] |= (__funnelshift_r(lo, hi, 28) & 127u) << sh;
+  w[2] |= ((lo >> 21) & 127u) << sh;
+  w[3] |= ((lo >> 14) & 127u) << sh;
+  w[4] |= ((lo >> 7) & 127u) << sh;
+  w[5] |= (lo & 127u) << sh;
+}
+
+__device__ __forceinline__ uint32_t oz_bias_bytes(uint32_t w) {
+  return ((w | 0x80808080u) - 0x40404040u) ^ 0x80808080u;
+}
+
+// Digits of four values (scale 2^e each) as the six plane words of a 4-byte
+// group: w[i] byte b = digit i of v[b].
+__device__ __forceinline__ void oz_digit_words(const double (&v)[4], int e,
+                                               uint32_t (&w)[kOzDigits]) {
+#pragma unroll
+  for (int s = 0; s < kOzDigits; ++s) w[s] = 0u;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) oz_put_digits(v[b], e, b, w);
+#pragma unroll
+  for (int s = 1; s < kOzDigits; ++s) w[s] = oz_bias_bytes(w[s]);
 }
 
 // Instruction descriptor: kind::i8, s8 x s8 -> s32, A and B K-major.
@@ -490,23 +536,18 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
     for (int h = 0; h < 2; ++h) {
 #pragma unroll 1
       for (int half = 0; half < 2; ++half) {
-        uint32_t w[kOzDigits][4];
+        uint32_t w[4][kOzDigits];
 #pragma unroll
         for (int i4 = 0; i4 < 4; ++i4) {
+          double v4[4];
 #pragma unroll
-          for (int s = 0; s < kOzDigits; ++s) w[s][i4] = 0u;
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            int8_t dg[kOzDigits];
-            oz_digits(value(h, c, 16 * half + 4 * i4 + b), ex[h], dg);
-#pragma unroll
-            for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
-          }
+          for (int b = 0; b < 4; ++b) v4[b] = value(h, c, 16 * half + 4 * i4 + b);
+          oz_digit_words(v4, ex[h], w[i4]);
         }
 #pragma unroll
         for (int s = 0; s < kOzDigits; ++s)
           *reinterpret_cast<uint4*>(dst + s * kOzAPlane + oz_off(row0 + h, 16 * half)) =
-              make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+              make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
       }
     }
   }
@@ -853,28 +894,23 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_ana_pack(OzAnaArgs a) 
     const int fold = rest & 1, hc = rest >> 1;
     const double sg = fold ? -1.0 : 1.0;
     const int ex = (int)exs[fold * RB + rr];
-    uint32_t w[kOzDigits][4];
+    uint32_t w[4][kOzDigits];
 #pragma unroll
     for (int i4 = 0; i4 < 4; ++i4) {
-#pragma unroll
-      for (int s = 0; s < kOzDigits; ++s) w[s][i4] = 0u;
+      double v4[4];
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
         const int j = 16 * hc + 4 * i4 + b;
-        const double v =
-            j < nhs ? stg[(size_t)j * RB + rr] + sg * stg[(size_t)(nhs + j) * RB + rr] : 0.0;
-        int8_t dg[kOzDigits];
-        oz_digits(v, ex, dg);
-#pragma unroll
-        for (int s = 0; s < kOzDigits; ++s) w[s][i4] |= (uint32_t)(uint8_t)dg[s] << (8 * b);
+        v4[b] = j < nhs ? stg[(size_t)j * RB + rr] + sg * stg[(size_t)(nhs + j) * RB + rr] : 0.0;
       }
+      oz_digit_words(v4, ex, w[i4]);
     }
     uint8_t* dst =
         a.aimg + oz_ana_img_chunk(t.n_m, nchj, rt, mc, fold, hc >> 1) * kOzAChunk;
 #pragma unroll
     for (int s = 0; s < kOzDigits; ++s)
       *reinterpret_cast<uint4*>(dst + s * kOzAPlane + oz_off(rq * RB + rr, 16 * (hc & 1))) =
-          make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+          make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
   }
 }
 

@@ -70,6 +70,56 @@ def test_scaling_rounds_like_ldexp():
         assert oz_scale(w, t) == math.ldexp(w, t)
 
 
+def digit_bytes(v, e):
+    """The pack kernels' byte form of the digits of v (scale 2^e), restated with
+    exact rationals: T = fma(v, 2^(41 - e), 1.5 2^52 + OFFSET) rounded once to
+    the nearest double (ties to even), the mantissa of T = 2^51 + U split into
+    its low and high words, the six 7-bit fields read with 32-bit shifts
+    (d_0 from eight bits of the high word, the rest by a borrow-free per-byte
+    subtraction of 64)."""
+    from fractions import Fraction
+
+    x = Fraction(v) * Fraction(2) ** (41 - e) + int(1.5 * 2 ** 52) + OFFSET
+    n, r = divmod(x, 1)
+    n = int(n)
+    if r > Fraction(1, 2) or (r == Fraction(1, 2) and n % 2):
+        n += 1
+    assert 2 ** 52 <= n < 2 ** 53  # one binade: the ulp of T is 1
+    mant = n - 2 ** 52
+    lo, hi = mant & 0xFFFFFFFF, (0x433 << 20) | (mant >> 32)
+    raw = [((hi << 32 | lo) >> 28) & 127, (lo >> 21) & 127, (lo >> 14) & 127, (lo >> 7) & 127,
+           lo & 127]
+    bias = lambda w: (((w | 0x80) - 0x40) ^ 0x80) & 0xFF  # one byte of oz_bias_bytes
+    return [((hi >> 3) + 192) & 0xFF] + [bias(w) for w in raw]
+
+
+def test_byte_digits_equal_integer_digits():
+    """The fma / word-split digits of the pack kernels equal the integer
+    method's digits (as int8 bytes) for values across the exponent range,
+    including the rounding ties and |v| rounding up to 2^e (d_0 = 64)."""
+    import math
+    import random
+
+    rnd = random.Random(1)
+    cases = []
+    for _ in range(4000):
+        e = rnd.randint(-900, 900)
+        v = rnd.uniform(-1.0, 1.0) * 2.0 ** e
+        cases.append((v, math.frexp(v)[1] if v else 0))
+        cases.append((v, (math.frexp(v)[1] if v else 0) + rnd.randint(0, 12)))  # row scale above
+    for e in (0, 5, -3):
+        top = 2.0 ** e
+        cases += [(math.nextafter(top, 0.0), e), (-math.nextafter(top, 0.0), e)]  # round to 2^41
+        cases += [((k + 0.5) * 2.0 ** (e - 41), e) for k in (-4, -3, 0, 1, 2, 7)]  # exact ties
+    cases += [(0.0, 0), (0.0, 7), (5e-324, -1073), (-5e-324, -1073)]
+    for v, e in cases:
+        Y = int(np.rint(np.ldexp(v, 41 - e)))
+        assert abs(Y) <= 2 ** 41
+        U = Y + OFFSET
+        ref = [(U >> 35) - 64] + [((U >> (7 * (5 - i))) & 127) - 64 for i in range(1, D)]
+        assert digit_bytes(v, e) == [d & 0xFF for d in ref], (v, e)
+
+
 def contract(A, B):
     da, ea = digits(A, 1)
     db, eb = digits(B, 0)
