@@ -721,17 +721,19 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
       double* north = a.Fs + (int64_t)it.mc * a.fs_m;
       double* south = north + a.fs_c;
       for (int combo = 0; combo < 2; ++combo, ++n) {
+        // the row and column exponents do not depend on the MMAs: their loads
+        // are issued before the wait for the accumulators
+        const int er =
+            R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + combo) * a.rows_pad + R] : 0;
+        // column exponents of this warp's 32 columns, one per lane, shared by shuffles
+        const int fe_l = __ldg(z.syn_fexp + ((int64_t)it.mc * 2 + combo) * nthw +
+                               it.tau * kOzSynN + 32 * half + lane);
         const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 22);
         if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
           live = false;
           break;
         }
         tc_fence_after();
-        const int er =
-            R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + combo) * a.rows_pad + R] : 0;
-        // column exponents of this warp's 32 columns, one per lane, shared by shuffles
-        const int fe_l = __ldg(z.syn_fexp + ((int64_t)it.mc * 2 + combo) * nthw +
-                               it.tau * kOzSynN + 32 * half + lane);
         const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16) + 32 * half;
 #pragma unroll 1
         for (int c0 = 0; c0 < 32; c0 += 16) {
@@ -1054,6 +1056,18 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
       const Item it = decode(item);
       if (!it.live) continue;
+      // row and column exponents of both table kinds, loaded before the wait
+      // for the accumulators (they do not depend on the MMAs); the kOzAnaN (32)
+      // column exponents one per lane, shared by shuffles
+      const int Rg = it.rt * kOzRows + R0;
+      int er2[2], fe2[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int fold = q ? 1 - it.par : it.par;
+        er2[q] = a.rexp[((int64_t)it.mc * 2 + fold) * a.rows_pad + Rg];
+        fe2[q] = __ldg(z.ana_fexp + ((int64_t)(it.mc * 2 + q) * 2 + it.par) * z.nlt * kOzAnaN +
+                       it.lt * kOzAnaN + lane);
+      }
       const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 32);
       ++n;
       // all four epilogue warps agree, since they meet at named barriers below
@@ -1063,15 +1077,9 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
       const int nlm = t.l_max - m + 1;
       const int ls = t.lstart[it.mc];
       const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16);
-      const int Rg = it.rt * kOzRows + R0;
 #pragma unroll 1
       for (int q = 0; q < 2; ++q) {
-        const int fold = q ? 1 - it.par : it.par;
-        const int er = a.rexp[((int64_t)it.mc * 2 + fold) * a.rows_pad + Rg];
-        // the kOzAnaN (32) column exponents, one per lane, shared by shuffles
-        const int fe_l = __ldg(z.ana_fexp +
-                               ((int64_t)(it.mc * 2 + q) * 2 + it.par) * z.nlt * kOzAnaN +
-                               it.lt * kOzAnaN + lane);
+        const int er = er2[q], fe_l = fe2[q];
 #pragma unroll 1
         for (int c0 = 0; c0 < kOzAnaN; c0 += 16) {
           uint32_t cg[kOzGroups][16];
