@@ -436,7 +436,7 @@ __device__ __forceinline__ void cp_commit_wait_all() {
 // |value| of each (row, combo); pass 1 walks them again and writes the six
 // digit planes of every chunk at the row's scale.
 __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   const Tables& t = a.t;
   const int rt = blockIdx.x, mc = blockIdx.y;
   const int m = mc * t.minc;
