@@ -12,14 +12,16 @@
 //
 // Shared-memory layout of a row: element i sits at w64_pos<Q>(i).  A warp's
 // 16-byte accesses go to the banks a quarter warp at a time, eight slots per
-// pass over the 32 banks.  For Q = 4, 8, 12 each group of eight slots is
-// rotated by an amount that depends on the group, so that the stride-Q
-// scatter of the first pass (eight lanes whose indices agree modulo 8 in
-// pairs or all together) lands on distinct slots while every aligned run of
-// eight (the other passes' reads and writes) stays conflict-free; the
-// rotation of Q = 12 repeats every four groups, so that the stride-32 reads
-// keep constant address offsets.  For Q = 16 the stride-16 scatter is
-// conflict-free with one pad slot per 16 (i + i / 16).
+// pass over the 32 banks.  For Q = 4, 8, 12 the slot of i within its group of
+// eight is XORed with the group number (its low two bits; three for Q = 8),
+// so that the stride-Q scatter of the first pass (eight lanes whose indices
+// agree modulo 8 in pairs or all together) lands on distinct slots while every
+// aligned run of eight (the other passes' reads and writes) stays
+// conflict-free.  The pattern repeats every four groups (eight for Q = 8), so
+// an index shift by a multiple of 32 (64) moves an element by the same amount
+// and the strided reads use one per-lane base with constant offsets.  For
+// Q = 16 the stride-16 scatter is conflict-free with one pad slot per 16
+// (i + i / 16).
 #pragma once
 
 #include "fft.cuh"
@@ -94,18 +96,29 @@ __device__ __forceinline__ cplx<double> r2c_post_d(cplx<double> Zk, cplx<double>
   return {0.5 * (F.x + t.y), 0.5 * (F.y - t.x)};
 }
 
-// Rotation of slot group g of a row (see the file comment; Q = 4, 8, 12).
-template <int Q>
-__device__ __forceinline__ int w64_rot(int g) {
-  if constexpr (Q == 8) return g & 7;
-  else return g & 3;
-}
-
-// Shared-memory position of element i (< H) of a row.
+// Shared-memory position of element i (< H) of a row (see the file comment).
 template <int Q>
 __device__ __forceinline__ int w64_pos(int i) {
   if constexpr (Q == 16) return pad16(i);
-  else return (i & ~7) | ((i + w64_rot<Q>(i >> 3)) & 7);
+  else if constexpr (Q == 8) return i ^ ((i >> 3) & 7);
+  else return i ^ ((i >> 3) & 3);
+}
+
+// Whether an index shift by c moves every element by w64_disp<Q>(c), and by
+// how much (c a compile-time constant after unrolling).
+template <int Q>
+__host__ __device__ constexpr bool w64_shift_ok(int c) {
+  return Q == 16 ? c % 16 == 0 : Q == 8 ? c % 64 == 0 : c % 32 == 0;
+}
+template <int Q>
+__host__ __device__ constexpr int w64_disp(int c) {
+  return Q == 16 ? c + c / 16 : c;
+}
+
+// Element base + c of a row, base < 32 with position pb = w64_pos<Q>(base).
+template <int Q>
+__device__ __forceinline__ cplx<double>& w64_at(cplx<double>* row, int base, int pb, int c) {
+  return w64_shift_ok<Q>(c) ? row[pb + w64_disp<Q>(c)] : row[w64_pos<Q>(base + c)];
 }
 
 // Slots of a row, plus one so that rows S apart start on different bank
@@ -206,9 +219,10 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W
     return w;
   };
   cplx<double> v[Q];
+  const int pl = w64_pos<Q>(lane);
   // pass 1: radix Q, span 1: butterfly `lane` reads x[lane + 32 r]
 #pragma unroll
-  for (int r = 0; r < Q; ++r) v[r] = row[w64_pos<Q>(lane + 32 * r)];
+  for (int r = 0; r < Q; ++r) v[r] = w64_at<Q>(row, lane, pl, 32 * r);
   __syncwarp();
   dft_q_d<Q, INV>(v);
 #pragma unroll
@@ -219,7 +233,7 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W
 #pragma unroll
   for (int it = 0; it < NB4; ++it)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[w64_pos<Q>(lane + 32 * it + 8 * Q * r)];
+    for (int r = 0; r < 4; ++r) v[4 * it + r] = w64_at<Q>(row, lane, pl, 32 * it + 8 * Q * r);
   __syncwarp();
 #pragma unroll
   for (int it = 0; it < NB4; ++it) {
@@ -236,7 +250,7 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W
 #pragma unroll
   for (int it = 0; it < NB4; ++it)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) v[4 * it + r] = row[w64_pos<Q>(lane + 32 * it + 8 * Q * r)];
+    for (int r = 0; r < 4; ++r) v[4 * it + r] = w64_at<Q>(row, lane, pl, 32 * it + 8 * Q * r);
   __syncwarp();
 #pragma unroll
   for (int it = 0; it < NB4; ++it) {
@@ -256,10 +270,12 @@ __device__ __forceinline__ void w64_row_fft(cplx<double>* row, int lane, const W
   for (int it = 0; it < Q / 2; ++it) {
     const int j = lane + 32 * it;
     const cplx<double> w = cj(it ? cmul(wl, w64_root<Q>(it)) : wl);
-    cplx<double> u[2] = {row[w64_pos<Q>(j)], cmul(row[w64_pos<Q>(j + 16 * Q)], w)};
+    cplx<double>& x0 = w64_at<Q>(row, lane, pl, 32 * it);
+    cplx<double>& x1 = w64_at<Q>(row, lane, pl, 32 * it + 16 * Q);
+    cplx<double> u[2] = {x0, cmul(x1, w)};
     dft_small<2, INV>(u);
-    row[w64_pos<Q>(j)] = u[0];
-    row[w64_pos<Q>(j + 16 * Q)] = u[1];
+    x0 = u[0];
+    x1 = u[1];
   }
   __syncwarp();
 }

@@ -341,44 +341,56 @@ __global__ void __launch_bounds__(kNlW64Threads, 2) k_nl_bouss_w64(NlBoussArgs a
   const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
   const double LF = a.LFfac_r ? a.LFfac_r[r] : a.LFfac;
   double mr = 0.0, mh = 0.0;
-  for (int i = tid; i < H; i += kNlW64Threads) {
-    const int si = w64_pos<Q>(i);
-    cplx<double> zin[NFI];
+  // grid points p = tid + T u, u < kPts (three at n_phi = 768): point p is
+  // component p & 1 of complex element p >> 1, so every thread has the same
+  // number of points; a point's outputs overwrite its own inputs.  All the
+  // thread's inputs are loaded before any point is formed (so their latencies
+  // overlap and the points' arithmetic can interleave).
+  constexpr int NPT = 2 * H, kPts = (NPT + kNlW64Threads - 1) / kNlW64Threads;
+  const double* bd = reinterpret_cast<const double*>(buf);
+  double* bw = reinterpret_cast<double*>(buf);
+  double in[kPts][NFI];
+  int sp[kPts];
 #pragma unroll
-    for (int f = 0; f < NFI; ++f) zin[f] = buf[f * S + si];
-    double out[2][NFO];
+  for (int u = 0; u < kPts; ++u) {
+    const int p = tid + u * kNlW64Threads;
+    sp[u] = 2 * w64_pos<Q>((p < NPT ? p : 0) >> 1) + (p & 1);  // double index in a row
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {  // grid points 2i and 2i+1
-      auto v = [&](int f) { return h ? zin[f].y : zin[f].x; };
-      BoussIn fi;
-      constexpr int iv = BF::IV;
-      if constexpr (MAG) {
-        fi.br = v(0); fi.bt = v(1); fi.bp = v(2); fi.cbr = v(3); fi.cbt = v(4); fi.cbp = v(5);
-      } else {
-        fi.br = fi.bt = fi.bp = fi.cbr = fi.cbt = fi.cbp = 0.0;
-      }
-      fi.vr = v(iv); fi.vt = v(iv + 1); fi.vp = v(iv + 2);
-      fi.cvr = v(iv + 3); fi.cvt = v(iv + 4); fi.cvp = v(iv + 5);
-      fi.s = v(iv + 6);
-      fi.xi = 0.0;
-      if constexpr (CHEM) fi.xi = v(iv + 7);
-      double vr2, vh2;
-      courant_point(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, or2, or4, orho1, orho2,
-                    ost2, LF, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
-      mr = fmax(mr, vr2);
-      mh = fmax(mh, vh2);
-      BoussOut o;
-      bouss_point(fi, or2, or4, ost2, LF, MAG, o);
+    for (int f = 0; f < NFI; ++f) in[u][f] = p < NPT ? bd[f * 2 * S + sp[u]] : 0.0;
+  }
 #pragma unroll
-      for (int q = 0; q < 6; ++q) out[h][q] = o.o[q];
-      if constexpr (MAG) { out[h][6] = o.o[6]; out[h][7] = o.o[7]; out[h][8] = o.o[8]; }
-      if constexpr (CHEM) {
-        constexpr int c = MAG ? 9 : 6;
-        out[h][c] = o.o[9]; out[h][c + 1] = o.o[10]; out[h][c + 2] = o.o[11];
-      }
+  for (int u = 0; u < kPts; ++u) {
+    if (tid + u * kNlW64Threads >= NPT) break;
+    auto v = [&](int f) { return in[u][f]; };
+    BoussIn fi;
+    constexpr int iv = BF::IV;
+    if constexpr (MAG) {
+      fi.br = v(0); fi.bt = v(1); fi.bp = v(2); fi.cbr = v(3); fi.cbt = v(4); fi.cbp = v(5);
+    } else {
+      fi.br = fi.bt = fi.bp = fi.cbr = fi.cbt = fi.cbp = 0.0;
+    }
+    fi.vr = v(iv); fi.vt = v(iv + 1); fi.vp = v(iv + 2);
+    fi.cvr = v(iv + 3); fi.cvt = v(iv + 4); fi.cvp = v(iv + 5);
+    fi.s = v(iv + 6);
+    fi.xi = 0.0;
+    if constexpr (CHEM) fi.xi = v(iv + 7);
+    double vr2, vh2;
+    courant_point(a.cour_mode, fi.vr, fi.vt, fi.vp, fi.br, fi.bt, fi.bp, or2, or4, orho1, orho2,
+                  ost2, LF, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+    mr = fmax(mr, vr2);
+    mh = fmax(mh, vh2);
+    BoussOut o;
+    bouss_point(fi, or2, or4, ost2, LF, MAG, o);
+    double out[NFO];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) out[q] = o.o[q];
+    if constexpr (MAG) { out[6] = o.o[6]; out[7] = o.o[7]; out[8] = o.o[8]; }
+    if constexpr (CHEM) {
+      constexpr int c = MAG ? 9 : 6;
+      out[c] = o.o[9]; out[c + 1] = o.o[10]; out[c + 2] = o.o[11];
     }
 #pragma unroll
-    for (int q = 0; q < NFO; ++q) buf[q * S + si] = {out[0][q], out[1][q]};
+    for (int q = 0; q < NFO; ++q) bw[q * 2 * S + sp[u]] = out[q];
   }
   block_max2(mr, mh, red);
   if (tid == 0) {
