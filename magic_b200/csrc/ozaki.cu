@@ -121,6 +121,14 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+// 8 consecutive int32 columns of this thread's TMEM lane, without the wait.
+__device__ __forceinline__ void tmem_ld8_i32_nowait(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+
 // v 2^s rounded once, as ldexp rounds it, without a library call.  For
 // -1022 <= s <= 1023 it is one multiplication by the exact power of two.  The
 // epilogues' exponents never exceed 1023; below -1022, v 2^(s + 1022) is exact
@@ -154,7 +162,8 @@ __device__ __forceinline__ double oz_i2d(uint32_t w) {
 // P2 = (C3 2^7 + C4) 2^7 + C5 are integers below 2^38, exact in FP64, and the
 // sum P1 2^21 + P2 (below 2^59) is rounded by the final fma alone; callers
 // scale by 2^(e - 35).
-__device__ __forceinline__ double oz_combine_u(const uint32_t (&c)[kOzGroups][16], int i) {
+template <int W>
+__device__ __forceinline__ double oz_combine_u(const uint32_t (&c)[kOzGroups][W], int i) {
   static_assert(kOzGroups == 6, "two exact halves of three groups each");
   const double p1 = fma(fma(oz_i2d(c[0][i]), 128.0, oz_i2d(c[1][i])), 128.0, oz_i2d(c[2][i]));
   const double p2 = fma(fma(oz_i2d(c[3][i]), 128.0, oz_i2d(c[4][i])), 128.0, oz_i2d(c[5][i]));
@@ -559,7 +568,8 @@ constexpr int kOzStages = 4;     // analysis ring
 // holds an item's symmetric half until its antisymmetric half is formed, so
 // that the epilogue writes the north (sym + asym) and south (sym - asym) rows.
 constexpr int kOzSynStages = 3;
-constexpr int kOzSynEpiWarps = 8;  // two per TMEM lane quarter, 32 columns each
+constexpr int kOzSynEpiWarps = 16;  // four per TMEM lane quarter, 16 columns each
+constexpr int kOzSynEpiCols = kOzSynN / (kOzSynEpiWarps / 4);
 constexpr int kOzSynThreads = 64 + 32 * kOzSynEpiWarps;
 constexpr int kOzSynTmemCols = 512;
 
@@ -709,8 +719,8 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
       umma_commit(done);
     }
   } else {
-    // epilogue: warps 2-9; warp w owns TMEM lane quarter w % 4 and the 32
-    // accumulator columns of half (w - 2) / 4
+    // epilogue: warps 2 .. 2 + kOzSynEpiWarps - 1; warp w owns TMEM lane
+    // quarter w % 4 and the kOzSynEpiCols accumulator columns of slice (w - 2) / 4
     const int quarter = warp & 3, half = (warp - 2) >> 2;
     const int R0 = quarter * 32 + lane;
     int n = 0;
@@ -725,27 +735,29 @@ __global__ void __launch_bounds__(kOzSynThreads, 1) k_oz_synth_gemm(OzSynArgs a)
         // are issued before the wait for the accumulators
         const int er =
             R < a.nrows ? a.rexp[((int64_t)it.mc * 2 + combo) * a.rows_pad + R] : 0;
-        // column exponents of this warp's 32 columns, one per lane, shared by shuffles
+        // column exponents of this warp's columns, one per lane, shared by shuffles
         const int fe_l = __ldg(z.syn_fexp + ((int64_t)it.mc * 2 + combo) * nthw +
-                               it.tau * kOzSynN + 32 * half + lane);
+                               it.tau * kOzSynN + kOzSynEpiCols * half +
+                               (lane % kOzSynEpiCols));
         const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 22);
         if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
           live = false;
           break;
         }
         tc_fence_after();
-        const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16) + 32 * half;
+        const uint32_t taddr =
+            tbase + ((uint32_t)(32 * quarter) << 16) + kOzSynEpiCols * half;
 #pragma unroll 1
-        for (int c0 = 0; c0 < 32; c0 += 16) {
-          uint32_t cg[kOzGroups][16];
+        for (int c0 = 0; c0 < kOzSynEpiCols; c0 += 8) {
+          uint32_t cg[kOzGroups][8];
 #pragma unroll
           for (int g = 0; g < kOzGroups; ++g)
-            tmem_ld16_i32_nowait(taddr + g * kOzSynN + c0, cg[g]);
+            tmem_ld8_i32_nowait(taddr + g * kOzSynN + c0, cg[g]);
           tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
+          for (int i = 0; i < 8; ++i) {
             const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
-            const int col = 32 * half + c0 + i;
+            const int col = kOzSynEpiCols * half + c0 + i;
             const double v = oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
             double* st = stash + col * kOzRows + R0;  // this thread's own entry
             if (combo == 0) {
