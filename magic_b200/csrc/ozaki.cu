@@ -172,6 +172,10 @@ __device__ __forceinline__ double oz_combine_u(const uint32_t (&c)[kOzGroups][W]
 
 // Named barrier over `n` threads that also ANDs a predicate across them, so
 // that all participants take the same branch afterwards.
+__device__ __forceinline__ void named_bar_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(n) : "memory");
+}
+
 __device__ __forceinline__ bool bar_and(int id, int n, bool v) {
   uint32_t r;
   asm volatile(
@@ -928,7 +932,9 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_ana_pack(OzAnaArgs a) 
   }
 }
 
-constexpr int kOzAnaThreads = 64 + 128;
+constexpr int kOzAnaEpiWarps = 16;  // four per TMEM lane quarter: (table kind, 16 columns)
+constexpr int kOzAnaEpiThreads = 32 * kOzAnaEpiWarps;
+constexpr int kOzAnaThreads = 64 + kOzAnaEpiThreads;
 constexpr int kOzXS = kOzAnaN + 1;  // padded exchange row (doubles)
 
 struct OzAnaSmem {
@@ -982,7 +988,7 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
       mbar_init(&empty[s], 1);
     }
     mbar_init(tfull, 1);
-    mbar_init(tempty, 128);
+    mbar_init(tempty, kOzAnaEpiThreads);
     mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -1056,9 +1062,12 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
       umma_commit(done);
     }
   } else {
-    // epilogue: warps 2-5, thread e = tid - 64 owns TMEM lane R0 = 32 (warp % 4) + lane
+    // epilogue: warps 2 .. 2 + kOzAnaEpiWarps - 1, thread e = tid - 64; warp w
+    // owns TMEM lane quarter w % 4 (R0 = 32 (w % 4) + lane) and, for slice
+    // sl = (w - 2) / 4, the 16 columns 16 (sl & 1) .. of table kind q = sl / 2
     const int e = tid - 64;
-    const int quarter = warp & 3;
+    const int quarter = warp & 3, sl = (warp - 2) >> 2;
+    const int qs = sl >> 1, cs = 16 * (sl & 1);
     const int R0 = quarter * 32 + lane;
     double* xch = reinterpret_cast<double*>(smem + OzAnaSmem::xch_off);  // [2][128][kOzXS]
     double* cf = reinterpret_cast<double*>(smem + OzAnaSmem::tab_off);   // [64]
@@ -1068,64 +1077,58 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
       const Item it = decode(item);
       if (!it.live) continue;
-      // row and column exponents of both table kinds, loaded before the wait
-      // for the accumulators (they do not depend on the MMAs); the kOzAnaN (32)
-      // column exponents one per lane, shared by shuffles
+      // the row exponent and this warp's 16 column exponents (one per lane,
+      // shared by shuffles), loaded before the wait for the accumulators
+      // (they do not depend on the MMAs)
       const int Rg = it.rt * kOzRows + R0;
-      int er2[2], fe2[2];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int fold = q ? 1 - it.par : it.par;
-        er2[q] = a.rexp[((int64_t)it.mc * 2 + fold) * a.rows_pad + Rg];
-        fe2[q] = __ldg(z.ana_fexp + ((int64_t)(it.mc * 2 + q) * 2 + it.par) * z.nlt * kOzAnaN +
-                       it.lt * kOzAnaN + lane);
-      }
+      const int fold = qs ? 1 - it.par : it.par;
+      const int er = a.rexp[((int64_t)it.mc * 2 + fold) * a.rows_pad + Rg];
+      const int fe_l = __ldg(z.ana_fexp +
+                             ((int64_t)(it.mc * 2 + qs) * 2 + it.par) * z.nlt * kOzAnaN +
+                             it.lt * kOzAnaN + cs + (lane & 15));
       const bool ok = mbar_wait(tfull, n & 1, abort_flag, a.err, 32);
       ++n;
-      // all four epilogue warps agree, since they meet at named barriers below
-      if (!bar_and(1, 128, ok && !*abort_flag)) break;
+      // all epilogue warps agree, since they meet at named barriers below
+      if (!bar_and(1, kOzAnaEpiThreads, ok && !*abort_flag)) break;
       tc_fence_after();
       const int m = it.mc * t.minc;
       const int nlm = t.l_max - m + 1;
       const int ls = t.lstart[it.mc];
       const uint32_t taddr = tbase + ((uint32_t)(32 * quarter) << 16);
 #pragma unroll 1
-      for (int q = 0; q < 2; ++q) {
-        const int er = er2[q], fe_l = fe2[q];
-#pragma unroll 1
-        for (int c0 = 0; c0 < kOzAnaN; c0 += 16) {
-          uint32_t cg[kOzGroups][16];
+      for (int c0 = 0; c0 < 16; c0 += 8) {
+        uint32_t cg[kOzGroups][8];
 #pragma unroll
-          for (int g = 0; g < kOzGroups; ++g)
-            tmem_ld16_i32_nowait(taddr + (uint32_t)((q * kOzGroups + g) * kOzAnaN + c0), cg[g]);
-          tmem_wait_ld();
+        for (int g = 0; g < kOzGroups; ++g)
+          tmem_ld8_i32_nowait(taddr + (uint32_t)((qs * kOzGroups + g) * kOzAnaN + cs + c0), cg[g]);
+        tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
-            xch[(q * kOzRows + R0) * kOzXS + c0 + i] = oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
-          }
+        for (int i = 0; i < 8; ++i) {
+          const int fe = __shfl_sync(0xffffffffu, fe_l, c0 + i);
+          xch[(qs * kOzRows + R0) * kOzXS + cs + c0 + i] =
+              oz_scale(oz_combine_u(cg, i), er + fe - 12 - 35);
         }
       }
       tc_fence_before();
       mbar_arrive(tempty);  // the accumulators are free for the next item's MMAs
       // row-program tables of this item
       const double dm = (double)m;
-      for (int r = e; r < 2 * a.n_out; r += 128) {
+      for (int r = e; r < 2 * a.n_out; r += kOzAnaEpiThreads) {
         const RowOp op = a.ops[r];
         cf[2 * r] = oz_coef(op.kP, dm);
         cf[2 * r + 1] = oz_coef(op.kD, dm);
         colx[2 * r] = 2 * op.tP + op.cP;
         colx[2 * r + 1] = kOzRows + 2 * op.tD + op.cD;
       }
-      for (int i = e; i < kOzAnaN; i += 128) {
+      for (int i = e; i < kOzAnaN; i += kOzAnaEpiThreads) {
         const double l = (double)(m + 2 * (it.lt * kOzAnaN + i) + it.par);
         osc[i] = l > 0.0 ? 1.0 / (l * (l + 1.0)) : 0.0;
       }
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
+      named_bar_sync(1, kOzAnaEpiThreads);
       const int lev0 = it.rt * a.lev_tile;
       const int nlev = min(a.lev_tile, a.n_lev - lev0);
       const int nel = a.n_out * a.lev_tile * kOzAnaN;
-      for (int x = e; x < nel; x += 128) {
+      for (int x = e; x < nel; x += kOzAnaEpiThreads) {
         const int lv = x % a.lev_tile, rest = x / a.lev_tile;
         const int i = rest % kOzAnaN, o = rest / kOzAnaN;
         const int kk = it.lt * kOzAnaN + i, k = 2 * kk + it.par;
@@ -1139,7 +1142,7 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
         const double sc = a.ops[2 * o].scale ? osc[i] : 1.0;
         a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] = make_double2(sc * re, sc * im);
       }
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");  // exchange buffer free again
+      named_bar_sync(1, kOzAnaEpiThreads);  // exchange buffer free again
     }
   }
   __syncwarp();
