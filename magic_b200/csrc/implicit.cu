@@ -344,6 +344,9 @@ __device__ __forceinline__ void band_solve_rows_w(const BandView& b, int n_r, in
     double W[KL + 1];
 #pragma unroll
     for (int q = 0; q <= KL; ++q) W[q] = q < n_r ? __dmul_rn(b.fr[q], x[2 * q]) : 0.0;
+    // unrolled so that the loads of later steps (factors, pivots, incoming
+    // entries: independent of the running window) issue ahead of the chain
+#pragma unroll 4
     for (int k = 1; k <= n_r - 1; ++k) {  // L y = P (fr rhs), 1-based k
       const int d = b.piv[k - 1] - k;     // 0 .. KL
 #pragma unroll
@@ -372,6 +375,7 @@ __device__ __forceinline__ void band_solve_rows_w(const BandView& b, int n_r, in
       const int j = n_r - 1 - M1 + q;
       V[q] = j >= 0 ? x[2 * j] : 0.0;
     }
+#pragma unroll 4
     for (int k = n_r; k >= 1; --k) {
       V[M1] = band_div(V[M1], abd[(M - 1) * n_r + (k - 1)], b.rd[k - 1]);
       // b(lb + i) += t abd(la + i, k), i < lm = min(k, M) - 1, la = M - lm,
