@@ -195,10 +195,10 @@ class ClockSampler:
 # in proportion to the rows, so the full-size launch is scaled by its row count.
 NCU_PHI_TRAFFIC = {"split": (230.161408e6 + 104.267520e6) / (13 * 17 + 9 * 15),
                    # the FP64 phi kernel of the digit-split stage (k_nl_bouss_w64)
-                   "ozaki": (347.765248e6 + 177.672960e6) / (13 * 17 + 9 * 15)}
+                   "ozaki": (347.744000e6 + 178.849280e6) / (13 * 17 + 9 * 15)}
 # warp instructions of the same launch (smsp__inst_executed.sum), per Fourier row
 NCU_PHI_INST = {"split": 184287744.0 / (13 * 17 + 9 * 15),
-                "ozaki": 228199296.0 / (13 * 17 + 9 * 15)}
+                "ozaki": 209674368.0 / (13 * 17 + 9 * 15)}
 
 
 def measured_peaks():
