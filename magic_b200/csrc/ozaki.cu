@@ -1069,6 +1069,8 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
     const int quarter = warp & 3, sl = (warp - 2) >> 2;
     const int qs = sl >> 1, cs = 16 * (sl & 1);
     const int R0 = quarter * 32 + lane;
+    const int lv_e = e % a.lev_tile, rest_e = e / a.lev_tile;
+    const int ddq = kOzAnaEpiThreads / a.lev_tile, ddr = kOzAnaEpiThreads - ddq * a.lev_tile;
     double* xch = reinterpret_cast<double*>(smem + OzAnaSmem::xch_off);  // [2][128][kOzXS]
     double* cf = reinterpret_cast<double*>(smem + OzAnaSmem::tab_off);   // [64]
     int* colx = reinterpret_cast<int*>(cf + 64);                        // [64]
@@ -1128,19 +1130,29 @@ __global__ void __launch_bounds__(kOzAnaThreads, 1) k_oz_anal_gemm(OzAnaArgs a) 
       const int lev0 = it.rt * a.lev_tile;
       const int nlev = min(a.lev_tile, a.n_lev - lev0);
       const int nel = a.n_out * a.lev_tile * kOzAnaN;
+      // x = lv + lev_tile (i + kOzAnaN o) advances by the thread count: (lv,
+      // rest) step by (ddr, ddq) with a carry, no division in the loop
+      int lv = lv_e, rest = rest_e;
       for (int x = e; x < nel; x += kOzAnaEpiThreads) {
-        const int lv = x % a.lev_tile, rest = x / a.lev_tile;
         const int i = rest % kOzAnaN, o = rest / kOzAnaN;
+        const int lv_x = lv;
+        lv += ddr;
+        rest += ddq;
+        if (lv >= a.lev_tile) {
+          lv -= a.lev_tile;
+          ++rest;
+        }
         const int kk = it.lt * kOzAnaN + i, k = 2 * kk + it.par;
-        if (lv >= nlev || kk >= it.nk || k >= nlm) continue;
-        const int base = lv * a.cols;
+        if (lv_x >= nlev || kk >= it.nk || k >= nlm) continue;
+        const int base = lv_x * a.cols;
         const int r4 = 4 * o;
         const double re = cf[r4] * xch[(base + colx[r4]) * kOzXS + i] +
                           cf[r4 + 1] * xch[(base + colx[r4 + 1]) * kOzXS + i];
         const double im = cf[r4 + 2] * xch[(base + colx[r4 + 2]) * kOzXS + i] +
                           cf[r4 + 3] * xch[(base + colx[r4 + 3]) * kOzXS + i];
         const double sc = a.ops[2 * o].scale ? osc[i] : 1.0;
-        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv] = make_double2(sc * re, sc * im);
+        a.out[o][(int64_t)(ls + k) * a.ld + a.out_col0 + lev0 + lv_x] =
+            make_double2(sc * re, sc * im);
       }
       named_bar_sync(1, kOzAnaEpiThreads);  // exchange buffer free again
     }
