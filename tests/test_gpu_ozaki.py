@@ -34,6 +34,10 @@ CASES = [
     (127, 1, 4, True, False),
     (255, 1, 3, True, False),
     (383, 1, 3, False, False),
+    # the other warp-FFT row lengths of the FP64 phi kernel (n_phi 256, 512, 1024)
+    (85, 1, 3, True, False),
+    (170, 1, 3, True, True),
+    (341, 1, 3, False, False),
 ]
 PAIR = {"Advt": "Advp", "Advp": "Advt", "VxBt": "VxBp", "VxBp": "VxBt"}
 

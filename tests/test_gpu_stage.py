@@ -22,6 +22,10 @@ CASES = [
     # (n_phi 1152), on a few levels
     (255, 1, 3, True, False),
     (383, 1, 3, False, False),
+    # the other warp-FFT row lengths (n_phi 256, 512, 1024)
+    (85, 1, 3, True, False),
+    (170, 1, 3, True, True),
+    (341, 1, 3, False, False),
 ]
 
 
