@@ -1,5 +1,6 @@
 // extern "C" entry points (include/magic_b200.h).
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -340,16 +341,24 @@ namespace mt {
 
 // Fixed scratch of mt_scal_to_spat_noalloc.  Host code must not pass the
 // symbol itself to a kernel (on the host it names a stand-in, not device
-// memory): its device address is looked up with cudaGetSymbolAddress in the
-// context current at each call (a host-side lookup that allocates nothing once
-// the module is loaded), so an address never outlives its context (a
-// cudaDeviceReset, or another context made current on the same device).
+// memory): its device address is looked up once per device with
+// cudaGetSymbolAddress while that device is current.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[MT_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+constexpr int kNoallocMaxDevices = 64;
+static void* g_noalloc_ptr[kNoallocMaxDevices] = {};
 
 static int noalloc_scratch(void** out) {
-  void* ptr = nullptr;
-  MT_CHECK_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-  *out = ptr;
+  int dev = -1;
+  MT_CHECK_CUDA(cudaGetDevice(&dev));
+  MT_REQUIRE(dev >= 0 && dev < kNoallocMaxDevices, MT_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    MT_CHECK_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *out = g_noalloc_ptr[dev];
   return MT_OK;
 }
 
