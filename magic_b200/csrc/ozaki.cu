@@ -568,10 +568,10 @@ __global__ void __launch_bounds__(kOzPackThreads, 2) k_oz_syn_pack(OzSynArgs a) 
 
 constexpr int kOzStages = 4;     // analysis ring
 // Synthesis: one CTA per SM, six accumulator groups of kOzSynN = 64 columns
-// (384 of 512 TMEM columns), a 3-stage ring, and a shared-memory stash that
+// (384 of 512 TMEM columns), a 4-stage ring, and a shared-memory stash that
 // holds an item's symmetric half until its antisymmetric half is formed, so
 // that the epilogue writes the north (sym + asym) and south (sym - asym) rows.
-constexpr int kOzSynStages = 3;
+constexpr int kOzSynStages = 4;
 constexpr int kOzSynEpiWarps = 16;  // four per TMEM lane quarter, 16 columns each
 constexpr int kOzSynEpiCols = kOzSynN / (kOzSynEpiWarps / 4);
 constexpr int kOzSynThreads = 64 + 32 * kOzSynEpiWarps;
