@@ -301,8 +301,8 @@ def run_anel(args, rank, world):
     boundaries with the angular-momentum corrections, dt 1e-6; seeded
     perturbations |c_lm| ~ 1e-3 (l+1)^-2), through magic_b200.step.AnelasticStep:
     the fused split-precision anelastic stage, beside the FP64 stage (composed
-    from the FP64 transform kernels as the reference composes it), both with the
-    same FP64 solves; device-timed with the state resident (2.9 GB of spectral
+    from the FP64 transform kernels as the reference composes it) and the fused
+    digit-split stage, all with the same FP64 solves; device-timed with the state resident (2.9 GB of spectral
     arrays, larger than L2)."""
     from magic_b200.step import AnelasticStep
 
@@ -340,6 +340,13 @@ def run_anel(args, rank, world):
     st64 = build("fp64")
     n64 = max(1, min(args.steps, 3))
     ms64 = timed(st64, n64)
+    del st64
+    torch.cuda.empty_cache()
+    stoz = build("ozaki")
+    noz = max(1, min(args.steps, 5))
+    msoz = timed(stoz, noz)
+    del stoz
+    torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps({"metric": "anelastic CNAB2 steps/s @lmax=383 vs FP64 stage, 1 B200",
                           "value": 1000.0 / ms, "unit": "steps/s", "n_gpus": 1,
@@ -359,6 +366,12 @@ def run_anel(args, rank, world):
                                          "ms_per_step": ms64, "steps": n64,
                                          "speedup": ms64 / ms,
                                          "what": "the same steps with the FP64 anelastic stage"},
+                          "ozaki_stage": {"value": 1000.0 / msoz, "unit": "steps/s",
+                                          "ms_per_step": msoz, "steps": noz,
+                                          "speedup_vs_fp64": ms64 / msoz,
+                                          "what": "the same steps with the fused digit-split "
+                                                  "anelastic stage (int8 digit-plane GEMMs, "
+                                                  "FP64 phi stage; ~1e-12 of scale)"},
                           "clocks": clocks.summary()}), flush=True)
 
 

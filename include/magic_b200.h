@@ -224,14 +224,19 @@ MT_API int mt_nl_bouss(const mt_plan* plan, int n_r, const mt_bouss_in* in,
                 const mt_bouss_out* out, const mt_bouss_params* p, double* dtrkc,
                 double* dthkc, void* work, size_t work_bytes, void* stream);
 
-/* ---- fused anelastic nonlinear stage (split precision) --------------------
+/* ---- fused anelastic nonlinear stage (split, digit-split precision) --------
  * The nonlinear part of radial_loop_anel (magic_torch/step_time.py:1215-1475):
  * Legendre synthesis of the 18 grid fields (19 with composition; velocity and
  * its derivatives zero on the two boundary levels as in the reference),
  * get_nl_anel products with viscous and Ohmic heating (get_nl_anel.py:41-136)
  * and Courant maxima in the phi stage, Legendre analysis of the bulk levels.
- * Requires a plan created with MT_PREC_SPLIT (FP64 callers compose the
- * drop-in transforms and mt_get_nl_anel exactly as radial_loop_anel does).
+ * Requires a plan created with MT_PREC_SPLIT (tcgen05 bf16x3 GEMMs, FP32 phi
+ * stage) or MT_PREC_OZAKI (int8 digit-plane GEMMs, FP64 phi stage, ~1e-12 of
+ * scale); FP64 plans compose the drop-in transforms and mt_get_nl_anel
+ * exactly as radial_loop_anel does.  On MT_PREC_OZAKI plans whose n_phi is
+ * too long for the FP64 phi stage's shared-memory buffers (the magnetic case
+ * at n_phi = 1152) mt_nl_anel_workspace returns 0 and mt_nl_anel
+ * MT_ERR_UNSUPPORTED: compose the stage there too.
  * Inputs: spectral (lm_max, ld) complex over n_r levels; b .. dj NULL
  * without magnetic field, xi NULL without composition. */
 typedef struct {

@@ -1048,9 +1048,9 @@ struct OzWs {
   int cols, lev_tile;
 };
 
-static OzWs oz_ws(const mt_plan* p, int n_r, int mag, int chem) {
+// Workspace of a digit-split stage with nfi grid fields and nfo products.
+static OzWs oz_stage_ws(const mt_plan* p, int n_r, int nfi, int nfo) {
   OzWs w;
-  const int nfi = bouss_nfi(mag, chem), nfo = bouss_nfo(mag, chem);
   w.rows_syn = (int64_t)n_r * 2 * nfi;
   w.rows_pad_s = (w.rows_syn + 127) / 128 * 128;
   w.g_level = 2 * nfo;  // doubles per level (even: 16-byte pieces)
@@ -1070,6 +1070,10 @@ static OzWs oz_ws(const mt_plan* p, int n_r, int mag, int chem) {
   const size_t ana = oz_ana_image_bytes(p->n_m, p->nhs, n_r - 2, w.lev_tile);
   w.total = w.aimg + al(std::max(syn, ana));
   return w;
+}
+
+static OzWs oz_ws(const mt_plan* p, int n_r, int mag, int chem) {
+  return oz_stage_ws(p, n_r, bouss_nfi(mag, chem), bouss_nfo(mag, chem));
 }
 
 template <bool MAG, bool CHEM>
@@ -1168,6 +1172,100 @@ static int nl_bouss_ozaki_t(const mt_plan* p, int n_r, const mt_bouss_in* in,
 
 namespace mt {
 
+// Source arrays, terms and row programs of the anelastic stage's synthesis
+// (the input assembly of radial_loop_anel, magic_torch/step_time.py:1233-1316),
+// shared by the split and digit-split argument blocks; returns the rows per
+// level (2 per grid field, in the field order of nl_point.cuh).
+template <typename A>
+static int fill_anel_synth(A& s, const mt_anel_in* in, bool mag, bool chem) {
+  int na = 0;
+  auto arr = [&](const double* ptr) {
+    s.arr[na] = (const double2*)ptr;
+    return na++;
+  };
+  int x = 0;
+  auto term = [&](int ia, int ib, int recipe) {
+    s.term[x].ia = (int8_t)ia;
+    s.term[x].ib = (int8_t)ib;
+    s.term[x].recipe = (int8_t)recipe;
+    s.term[x].pad = 0;
+    return x++;
+  };
+  const int iw = arr(in->w), idw = arr(in->dw), iddw = arr(in->ddw), iz = arr(in->z),
+            idz = arr(in->dz), is = arr(in->s);
+  const int tQv = term(iw, 0, kDlh), tdw = term(idw, 0, kRaw), tz = term(iz, 0, kRaw);
+  const int tQd = term(idw, 0, kDlh), tddw = term(iddw, 0, kRaw), tdz = term(idz, 0, kRaw);
+  const int tcv = term(iz, 0, kDlh), ts = term(is, 0, kRaw);
+  RowOp* o = s.ops;
+  syn_group_ops(o, tQv, tdw, tz);       // vr vt vp
+  syn_group_ops(o + 6, tQd, tddw, tdz);  // dvrdr dvtdr dvpdr
+  // dvrdt, dvrdp = grad of l(l+1) w: (dP X, i m P X)
+  o[12] = rop(0, 0, 0, tQv, 0, 1);
+  o[13] = rop(0, 0, 0, tQv, 1, 1);
+  o[14] = rop(tQv, 1, 4);
+  o[15] = rop(tQv, 0, 3);
+  // dvtdp, dvpdp before 1/sin^2: theta = i m dP dw - m^2 P z, phi = -m^2 P dw - i m dP z
+  o[16] = rop(tz, 0, 5, tdw, 1, 4);
+  o[17] = rop(tz, 1, 5, tdw, 0, 3);
+  o[18] = rop(tdw, 0, 5, tz, 1, 3);
+  o[19] = rop(tdw, 1, 5, tz, 0, 4);
+  ana_scalar_ops(o + 20, tcv);  // cvr = l(l+1) z
+  ana_scalar_ops(o + 22, ts);   // s
+  int rows = 24;
+  if (chem) {
+    const int ixi = arr(in->xi);
+    ana_scalar_ops(o + rows, term(ixi, 0, kRaw));
+    rows += 2;
+  }
+  if (mag) {
+    const int ib = arr(in->b), idb = arr(in->db), iaj = arr(in->aj), idj = arr(in->dj),
+              iddb = arr(in->ddb);
+    const int tQb = term(ib, 0, kDlh), tdb = term(idb, 0, kRaw), taj = term(iaj, 0, kRaw);
+    const int tQa = term(iaj, 0, kDlh), tdj = term(idj, 0, kRaw), tcT = term(ib, iddb, kCurlT);
+    syn_group_ops(o + rows, tQb, tdb, taj);
+    syn_group_ops(o + rows + 6, tQa, tdj, tcT);
+    rows += 12;
+  }
+  s.narr = na;
+  return rows;
+}
+
+// Row programs and outputs of the anelastic stage's analysis (the forward
+// transforms of radial_loop_anel, magic_torch/step_time.py:1319-1370) over the
+// products of nl_point.cuh; returns the number of outputs.
+template <typename A>
+static int fill_anel_anal(A& a, const mt_anel_out* out, bool mag, bool chem) {
+  int o = 0, r = 0;
+  r += ana_scalar_ops(&a.ops[r], 0);
+  a.out[o++] = (double2*)out->Advr;
+  r += ana_s_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advt;
+  r += ana_t_ops(&a.ops[r], 1, 2);
+  a.out[o++] = (double2*)out->Advp;
+  r += ana_scalar_ops(&a.ops[r], 3);
+  a.out[o++] = (double2*)out->VSr;
+  r += ana_s_ops(&a.ops[r], 4, 5);
+  a.out[o++] = (double2*)out->VSt;
+  if (mag) {
+    r += ana_scalar_ops(&a.ops[r], 6);
+    a.out[o++] = (double2*)out->VxBr;
+    r += ana_s_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBt;
+    r += ana_t_ops(&a.ops[r], 7, 8);
+    a.out[o++] = (double2*)out->VxBp;
+  }
+  if (chem) {
+    const int x0 = mag ? 9 : 6;
+    r += ana_scalar_ops(&a.ops[r], x0);
+    a.out[o++] = (double2*)out->VXir;
+    r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
+    a.out[o++] = (double2*)out->VXit;
+  }
+  r += ana_scalar_ops(&a.ops[r], anel_nfo(mag, chem) - 1);
+  a.out[o++] = (double2*)out->heat;
+  return o;
+}
+
 // Fused anelastic stage in split precision: synthesis (input assembly of
 // radial_loop_anel, magic_torch/step_time.py:1233-1316), phi stage
 // (nl_anel_split.cu), analysis of the bulk levels (:1329-1391), Courant steps.
@@ -1189,55 +1287,7 @@ static int nl_anel_split_t(const mt_plan* p, int n_r, const mt_anel_in* in,
     SplitSynArgs s{};
     s.t = p->tab;
     s.s = split_tables(p);
-    int na = 0;
-    auto arr = [&](const double* ptr) {
-      s.arr[na] = (const double2*)ptr;
-      return na++;
-    };
-    int x = 0;
-    auto term = [&](int ia, int ib, int recipe) {
-      s.term[x].ia = (int8_t)ia;
-      s.term[x].ib = (int8_t)ib;
-      s.term[x].recipe = (int8_t)recipe;
-      s.term[x].pad = 0;
-      return x++;
-    };
-    const int iw = arr(in->w), idw = arr(in->dw), iddw = arr(in->ddw), iz = arr(in->z),
-              idz = arr(in->dz), is = arr(in->s);
-    const int tQv = term(iw, 0, kDlh), tdw = term(idw, 0, kRaw), tz = term(iz, 0, kRaw);
-    const int tQd = term(idw, 0, kDlh), tddw = term(iddw, 0, kRaw), tdz = term(idz, 0, kRaw);
-    const int tcv = term(iz, 0, kDlh), ts = term(is, 0, kRaw);
-    RowOp* o = s.ops;
-    syn_group_ops(o, tQv, tdw, tz);       // vr vt vp
-    syn_group_ops(o + 6, tQd, tddw, tdz);  // dvrdr dvtdr dvpdr
-    // dvrdt, dvrdp = grad of l(l+1) w: (dP X, i m P X)
-    o[12] = rop(0, 0, 0, tQv, 0, 1);
-    o[13] = rop(0, 0, 0, tQv, 1, 1);
-    o[14] = rop(tQv, 1, 4);
-    o[15] = rop(tQv, 0, 3);
-    // dvtdp, dvpdp before 1/sin^2: theta = i m dP dw - m^2 P z, phi = -m^2 P dw - i m dP z
-    o[16] = rop(tz, 0, 5, tdw, 1, 4);
-    o[17] = rop(tz, 1, 5, tdw, 0, 3);
-    o[18] = rop(tdw, 0, 5, tz, 1, 3);
-    o[19] = rop(tdw, 1, 5, tz, 0, 4);
-    ana_scalar_ops(o + 20, tcv);  // cvr = l(l+1) z
-    ana_scalar_ops(o + 22, ts);   // s
-    int rows = 24;
-    if (CHEM) {
-      const int ixi = arr(in->xi);
-      ana_scalar_ops(o + rows, term(ixi, 0, kRaw));
-      rows += 2;
-    }
-    if (MAG) {
-      const int ib = arr(in->b), idb = arr(in->db), iaj = arr(in->aj), idj = arr(in->dj),
-                iddb = arr(in->ddb);
-      const int tQb = term(ib, 0, kDlh), tdb = term(idb, 0, kRaw), taj = term(iaj, 0, kRaw);
-      const int tQa = term(iaj, 0, kDlh), tdj = term(idj, 0, kRaw), tcT = term(ib, iddb, kCurlT);
-      syn_group_ops(o + rows, tQb, tdb, taj);
-      syn_group_ops(o + rows + 6, tQa, tdj, tcT);
-      rows += 12;
-    }
-    s.narr = na;
+    const int rows = fill_anel_synth(s, in, MAG, CHEM);
     s.n_lev = n_r;
     s.ld = in->ld;
     s.or2 = q->or2;
@@ -1304,35 +1354,7 @@ static int nl_anel_split_t(const mt_plan* p, int n_r, const mt_anel_in* in,
   a.g_j = g_j;
   a.g_level = W.g_level;
   a.n_lev = n_r - 2;
-  int o = 0, r = 0;
-  r += ana_scalar_ops(&a.ops[r], 0);
-  a.out[o++] = (double2*)out->Advr;
-  r += ana_s_ops(&a.ops[r], 1, 2);
-  a.out[o++] = (double2*)out->Advt;
-  r += ana_t_ops(&a.ops[r], 1, 2);
-  a.out[o++] = (double2*)out->Advp;
-  r += ana_scalar_ops(&a.ops[r], 3);
-  a.out[o++] = (double2*)out->VSr;
-  r += ana_s_ops(&a.ops[r], 4, 5);
-  a.out[o++] = (double2*)out->VSt;
-  if (MAG) {
-    r += ana_scalar_ops(&a.ops[r], 6);
-    a.out[o++] = (double2*)out->VxBr;
-    r += ana_s_ops(&a.ops[r], 7, 8);
-    a.out[o++] = (double2*)out->VxBt;
-    r += ana_t_ops(&a.ops[r], 7, 8);
-    a.out[o++] = (double2*)out->VxBp;
-  }
-  if (CHEM) {
-    const int x0 = MAG ? 9 : 6;
-    r += ana_scalar_ops(&a.ops[r], x0);
-    a.out[o++] = (double2*)out->VXir;
-    r += ana_s_ops(&a.ops[r], x0 + 1, x0 + 2);
-    a.out[o++] = (double2*)out->VXit;
-  }
-  r += ana_scalar_ops(&a.ops[r], nfo - 1);
-  a.out[o++] = (double2*)out->heat;
-  a.n_out = o;
+  a.n_out = fill_anel_anal(a, out, MAG, CHEM);
   a.cols = 2 * nfo;
   a.lev_tile = 128 / a.cols;
   a.ld = out->ld;
@@ -1340,6 +1362,111 @@ static int nl_anel_split_t(const mt_plan* p, int n_r, const mt_anel_in* in,
   a.aimg = (uint8_t*)(w + W.aimg);
   a.err = err;
   MT_TRY(launch_anal_split(a, st));
+  return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
+}
+
+// The digit-split anelastic stage runs where one CTA of its FP64 phi stage
+// holds a (theta row, level)'s buffers in shared memory.
+static bool anel_ozaki_fits(const mt_plan* p, int mag, int chem) {
+  return nl_anel_f64_smem(p->n_phi, mag, chem) > 0;
+}
+
+// Fused anelastic stage in digit-split precision: the synthesis row programs
+// of the split stage on the int8 digit-plane GEMMs (ozaki.cu), the FP64 phi
+// stage k_nl_anel_f64, and the analysis row programs on the digit-plane GEMMs,
+// with FP64 rows between them.
+template <bool MAG, bool CHEM>
+static int nl_anel_ozaki_t(const mt_plan* p, int n_r, const mt_anel_in* in,
+                           const mt_anel_out* out, const mt_anel_stage_params* q, double* dtrkc,
+                           double* dthkc, void* work, cudaStream_t st) {
+  const OzWs W = oz_stage_ws(p, n_r, anel_nfi(MAG, CHEM), anel_nfo(MAG, CHEM));
+  char* w = (char*)work;
+  int* err = (int*)(w + W.err);
+  double* Fs = (double*)(w + W.fs);
+  double* Gs = (double*)(w + W.gs);
+  unsigned long long* mx = (unsigned long long*)(w + W.mx);
+  const int64_t fs_j = W.rows_syn, fs_c = (int64_t)p->nhs * fs_j, fs_m = 2 * fs_c;
+  const int64_t g_j = (int64_t)(n_r - 2) * W.g_level, g_h = (int64_t)p->nhs * g_j, g_m = 2 * g_h;
+  MT_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  {
+    OzSynArgs s{};
+    s.t = p->tab;
+    s.z = ozaki_tables(p);
+    const int rows = fill_anel_synth(s, in, MAG, CHEM);
+    s.n_lev = n_r;
+    s.ld = in->ld;
+    s.or2 = q->or2;
+    s.nrows = (int)W.rows_syn;
+    s.row_per_level = rows;
+    s.stg_lev = std::min(n_r, 127 / rows + 2);
+    s.aimg = (uint8_t*)(w + W.aimg);
+    s.total_chunks = ozaki_syn_total_chunks(p);
+    s.rexp = (int*)(w + W.rexs);
+    s.rows_pad = W.rows_pad_s;
+    s.Fs = Fs;
+    s.fs_m = fs_m;
+    s.fs_c = fs_c;
+    s.fs_j = fs_j;
+    s.err = err;
+    MT_TRY(launch_oz_synth(s, st));
+  }
+  {
+    MT_CHECK_CUDA(cudaMemsetAsync(mx, 0, 2 * n_r * sizeof(unsigned long long), st));
+    NlAnelArgs nl{};
+    nl.t = p->tab;
+    nl.n_r = n_r;
+    nl.Fs64 = Fs;
+    nl.fs_m = fs_m;
+    nl.fs_c = fs_c;
+    nl.fs_j = fs_j;
+    nl.G64 = Gs;
+    nl.g_m = g_m;
+    nl.g_h = g_h;
+    nl.g_j = g_j;
+    nl.g_level = W.g_level;
+    nl.r = q->r;
+    nl.or1 = q->or1;
+    nl.or2 = q->or2;
+    nl.or4 = q->or4;
+    nl.beta = q->beta;
+    nl.orho1 = q->orho1;
+    nl.orho2 = q->orho2;
+    nl.otemp1 = q->otemp1;
+    nl.visc = q->visc;
+    nl.lambda_ = q->lambda_;
+    nl.delxr2 = q->delxr2;
+    nl.delxh2 = q->delxh2;
+    nl.LFfac = q->LFfac;
+    nl.ViscHeatFac = q->ViscHeatFac;
+    nl.OhmLossFac = MAG ? q->OhmLossFac : 0.0;
+    nl.cour_mode = MAG ? q->cour_mode : 0;
+    nl.cf2 = q->courfac * q->courfac;
+    nl.af2 = q->alffac * q->alffac;
+    const double h = 0.5 * (1.0 + q->opm);
+    nl.valfac = h * h;
+    nl.vr2max = mx;
+    nl.vh2max = mx + n_r;
+    MT_TRY(launch_nl_anel_f64(MAG, CHEM, nl, st));
+  }
+  OzAnaArgs a{};
+  a.t = p->tab;
+  a.z = ozaki_tables(p);
+  a.G = Gs;
+  a.g_m = g_m;
+  a.g_h = g_h;
+  a.g_j = g_j;
+  a.g_level = W.g_level;
+  a.n_lev = n_r - 2;
+  a.n_out = fill_anel_anal(a, out, MAG, CHEM);
+  a.cols = W.cols;
+  a.lev_tile = W.lev_tile;
+  a.ld = out->ld;
+  a.out_col0 = 1;
+  a.aimg = (uint8_t*)(w + W.aimg);
+  a.rexp = (int*)(w + W.rexa);
+  a.rows_pad = W.rows_pad_a;
+  a.err = err;
+  MT_TRY(launch_oz_anal(a, st));
   return launch_courant_finish(n_r, mx, mx + n_r, q->delxr2, q->delxh2, dtrkc, dthkc, st);
 }
 
@@ -1399,17 +1526,25 @@ int mt_nl_bouss(const mt_plan* p, int n_r, const mt_bouss_in* in, const mt_bouss
 
 
 size_t mt_nl_anel_workspace(const mt_plan* p, int n_r, int l_mag, int l_chem) {
-  if (!p || n_r < 3 || p->precision != MT_PREC_SPLIT) return 0;
-  return split_stage_ws(p, n_r, anel_nfi(l_mag, l_chem), anel_nfo(l_mag, l_chem)).total;
+  if (!p || n_r < 3) return 0;
+  if (p->precision == MT_PREC_SPLIT)
+    return split_stage_ws(p, n_r, anel_nfi(l_mag, l_chem), anel_nfo(l_mag, l_chem)).total;
+  if (p->precision == MT_PREC_OZAKI && anel_ozaki_fits(p, l_mag, l_chem))
+    return oz_stage_ws(p, n_r, anel_nfi(l_mag, l_chem), anel_nfo(l_mag, l_chem)).total;
+  return 0;
 }
 
 int mt_nl_anel(const mt_plan* p, int n_r, const mt_anel_in* in, const mt_anel_out* out,
                const mt_anel_stage_params* q, double* dtrkc, double* dthkc, void* work,
                size_t work_bytes, void* stream) {
   MT_TRY(check_plan(p));
-  MT_REQUIRE(p->precision == MT_PREC_SPLIT, MT_ERR_UNSUPPORTED,
-             "mt_nl_anel needs a MT_PREC_SPLIT plan (FP64 callers compose the drop-in "
-             "transforms and mt_get_nl_anel as radial_loop_anel does)");
+  MT_REQUIRE(p->precision == MT_PREC_SPLIT || p->precision == MT_PREC_OZAKI, MT_ERR_UNSUPPORTED,
+             "mt_nl_anel needs a MT_PREC_SPLIT or MT_PREC_OZAKI plan (FP64 callers compose "
+             "the drop-in transforms and mt_get_nl_anel as radial_loop_anel does)");
+  MT_REQUIRE(p->precision != MT_PREC_OZAKI || !q || anel_ozaki_fits(p, q->l_mag, q->l_chem),
+             MT_ERR_UNSUPPORTED,
+             "n_phi too long for the digit-split anelastic stage's phi buffers (compose the "
+             "drop-in transforms and mt_get_nl_anel instead)");
   MT_REQUIRE(in && out && q && dtrkc && dthkc && n_r >= 3, MT_ERR_ARG, "bad argument");
   MT_REQUIRE(in->w && in->dw && in->ddw && in->z && in->dz && in->s, MT_ERR_ARG,
              "null velocity/entropy input");
@@ -1429,6 +1564,13 @@ int mt_nl_anel(const mt_plan* p, int n_r, const mt_anel_in* in, const mt_anel_ou
   MT_REQUIRE(work && work_bytes >= mt_nl_anel_workspace(p, n_r, q->l_mag, q->l_chem),
              MT_ERR_WORKSPACE, "workspace too small");
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->precision == MT_PREC_OZAKI) {
+    if (q->l_mag)
+      return q->l_chem ? nl_anel_ozaki_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                       : nl_anel_ozaki_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+    return q->l_chem ? nl_anel_ozaki_t<false, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
+                     : nl_anel_ozaki_t<false, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);
+  }
   if (q->l_mag)
     return q->l_chem ? nl_anel_split_t<true, true>(p, n_r, in, out, q, dtrkc, dthkc, work, st)
                      : nl_anel_split_t<true, false>(p, n_r, in, out, q, dtrkc, dthkc, work, st);

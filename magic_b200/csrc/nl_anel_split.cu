@@ -23,75 +23,6 @@
 
 namespace mt {
 
-template <bool MAG, bool CHEM>
-struct AnelFields {
-  static constexpr int NFI = 12 + (CHEM ? 1 : 0) + (MAG ? 6 : 0);
-  static constexpr int NFO = 7 + (MAG ? 3 : 0) + (CHEM ? 3 : 0);
-  static constexpr int NB = NFI > NFO ? NFI : NFO;
-  static constexpr int IB = 12 + (CHEM ? 1 : 0);  // first magnetic grid field
-  static constexpr int IX = 6 + (MAG ? 3 : 0);    // first composition product
-  static constexpr int THW = 32 * ((NB + 1) / 2);  // threads of the half-warp variant
-  __host__ __device__ static constexpr bool radial(int o) {
-    return o == 0 || o == 3 || (MAG && o == 6) || (CHEM && o == IX) || o == NFO - 1;
-  }
-};
-
-// Per-level constants of the products in FP32.
-struct AnelLevel {
-  float R, or1, or2, or4, beta, orho1, otemp1, visc, lam, LF, vhf, ohm;
-};
-
-// get_nl_anel at one grid point (magic_torch/get_nl_anel.py:63-136).
-template <bool MAG, bool CHEM>
-__device__ __forceinline__ void anel_point(const float* v, const AnelLevel& L, float ost2,
-                                           float cosn, float* o) {
-  using F = AnelFields<MAG, CHEM>;
-  const float vr = v[0], vt = v[1], vp = v[2], dvrdr = v[3], dvtdr = v[4], dvpdr = v[5];
-  const float dvrdt = v[6], dvrdp = v[7], dvtdp = v[8], dvpdp = v[9], cvr = v[10], s = v[11];
-  float LFr = 0.f, LFt = 0.f, LFp = 0.f;
-  float br = 0.f, bt = 0.f, bp = 0.f, cbr = 0.f, cbt = 0.f, cbp = 0.f;
-  if constexpr (MAG) {
-    br = v[F::IB]; bt = v[F::IB + 1]; bp = v[F::IB + 2];
-    cbr = v[F::IB + 3]; cbt = v[F::IB + 4]; cbp = v[F::IB + 5];
-    LFr = L.LF * ost2 * (cbt * bp - cbp * bt);
-    LFt = L.LF * L.or4 * (cbp * br - cbr * bp);
-    LFp = L.LF * L.or4 * (cbr * bt - cbt * br);
-  }
-  o[0] = -L.or2 * L.orho1 * (vr * (dvrdr - (2.f * L.or1 + L.beta) * vr) +
-                             ost2 * (vt * (dvrdt - L.R * vt) + vp * (dvrdp - L.R * vp))) + LFr;
-  o[1] = L.or4 * L.orho1 * (-vr * (dvtdr - L.beta * vt) + vt * (cosn * vt + dvpdp + dvrdr) +
-                            vp * (cosn * vp - dvtdp)) + LFt;
-  o[2] = L.or4 * L.orho1 * (-vr * (dvpdr - L.beta * vp) - vt * (dvtdp + cvr) - vp * dvpdp) + LFp;
-  o[3] = vr * s;
-  o[4] = L.or2 * vt * s;
-  o[5] = L.or2 * vp * s;
-  if constexpr (MAG) {
-    o[6] = L.orho1 * ost2 * (vt * bp - vp * bt);
-    o[7] = L.orho1 * L.or4 * (vp * br - vr * bp);
-    o[8] = L.orho1 * L.or4 * (vr * bt - vt * br);
-  }
-  if constexpr (CHEM) {
-    const float xi = v[12];
-    o[F::IX] = vr * xi;
-    o[F::IX + 1] = L.or2 * vt * xi;
-    o[F::IX + 2] = L.or2 * vp * xi;
-  }
-  const float prefac = L.vhf * L.or4 * L.orho1 * L.otemp1 * L.visc;
-  const float beta_r = L.beta * L.R;
-  const float e_rr = dvrdr - (2.f * L.or1 + L.beta) * vr;
-  const float e_tt = cosn * vt + dvpdp + dvrdr - L.or1 * vr;
-  const float e_pp = dvpdp + cosn * vt + L.or1 * vr;
-  const float e_tp = 2.f * dvtdp + cvr - 2.f * cosn * vp;
-  const float e_rt = L.R * dvtdr - (2.f + beta_r) * vt + L.or1 * dvrdt;
-  const float e_rp = L.R * dvpdr - (2.f + beta_r) * vp + L.or1 * dvrdp;
-  const float bv = L.beta * vr;
-  float heat = prefac * (2.f * e_rr * e_rr + 2.f * e_tt * e_tt + 2.f * e_pp * e_pp + e_tp * e_tp +
-                         ost2 * (e_rt * e_rt + e_rp * e_rp) - (2.f / 3.f) * bv * bv);
-  if constexpr (MAG)
-    heat += L.ohm * L.lam * L.or2 * L.otemp1 * (L.or2 * cbr * cbr + ost2 * (cbt * cbt + cbp * cbp));
-  o[F::NFO - 1] = heat;
-}
-
 template <bool MAG, bool CHEM, int Q>
 __global__ void __launch_bounds__(Q > 0 ? AnelFields<MAG, CHEM>::THW : 256)
     k_nl_anel_split(NlAnelArgs a) {
@@ -157,7 +88,7 @@ __global__ void __launch_bounds__(Q > 0 ? AnelFields<MAG, CHEM>::THW : 256)
   __syncthreads();
 
   const bool bnd = r == 0 || r == a.n_r - 1;
-  AnelLevel L;
+  AnelLevel<float> L;
   L.R = (float)a.r[r];
   L.or1 = (float)a.or1[r];
   L.or2 = (float)a.or2[r];
@@ -202,7 +133,7 @@ __global__ void __launch_bounds__(Q > 0 ? AnelFields<MAG, CHEM>::THW : 256)
       mh = fmaxf(mh, vh2);
       if (!bnd) {
         float o[NFO];
-        anel_point<MAG, CHEM>(v, L, ost2, cosn, o);
+        anel_point<float, MAG, CHEM>(v, L, ost2, cosn, o);
 #pragma unroll
         for (int q = 0; q < NFO; ++q) {
           if (h) buf[q * S + si].y = o[q];

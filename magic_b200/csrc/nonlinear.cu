@@ -15,6 +15,8 @@
 #include "fft.cuh"
 #include "fft_w64.cuh"
 #include "fourier.cuh"
+#include "nl_point.cuh"
+#include "split_kernels.cuh"
 
 namespace mt {
 
@@ -478,6 +480,153 @@ static int launch_nl_bouss_io(bool mag, bool chem, const NlBoussArgs& a, cudaStr
                 : launch_nl_bouss_t<true, false, SPLIT_IO>(a, st);
   return chem ? launch_nl_bouss_t<false, true, SPLIT_IO>(a, st)
               : launch_nl_bouss_t<false, false, SPLIT_IO>(a, st);
+}
+
+// ------------------------------------------------------- fused anelastic (FP64)
+
+// The phi stage of the digit-split anelastic radial loop.  One CTA per
+// (theta row, level) with the block FFT: the synthesis wrote this hemisphere's
+// Fourier rows of the grid fields in FP64 (NlAnelArgs::Fs64; field order of
+// nl_point.cuh), the kernel inverse-transforms them, evaluates get_nl_anel
+// (magic_torch/get_nl_anel.py:63-136, viscous and Ohmic heating included) and
+// the Courant maxima (magic_torch/courant.py:25-77) at every grid point in
+// FP64, and forward-transforms the 10-13 products into the weighted rows the
+// analysis reads (NlAnelArgs::G64).  Velocity, its derivatives and cvr are
+// zero on the two boundary levels (radial_loop_anel synthesises them on the
+// bulk levels only, magic_torch/step_time.py:1233-1316); the phi-derivative
+// fields get their 1/sin^2(theta) factor here (torpol_to_dphspat,
+// magic_torch/sht.py:725-743).
+constexpr int kNlAnelThreads = 512;
+
+template <bool MAG, bool CHEM>
+__global__ void __launch_bounds__(kNlAnelThreads) k_nl_anel_f64(NlAnelArgs a) {
+  using F = AnelFields<MAG, CHEM>;
+  constexpr int NFI = F::NFI, NFO = F::NFO, NB = F::NB, T = kNlAnelThreads;
+  extern __shared__ double smem[];
+  __shared__ double red[32];
+  cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);
+  const Tables& t = a.t;
+  const int N = t.n_phi, H = N / 2, M = t.n_m;
+  const int S = padded_len(H);
+  const int row = blockIdx.x, r = blockIdx.y, tid = threadIdx.x;
+  cplx<double>* tws = buf + (NB + kFftRowBatch) * S;
+  fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
+  for (int i = tid; i < NFI * S; i += T) buf[i] = {0.0, 0.0};
+  __syncthreads();
+  const double* frow = a.Fs64 + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
+                       (int64_t)r * 2 * NFI;
+  for (int e = tid; e < M * NFI; e += T) {
+    const int k = e / NFI, f = e - k * NFI;
+    const double2 x = __ldg(reinterpret_cast<const double2*>(frow + k * a.fs_m) + f);
+    buf[f * S + pad16(k)] = {x.x, x.y};
+  }
+  __syncthreads();
+  for (int f = tid / 32; f < NFI; f += T / 32)
+    c2r_prepare_nl(buf + f * S, H, t.twiddle, tid % 32, 32);
+  __syncthreads();
+  fft_rows<true>(buf, buf + NB * S, NFI, H, S, t.fft_radix, t.fft_nstages, tws);
+  __syncthreads();
+
+  const bool bnd = r == 0 || r == a.n_r - 1;
+  AnelLevel<double> L;
+  L.R = a.r[r];
+  L.or1 = a.or1[r];
+  L.or2 = a.or2[r];
+  L.or4 = a.or4[r];
+  L.beta = a.beta[r];
+  L.orho1 = a.orho1[r];
+  L.otemp1 = a.otemp1[r];
+  L.visc = a.visc[r];
+  L.lam = a.lambda_[r];
+  L.LF = a.LFfac;
+  L.vhf = a.ViscHeatFac;
+  L.ohm = a.OhmLossFac;
+  const double ost2 = t.ost2[row], cosn = t.cosn[row], orho2 = a.orho2[r];
+  const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
+  double mr = 0.0, mh = 0.0;
+  for (int i = tid; i < H; i += T) {
+    const int si = pad16(i);
+    cplx<double> zin[NFI];
+#pragma unroll
+    for (int f = 0; f < NFI; ++f) zin[f] = buf[f * S + si];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {  // grid points 2i and 2i+1
+      double v[NFI];
+#pragma unroll
+      for (int f = 0; f < NFI; ++f) v[f] = h ? zin[f].y : zin[f].x;
+      if (bnd) {
+#pragma unroll
+        for (int f = 0; f <= 10; ++f) v[f] = 0.0;  // velocity, derivatives, cvr
+      }
+      v[8] *= ost2;  // dvtdp, dvpdp: torpol_to_dphspat's 1/sin^2
+      v[9] *= ost2;
+      double vr2, vh2;
+      if constexpr (MAG)
+        courant_point(a.cour_mode, v[0], v[1], v[2], v[F::IB], v[F::IB + 1], v[F::IB + 2], L.or2,
+                      L.or4, L.orho1, orho2, ost2, L.LF, a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+      else
+        courant_point(0, v[0], v[1], v[2], 0.0, 0.0, 0.0, L.or2, L.or4, L.orho1, orho2, ost2, L.LF,
+                      a.cf2, a.af2, valri2, valhi2, vr2, vh2);
+      mr = fmax(mr, vr2);
+      mh = fmax(mh, vh2);
+      if (!bnd) {
+        double o[NFO];
+        anel_point<double, MAG, CHEM>(v, L, ost2, cosn, o);
+        // complex element i (points 2i, 2i+1) belongs to this thread alone
+#pragma unroll
+        for (int q = 0; q < NFO; ++q) {
+          if (h) buf[q * S + si].y = o[q];
+          else buf[q * S + si].x = o[q];
+        }
+      }
+    }
+  }
+  const double vmr = block_max(mr, red);
+  if (tid == 0) atomic_max_pos(&a.vr2max[r], vmr);
+  const double vmh = block_max(mh, red);
+  if (tid == 0) atomic_max_pos(&a.vh2max[r], vmh);
+  if (bnd) return;  // boundary levels: Courant only
+  __syncthreads();
+  fft_rows<false>(buf, buf + NB * S, NFO, H, S, t.fft_radix, t.fft_nstages, tws);
+  __syncthreads();
+  const double ws = t.wq[row] / N, wv = t.wq_v[row] / N;
+  double* Gr = a.G64 + (int64_t)(row & 1) * a.g_h + (int64_t)(row >> 1) * a.g_j +
+               (int64_t)(r - 1) * a.g_level;
+  for (int e = tid; e < M * NFO; e += T) {
+    const int k = e / NFO, o = e - k * NFO;
+    const cplx<double>* z = buf + o * S;
+    const cplx<double> X = r2c_post(z[pad16(k)], z[pad16((H - k) % H)], k, t.twiddle);
+    const double w = F::radial(o) ? ws : wv;
+    reinterpret_cast<double2*>(Gr + k * a.g_m)[o] = make_double2(w * X.x, w * X.y);
+  }
+}
+
+size_t nl_anel_f64_smem(int n_phi, bool mag, bool chem) {
+  const int nfi = 12 + (chem ? 1 : 0) + (mag ? 6 : 0), nfo = 7 + (mag ? 3 : 0) + (chem ? 3 : 0);
+  const int NB = std::max(nfi, nfo);
+  const size_t sm =
+      ((size_t)(NB + kFftRowBatch) * padded_len(n_phi / 2) + n_phi / 2) * sizeof(double2);
+  return sm <= 227 * 1024 - 32 * sizeof(double) ? sm : 0;
+}
+
+template <bool MAG, bool CHEM>
+static int launch_nl_anel_f64_t(const NlAnelArgs& a, cudaStream_t st) {
+  const size_t sm = nl_anel_f64_smem(a.t.n_phi, MAG, CHEM);
+  MT_REQUIRE(sm > 0, MT_ERR_UNSUPPORTED, "n_phi too large for the FP64 anelastic phi stage");
+  auto kern = k_nl_anel_f64<MAG, CHEM>;
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 grid(a.t.n_theta, a.n_r);
+  kern<<<grid, kNlAnelThreads, sm, st>>>(a);
+  MT_CHECK_CUDA(cudaGetLastError());
+  return MT_OK;
+}
+
+int launch_nl_anel_f64(bool mag, bool chem, const NlAnelArgs& a, cudaStream_t st) {
+  if (mag)
+    return chem ? launch_nl_anel_f64_t<true, true>(a, st)
+                : launch_nl_anel_f64_t<true, false>(a, st);
+  return chem ? launch_nl_anel_f64_t<false, true>(a, st)
+              : launch_nl_anel_f64_t<false, false>(a, st);
 }
 
 int launch_nl_bouss(bool mag, bool chem, const NlBoussArgs& a, cudaStream_t st) {

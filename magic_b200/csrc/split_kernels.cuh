@@ -95,8 +95,17 @@ struct NlAnelArgs {
   int cour_mode;
   double cf2, af2, valfac;
   unsigned long long *vr2max, *vh2max;
+  // FP64 rows of the digit-split stage (k_nl_anel_f64), in place of Fs and G:
+  //   Fs64[m][north|south][theta pair][level * 2 nfi + 2 f + re/im]
+  //   G64[m][north|south][theta pair][(level - 1) * g_level + 2 o + re/im]
+  const double* Fs64;
+  double* G64;
 };
 int launch_nl_anel_split(bool mag, bool chem, const NlAnelArgs& a, cudaStream_t st);
+// FP64 anelastic phi stage; its dynamic shared memory (0 where n_phi is too
+// long for one CTA's buffers)
+int launch_nl_anel_f64(bool mag, bool chem, const NlAnelArgs& a, cudaStream_t st);
+size_t nl_anel_f64_smem(int n_phi, bool mag, bool chem);
 
 // phi stage of the split drop-in transforms (split_transforms.cu); rows are
 // (column b, field f), r = b * nf + f

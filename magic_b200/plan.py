@@ -532,8 +532,11 @@ class Plan:
                 l_mag=True, l_chem=False, damp=True, out=None, work=None):
         """Anelastic nonlinear stage (magic_torch/step_time.py:1215-1475: transforms,
         get_nl_anel with viscous and Ohmic heating, forward transforms, CFL): fused into
-        the tcgen05 pack/GEMM and FP32 phi kernels on split-precision plans, composed
-        from the FP64 kernels on FP64 and digit-split (ozaki) plans.
+        the tcgen05 pack/GEMM and FP32 phi kernels on split-precision plans, into the
+        int8 digit-plane GEMMs and an FP64 phi kernel on digit-split (ozaki) plans, and
+        composed from the FP64 kernels on FP64 plans (and on digit-split plans whose
+        n_phi is too long for the fused phi stage's shared-memory buffers, e.g. the
+        magnetic case at n_phi = 1152).
 
         ``fields``: dict of spectral (lm_max, n_r) complex128 arrays w, dw, ddw, z, dz, s
         (+ b, db, ddb, aj, dj if l_mag, xi if l_chem).  ``prof``: r, or1, or2, or4, beta,
@@ -543,11 +546,11 @@ class Plan:
         """
         w = fields["w"]
         n_r = w.shape[1]
-        if self.precision in ("fp64", "ozaki"):
+        L = _lib.lib()
+        need = L.mt_nl_anel_workspace(self._h, n_r, int(l_mag), int(l_chem)) if n_r >= 3 else 0
+        if self.precision == "fp64" or (self.precision == "ozaki" and need == 0):
             return self._nl_anel_composed(fields, prof, LFfac, ViscHeatFac, OhmLossFac, courfac,
                                           alffac, opm, l_mag, l_chem, damp, out)
-        L = _lib.lib()
-        need = L.mt_nl_anel_workspace(self._h, n_r, int(l_mag), int(l_chem))
         if need == 0:
             raise MagicError("nl_anel needs n_r >= 3")
         names = ["w", "dw", "ddw", "z", "dz", "s"] + (["b", "db", "ddb", "aj", "dj"] if l_mag

@@ -485,11 +485,12 @@ class AnelasticStep(BoussinesqStep):
 
     @property
     def work(self):
-        """Workspace of the fused (split-precision) anelastic stage; the FP64 and
-        digit-split plans compose the stage from the FP64 kernels and need none."""
+        """Workspace of the fused (split or digit-split) anelastic stage; FP64 plans
+        compose the stage from the FP64 kernels and need none (the plan reports 0
+        where the digit-split stage composes too)."""
         if self._work is None:
             n = self.plan.nl_anel_workspace(self.n_r, self.l_mag, False) \
-                if self.plan.precision == "split" else 0
+                if self.plan.precision in ("split", "ozaki") else 0
             self._work = torch.empty(max(int(n), 1), dtype=torch.uint8, device=self.device)
         return self._work
 

@@ -1,9 +1,10 @@
-"""GPU parity of the split-precision fused anelastic stage (bf16x3 tcgen05
-Legendre GEMMs, FP32 phi stage with get_nl_anel, viscous and Ohmic heating)
-against the FP64 oracle restatement of radial_loop_anel
-(magic_torch/step_time.py:1215-1475).
+"""GPU parity of the fused anelastic stages against the FP64 oracle
+restatement of radial_loop_anel (magic_torch/step_time.py:1215-1475): the
+split-precision stage (bf16x3 tcgen05 Legendre GEMMs, FP32 phi stage with
+get_nl_anel, viscous and Ohmic heating), the digit-split stage (int8
+digit-plane GEMMs, FP64 phi stage) and the FP64 composition.
 
-Tolerance: relative to the output's scale (the vector pair's max(|S|, |T|)
+Split tolerance: relative to the output's scale (the vector pair's max(|S|, |T|)
 for the S/T outputs), 2e-5 up to l_max = 127 and 5e-5 above, as for the
 Boussinesq stage; Courant steps 1e-5.  The l_max = 383 case (n_phi = 1152,
 block FFT) is the anelastic benchmark configuration's resolution with a few
@@ -113,3 +114,85 @@ def test_fp64_anel_stage_matches_oracle(l_max, minc, N, l_mag, l_chem):
         assert np.abs(got - ref[k]).max() / scale < tol, k
     assert np.abs(dt.cpu().numpy() - rdt).max() / np.abs(rdt).max() < 1e-12
     assert np.abs(dh.cpu().numpy() - rdh).max() / np.abs(rdh).max() < 1e-12
+
+
+OZAKI_CASES = [
+    (16, 1, 5, True, False),
+    (32, 4, 6, True, True),
+    (20, 1, 5, False, True),
+    (42, 1, 4, False, False),
+    (255, 1, 3, True, True),
+    (383, 1, 3, False, False),
+]
+
+
+@pytest.mark.parametrize("l_max,minc,N,l_mag,l_chem", OZAKI_CASES)
+def test_ozaki_anel_stage_matches_oracle(l_max, minc, N, l_mag, l_chem):
+    """Digit-split (ozaki) plans fuse the anelastic stage: the split stage's row
+    programs on the int8 digit-plane GEMMs and the FP64 phi kernel k_nl_anel_f64.
+    Tolerance 5e-13 l_max^2 of each output's scale, as for the digit-split
+    Boussinesq stage (the digits keep 41 bits of each operand row's largest value;
+    the analysis rows' 1/sin^2 weight makes the polar rows the largest); Courant
+    steps likewise.  The l_max = 383 case is the anelastic configuration's grid
+    (n_theta 576, n_phi 1152, block FFT).  Measured on B200: 2e-12 ... 4.4e-11
+    up to l_max = 42, 2.1e-8 (Advt; bound 3.3e-8) at l_max = 255, 8.7e-10 (VSr)
+    at l_max = 383; heat 1.3e-12 ... 2.8e-12 throughout."""
+    from magic_b200 import Plan
+
+    g = og.Grid(l_max, minc)
+    p = Plan(l_max, minc, precision="ozaki")
+    need = p.nl_anel_workspace(N, l_mag, l_chem)
+    assert need > 0, "the fused digit-split stage should cover this grid"
+    rng = np.random.default_rng(13 * l_max + N)
+    f = _fields(g, N, rng, l_mag, l_chem)
+    prof = ostage.anel_profiles(N, l_max=l_max)
+    LF, vhf, ohm, cf, af, opm = 200.0, 0.3, 0.2, 2.5, 1.0, 0.2
+    ref, rdt, rdh = ostage.nl_anel_stage(g, f, prof, LF, vhf, ohm, cf, af, opm, l_mag, l_chem)
+    cu = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()
+    work = torch.zeros(need, dtype=torch.uint8, device="cuda")
+    out, dt, dh = p.nl_anel({k: cu(v) for k, v in f.items()}, {k: cu(v) for k, v in prof.items()},
+                            LF, vhf, ohm, cf, af, opm, l_mag=l_mag, l_chem=l_chem, work=work)
+    torch.cuda.synchronize()
+    assert p.device_status(work) == 0, "device wait timed out"
+    assert set(out) == set(ref)
+    tol = 5e-13 * l_max ** 2
+    worst = {}
+    for k in ref:
+        got = out[k].cpu().numpy()
+        assert np.all(got[:, 0] == 0) and np.all(got[:, -1] == 0), k
+        scale = np.abs(ref[k]).max()
+        if k in PAIR:
+            scale = max(scale, np.abs(ref[PAIR[k]]).max())
+        worst[k] = np.abs(got - ref[k]).max() / scale
+    print("ozaki anel stage errors", {k: f"{v:.2e}" for k, v in worst.items()})
+    for k, v in worst.items():
+        assert v < tol, (k, v)
+    assert np.abs(dt.cpu().numpy() - rdt).max() / np.abs(rdt).max() < tol
+    assert np.abs(dh.cpu().numpy() - rdh).max() / np.abs(rdh).max() < tol
+
+
+def test_ozaki_anel_stage_falls_back_where_phi_buffers_do_not_fit():
+    """The magnetic stage at n_phi = 1152 needs more shared memory than a CTA has
+    for the FP64 phi stage: the entry point reports it (workspace 0) and the plan
+    composes the stage from the FP64 kernels, to the FP64 plan's tolerance."""
+    from magic_b200 import Plan
+
+    l_max, N = 383, 3
+    g = og.Grid(l_max, 1)
+    p = Plan(l_max, 1, precision="ozaki")
+    assert p.nl_anel_workspace(N, True, False) == 0
+    rng = np.random.default_rng(5)
+    f = _fields(g, N, rng, True, False)
+    prof = ostage.anel_profiles(N, l_max=l_max)
+    args = (200.0, 0.3, 0.2, 2.5, 1.0, 0.2)
+    ref, rdt, _ = ostage.nl_anel_stage(g, f, prof, *args, True, False)
+    cu = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()
+    out, dt, _ = p.nl_anel({k: cu(v) for k, v in f.items()}, {k: cu(v) for k, v in prof.items()},
+                           *args, l_mag=True, l_chem=False)
+    torch.cuda.synchronize()
+    for k in ref:
+        scale = np.abs(ref[k]).max()
+        if k in PAIR:
+            scale = max(scale, np.abs(ref[PAIR[k]]).max())
+        assert np.abs(out[k].cpu().numpy() - ref[k]).max() / scale < 4e-12, k
+    assert np.abs(dt.cpu().numpy() - rdt).max() / np.abs(rdt).max() < 1e-12
