@@ -299,10 +299,11 @@ def run_anel(args, rank, world):
     levels, standard (w, p) form; polytropic background with 5 density scale
     heights and index 2, Ek 1e-4, Ra 3e6, Pr 1, no magnetic field, stress-free
     boundaries with the angular-momentum corrections, dt 1e-6; seeded
-    perturbations |c_lm| ~ 1e-3 (l+1)^-2), through magic_b200.step.AnelasticStep:
-    the fused split-precision anelastic stage, beside the FP64 stage (composed
-    from the FP64 transform kernels as the reference composes it) and the fused
-    digit-split stage, all with the same FP64 solves; device-timed with the state resident (2.9 GB of spectral
+    perturbations |c_lm| ~ 1e-3 (l+1)^-2), through magic_b200.step.AnelasticStep
+    with the stage of --precision (default the fused digit-split stage), beside
+    the other two (unless --no-alt): the fused split-precision stage and the
+    FP64 stage (composed from the FP64 transform kernels as the reference
+    composes it), all with the same FP64 solves; device-timed with the state resident (2.9 GB of spectral
     arrays, larger than L2)."""
     from magic_b200.step import AnelasticStep
 
@@ -331,47 +332,47 @@ def run_anel(args, rank, world):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / nsteps
 
-    st = build("split")
+    main = args.precision
+    st = build(main)
     with ClockSampler(dev) as clocks:
         ms = timed(st, args.steps)
     ours, every = count_launches(lambda: st.step())
     del st
     torch.cuda.empty_cache()
-    st64 = build("fp64")
-    n64 = max(1, min(args.steps, 3))
-    ms64 = timed(st64, n64)
-    del st64
-    torch.cuda.empty_cache()
-    stoz = build("ozaki")
-    noz = max(1, min(args.steps, 5))
-    msoz = timed(stoz, noz)
-    del stoz
-    torch.cuda.empty_cache()
+    what = {"split": "the fused split-precision stage (bf16x3 tcgen05 GEMMs, FP32 phi stage)",
+            "ozaki": "the fused digit-split stage (int8 digit-plane GEMMs, FP64 phi stage; "
+                     "~1e-12 of scale)",
+            "fp64": "the FP64 stage (composed from the FP64 transform kernels)"}
+    alts = {}
+    for prec in ([] if args.no_alt else [q for q in ("fp64", "split", "ozaki") if q != main]):
+        sta = build(prec)
+        na = max(1, min(args.steps, 3 if prec == "fp64" else 5))
+        msa = timed(sta, na)
+        alts[prec] = {"value": 1000.0 / msa, "unit": "steps/s", "ms_per_step": msa, "steps": na,
+                      "what": "the same steps with " + what[prec]}
+        del sta
+        torch.cuda.empty_cache()
+    if "fp64" in alts:
+        alts["fp64"]["speedup"] = alts["fp64"]["ms_per_step"] / ms
+    dtype = {"split": "bf16x3/f32 stage, f64 solves", "ozaki": "int8 digits/f64 stage, f64 solves",
+             "fp64": "f64"}[main]
     if rank == 0:
         print(json.dumps({"metric": "anelastic CNAB2 steps/s @lmax=383 vs FP64 stage, 1 B200",
                           "value": 1000.0 / ms, "unit": "steps/s", "n_gpus": 1,
                           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                          "dtype": "bf16x3/f32 stage, f64 solves", "data": "synthetic",
+                          "dtype": dtype, "data": "synthetic",
                           "config": {"workload": "anelastic convection, whole CNAB2 step "
                                                  "(Chebyshev, standard (w, p) form, "
-                                                 "stress-free + AM corrections, split stage)",
+                                                 "stress-free + AM corrections), " + what[main],
+                                     "stage": main,
                                      "l_max": l_max, "n_theta": 576, "n_phi": 1152,
                                      "n_r": n_r, "strat": 5.0, "polind": 2.0, "ek": 1e-4,
                                      "ra": 3e6, "pr": 1.0, "dt": 1e-6, "l_mag": False,
                                      "l2": "state larger than L2", "parallelism": "replicas"},
                           "gpu_launches": ours * args.steps,
                           "kernels_per_step": {"library": ours, "all": every},
-                          "fp64_stage": {"value": 1000.0 / ms64, "unit": "steps/s",
-                                         "ms_per_step": ms64, "steps": n64,
-                                         "speedup": ms64 / ms,
-                                         "what": "the same steps with the FP64 anelastic stage"},
-                          "ozaki_stage": {"value": 1000.0 / msoz, "unit": "steps/s",
-                                          "ms_per_step": msoz, "steps": noz,
-                                          "speedup_vs_fp64": ms64 / msoz,
-                                          "what": "the same steps with the fused digit-split "
-                                                  "anelastic stage (int8 digit-plane GEMMs, "
-                                                  "FP64 phi stage; ~1e-12 of scale)"},
+                          **{f"{k}_stage": v for k, v in alts.items()},
                           "clocks": clocks.summary()}), flush=True)
 
 
