@@ -957,15 +957,21 @@ __global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
 }
 
 // The same update with the coupled solve on the FP64 tensor pipe, for
-// 2 n_r <= 256: CTA = 16 orders (4 m-tiles) of one degree, 8 warps.  The
-// rows' right-hand sides (w part, then p part, row stride fs) are the A
-// operand of solve_tile_dmma with the 2 n_r x 2 n_r operator streamed
-// through shared memory in 16-row chunks; the solution overwrites them.
-// Derivatives: thread = (4-row group, level), each D coefficient serving 4 rows.
+// 2 n_r <= 64 kNt (kNt n-tiles of 8 levels per warp): CTA = 16 orders (4
+// m-tiles) of one degree, 8 warps.  The rows' right-hand sides (w part, then p
+// part, row stride fs) are the A operand of solve_tile_dmma with the
+// 2 n_r x 2 n_r operator streamed through shared memory in 16-row chunks; the
+// solution overwrites them.  Derivatives: thread = (4-row group, level), each
+// D coefficient serving 4 rows.  kNt = 4 covers n_r <= 128 (two CTAs per SM by
+// registers), kNt = 6 n_r <= 192 (e.g. the 129 Chebyshev levels of the
+// anelastic benchmark; its shared memory allows one CTA per SM anyway).
 constexpr int kWpDmmaThreads = 256;
 constexpr int kWpDmmaMaxR = 128;
+constexpr int kWpDmmaWideMaxR = 192;
 
-__global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, int fs) {
+template <int kNt>
+__global__ void __launch_bounds__(kWpDmmaThreads, kNt == 4 ? 2 : 1)
+    k_update_wp_dmma(WpArgs a, int fs) {
   extern __shared__ __align__(16) double2 wpd[];
   __shared__ int lm_row[4 * kRows];
   constexpr int rows = 4 * kRows;
@@ -1004,7 +1010,7 @@ __global__ void __launch_bounds__(kWpDmmaThreads, 2) k_update_wp_dmma(WpArgs a, 
       f[j] = zero;
     }
   } else {
-    solve_tile_dmma<4>(Ml, n2, a.ldm, fs, f, mbuf, 4, mc0);
+    solve_tile_dmma<kNt>(Ml, n2, a.ldm, fs, f, mbuf, 4, mc0);
   }
   __syncthreads();
   const int groups = (nrow + kRows - 1) / kRows;
@@ -1485,16 +1491,16 @@ int mt_update_wp(const mt_plan* p, int n_r, const mt_wp_update* u, const mt_lop*
   a.D2 = radial_op_view(D2);
   a.D3 = radial_op_view(D3);
   a.P0 = radial_op_view(P0);
-  if (n_r <= kWpDmmaMaxR) {
+  if (n_r <= kWpDmmaWideMaxR) {
     // tensor-pipe tiling: rows 4 (mod 8) double2 apart (conflict-free A
     // fragments), the operator's 16-row chunks double-buffered
     const int fs = 2 * n_r + ((4 - 2 * n_r) & 7);
     const size_t sm = (size_t)4 * kRows * fs * sizeof(double2) +
                       (size_t)2 * kKc * a.ldm * sizeof(double);
-    MT_CHECK_CUDA(cudaFuncSetAttribute(k_update_wp_dmma,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    auto kern = n_r <= kWpDmmaMaxR ? k_update_wp_dmma<4> : k_update_wp_dmma<6>;
+    MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const dim3 grid((p->n_m + 4 * kRows - 1) / (4 * kRows), p->l_max + 1);
-    k_update_wp_dmma<<<grid, kWpDmmaThreads, sm, (cudaStream_t)stream>>>(a, fs);
+    kern<<<grid, kWpDmmaThreads, sm, (cudaStream_t)stream>>>(a, fs);
     MT_CHECK_CUDA(cudaGetLastError());
     return MT_OK;
   }

@@ -398,17 +398,21 @@ def test_update_wp_matches_reference():
 
 
 @pytest.mark.parametrize("l_max,minc,n_r,ktopv,scale", [(127, 1, 65, 2, 1.0), (32, 4, 33, 1, 1.0),
-                                                         (16, 1, 129, 2, 1e2)])
+                                                         (16, 1, 129, 2, 1e2),
+                                                         (8, 1, 193, 2, 3e3)])
 def test_update_wp_vs_oracle(l_max, minc, n_r, ktopv, scale):
     """l_max = 127 on 65 Chebyshev levels (no-slip) and l_max = 32, minc = 4 on 33
     levels (stress-free) with anelastic-like profiles, against the oracle's LU
-    solves (the tensor-pipe tiling, n_r <= 128); l_max = 16 on 129 levels takes
-    the FMA tiling.  The coupled Chebyshev operator is far worse conditioned than
-    the scalar ones (its p rows carry d3rMat): the tolerances are relative to each
-    array's largest value, 1e-11 for the fields and 1e-10 for the terms that
-    apply D2 / D3 to the new w, scaled by 100 at 129 levels (the conditioning
-    grows ~ n_r^4 and the D3 norm ~ n_r^6; measured there: fields <= 5.0e-12,
-    ddw 6.9e-10, p_impl 3.4e-9)."""
+    solves (the tensor-pipe tiling with four n-tiles per warp, n_r <= 128);
+    l_max = 16 on 129 levels takes the six-tile variant (n_r <= 192, the
+    anelastic benchmark's levels), l_max = 8 on 193 levels the FMA tiling.  The
+    coupled Chebyshev operator is far worse conditioned than the scalar ones (its
+    p rows carry d3rMat): the tolerances are relative to each array's largest
+    value, 1e-11 for the fields and 1e-10 for the terms that apply D2 / D3 to the
+    new w, scaled by 100 at 129 levels and 3000 at 193 (the conditioning grows
+    ~ n_r^4 and the D3 norm ~ n_r^6; measured at 129 levels: fields <= 5.0e-12,
+    ddw 6.9e-10, p_impl 3.4e-9; at 193: fields <= 2.7e-11, ddw 4.8e-9, p_impl
+    7.7e-8)."""
     from magic_b200 import Plan
     from magic_b200 import implicit as I
     from magic_b200.radial import RadialScheme
