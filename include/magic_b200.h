@@ -233,10 +233,10 @@ MT_API int mt_nl_bouss(const mt_plan* plan, int n_r, const mt_bouss_in* in,
  * Requires a plan created with MT_PREC_SPLIT (tcgen05 bf16x3 GEMMs, FP32 phi
  * stage) or MT_PREC_OZAKI (int8 digit-plane GEMMs, FP64 phi stage, ~1e-12 of
  * scale); FP64 plans compose the drop-in transforms and mt_get_nl_anel
- * exactly as radial_loop_anel does.  On MT_PREC_OZAKI plans whose n_phi is
- * too long for the FP64 phi stage's shared-memory buffers (the magnetic case
- * at n_phi = 1152) mt_nl_anel_workspace returns 0 and mt_nl_anel
- * MT_ERR_UNSUPPORTED: compose the stage there too.
+ * exactly as radial_loop_anel does.  The FP64 phi stage keeps the rows of
+ * one (theta row, level) in shared memory; where they would not fit (no plan
+ * within the n_phi limit of mt_plan_create) mt_nl_anel_workspace returns 0
+ * and mt_nl_anel MT_ERR_UNSUPPORTED.
  * Inputs: spectral (lm_max, ld) complex over n_r levels; b .. dj NULL
  * without magnetic field, xi NULL without composition. */
 typedef struct {

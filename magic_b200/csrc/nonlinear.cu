@@ -484,48 +484,149 @@ static int launch_nl_bouss_io(bool mag, bool chem, const NlBoussArgs& a, cudaStr
 
 // ------------------------------------------------------- fused anelastic (FP64)
 
-// The phi stage of the digit-split anelastic radial loop.  One CTA per
-// (theta row, level) with the block FFT: the synthesis wrote this hemisphere's
+// In-place mixed-radix FFT stages of the FP64 anelastic phi stage.  Stage
+// (radix R, span Ns) has the butterflies (row, blk, j), j < Ns, over the
+// elements blk R Ns + j + q Ns, q < R, of a row (row stride S; element i at
+// slot anel_slot(i, sw)).  Decimation in frequency (DIF): DFT over q, then
+// element q times w^(q j), w = exp(-2 pi i / (R Ns)) (conjugate for INV);
+// decimation in time (DIT): the twiddle first, then the DFT.  DIF stages from
+// the largest span down take a row in natural order to its transform in
+// mixed-radix digit-reversed order; DIT stages from span 1 up are the
+// transpose of that chain, so they take digit-reversed input to a
+// natural-order transform.  The synthesis runs DIF (inverse), the analysis DIT
+// (forward): the grid points in between are permuted along phi, which the
+// point products and Courant maxima do not see.  A thread takes one butterfly
+// position in the rows of a row group, so that its R - 1 twiddles (read from
+// the plan's table tw[n] = exp(-2 pi i n / (2 H)) through L1) serve several
+// rows.
+
+// Slot of element i in a row: the low three bits XORed with the next three
+// (sw = 7 when H is a multiple of 8, else 0), so that the stride-8 accesses of
+// a span-1 radix-8 stage fall on distinct bank quads while aligned runs of
+// eight stay conflict-free.
+__device__ __forceinline__ int anel_slot(int i, int sw) { return i ^ ((i >> 3) & sw); }
+
+template <int R, bool INV, bool DIF>
+__device__ __forceinline__ void fft_stage_ip(cplx<double>* buf, int nrows, int H, int S, int sw,
+                                             int Ns, const double2* __restrict__ tw) {
+  const int nbr = H / R, step = 2 * H / (R * Ns);
+  const int G = max(1, min(nrows, (int)blockDim.x / nbr));  // row groups
+  const float rcp_nbr = 1.0f / (float)nbr, rcp_ns = 1.0f / (float)Ns;
+  for (int it = threadIdx.x; it < nbr * G; it += blockDim.x) {
+    const int g = fdiv(it, rcp_nbr), i = it - g * nbr;
+    const int blk = fdiv(i, rcp_ns), j = i - blk * Ns;
+    const int base = blk * R * Ns + j;
+    cplx<double> w[R];
+    if (j > 0) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        const double2 t = __ldg(&tw[q * j * step]);
+        w[q] = {t.x, INV ? -t.y : t.y};
+      }
+    }
+    for (int row = g; row < nrows; row += G) {
+      cplx<double>* x = buf + row * S;
+      cplx<double> v[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[q] = x[anel_slot(base + q * Ns, sw)];
+      if (!DIF && j > 0) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmul(v[q], w[q]);
+      }
+      dft_small<R, INV>(v);
+      if (DIF && j > 0) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmul(v[q], w[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) x[anel_slot(base + q * Ns, sw)] = v[q];
+    }
+  }
+  __syncthreads();
+}
+
+// All stages of the rows: DIF (INV, synthesis) or DIT (forward, analysis) with
+// the plan's radices rad[0..nst) (span of stage s = rad[0] ... rad[s - 1]).
+template <bool INV>
+__device__ __forceinline__ void fft_rows_ip(cplx<double>* buf, int nrows, int H, int S, int sw,
+                                            const int* rad, int nst,
+                                            const double2* __restrict__ tw) {
+  constexpr bool DIF = INV;
+  int Ns = DIF ? H : 1;
+  for (int u = 0; u < nst; ++u) {
+    const int s = DIF ? nst - 1 - u : u;
+    const int r = rad[s];
+    if (DIF) Ns /= r;
+    switch (r) {
+      case 8: fft_stage_ip<8, INV, DIF>(buf, nrows, H, S, sw, Ns, tw); break;
+      case 4: fft_stage_ip<4, INV, DIF>(buf, nrows, H, S, sw, Ns, tw); break;
+      case 3: fft_stage_ip<3, INV, DIF>(buf, nrows, H, S, sw, Ns, tw); break;
+      case 2: fft_stage_ip<2, INV, DIF>(buf, nrows, H, S, sw, Ns, tw); break;
+      default: fft_stage_ip<5, INV, DIF>(buf, nrows, H, S, sw, Ns, tw); break;
+    }
+    if (!DIF) Ns *= r;
+  }
+}
+
+// The phi stage of the digit-split anelastic radial loop.  One CTA (256
+// threads) per (theta row, level): the synthesis wrote this hemisphere's
 // Fourier rows of the grid fields in FP64 (NlAnelArgs::Fs64; field order of
-// nl_point.cuh), the kernel inverse-transforms them, evaluates get_nl_anel
-// (magic_torch/get_nl_anel.py:63-136, viscous and Ohmic heating included) and
-// the Courant maxima (magic_torch/courant.py:25-77) at every grid point in
-// FP64, and forward-transforms the 10-13 products into the weighted rows the
-// analysis reads (NlAnelArgs::G64).  Velocity, its derivatives and cvr are
-// zero on the two boundary levels (radial_loop_anel synthesises them on the
-// bulk levels only, magic_torch/step_time.py:1233-1316); the phi-derivative
-// fields get their 1/sin^2(theta) factor here (torpol_to_dphspat,
-// magic_torch/sht.py:725-743).
-constexpr int kNlAnelThreads = 512;
+// nl_point.cuh), the kernel inverse-transforms them in place (fft_rows_ip),
+// evaluates get_nl_anel (magic_torch/get_nl_anel.py:63-136, viscous and Ohmic
+// heating included) and the Courant maxima (magic_torch/courant.py:25-77) at
+// every grid point in FP64, and forward-transforms the 10-13 products into the
+// weighted rows the analysis reads (NlAnelArgs::G64).  Shared memory holds
+// only the rows (max(nfi, nfo) x (H + 1) complex values; the odd row stride
+// puts consecutive rows on different banks), so that two CTAs share an SM
+// without magnetic field at n_phi = 1152.  Velocity, its derivatives and cvr
+// are zero on the two boundary levels (radial_loop_anel synthesises them on
+// the bulk levels only, magic_torch/step_time.py:1233-1316); the
+// phi-derivative fields get their 1/sin^2(theta) factor here
+// (torpol_to_dphspat, magic_torch/sht.py:725-743).
+constexpr int kNlAnelThreads = 256;
 
 template <bool MAG, bool CHEM>
-__global__ void __launch_bounds__(kNlAnelThreads) k_nl_anel_f64(NlAnelArgs a) {
+__global__ void __launch_bounds__(kNlAnelThreads, 2) k_nl_anel_f64(NlAnelArgs a) {
   using F = AnelFields<MAG, CHEM>;
-  constexpr int NFI = F::NFI, NFO = F::NFO, NB = F::NB, T = kNlAnelThreads;
+  constexpr int NFI = F::NFI, NFO = F::NFO, T = kNlAnelThreads;
   extern __shared__ double smem[];
   __shared__ double red[32];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem);
   const Tables& t = a.t;
-  const int N = t.n_phi, H = N / 2, M = t.n_m;
-  const int S = padded_len(H);
+  const int N = t.n_phi, H = N / 2, M = t.n_m, S = H + 1;
   const int row = blockIdx.x, r = blockIdx.y, tid = threadIdx.x;
-  cplx<double>* tws = buf + (NB + kFftRowBatch) * S;
-  fft_twiddles_to_smem(tws, H, t.twiddle, t.fft_radix, t.fft_nstages);
-  for (int i = tid; i < NFI * S; i += T) buf[i] = {0.0, 0.0};
-  __syncthreads();
+  const int sw = (H & 7) ? 0 : 7;
+  auto at = [&](int f, int i) -> cplx<double>& { return buf[f * S + anel_slot(i, sw)]; };
   const double* frow = a.Fs64 + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
                        (int64_t)r * 2 * NFI;
-  for (int e = tid; e < M * NFI; e += T) {
+  for (int e = tid; e < H * NFI; e += T) {
     const int k = e / NFI, f = e - k * NFI;
-    const double2 x = __ldg(reinterpret_cast<const double2*>(frow + k * a.fs_m) + f);
-    buf[f * S + pad16(k)] = {x.x, x.y};
+    cplx<double> z = {0.0, 0.0};
+    if (k < M) {
+      const double2 x = __ldg(reinterpret_cast<const double2*>(frow + k * a.fs_m) + f);
+      z = {x.x, x.y};
+    }
+    at(f, k) = z;
   }
   __syncthreads();
-  for (int f = tid / 32; f < NFI; f += T / 32)
-    c2r_prepare_nl(buf + f * S, H, t.twiddle, tid % 32, 32);
+  // real-row synthesis: Z[k], Z[H - k] from X[k], X[H - k] (c2r_pre)
+  for (int e = tid; e < NFI * (H / 2 + 1); e += T) {
+    const int f = e / (H / 2 + 1), k = e - f * (H / 2 + 1);
+    const int kc = H - k;
+    cplx<double> Xk = at(f, k);
+    if (k == 0) {
+      Xk.y = 0.0;
+      at(f, 0) = c2r_pre(Xk, cplx<double>{0.0, 0.0}, 0, t.twiddle);
+    } else {
+      const cplx<double> Xc = at(f, kc);
+      const cplx<double> Zk = c2r_pre(Xk, Xc, k, t.twiddle);
+      const cplx<double> Zc = c2r_pre(Xc, Xk, kc, t.twiddle);
+      at(f, k) = Zk;
+      if (kc != k) at(f, kc) = Zc;
+    }
+  }
   __syncthreads();
-  fft_rows<true>(buf, buf + NB * S, NFI, H, S, t.fft_radix, t.fft_nstages, tws);
-  __syncthreads();
+  fft_rows_ip<true>(buf, NFI, H, S, sw, t.fft_radix, t.fft_nstages, t.twiddle);
 
   const bool bnd = r == 0 || r == a.n_r - 1;
   AnelLevel<double> L;
@@ -545,12 +646,12 @@ __global__ void __launch_bounds__(kNlAnelThreads) k_nl_anel_f64(NlAnelArgs a) {
   const double valri2 = a.valfac / a.delxr2[r], valhi2 = a.valfac / a.delxh2[r];
   double mr = 0.0, mh = 0.0;
   for (int i = tid; i < H; i += T) {
-    const int si = pad16(i);
+    const int si = anel_slot(i, sw);
     cplx<double> zin[NFI];
 #pragma unroll
     for (int f = 0; f < NFI; ++f) zin[f] = buf[f * S + si];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {  // grid points 2i and 2i+1
+    for (int h = 0; h < 2; ++h) {  // the two real grid points of complex element i
       double v[NFI];
 #pragma unroll
       for (int f = 0; f < NFI; ++f) v[f] = h ? zin[f].y : zin[f].x;
@@ -572,7 +673,7 @@ __global__ void __launch_bounds__(kNlAnelThreads) k_nl_anel_f64(NlAnelArgs a) {
       if (!bnd) {
         double o[NFO];
         anel_point<double, MAG, CHEM>(v, L, ost2, cosn, o);
-        // complex element i (points 2i, 2i+1) belongs to this thread alone
+        // complex element i belongs to this thread alone
 #pragma unroll
         for (int q = 0; q < NFO; ++q) {
           if (h) buf[q * S + si].y = o[q];
@@ -587,15 +688,13 @@ __global__ void __launch_bounds__(kNlAnelThreads) k_nl_anel_f64(NlAnelArgs a) {
   if (tid == 0) atomic_max_pos(&a.vh2max[r], vmh);
   if (bnd) return;  // boundary levels: Courant only
   __syncthreads();
-  fft_rows<false>(buf, buf + NB * S, NFO, H, S, t.fft_radix, t.fft_nstages, tws);
-  __syncthreads();
+  fft_rows_ip<false>(buf, NFO, H, S, sw, t.fft_radix, t.fft_nstages, t.twiddle);
   const double ws = t.wq[row] / N, wv = t.wq_v[row] / N;
   double* Gr = a.G64 + (int64_t)(row & 1) * a.g_h + (int64_t)(row >> 1) * a.g_j +
                (int64_t)(r - 1) * a.g_level;
   for (int e = tid; e < M * NFO; e += T) {
     const int k = e / NFO, o = e - k * NFO;
-    const cplx<double>* z = buf + o * S;
-    const cplx<double> X = r2c_post(z[pad16(k)], z[pad16((H - k) % H)], k, t.twiddle);
+    const cplx<double> X = r2c_post(at(o, k), at(o, (H - k) % H), k, t.twiddle);
     const double w = F::radial(o) ? ws : wv;
     reinterpret_cast<double2*>(Gr + k * a.g_m)[o] = make_double2(w * X.x, w * X.y);
   }
@@ -604,8 +703,7 @@ __global__ void __launch_bounds__(kNlAnelThreads) k_nl_anel_f64(NlAnelArgs a) {
 size_t nl_anel_f64_smem(int n_phi, bool mag, bool chem) {
   const int nfi = 12 + (chem ? 1 : 0) + (mag ? 6 : 0), nfo = 7 + (mag ? 3 : 0) + (chem ? 3 : 0);
   const int NB = std::max(nfi, nfo);
-  const size_t sm =
-      ((size_t)(NB + kFftRowBatch) * padded_len(n_phi / 2) + n_phi / 2) * sizeof(double2);
+  const size_t sm = (size_t)NB * (n_phi / 2 + 1) * sizeof(double2);
   return sm <= 227 * 1024 - 32 * sizeof(double) ? sm : 0;
 }
 
@@ -615,6 +713,8 @@ static int launch_nl_anel_f64_t(const NlAnelArgs& a, cudaStream_t st) {
   MT_REQUIRE(sm > 0, MT_ERR_UNSUPPORTED, "n_phi too large for the FP64 anelastic phi stage");
   auto kern = k_nl_anel_f64<MAG, CHEM>;
   MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
   dim3 grid(a.t.n_theta, a.n_r);
   kern<<<grid, kNlAnelThreads, sm, st>>>(a);
   MT_CHECK_CUDA(cudaGetLastError());

@@ -534,9 +534,9 @@ class Plan:
         get_nl_anel with viscous and Ohmic heating, forward transforms, CFL): fused into
         the tcgen05 pack/GEMM and FP32 phi kernels on split-precision plans, into the
         int8 digit-plane GEMMs and an FP64 phi kernel on digit-split (ozaki) plans, and
-        composed from the FP64 kernels on FP64 plans (and on digit-split plans whose
-        n_phi is too long for the fused phi stage's shared-memory buffers, e.g. the
-        magnetic case at n_phi = 1152).
+        composed from the FP64 kernels on FP64 plans (and on a digit-split plan whose
+        phi rows would not fit one CTA's shared memory, which no plan within the
+        library's n_phi limit reaches).
 
         ``fields``: dict of spectral (lm_max, n_r) complex128 arrays w, dw, ddw, z, dz, s
         (+ b, db, ddb, aj, dj if l_mag, xi if l_chem).  ``prof``: r, or1, or2, or4, beta,
