@@ -599,15 +599,14 @@ __global__ void __launch_bounds__(kNlAnelThreads, 2) k_nl_anel_f64(NlAnelArgs a)
   auto at = [&](int f, int i) -> cplx<double>& { return buf[f * S + anel_slot(i, sw)]; };
   const double* frow = a.Fs64 + (int64_t)(row & 1) * a.fs_c + (int64_t)(row >> 1) * a.fs_j +
                        (int64_t)r * 2 * NFI;
+  // asynchronous 16-byte copies of the M wavenumbers (every thread keeps its
+  // copies in flight), zeros above
   for (int e = tid; e < H * NFI; e += T) {
     const int k = e / NFI, f = e - k * NFI;
-    cplx<double> z = {0.0, 0.0};
-    if (k < M) {
-      const double2 x = __ldg(reinterpret_cast<const double2*>(frow + k * a.fs_m) + f);
-      z = {x.x, x.y};
-    }
-    at(f, k) = z;
+    if (k < M) cp_async16(&at(f, k), reinterpret_cast<const double2*>(frow + k * a.fs_m) + f);
+    else at(f, k) = {0.0, 0.0};
   }
+  cp_async_wait_all();
   __syncthreads();
   // real-row synthesis: Z[k], Z[H - k] from X[k], X[H - k] (c2r_pre)
   for (int e = tid; e < NFI * (H / 2 + 1); e += T) {
