@@ -233,6 +233,71 @@ __device__ __forceinline__ void op_rows(const OpView& op, const double2* f, int 
   }
 }
 
+// (A f_r)[j] and (B f_r)[j] in one sweep when both operators share level j's
+// window (same width and first level: the dense Chebyshev operators), so that
+// each staged value feeds both; per output the same FMA chain as op_rows.
+// Falls back to two op_rows sweeps otherwise.
+__device__ __forceinline__ void op_rows2(const OpView& A, const OpView& B, const double2* f,
+                                         int fs, int j, double2 (&a)[kRows],
+                                         double2 (&b)[kRows]) {
+  const int k0 = __ldg(A.k0 + j);
+  if (A.W != B.W || __ldg(B.k0 + j) != k0) {
+    op_rows(A, f, fs, j, a);
+    op_rows(B, f, fs, j, b);
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) a[r] = b[r] = double2{0.0, 0.0};
+  for (int kk = 0; kk < A.W; ++kk) {
+    const double ca = __ldg(A.vals + (int64_t)kk * A.n_r + j);
+    const double cb = __ldg(B.vals + (int64_t)kk * B.n_r + j);
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const double2 v = f[r * fs + k0 + kk];
+      a[r].x = fma(ca, v.x, a[r].x);
+      a[r].y = fma(ca, v.y, a[r].y);
+      b[r].x = fma(cb, v.x, b[r].x);
+      b[r].y = fma(cb, v.y, b[r].y);
+    }
+  }
+}
+
+// The derivatives of the (w, p) update in one sweep where D1, D2, D3 share
+// level j's window: D1 w, D2 w, D3 w from the rows fw and D1 p from fp.
+__device__ __forceinline__ void op_rows_wp(const OpView& D1, const OpView& D2, const OpView& D3,
+                                           const double2* fw, const double2* fp, int fs, int j,
+                                           double2 (&d1)[kRows], double2 (&d2)[kRows],
+                                           double2 (&d3)[kRows], double2 (&dp)[kRows]) {
+  const int k0 = __ldg(D1.k0 + j);
+  if (D1.W != D2.W || D1.W != D3.W || __ldg(D2.k0 + j) != k0 || __ldg(D3.k0 + j) != k0) {
+    op_rows(D1, fw, fs, j, d1);
+    op_rows(D2, fw, fs, j, d2);
+    op_rows(D3, fw, fs, j, d3);
+    op_rows(D1, fp, fs, j, dp);
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) d1[r] = d2[r] = d3[r] = dp[r] = double2{0.0, 0.0};
+  for (int kk = 0; kk < D1.W; ++kk) {
+    const double c1 = __ldg(D1.vals + (int64_t)kk * D1.n_r + j);
+    const double c2 = __ldg(D2.vals + (int64_t)kk * D2.n_r + j);
+    const double c3 = __ldg(D3.vals + (int64_t)kk * D3.n_r + j);
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const double2 v = fw[r * fs + k0 + kk];
+      const double2 u = fp[r * fs + k0 + kk];
+      d1[r].x = fma(c1, v.x, d1[r].x);
+      d1[r].y = fma(c1, v.y, d1[r].y);
+      d2[r].x = fma(c2, v.x, d2[r].x);
+      d2[r].y = fma(c2, v.y, d2[r].y);
+      d3[r].x = fma(c3, v.x, d3[r].x);
+      d3[r].y = fma(c3, v.y, d3[r].y);
+      dp[r].x = fma(c1, u.x, dp[r].x);
+      dp[r].y = fma(c1, u.y, dp[r].y);
+    }
+  }
+}
+
 // Band factors of a banded per-degree operator set (null abd: dense form).
 struct BandView {
   const double* abd;
@@ -597,8 +662,7 @@ __global__ void __launch_bounds__(Bounds<kStaged, kNt == 2 ? 3 : 2>::kThreads,
     const int j = 2 * s.jp + h;
     if (j >= n_r) break;
     double2 d1[kRows], d2[kRows];
-    op_rows(a.D1, fr, fs, j, d1);
-    op_rows(a.D2, fr, fs, j, d2);
+    op_rows2(a.D1, a.D2, fr, fs, j, d1, d2);
     const double so = so_l * (a.so_r ? a.so_r[j] : 1.0);
     const double c1 = a.ib_r[j], c0 = (a.ic_r ? a.ic_r[j] : 0.0) + ic_l * a.ic_r2[j];
     const double ia = ia_l * a.ia_r[j];
@@ -1018,10 +1082,7 @@ __global__ void __launch_bounds__(kWpDmmaThreads, kNt == 4 ? 2 : 1)
     const int rg = e / n_r, j = e - rg * n_r;
     const double2* xw = f + rg * kRows * fs;
     double2 d1[kRows], d2[kRows], d3[kRows], dp[kRows];
-    op_rows(a.D1, xw, fs, j, d1);
-    op_rows(a.D2, xw, fs, j, d2);
-    op_rows(a.D3, xw, fs, j, d3);
-    op_rows(a.D1, xw + n_r, fs, j, dp);
+    op_rows_wp(a.D1, a.D2, a.D3, xw, xw + n_r, fs, j, d1, d2, d3, dp);
     const WpCoef c = wp_coef(a, l, j);
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
