@@ -1026,15 +1026,19 @@ __global__ void __launch_bounds__(kWpThreads) k_update_wp(WpArgs a) {
 // part, row stride fs) are the A operand of solve_tile_dmma with the
 // 2 n_r x 2 n_r operator streamed through shared memory in 16-row chunks; the
 // solution overwrites them.  Derivatives: thread = (4-row group, level), each
-// D coefficient serving 4 rows.  kNt = 4 covers n_r <= 128 (two CTAs per SM by
-// registers), kNt = 6 n_r <= 192 (e.g. the 129 Chebyshev levels of the
-// anelastic benchmark; its shared memory allows one CTA per SM anyway).
-constexpr int kWpDmmaThreads = 256;
+// D coefficient serving 4 rows.  kNt = 4 with 8 warps covers 2 n_r <= 256
+// (two CTAs per SM by registers); kNt = 6 with 9 warps covers 2 n_r <= 432 and
+// runs up to n_r = 192 (e.g. the 129 Chebyshev levels of the anelastic
+// benchmark; its shared memory allows one CTA per SM anyway).
+// The six-tile variant runs 9 warps: 129 levels give 33 n-tiles (at most four
+// per warp) and 4 x 129 derivative items (two rounds of 288 threads, where 256
+// threads would need a third round for four items).
 constexpr int kWpDmmaMaxR = 128;
 constexpr int kWpDmmaWideMaxR = 192;
+__host__ __device__ constexpr int wp_dmma_threads(int kNt) { return kNt == 4 ? 256 : 288; }
 
 template <int kNt>
-__global__ void __launch_bounds__(kWpDmmaThreads, kNt == 4 ? 2 : 1)
+__global__ void __launch_bounds__(wp_dmma_threads(kNt), kNt == 4 ? 2 : 1)
     k_update_wp_dmma(WpArgs a, int fs) {
   extern __shared__ __align__(16) double2 wpd[];
   __shared__ int lm_row[4 * kRows];
@@ -1558,10 +1562,11 @@ int mt_update_wp(const mt_plan* p, int n_r, const mt_wp_update* u, const mt_lop*
     const int fs = 2 * n_r + ((4 - 2 * n_r) & 7);
     const size_t sm = (size_t)4 * kRows * fs * sizeof(double2) +
                       (size_t)2 * kKc * a.ldm * sizeof(double);
-    auto kern = n_r <= kWpDmmaMaxR ? k_update_wp_dmma<4> : k_update_wp_dmma<6>;
+    const bool narrow = n_r <= kWpDmmaMaxR;
+    auto kern = narrow ? k_update_wp_dmma<4> : k_update_wp_dmma<6>;
     MT_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const dim3 grid((p->n_m + 4 * kRows - 1) / (4 * kRows), p->l_max + 1);
-    kern<<<grid, kWpDmmaThreads, sm, (cudaStream_t)stream>>>(a, fs);
+    kern<<<grid, wp_dmma_threads(narrow ? 4 : 6), sm, (cudaStream_t)stream>>>(a, fs);
     MT_CHECK_CUDA(cudaGetLastError());
     return MT_OK;
   }
