@@ -248,6 +248,7 @@ __device__ __forceinline__ void op_rows2(const OpView& A, const OpView& B, const
   }
 #pragma unroll
   for (int r = 0; r < kRows; ++r) a[r] = b[r] = double2{0.0, 0.0};
+#pragma unroll 4
   for (int kk = 0; kk < A.W; ++kk) {
     const double ca = __ldg(A.vals + (int64_t)kk * A.n_r + j);
     const double cb = __ldg(B.vals + (int64_t)kk * B.n_r + j);
@@ -278,6 +279,7 @@ __device__ __forceinline__ void op_rows_wp(const OpView& D1, const OpView& D2, c
   }
 #pragma unroll
   for (int r = 0; r < kRows; ++r) d1[r] = d2[r] = d3[r] = dp[r] = double2{0.0, 0.0};
+#pragma unroll 4
   for (int kk = 0; kk < D1.W; ++kk) {
     const double c1 = __ldg(D1.vals + (int64_t)kk * D1.n_r + j);
     const double c2 = __ldg(D2.vals + (int64_t)kk * D2.n_r + j);
