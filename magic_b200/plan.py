@@ -585,5 +585,5 @@ class Plan:
             work = self._work(need)
         check(L.mt_nl_anel(self._h, n_r, C.byref(ai), C.byref(ao), C.byref(ap), _ptr(dtr),
                            _ptr(dth), _ptr(work), work.numel(), self._stream()))
-        self._watch(work, "nl_anel")
+        self._watch(work, "nl_anel", fused=True)
         return out, dtr, dth
